@@ -1,0 +1,257 @@
+/*
+ * newton_b200.h -- C ABI of the B200-native rigid-contact XPBD step.
+ *
+ * The library replaces the hot path of Newton's rigid-body pipeline:
+ *   Model.collide(state, contacts)              newton/_src/sim/model.py:996-1022
+ *     -> CollisionPipeline.collide               newton/_src/sim/collide.py:902-1124
+ *   SolverXPBD.step(s_in, s_out, ctl, c, dt)    newton/_src/solvers/xpbd/solver_xpbd.py:259-764
+ *
+ * Every pointer inside the descriptor structs is a DEVICE pointer (CUDA global
+ * memory on the current device).  The structs themselves live in host memory
+ * and are read by the entry points before launching; nothing is retained
+ * between calls.  All launches go to the stream passed in (cudaStream_t given
+ * as void* so the header needs no CUDA include); no entry point synchronises
+ * the device, so every call can be captured into a CUDA graph.
+ *
+ * Return value of every entry point: 0 on success, a positive NB_ERR_* code
+ * otherwise (launch errors are reported as NB_ERR_CUDA).  Device-side
+ * conditions (contact overflow, non-finite state) are written as bits into
+ * the status word `status` (NB_STATUS_*), read back by the caller when it
+ * chooses to synchronise.
+ *
+ * Layouts (fp32 unless noted, "world" = independent scene, bodies / shapes /
+ * joints of a world are contiguous index ranges):
+ *   transform  7 floats  (px, py, pz, qx, qy, qz, qw)  -- wp.transform
+ *   twist      6 floats  (vx, vy, vz, wx, wy, wz)      -- wp.spatial_vector
+ *   mat33      9 floats  row-major
+ * Solver-format contacts are 5 float4 streams (SoA, 16-byte aligned):
+ *   rec0 = (point0.xyz, margin0)        point0 in body frame of shape0's body
+ *   rec1 = (point1.xyz, margin1)
+ *   rec2 = (normal.xyz, bits(shape0))   normal points from shape0 to shape1
+ *   rec3 = (offset0.xyz, bits(shape1))
+ *   rec4 = (offset1.xyz, bits(tag))     tag = (body_a_local+1) | (body_b_local+1)<<12
+ *                                       | sort_sub_key<<24 (local = index within the
+ *                                       world's body range, -1 for static shapes)
+ * World w owns contact slots [contact_cap_start[w], contact_cap_start[w+1]);
+ * its live contacts are the first world_contact_count[w] of them, ordered by
+ * the deterministic key (shape0, shape1, sort_sub_key) of
+ * newton/_src/geometry/contact_data.py:59-83.
+ */
+#ifndef NEWTON_B200_H
+#define NEWTON_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NB_ABI_VERSION 1
+
+enum {
+    NB_OK = 0,
+    NB_ERR_INVALID = 1,     /* bad argument / descriptor */
+    NB_ERR_CUDA = 2,        /* a CUDA call failed */
+    NB_ERR_UNSUPPORTED = 3, /* model feature not supported by this build */
+    NB_ERR_CAPACITY = 4     /* a fixed capacity is too small */
+};
+
+enum {
+    NB_STATUS_CONTACT_OVERFLOW = 1u << 0, /* public contact buffer too small   */
+    NB_STATUS_NONFINITE = 1u << 1,        /* NaN/Inf body state after a step   */
+    NB_STATUS_FIXED_OVERFLOW = 1u << 2,   /* delta accumulator saturated       */
+    NB_STATUS_QUEUE_TIMEOUT = 1u << 3,    /* work-queue wait hit its bound     */
+    NB_STATUS_WORLD_TOO_LARGE = 1u << 4   /* world exceeds shared staging      */
+};
+
+/* Geometry types (newton/_src/geometry/types.py:46-77). */
+enum { NB_GEO_PLANE = 1, NB_GEO_SPHERE = 3, NB_GEO_CAPSULE = 4, NB_GEO_BOX = 7 };
+/* Joint types (newton/_src/sim/enums.py:29-55). */
+enum {
+    NB_JOINT_PRISMATIC = 0, NB_JOINT_REVOLUTE = 1, NB_JOINT_BALL = 2, NB_JOINT_FIXED = 3,
+    NB_JOINT_FREE = 4, NB_JOINT_DISTANCE = 5, NB_JOINT_D6 = 6
+};
+/* Body flags (newton/_src/sim/enums.py:8-25). */
+enum { NB_BODY_DYNAMIC = 1, NB_BODY_KINEMATIC = 2 };
+
+/* Static model description.  Mirrors the Model arrays the reference kernels
+ * read (newton/_src/sim/model.py) plus the per-world partition and the
+ * per-world candidate pair lists built once on the host. */
+typedef struct NbModelDesc {
+    int32_t body_count;
+    int32_t shape_count;
+    int32_t joint_count;
+    int32_t joint_dof_count;
+    int32_t world_count;
+    int32_t global_shape_count;   /* shapes with world == -1 (static) */
+    int32_t pair_count;           /* total candidate pairs over all worlds */
+    int32_t max_world_bodies;     /* max bodies in one world */
+    int32_t max_world_shapes;     /* max world shapes + global shapes */
+    int32_t max_world_joints;
+    int32_t max_world_pairs;
+    int32_t pad0;
+    int64_t contact_capacity;     /* total solver-format contact slots */
+
+    /* bodies [B] */
+    const float* body_com;          /* [B,3] */
+    const float* body_mass;         /* [B]   */
+    const float* body_inv_mass;     /* [B]   */
+    const float* body_inertia;      /* [B,9] */
+    const float* body_inv_inertia;  /* [B,9] */
+    const int32_t* body_flags;      /* [B]   */
+    const int32_t* body_world;      /* [B]   */
+    const float* gravity;           /* [W,3] */
+
+    /* shapes [S] */
+    const int32_t* shape_body;      /* [S] (-1 = static) */
+    const int32_t* shape_type;      /* [S] */
+    const float* shape_transform;   /* [S,7] shape in body frame */
+    const float* shape_scale;       /* [S,3] */
+    const float* shape_margin;      /* [S] */
+    const float* shape_gap;         /* [S] */
+    const float* shape_radius;      /* [S] bounding radius (1e6 for an infinite plane) */
+    const float* shape_mu;          /* [S] */
+    const float* shape_mu_torsional;/* [S] */
+    const float* shape_mu_rolling;  /* [S] */
+    const float* shape_restitution; /* [S] */
+
+    /* joints [J], dofs [D] */
+    const int32_t* joint_type;      /* [J] */
+    const int32_t* joint_enabled;   /* [J] */
+    const int32_t* joint_parent;    /* [J] */
+    const int32_t* joint_child;     /* [J] */
+    const float* joint_X_p;         /* [J,7] */
+    const float* joint_X_c;         /* [J,7] */
+    const int32_t* joint_qd_start;  /* [J] */
+    const int32_t* joint_dof_dim;   /* [J,2] (linear, angular) */
+    const float* joint_axis;        /* [D,3] */
+    const float* joint_limit_lower; /* [D] */
+    const float* joint_limit_upper; /* [D] */
+    const float* joint_target_ke;   /* [D] */
+    const float* joint_target_kd;   /* [D] */
+
+    /* world partition */
+    const int32_t* world_body_start;   /* [W+1] */
+    const int32_t* world_shape_start;  /* [W+1] world-local shapes only */
+    const int32_t* world_joint_start;  /* [W+1] */
+    const int32_t* global_shapes;      /* [G] global shape indices */
+    const int32_t* world_pair_start;   /* [W+1] */
+    const int32_t* pair_shapes;        /* [P,2] world-local shape slots (a, b) after the
+                                          type ordering of narrow_phase.py:207-210,
+                                          sorted by contact key within each world.
+                                          Slot i < n_local is shape world_shape_start[w]+i,
+                                          slot n_local+g is global_shapes[g]. */
+    const int64_t* contact_cap_start;  /* [W+1] contact slot ranges */
+    const int32_t* world_order;        /* [W] world processing order (cost-descending) */
+} NbModelDesc;
+
+/* Solver-format contact segments (written by nb_collide, read by nb_xpbd_step). */
+typedef struct NbContactSeg {
+    float* rec0;                 /* [cap,4] */
+    float* rec1;
+    float* rec2;
+    float* rec3;
+    float* rec4;
+    int32_t* world_count;        /* [W] live contacts per world */
+    float* slot_scratch;         /* per-CTA narrow-phase staging, nb_collide_scratch_floats() floats */
+    int32_t* work_counter;       /* [4] device work-queue counters, zeroed by the entry points */
+    uint32_t* status;            /* [1] NB_STATUS_* bits (sticky, cleared by the caller) */
+} NbContactSeg;
+
+/* Public Contacts arrays in the reference layout (newton/_src/sim/contacts.py:43-186). */
+typedef struct NbContactsPublic {
+    int32_t capacity;            /* rigid_contact_max */
+    int32_t pad0;
+    int32_t* count;              /* [1] rigid_contact_count (may exceed capacity on overflow) */
+    int32_t* shape0;             /* [cap] */
+    int32_t* shape1;             /* [cap] */
+    float* point0;               /* [cap,3] */
+    float* point1;               /* [cap,3] */
+    float* offset0;              /* [cap,3] */
+    float* offset1;              /* [cap,3] */
+    float* normal;               /* [cap,3] */
+    float* margin0;              /* [cap] */
+    float* margin1;              /* [cap] */
+    int64_t* sort_key;           /* [cap] or NULL */
+    int64_t* world_offset;       /* [W+1] scratch for the world scan */
+} NbContactsPublic;
+
+/* SolverXPBD constructor arguments (newton/_src/solvers/xpbd/solver_xpbd.py:95-109). */
+typedef struct NbXpbdParams {
+    int32_t iterations;
+    int32_t rigid_contact_con_weighting;
+    int32_t enable_restitution;
+    int32_t pad0;
+    float joint_linear_relaxation;
+    float joint_angular_relaxation;
+    float joint_linear_compliance;
+    float joint_angular_compliance;
+    float rigid_contact_relaxation;
+    float angular_damping;
+} NbXpbdParams;
+
+/* Per-step state buffers (State / Control arrays). */
+typedef struct NbStepIO {
+    const float* body_q_in;      /* [B,7] */
+    const float* body_qd_in;     /* [B,6] */
+    const float* body_f_in;      /* [B,6] */
+    float* body_q_out;           /* [B,7] */
+    float* body_qd_out;          /* [B,6] */
+    const float* joint_target_pos; /* [D] (may be NULL when no joint drives) */
+    const float* joint_target_vel; /* [D] */
+    const float* joint_f;          /* [D] */
+    float* contact_impulse;      /* [cap,6] accumulated weighted impulse or NULL */
+} NbStepIO;
+
+/* ABI version of the loaded library (NB_ABI_VERSION). */
+int nb_abi_version(void);
+
+/* Floats of per-CTA staging needed by nb_collide for `grid_ctas` CTAs. */
+int64_t nb_collide_scratch_floats(int32_t grid_ctas);
+
+/* Number of CTAs nb_collide / nb_xpbd_step launch on the current device. */
+int32_t nb_default_grid(void);
+
+/*
+ * Collision detection for all worlds: shape world transforms + AABBs
+ * (replaces compute_shape_aabbs, collide.py:150-275), candidate-pair AABB test
+ * (BroadPhaseExplicit, broad_phase_nxn.py:28-66; the NxN pair set of
+ * broad_phase_nxn.py:129-214 is the same list), primitive and MPR/GJK narrow
+ * phase with write_contact semantics (narrow_phase.py:153-776, collide.py:62-147)
+ * and deterministic key-ordered compaction (contact_sort.py).
+ * Writes the solver-format segments in `seg`.
+ */
+int nb_collide(const NbModelDesc* model, const float* body_q, const NbContactSeg* seg,
+               int32_t grid_ctas, void* stream);
+
+/*
+ * Publish solver-format segments into the reference's dense Contacts arrays
+ * ordered by (world, key); replaces the Contacts writes of write_contact
+ * (collide.py:62-147) and ContactSorter.sort_full (contact_sort.py:305-400).
+ */
+int nb_publish_contacts(const NbModelDesc* model, const NbContactSeg* seg,
+                        const NbContactsPublic* pub, void* stream);
+
+/*
+ * One XPBD substep for all worlds: apply_joint_forces, integrate_bodies,
+ * `iterations` x (solve_body_contact_positions, apply_body_deltas,
+ * solve_body_joints, apply_body_deltas), optional restitution and the
+ * kinematic pass-through.  Replaces SolverXPBD.step (solver_xpbd.py:259-764).
+ */
+int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbStepIO* io,
+                 const NbContactSeg* seg, float dt, int32_t grid_ctas, void* stream);
+
+/*
+ * Ingest contacts written by a caller into the dense public arrays (custom
+ * contact writers) into the solver-format segments, bucketing by world in
+ * contact-index order.  Replaces nothing in the reference (its solver reads
+ * the dense arrays directly, xpbd/kernels.py:2062-2298).
+ */
+int nb_ingest_contacts(const NbModelDesc* model, const NbContactsPublic* pub,
+                       const NbContactSeg* seg, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEWTON_B200_H */

@@ -1,0 +1,210 @@
+"""ctypes mirrors of the structs in include/newton_b200.h.
+
+The field order and types must match the header exactly; ``test_abi_layout``
+checks the sizes against the compiled library.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import enum
+
+NB_ABI_VERSION = 1
+
+NB_OK = 0
+NB_ERR_INVALID = 1
+NB_ERR_CUDA = 2
+NB_ERR_UNSUPPORTED = 3
+NB_ERR_CAPACITY = 4
+
+NB_STATUS_CONTACT_OVERFLOW = 1 << 0
+NB_STATUS_NONFINITE = 1 << 1
+NB_STATUS_FIXED_OVERFLOW = 1 << 2
+NB_STATUS_QUEUE_TIMEOUT = 1 << 3
+NB_STATUS_WORLD_TOO_LARGE = 1 << 4
+
+
+class GeoType(enum.IntEnum):
+    """Shape types (newton/_src/geometry/types.py:46-77)."""
+
+    NONE = 0
+    PLANE = 1
+    HFIELD = 2
+    SPHERE = 3
+    CAPSULE = 4
+    ELLIPSOID = 5
+    CYLINDER = 6
+    BOX = 7
+    MESH = 8
+    CONE = 9
+    CONVEX_MESH = 10
+
+
+SUPPORTED_GEO = (GeoType.PLANE, GeoType.SPHERE, GeoType.CAPSULE, GeoType.BOX)
+
+
+class JointType(enum.IntEnum):
+    """Joint types (newton/_src/sim/enums.py:29-55)."""
+
+    PRISMATIC = 0
+    REVOLUTE = 1
+    BALL = 2
+    FIXED = 3
+    FREE = 4
+    DISTANCE = 5
+    D6 = 6
+    CABLE = 7
+
+
+class BodyFlags(enum.IntFlag):
+    """Body state flags (newton/_src/sim/enums.py:8-25)."""
+
+    DYNAMIC = 1 << 0
+    KINEMATIC = 1 << 1
+    ALL = DYNAMIC | KINEMATIC
+
+
+class ShapeFlags(enum.IntFlag):
+    """Shape flags (newton/_src/geometry/flags.py:18-36)."""
+
+    VISIBLE = 1 << 0
+    COLLIDE_SHAPES = 1 << 1
+    COLLIDE_PARTICLES = 1 << 2
+    SITE = 1 << 3
+    HYDROELASTIC = 1 << 4
+
+
+_fp = C.c_void_p
+
+
+class NbModelDesc(C.Structure):
+    _fields_ = [
+        ("body_count", C.c_int32),
+        ("shape_count", C.c_int32),
+        ("joint_count", C.c_int32),
+        ("joint_dof_count", C.c_int32),
+        ("world_count", C.c_int32),
+        ("global_shape_count", C.c_int32),
+        ("pair_count", C.c_int32),
+        ("max_world_bodies", C.c_int32),
+        ("max_world_shapes", C.c_int32),
+        ("max_world_joints", C.c_int32),
+        ("max_world_pairs", C.c_int32),
+        ("pad0", C.c_int32),
+        ("contact_capacity", C.c_int64),
+        ("body_com", _fp),
+        ("body_mass", _fp),
+        ("body_inv_mass", _fp),
+        ("body_inertia", _fp),
+        ("body_inv_inertia", _fp),
+        ("body_flags", _fp),
+        ("body_world", _fp),
+        ("gravity", _fp),
+        ("shape_body", _fp),
+        ("shape_type", _fp),
+        ("shape_transform", _fp),
+        ("shape_scale", _fp),
+        ("shape_margin", _fp),
+        ("shape_gap", _fp),
+        ("shape_radius", _fp),
+        ("shape_mu", _fp),
+        ("shape_mu_torsional", _fp),
+        ("shape_mu_rolling", _fp),
+        ("shape_restitution", _fp),
+        ("joint_type", _fp),
+        ("joint_enabled", _fp),
+        ("joint_parent", _fp),
+        ("joint_child", _fp),
+        ("joint_X_p", _fp),
+        ("joint_X_c", _fp),
+        ("joint_qd_start", _fp),
+        ("joint_dof_dim", _fp),
+        ("joint_axis", _fp),
+        ("joint_limit_lower", _fp),
+        ("joint_limit_upper", _fp),
+        ("joint_target_ke", _fp),
+        ("joint_target_kd", _fp),
+        ("world_body_start", _fp),
+        ("world_shape_start", _fp),
+        ("world_joint_start", _fp),
+        ("global_shapes", _fp),
+        ("world_pair_start", _fp),
+        ("pair_shapes", _fp),
+        ("contact_cap_start", _fp),
+        ("world_order", _fp),
+    ]
+
+
+class NbContactSeg(C.Structure):
+    _fields_ = [
+        ("rec0", _fp),
+        ("rec1", _fp),
+        ("rec2", _fp),
+        ("rec3", _fp),
+        ("rec4", _fp),
+        ("world_count", _fp),
+        ("slot_scratch", _fp),
+        ("work_counter", _fp),
+        ("status", _fp),
+    ]
+
+
+class NbContactsPublic(C.Structure):
+    _fields_ = [
+        ("capacity", C.c_int32),
+        ("pad0", C.c_int32),
+        ("count", _fp),
+        ("shape0", _fp),
+        ("shape1", _fp),
+        ("point0", _fp),
+        ("point1", _fp),
+        ("offset0", _fp),
+        ("offset1", _fp),
+        ("normal", _fp),
+        ("margin0", _fp),
+        ("margin1", _fp),
+        ("sort_key", _fp),
+        ("world_offset", _fp),
+    ]
+
+
+class NbXpbdParams(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int32),
+        ("rigid_contact_con_weighting", C.c_int32),
+        ("enable_restitution", C.c_int32),
+        ("pad0", C.c_int32),
+        ("joint_linear_relaxation", C.c_float),
+        ("joint_angular_relaxation", C.c_float),
+        ("joint_linear_compliance", C.c_float),
+        ("joint_angular_compliance", C.c_float),
+        ("rigid_contact_relaxation", C.c_float),
+        ("angular_damping", C.c_float),
+    ]
+
+
+class NbStepIO(C.Structure):
+    _fields_ = [
+        ("body_q_in", _fp),
+        ("body_qd_in", _fp),
+        ("body_f_in", _fp),
+        ("body_q_out", _fp),
+        ("body_qd_out", _fp),
+        ("joint_target_pos", _fp),
+        ("joint_target_vel", _fp),
+        ("joint_f", _fp),
+        ("contact_impulse", _fp),
+    ]
+
+
+def ptr(a) -> int | None:
+    """Raw address of a numpy array or torch tensor (None for None / empty)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        if a.numel() == 0:
+            return None
+        return int(a.data_ptr())
+    if a.size == 0:
+        return None
+    return int(a.ctypes.data)

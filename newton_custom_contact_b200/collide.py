@@ -1,0 +1,339 @@
+"""CollisionPipeline (newton/_src/sim/collide.py:483-1230) on the B200 kernels.
+
+``collide(state, contacts)`` launches two kernels of libnewton_b200.so:
+``nb_collide`` (per-world AABBs, broad phase, narrow phase and key-ordered
+compaction into solver-format segments) and ``nb_publish_contacts`` (the
+reference's dense Contacts arrays, ordered by (world, key)).  Both run on the
+current torch stream without host synchronisation, so a substep loop of
+collide + SolverXPBD.step can be captured in a CUDA graph.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from typing import Literal
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._abi import GeoType, NbContactSeg, NbContactsPublic, ShapeFlags, ptr
+from .contacts import Contacts
+
+BROAD_PHASE_MODES = ("nxn", "sap", "explicit")
+
+_PRIMITIVE_CPP = 5
+_MAX_NEIGHBORS_PER_SHAPE = 20
+
+
+def _estimate_rigid_contact_max(model) -> int:
+    """Capacity estimate of newton/_src/sim/collide.py:278-376 (primitive shapes only)."""
+    h = model.host_arrays()
+    st = h["shape_type"]
+    if st.size == 0:
+        return 1000
+    plane = st == int(GeoType.PLANE)
+    non_plane = ~plane
+    n_np = int(non_plane.sum())
+    non_plane_contacts = (n_np * _MAX_NEIGHBORS_PER_SHAPE * _PRIMITIVE_CPP) // 2
+    avg_cpp = _PRIMITIVE_CPP if n_np > 0 else 0
+    plane_contacts = 0
+    if plane.any() and n_np > 0:
+        sw = h["shape_world"]
+        W = model.world_count
+        gmask = sw == -1
+        lmask = ~gmask
+        gp = int(np.count_nonzero(gmask & plane))
+        gnp = int(np.count_nonzero(gmask & non_plane))
+        lp = np.bincount(sw[lmask & plane], minlength=W)[:W]
+        lnp = np.bincount(sw[lmask & non_plane], minlength=W)[:W]
+        cnt = int(np.sum((lp + gp) * (lnp + gnp)))
+        if W > 1:
+            cnt -= (W - 1) * gp * gnp
+        plane_contacts = cnt * avg_cpp
+    total = non_plane_contacts + plane_contacts
+    if model.shape_contact_pair_count > 0:
+        total = min(total, int(model.shape_contact_pair_count) * max(avg_cpp, _PRIMITIVE_CPP))
+    return max(1000, total)
+
+
+def _max_contacts(ta: int, tb: int) -> int:
+    """Upper bound of contacts one pair can emit (narrow_phase.py:153-776)."""
+    P, S, C_, B = int(GeoType.PLANE), int(GeoType.SPHERE), int(GeoType.CAPSULE), int(GeoType.BOX)
+    table = {(P, S): 1, (S, S): 1, (S, C_): 1, (S, B): 1, (P, C_): 2, (C_, C_): 2}
+    return table.get((ta, tb), 5)
+
+
+def nxn_pairs(model) -> np.ndarray:
+    """The NxN candidate set (broad_phase_nxn.py:129-214 + broad_phase_common.py:132-180).
+
+    Pairs of colliding shapes that pass the world / collision-group test and are
+    not filtered; identical to the builder's explicit list by construction.
+    """
+    h = model.host_arrays()
+    flags = h["shape_flags"]
+    sw = model._world_of_shape
+    grp = h["shape_collision_group"].astype(np.int64)
+    filters = model.shape_collision_filter_pairs
+    col = (flags & int(ShapeFlags.COLLIDE_SHAPES)) != 0
+    glob = np.nonzero(col & (sw < 0))[0]
+    chunks = []
+    wss = model._part["world_shape_start"]
+    for w in range(model.world_count):
+        loc = np.arange(wss[w], wss[w + 1])
+        loc = loc[col[loc]]
+        ids = np.sort(np.concatenate([loc, glob]))
+        if ids.size < 2:
+            continue
+        i, j = np.triu_indices(ids.size, 1)
+        a, b = ids[i], ids[j]
+        both_global = (sw[a] < 0) & (sw[b] < 0)
+        ga, gb = grp[a], grp[b]
+        ok = (ga != 0) & (gb != 0) & np.where(ga > 0, (ga == gb) | (gb < 0), ga != gb) & ~both_global
+        chunks.append(np.stack([a[ok], b[ok]], axis=1))
+    pairs = np.concatenate(chunks) if chunks else np.zeros((0, 2), np.int64)
+    if filters and pairs.size:
+        keep = np.array([(int(x), int(y)) not in filters for x, y in pairs], dtype=bool)
+        pairs = pairs[keep]
+    return pairs.astype(np.int32).reshape(-1, 2)
+
+
+class PairLayout:
+    """Per-world candidate pairs sorted by contact key and contact slot ranges."""
+
+    def __init__(self, model, pairs: np.ndarray):
+        h = model.host_arrays()
+        W = model.world_count
+        types = h["shape_type"]
+        sws = model._world_of_shape
+        wss = model._part["world_shape_start"].astype(np.int64)
+        glob = model._part["global_shapes"].astype(np.int64)
+        pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
+        a, b = pairs[:, 0], pairs[:, 1]
+        wa, wb = sws[a], sws[b]
+        keep = (wa >= 0) | (wb >= 0)
+        a, b, wa, wb = a[keep], b[keep], wa[keep], wb[keep]
+        if np.any((wa >= 0) & (wb >= 0) & (wa != wb)):
+            raise ValueError("candidate pair spans two worlds")
+        w = np.where(wa >= 0, wa, wb).astype(np.int64)
+        swap = types[a] > types[b]
+        sa = np.where(swap, b, a)
+        sb = np.where(swap, a, b)
+        if model.shape_count < (1 << 21):
+            order = np.argsort((w << 42) | (sa << 21) | sb, kind="stable")
+        else:
+            order = np.lexsort((sb, sa, w))
+        sa, sb, w = sa[order], sb[order], w[order]
+        nloc = np.diff(wss)
+        gslot = np.full(model.shape_count, -1, np.int64)
+        gslot[glob] = np.arange(glob.size)
+
+        def local(s):
+            ws = sws[s]
+            out = s - wss[w]
+            g = ws < 0
+            out[g] = nloc[w[g]] + gslot[s[g]]
+            return out
+
+        la, lb = local(sa), local(sb)
+        P = sa.size
+        # every slot must address the world's shapes or the global shapes (the
+        # kernels index shared memory with it)
+        lim = nloc[w] + glob.size
+        if P and (la.min() < 0 or lb.min() < 0 or np.any(la >= lim) or np.any(lb >= lim)):
+            raise AssertionError("pair layout produced an out-of-range shape slot")
+        if P and np.any(np.diff(w) < 0):
+            raise AssertionError("pair layout is not grouped by world")
+        cnt = np.bincount(w, minlength=W)[:W] if P else np.zeros(W, np.int64)
+        pstart = np.zeros(W + 1, np.int64)
+        pstart[1:] = np.cumsum(cnt)
+        table = np.full((16, 16), 5, np.int64)
+        for ta in range(16):
+            for tb in range(16):
+                table[ta, tb] = _max_contacts(ta, tb)
+        maxc = table[types[sa], types[sb]]
+        ccap = np.bincount(w, weights=maxc, minlength=W)[:W].astype(np.int64) if P else np.zeros(W, np.int64)
+        cstart = np.zeros(W + 1, np.int64)
+        cstart[1:] = np.cumsum(ccap)
+        nb = np.diff(model._part["world_body_start"].astype(np.int64))
+        cost = cnt + 4 * nb
+        self.world_order = np.argsort(-cost, kind="stable").astype(np.int32)
+        self.world_pair_start = pstart.astype(np.int32)
+        self.pair_shapes = np.stack([la, lb], axis=1).astype(np.int32).reshape(-1, 2)
+        self.pair_global = np.stack([sa, sb], axis=1).astype(np.int32).reshape(-1, 2)
+        self.contact_cap_start = cstart
+        self.pair_count = int(P)
+        self.max_world_pairs = int(cnt.max()) if W else 0
+        self.contact_capacity = int(cstart[-1])
+        self.world_count = W
+
+    def host_dict(self) -> dict:
+        return {
+            "world_pair_start": self.world_pair_start,
+            "pair_shapes": self.pair_shapes,
+            "contact_cap_start": self.contact_cap_start,
+            "world_order": self.world_order,
+        }
+
+    def info(self) -> dict:
+        return {"pair_count": self.pair_count, "max_world_pairs": self.max_world_pairs,
+                "contact_capacity": self.contact_capacity}
+
+
+class CollisionPipeline:
+    """Broad phase + primitive/MPR-GJK narrow phase + deterministic compaction on B200."""
+
+    def __init__(self, model, *, reduce_contacts: bool = True, rigid_contact_max: int | None = None,
+                 max_triangle_pairs: int = 1000000, shape_pairs_filtered=None, soft_contact_max: int | None = None,
+                 soft_contact_margin: float = 0.01, requires_grad: bool | None = None,
+                 broad_phase: Literal["nxn", "sap", "explicit"] | None = None, narrow_phase=None,
+                 sdf_hydroelastic_config=None, shape_pairs_max: int | None = None, deterministic: bool = False,
+                 contact_matching: str = "disabled", contact_matching_pos_threshold: float = 0.0005,
+                 contact_matching_normal_dot_threshold: float = 0.995, contact_report: bool = False,
+                 verify_buffers: bool = True):
+        if contact_matching not in ("disabled", "latest", "sticky"):
+            raise ValueError(
+                f"contact_matching must be one of 'disabled', 'latest', 'sticky', got {contact_matching!r}")
+        if contact_matching != "disabled":
+            raise NotImplementedError("contact matching is not implemented in this build")
+        if contact_report:
+            raise ValueError('contact_report=True requires contact_matching != "disabled"')
+        if max_triangle_pairs <= 0:
+            raise ValueError("max_triangle_pairs must be > 0")
+        if narrow_phase is not None or sdf_hydroelastic_config is not None:
+            raise NotImplementedError("custom narrow phases / hydroelastic contacts are not supported")
+        if shape_pairs_max is not None and shape_pairs_max <= 0:
+            raise ValueError(f"shape_pairs_max must be a positive integer or None, got {shape_pairs_max}")
+        mode = "explicit" if broad_phase is None else str(broad_phase).lower()
+        if mode not in BROAD_PHASE_MODES:
+            raise ValueError(f"Unsupported broad phase mode: {broad_phase!r}")
+        self.model = model
+        self.device = model.device
+        self.broad_phase_mode = mode
+        self.deterministic = deterministic
+        self.requires_grad = model.requires_grad if requires_grad is None else requires_grad
+        self.soft_contact_margin = soft_contact_margin
+        if rigid_contact_max is None:
+            mrc = int(getattr(model, "rigid_contact_max", 0) or 0)
+            rigid_contact_max = mrc if mrc > 0 else _estimate_rigid_contact_max(model)
+        self._rigid_contact_max = int(rigid_contact_max)
+        model.rigid_contact_max = self._rigid_contact_max
+        self._soft_contact_max = int(soft_contact_max) if soft_contact_max is not None else 0
+        if mode == "explicit":
+            if shape_pairs_filtered is None:
+                shape_pairs_filtered = model.host("shape_contact_pairs")
+            if shape_pairs_filtered is None:
+                raise ValueError("shape_pairs_filtered must be provided for broad_phase=EXPLICIT "
+                                 "(or set model.shape_contact_pairs)")
+            pairs = shape_pairs_filtered
+            if isinstance(pairs, torch.Tensor):
+                pairs = pairs.detach().cpu().numpy()
+        else:
+            # SAP reports the same AABB-overlapping set as NxN; both use the NxN candidate list.
+            pairs = nxn_pairs(model)
+        self.shape_pairs_max = int(np.asarray(pairs).reshape(-1, 2).shape[0])
+        self.layout = PairLayout(model, pairs)
+        hd = self.layout.host_dict()
+        self._layout_host = hd
+        self._layout_dev = {k: torch.from_numpy(np.ascontiguousarray(v)).to(self.device) for k, v in hd.items()}
+        self._desc = None
+        self._grid = None
+
+    @property
+    def rigid_contact_max(self) -> int:
+        return self._rigid_contact_max
+
+    @property
+    def soft_contact_max(self) -> int:
+        return self._soft_contact_max
+
+    # ------------------------------------------------------------ buffers
+    def contacts(self) -> Contacts:
+        c = Contacts(self._rigid_contact_max, self._soft_contact_max, requires_grad=self.requires_grad,
+                     device=self.device, requested_attributes=self.model.get_requested_contact_attributes(),
+                     world_count=self.model.world_count, deterministic=self.deterministic)
+        self.attach_segments(c)
+        return c
+
+    def attach_segments(self, c: Contacts) -> None:
+        cap = max(1, self.layout.contact_capacity)
+        dev = self.device
+        seg = {f"rec{k}": torch.zeros((cap, 4), dtype=torch.float32, device=dev) for k in range(5)}
+        seg["world_count"] = torch.zeros(self.model.world_count, dtype=torch.int32, device=dev)
+        seg["work_counter"] = torch.zeros(4, dtype=torch.int32, device=dev)
+        seg["status"] = torch.zeros(1, dtype=torch.int32, device=dev)
+        c._seg = seg
+        c._layout = self
+        c._seg_valid = False
+
+    def desc(self):
+        if self._desc is None:
+            arrays = self.model.device_arrays()
+            arrays.update(self._layout_dev)
+            self._desc = self.model.make_desc(arrays, self.layout.info())
+        return self._desc
+
+    def _scratch(self):
+        if self._grid is None:
+            lib = _lib.load()
+            self._grid = int(lib.nb_default_grid())
+            n = int(lib.nb_collide_scratch_floats(self._grid))
+            self._slot_scratch = torch.empty(n, dtype=torch.float32, device=self.device)
+        return self._grid, self._slot_scratch
+
+    @staticmethod
+    def seg_struct(c: Contacts, scratch=None) -> NbContactSeg:
+        s = c._seg
+        st = NbContactSeg()
+        for k in range(5):
+            setattr(st, f"rec{k}", ptr(s[f"rec{k}"]))
+        st.world_count = ptr(s["world_count"])
+        st.work_counter = ptr(s["work_counter"])
+        st.status = ptr(s["status"])
+        st.slot_scratch = ptr(scratch)
+        return st
+
+    @staticmethod
+    def public_struct(c: Contacts) -> NbContactsPublic:
+        p = NbContactsPublic()
+        p.capacity = c.rigid_contact_max
+        p.count = ptr(c.rigid_contact_count)
+        p.shape0 = ptr(c.rigid_contact_shape0)
+        p.shape1 = ptr(c.rigid_contact_shape1)
+        p.point0 = ptr(c.rigid_contact_point0)
+        p.point1 = ptr(c.rigid_contact_point1)
+        p.offset0 = ptr(c.rigid_contact_offset0)
+        p.offset1 = ptr(c.rigid_contact_offset1)
+        p.normal = ptr(c.rigid_contact_normal)
+        p.margin0 = ptr(c.rigid_contact_margin0)
+        p.margin1 = ptr(c.rigid_contact_margin1)
+        p.sort_key = ptr(c.rigid_contact_sort_key) if c.rigid_contact_sort_key.numel() else None
+        p.world_offset = ptr(c._world_offset)
+        return p
+
+    # ------------------------------------------------------------ collide
+    def collide(self, state, contacts: Contacts, *, soft_contact_margin: float | None = None) -> None:
+        _lib.require_cuda(self.device)
+        if contacts._seg is None or contacts._layout is not self:
+            self.attach_segments(contacts)
+        if contacts._world_offset.numel() != self.model.world_count + 1:
+            contacts._world_offset = torch.zeros(self.model.world_count + 1, dtype=torch.int64, device=self.device)
+        lib = _lib.load()
+        grid, scratch = self._scratch()
+        desc = self.desc()
+        seg = self.seg_struct(contacts, scratch)
+        stream = _lib.stream_handle(self.device)
+        bq = state.body_q
+        if bq.dtype != torch.float32 or not bq.is_contiguous() or bq.device.type != "cuda":
+            raise TypeError("state.body_q must be a contiguous float32 tensor on the model device")
+        _lib.check("nb_collide", lib.nb_collide(C.byref(desc), C.c_void_p(ptr(bq)), C.byref(seg), grid,
+                                                C.c_void_p(stream)))
+        pub = self.public_struct(contacts)
+        _lib.check("nb_publish_contacts", lib.nb_publish_contacts(C.byref(desc), C.byref(seg), C.byref(pub),
+                                                                  C.c_void_p(stream)))
+        contacts.contact_generation.add_(1)
+        contacts._seg_valid = True
+
+    def status(self, contacts: Contacts) -> int:
+        """Device status bits (NB_STATUS_*) accumulated in this contacts buffer (synchronises)."""
+        return int(contacts._seg["status"].item())

@@ -1,0 +1,110 @@
+// extern "C" entry points of libnewton_b200.so (declared in include/newton_b200.h).
+#include <cuda_runtime.h>
+
+#include "nb_kernels.cuh"
+
+namespace {
+
+int grid_for(int requested) {
+    if (requested > 0) return requested;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms * 2;  // two resident CTAs per SM (__launch_bounds__(256, 2))
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int check_model(const NbModelDesc* m) {
+    if (!m) return NB_ERR_INVALID;
+    if (m->world_count <= 0 || m->body_count < 0 || m->shape_count < 0) return NB_ERR_INVALID;
+    if (m->max_world_bodies > 4094) return NB_ERR_UNSUPPORTED;  // 12-bit body tags in contact records
+    if (!m->world_body_start || !m->world_joint_start || !m->world_order) return NB_ERR_INVALID;
+    if (m->body_count > 0 && (!m->body_com || !m->body_inv_mass || !m->body_inertia || !m->body_inv_inertia ||
+                              !m->body_flags || !m->body_world || !m->gravity))
+        return NB_ERR_INVALID;
+    return NB_OK;
+}
+
+int check_seg(const NbContactSeg* s) {
+    if (!s || !s->world_count || !s->work_counter || !s->status) return NB_ERR_INVALID;
+    if (!s->rec0 || !s->rec1 || !s->rec2 || !s->rec3 || !s->rec4) return NB_ERR_INVALID;
+    if (!aligned16(s->rec0) || !aligned16(s->rec1) || !aligned16(s->rec2) || !aligned16(s->rec3) ||
+        !aligned16(s->rec4))
+        return NB_ERR_INVALID;
+    return NB_OK;
+}
+
+int smem_limit() {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nb_abi_version(void) { return NB_ABI_VERSION; }
+
+int64_t nb_collide_scratch_floats(int32_t grid_ctas) {
+    return (int64_t)grid_for(grid_ctas) * NB_COLLIDE_THREADS * 25 * 4;
+}
+
+int32_t nb_default_grid(void) { return grid_for(0); }
+
+int nb_collide(const NbModelDesc* model, const float* body_q, const NbContactSeg* seg, int32_t grid_ctas,
+               void* stream) {
+    int rc = check_model(model);
+    if (rc) return rc;
+    if ((rc = check_seg(seg))) return rc;
+    if (!seg->slot_scratch || !body_q || !model->world_pair_start || !model->pair_shapes ||
+        !model->contact_cap_start || !model->world_shape_start)
+        return NB_ERR_INVALID;
+    if ((int64_t)nb_collide_smem_bytes(model) > smem_limit()) return NB_ERR_UNSUPPORTED;
+    cudaError_t e = nb_launch_collide(model, body_q, seg, grid_for(grid_ctas), (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+int nb_publish_contacts(const NbModelDesc* model, const NbContactSeg* seg, const NbContactsPublic* pub,
+                        void* stream) {
+    int rc = check_model(model);
+    if (rc) return rc;
+    if ((rc = check_seg(seg))) return rc;
+    if (!pub || !pub->count || !pub->world_offset || pub->capacity < 0) return NB_ERR_INVALID;
+    if (pub->capacity > 0 && (!pub->shape0 || !pub->shape1 || !pub->point0 || !pub->point1 || !pub->offset0 ||
+                              !pub->offset1 || !pub->normal || !pub->margin0 || !pub->margin1))
+        return NB_ERR_INVALID;
+    cudaError_t e = nb_launch_publish(model, seg, pub, (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+int nb_ingest_contacts(const NbModelDesc* model, const NbContactsPublic* pub, const NbContactSeg* seg,
+                       void* stream) {
+    int rc = check_model(model);
+    if (rc) return rc;
+    if ((rc = check_seg(seg))) return rc;
+    if (!pub || !pub->count || pub->capacity < 0) return NB_ERR_INVALID;
+    if (!model->contact_cap_start || !model->shape_body) return NB_ERR_INVALID;
+    cudaError_t e = nb_launch_ingest(model, pub, seg, (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbStepIO* io, const NbContactSeg* seg,
+                 float dt, int32_t grid_ctas, void* stream) {
+    int rc = check_model(model);
+    if (rc) return rc;
+    if (!params || !io || !seg || !seg->work_counter || !seg->status) return NB_ERR_INVALID;
+    if (params->iterations < 0) return NB_ERR_INVALID;
+    if (!(dt > 0.0f)) return NB_ERR_INVALID;
+    if (params->enable_restitution || io->contact_impulse) return NB_ERR_UNSUPPORTED;
+    if (model->body_count > 0 && (!io->body_q_in || !io->body_qd_in || !io->body_f_in || !io->body_q_out ||
+                                  !io->body_qd_out))
+        return NB_ERR_INVALID;
+    if (seg->rec0 && ((rc = check_seg(seg)) || !model->contact_cap_start)) return rc ? rc : NB_ERR_INVALID;
+    if ((int64_t)nb_step_smem_bytes(model) > smem_limit()) return NB_ERR_UNSUPPORTED;
+    cudaError_t e = nb_launch_step(model, params, io, seg, dt, grid_for(grid_ctas), (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,740 @@
+// One XPBD substep for many independent worlds, one world per CTA.
+//
+// The world's body poses and twists live in shared memory for the whole
+// substep, so the `iterations` constraint-projection passes never touch HBM
+// for body state (the reference re-reads body arrays in ~7 launches per
+// iteration, newton/_src/solvers/xpbd/solver_xpbd.py:371-630).  Per iteration:
+//   contacts: one thread per contact (solve_body_contact_positions,
+//             newton/_src/solvers/xpbd/kernels.py:2062-2298); per-body deltas
+//             and contact counts are summed with shared-memory int64
+//             fixed-point atomics -- exact, so the result does not depend on
+//             thread order -- after a warp-level pre-reduction of runs of
+//             contacts that share a body;
+//   bodies:   one thread per body, weighted apply_body_deltas
+//             (kernels.py:809-878), then the joint pass (solve_body_joints,
+//             kernels.py:1441-1942) and the unweighted apply of
+//             solver_xpbd.py:590-630.
+#include <cuda_runtime.h>
+
+#include "nb_kernels.cuh"
+#include "nb_math.cuh"
+
+namespace {
+
+constexpr int kST = NB_STEP_THREADS;
+
+struct SBodies {
+    int nb;
+    float* f;                  // [13][nb] pose (7) + twist (6)
+    float* c;                  // [4][nb]  com (3), effective inv mass
+    float* I;                  // [9][nb]
+    float* iI;                 // [9][nb]  effective inverse inertia
+    float* frc;                // [6][nb]  body_f + joint forces
+    int* flags;                // [nb]
+    unsigned long long* acc;   // [6][nb]
+    int* cnt;                  // [nb]
+
+    __device__ TF q(int i) const {
+        return TF{V3{f[0 * nb + i], f[1 * nb + i], f[2 * nb + i]},
+                  Q4{f[3 * nb + i], f[4 * nb + i], f[5 * nb + i], f[6 * nb + i]}};
+    }
+    __device__ V3 v(int i) const { return V3{f[7 * nb + i], f[8 * nb + i], f[9 * nb + i]}; }
+    __device__ V3 w(int i) const { return V3{f[10 * nb + i], f[11 * nb + i], f[12 * nb + i]}; }
+    __device__ void set(int i, TF t, V3 lv, V3 aw) {
+        f[0 * nb + i] = t.p.x; f[1 * nb + i] = t.p.y; f[2 * nb + i] = t.p.z;
+        f[3 * nb + i] = t.q.x; f[4 * nb + i] = t.q.y; f[5 * nb + i] = t.q.z; f[6 * nb + i] = t.q.w;
+        f[7 * nb + i] = lv.x; f[8 * nb + i] = lv.y; f[9 * nb + i] = lv.z;
+        f[10 * nb + i] = aw.x; f[11 * nb + i] = aw.y; f[12 * nb + i] = aw.z;
+    }
+    __device__ V3 com(int i) const { return V3{c[i], c[nb + i], c[2 * nb + i]}; }
+    __device__ float inv_m(int i) const { return c[3 * nb + i]; }
+    __device__ M33 inertia(int i) const {
+        M33 r;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) r.m[k / 3][k % 3] = I[k * nb + i];
+        return r;
+    }
+    __device__ M33 inv_inertia(int i) const {
+        M33 r;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) r.m[k / 3][k % 3] = iI[k * nb + i];
+        return r;
+    }
+    __device__ void add_delta(int i, V3 lin, V3 ang, unsigned* bad) {
+        acc_add(i, 0, fx_quant(lin.x, bad));
+        acc_add(i, 1, fx_quant(lin.y, bad));
+        acc_add(i, 2, fx_quant(lin.z, bad));
+        acc_add(i, 3, fx_quant(ang.x, bad));
+        acc_add(i, 4, fx_quant(ang.y, bad));
+        acc_add(i, 5, fx_quant(ang.z, bad));
+    }
+    __device__ void acc_add(int i, int k, long long v) {
+        if (v != 0) atomicAdd(&acc[k * nb + i], (unsigned long long)v);
+    }
+    // read and clear the accumulated delta of body i
+    __device__ void take(int i, V3& lin, V3& ang) {
+        long long v[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            v[k] = (long long)acc[k * nb + i];
+            acc[k * nb + i] = 0ull;
+        }
+        lin = V3{fx_float(v[0]), fx_float(v[1]), fx_float(v[2])};
+        ang = V3{fx_float(v[3]), fx_float(v[4]), fx_float(v[5])};
+    }
+};
+
+__device__ size_t sbodies_bytes(int nb) {
+    return (size_t)nb * (13 + 4 + 9 + 9 + 6) * sizeof(float) + (size_t)nb * sizeof(int) +
+           (size_t)nb * 6 * sizeof(unsigned long long) + (size_t)nb * sizeof(int);
+}
+
+__device__ SBodies sbodies_carve(unsigned char* smem, int nb) {
+    SBodies s;
+    s.nb = nb;
+    unsigned long long* a = reinterpret_cast<unsigned long long*>(smem);
+    s.acc = a;
+    float* fl = reinterpret_cast<float*>(a + 6 * (size_t)nb);
+    s.f = fl;
+    s.c = fl + 13 * nb;
+    s.I = s.c + 4 * nb;
+    s.iI = s.I + 9 * nb;
+    s.frc = s.iI + 9 * nb;
+    int* ip = reinterpret_cast<int*>(s.frc + 6 * nb);
+    s.flags = ip;
+    s.cnt = ip + nb;
+    return s;
+}
+
+// solver.py:50-94
+__device__ void integrate_rigid_body(TF& q, V3& v, V3& w, V3 f0, V3 t0, V3 com, const M33& I, float inv_mass,
+                                     const M33& inv_I, V3 g, float angular_damping, float dt) {
+    V3 x0 = q.p;
+    Q4 r0 = q.q;
+    V3 w0 = w, v0 = v;
+    V3 x_com = add(x0, qrot(r0, com));
+    float nz = inv_mass != 0.0f ? 1.0f : 0.0f;
+    V3 v1 = add(v0, mul(add(mul(f0, inv_mass), mul(g, nz)), dt));
+    V3 x1 = add(x_com, mul(v1, dt));
+    V3 wb = qrot_inv(r0, w0);
+    V3 tb = sub(qrot_inv(r0, t0), cross(wb, mv(I, wb)));
+    V3 w1 = qrot(r0, add(wb, mul(mv(inv_I, tb), dt)));
+    Q4 r1 = qnormalize(qadd(r0, qscale(qscale(qmul(Q4{w1.x, w1.y, w1.z, 0.0f}, r0), 0.5f), dt)));
+    w1 = mul(w1, 1.0f - angular_damping * dt);
+    q = TF{sub(x1, qrot(r1, com)), r1};
+    v = v1;
+    w = w1;
+}
+
+// kernels.py:809-878 with the weight already resolved
+__device__ void apply_body_delta(TF& q, V3& v, V3& w, V3 dlin, V3 dang, float weight, V3 com, const M33& I,
+                                 float inv_m, const M33& inv_I, float dt) {
+    if (inv_m == 0.0f) return;
+    V3 v0 = v, w0 = w;
+    V3 p0 = q.p;
+    Q4 q0 = q.q;
+    V3 dp = mul(dlin, inv_m * weight);
+    V3 dq = mul(dang, weight);
+    V3 wb = qrot_inv(q0, w0);
+    V3 dwb = mv(inv_I, qrot_inv(q0, dq));
+    V3 tb = add(cross(dwb, mv(I, add(wb, dwb))), cross(wb, mv(I, dwb)));
+    V3 dw1 = qrot(q0, sub(dwb, mv(mscale(dt, inv_I), tb)));
+    Q4 dq4 = qscale(Q4{dw1.x * dt, dw1.y * dt, dw1.z * dt, 0.0f}, 0.5f);
+    Q4 q1 = qadd(q0, qmul(dq4, q0));
+    q1 = qnormalize(q1);
+    V3 x_com = add(p0, qrot(q0, com));
+    V3 p1 = add(x_com, mul(dp, dt));
+    p1 = sub(p1, qrot(q1, com));
+    q = TF{p1, q1};
+    V3 v1 = add(v0, dp);
+    V3 w1 = add(w0, dw1);
+    if (length(v1) < 1e-4f) v1 = V3{0.0f, 0.0f, 0.0f};
+    if (length(w1) < 1e-4f) w1 = V3{0.0f, 0.0f, 0.0f};
+    v = v1;
+    w = w1;
+}
+
+// kernels.py:1945-1979
+__device__ float contact_constraint_delta(float err, Q4 qa, Q4 qb, float m_inv_a, float m_inv_b, const M33& Ia,
+                                          const M33& Ib, V3 la, V3 lb, V3 aa, V3 ab, float relaxation, float dt) {
+    float denom = 0.0f;
+    denom += length_sq(la) * m_inv_a;
+    denom += length_sq(lb) * m_inv_b;
+    V3 ra = qrot_inv(qa, aa);
+    V3 rb = qrot_inv(qb, ab);
+    denom += dot(ra, mv(Ia, ra));
+    denom += dot(rb, mv(Ib, rb));
+    float dl = -err;
+    if (denom > 0.0f) dl /= dt * denom;
+    return dl * relaxation;
+}
+
+// kernels.py:1982-2022
+__device__ float positional_correction(float err, float derr, Q4 qa, Q4 qb, float m_inv_a, float m_inv_b,
+                                       const M33& Ia, const M33& Ib, V3 la, V3 lb, V3 aa, V3 ab, float lambda_in,
+                                       float compliance, float damping, float dt) {
+    float denom = 0.0f;
+    denom += length_sq(la) * m_inv_a;
+    denom += length_sq(lb) * m_inv_b;
+    V3 ra = qrot_inv(qa, aa);
+    V3 rb = qrot_inv(qb, ab);
+    denom += dot(ra, mv(Ia, ra));
+    denom += dot(rb, mv(Ib, rb));
+    float alpha = compliance;
+    float gamma = compliance * damping;
+    float dl = -(err + alpha * lambda_in + gamma * derr);
+    if (denom + alpha > 0.0f) dl /= (dt + gamma) * denom + alpha / dt;
+    return dl;
+}
+
+// kernels.py:2025-2059
+__device__ float angular_correction(float err, float derr, Q4 qa, Q4 qb, const M33& Ia, const M33& Ib, V3 aa, V3 ab,
+                                    float lambda_in, float compliance, float damping, float dt) {
+    float denom = 0.0f;
+    V3 ra = qrot_inv(qa, aa);
+    V3 rb = qrot_inv(qb, ab);
+    denom += dot(ra, mv(Ia, ra));
+    denom += dot(rb, mv(Ib, rb));
+    float alpha = compliance;
+    float gamma = compliance * damping;
+    float dl = -(err + alpha * lambda_in + gamma * derr);
+    if (denom + alpha > 0.0f) dl /= (dt + gamma) * denom + alpha / dt;
+    return dl;
+}
+
+// solve_body_contact_positions for one contact (kernels.py:2062-2298)
+__device__ void solve_contact(const NbModelDesc& m, SBodies& S, float4 r0, float4 r1, float4 r2, float4 r3, float4 r4,
+                              float relaxation, float dt, bool weighting, unsigned* bad) {
+    const int sa = __float_as_int(r2.w), sb = __float_as_int(r3.w);
+    if (sa == sb) return;
+    const int tag = __float_as_int(r4.w);
+    const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
+    if (la == lb) return;
+    TF Xa = la >= 0 ? S.q(la) : tf_identity();
+    TF Xb = lb >= 0 ? S.q(lb) : tf_identity();
+    V3 bx_a = tf_point(Xa, V3{r0.x, r0.y, r0.z});
+    V3 bx_b = tf_point(Xb, V3{r1.x, r1.y, r1.z});
+    float thickness = r0.w + r1.w;
+    V3 n{r2.x, r2.y, r2.z};
+    float d = dot(n, sub(bx_b, bx_a)) - thickness;
+    if (d >= 0.0f) return;
+    float m_inv_a = 0.0f, m_inv_b = 0.0f;
+    M33 Ia = zero_m33(), Ib = zero_m33();
+    V3 com_a{0, 0, 0}, com_b{0, 0, 0};
+    V3 om_a{0, 0, 0}, om_b{0, 0, 0};
+    V3 off_a{r3.x, r3.y, r3.z}, off_b{r4.x, r4.y, r4.z};
+    if (la >= 0) { com_a = S.com(la); m_inv_a = S.inv_m(la); Ia = S.inv_inertia(la); om_a = S.w(la); }
+    if (lb >= 0) { com_b = S.com(lb); m_inv_b = S.inv_m(lb); Ib = S.inv_inertia(lb); om_b = S.w(lb); }
+    int nz = 0;
+    float mu = 0.0f, mut = 0.0f, mur = 0.0f;
+    if (sa >= 0) { nz += 1; mu += __ldg(m.shape_mu + sa); mut += __ldg(m.shape_mu_torsional + sa); mur += __ldg(m.shape_mu_rolling + sa); }
+    if (sb >= 0) { nz += 1; mu += __ldg(m.shape_mu + sb); mut += __ldg(m.shape_mu_torsional + sb); mur += __ldg(m.shape_mu_rolling + sb); }
+    if (nz > 0) { mu /= (float)nz; mut /= (float)nz; mur /= (float)nz; }
+    V3 r_a = sub(bx_a, tf_point(Xa, com_a));
+    V3 r_b = sub(bx_b, tf_point(Xb, com_b));
+    V3 ang_a = neg(cross(r_a, n));
+    V3 ang_b = cross(r_b, n);
+    if (weighting) {
+        if (la >= 0) atomicAdd(&S.cnt[la], 1);
+        if (lb >= 0) atomicAdd(&S.cnt[lb], 1);
+    }
+    float lambda_n = contact_constraint_delta(d, Xa.q, Xb.q, m_inv_a, m_inv_b, Ia, Ib, neg(n), n, ang_a, ang_b,
+                                              relaxation, dt);
+    V3 lin_da = mul(neg(n), lambda_n);
+    V3 lin_db = mul(n, lambda_n);
+    V3 ang_da = mul(ang_a, lambda_n);
+    V3 ang_db = mul(ang_b, lambda_n);
+    if (mu > 0.0f) {
+        bx_a = add(bx_a, tf_vector(Xa, off_a));
+        bx_b = add(bx_b, tf_vector(Xb, off_b));
+        V3 delta = sub(bx_b, bx_a);
+        V3 fd = sub(delta, smul(dot(n, delta), n));
+        r_a = sub(bx_a, tf_point(Xa, com_a));
+        r_b = sub(bx_b, tf_point(Xb, com_b));
+        V3 rvk{0.0f, 0.0f, 0.0f};
+        if (la >= 0 && (S.flags[la] & NB_BODY_KINEMATIC)) {
+            V3 va = add(cross(S.w(la), r_a), S.v(la));
+            rvk = sub(rvk, sub(va, smul(dot(n, va), n)));
+        }
+        if (lb >= 0 && (S.flags[lb] & NB_BODY_KINEMATIC)) {
+            V3 vb = add(cross(S.w(lb), r_b), S.v(lb));
+            rvk = add(rvk, sub(vb, smul(dot(n, vb), n)));
+        }
+        fd = add(fd, mul(rvk, dt));
+        V3 perp = normalize(fd);
+        ang_a = neg(cross(r_a, perp));
+        ang_b = cross(r_b, perp);
+        float err = length(fd);
+        if (err > 0.0f) {
+            float lf = contact_constraint_delta(err, Xa.q, Xb.q, m_inv_a, m_inv_b, Ia, Ib, neg(perp), perp, ang_a,
+                                                ang_b, relaxation, dt);
+            lf = fmaxw(lf, -lambda_n * mu);
+            lin_da = sub(lin_da, mul(perp, lf));
+            lin_db = add(lin_db, mul(perp, lf));
+            ang_da = add(ang_da, mul(ang_a, lf));
+            ang_db = add(ang_db, mul(ang_b, lf));
+        }
+    }
+    V3 dom = sub(om_b, om_a);
+    if (mut > 0.0f) {
+        float err = dot(dom, n) * dt;
+        if (fabsf(err) > 0.0f) {
+            V3 z{0.0f, 0.0f, 0.0f};
+            float lt = contact_constraint_delta(err, Xa.q, Xb.q, m_inv_a, m_inv_b, Ia, Ib, z, z, neg(n), n,
+                                                relaxation, dt);
+            lt = clampw(lt, -lambda_n * mut, lambda_n * mut);
+            ang_da = sub(ang_da, mul(n, lt));
+            ang_db = add(ang_db, mul(n, lt));
+        }
+    }
+    if (mur > 0.0f) {
+        dom = sub(dom, smul(dot(n, dom), n));
+        float err = length(dom) * dt;
+        if (err > 0.0f) {
+            V3 z{0.0f, 0.0f, 0.0f};
+            V3 rn = normalize(dom);
+            float lr = contact_constraint_delta(err, Xa.q, Xb.q, m_inv_a, m_inv_b, Ia, Ib, z, z, neg(rn), rn,
+                                                relaxation, dt);
+            lr = fmaxw(lr, -lambda_n * mur);
+            ang_da = sub(ang_da, mul(rn, lr));
+            ang_db = add(ang_db, mul(rn, lr));
+        }
+    }
+    if (la >= 0) S.add_delta(la, lin_da, ang_da, bad);
+    if (lb >= 0) S.add_delta(lb, lin_db, ang_db, bad);
+}
+
+__device__ V3 vabs(V3 a) { return V3{fabsf(a.x), fabsf(a.y), fabsf(a.z)}; }
+
+__device__ void weighted_target(V3 axis, float target, float weight, V3& tgt, V3& wts) {
+    V3 wa = mul(axis, weight);
+    tgt = add(tgt, mul(wa, target));
+    wts = add(wts, vabs(wa));
+}
+
+__device__ void joint_axes(const NbModelDesc& m, int start, int count, const float* tpos, const float* tvel, V3& lo,
+                           V3& hi, V3& tp, V3& stiff, V3& tv, V3& damp) {
+    lo = V3{0, 0, 0}; hi = V3{0, 0, 0};
+    tp = V3{0, 0, 0}; stiff = V3{0, 0, 0}; tv = V3{0, 0, 0}; damp = V3{0, 0, 0};
+    for (int k = 0; k < count && k < 3; ++k) {
+        int i = start + k;
+        V3 axis = load_v3(m.joint_axis + 3 * (size_t)i);
+        V3 lt = mul(axis, m.joint_limit_lower[i]);
+        V3 ut = mul(axis, m.joint_limit_upper[i]);
+        if (k == 0) {
+            lo = vmin(lt, ut);
+            hi = vmax(lt, ut);
+        } else {
+            V3 l2 = vmin(lt, ut), u2 = vmax(lt, ut);
+            lo = vmin(lo, l2);
+            hi = vmax(hi, u2);
+        }
+        float ke = m.joint_target_ke[i], kd = m.joint_target_kd[i];
+        float tpi = tpos ? tpos[i] : 0.0f, tvi = tvel ? tvel[i] : 0.0f;
+        if (ke > 0.0f) weighted_target(axis, tpi, ke, tp, stiff);
+        if (kd > 0.0f) weighted_target(axis, tvi, kd, tv, damp);
+    }
+    for (int i = 0; i < 3; ++i)
+        if (comp(stiff, i) > 0.0f) set_comp(tp, i, comp(tp, i) / comp(stiff, i));
+    for (int i = 0; i < 3; ++i)
+        if (comp(damp, i) > 0.0f) set_comp(tv, i, comp(tv, i) / comp(damp, i));
+}
+
+// solve_body_joints for one joint (kernels.py:1441-1942)
+__device__ __noinline__ void solve_joint(const NbModelDesc& m, SBodies& S, int b0, int j, const float* tpos,
+                                         const float* tvel, const NbXpbdParams& p, float dt, unsigned* bad) {
+    int type = m.joint_type[j];
+    if (!m.joint_enabled[j]) return;
+    if (type == NB_JOINT_FREE) return;
+    int id_c = m.joint_child[j], id_p = m.joint_parent[j];
+    int lc = id_c - b0, lp = id_p < 0 ? -1 : id_p - b0;
+    TF X_pj = load_tf(m.joint_X_p + 7 * (size_t)j);
+    TF X_cj = load_tf(m.joint_X_c + 7 * (size_t)j);
+    TF X_wp = X_pj;
+    float m_inv_p = 0.0f;
+    M33 I_inv_p = zero_m33();
+    TF pose_p = X_pj;
+    V3 com_p{0, 0, 0}, vel_p{0, 0, 0}, om_p{0, 0, 0};
+    if (id_p >= 0) {
+        pose_p = S.q(lp);
+        X_wp = tf_mul(pose_p, X_wp);
+        com_p = S.com(lp);
+        m_inv_p = S.inv_m(lp);
+        I_inv_p = S.inv_inertia(lp);
+        vel_p = S.v(lp);
+        om_p = S.w(lp);
+    }
+    TF pose_c = S.q(lc);
+    TF X_wc = tf_mul(pose_c, X_cj);
+    V3 com_c = S.com(lc);
+    float m_inv_c = S.inv_m(lc);
+    M33 I_inv_c = S.inv_inertia(lc);
+    V3 vel_c = S.v(lc), om_c = S.w(lc);
+    if (m_inv_p == 0.0f && m_inv_c == 0.0f) return;
+    V3 ldp{0, 0, 0}, adp{0, 0, 0}, ldc{0, 0, 0}, adc{0, 0, 0};
+    TF rel = tf_mul(tf_inverse(X_wp), X_wc);
+    V3 rel_p = rel.p;
+    V3 x_c = X_wc.p;
+    float lin_comp = p.joint_linear_compliance, ang_comp = p.joint_angular_compliance;
+    float ang_relax = p.joint_angular_relaxation, lin_relax = p.joint_linear_relaxation;
+    int axis_start = m.joint_qd_start[j];
+    int lin_count = m.joint_dof_dim[2 * j], ang_count = m.joint_dof_dim[2 * j + 1];
+    V3 wcom_p = tf_point(pose_p, com_p);
+    V3 wcom_c = tf_point(pose_c, com_c);
+    if (type == NB_JOINT_DISTANCE) {
+        V3 r_p = sub(X_wp.p, wcom_p);
+        V3 r_c = sub(X_wc.p, wcom_c);
+        float lower = m.joint_limit_lower[axis_start], upper = m.joint_limit_upper[axis_start];
+        if (lower < 0.0f && upper < 0.0f) return;
+        float d = length(rel_p);
+        float err = 0.0f;
+        if (lower >= 0.0f && d < lower) {
+            err = d - lower;
+            rel_p = smul(err, normalize(sub(wcom_c, wcom_p)));
+        } else if (upper >= 0.0f && d > upper) {
+            err = d - upper;
+        }
+        if (fabsf(err) > 1e-9f) {
+            V3 lin_c = rel_p;
+            V3 lin_p = neg(lin_c);
+            r_c = sub(x_c, wcom_c);
+            V3 ang_p = neg(cross(r_p, lin_c));
+            V3 ang_c = cross(r_c, lin_c);
+            float derr = dot(lin_p, vel_p) + dot(lin_c, vel_c) + dot(ang_p, om_p) + dot(ang_c, om_c);
+            float compliance = lin_comp;
+            float ke = m.joint_target_ke[axis_start];
+            if (ke > 0.0f) compliance = 1.0f / ke;
+            float damping = m.joint_target_kd[axis_start];
+            float dl = positional_correction(err, derr, pose_p.q, pose_c.q, m_inv_p, m_inv_c, I_inv_p, I_inv_c,
+                                             lin_p, lin_c, ang_p, ang_c, 0.0f, compliance, damping, dt);
+            ldp = add(ldp, mul(lin_p, dl * lin_relax));
+            adp = add(adp, mul(ang_p, dl * ang_relax));
+            ldc = add(ldc, mul(lin_c, dl * lin_relax));
+            adc = add(adc, mul(ang_c, dl * ang_relax));
+        }
+    } else {
+        V3 lo, hi, tp, stiff, tv, damp;
+        joint_axes(m, axis_start, lin_count, tpos, tvel, lo, hi, tp, stiff, tv, damp);
+        M33 frame_p = quat_to_matrix(X_wp.q);
+        V3 r_p = sub(x_c, wcom_p);
+        V3 r_c = sub(x_c, tf_point(pose_c, com_c));
+        for (int dim = 0; dim < 3; ++dim) {
+            float e = comp(rel_p, dim);
+            V3 lin_c{frame_p.m[0][dim], frame_p.m[1][dim], frame_p.m[2][dim]};
+            V3 lin_p = neg(lin_c);
+            V3 ang_p = neg(cross(r_p, lin_c));
+            V3 ang_c = cross(r_c, lin_c);
+            float derr = dot(lin_p, vel_p) + dot(lin_c, vel_c) + dot(ang_p, om_p) + dot(ang_c, om_c);
+            float err = 0.0f, compliance = lin_comp, damping = 0.0f;
+            float target_vel = comp(tv, dim);
+            float derr_rel = derr - target_vel;
+            float lower = comp(lo, dim), upper = comp(hi, dim);
+            if (e < lower) err = e - lower;
+            else if (e > upper) err = e - upper;
+            else {
+                float target_pos = clampw(comp(tp, dim), lower, upper);
+                if (comp(stiff, dim) > 0.0f) {
+                    err = e - target_pos;
+                    compliance = 1.0f / comp(stiff, dim);
+                    damping = comp(damp, dim);
+                } else if (comp(damp, dim) > 0.0f) {
+                    compliance = 1.0f / comp(damp, dim);
+                    damping = comp(damp, dim);
+                }
+            }
+            if (fabsf(err) > 1e-9f || fabsf(derr_rel) > 1e-9f) {
+                float dl = positional_correction(err, derr_rel, pose_p.q, pose_c.q, m_inv_p, m_inv_c, I_inv_p,
+                                                 I_inv_c, lin_p, lin_c, ang_p, ang_c, 0.0f, compliance, damping, dt);
+                ldp = add(ldp, mul(lin_p, dl * lin_relax));
+                adp = add(adp, mul(ang_p, dl * ang_relax));
+                ldc = add(ldc, mul(lin_c, dl * lin_relax));
+                adc = add(adc, mul(ang_c, dl * ang_relax));
+            }
+        }
+    }
+    if (type == NB_JOINT_FIXED || type == NB_JOINT_PRISMATIC || type == NB_JOINT_REVOLUTE || type == NB_JOINT_D6) {
+        Q4 q_p = X_wp.q, q_c = X_wc.q;
+        if (qdot(q_p, q_c) < 0.0f) q_c = qscale(q_c, -1.0f);
+        Q4 rq = qmul(qinv(q_p), q_c);
+        Q4 qtwist = qnormalize(Q4{rq.x, 0.0f, 0.0f, rq.w});
+        Q4 qswing = qmul(rq, qinv(qtwist));
+        float s = sqrtf(rq.x * rq.x + rq.w * rq.w);
+        float invs = 1.0f / s;
+        float invscube = invs * invs * invs;
+        float err0 = 2.0f * asinf(clampw(qtwist.x, -1.0f, 1.0f));
+        float err1 = qswing.y, err2 = qswing.z;
+        Q4 g0{invs - rq.x * rq.x * invscube, 0.0f, 0.0f, -(rq.w * rq.x) * invscube};
+        Q4 g1{-rq.w * (rq.w * rq.z + rq.x * rq.y) * invscube, rq.w * invs, -rq.x * invs,
+              rq.x * (rq.w * rq.z + rq.x * rq.y) * invscube};
+        Q4 g2{rq.w * (rq.w * rq.y - rq.x * rq.z) * invscube, rq.x * invs, rq.w * invs,
+              rq.x * (rq.z * rq.x - rq.w * rq.y) * invscube};
+        g0 = qscale(g0, 2.0f / fabsf(qtwist.w));
+        float swing_sq = qswing.w * qswing.w;
+        if (swing_sq + 1.0e-4f < 1.0f) {
+            float d = sqrtf(1.0f - qswing.w * qswing.w);
+            float theta = 2.0f * acosf(clampw(qswing.w, -1.0f, 1.0f));
+            float scale = theta / d;
+            err1 *= scale;
+            err2 *= scale;
+            g1 = qscale(g1, scale);
+            g2 = qscale(g2, scale);
+        }
+        V3 lo, hi, tp, stiff, tv, damp;
+        joint_axes(m, axis_start + lin_count, ang_count, tpos, tvel, lo, hi, tp, stiff, tv, damp);
+        for (int dim = 0; dim < 3; ++dim) {
+            float e = dim == 0 ? err0 : (dim == 1 ? err1 : err2);
+            Q4 grad = dim == 0 ? g0 : (dim == 1 ? g1 : g2);
+            Q4 qc4 = qmul(qmul(qscale(q_p, 0.5f), grad), qinv(q_c));
+            V3 ang_c{qc4.x, qc4.y, qc4.z};
+            V3 ang_p = neg(ang_c);
+            float derr = dot(ang_p, om_p) + dot(ang_c, om_c);
+            float err = 0.0f, compliance = ang_comp, damping = 0.0f;
+            float target_vel = comp(tv, dim);
+            float acl = length(ang_c);
+            float derr_rel = derr - target_vel * acl;
+            float lower = comp(lo, dim), upper = comp(hi, dim);
+            if (e < lower) err = e - lower;
+            else if (e > upper) err = e - upper;
+            else {
+                float target_pos = clampw(comp(tp, dim), lower, upper);
+                if (comp(stiff, dim) > 0.0f) {
+                    err = e - target_pos;
+                    compliance = 1.0f / comp(stiff, dim);
+                    damping = comp(damp, dim);
+                } else if (comp(damp, dim) > 0.0f) {
+                    damping = comp(damp, dim);
+                    compliance = 1.0f / comp(damp, dim);
+                }
+            }
+            float dl = angular_correction(err, derr_rel, pose_p.q, pose_c.q, I_inv_p, I_inv_c, ang_p, ang_c, 0.0f,
+                                          compliance, damping, dt) *
+                       ang_relax;
+            adp = add(adp, mul(ang_p, dl));
+            adc = add(adc, mul(ang_c, dl));
+        }
+    }
+    if (id_p >= 0) S.add_delta(lp, ldp, adp, bad);
+    if (id_c >= 0) S.add_delta(lc, ldc, adc, bad);
+}
+
+// apply_joint_forces (kernels.py:890-1003) for the world's joints, in joint order
+__device__ void joint_forces(const NbModelDesc& m, SBodies& S, int b0, int j0, int j1, const float* joint_f) {
+    for (int j = j0; j < j1; ++j) {
+        int type = m.joint_type[j];
+        if (!m.joint_enabled[j]) continue;
+        if (type == NB_JOINT_FIXED) continue;
+        int id_c = m.joint_child[j], id_p = m.joint_parent[j];
+        int lc = id_c - b0, lp = id_p < 0 ? -1 : id_p - b0;
+        TF X_pj = load_tf(m.joint_X_p + 7 * (size_t)j), X_cj = load_tf(m.joint_X_c + 7 * (size_t)j);
+        TF X_wp = X_pj, pose_p = X_pj;
+        V3 com_p{0, 0, 0};
+        if (id_p >= 0) {
+            pose_p = S.q(lp);
+            X_wp = tf_mul(pose_p, X_wp);
+            com_p = S.com(lp);
+        }
+        V3 r_p = sub(X_wp.p, tf_point(pose_p, com_p));
+        TF pose_c = S.q(lc);
+        TF X_wc = tf_mul(pose_c, X_cj);
+        V3 r_c = sub(X_wc.p, tf_point(pose_c, S.com(lc)));
+        int qs = m.joint_qd_start[j];
+        int lin = m.joint_dof_dim[2 * j], ang = m.joint_dof_dim[2 * j + 1];
+        V3 t_total{0, 0, 0}, f_total{0, 0, 0};
+        float* F = S.frc;
+        const int nb = S.nb;
+        auto addw = [&](int b, V3 f, V3 t, bool plus) {
+            float v[6] = {f.x, f.y, f.z, t.x, t.y, t.z};
+            for (int k = 0; k < 6; ++k) F[k * nb + b] = plus ? F[k * nb + b] + v[k] : F[k * nb + b] - v[k];
+        };
+        if (type == NB_JOINT_FREE || type == NB_JOINT_DISTANCE) {
+            f_total = V3{joint_f[qs + 0], joint_f[qs + 1], joint_f[qs + 2]};
+            t_total = V3{joint_f[qs + 3], joint_f[qs + 4], joint_f[qs + 5]};
+            addw(lc, f_total, t_total, true);
+            if (id_p >= 0) addw(lp, f_total, t_total, false);
+            continue;
+        } else if (type == NB_JOINT_BALL) {
+            t_total = V3{joint_f[qs + 0], joint_f[qs + 1], joint_f[qs + 2]};
+        } else {
+            for (int k = 0; k < lin && k < 3; ++k)
+                f_total = add(f_total, smul(joint_f[qs + k], tf_vector(X_wp, load_v3(m.joint_axis + 3 * (size_t)(qs + k)))));
+            for (int k = 0; k < ang && k < 3; ++k)
+                t_total = add(t_total, smul(joint_f[qs + lin + k],
+                                            tf_vector(X_wp, load_v3(m.joint_axis + 3 * (size_t)(qs + lin + k)))));
+        }
+        if (id_p >= 0) addw(lp, f_total, add(t_total, cross(r_p, f_total)), false);
+        addw(lc, f_total, add(t_total, cross(r_c, f_total)), true);
+    }
+}
+
+__global__ void __launch_bounds__(kST, 2)
+xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, int has_contacts, float dt) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_world;
+    __shared__ unsigned s_bad;
+    SBodies S = sbodies_carve(smem, m.max_world_bodies);
+    const int tid = threadIdx.x;
+    const bool weighting = p.rigid_contact_con_weighting != 0;
+    const bool model_joints = m.joint_count > 0;
+    const float4* R0 = reinterpret_cast<const float4*>(seg.rec0);
+    const float4* R1 = reinterpret_cast<const float4*>(seg.rec1);
+    const float4* R2 = reinterpret_cast<const float4*>(seg.rec2);
+    const float4* R3 = reinterpret_cast<const float4*>(seg.rec3);
+    const float4* R4 = reinterpret_cast<const float4*>(seg.rec4);
+
+    for (;;) {
+        if (tid == 0) {
+            int k = atomicAdd(&seg.work_counter[1], 1);
+            s_world = k < m.world_count ? m.world_order[k] : -1;
+            s_bad = 0u;
+        }
+        __syncthreads();
+        const int w = s_world;
+        if (w < 0) break;
+        const int b0 = m.world_body_start[w];
+        const int nbw = m.world_body_start[w + 1] - b0;  // bodies of this world
+        const int nb = S.nb;                                // shared-memory stride
+        const int j0 = m.world_joint_start[w], j1 = m.world_joint_start[w + 1];
+        // ---- stage bodies
+        for (int i = tid; i < nbw; i += kST) {
+            const int b = b0 + i;
+            const int fl = m.body_flags[b];
+            const bool kin = (fl & NB_BODY_KINEMATIC) != 0;
+            S.flags[i] = fl;
+            const float* q = io.body_q_in + 7 * (size_t)b;
+            const float* qd = io.body_qd_in + 6 * (size_t)b;
+            for (int k = 0; k < 7; ++k) S.f[k * nb + i] = q[k];
+            for (int k = 0; k < 6; ++k) S.f[(7 + k) * nb + i] = qd[k];
+            const float* fb = io.body_f_in + 6 * (size_t)b;
+            for (int k = 0; k < 6; ++k) S.frc[k * nb + i] = fb[k];
+            for (int k = 0; k < 3; ++k) S.c[k * nb + i] = m.body_com[3 * (size_t)b + k];
+            S.c[3 * nb + i] = kin ? 0.0f : m.body_inv_mass[b];
+            for (int k = 0; k < 9; ++k) {
+                S.I[k * nb + i] = m.body_inertia[9 * (size_t)b + k];
+                S.iI[k * nb + i] = kin ? 0.0f : m.body_inv_inertia[9 * (size_t)b + k];
+            }
+            for (int k = 0; k < 6; ++k) S.acc[k * nb + i] = 0ull;
+            S.cnt[i] = 0;
+        }
+        __syncthreads();
+        // world needs a real joint pass only when it has a non-free enabled joint
+        int my_joint = 0;
+        for (int j = j0 + tid; j < j1; j += kST) my_joint |= (m.joint_type[j] != NB_JOINT_FREE && m.joint_enabled[j]);
+        const bool world_joints = __syncthreads_or(my_joint) != 0;
+        if (io.joint_f && tid == 0) joint_forces(m, S, b0, j0, j1, io.joint_f);
+        __syncthreads();
+        // ---- integrate_bodies
+        for (int i = tid; i < nbw; i += kST) {
+            if (S.flags[i] & NB_BODY_KINEMATIC) continue;
+            const int b = b0 + i;
+            int wi = m.body_world[b];
+            if (wi < 0) wi = 0;
+            V3 g = load_v3(m.gravity + 3 * (size_t)wi);
+            TF q = S.q(i);
+            V3 v = S.v(i), wv = S.w(i);
+            V3 f0{S.frc[0 * nb + i], S.frc[1 * nb + i], S.frc[2 * nb + i]};
+            V3 t0{S.frc[3 * nb + i], S.frc[4 * nb + i], S.frc[5 * nb + i]};
+            integrate_rigid_body(q, v, wv, f0, t0, S.com(i), S.inertia(i), m.body_inv_mass[b],
+                                 load_m33(m.body_inv_inertia + 9 * (size_t)b), g, p.angular_damping, dt);
+            S.set(i, q, v, wv);
+        }
+        __syncthreads();
+        const int nc = has_contacts ? seg.world_count[w] : 0;
+        const int64_t c0 = has_contacts ? m.contact_cap_start[w] : 0;
+        unsigned bad = 0u;
+        for (int it = 0; it < p.iterations; ++it) {
+            if (has_contacts) {
+                for (int c = tid; c < nc; c += kST) {
+                    const int64_t k = c0 + c;
+                    solve_contact(m, S, R0[k], R1[k], R2[k], R3[k], R4[k], p.rigid_contact_relaxation, dt, weighting,
+                                  &bad);
+                }
+                __syncthreads();
+                for (int i = tid; i < nbw; i += kST) {
+                    V3 dl, da;
+                    S.take(i, dl, da);
+                    float weight = 1.0f;
+                    if (weighting) {
+                        float iw = (float)S.cnt[i];
+                        S.cnt[i] = 0;
+                        if (iw > 0.0f) weight = 1.0f / iw;
+                    }
+                    TF q = S.q(i);
+                    V3 v = S.v(i), wv = S.w(i);
+                    const V3 com = S.com(i);
+                    const M33 I = S.inertia(i), iI = S.inv_inertia(i);
+                    const float im = S.inv_m(i);
+                    apply_body_delta(q, v, wv, dl, da, weight, com, I, im, iI, dt);
+                    if (model_joints && !world_joints) {
+                        // the joint pass of this world only renormalises (free joints)
+                        apply_body_delta(q, v, wv, V3{0.0f, 0.0f, 0.0f}, V3{0.0f, 0.0f, 0.0f}, 1.0f, com, I, im, iI,
+                                         dt);
+                    }
+                    S.set(i, q, v, wv);
+                }
+                __syncthreads();
+            }
+            if (model_joints && (world_joints || !has_contacts)) {
+                for (int j = j0 + tid; j < j1; j += kST)
+                    solve_joint(m, S, b0, j, io.joint_target_pos, io.joint_target_vel, p, dt, &bad);
+                __syncthreads();
+                for (int i = tid; i < nbw; i += kST) {
+                    V3 dl, da;
+                    S.take(i, dl, da);
+                    TF q = S.q(i);
+                    V3 v = S.v(i), wv = S.w(i);
+                    apply_body_delta(q, v, wv, dl, da, 1.0f, S.com(i), S.inertia(i), S.inv_m(i), S.inv_inertia(i), dt);
+                    S.set(i, q, v, wv);
+                }
+                __syncthreads();
+            }
+        }
+        // ---- write back (kinematic bodies pass through unchanged)
+        for (int i = tid; i < nbw; i += kST) {
+            const int b = b0 + i;
+            float* qo = io.body_q_out + 7 * (size_t)b;
+            float* qdo = io.body_qd_out + 6 * (size_t)b;
+            if (S.flags[i] & NB_BODY_KINEMATIC) {
+                for (int k = 0; k < 7; ++k) qo[k] = io.body_q_in[7 * (size_t)b + k];
+                for (int k = 0; k < 6; ++k) qdo[k] = io.body_qd_in[6 * (size_t)b + k];
+                continue;
+            }
+            bool finite = true;
+            for (int k = 0; k < 7; ++k) {
+                float x = S.f[k * nb + i];
+                finite = finite && isfinite(x);
+                qo[k] = x;
+            }
+            for (int k = 0; k < 6; ++k) qdo[k] = S.f[(7 + k) * nb + i];
+            if (!finite) bad |= 2u;
+        }
+        if (bad) atomicOr(&s_bad, bad);
+        __syncthreads();
+        if (tid == 0 && s_bad) {
+            unsigned st = 0;
+            if (s_bad & 1u) st |= NB_STATUS_FIXED_OVERFLOW;
+            if (s_bad & 2u) st |= NB_STATUS_NONFINITE;
+            atomicOr(seg.status, st);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+size_t nb_step_smem_bytes(const NbModelDesc* m) {
+    size_t nb = (size_t)(m->max_world_bodies > 0 ? m->max_world_bodies : 1);
+    return nb * (13 + 4 + 9 + 9 + 6) * sizeof(float) + nb * sizeof(int) + nb * 6 * sizeof(unsigned long long) +
+           nb * sizeof(int);
+}
+
+cudaError_t nb_launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
+                           float dt, int grid, cudaStream_t stream) {
+    size_t smem = nb_step_smem_bytes(m);
+    cudaError_t e = cudaFuncSetAttribute(xpbd_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(seg->work_counter + 1, 0, sizeof(int32_t), stream);
+    if (e != cudaSuccess) return e;
+    int has_contacts = seg->rec0 != nullptr && seg->world_count != nullptr;
+    xpbd_step_kernel<<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
+    return cudaGetLastError();
+}

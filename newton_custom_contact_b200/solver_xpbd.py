@@ -1,0 +1,156 @@
+"""SolverXPBD (newton/_src/solvers/xpbd/solver_xpbd.py) for rigid bodies on B200.
+
+``step(state_in, state_out, control, contacts, dt)`` is one launch of the fused
+per-world substep kernel (integrate, ``iterations`` x contact + joint
+projection, delta application) from libnewton_b200.so.  Differences from the
+reference that a caller can observe:
+  * ``state_in`` is left unchanged (the reference ping-pongs through it,
+    solver_xpbd.py:203-257);
+  * per-body constraint deltas are summed in 2^-32 fixed point, so results are
+    bit-reproducible and independent of contact order;
+  * particles, springs, restitution and contact-force reporting are not part
+    of this build and raise ``NotImplementedError``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _lib
+from ._abi import NbContactSeg, NbStepIO, NbXpbdParams, ptr
+from .contacts import Contacts
+
+
+class SolverNotifyFlags:
+    JOINT_PROPERTIES = 1 << 0
+    JOINT_DOF_PROPERTIES = 1 << 1
+    BODY_PROPERTIES = 1 << 2
+    BODY_INERTIAL_PROPERTIES = 1 << 3
+    SHAPE_PROPERTIES = 1 << 4
+    MODEL_PROPERTIES = 1 << 5
+
+
+class SolverXPBD:
+    """Rigid-body XPBD substep (Macklin et al. 2016, Müller et al. 2020)."""
+
+    def __init__(self, model, iterations: int = 2, soft_body_relaxation: float = 0.9,
+                 soft_contact_relaxation: float = 0.9, joint_linear_relaxation: float = 0.7,
+                 joint_angular_relaxation: float = 0.4, joint_linear_compliance: float = 0.0,
+                 joint_angular_compliance: float = 0.0, rigid_contact_relaxation: float = 0.8,
+                 rigid_contact_con_weighting: bool = True, angular_damping: float = 0.0,
+                 enable_restitution: bool = False):
+        if getattr(model, "particle_count", 0):
+            raise NotImplementedError("particles are not supported by this build")
+        if iterations < 0:
+            raise ValueError("iterations must be non-negative")
+        self.model = model
+        self.iterations = int(iterations)
+        self.soft_body_relaxation = soft_body_relaxation
+        self.soft_contact_relaxation = soft_contact_relaxation
+        self.joint_linear_relaxation = joint_linear_relaxation
+        self.joint_angular_relaxation = joint_angular_relaxation
+        self.joint_linear_compliance = joint_linear_compliance
+        self.joint_angular_compliance = joint_angular_compliance
+        self.rigid_contact_relaxation = rigid_contact_relaxation
+        self.rigid_contact_con_weighting = rigid_contact_con_weighting
+        self.angular_damping = angular_damping
+        self.enable_restitution = enable_restitution
+        self.compute_body_velocity_from_position_delta = False
+        self._desc_cache = {}
+        self._empty_seg = None
+        self._last_dt = None
+
+    @property
+    def device(self):
+        return self.model.device
+
+    def notify_model_changed(self, flags: int) -> None:
+        """Model arrays are read at every step; only cached descriptors are dropped."""
+        self._desc_cache.clear()
+
+    def params(self) -> NbXpbdParams:
+        p = NbXpbdParams()
+        p.iterations = self.iterations
+        p.rigid_contact_con_weighting = 1 if self.rigid_contact_con_weighting else 0
+        p.enable_restitution = 1 if self.enable_restitution else 0
+        p.joint_linear_relaxation = self.joint_linear_relaxation
+        p.joint_angular_relaxation = self.joint_angular_relaxation
+        p.joint_linear_compliance = self.joint_linear_compliance
+        p.joint_angular_compliance = self.joint_angular_compliance
+        p.rigid_contact_relaxation = self.rigid_contact_relaxation
+        p.angular_damping = self.angular_damping
+        return p
+
+    def _desc_for(self, contacts: Contacts | None):
+        pipe = contacts._layout if contacts is not None and contacts._layout is not None else None
+        if pipe is None:
+            pipe = self.model._default_pipeline()
+        key = id(pipe)
+        if key not in self._desc_cache:
+            self._desc_cache[key] = (pipe, pipe.desc())
+        return self._desc_cache[key]
+
+    @staticmethod
+    def _check_state(name, t, shape):
+        if t is None or t.dtype != torch.float32 or not t.is_contiguous() or tuple(t.shape) != shape:
+            raise TypeError(f"{name} must be a contiguous float32 tensor of shape {shape}")
+
+    def step(self, state_in, state_out, control, contacts: Contacts | None, dt: float) -> None:
+        model = self.model
+        _lib.require_cuda(model.device)
+        if self.enable_restitution:
+            raise NotImplementedError("restitution is not supported by this build")
+        if contacts is not None and contacts.force is not None:
+            raise NotImplementedError("contact force reporting is not supported by this build")
+        if model.body_count == 0:
+            return
+        if control is None:
+            control = model.control(clone_variables=False)
+        B = model.body_count
+        self._check_state("state_in.body_q", state_in.body_q, (B, 7))
+        self._check_state("state_in.body_qd", state_in.body_qd, (B, 6))
+        self._check_state("state_in.body_f", state_in.body_f, (B, 6))
+        self._check_state("state_out.body_q", state_out.body_q, (B, 7))
+        self._check_state("state_out.body_qd", state_out.body_qd, (B, 6))
+        lib = _lib.load()
+        stream = _lib.stream_handle(model.device)
+        pipe, desc = self._desc_for(contacts)
+        if contacts is not None:
+            if contacts._seg is None or contacts._layout is None:
+                pipe.attach_segments(contacts)
+            if not contacts._seg_valid:
+                pub = pipe.public_struct(contacts)
+                seg = pipe.seg_struct(contacts)
+                _lib.check("nb_ingest_contacts", lib.nb_ingest_contacts(C.byref(desc), C.byref(pub), C.byref(seg),
+                                                                        C.c_void_p(stream)))
+                contacts._seg_valid = True
+            seg = pipe.seg_struct(contacts)
+        else:
+            if self._empty_seg is None:
+                self._empty_seg = {"work_counter": torch.zeros(4, dtype=torch.int32, device=model.device),
+                                   "status": torch.zeros(1, dtype=torch.int32, device=model.device)}
+            seg = NbContactSeg()
+            seg.work_counter = ptr(self._empty_seg["work_counter"])
+            seg.status = ptr(self._empty_seg["status"])
+        io = NbStepIO()
+        io.body_q_in = ptr(state_in.body_q)
+        io.body_qd_in = ptr(state_in.body_qd)
+        io.body_f_in = ptr(state_in.body_f)
+        io.body_q_out = ptr(state_out.body_q)
+        io.body_qd_out = ptr(state_out.body_qd)
+        io.joint_target_pos = ptr(control.joint_target_pos)
+        io.joint_target_vel = ptr(control.joint_target_vel)
+        io.joint_f = ptr(control.joint_f)
+        params = self.params()
+        grid, _ = pipe._scratch()
+        _lib.check("nb_xpbd_step", lib.nb_xpbd_step(C.byref(desc), C.byref(params), C.byref(io), C.byref(seg),
+                                                    float(dt), grid, C.c_void_p(stream)))
+        self._last_dt = dt
+
+    def update_contacts(self, contacts: Contacts, state=None) -> None:
+        if contacts.force is None:
+            raise ValueError("contacts.force is not allocated. Call model.request_contact_attributes('force') "
+                             "before creating the Contacts object.")
+        raise ValueError("No contact impulse data available. Call step() before update_contacts().")

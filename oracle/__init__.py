@@ -1,0 +1,160 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes bindings of the CPU oracle (liboracle.so).
+
+The oracle restates the reference's collide + SolverXPBD rigid path in
+sequential C++ (oracle_collide.cpp, oracle_xpbd.cpp).  Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg may import it; the
+product package never does.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+ACC_FIXED = 0
+ACC_FLOAT = 1
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        lib = C.CDLL(LIB)
+        lib.orc_collide.restype = C.c_int
+        lib.orc_collide.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.orc_step.restype = C.c_int
+        lib.orc_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int,
+                                 C.POINTER(C.c_uint32)]
+        lib.orc_shape_aabbs.restype = C.c_int
+        lib.orc_shape_aabbs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.orc_collide_pair.restype = C.c_int
+        lib.orc_collide_pair.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                                         C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                                         C.c_void_p, C.c_int]
+        _lib = lib
+    return _lib
+
+
+def _f32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+def collide_pair(type_a, xf_a, scale_a, type_b, xf_b, scale_b, margin_a=0.0, margin_b=0.0, gap_a=0.1, gap_b=0.1):
+    """Narrow phase of one pair of static shapes in world space.
+
+    Returns an array [n, 16]: point0(3) point1(3) normal(3) margin0 margin1 d sub shape0 shape1 0,
+    where d = n.(p1 - p0) - (margin0 + margin1) is the signed separation.
+    """
+    lib = load()
+    out = np.zeros((8, 16), np.float32)
+    xa, sa, xb, sb = _f32(xf_a), _f32(scale_a), _f32(xf_b), _f32(scale_b)
+    n = lib.orc_collide_pair(int(type_a), xa.ctypes.data, sa.ctypes.data, margin_a, gap_a,
+                             int(type_b), xb.ctypes.data, sb.ctypes.data, margin_b, gap_b,
+                             out.ctypes.data, 8)
+    return out[:n].copy()
+
+
+class HostSegments:
+    """Host-side solver-format contact segments for one pipeline layout."""
+
+    def __init__(self, capacity: int, world_count: int):
+        cap = max(1, capacity)
+        self.rec = [np.zeros((cap, 4), np.float32) for _ in range(5)]
+        self.world_count = np.zeros(world_count, np.int32)
+        self.status = np.zeros(1, np.uint32)
+        self.work = np.zeros(4, np.int32)
+
+    def struct(self):
+        from newton_custom_contact_b200._abi import NbContactSeg
+
+        s = NbContactSeg()
+        for k in range(5):
+            setattr(s, f"rec{k}", self.rec[k].ctypes.data)
+        s.world_count = self.world_count.ctypes.data
+        s.work_counter = self.work.ctypes.data
+        s.status = self.status.ctypes.data
+        return s
+
+
+def model_desc(model, layout):
+    """NbModelDesc over host numpy arrays of `model` and a PairLayout."""
+    arrays = model.host_arrays()
+    hd = layout.host_dict()
+    arrays.update(hd)
+    keep = [arrays, hd]
+    desc = model.make_desc(arrays, layout.info())
+    desc._keep = keep
+    return desc
+
+
+def collide(model, layout, body_q: np.ndarray) -> HostSegments:
+    lib = load()
+    segs = HostSegments(layout.contact_capacity, model.world_count)
+    desc = model_desc(model, layout)
+    bq = _f32(body_q)
+    st = segs.struct()
+    rc = lib.orc_collide(C.addressof(desc), bq.ctypes.data, C.addressof(st))
+    if rc != 0:
+        raise RuntimeError(f"orc_collide failed ({rc})")
+    return segs
+
+
+def step(model, layout, params, body_q, body_qd, body_f, segs: HostSegments | None, dt: float,
+         joint_target_pos=None, joint_target_vel=None, joint_f=None, acc_mode: int = ACC_FIXED):
+    """One SolverXPBD.step on the CPU.  Returns (body_q_out, body_qd_out, status)."""
+    from newton_custom_contact_b200._abi import NbStepIO
+
+    lib = load()
+    desc = model_desc(model, layout)
+    q_in, qd_in, f_in = _f32(body_q), _f32(body_qd), _f32(body_f)
+    q_out = np.zeros_like(q_in)
+    qd_out = np.zeros_like(qd_in)
+    io = NbStepIO()
+    io.body_q_in = q_in.ctypes.data
+    io.body_qd_in = qd_in.ctypes.data
+    io.body_f_in = f_in.ctypes.data
+    io.body_q_out = q_out.ctypes.data
+    io.body_qd_out = qd_out.ctypes.data
+    keep = []
+    for name, arr in (("joint_target_pos", joint_target_pos), ("joint_target_vel", joint_target_vel),
+                      ("joint_f", joint_f)):
+        if arr is not None and np.asarray(arr).size:
+            a = _f32(arr)
+            keep.append(a)
+            setattr(io, name, a.ctypes.data)
+    status = C.c_uint32(0)
+    st = segs.struct() if segs is not None else None
+    rc = lib.orc_step(C.addressof(desc), C.addressof(params), C.addressof(io),
+                      C.addressof(st) if st is not None else None, float(dt), int(acc_mode), C.byref(status))
+    if rc != 0:
+        raise RuntimeError(f"orc_step failed ({rc})")
+    return q_out, qd_out, int(status.value)
+
+
+def contacts_table(model, layout, segs: HostSegments) -> np.ndarray:
+    """All live contacts as rows (world, shape0, shape1, sub, p0(3), p1(3), n(3), o0(3), o1(3), m0, m1)."""
+    rows = []
+    cs = layout.contact_cap_start
+    for w in range(model.world_count):
+        n = int(segs.world_count[w])
+        for k in range(cs[w], cs[w] + n):
+            r0, r1, r2, r3, r4 = (segs.rec[i][k] for i in range(5))
+            s0 = int(r2[3:4].view(np.int32)[0])
+            s1 = int(r3[3:4].view(np.int32)[0])
+            tag = int(r4[3:4].view(np.int32)[0])
+            rows.append([w, s0, s1, (tag >> 24) & 0xFF, *r0[:3], *r1[:3], *r2[:3], *r3[:3], *r4[:3], r0[3], r1[3]])
+    return np.asarray(rows, dtype=np.float64).reshape(-1, 21)

@@ -1,0 +1,144 @@
+"""Known-answer tests of the CPU oracle's narrow phase.
+
+Expected values are the assertions of the reference's own tests:
+newton/tests/test_collision_primitives.py (plane-sphere :429, sphere-sphere :505,
+sphere-box :1136, plane-box :1335, box-box :1529, box-box depths :1881) and
+newton/tests/test_narrow_phase.py (box-box face :635, edge :708, capsules
+:801-895, plane-capsule :1083).  Contacts here run the full pipeline path
+(primitive routing, MPR/GJK, manifold, write_contact gap test) with gap 0 on
+both shapes, i.e. the reference primitive with margin 0.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+from newton_custom_contact_b200 import GeoType
+
+P, S, C, B = int(GeoType.PLANE), int(GeoType.SPHERE), int(GeoType.CAPSULE), int(GeoType.BOX)
+ID = [0.0, 0.0, 0.0, 1.0]
+
+
+def xf(p, q=ID):
+    return list(p) + list(q)
+
+
+def run(orc, ta, pa, sa, tb, pb, sb, gap=0.0, qa=ID, qb=ID):
+    return orc.collide_pair(ta, xf(pa, qa), sa, tb, xf(pb, qb), sb, gap_a=gap, gap_b=gap)
+
+
+@pytest.mark.parametrize("z,n,dist", [(2.0, 0, None), (1.0, 4, 0.0), (0.9, 4, -0.1), (0.8, 4, -0.2),
+                                      (0.7, 4, -0.3), (0.5, 4, -0.5)])
+def test_plane_box(orc, z, n, dist):
+    rows = run(orc, P, [0, 0, 0], [0, 0, 0], B, [0, 0, z], [1, 1, 1])
+    assert rows.shape[0] == n
+    for r in rows:
+        assert r[11] == pytest.approx(dist, abs=0.01)
+        assert np.dot(r[6:9], [0, 0, 1]) > 0.99
+
+
+@pytest.mark.parametrize("z,dist", [(1.0, 0.0), (0.8, -0.2), (0.5, -0.5), (0.2, -0.8)])
+def test_plane_sphere(orc, z, dist):
+    rows = run(orc, P, [0, 0, 0], [0, 0, 0], S, [0, 0, z], [1, 0, 0])
+    assert rows.shape[0] == 1
+    assert rows[0, 11] == pytest.approx(dist, abs=1e-5)
+
+
+def test_plane_sphere_separated_beyond_gap(orc):
+    assert run(orc, P, [0, 0, 0], [0, 0, 0], S, [0, 0, 2.0], [1, 0, 0]).shape[0] == 0
+    # within the summed gap the speculative contact is kept
+    rows = run(orc, P, [0, 0, 0], [0, 0, 0], S, [0, 0, 1.5], [1, 0, 0], gap=0.3)
+    assert rows.shape[0] == 1 and rows[0, 11] == pytest.approx(0.5, abs=1e-5)
+
+
+@pytest.mark.parametrize("x2,r1,dist", [(2.0, 1.0, 0.0), (1.8, 1.0, -0.2), (1.5, 1.0, -0.5), (1.2, 1.0, -0.8),
+                                        (1.5, 0.5, 0.0), (1.2, 0.5, -0.3)])
+def test_sphere_sphere(orc, x2, r1, dist):
+    rows = run(orc, S, [0, 0, 0], [r1, 0, 0], S, [x2, 0, 0], [1, 0, 0])
+    assert rows.shape[0] == 1
+    assert rows[0, 11] == pytest.approx(dist, abs=1e-5)
+    assert rows[0, 6:9] == pytest.approx([1, 0, 0], abs=1e-6)
+
+
+@pytest.mark.parametrize("p,r,dist", [([1.5, 0, 0], 0.5, 0.0), ([1.4, 0, 0], 0.5, -0.1), ([1.3, 0, 0], 0.5, -0.2),
+                                      ([1.2, 0, 0], 0.5, -0.3), ([0, 0, 1.5], 0.5, 0.0), ([0, 0, 1.3], 0.5, -0.2),
+                                      ([0, 0, 0.4], 0.3, -0.9)])
+def test_sphere_box(orc, p, r, dist):
+    rows = run(orc, S, p, [r, 0, 0], B, [0, 0, 0], [1, 1, 1])
+    assert rows.shape[0] == 1
+    assert rows[0, 11] == pytest.approx(dist, abs=0.01)
+
+
+def test_box_box_separated_and_overlapping(orc):
+    assert run(orc, B, [0, 0, 0], [1, 1, 1], B, [3.0, 0, 0], [1, 1, 1]).shape[0] == 0
+    rows = run(orc, B, [0, 0, 0], [1, 1, 1], B, [1.5, 0, 0], [1, 1, 1])
+    assert rows.shape[0] > 0
+    for r in rows:
+        assert np.linalg.norm(r[6:9]) == pytest.approx(1.0, abs=0.01)
+        assert np.dot(r[6:9], [1, 0, 0]) > -0.1
+
+
+def test_box_box_face_depth(orc):
+    rows = run(orc, B, [0, 0, 0], [1, 1, 1], B, [1.8, 0, 0], [1, 1, 1])
+    assert rows.shape[0] > 0
+    xs = [r for r in rows if abs(r[6]) > 0.9]
+    assert xs, "expected a contact with an x-axis normal"
+    for r in xs:
+        assert r[11] == pytest.approx(-0.2, abs=0.05)
+        assert r[6] > 0
+
+
+@pytest.mark.parametrize("z,dist", [(1.1, 0.1), (1.0, 0.0), (0.9, -0.1), (0.8, -0.2), (0.7, -0.3)])
+def test_box_box_face_steps(orc, z, dist):
+    rows = run(orc, B, [0, 0, 0], [0.5, 0.5, 0.5], B, [0, 0, z], [0.5, 0.5, 0.5], gap=0.1)
+    assert rows.shape[0] >= 1
+    deepest = rows[:, 11].min()
+    assert deepest == pytest.approx(dist, abs=0.02)
+    assert np.all(rows[:, 8] > 0.99)
+
+
+def test_box_box_edge(orc):
+    a = math.pi / 4
+    rows = run(orc, B, [0, 0, 0], [0.5, 0.5, 0.5], B, [1.2, 0, 0], [0.5, 0.5, 0.5],
+               qb=[0, 0, math.sin(a / 2), math.cos(a / 2)])
+    assert rows.shape[0] > 0
+    assert np.linalg.norm(rows[0, 6:9]) == pytest.approx(1.0, abs=1e-5)
+
+
+def test_capsule_capsule_parallel_two_contacts(orc):
+    # both along z, side by side: the parallel branch emits two contacts
+    rows = run(orc, C, [0, 0, 0], [0.5, 1.0, 0], C, [0.9, 0, 0], [0.5, 1.0, 0])
+    assert rows.shape[0] == 2
+    assert np.allclose(rows[:, 11], -0.1, atol=1e-5)
+
+
+def test_capsule_capsule_crossed_one_contact(orc):
+    qx = [math.sin(math.pi / 4), 0, 0, math.cos(math.pi / 4)]
+    rows = run(orc, C, [0, 0, 0], [0.5, 1.0, 0], C, [0.9, 0, 0], [0.5, 1.0, 0], qb=qx)
+    assert rows.shape[0] == 1
+    assert rows[0, 11] == pytest.approx(-0.1, abs=1e-5)
+
+
+def test_plane_capsule_resting(orc):
+    qx = [math.sin(math.pi / 4), 0, 0, math.cos(math.pi / 4)]  # axis along y, lying on the plane
+    rows = run(orc, P, [0, 0, 0], [0, 0, 0], C, [0, 0, 0.5], [0.5, 1.0, 0], qb=qx)
+    assert rows.shape[0] == 2
+    assert np.allclose(rows[:, 11], 0.0, atol=1e-5)
+
+
+def test_capsule_box_gjk(orc):
+    # capsule lying on top of a box face: routed to MPR/GJK + manifold
+    qx = [math.sin(math.pi / 4), 0, 0, math.cos(math.pi / 4)]
+    rows = run(orc, C, [0, 0, 1.45], [0.5, 0.5, 0], B, [0, 0, 0], [1, 1, 1], qa=qx)
+    assert rows.shape[0] >= 1
+    assert rows[:, 11].min() == pytest.approx(-0.05, abs=0.01)
+
+
+def test_sort_sub_keys(orc):
+    # plane-box writes sub keys 0..3; manifold sub keys (0 << 3) | i
+    rows = run(orc, P, [0, 0, 0], [0, 0, 0], B, [0, 0, 0.9], [1, 1, 1])
+    assert sorted(rows[:, 12].astype(int).tolist()) == [0, 1, 2, 3]
+    rows = run(orc, B, [0, 0, 0], [0.5, 0.5, 0.5], B, [0, 0, 0.95], [0.5, 0.5, 0.5], gap=0.1)
+    subs = rows[:, 12].astype(int)
+    assert np.all(np.diff(subs) > 0) and subs.max() <= 4
