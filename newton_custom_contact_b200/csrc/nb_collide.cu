@@ -321,9 +321,15 @@ size_t nb_collide_smem_bytes(const NbModelDesc* m) {
 cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const NbContactSeg* seg, int grid,
                               cudaStream_t stream) {
     size_t smem = nb_collide_smem_bytes(m);
-    cudaError_t e = cudaFuncSetAttribute(collide_worlds_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
+    // raise the dynamic shared-memory limit only when needed, so calls made
+    // during CUDA-graph capture (after a first eager call) touch no attributes
+    static size_t configured = 0;
+    cudaError_t e;
+    if (smem > configured) {
+        e = cudaFuncSetAttribute(collide_worlds_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = smem;
+    }
     e = cudaMemsetAsync(seg->work_counter, 0, sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
     collide_worlds_kernel<<<grid, kCT, smem, stream>>>(*m, body_q, *seg);

@@ -8,8 +8,7 @@
 //             newton/_src/solvers/xpbd/kernels.py:2062-2298); per-body deltas
 //             and contact counts are summed with shared-memory int64
 //             fixed-point atomics -- exact, so the result does not depend on
-//             thread order -- after a warp-level pre-reduction of runs of
-//             contacts that share a body;
+//             thread order;
 //   bodies:   one thread per body, weighted apply_body_deltas
 //             (kernels.py:809-878), then the joint pass (solve_body_joints,
 //             kernels.py:1441-1942) and the unweighted apply of
@@ -730,8 +729,13 @@ size_t nb_step_smem_bytes(const NbModelDesc* m) {
 cudaError_t nb_launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
                            float dt, int grid, cudaStream_t stream) {
     size_t smem = nb_step_smem_bytes(m);
-    cudaError_t e = cudaFuncSetAttribute(xpbd_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    static size_t configured = 0;
+    cudaError_t e;
+    if (smem > configured) {
+        e = cudaFuncSetAttribute(xpbd_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = smem;
+    }
     e = cudaMemsetAsync(seg->work_counter + 1, 0, sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
     int has_contacts = seg->rec0 != nullptr && seg->world_count != nullptr;
