@@ -210,12 +210,11 @@ def run_ours(args, rank, world_size, local_rank):
         for _ in range(substeps):
             a.clear_forces()
             desc = pipe.desc()
-            grid, scratch = pipe._scratch()
-            seg = pipe.seg_struct(contacts, scratch)
+            seg = pipe.seg_struct(contacts)
             h = _lib.stream_handle(dev)
             ev[0].record(stream)
             _lib.check("nb_collide", lib.nb_collide(C.byref(desc), C.c_void_p(a.body_q.data_ptr()), C.byref(seg),
-                                                    grid, C.c_void_p(h)))
+                                                    0, C.c_void_p(h)))
             ev[1].record(stream)
             pub = pipe.public_struct(contacts)
             _lib.check("nb_publish_contacts", lib.nb_publish_contacts(C.byref(desc), C.byref(seg), C.byref(pub),
@@ -231,6 +230,7 @@ def run_ours(args, rank, world_size, local_rank):
             a, b = b, a
     torch.cuda.synchronize()
     n_contacts = float(contacts._seg["world_count"].sum().item())
+    n_candidates = float(contacts._seg["cand_count"].sum().item())
     # timed region: K graph replays, L2 flushed between them (outside the events)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]

@@ -24,18 +24,24 @@
  *   transform  7 floats  (px, py, pz, qx, qy, qz, qw)  -- wp.transform
  *   twist      6 floats  (vx, vy, vz, wx, wy, wz)      -- wp.spatial_vector
  *   mat33      9 floats  row-major
- * Solver-format contacts are 5 float4 streams (SoA, 16-byte aligned):
- *   rec0 = (point0.xyz, margin0)        point0 in body frame of shape0's body
- *   rec1 = (point1.xyz, margin1)
- *   rec2 = (normal.xyz, bits(shape0))   normal points from shape0 to shape1
- *   rec3 = (offset0.xyz, bits(shape1))
- *   rec4 = (offset1.xyz, bits(tag))     tag = (body_a_local+1) | (body_b_local+1)<<12
- *                                       | sort_sub_key<<24 (local = index within the
- *                                       world's body range, -1 for static shapes)
- * World w owns contact slots [contact_cap_start[w], contact_cap_start[w+1]);
- * its live contacts are the first world_contact_count[w] of them, ordered by
- * the deterministic key (shape0, shape1, sort_sub_key) of
- * newton/_src/geometry/contact_data.py:59-83.
+ * Contacts live in per-candidate slots: each candidate pair (a world's pair
+ * that passed the AABB test) owns 5 contact slots of 5 float4 (80 bytes):
+ *   f4[0] = (point0.xyz, margin0)        point0 in body frame of shape0's body
+ *   f4[1] = (point1.xyz, margin1)
+ *   f4[2] = (normal.xyz, bits(shape0))   normal points from shape0 to shape1
+ *   f4[3] = (offset0.xyz, bits(shape1))
+ *   f4[4] = (offset1.xyz, bits(tag))     tag = (body_a_local+1) | (body_b_local+1)<<12
+ *                                        | sort_sub_key<<24 (local = index within the
+ *                                        world's body range, -1 for static shapes)
+ * Candidate c of world w is one of [world_pair_start[w], world_pair_start[w] +
+ * cand_count[w]), ordered by the deterministic key (shape0, shape1) of
+ * newton/_src/geometry/contact_data.py:59-83; its counts[c] contacts are in
+ * sort_sub_key order, so walking candidates then slots gives key order.
+ * The solver reads dense records (NbContactSeg.rec) with the same fields,
+ * regrouped so a penetration test reads the first 48 bytes:
+ *   f4[0] = (point0.xyz, margin0)   f4[1] = (point1.xyz, margin1)
+ *   f4[2] = (normal.xyz, bits(tag)) f4[3] = (offset0.xyz, bits(shape0))
+ *   f4[4] = (offset1.xyz, bits(shape1))
  */
 #ifndef NEWTON_B200_H
 #define NEWTON_B200_H
@@ -46,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 1
+#define NB_ABI_VERSION 3
 
 enum {
     NB_OK = 0,
@@ -90,7 +96,7 @@ typedef struct NbModelDesc {
     int32_t max_world_joints;
     int32_t max_world_pairs;
     int32_t pad0;
-    int64_t contact_capacity;     /* total solver-format contact slots */
+    int64_t contact_capacity;     /* contact slots = 5 * pair_count */
 
     /* bodies [B] */
     const float* body_com;          /* [B,3] */
@@ -136,25 +142,41 @@ typedef struct NbModelDesc {
     const int32_t* world_joint_start;  /* [W+1] */
     const int32_t* global_shapes;      /* [G] global shape indices */
     const int32_t* world_pair_start;   /* [W+1] */
-    const int32_t* pair_shapes;        /* [P,2] world-local shape slots (a, b) after the
+    const uint32_t* pair_shapes;       /* [P+4] packed world-local shape slots a | b<<16 after the
                                           type ordering of narrow_phase.py:207-210,
                                           sorted by contact key within each world.
                                           Slot i < n_local is shape world_shape_start[w]+i,
                                           slot n_local+g is global_shapes[g]. */
-    const int64_t* contact_cap_start;  /* [W+1] contact slot ranges */
-    const int32_t* world_order;        /* [W] world processing order (cost-descending) */
+    const int32_t* world_order;        /* [W] worlds by decreasing cost (broad phase order) */
+    /* solver schedule: batches of worlds that share one CTA's shared memory */
+    int32_t batch_count;
+    int32_t worlds_per_group;          /* 1 = one world per thread group */
+    int32_t group_threads;             /* threads per world group: 32 (warp) ... 256 (CTA) */
+    int32_t cta_threads;               /* threads per CTA of nb_xpbd_step */
+    int32_t smem_floats_per_batch;     /* shared-memory arena of one batch, in 4-byte words */
+    int32_t pad1;
+    const int32_t* batch_world;        /* [batch_count, cta_threads/group_threads] world ids, -1 = none */
+    const int32_t* batch_slab;         /* [batch_count, cta_threads/group_threads] arena offsets (words) */
 } NbModelDesc;
 
-/* Solver-format contact segments (written by nb_collide, read by nb_xpbd_step). */
+/* Contact slots and the per-substep collision work buffers (written by
+ * nb_collide, read by nb_publish_contacts), and the solver's dense contact
+ * records (written by nb_publish_contacts or nb_ingest_contacts, read by
+ * nb_xpbd_step): world w's contacts are rec[world_base[w] + k],
+ * k < world_count[w], in the solver record layout.  pair_count is
+ * NbModelDesc.pair_count. */
 typedef struct NbContactSeg {
-    float* rec0;                 /* [cap,4] */
-    float* rec1;
-    float* rec2;
-    float* rec3;
-    float* rec4;
-    int32_t* world_count;        /* [W] live contacts per world */
-    float* slot_scratch;         /* per-CTA narrow-phase staging, nb_collide_scratch_floats() floats */
-    int32_t* work_counter;       /* [4] device work-queue counters, zeroed by the entry points */
+    float* slots;                /* [pair_count*5, 20] contact slots (5 float4 each), 16-byte aligned */
+    float* rec;                  /* [pair_count*5, 20] dense solver contact records, 16-byte aligned */
+    int64_t* world_base;         /* [W] first rec index of each world */
+    int32_t* cand;               /* [pair_count] pair index of each candidate (world-major, key order) */
+    int32_t* cand_count;         /* [W] candidates per world */
+    uint8_t* counts;             /* [pair_count] contacts written by each candidate (0..5) */
+    int32_t* queue;              /* [2*pair_count, 2] narrow-phase work items (candidate, world):
+                                    analytic queue from the front, MPR/GJK queue from the back */
+    int32_t* world_count;        /* [W] contacts per world */
+    float* geom;                 /* [shape_count, 20] world-space shape geometry staged per substep */
+    int32_t* work_counter;       /* [8] device counters, zeroed by the entry points */
     uint32_t* status;            /* [1] NB_STATUS_* bits (sticky, cleared by the caller) */
 } NbContactSeg;
 
@@ -206,10 +228,8 @@ typedef struct NbStepIO {
 /* ABI version of the loaded library (NB_ABI_VERSION). */
 int nb_abi_version(void);
 
-/* Floats of per-CTA staging needed by nb_collide for `grid_ctas` CTAs. */
-int64_t nb_collide_scratch_floats(int32_t grid_ctas);
 
-/* Number of CTAs nb_collide / nb_xpbd_step launch on the current device. */
+/* Number of CTAs the persistent kernels launch on the current device. */
 int32_t nb_default_grid(void);
 
 /*
@@ -242,10 +262,11 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
                  const NbContactSeg* seg, float dt, int32_t grid_ctas, void* stream);
 
 /*
- * Ingest contacts written by a caller into the dense public arrays (custom
- * contact writers) into the solver-format segments, bucketing by world in
- * contact-index order.  Replaces nothing in the reference (its solver reads
- * the dense arrays directly, xpbd/kernels.py:2062-2298).
+ * Move contacts a caller wrote into the dense public arrays (custom contact
+ * writers) into solver records, bucketed by world.  Replaces nothing in the
+ * reference (its solver reads the dense arrays directly,
+ * xpbd/kernels.py:2062-2298); the record order inside a world does not change
+ * the solver's result because per-body deltas are summed exactly.
  */
 int nb_ingest_contacts(const NbModelDesc* model, const NbContactsPublic* pub,
                        const NbContactSeg* seg, void* stream);

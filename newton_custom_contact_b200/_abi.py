@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 1
+NB_ABI_VERSION = 3
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -130,20 +130,29 @@ class NbModelDesc(C.Structure):
         ("global_shapes", _fp),
         ("world_pair_start", _fp),
         ("pair_shapes", _fp),
-        ("contact_cap_start", _fp),
         ("world_order", _fp),
+        ("batch_count", C.c_int32),
+        ("worlds_per_group", C.c_int32),
+        ("group_threads", C.c_int32),
+        ("cta_threads", C.c_int32),
+        ("smem_floats_per_batch", C.c_int32),
+        ("pad1", C.c_int32),
+        ("batch_world", _fp),
+        ("batch_slab", _fp),
     ]
 
 
 class NbContactSeg(C.Structure):
     _fields_ = [
-        ("rec0", _fp),
-        ("rec1", _fp),
-        ("rec2", _fp),
-        ("rec3", _fp),
-        ("rec4", _fp),
+        ("slots", _fp),
+        ("rec", _fp),
+        ("world_base", _fp),
+        ("cand", _fp),
+        ("cand_count", _fp),
+        ("counts", _fp),
+        ("queue", _fp),
         ("world_count", _fp),
-        ("slot_scratch", _fp),
+        ("geom", _fp),
         ("work_counter", _fp),
         ("status", _fp),
     ]

@@ -27,7 +27,6 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
 EXPORTS = (
     "nb_abi_version",
-    "nb_collide_scratch_floats",
     "nb_default_grid",
     "nb_collide",
     "nb_publish_contacts",
@@ -66,8 +65,6 @@ def load(path: str | None = None) -> C.CDLL:
         )
     lib = C.CDLL(p)
     lib.nb_abi_version.restype = C.c_int
-    lib.nb_collide_scratch_floats.restype = C.c_int64
-    lib.nb_collide_scratch_floats.argtypes = [C.c_int32]
     lib.nb_default_grid.restype = C.c_int32
     lib.nb_collide.restype = C.c_int
     lib.nb_collide.argtypes = [C.POINTER(NbModelDesc), C.c_void_p, C.POINTER(NbContactSeg), C.c_int32, C.c_void_p]

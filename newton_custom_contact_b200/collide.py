@@ -147,31 +147,27 @@ class PairLayout:
         cnt = np.bincount(w, minlength=W)[:W] if P else np.zeros(W, np.int64)
         pstart = np.zeros(W + 1, np.int64)
         pstart[1:] = np.cumsum(cnt)
-        table = np.full((16, 16), 5, np.int64)
-        for ta in range(16):
-            for tb in range(16):
-                table[ta, tb] = _max_contacts(ta, tb)
-        maxc = table[types[sa], types[sb]]
-        ccap = np.bincount(w, weights=maxc, minlength=W)[:W].astype(np.int64) if P else np.zeros(W, np.int64)
-        cstart = np.zeros(W + 1, np.int64)
-        cstart[1:] = np.cumsum(ccap)
         nb = np.diff(model._part["world_body_start"].astype(np.int64))
         cost = cnt + 4 * nb
         self.world_order = np.argsort(-cost, kind="stable").astype(np.int32)
         self.world_pair_start = pstart.astype(np.int32)
-        self.pair_shapes = np.stack([la, lb], axis=1).astype(np.int32).reshape(-1, 2)
+        if P and max(la.max(), lb.max()) >= (1 << 16):
+            raise ValueError("a world has more than 65535 shapes")
+        # packed (slot_a | slot_b << 16), padded so the kernel can read 4 pairs per 16-byte load
+        packed = np.zeros(P + 4, np.uint32)
+        packed[:P] = (la.astype(np.uint32) & 0xFFFF) | (lb.astype(np.uint32) << 16)
+        self.pair_shapes = packed
+        self.pair_slots = np.stack([la, lb], axis=1).astype(np.int32).reshape(-1, 2)
         self.pair_global = np.stack([sa, sb], axis=1).astype(np.int32).reshape(-1, 2)
-        self.contact_cap_start = cstart
         self.pair_count = int(P)
         self.max_world_pairs = int(cnt.max()) if W else 0
-        self.contact_capacity = int(cstart[-1])
+        self.contact_capacity = 5 * int(P)
         self.world_count = W
 
     def host_dict(self) -> dict:
         return {
             "world_pair_start": self.world_pair_start,
             "pair_shapes": self.pair_shapes,
-            "contact_cap_start": self.contact_cap_start,
             "world_order": self.world_order,
         }
 
@@ -238,6 +234,7 @@ class CollisionPipeline:
         self._layout_dev = {k: torch.from_numpy(np.ascontiguousarray(v)).to(self.device) for k, v in hd.items()}
         self._desc = None
         self._grid = None
+        self._schedule = None
 
     @property
     def rigid_contact_max(self) -> int:
@@ -256,41 +253,59 @@ class CollisionPipeline:
         return c
 
     def attach_segments(self, c: Contacts) -> None:
-        cap = max(1, self.layout.contact_capacity)
+        P = max(1, self.layout.pair_count)
+        W = self.model.world_count
         dev = self.device
-        seg = {f"rec{k}": torch.zeros((cap, 4), dtype=torch.float32, device=dev) for k in range(5)}
-        seg["world_count"] = torch.zeros(self.model.world_count, dtype=torch.int32, device=dev)
-        seg["work_counter"] = torch.zeros(4, dtype=torch.int32, device=dev)
-        seg["status"] = torch.zeros(1, dtype=torch.int32, device=dev)
+        i32 = dict(dtype=torch.int32, device=dev)
+        seg = {
+            "slots": torch.zeros((P * 5, 20), dtype=torch.float32, device=dev),
+            "rec": torch.zeros((P * 5, 20), dtype=torch.float32, device=dev),
+            "world_base": torch.zeros(W, dtype=torch.int64, device=dev),
+            "cand": torch.zeros(P, **i32),
+            "cand_count": torch.zeros(W, **i32),
+            "counts": torch.zeros(P, dtype=torch.uint8, device=dev),
+            "queue": torch.zeros((2 * P, 2), **i32),
+            "world_count": torch.zeros(W, **i32),
+            "geom": torch.zeros((max(1, self.model.shape_count), 20), dtype=torch.float32, device=dev),
+            "work_counter": torch.zeros(8, **i32),
+            "status": torch.zeros(1, **i32),
+        }
         c._seg = seg
         c._layout = self
         c._seg_valid = False
 
+    def set_step_schedule(self, group_threads: int | None = None) -> None:
+        """Pack worlds into shared-memory batches for the step kernel (see schedule.py)."""
+        from .schedule import build_schedule
+
+        sched = build_schedule(self.model, group_threads)
+        self._schedule = sched
+        self._layout_dev["batch_world"] = torch.from_numpy(sched.batch_world.reshape(-1)).to(self.device)
+        self._layout_dev["batch_slab"] = torch.from_numpy(sched.batch_slab.reshape(-1)).to(self.device)
+        self._desc = None
+
     def desc(self):
         if self._desc is None:
+            if getattr(self, "_schedule", None) is None:
+                self.set_step_schedule()
             arrays = self.model.device_arrays()
             arrays.update(self._layout_dev)
+            arrays["schedule"] = self._schedule
             self._desc = self.model.make_desc(arrays, self.layout.info())
         return self._desc
 
-    def _scratch(self):
+    def grid(self) -> int:
         if self._grid is None:
-            lib = _lib.load()
-            self._grid = int(lib.nb_default_grid())
-            n = int(lib.nb_collide_scratch_floats(self._grid))
-            self._slot_scratch = torch.empty(n, dtype=torch.float32, device=self.device)
-        return self._grid, self._slot_scratch
+            self._grid = int(_lib.load().nb_default_grid())
+        return self._grid
 
     @staticmethod
-    def seg_struct(c: Contacts, scratch=None) -> NbContactSeg:
+    def seg_struct(c: Contacts) -> NbContactSeg:
         s = c._seg
         st = NbContactSeg()
-        for k in range(5):
-            setattr(st, f"rec{k}", ptr(s[f"rec{k}"]))
-        st.world_count = ptr(s["world_count"])
-        st.work_counter = ptr(s["work_counter"])
-        st.status = ptr(s["status"])
-        st.slot_scratch = ptr(scratch)
+        for k in ("slots", "rec", "world_base", "cand", "cand_count", "counts", "queue", "world_count", "geom",
+                  "work_counter", "status"):
+            setattr(st, k, ptr(s[k]))
         return st
 
     @staticmethod
@@ -319,9 +334,9 @@ class CollisionPipeline:
         if contacts._world_offset.numel() != self.model.world_count + 1:
             contacts._world_offset = torch.zeros(self.model.world_count + 1, dtype=torch.int64, device=self.device)
         lib = _lib.load()
-        grid, scratch = self._scratch()
+        grid = 0  # narrow-phase grid: library default
         desc = self.desc()
-        seg = self.seg_struct(contacts, scratch)
+        seg = self.seg_struct(contacts)
         stream = _lib.stream_handle(self.device)
         bq = state.body_q
         if bq.dtype != torch.float32 or not bq.is_contiguous() or bq.device.type != "cuda":

@@ -9,7 +9,7 @@ int grid_for(int requested) {
     if (requested > 0) return requested;
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return sms * 2;  // two resident CTAs per SM (__launch_bounds__(256, 2))
+    return sms * 2;  // two resident CTAs per SM (__launch_bounds__(256, 2) kernels)
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -27,10 +27,27 @@ int check_model(const NbModelDesc* m) {
 
 int check_seg(const NbContactSeg* s) {
     if (!s || !s->world_count || !s->work_counter || !s->status) return NB_ERR_INVALID;
-    if (!s->rec0 || !s->rec1 || !s->rec2 || !s->rec3 || !s->rec4) return NB_ERR_INVALID;
-    if (!aligned16(s->rec0) || !aligned16(s->rec1) || !aligned16(s->rec2) || !aligned16(s->rec3) ||
-        !aligned16(s->rec4))
+    if (!s->slots || !s->rec || !s->world_base || !s->cand || !s->cand_count || !s->counts || !s->queue || !s->geom)
         return NB_ERR_INVALID;
+    if (!aligned16(s->slots) || !aligned16(s->rec) || !aligned16(s->geom) ||
+        (reinterpret_cast<uintptr_t>(s->queue) & 7u) || (reinterpret_cast<uintptr_t>(s->world_base) & 7u))
+        return NB_ERR_INVALID;
+    return NB_OK;
+}
+
+// the step reads only the dense solver records
+int check_step_seg(const NbContactSeg* s) {
+    if (!s->world_count || !s->world_base || !aligned16(s->rec)) return NB_ERR_INVALID;
+    if (reinterpret_cast<uintptr_t>(s->world_base) & 7u) return NB_ERR_INVALID;
+    return NB_OK;
+}
+
+int check_schedule(const NbModelDesc* m) {
+    if (m->cta_threads != NB_STEP_THREADS) return NB_ERR_INVALID;
+    const int g = m->group_threads;
+    if (g != 32 && g != 64 && g != 128 && g != 256) return NB_ERR_INVALID;
+    if (m->batch_count < 0 || (m->batch_count > 0 && (!m->batch_world || !m->batch_slab))) return NB_ERR_INVALID;
+    if (m->smem_floats_per_batch <= 0) return NB_ERR_INVALID;
     return NB_OK;
 }
 
@@ -47,10 +64,6 @@ extern "C" {
 
 int nb_abi_version(void) { return NB_ABI_VERSION; }
 
-int64_t nb_collide_scratch_floats(int32_t grid_ctas) {
-    return (int64_t)grid_for(grid_ctas) * NB_COLLIDE_THREADS * 25 * 4;
-}
-
 int32_t nb_default_grid(void) { return grid_for(0); }
 
 int nb_collide(const NbModelDesc* model, const float* body_q, const NbContactSeg* seg, int32_t grid_ctas,
@@ -58,8 +71,8 @@ int nb_collide(const NbModelDesc* model, const float* body_q, const NbContactSeg
     int rc = check_model(model);
     if (rc) return rc;
     if ((rc = check_seg(seg))) return rc;
-    if (!seg->slot_scratch || !body_q || !model->world_pair_start || !model->pair_shapes ||
-        !model->contact_cap_start || !model->world_shape_start)
+    if (!body_q || !model->world_pair_start || !model->pair_shapes || !model->world_shape_start ||
+        (model->global_shape_count > 0 && !model->global_shapes))
         return NB_ERR_INVALID;
     if ((int64_t)nb_collide_smem_bytes(model) > smem_limit()) return NB_ERR_UNSUPPORTED;
     cudaError_t e = nb_launch_collide(model, body_q, seg, grid_for(grid_ctas), (cudaStream_t)stream);
@@ -85,7 +98,7 @@ int nb_ingest_contacts(const NbModelDesc* model, const NbContactsPublic* pub, co
     if (rc) return rc;
     if ((rc = check_seg(seg))) return rc;
     if (!pub || !pub->count || pub->capacity < 0) return NB_ERR_INVALID;
-    if (!model->contact_cap_start || !model->shape_body) return NB_ERR_INVALID;
+    if (!model->world_pair_start || !model->shape_body) return NB_ERR_INVALID;
     cudaError_t e = nb_launch_ingest(model, pub, seg, (cudaStream_t)stream);
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
@@ -101,7 +114,8 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
     if (model->body_count > 0 && (!io->body_q_in || !io->body_qd_in || !io->body_f_in || !io->body_q_out ||
                                   !io->body_qd_out))
         return NB_ERR_INVALID;
-    if (seg->rec0 && ((rc = check_seg(seg)) || !model->contact_cap_start)) return rc ? rc : NB_ERR_INVALID;
+    if ((rc = check_schedule(model))) return rc;
+    if (seg->rec && (rc = check_step_seg(seg))) return rc;
     if ((int64_t)nb_step_smem_bytes(model) > smem_limit()) return NB_ERR_UNSUPPORTED;
     cudaError_t e = nb_launch_step(model, params, io, seg, dt, grid_for(grid_ctas), (cudaStream_t)stream);
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;

@@ -1,19 +1,26 @@
-// Collision detection for many independent worlds, one world per CTA.
+// Collision detection for many independent worlds.
 //
-// A persistent grid pulls worlds (largest first) from a device counter.  Per
-// world the CTA
-//   1. computes every shape's world transform + AABB into shared memory
-//      (compute_shape_aabbs, newton/_src/sim/collide.py:150-275),
-//   2. tests the world's candidate pairs (explicit pair list, sorted by
-//      contact key) and compacts the overlapping ones *in order* with
-//      ballot/popc prefix sums (BroadPhaseExplicit,
-//      newton/_src/geometry/broad_phase_nxn.py:28-66),
-//   3. runs the narrow phase one candidate per thread, staging each
-//      candidate's <= 5 contacts in per-CTA scratch,
-//   4. block-scans the per-candidate counts and copies the contacts into the
-//      world's segment, so the segment is sorted by the deterministic key
-//      (shape_a, shape_b, sub_key) of newton/_src/geometry/contact_data.py:59-83
-//      without a global sort (ContactSorter, contact_sort.py:194-445).
+// Three kernels per substep:
+//   1. broadphase_kernel -- one warp per world (worlds pulled from a device
+//      counter, largest first).  The warp computes every shape's world
+//      transform and AABB (compute_shape_aabbs, newton/_src/sim/collide.py:150-275),
+//      stages the AABBs in shared memory and the full geometry in global
+//      memory, then tests the world's candidate pairs (explicit pair list
+//      sorted by contact key; BroadPhaseExplicit,
+//      newton/_src/geometry/broad_phase_nxn.py:28-66) 32 at a time.  Hits are
+//      compacted *in order* with __ballot_sync / __popc into the world's
+//      candidate list and pushed to one of two work queues: pairs the analytic
+//      primitive path finishes and pairs that need MPR/GJK, so the narrow
+//      phase runs on convergent warps.
+//   2. narrowphase_kernel -- one thread per candidate of every world (flat
+//      over both queues): primitive / MPR / GJK / manifold narrow phase with
+//      write_contact semantics (narrow_phase.py:153-776, collide.py:62-147),
+//      <= 5 contacts written into the candidate's own slots.
+//   3. publish (world_scan_kernel + publish_kernel) -- the reference's dense
+//      Contacts arrays ordered by (world, key): walking a world's candidates
+//      in order and each candidate's slots in sub-key order is exactly the key
+//      order of newton/_src/geometry/contact_data.py:59-83, so no sort is needed
+//      (ContactSorter, contact_sort.py:194-445).
 #include <cuda_runtime.h>
 
 #include "nb_geom.cuh"
@@ -23,177 +30,224 @@ namespace {
 
 using namespace nbg;
 
-constexpr int kCT = NB_COLLIDE_THREADS;     // threads per CTA
-constexpr int kMaxCand = 2048;              // candidates buffered per pass
-constexpr int kSlotF4 = 25;                 // 5 contacts x 5 float4 per candidate
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kBT = 256;             // broad phase: threads per CTA (8 worlds in flight)
+constexpr int kNT = 128;             // narrow phase: threads per CTA
+constexpr int kSlotF4 = 25;          // 5 contacts x 5 float4 per candidate
 
-__device__ __forceinline__ int block_exclusive_scan(int v, int* warp_tmp, int& total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+__device__ __forceinline__ void store_geom(float4* g, const Geom& x) {
+    g[0] = make_float4(x.xf.p.x, x.xf.p.y, x.xf.p.z, x.margin);
+    g[1] = make_float4(x.xf.q.x, x.xf.q.y, x.xf.q.z, x.xf.q.w);
+    g[2] = make_float4(x.scale.x, x.scale.y, x.scale.z, x.gap);
+    g[3] = make_float4(x.lo.x, x.lo.y, x.lo.z, __int_as_float(x.type));
+    g[4] = make_float4(x.hi.x, x.hi.y, x.hi.z, __int_as_float(x.body));
+}
+
+__device__ __forceinline__ Geom load_geom(const float4* g, int sid) {
+    float4 a = g[0], b = g[1], c = g[2], d = g[3], e = g[4];
+    Geom x;
+    x.xf = TF{V3{a.x, a.y, a.z}, Q4{b.x, b.y, b.z, b.w}};
+    x.margin = a.w;
+    x.scale = V3{c.x, c.y, c.z};
+    x.gap = c.w;
+    x.lo = V3{d.x, d.y, d.z};
+    x.type = __float_as_int(d.w);
+    x.hi = V3{e.x, e.y, e.z};
+    x.body = __float_as_int(e.w);
+    x.sid = sid;
+    return x;
+}
+
+// pairs the analytic path of narrow_phase.py:198-591 finishes without falling
+// through to MPR/GJK (plane-box falls through only when no corner is within
+// the gap, where the plane's bounding-sphere test rejects it at once)
+__device__ __forceinline__ bool analytic_pair(int ta, int tb) {
+    if (ta == NB_GEO_SPHERE || tb == NB_GEO_SPHERE) return true;
+    if (ta == NB_GEO_CAPSULE && tb == NB_GEO_CAPSULE) return true;
+    if (ta == NB_GEO_PLANE && (tb == NB_GEO_CAPSULE || tb == NB_GEO_BOX)) return true;
+    return false;
+}
+
+__device__ __forceinline__ int warp_exclusive_scan(int v, int lane, int& total) {
     int x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, x, o);
+        const int y = __shfl_up_sync(kFull, x, o);
         if (lane >= o) x += y;
     }
-    if (lane == 31) warp_tmp[warp] = x;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int run = 0;
-        for (int i = 0; i < kCT / 32; ++i) {
-            int t = warp_tmp[i];
-            warp_tmp[i] = run;
-            run += t;
-        }
-        warp_tmp[kCT / 32] = run;
-    }
-    __syncthreads();
-    int excl = warp_tmp[warp] + x - v;
-    total = warp_tmp[kCT / 32];
-    __syncthreads();
-    return excl;
+    total = __shfl_sync(kFull, x, 31);
+    return x - v;
 }
 
-__global__ void __launch_bounds__(kCT, 2)
-collide_worlds_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    Geom* geo = reinterpret_cast<Geom*>(smem);
-    int* cand = reinterpret_cast<int*>(geo + m.max_world_shapes);
-    __shared__ int s_world, s_total, s_ncand;
-    __shared__ int warp_tmp[kCT / 32 + 1];
-
-    float4* scratch = reinterpret_cast<float4*>(seg.slot_scratch) + (size_t)blockIdx.x * kCT * kSlotF4;
-    float4* rec0 = reinterpret_cast<float4*>(seg.rec0);
-    float4* rec1 = reinterpret_cast<float4*>(seg.rec1);
-    float4* rec2 = reinterpret_cast<float4*>(seg.rec2);
-    float4* rec3 = reinterpret_cast<float4*>(seg.rec3);
-    float4* rec4 = reinterpret_cast<float4*>(seg.rec4);
-    const int tid = threadIdx.x;
-
+__global__ void __launch_bounds__(kBT)
+broadphase_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
+    extern __shared__ __align__(16) float4 sbox[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nsh = m.max_world_shapes;
+    float4* lo = sbox + (size_t)warp * 2 * nsh;   // (lo.xyz, type)
+    float4* hi = lo + nsh;                         // (hi.xyz, 0)
+    float4* geom = reinterpret_cast<float4*>(seg.geom);
+    int2* queue = reinterpret_cast<int2*>(seg.queue);
+    // pairs packed as (slot_a | slot_b << 16), read four per lane with one 16-byte load
+    const uint4* packed = reinterpret_cast<const uint4*>(m.pair_shapes);
+    const int P = m.pair_count;
     for (;;) {
-        if (tid == 0) {
-            int k = atomicAdd(&seg.work_counter[0], 1);
-            s_world = k < m.world_count ? m.world_order[k] : -1;
-            s_total = 0;
-        }
-        __syncthreads();
-        const int w = s_world;
-        if (w < 0) break;
+        int k = 0;
+        if (lane == 0) k = atomicAdd(&seg.work_counter[0], 1);
+        k = __shfl_sync(kFull, k, 0);
+        if (k >= m.world_count) break;
+        const int w = m.world_order[k];
         const int s0 = m.world_shape_start[w];
         const int nloc = m.world_shape_start[w + 1] - s0;
         const int ns = nloc + m.global_shape_count;
-        const int b0 = m.world_body_start[w];
-        for (int i = tid; i < ns; i += kCT) {
-            int s = i < nloc ? s0 + i : m.global_shapes[i - nloc];
-            int b = m.shape_body[s];
+        for (int i = lane; i < ns; i += 32) {
+            const int s = i < nloc ? s0 + i : m.global_shapes[i - nloc];
+            const int b = m.shape_body[s];
             TF xs = load_tf(m.shape_transform + 7 * (size_t)s);
             TF xf = b == -1 ? xs : tf_mul(load_tf(body_q + 7 * (size_t)b), xs);
             Geom g;
             shape_geom(g, xf, m.shape_type[s], load_v3(m.shape_scale + 3 * (size_t)s), m.shape_margin[s],
                        m.shape_gap[s], m.shape_radius[s], b);
-            g.sid = s;
-            geo[i] = g;
+            lo[i] = make_float4(g.lo.x, g.lo.y, g.lo.z, __int_as_float(g.type));
+            hi[i] = make_float4(g.hi.x, g.hi.y, g.hi.z, 0.0f);
+            // global shapes are static: the first world processed stages them
+            if (i < nloc || k == 0) store_geom(geom + 5 * (size_t)s, g);
         }
-        __syncthreads();
-        const int p_begin = m.world_pair_start[w], p_end = m.world_pair_start[w + 1];
-        const int64_t cbase = m.contact_cap_start[w];
-        const int64_t ccap = m.contact_cap_start[w + 1] - cbase;
-        int pnext = p_begin;
-        while (pnext < p_end) {
-            // ---- broad phase: ordered compaction of overlapping pairs
-            if (tid == 0) s_ncand = 0;
-            __syncthreads();
-            while (pnext < p_end && s_ncand + kCT <= kMaxCand) {
-                int p = pnext + tid;
-                bool hit = false;
-                if (p < p_end) {
-                    int la = m.pair_shapes[2 * (size_t)p], lb = m.pair_shapes[2 * (size_t)p + 1];
-                    // slots index the shared geometry table: never trust them blindly
-                    bool valid = (unsigned)la < (unsigned)ns && (unsigned)lb < (unsigned)ns;
-                    if (!valid) atomicOr(seg.status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
-                    hit = valid && la != lb && aabb_overlap(geo[la], geo[lb]);
+        __syncwarp();
+        const int p0 = m.world_pair_start[w], p1 = m.world_pair_start[w + 1];
+        int ncand = 0;
+        for (int base = p0 & ~3; base < p1; base += 128) {
+            const int q = base + 4 * lane;  // multiple of 4: 16-byte aligned
+            uint4 pk = make_uint4(0u, 0u, 0u, 0u);
+            if (q < p1) pk = packed[q >> 2];
+            const unsigned pw[4] = {pk.x, pk.y, pk.z, pk.w};
+            unsigned hit = 0u, easy = 0u;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int p = q + r;
+                if (p < p0 || p >= p1) continue;
+                const int la = (int)(pw[r] & 0xFFFFu), lb = (int)(pw[r] >> 16);
+                // slots index shared memory: never trust them blindly
+                if (la >= ns || lb >= ns) {
+                    atomicOr(seg.status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
+                    continue;
                 }
-                unsigned bal = __ballot_sync(0xffffffffu, hit);
-                int lane = tid & 31, warp = tid >> 5;
-                if (lane == 0) warp_tmp[warp] = __popc(bal);
-                __syncthreads();
-                if (tid == 0) {
-                    int run = 0;
-                    for (int i = 0; i < kCT / 32; ++i) {
-                        int t = warp_tmp[i];
-                        warp_tmp[i] = run;
-                        run += t;
-                    }
-                    warp_tmp[kCT / 32] = run;
+                if (la == lb) continue;
+                const float4 al = lo[la], ah = hi[la], bl = lo[lb], bh = hi[lb];
+                const float c = 0.0f + 0.0f;
+                if (al.x <= bh.x + c && ah.x >= bl.x - c && al.y <= bh.y + c && ah.y >= bl.y - c &&
+                    al.z <= bh.z + c && ah.z >= bl.z - c) {
+                    hit |= 1u << r;
+                    if (analytic_pair(__float_as_int(al.w), __float_as_int(bl.w))) easy |= 1u << r;
                 }
-                __syncthreads();
-                if (hit) cand[s_ncand + warp_tmp[warp] + __popc(bal & ((1u << lane) - 1u))] = p;
-                __syncthreads();
-                if (tid == 0) s_ncand += warp_tmp[kCT / 32];
-                pnext += kCT;
-                __syncthreads();
             }
-            const int ncand = s_ncand;
-            // ---- narrow phase in rounds of kCT candidates
-            for (int r = 0; r < ncand; r += kCT) {
-                int ci = r + tid;
-                int n = 0;
-                float4* myslots = scratch + (size_t)tid * kSlotF4;
-                if (ci < ncand) {
-                    int p = cand[ci];
-                    int la = m.pair_shapes[2 * (size_t)p], lb = m.pair_shapes[2 * (size_t)p + 1];
-                    const Geom& ga = geo[la];
-                    const Geom& gb = geo[lb];
-                    Writer wr;
-                    wr.slots = myslots;
-                    wr.n = 0;
-                    wr.inv_a = ga.body == -1 ? tf_identity() : tf_inverse(load_tf(body_q + 7 * (size_t)ga.body));
-                    wr.inv_b = gb.body == -1 ? tf_identity() : tf_inverse(load_tf(body_q + 7 * (size_t)gb.body));
-                    wr.gap = m.shape_gap[ga.sid] + m.shape_gap[gb.sid];
-                    wr.shape_a = ga.sid;
-                    wr.shape_b = gb.sid;
-                    int lba = ga.body < 0 ? -1 : ga.body - b0;
-                    int lbb = gb.body < 0 ? -1 : gb.body - b0;
-                    wr.tag = ((lba + 1) & 0xFFF) | (((lbb + 1) & 0xFFF) << 12);
-                    narrow_pair(wr, ga, gb);
-                    n = wr.n;
-                }
-                int total;
-                int off = block_exclusive_scan(n, warp_tmp, total);
-                const int base = s_total;
-                for (int k = 0; k < n; ++k) {
-                    int64_t dst = (int64_t)base + off + k;
-                    if (dst < ccap) {
-                        dst += cbase;
-                        const float4* sl = myslots + 5 * k;
-                        rec0[dst] = sl[0];
-                        rec1[dst] = sl[1];
-                        rec2[dst] = sl[2];
-                        rec3[dst] = sl[3];
-                        rec4[dst] = sl[4];
-                    }
-                }
-                __syncthreads();
-                if (tid == 0) s_total = base + total;
-                __syncthreads();
+            int tot_h, tot_a;
+            const int nh = __popc(hit), na = __popc(easy);
+            const int off_h = warp_exclusive_scan(nh, lane, tot_h);
+            const int off_a = warp_exclusive_scan(na, lane, tot_a);
+            const int off_g = off_h - off_a, tot_g = tot_h - tot_a;
+            int qa = 0, qg = 0;
+            if (lane == 0) {
+                if (tot_a) qa = atomicAdd(&seg.work_counter[2], tot_a);
+                if (tot_g) qg = atomicAdd(&seg.work_counter[3], tot_g);
             }
+            qa = __shfl_sync(kFull, qa, 0);
+            qg = __shfl_sync(kFull, qg, 0);
+            int ih = 0, ia = 0, ig = 0;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if (!(hit >> r & 1u)) continue;
+                const int c = p0 + ncand + off_h + ih++;
+                seg.cand[c] = q + r;
+                if (easy >> r & 1u) queue[qa + off_a + ia++] = make_int2(c, w);
+                else queue[2 * (size_t)P - 1 - (qg + off_g + ig++)] = make_int2(c, w);
+            }
+            ncand += tot_h;
         }
-        if (tid == 0) {
-            int t = s_total;
-            if ((int64_t)t > ccap) {
-                atomicOr(seg.status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
-                t = (int)ccap;
-            }
-            seg.world_count[w] = t;
+        if (lane == 0) {
+            seg.cand_count[w] = ncand;
+            seg.world_count[w] = 0;
         }
-        __syncthreads();
     }
 }
 
-// Exclusive scan of world contact counts (single CTA) -> world_offset[W+1],
-// count[0] = total (may exceed the public capacity, as in the reference).
+struct NarrowItem {
+    int c, w;
+    Geom ga, gb;
+    Writer wr;
+};
+
+__device__ __forceinline__ void narrow_setup(const NbModelDesc& m, const NbContactSeg& seg, const float* body_q,
+                                             int2 e, NarrowItem& it) {
+    const float4* geom = reinterpret_cast<const float4*>(seg.geom);
+    it.c = e.x;
+    it.w = e.y;
+    const unsigned pw = reinterpret_cast<const unsigned*>(m.pair_shapes)[seg.cand[it.c]];
+    const int la = (int)(pw & 0xFFFFu), lb = (int)(pw >> 16);
+    const int s0 = m.world_shape_start[it.w];
+    const int nloc = m.world_shape_start[it.w + 1] - s0;
+    const int sa = la < nloc ? s0 + la : m.global_shapes[la - nloc];
+    const int sb = lb < nloc ? s0 + lb : m.global_shapes[lb - nloc];
+    it.ga = load_geom(geom + 5 * (size_t)sa, sa);
+    it.gb = load_geom(geom + 5 * (size_t)sb, sb);
+    const int b0 = m.world_body_start[it.w];
+    it.wr.slots = reinterpret_cast<float4*>(seg.slots) + (size_t)it.c * kSlotF4;
+    it.wr.n = 0;
+    it.wr.inv_a = it.ga.body == -1 ? tf_identity() : tf_inverse(load_tf(body_q + 7 * (size_t)it.ga.body));
+    it.wr.inv_b = it.gb.body == -1 ? tf_identity() : tf_inverse(load_tf(body_q + 7 * (size_t)it.gb.body));
+    it.wr.gap = it.ga.gap + it.gb.gap;
+    it.wr.shape_a = sa;
+    it.wr.shape_b = sb;
+    const int lba = it.ga.body < 0 ? -1 : it.ga.body - b0;
+    const int lbb = it.gb.body < 0 ? -1 : it.gb.body - b0;
+    it.wr.tag = ((lba + 1) & 0xFFF) | (((lbb + 1) & 0xFFF) << 12);
+}
+
+__device__ __forceinline__ void narrow_finish(const NbContactSeg& seg, const NarrowItem& it) {
+    seg.counts[it.c] = (uint8_t)it.wr.n;
+    if (it.wr.n) atomicAdd(&seg.world_count[it.w], it.wr.n);
+}
+
+// analytic queue: sphere / capsule / plane pairs; a plane-box pair with no
+// corner inside the gap is forwarded to the MPR/GJK queue (narrow_phase.py:598-603)
+__global__ void __launch_bounds__(kNT)
+narrow_analytic_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
+    const int n0 = seg.work_counter[2];
+    const int P = m.pair_count;
+    int2* queue = reinterpret_cast<int2*>(seg.queue);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n0; i += gridDim.x * blockDim.x) {
+        const int2 e = queue[i];
+        NarrowItem it;
+        narrow_setup(m, seg, body_q, e, it);
+        if (narrow_analytic(it.wr, it.ga, it.gb)) {
+            narrow_finish(seg, it);
+        } else {
+            const int k = atomicAdd(&seg.work_counter[3], 1);
+            queue[2 * (size_t)P - 1 - k] = e;
+        }
+    }
+}
+
+// MPR / GJK / manifold queue
+__global__ void __launch_bounds__(kNT)
+narrow_gjk_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
+    const int n1 = seg.work_counter[3];
+    const int P = m.pair_count;
+    const int2* queue = reinterpret_cast<const int2*>(seg.queue);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += gridDim.x * blockDim.x) {
+        NarrowItem it;
+        narrow_setup(m, seg, body_q, queue[2 * (size_t)P - 1 - i], it);
+        gjk_pair(it.wr, it.ga, it.gb);
+        narrow_finish(seg, it);
+    }
+}
+
+// Exclusive scan of world contact counts (single CTA) -> world_offset[W+1]
+// (public arrays) and world_base[W] (solver records; same offsets), count[0]
+// = total (may exceed the public capacity, as in the reference).
 __global__ void __launch_bounds__(1024) world_scan_kernel(int W, const int32_t* __restrict__ world_count,
-                                                          int64_t* world_offset, int32_t* count_out, int cap,
-                                                          uint32_t* status) {
+                                                          int64_t* world_offset, int64_t* world_base,
+                                                          int32_t* count_out, int cap, uint32_t* status) {
     __shared__ int64_t warp_sums[32];
     __shared__ int64_t carry;
     if (threadIdx.x == 0) carry = 0;
@@ -205,7 +259,7 @@ __global__ void __launch_bounds__(1024) world_scan_kernel(int W, const int32_t* 
         int64_t x = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+            int64_t y = __shfl_up_sync(kFull, x, o);
             if (lane >= o) x += y;
         }
         if (lane == 31) warp_sums[warp] = x;
@@ -220,7 +274,10 @@ __global__ void __launch_bounds__(1024) world_scan_kernel(int W, const int32_t* 
         }
         __syncthreads();
         int64_t excl = carry + warp_sums[warp] + x - v;
-        if (i < W) world_offset[i] = excl;
+        if (i < W) {
+            world_offset[i] = excl;
+            world_base[i] = excl;
+        }
         __syncthreads();
         if (threadIdx.x == 1023) carry = excl + v;
         __syncthreads();
@@ -232,43 +289,67 @@ __global__ void __launch_bounds__(1024) world_scan_kernel(int W, const int32_t* 
     }
 }
 
-// Dense public Contacts arrays ordered by (world, key).
+// Dense public Contacts arrays ordered by (world, key), and the same contacts
+// as solver records (rec), contiguous per world; one warp per world.
 __global__ void __launch_bounds__(256) publish_kernel(NbModelDesc m, NbContactSeg seg, NbContactsPublic pub) {
-    const int w = blockIdx.x;
-    if (w >= m.world_count) return;
-    const int n = seg.world_count[w];
-    const int64_t src0 = m.contact_cap_start[w];
-    const int64_t dst0 = pub.world_offset[w];
-    const float4* rec0 = reinterpret_cast<const float4*>(seg.rec0);
-    const float4* rec1 = reinterpret_cast<const float4*>(seg.rec1);
-    const float4* rec2 = reinterpret_cast<const float4*>(seg.rec2);
-    const float4* rec3 = reinterpret_cast<const float4*>(seg.rec3);
-    const float4* rec4 = reinterpret_cast<const float4*>(seg.rec4);
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        int64_t d = dst0 + k;
-        if (d >= pub.capacity) break;
-        int64_t s = src0 + k;
-        float4 a = rec0[s], b = rec1[s], c = rec2[s], e = rec3[s], f = rec4[s];
-        int s0 = __float_as_int(c.w), s1 = __float_as_int(e.w);
-        pub.shape0[d] = s0;
-        pub.shape1[d] = s1;
-        pub.point0[3 * d] = a.x; pub.point0[3 * d + 1] = a.y; pub.point0[3 * d + 2] = a.z;
-        pub.point1[3 * d] = b.x; pub.point1[3 * d + 1] = b.y; pub.point1[3 * d + 2] = b.z;
-        pub.normal[3 * d] = c.x; pub.normal[3 * d + 1] = c.y; pub.normal[3 * d + 2] = c.z;
-        pub.offset0[3 * d] = e.x; pub.offset0[3 * d + 1] = e.y; pub.offset0[3 * d + 2] = e.z;
-        pub.offset1[3 * d] = f.x; pub.offset1[3 * d + 1] = f.y; pub.offset1[3 * d + 2] = f.z;
-        pub.margin0[d] = a.w;
-        pub.margin1[d] = b.w;
-        if (pub.sort_key) {
-            int sub = (__float_as_int(f.w) >> 24) & 0xFF;
-            pub.sort_key[d] = ((int64_t)(s0 & 0xFFFFF) << 43) | ((int64_t)(s1 & 0xFFFFF) << 23) | (int64_t)sub;
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const float4* slots = reinterpret_cast<const float4*>(seg.slots);
+    float4* rec = reinterpret_cast<float4*>(seg.rec);
+    for (int w = gw; w < m.world_count; w += nw) {
+        const int nc = seg.cand_count[w];
+        const int c0 = m.world_pair_start[w];
+        const int64_t dst0 = pub.world_offset[w];
+        int64_t running = 0;
+        for (int base = 0; base < nc; base += 32) {
+            const int i = base + lane;
+            const int n = i < nc ? (int)seg.counts[c0 + i] : 0;
+            int x = n;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(kFull, x, o);
+                if (lane >= o) x += y;
+            }
+            const int tot = __shfl_sync(kFull, x, 31);
+            const int excl = x - n;
+            for (int j = 0; j < n; ++j) {
+                const int64_t d = dst0 + running + excl + j;
+                const float4* sl = slots + ((size_t)(c0 + i) * 5 + j) * 5;
+                const float4 a = sl[0], b = sl[1], c = sl[2], e = sl[3], f = sl[4];
+                // solver record: the tag moves next to the normal so the
+                // penetration test reads the first 48 bytes only
+                float4* r = rec + (size_t)d * 5;  // rec holds 5 * pair_count records: never overflows
+                r[0] = a;
+                r[1] = b;
+                r[2] = make_float4(c.x, c.y, c.z, f.w);
+                r[3] = make_float4(e.x, e.y, e.z, c.w);
+                r[4] = make_float4(f.x, f.y, f.z, e.w);
+                if (d >= pub.capacity) continue;
+                const int s0 = __float_as_int(c.w), s1 = __float_as_int(e.w);
+                pub.shape0[d] = s0;
+                pub.shape1[d] = s1;
+                pub.point0[3 * d] = a.x; pub.point0[3 * d + 1] = a.y; pub.point0[3 * d + 2] = a.z;
+                pub.point1[3 * d] = b.x; pub.point1[3 * d + 1] = b.y; pub.point1[3 * d + 2] = b.z;
+                pub.normal[3 * d] = c.x; pub.normal[3 * d + 1] = c.y; pub.normal[3 * d + 2] = c.z;
+                pub.offset0[3 * d] = e.x; pub.offset0[3 * d + 1] = e.y; pub.offset0[3 * d + 2] = e.z;
+                pub.offset1[3 * d] = f.x; pub.offset1[3 * d + 1] = f.y; pub.offset1[3 * d + 2] = f.z;
+                pub.margin0[d] = a.w;
+                pub.margin1[d] = b.w;
+                if (pub.sort_key) {
+                    const int sub = (__float_as_int(f.w) >> 24) & 0xFF;
+                    pub.sort_key[d] = ((int64_t)(s0 & 0xFFFFF) << 43) | ((int64_t)(s1 & 0xFFFFF) << 23) | (int64_t)sub;
+                }
+            }
+            running += tot;
         }
     }
 }
 
-// Custom contacts written into the public arrays -> per-world segments.
-// Contacts of a world land in an arbitrary order; the solver's fixed-point
-// accumulation makes its result independent of that order.
+// Custom contacts in the public arrays -> solver records.  World w's k-th
+// contact goes to record world_pair_start[w]*5 + k (every world owns room for
+// 5 contacts per candidate pair); ingest_finalize_kernel clamps the counts and
+// sets world_base.
 __global__ void ingest_kernel(NbModelDesc m, NbContactsPublic pub, NbContactSeg seg) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     int n = pub.count[0] < pub.capacity ? pub.count[0] : pub.capacity;
@@ -282,7 +363,6 @@ __global__ void ingest_kernel(NbModelDesc m, NbContactsPublic pub, NbContactSeg 
     int b1 = s1 >= 0 ? m.shape_body[s1] : -1;
     int bw = b0 >= 0 ? b0 : b1;
     if (bw < 0) return;  // static-static: never moves anything
-    // world of a body: binary search in world_body_start
     int lo = 0, hi = m.world_count;
     while (hi - lo > 1) {
         int mid = (lo + hi) >> 1;
@@ -296,26 +376,41 @@ __global__ void ingest_kernel(NbModelDesc m, NbContactsPublic pub, NbContactSeg 
         atomicOr(seg.status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);  // cross-world contact: dropped
         return;
     }
-    int slot = atomicAdd(&seg.world_count[w], 1);
-    const int64_t cap = m.contact_cap_start[w + 1] - m.contact_cap_start[w];
-    if (slot >= cap) {
+    const int k = atomicAdd(&seg.world_count[w], 1);
+    const int64_t cap = 5 * (int64_t)(m.world_pair_start[w + 1] - m.world_pair_start[w]);
+    if (k >= cap) {
         atomicOr(seg.status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
         return;
     }
-    int64_t d = m.contact_cap_start[w] + slot;
     int la = b0 < 0 ? -1 : b0 - wb, lb = b1 < 0 ? -1 : b1 - wb;
     int tag = ((la + 1) & 0xFFF) | (((lb + 1) & 0xFFF) << 12);
-    reinterpret_cast<float4*>(seg.rec0)[d] = make_float4(pub.point0[3 * c], pub.point0[3 * c + 1], pub.point0[3 * c + 2], pub.margin0[c]);
-    reinterpret_cast<float4*>(seg.rec1)[d] = make_float4(pub.point1[3 * c], pub.point1[3 * c + 1], pub.point1[3 * c + 2], pub.margin1[c]);
-    reinterpret_cast<float4*>(seg.rec2)[d] = make_float4(pub.normal[3 * c], pub.normal[3 * c + 1], pub.normal[3 * c + 2], __int_as_float(s0));
-    reinterpret_cast<float4*>(seg.rec3)[d] = make_float4(pub.offset0[3 * c], pub.offset0[3 * c + 1], pub.offset0[3 * c + 2], __int_as_float(s1));
-    reinterpret_cast<float4*>(seg.rec4)[d] = make_float4(pub.offset1[3 * c], pub.offset1[3 * c + 1], pub.offset1[3 * c + 2], __int_as_float(tag));
+    float4* sl = reinterpret_cast<float4*>(seg.rec) + ((size_t)m.world_pair_start[w] * 5 + k) * 5;
+    sl[0] = make_float4(pub.point0[3 * c], pub.point0[3 * c + 1], pub.point0[3 * c + 2], pub.margin0[c]);
+    sl[1] = make_float4(pub.point1[3 * c], pub.point1[3 * c + 1], pub.point1[3 * c + 2], pub.margin1[c]);
+    sl[2] = make_float4(pub.normal[3 * c], pub.normal[3 * c + 1], pub.normal[3 * c + 2], __int_as_float(tag));
+    sl[3] = make_float4(pub.offset0[3 * c], pub.offset0[3 * c + 1], pub.offset0[3 * c + 2], __int_as_float(s0));
+    sl[4] = make_float4(pub.offset1[3 * c], pub.offset1[3 * c + 1], pub.offset1[3 * c + 2], __int_as_float(s1));
+}
+
+__global__ void ingest_finalize_kernel(NbModelDesc m, NbContactSeg seg) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= m.world_count) return;
+    const int c0 = m.world_pair_start[w];
+    const int cap = 5 * (m.world_pair_start[w + 1] - c0);
+    seg.world_count[w] = seg.world_count[w] < cap ? seg.world_count[w] : cap;
+    seg.world_base[w] = 5 * (int64_t)c0;
+}
+
+int sm_count() {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
 }
 
 }  // namespace
 
 size_t nb_collide_smem_bytes(const NbModelDesc* m) {
-    return (size_t)m->max_world_shapes * sizeof(Geom) + (size_t)kMaxCand * sizeof(int);
+    return (size_t)(kBT / 32) * 2 * (size_t)m->max_world_shapes * sizeof(float4);
 }
 
 cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const NbContactSeg* seg, int grid,
@@ -326,23 +421,33 @@ cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const N
     static size_t configured = 0;
     cudaError_t e;
     if (smem > configured) {
-        e = cudaFuncSetAttribute(collide_worlds_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaFuncSetAttribute(broadphase_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         configured = smem;
     }
-    e = cudaMemsetAsync(seg->work_counter, 0, sizeof(int32_t), stream);
+    e = cudaMemsetAsync(seg->work_counter, 0, 4 * sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
-    collide_worlds_kernel<<<grid, kCT, smem, stream>>>(*m, body_q, *seg);
+    const int sms = sm_count();
+    broadphase_kernel<<<sms * 4, kBT, smem, stream>>>(*m, body_q, *seg);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int ng = grid > 0 ? grid : sms * 8;
+    narrow_analytic_kernel<<<ng, kNT, 0, stream>>>(*m, body_q, *seg);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    narrow_gjk_kernel<<<ng, kNT, 0, stream>>>(*m, body_q, *seg);
     return cudaGetLastError();
 }
 
 cudaError_t nb_launch_publish(const NbModelDesc* m, const NbContactSeg* seg, const NbContactsPublic* pub,
                               cudaStream_t stream) {
-    world_scan_kernel<<<1, 1024, 0, stream>>>(m->world_count, seg->world_count, pub->world_offset, pub->count,
+    world_scan_kernel<<<1, 1024, 0, stream>>>(m->world_count, seg->world_count, pub->world_offset, seg->world_base,
+                                              pub->count,
                                               pub->capacity, seg->status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    publish_kernel<<<m->world_count, 256, 0, stream>>>(*m, *seg, *pub);
+    const int blocks = (m->world_count * 32 + 255) / 256;
+    publish_kernel<<<blocks < 1 ? 1 : blocks, 256, 0, stream>>>(*m, *seg, *pub);
     return cudaGetLastError();
 }
 
@@ -350,7 +455,11 @@ cudaError_t nb_launch_ingest(const NbModelDesc* m, const NbContactsPublic* pub, 
                              cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(seg->world_count, 0, sizeof(int32_t) * (size_t)m->world_count, stream);
     if (e != cudaSuccess) return e;
-    if (pub->capacity <= 0) return cudaSuccess;
-    ingest_kernel<<<(pub->capacity + 255) / 256, 256, 0, stream>>>(*m, *pub, *seg);
+    if (pub->capacity > 0) {
+        ingest_kernel<<<(pub->capacity + 255) / 256, 256, 0, stream>>>(*m, *pub, *seg);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    ingest_finalize_kernel<<<(m->world_count + 255) / 256, 256, 0, stream>>>(*m, *seg);
     return cudaGetLastError();
 }

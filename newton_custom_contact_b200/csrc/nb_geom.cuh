@@ -1124,8 +1124,10 @@ __device__ __noinline__ void gjk_pair(Writer& w, const Geom& ga, const Geom& gb)
     build_manifold(w, p, qa, pa, point_a, point_b, normal, tmpl);
 }
 
-// narrow_phase_primitive_kernel body for one pair (type_a <= type_b)
-__device__ __noinline__ void narrow_pair(Writer& w, const Geom& ga, const Geom& gb) {
+// narrow_phase_primitive_kernel body for one pair (type_a <= type_b).
+// Returns false when the pair falls through to MPR/GJK (no analytic branch
+// produced a finite distance, narrow_phase.py:598-603).
+__device__ __forceinline__ bool narrow_analytic(Writer& w, const Geom& ga, const Geom& gb) {
     int ta = ga.type, tb = gb.type;
     V3 sca = ga.scale, scb = gb.scale;
     V3 pos_a = ga.xf.p, pos_b = gb.xf.p;
@@ -1201,9 +1203,14 @@ __device__ __noinline__ void narrow_pair(Writer& w, const Geom& ga, const Geom& 
             cd.sub_key = i;
             write_contact(w, cd, false);
         }
-        return;
+        return true;
     }
-    gjk_pair(w, ga, gb);
+    return false;
+}
+
+// full narrow phase of one pair: analytic primitives, else MPR/GJK + manifold
+__device__ __noinline__ void narrow_pair(Writer& w, const Geom& ga, const Geom& gb) {
+    if (!narrow_analytic(w, ga, gb)) gjk_pair(w, ga, gb);
 }
 
 }  // namespace nbg

@@ -1,18 +1,24 @@
-// One XPBD substep for many independent worlds, one world per CTA.
+// One XPBD substep for many independent worlds.
 //
-// The world's body poses and twists live in shared memory for the whole
-// substep, so the `iterations` constraint-projection passes never touch HBM
-// for body state (the reference re-reads body arrays in ~7 launches per
-// iteration, newton/_src/solvers/xpbd/solver_xpbd.py:371-630).  Per iteration:
-//   contacts: one thread per contact (solve_body_contact_positions,
-//             newton/_src/solvers/xpbd/kernels.py:2062-2298); per-body deltas
-//             and contact counts are summed with shared-memory int64
-//             fixed-point atomics -- exact, so the result does not depend on
-//             thread order;
-//   bodies:   one thread per body, weighted apply_body_deltas
-//             (kernels.py:809-878), then the joint pass (solve_body_joints,
-//             kernels.py:1441-1942) and the unweighted apply of
-//             solver_xpbd.py:590-630.
+// Worlds are processed by thread groups of G threads (G = 32: one warp per
+// world, up to G = 256: one CTA per world for scenes with few, large worlds).
+// A host-side scheduler packs worlds of similar size into batches that share
+// one CTA's shared-memory arena; each world's body poses, twists and mass
+// properties live in its own slab for the whole substep, so the `iterations`
+// constraint-projection passes never touch HBM for body state (the reference
+// re-reads body arrays in ~7 launches per iteration,
+// newton/_src/solvers/xpbd/solver_xpbd.py:371-630).  Per iteration:
+//   contacts: the group's threads test the world's dense contact records,
+//             compact the penetrating ones and solve those
+//             (solve_body_contact_positions, newton/_src/solvers/xpbd/kernels.py:2062-2298);
+//             per-body deltas and contact counts are summed with shared-memory
+//             int64 fixed-point atomics -- exact, so the result does not depend
+//             on thread or contact order;
+//   bodies:   weighted apply_body_deltas (kernels.py:809-878), then the joint
+//             pass (solve_body_joints, kernels.py:1441-1942) and the unweighted
+//             apply of solver_xpbd.py:590-630.
+// Group barriers are __syncwarp (G = 32), named barriers (G = 64, 128) or
+// __syncthreads (G = 256).
 #include <cuda_runtime.h>
 
 #include "nb_kernels.cuh"
@@ -20,15 +26,15 @@
 
 namespace {
 
-constexpr int kST = NB_STEP_THREADS;
+constexpr int kST = NB_STEP_THREADS;  // threads per CTA
 
 struct SBodies {
-    int nb;
+    int nb;                    // bodies of this world (also the SoA stride)
     float* f;                  // [13][nb] pose (7) + twist (6)
     float* c;                  // [4][nb]  com (3), effective inv mass
     float* I;                  // [9][nb]
     float* iI;                 // [9][nb]  effective inverse inertia
-    float* frc;                // [6][nb]  body_f + joint forces
+    float* frc;                // [6][nb]  body_f + joint forces (aliases acc before integration)
     int* flags;                // [nb]
     unsigned long long* acc;   // [6][nb]
     int* cnt;                  // [nb]
@@ -70,39 +76,52 @@ struct SBodies {
     __device__ void acc_add(int i, int k, long long v) {
         if (v != 0) atomicAdd(&acc[k * nb + i], (unsigned long long)v);
     }
-    // read and clear the accumulated delta of body i
-    __device__ void take(int i, V3& lin, V3& ang) {
+    // read and clear the accumulated delta of body i; false when it is all zero
+    __device__ bool take(int i, V3& lin, V3& ang) {
         long long v[6];
+        unsigned long long any = 0ull;
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             v[k] = (long long)acc[k * nb + i];
+            any |= (unsigned long long)v[k];
             acc[k * nb + i] = 0ull;
         }
         lin = V3{fx_float(v[0]), fx_float(v[1]), fx_float(v[2])};
         ang = V3{fx_float(v[3]), fx_float(v[4]), fx_float(v[5])};
+        return any != 0ull;
     }
 };
 
-__device__ size_t sbodies_bytes(int nb) {
-    return (size_t)nb * (13 + 4 + 9 + 9 + 6) * sizeof(float) + (size_t)nb * sizeof(int) +
-           (size_t)nb * 6 * sizeof(unsigned long long) + (size_t)nb * sizeof(int);
-}
+// 4-byte words of one world's slab: acc (12 words/body, 8-byte aligned first),
+// f 13, c 4, I 9, iI 9, flags 1, cnt 1
+__host__ __device__ constexpr int slab_words_per_body() { return 12 + 13 + 4 + 9 + 9 + 1 + 1; }
 
-__device__ SBodies sbodies_carve(unsigned char* smem, int nb) {
+__device__ SBodies sbodies_carve(unsigned char* slab, int nb) {
     SBodies s;
     s.nb = nb;
-    unsigned long long* a = reinterpret_cast<unsigned long long*>(smem);
+    unsigned long long* a = reinterpret_cast<unsigned long long*>(slab);
     s.acc = a;
+    s.frc = reinterpret_cast<float*>(a);  // used only before integration
     float* fl = reinterpret_cast<float*>(a + 6 * (size_t)nb);
     s.f = fl;
     s.c = fl + 13 * nb;
     s.I = s.c + 4 * nb;
     s.iI = s.I + 9 * nb;
-    s.frc = s.iI + 9 * nb;
-    int* ip = reinterpret_cast<int*>(s.frc + 6 * nb);
+    int* ip = reinterpret_cast<int*>(s.iI + 9 * nb);
     s.flags = ip;
     s.cnt = ip + nb;
     return s;
+}
+
+template <int G>
+__device__ __forceinline__ void group_sync(int g) {
+    if constexpr (G == 32) {
+        __syncwarp();
+    } else if constexpr (G == kST) {
+        __syncthreads();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(G) : "memory");
+    }
 }
 
 // solver.py:50-94
@@ -153,6 +172,21 @@ __device__ void apply_body_delta(TF& q, V3& v, V3& w, V3 dlin, V3 dang, float we
     w = w1;
 }
 
+// apply_body_delta with an all-zero delta in closed form.  With dlin = dang = 0
+// every intermediate of the general path (dp, dwb, tb, dw1) is a signed zero,
+// so q1 = normalize(q0), p1 = (p0 + R(q0) com) - R(q1) com, and v, w only
+// pass the |x| < 1e-4 test; results equal the general path's up to the sign
+// of zero components.
+__device__ __forceinline__ void apply_zero_delta(TF& q, V3& v, V3& w, V3 com, float inv_m) {
+    if (inv_m == 0.0f) return;
+    const Q4 q0 = q.q;
+    const Q4 q1 = qnormalize(q0);
+    const V3 x_com = add(q.p, qrot(q0, com));
+    q = TF{sub(x_com, qrot(q1, com)), q1};
+    if (length(v) < 1e-4f) v = V3{0.0f, 0.0f, 0.0f};
+    if (length(w) < 1e-4f) w = V3{0.0f, 0.0f, 0.0f};
+}
+
 // kernels.py:1945-1979
 __device__ float contact_constraint_delta(float err, Q4 qa, Q4 qb, float m_inv_a, float m_inv_b, const M33& Ia,
                                           const M33& Ib, V3 la, V3 lb, V3 aa, V3 ab, float relaxation, float dt) {
@@ -201,22 +235,42 @@ __device__ float angular_correction(float err, float derr, Q4 qa, Q4 qb, const M
     return dl;
 }
 
+// Penetration depth of one solver record (the first test of
+// solve_body_contact_positions, kernels.py:2100-2130); reads 48 bytes.
+__device__ __forceinline__ float contact_depth(const SBodies& S, float4 r0, float4 r1, float4 r2, int la, int lb,
+                                               TF& Xa, TF& Xb, V3& bx_a, V3& bx_b) {
+    Xa = la >= 0 ? S.q(la) : tf_identity();
+    Xb = lb >= 0 ? S.q(lb) : tf_identity();
+    bx_a = tf_point(Xa, V3{r0.x, r0.y, r0.z});
+    bx_b = tf_point(Xb, V3{r1.x, r1.y, r1.z});
+    const float thickness = r0.w + r1.w;
+    return dot(V3{r2.x, r2.y, r2.z}, sub(bx_b, bx_a)) - thickness;
+}
+
+// true when solve_contact would move a body (NaN depths count, so they
+// propagate exactly as in the reference)
+__device__ __forceinline__ bool contact_active(const SBodies& S, float4 r0, float4 r1, float4 r2) {
+    const int tag = __float_as_int(r2.w);
+    const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
+    if (la == lb) return false;
+    TF Xa, Xb;
+    V3 bx_a, bx_b;
+    return !(contact_depth(S, r0, r1, r2, la, lb, Xa, Xb, bx_a, bx_b) >= 0.0f);
+}
+
 // solve_body_contact_positions for one contact (kernels.py:2062-2298)
 __device__ void solve_contact(const NbModelDesc& m, SBodies& S, float4 r0, float4 r1, float4 r2, float4 r3, float4 r4,
                               float relaxation, float dt, bool weighting, unsigned* bad) {
-    const int sa = __float_as_int(r2.w), sb = __float_as_int(r3.w);
+    const int sa = __float_as_int(r3.w), sb = __float_as_int(r4.w);
     if (sa == sb) return;
-    const int tag = __float_as_int(r4.w);
+    const int tag = __float_as_int(r2.w);
     const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
     if (la == lb) return;
-    TF Xa = la >= 0 ? S.q(la) : tf_identity();
-    TF Xb = lb >= 0 ? S.q(lb) : tf_identity();
-    V3 bx_a = tf_point(Xa, V3{r0.x, r0.y, r0.z});
-    V3 bx_b = tf_point(Xb, V3{r1.x, r1.y, r1.z});
-    float thickness = r0.w + r1.w;
-    V3 n{r2.x, r2.y, r2.z};
-    float d = dot(n, sub(bx_b, bx_a)) - thickness;
+    TF Xa, Xb;
+    V3 bx_a, bx_b;
+    const float d = contact_depth(S, r0, r1, r2, la, lb, Xa, Xb, bx_a, bx_b);
     if (d >= 0.0f) return;
+    const V3 n{r2.x, r2.y, r2.z};
     float m_inv_a = 0.0f, m_inv_b = 0.0f;
     M33 Ia = zero_m33(), Ib = zero_m33();
     V3 com_a{0, 0, 0}, com_b{0, 0, 0};
@@ -565,180 +619,245 @@ __device__ void joint_forces(const NbModelDesc& m, SBodies& S, int b0, int j0, i
     }
 }
 
+// contacts examined per compaction round of the contact pass
+constexpr int kChunk = 256;
+
+// Contact pass of one iteration for one world.  Few contacts penetrate at any
+// time, so the group first tests a chunk of records (one per thread, 48-byte
+// reads), compacts the penetrating ones into a shared list and then solves the
+// list with every thread busy.  Order does not matter: deltas are summed
+// exactly.  nact[2] alternates between chunks so that resetting one counter
+// never races with the next chunk's appends; both are zero on entry and on
+// return (visible to the group after its next barrier).
+template <int G>
+__device__ __forceinline__ void contact_pass(const NbModelDesc& m, SBodies& S, const float4* __restrict__ R, int nc,
+                                             unsigned char* list, int* nact, int g, int t, float relaxation, float dt,
+                                             bool weighting, unsigned* bad) {
+    int parity = 0;
+    for (int base = 0; base < nc; base += kChunk, parity ^= 1) {
+        const int lim = nc - base < kChunk ? nc - base : kChunk;
+        for (int k = t; k < lim; k += G) {
+            const float4* r = R + (size_t)(base + k) * 5;
+            if (contact_active(S, r[0], r[1], r[2])) list[atomicAdd(&nact[parity], 1)] = (unsigned char)k;
+        }
+        group_sync<G>(g);
+        if (t == 0) nact[parity ^ 1] = 0;
+        const int na = nact[parity];
+        for (int a = t; a < na; a += G) {
+            const float4* r = R + (size_t)(base + list[a]) * 5;
+            solve_contact(m, S, r[0], r[1], r[2], r[3], r[4], relaxation, dt, weighting, bad);
+        }
+        group_sync<G>(g);
+    }
+    if (t == 0) nact[0] = nact[1] = 0;
+}
+
+template <int G>
 __global__ void __launch_bounds__(kST, 2)
 xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, int has_contacts, float dt) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_world;
+    extern __shared__ __align__(16) unsigned char arena[];
+    constexpr int kGroups = kST / G;
+    __shared__ int s_batch;
     __shared__ unsigned s_bad;
-    SBodies S = sbodies_carve(smem, m.max_world_bodies);
-    const int tid = threadIdx.x;
+    __shared__ int s_flag[kGroups];
+    __shared__ int s_nact[kGroups][2];
+    __shared__ unsigned char s_list[kGroups][kChunk];
+    const int g = threadIdx.x / G;   // group within the CTA
+    const int t = threadIdx.x % G;   // thread within the group
     const bool weighting = p.rigid_contact_con_weighting != 0;
     const bool model_joints = m.joint_count > 0;
-    const float4* R0 = reinterpret_cast<const float4*>(seg.rec0);
-    const float4* R1 = reinterpret_cast<const float4*>(seg.rec1);
-    const float4* R2 = reinterpret_cast<const float4*>(seg.rec2);
-    const float4* R3 = reinterpret_cast<const float4*>(seg.rec3);
-    const float4* R4 = reinterpret_cast<const float4*>(seg.rec4);
+    const float4* rec = reinterpret_cast<const float4*>(seg.rec);
+    if (threadIdx.x == 0) s_bad = 0u;
 
     for (;;) {
-        if (tid == 0) {
-            int k = atomicAdd(&seg.work_counter[1], 1);
-            s_world = k < m.world_count ? m.world_order[k] : -1;
-            s_bad = 0u;
-        }
+        if (threadIdx.x == 0) s_batch = atomicAdd(&seg.work_counter[4], 1);
         __syncthreads();
-        const int w = s_world;
-        if (w < 0) break;
-        const int b0 = m.world_body_start[w];
-        const int nbw = m.world_body_start[w + 1] - b0;  // bodies of this world
-        const int nb = S.nb;                                // shared-memory stride
-        const int j0 = m.world_joint_start[w], j1 = m.world_joint_start[w + 1];
-        // ---- stage bodies
-        for (int i = tid; i < nbw; i += kST) {
-            const int b = b0 + i;
-            const int fl = m.body_flags[b];
-            const bool kin = (fl & NB_BODY_KINEMATIC) != 0;
-            S.flags[i] = fl;
-            const float* q = io.body_q_in + 7 * (size_t)b;
-            const float* qd = io.body_qd_in + 6 * (size_t)b;
-            for (int k = 0; k < 7; ++k) S.f[k * nb + i] = q[k];
-            for (int k = 0; k < 6; ++k) S.f[(7 + k) * nb + i] = qd[k];
-            const float* fb = io.body_f_in + 6 * (size_t)b;
-            for (int k = 0; k < 6; ++k) S.frc[k * nb + i] = fb[k];
-            for (int k = 0; k < 3; ++k) S.c[k * nb + i] = m.body_com[3 * (size_t)b + k];
-            S.c[3 * nb + i] = kin ? 0.0f : m.body_inv_mass[b];
-            for (int k = 0; k < 9; ++k) {
-                S.I[k * nb + i] = m.body_inertia[9 * (size_t)b + k];
-                S.iI[k * nb + i] = kin ? 0.0f : m.body_inv_inertia[9 * (size_t)b + k];
-            }
-            for (int k = 0; k < 6; ++k) S.acc[k * nb + i] = 0ull;
-            S.cnt[i] = 0;
-        }
-        __syncthreads();
-        // world needs a real joint pass only when it has a non-free enabled joint
-        int my_joint = 0;
-        for (int j = j0 + tid; j < j1; j += kST) my_joint |= (m.joint_type[j] != NB_JOINT_FREE && m.joint_enabled[j]);
-        const bool world_joints = __syncthreads_or(my_joint) != 0;
-        if (io.joint_f && tid == 0) joint_forces(m, S, b0, j0, j1, io.joint_f);
-        __syncthreads();
-        // ---- integrate_bodies
-        for (int i = tid; i < nbw; i += kST) {
-            if (S.flags[i] & NB_BODY_KINEMATIC) continue;
-            const int b = b0 + i;
-            int wi = m.body_world[b];
-            if (wi < 0) wi = 0;
-            V3 g = load_v3(m.gravity + 3 * (size_t)wi);
-            TF q = S.q(i);
-            V3 v = S.v(i), wv = S.w(i);
-            V3 f0{S.frc[0 * nb + i], S.frc[1 * nb + i], S.frc[2 * nb + i]};
-            V3 t0{S.frc[3 * nb + i], S.frc[4 * nb + i], S.frc[5 * nb + i]};
-            integrate_rigid_body(q, v, wv, f0, t0, S.com(i), S.inertia(i), m.body_inv_mass[b],
-                                 load_m33(m.body_inv_inertia + 9 * (size_t)b), g, p.angular_damping, dt);
-            S.set(i, q, v, wv);
-        }
-        __syncthreads();
-        const int nc = has_contacts ? seg.world_count[w] : 0;
-        const int64_t c0 = has_contacts ? m.contact_cap_start[w] : 0;
-        unsigned bad = 0u;
-        for (int it = 0; it < p.iterations; ++it) {
-            if (has_contacts) {
-                for (int c = tid; c < nc; c += kST) {
-                    const int64_t k = c0 + c;
-                    solve_contact(m, S, R0[k], R1[k], R2[k], R3[k], R4[k], p.rigid_contact_relaxation, dt, weighting,
-                                  &bad);
+        const int b = s_batch;
+        if (b >= m.batch_count) break;
+        const int w = m.batch_world[b * kGroups + g];
+        if (w >= 0) {
+            const int b0 = m.world_body_start[w];
+            const int nb = m.world_body_start[w + 1] - b0;
+            SBodies S = sbodies_carve(arena + 4 * (size_t)m.batch_slab[b * kGroups + g], nb);
+            const int j0 = m.world_joint_start[w], j1 = m.world_joint_start[w + 1];
+            // ---- stage bodies (body_f + joint forces go to frc, aliased on acc)
+            for (int i = t; i < nb; i += G) {
+                const int bi = b0 + i;
+                const int fl = m.body_flags[bi];
+                const bool kin = (fl & NB_BODY_KINEMATIC) != 0;
+                S.flags[i] = fl;
+                const float* q = io.body_q_in + 7 * (size_t)bi;
+                const float* qd = io.body_qd_in + 6 * (size_t)bi;
+                for (int k = 0; k < 7; ++k) S.f[k * nb + i] = q[k];
+                for (int k = 0; k < 6; ++k) S.f[(7 + k) * nb + i] = qd[k];
+                const float* fb = io.body_f_in + 6 * (size_t)bi;
+                for (int k = 0; k < 6; ++k) S.frc[k * nb + i] = fb[k];
+                for (int k = 0; k < 3; ++k) S.c[k * nb + i] = m.body_com[3 * (size_t)bi + k];
+                S.c[3 * nb + i] = kin ? 0.0f : m.body_inv_mass[bi];
+                for (int k = 0; k < 9; ++k) {
+                    S.I[k * nb + i] = m.body_inertia[9 * (size_t)bi + k];
+                    S.iI[k * nb + i] = kin ? 0.0f : m.body_inv_inertia[9 * (size_t)bi + k];
                 }
-                __syncthreads();
-                for (int i = tid; i < nbw; i += kST) {
-                    V3 dl, da;
-                    S.take(i, dl, da);
-                    float weight = 1.0f;
-                    if (weighting) {
-                        float iw = (float)S.cnt[i];
-                        S.cnt[i] = 0;
-                        if (iw > 0.0f) weight = 1.0f / iw;
-                    }
+                S.cnt[i] = 0;
+            }
+            // bit 0: the world has a non-free enabled joint (needs a real joint pass);
+            // bit 1: some joint of the world has a non-zero joint_f entry
+            if (t == 0) s_flag[g] = 0;
+            group_sync<G>(g);
+            for (int j = j0 + t; j < j1; j += G) {
+                if (m.joint_type[j] != NB_JOINT_FREE && m.joint_enabled[j]) atomicOr(&s_flag[g], 1);
+                if (io.joint_f) {
+                    const int qs = m.joint_qd_start[j];
+                    const int nd = m.joint_dof_dim[2 * j] + m.joint_dof_dim[2 * j + 1];
+                    for (int k = 0; k < nd; ++k)
+                        if (io.joint_f[qs + k] != 0.0f) atomicOr(&s_flag[g], 2);
+                }
+            }
+            group_sync<G>(g);
+            // apply_joint_forces adds joint_f in joint order; all-zero forces change nothing
+            if ((s_flag[g] & 2) && t == 0) joint_forces(m, S, b0, j0, j1, io.joint_f);
+            group_sync<G>(g);
+            const bool world_joints = (s_flag[g] & 1) != 0;
+            // ---- integrate_bodies (state in registers, frc read before acc is zeroed)
+            for (int i = t; i < nb; i += G) {
+                const V3 f0{S.frc[0 * nb + i], S.frc[1 * nb + i], S.frc[2 * nb + i]};
+                const V3 t0{S.frc[3 * nb + i], S.frc[4 * nb + i], S.frc[5 * nb + i]};
+                if (!(S.flags[i] & NB_BODY_KINEMATIC)) {
+                    const int bi = b0 + i;
+                    int wi = m.body_world[bi];
+                    if (wi < 0) wi = 0;
+                    V3 gv = load_v3(m.gravity + 3 * (size_t)wi);
                     TF q = S.q(i);
                     V3 v = S.v(i), wv = S.w(i);
-                    const V3 com = S.com(i);
-                    const M33 I = S.inertia(i), iI = S.inv_inertia(i);
-                    const float im = S.inv_m(i);
-                    apply_body_delta(q, v, wv, dl, da, weight, com, I, im, iI, dt);
-                    if (model_joints && !world_joints) {
-                        // the joint pass of this world only renormalises (free joints)
-                        apply_body_delta(q, v, wv, V3{0.0f, 0.0f, 0.0f}, V3{0.0f, 0.0f, 0.0f}, 1.0f, com, I, im, iI,
-                                         dt);
+                    integrate_rigid_body(q, v, wv, f0, t0, S.com(i), S.inertia(i), m.body_inv_mass[bi],
+                                         load_m33(m.body_inv_inertia + 9 * (size_t)bi), gv, p.angular_damping, dt);
+                    S.set(i, q, v, wv);
+                }
+            }
+            group_sync<G>(g);
+            for (int i = t; i < nb; i += G)
+                for (int k = 0; k < 6; ++k) S.acc[k * nb + i] = 0ull;
+            if (t == 0) s_nact[g][0] = s_nact[g][1] = 0;
+            group_sync<G>(g);
+            const int nc = has_contacts ? seg.world_count[w] : 0;
+            const float4* R = has_contacts ? rec + (size_t)seg.world_base[w] * 5 : rec;
+            unsigned bad = 0u;
+            for (int it = 0; it < p.iterations; ++it) {
+                if (has_contacts) {
+                    contact_pass<G>(m, S, R, nc, s_list[g], s_nact[g], g, t, p.rigid_contact_relaxation, dt,
+                                    weighting, &bad);
+                    for (int i = t; i < nb; i += G) {
+                        V3 dl, da;
+                        const bool moved = S.take(i, dl, da);
+                        float weight = 1.0f;
+                        if (weighting) {
+                            float iw = (float)S.cnt[i];
+                            S.cnt[i] = 0;
+                            if (iw > 0.0f) weight = 1.0f / iw;
+                        }
+                        TF q = S.q(i);
+                        V3 v = S.v(i), wv = S.w(i);
+                        const V3 com = S.com(i);
+                        const float im = S.inv_m(i);
+                        if (moved || world_joints) {
+                            apply_body_delta(q, v, wv, dl, da, weight, com, S.inertia(i), im, S.inv_inertia(i), dt);
+                        } else {
+                            // no contact touched the body: the closed form, exact up to
+                            // the sign of zeros, which no later step of a world
+                            // without real joints can tell apart
+                            apply_zero_delta(q, v, wv, com, im);
+                        }
+                        if (model_joints && !world_joints) {
+                            // the joint pass of this world only renormalises (free joints)
+                            apply_zero_delta(q, v, wv, com, im);
+                        }
+                        S.set(i, q, v, wv);
                     }
-                    S.set(i, q, v, wv);
+                    group_sync<G>(g);
                 }
-                __syncthreads();
-            }
-            if (model_joints && (world_joints || !has_contacts)) {
-                for (int j = j0 + tid; j < j1; j += kST)
-                    solve_joint(m, S, b0, j, io.joint_target_pos, io.joint_target_vel, p, dt, &bad);
-                __syncthreads();
-                for (int i = tid; i < nbw; i += kST) {
-                    V3 dl, da;
-                    S.take(i, dl, da);
-                    TF q = S.q(i);
-                    V3 v = S.v(i), wv = S.w(i);
-                    apply_body_delta(q, v, wv, dl, da, 1.0f, S.com(i), S.inertia(i), S.inv_m(i), S.inv_inertia(i), dt);
-                    S.set(i, q, v, wv);
+                if (model_joints && (world_joints || !has_contacts)) {
+                    for (int j = j0 + t; j < j1; j += G)
+                        solve_joint(m, S, b0, j, io.joint_target_pos, io.joint_target_vel, p, dt, &bad);
+                    group_sync<G>(g);
+                    for (int i = t; i < nb; i += G) {
+                        V3 dl, da;
+                        S.take(i, dl, da);
+                        TF q = S.q(i);
+                        V3 v = S.v(i), wv = S.w(i);
+                        apply_body_delta(q, v, wv, dl, da, 1.0f, S.com(i), S.inertia(i), S.inv_m(i),
+                                         S.inv_inertia(i), dt);
+                        S.set(i, q, v, wv);
+                    }
+                    group_sync<G>(g);
                 }
-                __syncthreads();
             }
-        }
-        // ---- write back (kinematic bodies pass through unchanged)
-        for (int i = tid; i < nbw; i += kST) {
-            const int b = b0 + i;
-            float* qo = io.body_q_out + 7 * (size_t)b;
-            float* qdo = io.body_qd_out + 6 * (size_t)b;
-            if (S.flags[i] & NB_BODY_KINEMATIC) {
-                for (int k = 0; k < 7; ++k) qo[k] = io.body_q_in[7 * (size_t)b + k];
-                for (int k = 0; k < 6; ++k) qdo[k] = io.body_qd_in[6 * (size_t)b + k];
-                continue;
+            // ---- write back (kinematic bodies pass through unchanged)
+            for (int i = t; i < nb; i += G) {
+                const int bi = b0 + i;
+                float* qo = io.body_q_out + 7 * (size_t)bi;
+                float* qdo = io.body_qd_out + 6 * (size_t)bi;
+                if (S.flags[i] & NB_BODY_KINEMATIC) {
+                    for (int k = 0; k < 7; ++k) qo[k] = io.body_q_in[7 * (size_t)bi + k];
+                    for (int k = 0; k < 6; ++k) qdo[k] = io.body_qd_in[6 * (size_t)bi + k];
+                    continue;
+                }
+                bool finite = true;
+                for (int k = 0; k < 7; ++k) {
+                    float x = S.f[k * nb + i];
+                    finite = finite && isfinite(x);
+                    qo[k] = x;
+                }
+                for (int k = 0; k < 6; ++k) {
+                    float x = S.f[(7 + k) * nb + i];
+                    finite = finite && isfinite(x);
+                    qdo[k] = x;
+                }
+                if (!finite) bad |= 2u;
             }
-            bool finite = true;
-            for (int k = 0; k < 7; ++k) {
-                float x = S.f[k * nb + i];
-                finite = finite && isfinite(x);
-                qo[k] = x;
-            }
-            for (int k = 0; k < 6; ++k) qdo[k] = S.f[(7 + k) * nb + i];
-            if (!finite) bad |= 2u;
+            if (bad) atomicOr(&s_bad, bad);
         }
-        if (bad) atomicOr(&s_bad, bad);
-        __syncthreads();
-        if (tid == 0 && s_bad) {
-            unsigned st = 0;
-            if (s_bad & 1u) st |= NB_STATUS_FIXED_OVERFLOW;
-            if (s_bad & 2u) st |= NB_STATUS_NONFINITE;
-            atomicOr(seg.status, st);
-        }
-        __syncthreads();
+        __syncthreads();  // every group is done with the arena before the next batch
+    }
+    if (threadIdx.x == 0 && s_bad) {
+        unsigned st = 0;
+        if (s_bad & 1u) st |= NB_STATUS_FIXED_OVERFLOW;
+        if (s_bad & 2u) st |= NB_STATUS_NONFINITE;
+        atomicOr(seg.status, st);
     }
 }
 
 }  // namespace
 
-size_t nb_step_smem_bytes(const NbModelDesc* m) {
-    size_t nb = (size_t)(m->max_world_bodies > 0 ? m->max_world_bodies : 1);
-    return nb * (13 + 4 + 9 + 9 + 6) * sizeof(float) + nb * sizeof(int) + nb * 6 * sizeof(unsigned long long) +
-           nb * sizeof(int);
-}
+size_t nb_step_smem_bytes(const NbModelDesc* m) { return (size_t)m->smem_floats_per_batch * 4; }
 
-cudaError_t nb_launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
-                           float dt, int grid, cudaStream_t stream) {
-    size_t smem = nb_step_smem_bytes(m);
+namespace {
+template <int G>
+cudaError_t launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
+                        float dt, int grid, cudaStream_t stream) {
+    const size_t smem = nb_step_smem_bytes(m);
     static size_t configured = 0;
-    cudaError_t e;
     if (smem > configured) {
-        e = cudaFuncSetAttribute(xpbd_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(xpbd_step_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
         if (e != cudaSuccess) return e;
         configured = smem;
     }
-    e = cudaMemsetAsync(seg->work_counter + 1, 0, sizeof(int32_t), stream);
-    if (e != cudaSuccess) return e;
-    int has_contacts = seg->rec0 != nullptr && seg->world_count != nullptr;
-    xpbd_step_kernel<<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
+    const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
+    xpbd_step_kernel<G><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
     return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t nb_launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
+                           float dt, int grid, cudaStream_t stream) {
+    if (m->cta_threads != kST) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(seg->work_counter + 4, 0, sizeof(int32_t), stream);
+    if (e != cudaSuccess) return e;
+    switch (m->group_threads) {
+        case 32: return launch_step<32>(m, p, io, seg, dt, grid, stream);
+        case 64: return launch_step<64>(m, p, io, seg, dt, grid, stream);
+        case 128: return launch_step<128>(m, p, io, seg, dt, grid, stream);
+        case 256: return launch_step<256>(m, p, io, seg, dt, grid, stream);
+        default: return cudaErrorInvalidValue;
+    }
 }

@@ -321,8 +321,16 @@ class Model:
             d.contact_capacity = int(pair_info["contact_capacity"])
             d.world_pair_start = ptr(arrays["world_pair_start"])
             d.pair_shapes = ptr(arrays["pair_shapes"])
-            d.contact_cap_start = ptr(arrays["contact_cap_start"])
             d.world_order = ptr(arrays["world_order"])
+        sched = arrays.get("schedule")
+        if sched is not None:
+            d.batch_count = int(sched.batch_count)
+            d.worlds_per_group = 1
+            d.group_threads = int(sched.group_threads)
+            d.cta_threads = int(sched.cta_threads)
+            d.smem_floats_per_batch = int(sched.arena_words)
+            d.batch_world = ptr(arrays["batch_world"])
+            d.batch_slab = ptr(arrays["batch_slab"])
         return d
 
     def host_arrays(self) -> dict:

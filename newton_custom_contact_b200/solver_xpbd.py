@@ -87,10 +87,7 @@ class SolverXPBD:
         pipe = contacts._layout if contacts is not None and contacts._layout is not None else None
         if pipe is None:
             pipe = self.model._default_pipeline()
-        key = id(pipe)
-        if key not in self._desc_cache:
-            self._desc_cache[key] = (pipe, pipe.desc())
-        return self._desc_cache[key]
+        return pipe, pipe.desc()
 
     @staticmethod
     def _check_state(name, t, shape):
@@ -129,10 +126,11 @@ class SolverXPBD:
             seg = pipe.seg_struct(contacts)
         else:
             if self._empty_seg is None:
-                self._empty_seg = {"work_counter": torch.zeros(4, dtype=torch.int32, device=model.device),
+                self._empty_seg = {"work_counter": torch.zeros(8, dtype=torch.int32, device=model.device),
                                    "status": torch.zeros(1, dtype=torch.int32, device=model.device)}
             seg = NbContactSeg()
             seg.work_counter = ptr(self._empty_seg["work_counter"])
+            seg.world_count = None
             seg.status = ptr(self._empty_seg["status"])
         io = NbStepIO()
         io.body_q_in = ptr(state_in.body_q)
@@ -144,7 +142,7 @@ class SolverXPBD:
         io.joint_target_vel = ptr(control.joint_target_vel)
         io.joint_f = ptr(control.joint_f)
         params = self.params()
-        grid, _ = pipe._scratch()
+        grid = pipe.grid()
         _lib.check("nb_xpbd_step", lib.nb_xpbd_step(C.byref(desc), C.byref(params), C.byref(io), C.byref(seg),
                                                     float(dt), grid, C.c_void_p(stream)))
         self._last_dt = dt

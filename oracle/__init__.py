@@ -68,6 +68,11 @@ def collide_pair(type_a, xf_a, scale_a, type_b, xf_b, scale_b, margin_a=0.0, mar
     return out[:n].copy()
 
 
+class OrcSeg(C.Structure):
+    _fields_ = [("rec0", C.c_void_p), ("rec1", C.c_void_p), ("rec2", C.c_void_p), ("rec3", C.c_void_p),
+                ("rec4", C.c_void_p), ("world_count", C.c_void_p)]
+
+
 class HostSegments:
     """Host-side solver-format contact segments for one pipeline layout."""
 
@@ -79,14 +84,10 @@ class HostSegments:
         self.work = np.zeros(4, np.int32)
 
     def struct(self):
-        from newton_custom_contact_b200._abi import NbContactSeg
-
-        s = NbContactSeg()
+        s = OrcSeg()
         for k in range(5):
             setattr(s, f"rec{k}", self.rec[k].ctypes.data)
         s.world_count = self.world_count.ctypes.data
-        s.work_counter = self.work.ctypes.data
-        s.status = self.status.ctypes.data
         return s
 
 
@@ -148,7 +149,7 @@ def step(model, layout, params, body_q, body_qd, body_f, segs: HostSegments | No
 def contacts_table(model, layout, segs: HostSegments) -> np.ndarray:
     """All live contacts as rows (world, shape0, shape1, sub, p0(3), p1(3), n(3), o0(3), o1(3), m0, m1)."""
     rows = []
-    cs = layout.contact_cap_start
+    cs = 5 * layout.world_pair_start.astype(np.int64)
     for w in range(model.world_count):
         n = int(segs.world_count[w])
         for k in range(cs[w], cs[w] + n):

@@ -1260,7 +1260,7 @@ extern "C" {
 // Collide every world into host-side solver-format segments (seg->rec0..rec4 as
 // float[cap*4] arrays, seg->world_count).  Pairs come from model->pair_shapes.
 // Returns NB_ERR_CAPACITY if a world's segment would overflow.
-int orc_collide(const NbModelDesc* m, const float* body_q, const NbContactSeg* seg) {
+int orc_collide(const NbModelDesc* m, const float* body_q, const OrcSeg* seg) {
     int rc = 0;
 #pragma omp parallel for schedule(dynamic, 1)
     for (int w = 0; w < m->world_count; ++w) {
@@ -1274,7 +1274,7 @@ int orc_collide(const NbModelDesc* m, const float* body_q, const NbContactSeg* s
         std::vector<OutContact> out;
         Writer wr{m, body_q, &out};
         for (int p = m->world_pair_start[w]; p < m->world_pair_start[w + 1]; ++p) {
-            int la = m->pair_shapes[2 * p], lb = m->pair_shapes[2 * p + 1];
+            int la = (int)(m->pair_shapes[p] & 0xFFFFu), lb = (int)(m->pair_shapes[p] >> 16);
             int sa = ids[la], sb = ids[lb];
             const GeomWS& ga = gws[la];
             const GeomWS& gb = gws[lb];
@@ -1282,7 +1282,7 @@ int orc_collide(const NbModelDesc* m, const float* body_q, const NbContactSeg* s
             if (!aabb_overlap(ga, gb)) continue;
             narrow_pair(wr, ga, gb, sa, sb);
         }
-        int64_t c0 = m->contact_cap_start[w], c1 = m->contact_cap_start[w + 1];
+        int64_t c0 = 5 * (int64_t)m->world_pair_start[w], c1 = 5 * (int64_t)m->world_pair_start[w + 1];
         if ((int64_t)out.size() > c1 - c0) {
 #pragma omp atomic write
             rc = NB_ERR_CAPACITY;

@@ -10,6 +10,20 @@
 #include <cmath>
 #include <cstdint>
 
+// Host-side contact segments of the oracle: world w's contacts are stored
+// contiguously from index 5 * world_pair_start[w] in five float4 streams with
+// the record layout of the library's contact slots.
+extern "C" {
+typedef struct OrcSeg {
+    float* rec0;
+    float* rec1;
+    float* rec2;
+    float* rec3;
+    float* rec4;
+    int32_t* world_count;
+} OrcSeg;
+}
+
 namespace orc {
 
 struct V3 { float x, y, z; };

@@ -189,7 +189,7 @@ struct ContactIn {
     int s0, s1;
 };
 
-static ContactIn load_contact(const NbContactSeg* seg, int64_t k) {
+static ContactIn load_contact(const OrcSeg* seg, int64_t k) {
     ContactIn c;
     const float* r0 = seg->rec0 + 4 * k;
     const float* r1 = seg->rec1 + 4 * k;
@@ -594,7 +594,7 @@ extern "C" {
 // One SolverXPBD.step over all worlds (host pointers).  seg == NULL means no
 // contacts.  `acc_mode` selects ORC_ACC_FIXED (0) or ORC_ACC_FLOAT (1).
 // `status` receives NB_STATUS_* bits.
-int orc_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg, float dt,
+int orc_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const OrcSeg* seg, float dt,
              int acc_mode, uint32_t* status) {
     int B = m->body_count;
     std::vector<float> body_f(io->body_f_in, io->body_f_in + 6 * (size_t)B);
@@ -644,7 +644,7 @@ int orc_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, co
         int64_t c0 = 0;
         int nc = 0;
         if (seg) {
-            c0 = m->contact_cap_start[w];
+            c0 = 5 * (int64_t)m->world_pair_start[w];
             nc = seg->world_count[w];
         }
         int j0 = m->world_joint_start[w], j1 = m->world_joint_start[w + 1];

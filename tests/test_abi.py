@@ -35,12 +35,27 @@ def test_library_exports_all_symbols(lib):
     assert lib.nb_abi_version() == _abi.NB_ABI_VERSION
 
 
-def test_struct_sizes_match_header():
-    # pointer-sized fields after the int header; sizes must be multiples of 8
-    assert C.sizeof(_abi.NbModelDesc) == 12 * 4 + 8 + 8 * (len(_abi.NbModelDesc._fields_) - 13)
-    assert C.sizeof(_abi.NbContactSeg) == 9 * 8
-    assert C.sizeof(_abi.NbXpbdParams) == 4 * 4 + 6 * 4
-    assert C.sizeof(_abi.NbStepIO) == 9 * 8
+def test_struct_layouts_match_header(tmp_path):
+    """sizeof / offsetof of every struct, compiled from the header, equal the ctypes mirrors."""
+    structs = {"NbModelDesc": _abi.NbModelDesc, "NbContactSeg": _abi.NbContactSeg,
+               "NbContactsPublic": _abi.NbContactsPublic, "NbXpbdParams": _abi.NbXpbdParams,
+               "NbStepIO": _abi.NbStepIO}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "newton_b200.h"', "int main(void) {"]
+    for name, cls in structs.items():
+        lines.append(f'printf("{name} %zu\\n", sizeof({name}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{name}.{fname} %zu\\n", offsetof({name}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    c_vals = dict(line.split() for line in out if line.strip())
+    for name, cls in structs.items():
+        assert int(c_vals[name]) == C.sizeof(cls), name
+        for fname, _ in cls._fields_:
+            assert int(c_vals[f"{name}.{fname}"]) == getattr(cls, fname).offset, f"{name}.{fname}"
 
 
 def test_invalid_arguments_rejected_without_gpu(lib):

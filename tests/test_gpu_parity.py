@@ -19,25 +19,30 @@ def _small_c2(worlds=48, seed=7):
     return scenes.scene_c2(seed=seed, worlds=worlds, nmin=8, nmax=40, device="cuda")
 
 
-def _segments_gpu(contacts):
-    seg = contacts._seg
-    return [seg[f"rec{k}"].cpu().numpy() for k in range(5)], seg["world_count"].cpu().numpy()
-
-
-def _assert_segments_equal(model, layout, gpu_rec, gpu_wc, segs):
-    assert np.array_equal(gpu_wc, segs.world_count), "per-world contact counts differ"
-    cs = layout.contact_cap_start
-    for w in range(model.world_count):
-        n = int(segs.world_count[w])
-        sl = slice(int(cs[w]), int(cs[w]) + n)
-        for k in range(5):
-            a = gpu_rec[k][sl].view(np.uint32)
-            b = segs.rec[k][sl].view(np.uint32)
-            assert np.array_equal(a, b), f"world {w} rec{k} differs"
+def _published(contacts):
+    n = int(contacts.rigid_contact_count.item())
+    out = {k: getattr(contacts, f"rigid_contact_{k}")[:n].cpu().numpy()
+           for k in ("shape0", "shape1", "point0", "point1", "offset0", "offset1", "normal", "margin0", "margin1")}
+    return n, out
 
 
 def _bits_equal(a, b):
     return np.array_equal(np.asarray(a, np.float32).view(np.uint32), np.asarray(b, np.float32).view(np.uint32))
+
+
+def _assert_contacts_equal(model, pipe, contacts, segs, orc):
+    """GPU dense contacts (world, key order) == oracle contacts, bit for bit."""
+    assert np.array_equal(contacts._seg["world_count"].cpu().numpy(), segs.world_count), "per-world counts differ"
+    table = orc.contacts_table(model, pipe.layout, segs)
+    n, got = _published(contacts)
+    assert n == table.shape[0] and n > 0
+    assert np.array_equal(got["shape0"], table[:, 1].astype(np.int32))
+    assert np.array_equal(got["shape1"], table[:, 2].astype(np.int32))
+    for name, cols in (("point0", slice(4, 7)), ("point1", slice(7, 10)), ("normal", slice(10, 13)),
+                       ("offset0", slice(13, 16)), ("offset1", slice(16, 19))):
+        assert _bits_equal(got[name], table[:, cols]), name
+    assert _bits_equal(got["margin0"], table[:, 19]) and _bits_equal(got["margin1"], table[:, 20])
+    return table
 
 
 @pytest.mark.parametrize("scene", ["c1", "c2"])
@@ -49,43 +54,49 @@ def test_collide_bit_exact(cuda, orc, scene):
     pipe.collide(state, contacts)
     torch.cuda.synchronize()
     segs = orc.collide(model, pipe.layout, model.host("body_q"))
-    rec, wc = _segments_gpu(contacts)
-    assert wc.sum() > 0
-    _assert_segments_equal(model, pipe.layout, rec, wc, segs)
+    _assert_contacts_equal(model, pipe, contacts, segs, orc)
 
 
-def test_public_contacts_match_segments(cuda, orc):
+def test_public_contacts_sorted_keys(cuda, orc):
     model, _ = _small_c2(worlds=16)
     pipe = CollisionPipeline(model, deterministic=True)
     contacts = pipe.contacts()
     pipe.collide(model.state(), contacts)
     torch.cuda.synchronize()
-    n = int(contacts.rigid_contact_count.item())
-    table = orc.contacts_table(model, pipe.layout, orc.collide(model, pipe.layout, model.host("body_q")))
-    assert n == table.shape[0]
-    s0 = contacts.rigid_contact_shape0[:n].cpu().numpy()
-    s1 = contacts.rigid_contact_shape1[:n].cpu().numpy()
-    assert np.array_equal(s0, table[:, 1].astype(np.int32))
-    assert np.array_equal(s1, table[:, 2].astype(np.int32))
-    assert _bits_equal(contacts.rigid_contact_point0[:n].cpu().numpy(), table[:, 4:7])
-    assert _bits_equal(contacts.rigid_contact_normal[:n].cpu().numpy(), table[:, 10:13])
+    segs = orc.collide(model, pipe.layout, model.host("body_q"))
+    table = _assert_contacts_equal(model, pipe, contacts, segs, orc)
+    n = table.shape[0]
     keys = contacts.rigid_contact_sort_key[:n].cpu().numpy()
-    # within a world the contacts are in deterministic key order
     wid = table[:, 0].astype(np.int64)
     for w in np.unique(wid):
-        k = keys[wid == w]
-        assert np.all(np.diff(k) > 0)
-    # canonical sort of (shape0, shape1, sub) reproduces the oracle set exactly
-    ref = np.lexsort((table[:, 3], table[:, 2], table[:, 1]))
-    got = np.argsort(keys, kind="stable")
-    assert np.array_equal(keys[got], (table[ref, 1].astype(np.int64) << 43) | (table[ref, 2].astype(np.int64) << 23)
-                          | table[ref, 3].astype(np.int64))
+        assert np.all(np.diff(keys[wid == w]) > 0), "contacts of a world are not in key order"
+    expect = (table[:, 1].astype(np.int64) << 43) | (table[:, 2].astype(np.int64) << 23) | table[:, 3].astype(np.int64)
+    assert np.array_equal(np.sort(keys), np.sort(expect))
 
 
-def _run_loop(model, info, substeps, orc, iterations=None):
+def test_collide_all_group_sizes_and_nxn(cuda, orc):
+    """The NxN candidate set equals the explicit list; contacts identical."""
+    model, _ = _small_c2(worlds=12)
+    a = CollisionPipeline(model, broad_phase="explicit")
+    b = CollisionPipeline(model, broad_phase="nxn")
+    ca, cb = a.contacts(), b.contacts()
+    s = model.state()
+    a.collide(s, ca)
+    b.collide(s, cb)
+    torch.cuda.synchronize()
+    na, pa = _published(ca)
+    nb, pb = _published(cb)
+    assert na == nb
+    for k in pa:
+        assert np.array_equal(pa[k], pb[k]), k
+
+
+def _run_loop(model, info, substeps, orc, iterations=None, group_threads=None):
     """collide + step loop on the GPU (drop-in API) and on the oracle; returns both trajectories' end states."""
     it = iterations or info["iterations"]
     pipe = CollisionPipeline(model)
+    if group_threads:
+        pipe.set_step_schedule(group_threads)
     solver = SolverXPBD(model, iterations=it)
     s0, s1 = model.state(), model.state()
     contacts = pipe.contacts()
@@ -118,10 +129,10 @@ def test_step_parity_c1(cuda, orc, substeps):
     assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
 
 
-@pytest.mark.parametrize("substeps", [1, 16])
-def test_step_parity_c2(cuda, orc, substeps):
+@pytest.mark.parametrize("substeps,group", [(1, None), (16, None), (4, 32), (4, 64), (4, 128), (4, 256)])
+def test_step_parity_c2(cuda, orc, substeps, group):
     model, info = _small_c2()
-    gq, gqd, q, qd = _run_loop(model, info, substeps, orc)
+    gq, gqd, q, qd = _run_loop(model, info, substeps, orc, group_threads=group)
     np.testing.assert_allclose(gq, q, rtol=1e-5, atol=1e-6)
     assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
 
