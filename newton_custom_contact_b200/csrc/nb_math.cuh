@@ -137,7 +137,7 @@ NB_D TF tf_inverse(TF t) {
 NB_D long long fx_quant(float x, unsigned* bad) {
     float y = x * NB_FX_SCALE;
     if (!(fabsf(y) < NB_FX_LIMIT)) {
-        *bad = 1u;
+        *bad |= 1u;
         if (y != y) y = 0.0f;
         else y = y > 0.0f ? NB_FX_LIMIT : -NB_FX_LIMIT;
     }

@@ -181,12 +181,15 @@ def _bounding_radius(t, s):
     return float(s[0] + s[1])
 
 
-def scene_c2(seed: int = 1, worlds: int = 4096, nmin: int = 8, nmax: int = 128, device=None):
+def scene_c2(seed: int = 1, worlds: int = 4096, nmin: int = 8, nmax: int = 128, device=None,
+             keep_worlds: int | None = None):
     """Uneven worlds of box / sphere / capsule bodies.  Returns (model, info).
 
     Body i of every world is placed in the same vectorised round: up to 64
     uniform draws in the 1 x 1 x 2 m column, accepting the first that keeps
     bounding spheres apart; otherwise it is raised above the world's bodies.
+    ``keep_worlds`` keeps only the first worlds of the generated scene (the
+    same bodies and poses as in the full scene), e.g. for a CPU sample.
     """
     rng = np.random.default_rng(seed)
     counts = rng.integers(nmin, nmax + 1, size=worlds)
@@ -234,9 +237,14 @@ def scene_c2(seed: int = 1, worlds: int = 4096, nmin: int = 8, nmax: int = 128, 
     quats = random_quats(rng, worlds * nmax_w).reshape(worlds, nmax_w, 4)
     mu_w = rng.uniform(0.3, 1.0, size=worlds)
     mask = np.arange(nmax_w)[None, :] < counts[:, None]
-    bw = np.broadcast_to(np.arange(worlds)[:, None], (worlds, nmax_w))[mask]
+    if keep_worlds is not None:
+        if not 0 < keep_worlds <= worlds:
+            raise ValueError("keep_worlds must be in [1, worlds]")
+        mask &= (np.arange(worlds) < keep_worlds)[:, None]
+        worlds = keep_worlds
+    bw = np.broadcast_to(np.arange(mask.shape[0])[:, None], mask.shape)[mask]
     poses = np.concatenate([pos, quats], axis=2)[mask]
-    mu = np.broadcast_to(mu_w[:, None], (worlds, nmax_w))[mask]
+    mu = np.broadcast_to(mu_w[:, None], mask.shape)[mask]
     model = assemble_free_bodies(bw, types[mask], scales[mask], poses, mu, worlds, plane_mu=0.5, device=device)
     return model, dict(dt=1.0 / 60.0, substeps=8, iterations=8, name=f"C2: {worlds} uneven worlds")
 
