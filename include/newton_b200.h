@@ -271,6 +271,23 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
 int nb_ingest_contacts(const NbModelDesc* model, const NbContactsPublic* pub,
                        const NbContactSeg* seg, void* stream);
 
+/*
+ * nb_publish_contacts without the caller's scan scratch: same outputs, but
+ * pub->world_offset is ignored (may be NULL) and the world offsets live in a
+ * file-scope device array of NB_PUBLISH_STATIC_MAX_WORLDS + 1 entries.  It
+ * allocates nothing, for callers that cannot allocate device memory or hold
+ * only the reference Contacts arrays (which have no per-world offsets).  No
+ * counterpart in the reference.  Returns NB_ERR_CAPACITY when
+ * model->world_count > NB_PUBLISH_STATIC_MAX_WORLDS.  One scratch array per
+ * device: calls that may overlap in time on one device race; calls on one
+ * stream are ordered.  Nothing in the scratch must start at zero.  The first
+ * call on a device looks up the array's address (cudaGetSymbolAddress); make
+ * it before any stream capture.
+ */
+#define NB_PUBLISH_STATIC_MAX_WORLDS 65536
+int nb_publish_contacts_static(const NbModelDesc* model, const NbContactSeg* seg,
+                               const NbContactsPublic* pub, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

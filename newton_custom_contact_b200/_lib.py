@@ -32,6 +32,7 @@ EXPORTS = (
     "nb_publish_contacts",
     "nb_xpbd_step",
     "nb_ingest_contacts",
+    "nb_publish_contacts_static",
 )
 
 _lib = None
@@ -77,6 +78,9 @@ def load(path: str | None = None) -> C.CDLL:
     lib.nb_ingest_contacts.restype = C.c_int
     lib.nb_ingest_contacts.argtypes = [C.POINTER(NbModelDesc), C.POINTER(NbContactsPublic), C.POINTER(NbContactSeg),
                                        C.c_void_p]
+    lib.nb_publish_contacts_static.restype = C.c_int
+    lib.nb_publish_contacts_static.argtypes = [C.POINTER(NbModelDesc), C.POINTER(NbContactSeg),
+                                               C.POINTER(NbContactsPublic), C.c_void_p]
     v = lib.nb_abi_version()
     if v != NB_ABI_VERSION:
         raise RuntimeError(f"{LIB_NAME} ABI version {v} != {NB_ABI_VERSION}; rebuild the library")
