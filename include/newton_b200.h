@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 3
+#define NB_ABI_VERSION 4
 
 enum {
     NB_OK = 0,
@@ -178,6 +178,8 @@ typedef struct NbContactSeg {
     float* geom;                 /* [shape_count, 20] world-space shape geometry staged per substep */
     int32_t* work_counter;       /* [8] device counters, zeroed by the entry points */
     uint32_t* status;            /* [1] NB_STATUS_* bits (sticky, cleared by the caller) */
+    int32_t* rec_index;          /* [pair_count*5] public contact index of each record, or NULL;
+                                    needed only for per-contact impulses (written by publish / ingest) */
 } NbContactSeg;
 
 /* Public Contacts arrays in the reference layout (newton/_src/sim/contacts.py:43-186). */
@@ -222,7 +224,12 @@ typedef struct NbStepIO {
     const float* joint_target_pos; /* [D] (may be NULL when no joint drives) */
     const float* joint_target_vel; /* [D] */
     const float* joint_f;          /* [D] */
-    float* contact_impulse;      /* [cap,6] accumulated weighted impulse or NULL */
+    float* contact_impulse;      /* [cap,6] accumulated weighted A-side impulse per public contact, or
+                                    NULL; the caller zeroes it before the step (solver_xpbd.py:286-291) */
+    float* impulse_scratch;      /* [pair_count*5, 6] zero-filled scratch, required with contact_impulse;
+                                    left zero-filled on return */
+    int32_t contact_impulse_capacity; /* rows of contact_impulse (rigid_contact_max) */
+    int32_t pad0;
 } NbStepIO;
 
 /* ABI version of the loaded library (NB_ABI_VERSION). */
@@ -260,6 +267,15 @@ int nb_publish_contacts(const NbModelDesc* model, const NbContactSeg* seg,
  */
 int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbStepIO* io,
                  const NbContactSeg* seg, float dt, int32_t grid_ctas, void* stream);
+
+/*
+ * contacts.force from the impulses a step accumulated: force = impulse / dt for
+ * rows < count[0] (read on the device), zero for the rest of `capacity` rows.
+ * Replaces convert_contact_impulse_to_force (xpbd/kernels.py:2363-2393) as
+ * launched by SolverXPBD.update_contacts (solver_xpbd.py:766-821).
+ */
+int nb_contact_forces(const float* contact_impulse, const int32_t* count, int32_t capacity, float dt,
+                      float* force, void* stream);
 
 /*
  * Move contacts a caller wrote into the dense public arrays (custom contact

@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 3
+NB_ABI_VERSION = 4
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -155,6 +155,7 @@ class NbContactSeg(C.Structure):
         ("geom", _fp),
         ("work_counter", _fp),
         ("status", _fp),
+        ("rec_index", _fp),
     ]
 
 
@@ -203,6 +204,9 @@ class NbStepIO(C.Structure):
         ("joint_target_vel", _fp),
         ("joint_f", _fp),
         ("contact_impulse", _fp),
+        ("impulse_scratch", _fp),
+        ("contact_impulse_capacity", C.c_int32),
+        ("pad0", C.c_int32),
     ]
 
 

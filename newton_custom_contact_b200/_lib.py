@@ -33,6 +33,7 @@ EXPORTS = (
     "nb_xpbd_step",
     "nb_ingest_contacts",
     "nb_publish_contacts_static",
+    "nb_contact_forces",
 )
 
 _lib = None
@@ -78,6 +79,8 @@ def load(path: str | None = None) -> C.CDLL:
     lib.nb_ingest_contacts.restype = C.c_int
     lib.nb_ingest_contacts.argtypes = [C.POINTER(NbModelDesc), C.POINTER(NbContactsPublic), C.POINTER(NbContactSeg),
                                        C.c_void_p]
+    lib.nb_contact_forces.restype = C.c_int
+    lib.nb_contact_forces.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_void_p, C.c_void_p]
     lib.nb_publish_contacts_static.restype = C.c_int
     lib.nb_publish_contacts_static.argtypes = [C.POINTER(NbModelDesc), C.POINTER(NbContactSeg),
                                                C.POINTER(NbContactsPublic), C.c_void_p]

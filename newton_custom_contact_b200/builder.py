@@ -420,8 +420,17 @@ class ModelBuilder:
         return b
 
     # ------------------------------------------------------------------ joints
+    @staticmethod
+    def _default_filter_parent(joint_type, parent: int) -> bool:
+        """builder.py:1258-1263: False for non-fixed joints to world, True otherwise."""
+        if parent == -1:
+            return int(joint_type) == int(JointType.FIXED)
+        return True
+
     def _add_joint(self, jtype, parent, child, parent_xform, child_xform, lin_axes, ang_axes,
-                   collision_filter_parent=True, enabled=True):
+                   collision_filter_parent=None, enabled=True):
+        if collision_filter_parent is None:
+            collision_filter_parent = self._default_filter_parent(jtype, parent)
         j = self.joint_count
         self.joint_type.append(int(jtype))
         self.joint_enabled.append(bool(enabled))
@@ -444,9 +453,14 @@ class ModelBuilder:
             self.joint_target_vel.append(float(ax.get("target_vel", 0.0)))
         self.joint_parents.setdefault(child, []).append((parent, j))
         self.joint_children.setdefault(parent, []).append((child, j))
-        if collision_filter_parent and parent >= 0:
-            for ps in self.body_shapes.get(parent, []):
-                for cs in self.body_shapes.get(child, []):
+        if collision_filter_parent:
+            # builder.py:3878-3885 (parent -1: the static shapes)
+            for cs in self.body_shapes.get(child, []):
+                if not self.shape_flags[cs] & ShapeFlags.COLLIDE_SHAPES:
+                    continue
+                for ps in self.body_shapes.get(parent, []):
+                    if not self.shape_flags[ps] & ShapeFlags.COLLIDE_SHAPES:
+                        continue
                     self.add_shape_collision_filter_pair(ps, cs)
         return j
 
@@ -459,7 +473,7 @@ class ModelBuilder:
     def add_joint_revolute(self, parent: int, child: int, parent_xform=None, child_xform=None, axis=(1.0, 0.0, 0.0),
                            target_pos: float = 0.0, target_vel: float = 0.0, target_ke: float = 0.0,
                            target_kd: float = 0.0, limit_lower: float = -1e6, limit_upper: float = 1e6,
-                           collision_filter_parent: bool = True, enabled: bool = True, label=None):
+                           collision_filter_parent: bool | None = None, enabled: bool = True, label=None):
         ax = {"axis": axis, "limit_lower": limit_lower, "limit_upper": limit_upper, "target_ke": target_ke,
               "target_kd": target_kd, "target_pos": target_pos, "target_vel": target_vel}
         return self._add_joint(JointType.REVOLUTE, parent, child, parent_xform, child_xform, [], [ax],
@@ -467,7 +481,7 @@ class ModelBuilder:
 
     def add_joint_prismatic(self, parent: int, child: int, parent_xform=None, child_xform=None,
                             axis=(1.0, 0.0, 0.0), target_pos=0.0, target_vel=0.0, target_ke=0.0, target_kd=0.0,
-                            limit_lower=-1e6, limit_upper=1e6, collision_filter_parent=True, enabled=True,
+                            limit_lower=-1e6, limit_upper=1e6, collision_filter_parent=None, enabled=True,
                             label=None):
         ax = {"axis": axis, "limit_lower": limit_lower, "limit_upper": limit_upper, "target_ke": target_ke,
               "target_kd": target_kd, "target_pos": target_pos, "target_vel": target_vel}
@@ -475,12 +489,12 @@ class ModelBuilder:
                                collision_filter_parent, enabled)
 
     def add_joint_fixed(self, parent: int, child: int, parent_xform=None, child_xform=None,
-                        collision_filter_parent=True, enabled=True, label=None):
+                        collision_filter_parent=None, enabled=True, label=None):
         return self._add_joint(JointType.FIXED, parent, child, parent_xform, child_xform, [], [],
                                collision_filter_parent, enabled)
 
     def add_joint_ball(self, parent: int, child: int, parent_xform=None, child_xform=None,
-                       collision_filter_parent=True, enabled=True, label=None):
+                       collision_filter_parent=None, enabled=True, label=None):
         axes = [{"axis": e} for e in np.eye(3)]
         return self._add_joint(JointType.BALL, parent, child, parent_xform, child_xform, [], axes,
                                collision_filter_parent, enabled)

@@ -270,6 +270,10 @@ class CollisionPipeline:
             "work_counter": torch.zeros(8, **i32),
             "status": torch.zeros(1, **i32),
         }
+        if c.force is not None:
+            # per-contact impulses: public index of every solver record + the step's scratch
+            seg["rec_index"] = torch.full((P * 5,), -1, **i32)
+            seg["impulse_scratch"] = torch.zeros((P * 5, 6), dtype=torch.float32, device=dev)
         c._seg = seg
         c._layout = self
         c._seg_valid = False
@@ -306,6 +310,7 @@ class CollisionPipeline:
         for k in ("slots", "rec", "world_base", "cand", "cand_count", "counts", "queue", "world_count", "geom",
                   "work_counter", "status"):
             setattr(st, k, ptr(s[k]))
+        st.rec_index = ptr(s["rec_index"]) if "rec_index" in s else None
         return st
 
     @staticmethod

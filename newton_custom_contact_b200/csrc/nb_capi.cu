@@ -110,7 +110,8 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
     if (!params || !io || !seg || !seg->work_counter || !seg->status) return NB_ERR_INVALID;
     if (params->iterations < 0) return NB_ERR_INVALID;
     if (!(dt > 0.0f)) return NB_ERR_INVALID;
-    if (params->enable_restitution || io->contact_impulse) return NB_ERR_UNSUPPORTED;
+    if (io->contact_impulse && (!io->impulse_scratch || io->contact_impulse_capacity < 0)) return NB_ERR_INVALID;
+    if (params->enable_restitution && seg->rec && !model->shape_restitution) return NB_ERR_INVALID;
     if (model->body_count > 0 && (!io->body_q_in || !io->body_qd_in || !io->body_f_in || !io->body_q_out ||
                                   !io->body_qd_out))
         return NB_ERR_INVALID;
@@ -118,6 +119,14 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
     if (seg->rec && (rc = check_step_seg(seg))) return rc;
     if ((int64_t)nb_step_smem_bytes(model) > smem_limit()) return NB_ERR_UNSUPPORTED;
     cudaError_t e = nb_launch_step(model, params, io, seg, dt, grid_for(grid_ctas), (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+int nb_contact_forces(const float* contact_impulse, const int32_t* count, int32_t capacity, float dt, float* force,
+                      void* stream) {
+    if (capacity < 0 || (capacity > 0 && (!contact_impulse || !count || !force))) return NB_ERR_INVALID;
+    if (!(dt > 0.0f)) return NB_ERR_INVALID;
+    cudaError_t e = nb_launch_contact_forces(contact_impulse, count, capacity, dt, force, (cudaStream_t)stream);
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
 

@@ -325,6 +325,7 @@ __global__ void __launch_bounds__(256) publish_kernel(NbModelDesc m, NbContactSe
                 r[2] = make_float4(c.x, c.y, c.z, f.w);
                 r[3] = make_float4(e.x, e.y, e.z, c.w);
                 r[4] = make_float4(f.x, f.y, f.z, e.w);
+                if (seg.rec_index) seg.rec_index[d] = d < pub.capacity ? (int32_t)d : -1;
                 if (d >= pub.capacity) continue;
                 const int s0 = __float_as_int(c.w), s1 = __float_as_int(e.w);
                 pub.shape0[d] = s0;
@@ -384,7 +385,9 @@ __global__ void ingest_kernel(NbModelDesc m, NbContactsPublic pub, NbContactSeg 
     }
     int la = b0 < 0 ? -1 : b0 - wb, lb = b1 < 0 ? -1 : b1 - wb;
     int tag = ((la + 1) & 0xFFF) | (((lb + 1) & 0xFFF) << 12);
-    float4* sl = reinterpret_cast<float4*>(seg.rec) + ((size_t)m.world_pair_start[w] * 5 + k) * 5;
+    const size_t ri = (size_t)m.world_pair_start[w] * 5 + k;
+    if (seg.rec_index) seg.rec_index[ri] = c;
+    float4* sl = reinterpret_cast<float4*>(seg.rec) + ri * 5;
     sl[0] = make_float4(pub.point0[3 * c], pub.point0[3 * c + 1], pub.point0[3 * c + 2], pub.margin0[c]);
     sl[1] = make_float4(pub.point1[3 * c], pub.point1[3 * c + 1], pub.point1[3 * c + 2], pub.margin1[c]);
     sl[2] = make_float4(pub.normal[3 * c], pub.normal[3 * c + 1], pub.normal[3 * c + 2], __int_as_float(tag));

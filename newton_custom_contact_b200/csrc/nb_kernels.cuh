@@ -18,3 +18,5 @@ cudaError_t nb_launch_ingest(const NbModelDesc* m, const NbContactsPublic* pub, 
                              cudaStream_t stream);
 cudaError_t nb_launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
                            float dt, int grid, cudaStream_t stream);
+cudaError_t nb_launch_contact_forces(const float* imp, const int32_t* count, int cap, float dt, float* force,
+                                     cudaStream_t stream);

@@ -33,6 +33,42 @@ NB_D V3 vmax(V3 a, V3 b) { return V3{a.x > b.x ? a.x : b.x, a.y > b.y ? a.y : b.
 NB_D float fmaxw(float a, float b) { return a > b ? a : b; }
 NB_D float fminw(float a, float b) { return a < b ? a : b; }
 NB_D float clampw(float x, float lo, float hi) { return fminw(fmaxw(x, lo), hi); }
+
+// asin / acos in fp32, shared bit for bit with the CPU oracle (the joint
+// solve's twist and swing angles, xpbd/kernels.py:1749-1809, need the same
+// rounding on both sides).  Own approximation: asin x = x + x z P(z), z = x^2,
+// on |x| <= 1/2 with P a degree-5 least-squares fit of (asin x - x) / x^3
+// (relative-error weighted, iteratively reweighted toward minimax); above 1/2,
+// asin x = 2 (pi/4 - asin(sqrt((1 - x) / 2))) with pi/4 split in two floats.
+// Max error against float64 over [-1, 1]: 1.8 ulp (asin), 1.3 ulp (acos).
+NB_D float nb_asin_poly(float z) {
+    float p = 0.03597569838166237f;
+    p = p * z + 0.015487337484955788f;
+    p = p * z + 0.03154779598116875f;
+    p = p * z + 0.044545069336891174f;
+    p = p * z + 0.07500383257865906f;
+    p = p * z + 0.16666661202907562f;
+    return p;
+}
+NB_D float nb_asin(float x) {
+    const float a = fabsf(x);
+    float r;
+    if (a <= 0.5f) {
+        const float z = a * a;
+        r = a + (a * z) * nb_asin_poly(z);
+    } else {
+        const float z = (1.0f - a) * 0.5f;
+        const float s = sqrtf(z);
+        const float t = s + (s * z) * nb_asin_poly(z);
+        r = 2.0f * ((0.7853981852531433f - t) + -2.1855694143368964e-08f);
+    }
+    return x < 0.0f ? -r : r;
+}
+NB_D float nb_acos(float x) {
+    if (fabsf(x) <= 0.5f) return (1.5707963705062866f - nb_asin(x)) + -4.371139000186243e-08f;
+    if (x > 0.0f) return 2.0f * nb_asin(sqrtf((1.0f - x) * 0.5f));
+    return (3.1415927410125732f - 2.0f * nb_asin(sqrtf((1.0f + x) * 0.5f))) + -8.742277657347586e-08f;
+}
 NB_D float comp(V3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
 NB_D void set_comp(V3& a, int i, float v) {
     if (i == 0) a.x = v;

@@ -259,8 +259,10 @@ __device__ __forceinline__ bool contact_active(const SBodies& S, float4 r0, floa
 }
 
 // solve_body_contact_positions for one contact (kernels.py:2062-2298)
+// imp (optional) receives the A-side spatial delta (the contact_impulse_iter
+// entry of the reference) of an active contact.
 __device__ void solve_contact(const NbModelDesc& m, SBodies& S, float4 r0, float4 r1, float4 r2, float4 r3, float4 r4,
-                              float relaxation, float dt, bool weighting, unsigned* bad) {
+                              float relaxation, float dt, bool weighting, unsigned* bad, float* imp) {
     const int sa = __float_as_int(r3.w), sb = __float_as_int(r4.w);
     if (sa == sb) return;
     const int tag = __float_as_int(r2.w);
@@ -355,6 +357,123 @@ __device__ void solve_contact(const NbModelDesc& m, SBodies& S, float4 r0, float
     }
     if (la >= 0) S.add_delta(la, lin_da, ang_da, bad);
     if (lb >= 0) S.add_delta(lb, lin_db, ang_db, bad);
+    if (imp) {
+        imp[0] = lin_da.x; imp[1] = lin_da.y; imp[2] = lin_da.z;
+        imp[3] = ang_da.x; imp[4] = ang_da.y; imp[5] = ang_da.z;
+    }
+}
+
+// velocity_at_point (newton/_src/math/spatial.py:54-80): v + w x r
+__device__ __forceinline__ V3 velocity_at(V3 v, V3 w, V3 r) { return add(cross(w, r), v); }
+
+// apply_rigid_restitution (kernels.py:2471-2620) for one solver record:
+// pre-step poses / twists from the step's inputs, current twists from the
+// slab; velocity deltas go to the fixed-point accumulators.
+__device__ __noinline__ void restitution_contact(const NbModelDesc& m, SBodies& S, const float4* r, int b0,
+                                                 const float* __restrict__ q_prev, const float* __restrict__ qd_prev,
+                                                 float dt, unsigned* bad) {
+    const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
+    const int sa = __float_as_int(r3.w), sb = __float_as_int(r4.w);
+    if (sa == sb) return;
+    int nz = 0;
+    float rest = 0.0f;
+    if (sa >= 0) { nz += 1; rest += __ldg(m.shape_restitution + sa); }
+    if (sb >= 0) { nz += 1; rest += __ldg(m.shape_restitution + sb); }
+    if (nz > 0) rest /= (float)nz;
+    const int tag = __float_as_int(r2.w);
+    const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
+    if (la == lb) return;
+    float m_inv_a = 0.0f, m_inv_b = 0.0f;
+    M33 Ia = zero_m33(), Ib = zero_m33();
+    TF Xa = tf_identity(), Xb = tf_identity();
+    V3 com_a{0, 0, 0}, com_b{0, 0, 0};
+    V3 v_a{0, 0, 0}, v_b{0, 0, 0}, v_a_new{0, 0, 0}, v_b_new{0, 0, 0};
+    float inv_mass = 0.0f;
+    if (la >= 0) { Xa = load_tf(q_prev + 7 * (size_t)(b0 + la)); m_inv_a = S.inv_m(la); Ia = S.inv_inertia(la); com_a = S.com(la); }
+    if (lb >= 0) { Xb = load_tf(q_prev + 7 * (size_t)(b0 + lb)); m_inv_b = S.inv_m(lb); Ib = S.inv_inertia(lb); com_b = S.com(lb); }
+    const V3 n{r2.x, r2.y, r2.z};
+    V3 bx_a = tf_point(Xa, add(V3{r0.x, r0.y, r0.z}, V3{r3.x, r3.y, r3.z}));
+    V3 bx_b = tf_point(Xb, add(V3{r1.x, r1.y, r1.z}, V3{r4.x, r4.y, r4.z}));
+    const float thickness = r0.w + r1.w;
+    const float d = dot(n, sub(bx_b, bx_a)) - thickness;
+    if (d >= 0.0f) return;
+    V3 r_a = sub(bx_a, tf_point(Xa, com_a));
+    V3 r_b = sub(bx_b, tf_point(Xb, com_b));
+    V3 rxn_a{0, 0, 0}, rxn_b{0, 0, 0};
+    if (la >= 0) {
+        const int wi = m.body_world[b0 + la];
+        const V3 g = load_v3(m.gravity + 3 * (size_t)(wi > 0 ? wi : 0));
+        const float* qd = qd_prev + 6 * (size_t)(b0 + la);
+        v_a = add(velocity_at(V3{qd[0], qd[1], qd[2]}, V3{qd[3], qd[4], qd[5]}, r_a), mul(g, dt));
+        v_a_new = velocity_at(S.v(la), S.w(la), r_a);
+        rxn_a = qrot_inv(Xa.q, cross(r_a, n));
+        inv_mass += m_inv_a + dot(rxn_a, mv(Ia, rxn_a));
+    }
+    if (lb >= 0) {
+        const int wi = m.body_world[b0 + lb];
+        const V3 g = load_v3(m.gravity + 3 * (size_t)(wi > 0 ? wi : 0));
+        const float* qd = qd_prev + 6 * (size_t)(b0 + lb);
+        v_b = add(velocity_at(V3{qd[0], qd[1], qd[2]}, V3{qd[3], qd[4], qd[5]}, r_b), mul(g, dt));
+        v_b_new = velocity_at(S.v(lb), S.w(lb), r_b);
+        rxn_b = qrot_inv(Xb.q, cross(r_b, n));
+        inv_mass += m_inv_b + dot(rxn_b, mv(Ib, rxn_b));
+    }
+    if (inv_mass == 0.0f) return;
+    const float rel_old = dot(n, sub(v_b, v_a));
+    const float rel_new = dot(n, sub(v_b_new, v_a_new));
+    if (rel_old >= 0.0f) return;
+    const float dv = (-rel_new - rest * rel_old) / inv_mass;
+    if (la >= 0) {
+        const float dva = -dv;
+        S.add_delta(la, mul(mul(n, m_inv_a), dva), qrot(Xa.q, mul(mv(Ia, rxn_a), dva)), bad);
+    }
+    if (lb >= 0) {
+        const float dvb = dv;
+        S.add_delta(lb, mul(mul(n, m_inv_b), dvb), qrot(Xb.q, mul(mv(Ib, rxn_b), dvb)), bad);
+    }
+}
+
+// accumulate_weighted_contact_impulse (kernels.py:2301-2360) for the world's
+// records: raw iteration impulses from the scratch (all zero for contacts
+// that were not active), weighted by this iteration's body contact counts,
+// added to the public contact's row; the scratch is cleared again.
+template <int G>
+__device__ __forceinline__ void accumulate_impulses(const SBodies& S, const float4* __restrict__ R, int nc,
+                                                    int64_t rec_base, const int32_t* __restrict__ rec_index,
+                                                    float* __restrict__ scratch, float* __restrict__ out, int cap,
+                                                    bool weighting, int t) {
+    for (int k = t; k < nc; k += G) {
+        float* sc = scratch + (size_t)(rec_base + k) * 6;
+        float raw[6];
+        unsigned bits = 0u;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            raw[i] = sc[i];
+            bits |= __float_as_uint(raw[i]);
+        }
+        if (bits == 0u) continue;
+        const int tag = __float_as_int(R[(size_t)k * 5 + 2].w);
+        const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
+        float weight = 1.0f;
+        if (weighting) {
+            const float na = la >= 0 ? (float)S.cnt[la] : 0.0f;
+            const float nb = lb >= 0 ? (float)S.cnt[lb] : 0.0f;
+            const float ns = na + nb;
+            if (ns > 0.0f) {
+                if (na == 0.0f) weight = 1.0f / nb;
+                else if (nb == 0.0f) weight = 1.0f / na;
+                else weight = 2.0f / ns;
+            }
+        }
+        const int64_t pub = rec_index ? (int64_t)rec_index[rec_base + k] : rec_base + k;
+        if (pub >= 0 && pub < cap) {
+            float* o = out + (size_t)pub * 6;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) o[i] = o[i] + raw[i] * weight;
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) sc[i] = 0.0f;
+    }
 }
 
 __device__ V3 vabs(V3 a) { return V3{fabsf(a.x), fabsf(a.y), fabsf(a.z)}; }
@@ -514,7 +633,7 @@ __device__ __noinline__ void solve_joint(const NbModelDesc& m, SBodies& S, int b
         float s = sqrtf(rq.x * rq.x + rq.w * rq.w);
         float invs = 1.0f / s;
         float invscube = invs * invs * invs;
-        float err0 = 2.0f * asinf(clampw(qtwist.x, -1.0f, 1.0f));
+        float err0 = 2.0f * nb_asin(clampw(qtwist.x, -1.0f, 1.0f));
         float err1 = qswing.y, err2 = qswing.z;
         Q4 g0{invs - rq.x * rq.x * invscube, 0.0f, 0.0f, -(rq.w * rq.x) * invscube};
         Q4 g1{-rq.w * (rq.w * rq.z + rq.x * rq.y) * invscube, rq.w * invs, -rq.x * invs,
@@ -525,7 +644,7 @@ __device__ __noinline__ void solve_joint(const NbModelDesc& m, SBodies& S, int b
         float swing_sq = qswing.w * qswing.w;
         if (swing_sq + 1.0e-4f < 1.0f) {
             float d = sqrtf(1.0f - qswing.w * qswing.w);
-            float theta = 2.0f * acosf(clampw(qswing.w, -1.0f, 1.0f));
+            float theta = 2.0f * nb_acos(clampw(qswing.w, -1.0f, 1.0f));
             float scale = theta / d;
             err1 *= scale;
             err2 *= scale;
@@ -632,7 +751,7 @@ constexpr int kChunk = 256;
 template <int G>
 __device__ __forceinline__ void contact_pass(const NbModelDesc& m, SBodies& S, const float4* __restrict__ R, int nc,
                                              unsigned char* list, int* nact, int g, int t, float relaxation, float dt,
-                                             bool weighting, unsigned* bad) {
+                                             bool weighting, unsigned* bad, float* imp_scratch) {
     int parity = 0;
     for (int base = 0; base < nc; base += kChunk, parity ^= 1) {
         const int lim = nc - base < kChunk ? nc - base : kChunk;
@@ -644,8 +763,10 @@ __device__ __forceinline__ void contact_pass(const NbModelDesc& m, SBodies& S, c
         if (t == 0) nact[parity ^ 1] = 0;
         const int na = nact[parity];
         for (int a = t; a < na; a += G) {
-            const float4* r = R + (size_t)(base + list[a]) * 5;
-            solve_contact(m, S, r[0], r[1], r[2], r[3], r[4], relaxation, dt, weighting, bad);
+            const int k = base + list[a];
+            const float4* r = R + (size_t)k * 5;
+            solve_contact(m, S, r[0], r[1], r[2], r[3], r[4], relaxation, dt, weighting, bad,
+                          imp_scratch ? imp_scratch + (size_t)k * 6 : nullptr);
         }
         group_sync<G>(g);
     }
@@ -740,12 +861,19 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
             if (t == 0) s_nact[g][0] = s_nact[g][1] = 0;
             group_sync<G>(g);
             const int nc = has_contacts ? seg.world_count[w] : 0;
-            const float4* R = has_contacts ? rec + (size_t)seg.world_base[w] * 5 : rec;
+            const int64_t rec_base = has_contacts ? seg.world_base[w] : 0;
+            const float4* R = rec + (size_t)rec_base * 5;
+            const bool want_imp = has_contacts && io.contact_impulse != nullptr;
             unsigned bad = 0u;
             for (int it = 0; it < p.iterations; ++it) {
                 if (has_contacts) {
                     contact_pass<G>(m, S, R, nc, s_list[g], s_nact[g], g, t, p.rigid_contact_relaxation, dt,
-                                    weighting, &bad);
+                                    weighting, &bad, want_imp ? io.impulse_scratch + (size_t)rec_base * 6 : nullptr);
+                    if (want_imp) {
+                        accumulate_impulses<G>(S, R, nc, rec_base, seg.rec_index, io.impulse_scratch,
+                                               io.contact_impulse, io.contact_impulse_capacity, weighting, t);
+                        group_sync<G>(g);
+                    }
                     for (int i = t; i < nb; i += G) {
                         V3 dl, da;
                         const bool moved = S.take(i, dl, da);
@@ -791,6 +919,20 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
                     group_sync<G>(g);
                 }
             }
+            // ---- restitution (solver_xpbd.py:685-755), after all iterations
+            if (has_contacts && p.enable_restitution) {
+                for (int k = t; k < nc; k += G)
+                    restitution_contact(m, S, R + (size_t)k * 5, b0, io.body_q_in, io.body_qd_in, dt, &bad);
+                group_sync<G>(g);
+                // apply_body_delta_velocities (kernels.py:881-887)
+                for (int i = t; i < nb; i += G) {
+                    V3 dl, da;
+                    S.take(i, dl, da);
+                    const V3 v = S.v(i), wv = S.w(i);
+                    S.set(i, S.q(i), add(v, dl), add(wv, da));
+                }
+                group_sync<G>(g);
+            }
             // ---- write back (kinematic bodies pass through unchanged)
             for (int i = t; i < nb; i += G) {
                 const int bi = b0 + i;
@@ -829,6 +971,32 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
 }  // namespace
 
 size_t nb_step_smem_bytes(const NbModelDesc* m) { return (size_t)m->smem_floats_per_batch * 4; }
+
+namespace {
+// convert_contact_impulse_to_force (kernels.py:2363-2393)
+__global__ void contact_force_kernel(const float* __restrict__ imp, const int32_t* __restrict__ count, int cap,
+                                     float dt, float* __restrict__ force) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= cap) return;
+    float* f = force + (size_t)tid * 6;
+    if (tid >= count[0]) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) f[i] = 0.0f;
+        return;
+    }
+    const float inv_dt = 1.0f / dt;
+    const float* p = imp + (size_t)tid * 6;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) f[i] = p[i] * inv_dt;
+}
+}  // namespace
+
+cudaError_t nb_launch_contact_forces(const float* imp, const int32_t* count, int cap, float dt, float* force,
+                                     cudaStream_t stream) {
+    if (cap <= 0) return cudaSuccess;
+    contact_force_kernel<<<(cap + 255) / 256, 256, 0, stream>>>(imp, count, cap, dt, force);
+    return cudaGetLastError();
+}
 
 namespace {
 template <int G>

@@ -80,7 +80,8 @@ def _radius_batch(types, scales):
 
 def assemble_free_bodies(body_world: np.ndarray, types: np.ndarray, scales: np.ndarray, poses: np.ndarray,
                          mu: np.ndarray, world_count: int, plane_mu: float = 0.5, qd: np.ndarray | None = None,
-                         device=None, uses_worlds: bool = True, gravity=(0.0, 0.0, -9.81)) -> Model:
+                         device=None, uses_worlds: bool = True, gravity=(0.0, 0.0, -9.81),
+                         restitution: float = 0.0) -> Model:
     """Model of free bodies (one primitive shape each) + a global ground plane (shape 0)."""
     B = types.shape[0]
     f32 = np.float32
@@ -115,7 +116,7 @@ def assemble_free_bodies(body_world: np.ndarray, types: np.ndarray, scales: np.n
     h["shape_material_mu"] = np.concatenate([[plane_mu], mu]).astype(f32)
     h["shape_material_mu_torsional"] = np.full(S, 0.005, f32)
     h["shape_material_mu_rolling"] = np.full(S, 0.0001, f32)
-    h["shape_material_restitution"] = np.zeros(S, f32)
+    h["shape_material_restitution"] = np.full(S, restitution, f32)
     h["shape_world"] = np.concatenate([[-1], body_world if uses_worlds else np.full(B, -1)]).astype(np.int32)
     h["shape_flags"] = np.full(S, _SHAPE_FLAGS, np.int32)
     h["shape_collision_group"] = np.ones(S, np.int32)
@@ -249,7 +250,7 @@ def scene_c2(seed: int = 1, worlds: int = 4096, nmin: int = 8, nmax: int = 128, 
     return model, dict(dt=1.0 / 60.0, substeps=8, iterations=8, name=f"C2: {worlds} uneven worlds")
 
 
-def scene_c5(seed: int = 5, worlds: int = 1024, height: int = 16, device=None):
+def scene_c5(seed: int = 5, worlds: int = 1024, height: int = 16, device=None, restitution: float = 0.0):
     """16-box stacks with random initial twists.  Returns (model, info)."""
     rng = np.random.default_rng(seed)
     h = 0.1
@@ -264,7 +265,8 @@ def scene_c5(seed: int = 5, worlds: int = 1024, height: int = 16, device=None):
     mu = np.repeat(mu_w, height)
     qd = rng.normal(0.0, 0.1, size=(n, 6))
     model = assemble_free_bodies(np.repeat(np.arange(worlds), height), np.full(n, int(GeoType.BOX)),
-                                 np.full((n, 3), h), poses, mu, worlds, plane_mu=0.6, qd=qd, device=device)
+                                 np.full((n, 3), h), poses, mu, worlds, plane_mu=0.6, qd=qd, device=device,
+                                 restitution=restitution)
     return model, dict(dt=1.0 / 600.0, substeps=64, iterations=8, name=f"C5: {worlds} x {height}-box stacks")
 
 

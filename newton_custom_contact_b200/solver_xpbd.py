@@ -61,6 +61,8 @@ class SolverXPBD:
         self._desc_cache = {}
         self._empty_seg = None
         self._last_dt = None
+        self._contact_impulse = None
+        self._contact_impulse_capacity = 0
 
     @property
     def device(self):
@@ -97,10 +99,6 @@ class SolverXPBD:
     def step(self, state_in, state_out, control, contacts: Contacts | None, dt: float) -> None:
         model = self.model
         _lib.require_cuda(model.device)
-        if self.enable_restitution:
-            raise NotImplementedError("restitution is not supported by this build")
-        if contacts is not None and contacts.force is not None:
-            raise NotImplementedError("contact force reporting is not supported by this build")
         if model.body_count == 0:
             return
         if control is None:
@@ -141,14 +139,42 @@ class SolverXPBD:
         io.joint_target_pos = ptr(control.joint_target_pos)
         io.joint_target_vel = ptr(control.joint_target_vel)
         io.joint_f = ptr(control.joint_f)
+        impulse = None
+        if contacts is not None and contacts.force is not None:
+            # solver-owned accumulated impulse (solver_xpbd.py:286-291), zeroed every step
+            cap = contacts.rigid_contact_max
+            impulse = self._contact_impulse
+            if impulse is None or impulse.shape[0] != cap or impulse.device != model.device:
+                impulse = torch.zeros((max(cap, 1), 6), dtype=torch.float32, device=model.device)
+            else:
+                impulse.zero_()
+            io.contact_impulse = ptr(impulse)
+            io.impulse_scratch = ptr(contacts._seg["impulse_scratch"])
+            io.contact_impulse_capacity = cap
         params = self.params()
         grid = pipe.grid()
         _lib.check("nb_xpbd_step", lib.nb_xpbd_step(C.byref(desc), C.byref(params), C.byref(io), C.byref(seg),
                                                     float(dt), grid, C.c_void_p(stream)))
+        self._contact_impulse = impulse
+        self._contact_impulse_capacity = contacts.rigid_contact_max if contacts is not None else 0
         self._last_dt = dt
 
     def update_contacts(self, contacts: Contacts, state=None) -> None:
+        """Populate ``contacts.force`` (force [N], torque [N m] per contact) from the impulses the last
+        ``step`` accumulated (solver_xpbd.py:766-821); same errors as the reference."""
         if contacts.force is None:
             raise ValueError("contacts.force is not allocated. Call model.request_contact_attributes('force') "
                              "before creating the Contacts object.")
-        raise ValueError("No contact impulse data available. Call step() before update_contacts().")
+        if self._contact_impulse is None:
+            raise ValueError("No contact impulse data available. Call step() before update_contacts().")
+        if contacts.rigid_contact_max != self._contact_impulse_capacity:
+            raise ValueError(
+                f"Contacts capacity mismatch: update_contacts() received rigid_contact_max="
+                f"{contacts.rigid_contact_max}, but step() used {self._contact_impulse_capacity}. "
+                f"Pass the same Contacts instance to both step() and update_contacts().")
+        lib = _lib.load()
+        stream = _lib.stream_handle(self.model.device)
+        _lib.check("nb_contact_forces", lib.nb_contact_forces(
+            C.c_void_p(ptr(self._contact_impulse)), C.c_void_p(ptr(contacts.rigid_contact_count)),
+            int(contacts.rigid_contact_max), float(self._last_dt), C.c_void_p(ptr(contacts.force)),
+            C.c_void_p(stream)))

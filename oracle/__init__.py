@@ -39,6 +39,10 @@ def load() -> C.CDLL:
         lib.orc_step.restype = C.c_int
         lib.orc_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int,
                                  C.POINTER(C.c_uint32)]
+        lib.orc_asin.restype = C.c_float
+        lib.orc_asin.argtypes = [C.c_float]
+        lib.orc_acos.restype = C.c_float
+        lib.orc_acos.argtypes = [C.c_float]
         lib.orc_shape_aabbs.restype = C.c_int
         lib.orc_shape_aabbs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.orc_collide_pair.restype = C.c_int
@@ -115,8 +119,10 @@ def collide(model, layout, body_q: np.ndarray) -> HostSegments:
 
 
 def step(model, layout, params, body_q, body_qd, body_f, segs: HostSegments | None, dt: float,
-         joint_target_pos=None, joint_target_vel=None, joint_f=None, acc_mode: int = ACC_FIXED):
-    """One SolverXPBD.step on the CPU.  Returns (body_q_out, body_qd_out, status)."""
+         joint_target_pos=None, joint_target_vel=None, joint_f=None, acc_mode: int = ACC_FIXED,
+         want_impulse: bool = False):
+    """One SolverXPBD.step on the CPU.  Returns (body_q_out, body_qd_out, status), plus the
+    accumulated weighted contact impulse [slot, 6] (indexed like ``segs``) when ``want_impulse``."""
     from newton_custom_contact_b200._abi import NbStepIO
 
     lib = load()
@@ -137,12 +143,18 @@ def step(model, layout, params, body_q, body_qd, body_f, segs: HostSegments | No
             a = _f32(arr)
             keep.append(a)
             setattr(io, name, a.ctypes.data)
+    imp = None
+    if want_impulse:
+        imp = np.zeros((segs.rec[0].shape[0] if segs is not None else 1, 6), np.float32)
+        io.contact_impulse = imp.ctypes.data
     status = C.c_uint32(0)
     st = segs.struct() if segs is not None else None
     rc = lib.orc_step(C.addressof(desc), C.addressof(params), C.addressof(io),
                       C.addressof(st) if st is not None else None, float(dt), int(acc_mode), C.byref(status))
     if rc != 0:
         raise RuntimeError(f"orc_step failed ({rc})")
+    if want_impulse:
+        return q_out, qd_out, int(status.value), imp
     return q_out, qd_out, int(status.value)
 
 

@@ -10,6 +10,8 @@
 //   compute_positional/angular_correction     newton/_src/solvers/xpbd/kernels.py:1982-2059
 //   apply_body_deltas                         newton/_src/solvers/xpbd/kernels.py:809-878
 //   accumulate_weighted_contact_impulse       newton/_src/solvers/xpbd/kernels.py:2301-2360
+//   apply_rigid_restitution                   newton/_src/solvers/xpbd/kernels.py:2471-2620
+//   apply_body_delta_velocities               newton/_src/solvers/xpbd/kernels.py:881-887
 //   SolverXPBD.step orchestration             newton/_src/solvers/xpbd/solver_xpbd.py:259-764
 //
 // The reference sums per-body deltas with float atomics, i.e. in an unspecified
@@ -477,7 +479,7 @@ static void solve_joint(World& W, int j, const float* tpos, const float* tvel, c
         float s = std::sqrt(rq.x * rq.x + rq.w * rq.w);
         float invs = 1.0f / s;
         float invscube = invs * invs * invs;
-        float err0 = 2.0f * std::asin(clampw(qtwist.x, -1.0f, 1.0f));
+        float err0 = 2.0f * nb_asin(clampw(qtwist.x, -1.0f, 1.0f));
         float err1 = qswing.y, err2 = qswing.z;
         Q4 g0{invs - rq.x * rq.x * invscube, 0.0f, 0.0f, -(rq.w * rq.x) * invscube};
         Q4 g1{-rq.w * (rq.w * rq.z + rq.x * rq.y) * invscube, rq.w * invs, -rq.x * invs,
@@ -488,7 +490,7 @@ static void solve_joint(World& W, int j, const float* tpos, const float* tvel, c
         float swing_sq = qswing.w * qswing.w;
         if (swing_sq + 1.0e-4f < 1.0f) {
             float d = std::sqrt(1.0f - qswing.w * qswing.w);
-            float theta = 2.0f * std::acos(clampw(qswing.w, -1.0f, 1.0f));
+            float theta = 2.0f * nb_acos(clampw(qswing.w, -1.0f, 1.0f));
             float scale = theta / d;
             err1 *= scale;
             err2 *= scale;
@@ -587,6 +589,81 @@ static void joint_forces(const NbModelDesc* m, int j0, int j1, const float* body
 
 }  // namespace orc
 
+namespace orc {
+
+// velocity_at_point (newton/_src/math/spatial.py:54-80): v + w x r
+static V3 velocity_at(V3 v, V3 w, V3 r) { return add(cross(w, r), v); }
+
+// apply_rigid_restitution (kernels.py:2471-2620) for one contact.  Poses and
+// twists from before the step (q_prev, qd_prev), current twists from the
+// world state; velocity deltas go to `acc`.
+static void restitution_contact(World& W, const ContactIn& c, const float* q_prev, const float* qd_prev, float dt,
+                                Acc& acc) {
+    const NbModelDesc* m = W.m;
+    int sa = c.s0, sb = c.s1;
+    if (sa == sb) return;
+    int ba = -1, bb = -1;
+    int nz = 0;
+    float rest = 0.0f;
+    if (sa >= 0) { nz += 1; rest += m->shape_restitution[sa]; ba = m->shape_body[sa]; }
+    if (sb >= 0) { nz += 1; rest += m->shape_restitution[sb]; bb = m->shape_body[sb]; }
+    if (nz > 0) rest /= (float)nz;
+    if (ba == bb) return;
+    int la = W.local(ba), lb = W.local(bb);
+    float m_inv_a = 0.0f, m_inv_b = 0.0f;
+    M33 Ia = zero_m33(), Ib = zero_m33();
+    TF Xa = tf_identity(), Xb = tf_identity();
+    V3 com_a{0, 0, 0}, com_b{0, 0, 0};
+    V3 v_a{0, 0, 0}, v_b{0, 0, 0}, v_a_new{0, 0, 0}, v_b_new{0, 0, 0};
+    float inv_mass = 0.0f;
+    if (ba >= 0) { Xa = load_tf(q_prev + 7 * (size_t)ba); m_inv_a = W.inv_m[la]; Ia = W.invI[la]; com_a = W.com[la]; }
+    if (bb >= 0) { Xb = load_tf(q_prev + 7 * (size_t)bb); m_inv_b = W.inv_m[lb]; Ib = W.invI[lb]; com_b = W.com[lb]; }
+    V3 bx_a = tf_point(Xa, add(c.p0, c.o0));
+    V3 bx_b = tf_point(Xb, add(c.p1, c.o1));
+    float thickness = c.m0 + c.m1;
+    V3 n = c.n;
+    float d = dot(n, sub(bx_b, bx_a)) - thickness;
+    if (d >= 0.0f) return;
+    V3 r_a = sub(bx_a, tf_point(Xa, com_a));
+    V3 r_b = sub(bx_b, tf_point(Xb, com_b));
+    V3 rxn_a{0, 0, 0}, rxn_b{0, 0, 0};
+    if (ba >= 0) {
+        int wi = m->body_world[ba];
+        V3 g = load_v3(m->gravity + 3 * (size_t)(wi > 0 ? wi : 0));
+        const float* qd = qd_prev + 6 * (size_t)ba;
+        v_a = add(velocity_at(V3{qd[0], qd[1], qd[2]}, V3{qd[3], qd[4], qd[5]}, r_a), mul(g, dt));
+        v_a_new = velocity_at(W.st[la].v, W.st[la].w, r_a);
+        rxn_a = qrot_inv(Xa.q, cross(r_a, n));
+        inv_mass += m_inv_a + dot(rxn_a, mv(Ia, rxn_a));
+    }
+    if (bb >= 0) {
+        int wi = m->body_world[bb];
+        V3 g = load_v3(m->gravity + 3 * (size_t)(wi > 0 ? wi : 0));
+        const float* qd = qd_prev + 6 * (size_t)bb;
+        v_b = add(velocity_at(V3{qd[0], qd[1], qd[2]}, V3{qd[3], qd[4], qd[5]}, r_b), mul(g, dt));
+        v_b_new = velocity_at(W.st[lb].v, W.st[lb].w, r_b);
+        rxn_b = qrot_inv(Xb.q, cross(r_b, n));
+        inv_mass += m_inv_b + dot(rxn_b, mv(Ib, rxn_b));
+    }
+    if (inv_mass == 0.0f) return;
+    float rel_old = dot(n, sub(v_b, v_a));
+    float rel_new = dot(n, sub(v_b_new, v_a_new));
+    if (rel_old >= 0.0f) return;
+    float dv = (-rel_new - rest * rel_old) / inv_mass;
+    if (ba >= 0) {
+        float dva = -dv;
+        V3 dq = qrot(Xa.q, mul(mv(Ia, rxn_a), dva));
+        acc.add(la, mul(mul(n, m_inv_a), dva), dq);
+    }
+    if (bb >= 0) {
+        float dvb = dv;
+        V3 dq = qrot(Xb.q, mul(mv(Ib, rxn_b), dvb));
+        acc.add(lb, mul(mul(n, m_inv_b), dvb), dq);
+    }
+}
+
+}  // namespace orc
+
 using namespace orc;
 
 extern "C" {
@@ -594,6 +671,10 @@ extern "C" {
 // One SolverXPBD.step over all worlds (host pointers).  seg == NULL means no
 // contacts.  `acc_mode` selects ORC_ACC_FIXED (0) or ORC_ACC_FLOAT (1).
 // `status` receives NB_STATUS_* bits.
+// the shared asin / acos (for the accuracy test)
+float orc_asin(float x) { return nb_asin(x); }
+float orc_acos(float x) { return nb_acos(x); }
+
 int orc_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const OrcSeg* seg, float dt,
              int acc_mode, uint32_t* status) {
     int B = m->body_count;
@@ -711,6 +792,18 @@ int orc_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, co
                     acc.get(i, dl, da);
                     apply_body_delta(W.st[i], dl, da, 1.0f, W.com[i], W.I[i], W.inv_m[i], W.invI[i], dt);
                 }
+            }
+        }
+        if (seg && p->enable_restitution) {
+            // solver_xpbd.py:685-755: after the iterations, from the pre-step state
+            acc.reset(W.nb);
+            for (int c = 0; c < nc; ++c)
+                restitution_contact(W, load_contact(seg, c0 + c), io->body_q_in, io->body_qd_in, dt, acc);
+            for (int i = 0; i < W.nb; ++i) {
+                V3 dl, da;
+                acc.get(i, dl, da);
+                W.st[i].v = add(W.st[i].v, dl);
+                W.st[i].w = add(W.st[i].w, da);
             }
         }
         for (int i = 0; i < W.nb; ++i) {

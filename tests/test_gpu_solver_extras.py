@@ -1,0 +1,174 @@
+"""CUDA path vs the CPU oracle for the solver's optional parts, bit for bit:
+restitution (apply_rigid_restitution, xpbd/kernels.py:2471-2620), per-contact
+forces (accumulate_weighted_contact_impulse + convert_contact_impulse_to_force,
+kernels.py:2301-2393, SolverXPBD.update_contacts, solver_xpbd.py:766-821) and
+the articulated C3 scene (solve_body_joints with revolute drives and limits).
+The oracle itself is checked against the reference's physical tests in
+test_oracle_physics.py.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from newton_custom_contact_b200 import CollisionPipeline, JointType, ModelBuilder, SolverXPBD, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits_equal(a, b):
+    return np.array_equal(np.asarray(a, np.float32).view(np.uint32), np.asarray(b, np.float32).view(np.uint32))
+
+
+def _oracle_public_order(model, lay, segs):
+    """Oracle slot index of every contact in public (world, key) order."""
+    cs = 5 * lay.world_pair_start.astype(np.int64)
+    return np.concatenate([np.arange(cs[w], cs[w] + int(segs.world_count[w])) for w in range(model.world_count)])
+
+
+def _run(model, substeps, dt, iterations, orc, restitution=False, forces=False, joint_target_pos=None):
+    """GPU and oracle loops side by side; per substep compares forces when requested."""
+    if forces:
+        model.request_contact_attributes("force")
+    pipe = CollisionPipeline(model)
+    solver = SolverXPBD(model, iterations=iterations, enable_restitution=restitution)
+    control = model.control()
+    if joint_target_pos is not None:
+        control.joint_target_pos.copy_(torch.as_tensor(joint_target_pos, dtype=torch.float32))
+    s0, s1 = model.state(), model.state()
+    contacts = pipe.contacts()
+    q = model.host("body_q").copy()
+    qd = model.host("body_qd").copy()
+    f = np.zeros((model.body_count, 6), np.float32)
+    p = solver.params()
+    jt = control.joint_target_pos.cpu().numpy() if model.joint_dof_count else None
+    jv = control.joint_target_vel.cpu().numpy() if model.joint_dof_count else None
+    jf = np.zeros(model.joint_dof_count, np.float32)
+    checked = 0
+    for _ in range(substeps):
+        s0.clear_forces()
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, control, contacts, dt)
+        segs = orc.collide(model, pipe.layout, q)
+        out = orc.step(model, pipe.layout, p, q, qd, f, segs, dt, joint_target_pos=jt, joint_target_vel=jv,
+                       joint_f=jf, want_impulse=forces)
+        q, qd = out[0], out[1]
+        if forces:
+            solver.update_contacts(contacts)
+            torch.cuda.synchronize()
+            n = int(contacts.rigid_contact_count.item())
+            got = contacts.force[:n].cpu().numpy()
+            inv_dt = np.float32(1.0) / np.float32(dt)
+            want = out[3][_oracle_public_order(model, pipe.layout, segs)] * inv_dt
+            assert got.shape == want.shape
+            assert _bits_equal(got, want), np.abs(got - want).max()
+            assert not contacts.force[n:].any()
+            checked += int(np.count_nonzero(np.abs(want).sum(axis=1)))
+        s0, s1 = s1, s0
+    torch.cuda.synchronize()
+    return s0.body_q.cpu().numpy(), s0.body_qd.cpu().numpy(), q, qd, checked
+
+
+def test_restitution_parity(cuda, orc):
+    model, info = scenes.scene_c5(worlds=16, device="cuda", restitution=0.5)
+    gq, gqd, q, qd, _ = _run(model, 16, 1.0 / 600.0, 8, orc, restitution=True)
+    np.testing.assert_allclose(gq, q, rtol=1e-5, atol=1e-6)
+    assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
+
+
+def test_restitution_changes_the_step(cuda, orc):
+    """The restitution pass is live on this scene (not a no-op)."""
+    model, _ = scenes.scene_c5(worlds=16, device="cuda", restitution=0.5)
+    a = _run(model, 4, 1.0 / 600.0, 8, orc, restitution=True)
+    model2, _ = scenes.scene_c5(worlds=16, device="cuda", restitution=0.5)
+    b = _run(model2, 4, 1.0 / 600.0, 8, orc, restitution=False)
+    assert not np.array_equal(a[1], b[1])
+
+
+def test_contact_force_parity(cuda, orc):
+    model, info = scenes.scene_c5(worlds=16, device="cuda")
+    gq, gqd, q, qd, checked = _run(model, 8, 1.0 / 600.0, 8, orc, forces=True)
+    assert checked > 0
+    assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
+
+
+def test_contact_force_parity_c2_with_restitution(cuda, orc):
+    model, info = scenes.scene_c2(seed=7, worlds=24, nmin=8, nmax=40, device="cuda")
+    gq, gqd, q, qd, checked = _run(model, 4, info["dt"] / info["substeps"], info["iterations"], orc,
+                                   restitution=True, forces=True)
+    assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
+
+
+def test_forces_of_ingested_contacts(cuda, orc):
+    """Custom contacts in reversed order: each contact's force lands on its own public row."""
+    model, info = scenes.scene_c5(worlds=8, device="cuda")
+    model.request_contact_attributes("force")
+    pipe = CollisionPipeline(model)
+    solver = SolverXPBD(model, iterations=8)
+    s0 = model.state()
+    c1 = pipe.contacts()
+    pipe.collide(s0, c1)
+    out_a = model.state()
+    solver.step(s0, out_a, None, c1, 1.0 / 600.0)
+    solver.update_contacts(c1)
+    fa = c1.force.clone()
+    c2 = pipe.contacts()
+    n = int(c1.rigid_contact_count.item())
+    idx = torch.arange(n - 1, -1, -1, device="cuda")
+    for name in ("shape0", "shape1", "point0", "point1", "offset0", "offset1", "normal", "margin0", "margin1"):
+        getattr(c2, f"rigid_contact_{name}")[:n] = getattr(c1, f"rigid_contact_{name}")[:n][idx]
+    c2.rigid_contact_count.fill_(n)
+    c2.mark_dense_modified()
+    out_b = model.state()
+    solver.step(s0, out_b, None, c2, 1.0 / 600.0)
+    solver.update_contacts(c2)
+    torch.cuda.synchronize()
+    assert torch.equal(out_a.body_q, out_b.body_q)
+    assert torch.equal(c2.force[:n], fa[:n][idx])
+    assert fa[:n].abs().sum() > 0
+
+
+def test_update_contacts_errors(cuda):
+    b = ModelBuilder()
+    b.add_ground_plane()
+    body = b.add_body(xform=((0.0, 0.0, 0.25), (0.0, 0.0, 0.0, 1.0)))
+    b.add_shape_sphere(body, radius=0.25)
+    model = b.finalize(device="cuda")
+    solver = SolverXPBD(model, iterations=2)
+    s0, s1 = model.state(), model.state()
+    contacts = model.contacts()
+    model.collide(s0, contacts)
+    solver.step(s0, s1, model.control(), contacts, 1.0 / 60.0)
+    assert contacts.force is None
+    with pytest.raises(ValueError):
+        solver.update_contacts(contacts)
+    model.request_contact_attributes("force")
+    pipe = CollisionPipeline(model)
+    c2 = pipe.contacts()
+    fresh = SolverXPBD(model, iterations=2)
+    with pytest.raises(ValueError):
+        fresh.update_contacts(c2)  # no step yet
+    pipe.collide(s0, c2)
+    fresh.step(s0, s1, None, c2, 1.0 / 60.0)
+    other = CollisionPipeline(model, rigid_contact_max=c2.rigid_contact_max + 7).contacts()
+    with pytest.raises(ValueError):
+        fresh.update_contacts(other)  # capacity mismatch
+
+
+@pytest.mark.parametrize("substeps", [1, 8])
+def test_step_parity_c3_arms(cuda, orc, substeps):
+    """Revolute drives and limits (solve_body_joints).  The twist / swing angles
+    use the library's own asin / acos on both sides (a device / host-libm
+    last-ulp difference would be amplified by 1/dt into the velocities), so
+    the trajectories agree bit for bit."""
+    model, info = scenes.scene_c3(worlds=6, device="cuda")
+    # drive targets A sin(phase) on the arms' revolute dofs (free joints of the boxes stay 0)
+    rev = np.nonzero(model.host("joint_type") == int(JointType.REVOLUTE))[0]
+    targets = np.zeros(model.joint_dof_count, np.float32)
+    targets[model.host("joint_qd_start")[rev]] = 0.5 * np.sin(info["phases"]).reshape(-1)
+    gq, gqd, q, qd, _ = _run(model, substeps, info["dt"] / info["substeps"], info["iterations"], orc,
+                             joint_target_pos=targets)
+    np.testing.assert_allclose(gq, q, rtol=1e-5, atol=1e-6)
+    assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
+    # the arms are live: joint drives moved the links
+    assert not np.allclose(gq[: 7], model.host("body_q")[: 7], atol=1e-7)

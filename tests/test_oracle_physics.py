@@ -1,0 +1,188 @@
+"""Physical known-answer tests of the CPU oracle's solver extras.
+
+Scenes and assertions are those of the reference's own tests:
+  * restitution: newton/tests/test_physics_validation.py:644-723 (sphere dropped
+    1 m, rebound height e^2 * h within 1 %, ratio of the two within 1 %), with
+    SolverXPBD(iterations=10, angular_damping=0, enable_restitution=True)
+    (:1662-1671).  The reference uses a Y-up builder; this one is Z-up, so the
+    same drop runs along Z.
+  * contact forces: newton/tests/test_solver_xpbd.py:469-656 (static
+    equilibrium of a small sphere, a heavy sphere, a box and a three-cube
+    pyramid; iterations=32, rigid_contact_con_weighting=True) and :658-726
+    (zero force in free fall and for a pair inside the gap).
+The CUDA path is compared with the oracle bit for bit in test_gpu_solver_extras.py.
+"""
+
+import numpy as np
+import pytest
+
+from newton_custom_contact_b200 import ModelBuilder, SolverXPBD
+from newton_custom_contact_b200.collide import PairLayout
+
+
+def _sim(orc, model, solver, dt, steps, on_step=None, want_impulse=False):
+    lay = PairLayout(model, model.host("shape_contact_pairs"))
+    p = solver.params()
+    q = model.host("body_q").copy()
+    qd = model.host("body_qd").copy()
+    f = np.zeros((model.body_count, 6), np.float32)
+    for i in range(steps):
+        segs = orc.collide(model, lay, q)
+        out = orc.step(model, lay, p, q, qd, f, segs, dt, want_impulse=want_impulse)
+        q, qd = out[0], out[1]
+        if on_step is not None:
+            on_step(i, q, qd, segs, lay, out[3] if want_impulse else None)
+    return q, qd
+
+
+def _forces_by_contact(orc, model, lay, segs, imp, dt):
+    """[(shape0, shape1, force6)] for every live contact (impulse / dt, kernels.py:2363-2393)."""
+    tab = orc.contacts_table(model, lay, segs)
+    cs = 5 * lay.world_pair_start.astype(np.int64)
+    slots = np.concatenate([np.arange(cs[w], cs[w] + int(segs.world_count[w])) for w in range(model.world_count)])
+    return tab[:, 1].astype(int), tab[:, 2].astype(int), imp[slots] * np.float32(1.0 / dt)
+
+
+def test_oracle_restitution_bounce(orc):
+    g, h_drop, radius = -10.0, 1.0, 0.05
+    rebound = {}
+    for e in (0.5, 0.8):
+        cfg = ModelBuilder.ShapeConfig()
+        cfg.mu = 0.0
+        cfg.restitution = e
+        cfg.margin = 0.001
+        cfg.gap = 0.0
+        b = ModelBuilder(gravity=g)
+        b.add_ground_plane(cfg=cfg)
+        body = b.add_body(xform=((0.0, 0.0, radius + h_drop), (0.0, 0.0, 0.0, 1.0)))
+        b.add_shape_sphere(body, radius=radius, cfg=cfg)
+        model = b.finalize(device="cpu")
+        solver = SolverXPBD(model, iterations=10, angular_damping=0.0, enable_restitution=True)
+        sim_dt = 1e-3
+        steps = int(3.0 * np.sqrt(2.0 * h_drop / abs(g)) / sim_dt)
+        z = []
+        _sim(orc, model, solver, sim_dt, steps, on_step=lambda i, q, qd, s, l, im: z.append(float(q[0, 2])))
+        z = np.array(z)
+        assert z.min() > -0.01
+        impact = next(i for i in range(1, len(z) - 1) if z[i] < z[i - 1] and z[i] <= z[i + 1])
+        h = z[impact:].max() - radius
+        assert abs(h - e * e * h_drop) <= 0.01 * e * e * h_drop, (e, h)
+        rebound[e] = h
+    ratio = rebound[0.8] / rebound[0.5]
+    assert abs(ratio - 2.56) <= 0.01 * 2.56
+
+
+def test_oracle_contact_force_static_equilibrium(orc):
+    gravity = 9.81
+    sr, sd = 0.25, 1000.0
+    hr, hd = 0.5, 2000.0
+    bh, cube_h = 0.5, 0.5
+    sphere_m = sd * 4.0 / 3.0 * np.pi * sr ** 3
+    heavy_m = hd * 4.0 / 3.0 * np.pi * hr ** 3
+    box_m = 1000.0 * (2 * bh) ** 3
+    cube_mg = 1000.0 * (2 * cube_h) ** 3 * gravity
+    ident = (0.0, 0.0, 0.0, 1.0)
+    b = ModelBuilder()
+    b.add_ground_plane()
+    b.default_shape_cfg.density = sd
+    sphere = b.add_body(xform=((0.0, 0.0, sr), ident))
+    b.add_shape_sphere(sphere, radius=sr)
+    b.default_shape_cfg.density = hd
+    heavy = b.add_body(xform=((10.0, 0.0, hr), ident))
+    b.add_shape_sphere(heavy, radius=hr)
+    b.default_shape_cfg.density = 1000.0
+    box = b.add_body(xform=((20.0, 0.0, bh), ident))
+    b.add_shape_box(box, hx=bh, hy=bh, hz=bh)
+    left = b.add_body(xform=((30.0 - cube_h, 0.0, cube_h), ident))
+    b.add_shape_box(left, hx=cube_h, hy=cube_h, hz=cube_h)
+    right = b.add_body(xform=((30.0 + cube_h, 0.0, cube_h), ident))
+    b.add_shape_box(right, hx=cube_h, hy=cube_h, hz=cube_h)
+    top = b.add_body(xform=((30.0, 0.0, 3.0 * cube_h), ident))
+    b.add_shape_box(top, hx=cube_h, hy=cube_h, hz=cube_h)
+    model = b.finalize(device="cpu")
+    solver = SolverXPBD(model, iterations=32, rigid_contact_con_weighting=True)
+    shape_body = model.host("shape_body")
+    sub_dt = 1.0 / 60.0 / 8
+    settle, avg = 200, 60
+    acc = {"sphere": np.zeros(3), "heavy": np.zeros(3), "box": np.zeros(3), "left": 0.0, "right": 0.0,
+           "box_contacts": []}
+
+    def on_step(i, q, qd, segs, lay, imp):
+        if i < settle * 8 or (i + 1) % 8:
+            return  # update_contacts after the last substep of every averaged frame
+        s0, s1, f = _forces_by_contact(orc, model, lay, segs, imp, sub_dt)
+        nbox = 0
+        for a, c, fc in zip(s0, s1, f):
+            if a == 0:
+                other, fv = c, fc[:3]
+            elif c == 0:
+                other, fv = a, -fc[:3]
+            else:
+                continue
+            ob = shape_body[other]
+            if ob == sphere:
+                acc["sphere"] += fv
+            elif ob == heavy:
+                acc["heavy"] += fv
+            elif ob == box:
+                acc["box"] += fv
+                nbox += 1
+            elif ob == left:
+                acc["left"] += -fv[2]
+            elif ob == right:
+                acc["right"] += -fv[2]
+        acc["box_contacts"].append(nbox)
+
+    _sim(orc, model, solver, sub_dt, (settle + avg) * 8, on_step=on_step, want_impulse=True)
+    assert min(acc["box_contacts"]) > 1
+    sph, hv, bx = acc["sphere"] / avg, acc["heavy"] / avg, acc["box"] / avg
+    np.testing.assert_allclose(sph[2], -sphere_m * gravity, rtol=0.05)
+    np.testing.assert_allclose(sph[:2], 0.0, atol=0.5)
+    np.testing.assert_allclose(hv[2], -heavy_m * gravity, rtol=0.05)
+    np.testing.assert_allclose(hv[:2], 0.0, atol=0.5)
+    np.testing.assert_allclose(bx[2], -box_m * gravity, rtol=0.10)
+    np.testing.assert_allclose(bx[:2], 0.0, atol=1.0)
+    np.testing.assert_allclose(acc["left"] / avg, 1.5 * cube_mg, rtol=0.15)
+    np.testing.assert_allclose(acc["right"] / avg, 1.5 * cube_mg, rtol=0.15)
+
+
+def test_oracle_contact_force_zero_free_fall_and_inside_gap(orc):
+    ident = (0.0, 0.0, 0.0, 1.0)
+    # free fall, no ground
+    b = ModelBuilder()
+    body = b.add_body(xform=((0.0, 0.0, 5.0), ident))
+    b.add_shape_sphere(body, radius=0.25)
+    model = b.finalize(device="cpu")
+    seen = []
+    _sim(orc, model, SolverXPBD(model, iterations=2), 1.0 / 60.0, 1, want_impulse=True,
+         on_step=lambda i, q, qd, s, l, imp: seen.append(np.abs(imp).max()))
+    assert seen[0] == 0.0
+    # pair inside a 1 m gap, not touching, no gravity
+    b = ModelBuilder(gravity=0.0)
+    b.default_shape_cfg.gap = 1.0
+    b.add_ground_plane()
+    body = b.add_body(xform=((0.0, 0.0, 0.25 + 0.5), ident))
+    b.add_shape_sphere(body, radius=0.25)
+    model = b.finalize(device="cpu")
+    out = {}
+
+    def grab(i, q, qd, segs, lay, imp):
+        out["n"] = int(segs.world_count.sum())
+        out["f"] = _forces_by_contact(orc, model, lay, segs, imp, 1.0 / 60.0)[2]
+
+    _sim(orc, model, SolverXPBD(model, iterations=2), 1.0 / 60.0, 1, want_impulse=True, on_step=grab)
+    assert out["n"] > 0
+    np.testing.assert_allclose(out["f"][:, :3], 0.0, atol=1e-6)
+
+
+def test_shared_asin_acos_accuracy(orc):
+    """The asin / acos used by the joint solve on both sides: within 2 ulp of float64 on [-1, 1]."""
+    lib = orc.load()
+    xs = np.concatenate([np.linspace(-1.0, 1.0, 20001, dtype=np.float32),
+                         np.float32([0.0, -0.0, 1e-30, 1e-10, 1e-5, 0.4999999, 0.5, 0.5000001, 0.9999999])])
+    for fn, ref in ((lib.orc_asin, np.arcsin), (lib.orc_acos, np.arccos)):
+        got = np.array([fn(float(x)) for x in xs], np.float32)
+        exact = ref(xs.astype(np.float64))
+        ulp = np.spacing(np.abs(exact).astype(np.float32)).astype(np.float64)
+        assert (np.abs(got.astype(np.float64) - exact) / ulp).max() <= 2.0
+    assert lib.orc_asin(1.0) == np.float32(np.pi / 2) and lib.orc_acos(1.0) == 0.0
