@@ -1,6 +1,6 @@
 // Collision detection for many independent worlds.
 //
-// Three kernels per substep:
+// Kernels per substep:
 //   1. broadphase_kernel -- one warp per world (worlds pulled from a device
 //      counter, largest first).  The warp computes every shape's world
 //      transform and AABB (compute_shape_aabbs, newton/_src/sim/collide.py:150-275),
@@ -12,10 +12,12 @@
 //      candidate list and pushed to one of two work queues: pairs the analytic
 //      primitive path finishes and pairs that need MPR/GJK, so the narrow
 //      phase runs on convergent warps.
-//   2. narrowphase_kernel -- one thread per candidate of every world (flat
-//      over both queues): primitive / MPR / GJK / manifold narrow phase with
+//   2. narrow phase -- one thread per candidate of every world, with
 //      write_contact semantics (narrow_phase.py:153-776, collide.py:62-147),
-//      <= 5 contacts written into the candidate's own slots.
+//      <= 5 contacts written into the candidate's own slots:
+//      narrow_analytic_kernel (primitive pairs), gjk_prefilter_kernel (drops
+//      pairs that are provably farther apart than the contact threshold and
+//      compacts the rest), narrow_gjk_kernel (MPR / GJK / manifold).
 //   3. publish (world_scan_kernel + publish_kernel) -- the reference's dense
 //      Contacts arrays ordered by (world, key): walking a world's candidates
 //      in order and each candidate's slots in sub-key order is exactly the key
@@ -228,15 +230,127 @@ narrow_analytic_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContac
     }
 }
 
-// MPR / GJK / manifold queue
+// ---- separation prefilter of the MPR/GJK queue
+
+__device__ __forceinline__ V3 mat_col(const M33& r, int k) { return V3{r.m[0][k], r.m[1][k], r.m[2][k]}; }
+
+__device__ __forceinline__ float bounding_radius(const Geom& g) {
+    if (g.type == NB_GEO_BOX) return length(g.scale);
+    if (g.type == NB_GEO_CAPSULE) return g.scale.x + g.scale.y;
+    return g.scale.x;  // sphere
+}
+
+// extent of a box (half extents h, axes R) along unit axis L
+__device__ __forceinline__ float box_extent(const M33& R, V3 h, V3 L) {
+    return fabsf(dot(L, mat_col(R, 0))) * h.x + fabsf(dot(L, mat_col(R, 1))) * h.y +
+           fabsf(dot(L, mat_col(R, 2))) * h.z;
+}
+
+// True only when the pair provably produces no contact: a lower bound of the
+// distance between the two shapes (bounding spheres; separating axes for
+// box-box and capsule-box; the signed distance of the bounding sphere for an
+// infinite plane) exceeds the contact threshold gap_a + gap_b + margin_a +
+// margin_b by a slack that covers fp32 rounding and MPR's 1e-4 inflation.  Such
+// a pair makes MPR find no overlap and leaves the GJK distance above the
+// threshold (narrow_phase.py:627-776, collision_core.py:626-725), so the
+// reference path writes nothing for it either.
+__device__ __noinline__ bool gjk_pair_separated(const Geom& a, const Geom& b) {
+    const V3 pa = a.xf.p, pb = b.xf.p;
+    const float mag = fmaxf(fmaxf(fabsf(pa.x), fmaxf(fabsf(pa.y), fabsf(pa.z))),
+                            fmaxf(fabsf(pb.x), fmaxf(fabsf(pb.y), fabsf(pb.z))));
+    const float thr = a.gap + b.gap + a.margin + b.margin + 2.0e-3f + 1.0e-5f * mag;
+    if (a.type == NB_GEO_PLANE || b.type == NB_GEO_PLANE) {
+        const Geom& pl = a.type == NB_GEO_PLANE ? a : b;
+        const Geom& o = a.type == NB_GEO_PLANE ? b : a;
+        if (o.type == NB_GEO_PLANE || pl.scale.x != 0.0f || pl.scale.y != 0.0f) return false;  // finite planes
+        const V3 n = qrot(pl.xf.q, V3{0.0f, 0.0f, 1.0f});
+        return dot(sub(o.xf.p, pl.xf.p), n) - bounding_radius(o) > thr;
+    }
+    const V3 d = sub(pb, pa);
+    if (length(d) - bounding_radius(a) - bounding_radius(b) > thr) return true;
+    const bool box_a = a.type == NB_GEO_BOX, box_b = b.type == NB_GEO_BOX;
+    if (box_a && box_b) {
+        const M33 Ra = quat_to_matrix(a.xf.q), Rb = quat_to_matrix(b.xf.q);
+        for (int i = 0; i < 3; ++i) {
+            V3 L = mat_col(Ra, i);
+            if (fabsf(dot(d, L)) - box_extent(Ra, a.scale, L) - box_extent(Rb, b.scale, L) > thr) return true;
+            L = mat_col(Rb, i);
+            if (fabsf(dot(d, L)) - box_extent(Ra, a.scale, L) - box_extent(Rb, b.scale, L) > thr) return true;
+        }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                const V3 c = cross(mat_col(Ra, i), mat_col(Rb, j));
+                const float len = length(c);
+                if (!(len > 1.0e-3f)) continue;  // near-parallel edges: covered by the face axes
+                const V3 L = smul(1.0f / len, c);
+                if (fabsf(dot(d, L)) - box_extent(Ra, a.scale, L) - box_extent(Rb, b.scale, L) > thr) return true;
+            }
+        return false;
+    }
+    if ((box_a && b.type == NB_GEO_CAPSULE) || (box_b && a.type == NB_GEO_CAPSULE)) {
+        const Geom& bx = box_a ? a : b;
+        const Geom& cp = box_a ? b : a;
+        const M33 Rb = quat_to_matrix(bx.xf.q);
+        const V3 u = qrot(cp.xf.q, V3{0.0f, 0.0f, 1.0f});
+        const float r = cp.scale.x, hh = cp.scale.y;
+        for (int i = 0; i < 4; ++i) {
+            const V3 L = i < 3 ? mat_col(Rb, i) : u;
+            if (fabsf(dot(d, L)) - box_extent(Rb, bx.scale, L) - (fabsf(dot(u, L)) * hh + r) > thr) return true;
+        }
+        for (int i = 0; i < 3; ++i) {
+            const V3 c = cross(u, mat_col(Rb, i));
+            const float len = length(c);
+            if (!(len > 1.0e-3f)) continue;
+            const V3 L = smul(1.0f / len, c);
+            if (fabsf(dot(d, L)) - box_extent(Rb, bx.scale, L) - (fabsf(dot(u, L)) * hh + r) > thr) return true;
+        }
+    }
+    return false;
+}
+
+// One thread per MPR/GJK item: provably separated pairs get zero contacts,
+// the rest are compacted (warp-aggregated) into the queue's front, which the
+// analytic kernel has consumed; front and back cannot overlap (the back holds
+// at most pair_count items of 2 * pair_count).
 __global__ void __launch_bounds__(kNT)
-narrow_gjk_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
+gjk_prefilter_kernel(NbModelDesc m, NbContactSeg seg) {
     const int n1 = seg.work_counter[3];
     const int P = m.pair_count;
+    int2* queue = reinterpret_cast<int2*>(seg.queue);
+    const float4* geom = reinterpret_cast<const float4*>(seg.geom);
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n1; base += stride) {
+        const int i = base + lane;
+        bool keep = false;
+        int2 e = make_int2(0, 0);
+        if (i < n1) {
+            e = queue[2 * (size_t)P - 1 - i];
+            const unsigned pw = reinterpret_cast<const unsigned*>(m.pair_shapes)[seg.cand[e.x]];
+            const int la = (int)(pw & 0xFFFFu), lb = (int)(pw >> 16);
+            const int s0 = m.world_shape_start[e.y];
+            const int nloc = m.world_shape_start[e.y + 1] - s0;
+            const int sa = la < nloc ? s0 + la : m.global_shapes[la - nloc];
+            const int sb = lb < nloc ? s0 + lb : m.global_shapes[lb - nloc];
+            keep = !gjk_pair_separated(load_geom(geom + 5 * (size_t)sa, sa), load_geom(geom + 5 * (size_t)sb, sb));
+            if (!keep) seg.counts[e.x] = 0;
+        }
+        const unsigned bal = __ballot_sync(kFull, keep);
+        int off = 0;
+        if (lane == 0 && bal) off = atomicAdd(&seg.work_counter[5], __popc(bal));
+        off = __shfl_sync(kFull, off, 0);
+        if (keep) queue[off + __popc(bal & ((1u << lane) - 1u))] = e;
+    }
+}
+
+// MPR / GJK / manifold on the items that survived the prefilter
+__global__ void __launch_bounds__(kNT)
+narrow_gjk_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
+    const int n = seg.work_counter[5];
     const int2* queue = reinterpret_cast<const int2*>(seg.queue);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += gridDim.x * blockDim.x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         NarrowItem it;
-        narrow_setup(m, seg, body_q, queue[2 * (size_t)P - 1 - i], it);
+        narrow_setup(m, seg, body_q, queue[i], it);
         gjk_pair(it.wr, it.ga, it.gb);
         narrow_finish(seg, it);
     }
@@ -430,12 +544,17 @@ cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const N
     }
     e = cudaMemsetAsync(seg->work_counter, 0, 4 * sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(seg->work_counter + 5, 0, sizeof(int32_t), stream);
+    if (e != cudaSuccess) return e;
     const int sms = sm_count();
     broadphase_kernel<<<sms * 4, kBT, smem, stream>>>(*m, body_q, *seg);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const int ng = grid > 0 ? grid : sms * 8;
     narrow_analytic_kernel<<<ng, kNT, 0, stream>>>(*m, body_q, *seg);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    gjk_prefilter_kernel<<<ng, kNT, 0, stream>>>(*m, *seg);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     narrow_gjk_kernel<<<ng, kNT, 0, stream>>>(*m, body_q, *seg);

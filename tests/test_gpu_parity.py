@@ -174,3 +174,26 @@ def test_custom_contacts_ingested(cuda, orc):
     torch.cuda.synchronize()
     assert torch.equal(out_a.body_q, out_b.body_q)
     assert torch.equal(out_a.body_qd, out_b.body_qd)
+
+
+def test_collide_bit_exact_in_piled_state(cuda, orc):
+    """Contacts after 25 frames of a 96-world drop (bodies landed and piled up,
+    many box-box / box-capsule pairs near contact) equal the oracle's on the
+    same poses: the MPR/GJK separation prefilter drops no contact."""
+    model, info = scenes.scene_c2(seed=11, worlds=96, device="cuda")
+    pipe = CollisionPipeline(model)
+    solver = SolverXPBD(model, iterations=info["iterations"])
+    s0, s1 = model.state(), model.state()
+    contacts = pipe.contacts()
+    dt = info["dt"] / info["substeps"]
+    for _ in range(25 * info["substeps"]):
+        s0.clear_forces()
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, dt)
+        s0, s1 = s1, s0
+    pipe.collide(s0, contacts)
+    torch.cuda.synchronize()
+    assert pipe.status(contacts) == 0
+    segs = orc.collide(model, pipe.layout, s0.body_q.cpu().numpy())
+    table = _assert_contacts_equal(model, pipe, contacts, segs, orc)
+    assert table.shape[0] > 5000
