@@ -249,7 +249,7 @@ int32_t nb_default_grid(void);
  * Writes the solver-format segments in `seg`.
  */
 int nb_collide(const NbModelDesc* model, const float* body_q, const NbContactSeg* seg,
-               int32_t grid_ctas, void* stream);
+               int32_t grid_ctas, void* stream);  /* grid_ctas: narrow-phase CTAs, <= 0 = library default */
 
 /*
  * Publish solver-format segments into the reference's dense Contacts arrays

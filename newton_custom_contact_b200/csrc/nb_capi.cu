@@ -75,7 +75,9 @@ int nb_collide(const NbModelDesc* model, const float* body_q, const NbContactSeg
         (model->global_shape_count > 0 && !model->global_shapes))
         return NB_ERR_INVALID;
     if ((int64_t)nb_collide_smem_bytes(model) > smem_limit()) return NB_ERR_UNSUPPORTED;
-    cudaError_t e = nb_launch_collide(model, body_q, seg, grid_for(grid_ctas), (cudaStream_t)stream);
+    // grid_ctas <= 0: each narrow-phase kernel uses its own default (enough CTAs
+    // to reach its register-limited occupancy)
+    cudaError_t e = nb_launch_collide(model, body_q, seg, grid_ctas > 0 ? grid_ctas : 0, (cudaStream_t)stream);
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
 

@@ -550,14 +550,23 @@ cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const N
     broadphase_kernel<<<sms * 4, kBT, smem, stream>>>(*m, body_q, *seg);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const int ng = grid > 0 ? grid : sms * 8;
-    narrow_analytic_kernel<<<ng, kNT, 0, stream>>>(*m, body_q, *seg);
+    // default grids: one wave at the kernel's occupancy (grid-stride loops)
+    static int occ_analytic = 0, occ_prefilter = 0, occ_gjk = 0;
+    if (!occ_gjk) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_analytic, narrow_analytic_kernel, kNT, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_prefilter, gjk_prefilter_kernel, kNT, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_gjk, narrow_gjk_kernel, kNT, 0);
+        occ_analytic = occ_analytic > 0 ? occ_analytic : 4;
+        occ_prefilter = occ_prefilter > 0 ? occ_prefilter : 4;
+        occ_gjk = occ_gjk > 0 ? occ_gjk : 4;
+    }
+    narrow_analytic_kernel<<<grid > 0 ? grid : sms * occ_analytic, kNT, 0, stream>>>(*m, body_q, *seg);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    gjk_prefilter_kernel<<<ng, kNT, 0, stream>>>(*m, *seg);
+    gjk_prefilter_kernel<<<grid > 0 ? grid : sms * occ_prefilter, kNT, 0, stream>>>(*m, *seg);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    narrow_gjk_kernel<<<ng, kNT, 0, stream>>>(*m, body_q, *seg);
+    narrow_gjk_kernel<<<grid > 0 ? grid : sms * occ_gjk, kNT, 0, stream>>>(*m, body_q, *seg);
     return cudaGetLastError();
 }
 
