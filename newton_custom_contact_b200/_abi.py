@@ -136,7 +136,7 @@ class NbModelDesc(C.Structure):
         ("group_threads", C.c_int32),
         ("cta_threads", C.c_int32),
         ("smem_floats_per_batch", C.c_int32),
-        ("pad1", C.c_int32),
+        ("step_mode", C.c_int32),
         ("batch_world", _fp),
         ("batch_slab", _fp),
     ]

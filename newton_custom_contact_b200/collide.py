@@ -278,11 +278,13 @@ class CollisionPipeline:
         c._layout = self
         c._seg_valid = False
 
-    def set_step_schedule(self, group_threads: int | None = None) -> None:
-        """Pack worlds into shared-memory batches for the step kernel (see schedule.py)."""
+    def set_step_schedule(self, group_threads: int | None = None, mode: str | None = None) -> None:
+        """Choose how the step kernel maps worlds to warps / CTAs (see schedule.py):
+        ``mode`` "warp", "warp_compact" or "batch" (with ``group_threads``); default: the
+        first warp mode the largest world fits, else batches."""
         from .schedule import build_schedule
 
-        sched = build_schedule(self.model, group_threads)
+        sched = build_schedule(self.model, group_threads, mode)
         self._schedule = sched
         self._layout_dev["batch_world"] = torch.from_numpy(sched.batch_world.reshape(-1)).to(self.device)
         self._layout_dev["batch_slab"] = torch.from_numpy(sched.batch_slab.reshape(-1)).to(self.device)

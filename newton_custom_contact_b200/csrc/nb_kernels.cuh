@@ -20,3 +20,4 @@ cudaError_t nb_launch_step(const NbModelDesc* m, const NbXpbdParams* p, const Nb
                            float dt, int grid, cudaStream_t stream);
 cudaError_t nb_launch_contact_forces(const float* imp, const int32_t* count, int cap, float dt, float* force,
                                      cudaStream_t stream);
+int nb_step_slab_words(int compact);

@@ -28,12 +28,25 @@ namespace {
 
 constexpr int kST = NB_STEP_THREADS;  // threads per CTA
 
-struct SBodies {
+// Per-world body state in shared memory.  kCompact = false: everything the
+// substep touches is staged (49 words per body); kCompact = true: only the
+// mutable part (pose, twist, delta accumulators, flags, contact count: 27
+// words per body) is staged and the static mass properties are read from the
+// model (read-only path), so worlds of up to 128 bodies fit one warp's share
+// of the arena.
+template <bool kCompact>
+struct SBodiesT {
+    static constexpr bool compact = kCompact;
     int nb;                    // bodies of this world (also the SoA stride)
+    int b0;                    // global index of the world's first body
     float* f;                  // [13][nb] pose (7) + twist (6)
-    float* c;                  // [4][nb]  com (3), effective inv mass
-    float* I;                  // [9][nb]
-    float* iI;                 // [9][nb]  effective inverse inertia
+    float* c;                  // [4][nb]  com (3), effective inv mass          (full layout)
+    float* I;                  // [9][nb]                                         (full layout)
+    float* iI;                 // [9][nb]  effective inverse inertia              (full layout)
+    const float* g_com;        // model arrays                                    (compact layout)
+    const float* g_inv_m;
+    const float* g_I;
+    const float* g_iI;
     float* frc;                // [6][nb]  body_f + joint forces (aliases acc before integration)
     int* flags;                // [nb]
     unsigned long long* acc;   // [6][nb]
@@ -51,18 +64,42 @@ struct SBodies {
         f[7 * nb + i] = lv.x; f[8 * nb + i] = lv.y; f[9 * nb + i] = lv.z;
         f[10 * nb + i] = aw.x; f[11 * nb + i] = aw.y; f[12 * nb + i] = aw.z;
     }
-    __device__ V3 com(int i) const { return V3{c[i], c[nb + i], c[2 * nb + i]}; }
-    __device__ float inv_m(int i) const { return c[3 * nb + i]; }
+    __device__ bool kinematic(int i) const { return (flags[i] & NB_BODY_KINEMATIC) != 0; }
+    __device__ V3 com(int i) const {
+        if constexpr (kCompact) {
+            const float* r = g_com + 3 * (size_t)(b0 + i);
+            return V3{__ldg(r), __ldg(r + 1), __ldg(r + 2)};
+        } else {
+            return V3{c[i], c[nb + i], c[2 * nb + i]};
+        }
+    }
+    __device__ float inv_m(int i) const {
+        if constexpr (kCompact) return kinematic(i) ? 0.0f : __ldg(g_inv_m + b0 + i);
+        else return c[3 * nb + i];
+    }
     __device__ M33 inertia(int i) const {
         M33 r;
+        if constexpr (kCompact) {
+            const float* a = g_I + 9 * (size_t)(b0 + i);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) r.m[k / 3][k % 3] = I[k * nb + i];
+            for (int k = 0; k < 9; ++k) r.m[k / 3][k % 3] = __ldg(a + k);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) r.m[k / 3][k % 3] = I[k * nb + i];
+        }
         return r;
     }
     __device__ M33 inv_inertia(int i) const {
         M33 r;
+        if constexpr (kCompact) {
+            const float* a = g_iI + 9 * (size_t)(b0 + i);
+            const bool kin = kinematic(i);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) r.m[k / 3][k % 3] = iI[k * nb + i];
+            for (int k = 0; k < 9; ++k) r.m[k / 3][k % 3] = kin ? 0.0f : __ldg(a + k);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) r.m[k / 3][k % 3] = iI[k * nb + i];
+        }
         return r;
     }
     __device__ void add_delta(int i, V3 lin, V3 ang, unsigned* bad) {
@@ -93,21 +130,35 @@ struct SBodies {
 };
 
 // 4-byte words of one world's slab: acc (12 words/body, 8-byte aligned first),
-// f 13, c 4, I 9, iI 9, flags 1, cnt 1
-__host__ __device__ constexpr int slab_words_per_body() { return 12 + 13 + 4 + 9 + 9 + 1 + 1; }
+// f 13, [c 4, I 9, iI 9,] flags 1, cnt 1
+template <bool kCompact>
+__host__ __device__ constexpr int slab_words_per_body() { return kCompact ? 12 + 13 + 1 + 1 : 12 + 13 + 4 + 9 + 9 + 1 + 1; }
 
-__device__ SBodies sbodies_carve(unsigned char* slab, int nb) {
-    SBodies s;
+template <bool kCompact>
+__device__ SBodiesT<kCompact> sbodies_carve(unsigned char* slab, const NbModelDesc& m, int b0, int nb) {
+    SBodiesT<kCompact> s;
     s.nb = nb;
+    s.b0 = b0;
     unsigned long long* a = reinterpret_cast<unsigned long long*>(slab);
     s.acc = a;
     s.frc = reinterpret_cast<float*>(a);  // used only before integration
     float* fl = reinterpret_cast<float*>(a + 6 * (size_t)nb);
     s.f = fl;
-    s.c = fl + 13 * nb;
-    s.I = s.c + 4 * nb;
-    s.iI = s.I + 9 * nb;
-    int* ip = reinterpret_cast<int*>(s.iI + 9 * nb);
+    s.g_com = m.body_com;
+    s.g_inv_m = m.body_inv_mass;
+    s.g_I = m.body_inertia;
+    s.g_iI = m.body_inv_inertia;
+    float* after;
+    if constexpr (kCompact) {
+        s.c = s.I = s.iI = nullptr;
+        after = s.f + 13 * nb;
+    } else {
+        s.c = fl + 13 * nb;
+        s.I = s.c + 4 * nb;
+        s.iI = s.I + 9 * nb;
+        after = s.iI + 9 * nb;
+    }
+    int* ip = reinterpret_cast<int*>(after);
     s.flags = ip;
     s.cnt = ip + nb;
     return s;
@@ -237,7 +288,8 @@ __device__ float angular_correction(float err, float derr, Q4 qa, Q4 qb, const M
 
 // Penetration depth of one solver record (the first test of
 // solve_body_contact_positions, kernels.py:2100-2130); reads 48 bytes.
-__device__ __forceinline__ float contact_depth(const SBodies& S, float4 r0, float4 r1, float4 r2, int la, int lb,
+template <class SB>
+__device__ __forceinline__ float contact_depth(const SB& S, float4 r0, float4 r1, float4 r2, int la, int lb,
                                                TF& Xa, TF& Xb, V3& bx_a, V3& bx_b) {
     Xa = la >= 0 ? S.q(la) : tf_identity();
     Xb = lb >= 0 ? S.q(lb) : tf_identity();
@@ -249,7 +301,8 @@ __device__ __forceinline__ float contact_depth(const SBodies& S, float4 r0, floa
 
 // true when solve_contact would move a body (NaN depths count, so they
 // propagate exactly as in the reference)
-__device__ __forceinline__ bool contact_active(const SBodies& S, float4 r0, float4 r1, float4 r2) {
+template <class SB>
+__device__ __forceinline__ bool contact_active(const SB& S, float4 r0, float4 r1, float4 r2) {
     const int tag = __float_as_int(r2.w);
     const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
     if (la == lb) return false;
@@ -261,7 +314,8 @@ __device__ __forceinline__ bool contact_active(const SBodies& S, float4 r0, floa
 // solve_body_contact_positions for one contact (kernels.py:2062-2298)
 // imp (optional) receives the A-side spatial delta (the contact_impulse_iter
 // entry of the reference) of an active contact.
-__device__ void solve_contact(const NbModelDesc& m, SBodies& S, float4 r0, float4 r1, float4 r2, float4 r3, float4 r4,
+template <class SB>
+__device__ void solve_contact(const NbModelDesc& m, SB& S, float4 r0, float4 r1, float4 r2, float4 r3, float4 r4,
                               float relaxation, float dt, bool weighting, unsigned* bad, float* imp) {
     const int sa = __float_as_int(r3.w), sb = __float_as_int(r4.w);
     if (sa == sb) return;
@@ -369,7 +423,8 @@ __device__ __forceinline__ V3 velocity_at(V3 v, V3 w, V3 r) { return add(cross(w
 // apply_rigid_restitution (kernels.py:2471-2620) for one solver record:
 // pre-step poses / twists from the step's inputs, current twists from the
 // slab; velocity deltas go to the fixed-point accumulators.
-__device__ __noinline__ void restitution_contact(const NbModelDesc& m, SBodies& S, const float4* r, int b0,
+template <class SB>
+__device__ __noinline__ void restitution_contact(const NbModelDesc& m, SB& S, const float4* r, int b0,
                                                  const float* __restrict__ q_prev, const float* __restrict__ qd_prev,
                                                  float dt, unsigned* bad) {
     const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
@@ -437,8 +492,8 @@ __device__ __noinline__ void restitution_contact(const NbModelDesc& m, SBodies& 
 // records: raw iteration impulses from the scratch (all zero for contacts
 // that were not active), weighted by this iteration's body contact counts,
 // added to the public contact's row; the scratch is cleared again.
-template <int G>
-__device__ __forceinline__ void accumulate_impulses(const SBodies& S, const float4* __restrict__ R, int nc,
+template <int G, class SB>
+__device__ __forceinline__ void accumulate_impulses(const SB& S, const float4* __restrict__ R, int nc,
                                                     int64_t rec_base, const int32_t* __restrict__ rec_index,
                                                     float* __restrict__ scratch, float* __restrict__ out, int cap,
                                                     bool weighting, int t) {
@@ -513,7 +568,8 @@ __device__ void joint_axes(const NbModelDesc& m, int start, int count, const flo
 }
 
 // solve_body_joints for one joint (kernels.py:1441-1942)
-__device__ __noinline__ void solve_joint(const NbModelDesc& m, SBodies& S, int b0, int j, const float* tpos,
+template <class SB>
+__device__ __noinline__ void solve_joint(const NbModelDesc& m, SB& S, int b0, int j, const float* tpos,
                                          const float* tvel, const NbXpbdParams& p, float dt, unsigned* bad) {
     int type = m.joint_type[j];
     if (!m.joint_enabled[j]) return;
@@ -690,7 +746,8 @@ __device__ __noinline__ void solve_joint(const NbModelDesc& m, SBodies& S, int b
 }
 
 // apply_joint_forces (kernels.py:890-1003) for the world's joints, in joint order
-__device__ void joint_forces(const NbModelDesc& m, SBodies& S, int b0, int j0, int j1, const float* joint_f) {
+template <class SB>
+__device__ void joint_forces(const NbModelDesc& m, SB& S, int b0, int j0, int j1, const float* joint_f) {
     for (int j = j0; j < j1; ++j) {
         int type = m.joint_type[j];
         if (!m.joint_enabled[j]) continue;
@@ -748,8 +805,8 @@ constexpr int kChunk = 256;
 // exactly.  nact[2] alternates between chunks so that resetting one counter
 // never races with the next chunk's appends; both are zero on entry and on
 // return (visible to the group after its next barrier).
-template <int G>
-__device__ __forceinline__ void contact_pass(const NbModelDesc& m, SBodies& S, const float4* __restrict__ R, int nc,
+template <int G, class SB>
+__device__ __forceinline__ void contact_pass(const NbModelDesc& m, SB& S, const float4* __restrict__ R, int nc,
                                              unsigned char* list, int* nact, int g, int t, float relaxation, float dt,
                                              bool weighting, unsigned* bad, float* imp_scratch) {
     int parity = 0;
@@ -773,6 +830,183 @@ __device__ __forceinline__ void contact_pass(const NbModelDesc& m, SBodies& S, c
     if (t == 0) nact[0] = nact[1] = 0;
 }
 
+// One world's substep with a group of G threads: stage, joint forces,
+// integrate, `iterations` x (contacts, weighted apply, joints, apply),
+// restitution, write-back.  The caller carved the world's slab into S.
+template <int G, class SB>
+__device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdParams& p, const NbStepIO& io,
+                                           const NbContactSeg& seg, bool has_contacts, float dt, int w, SB& S,
+                                           int g, int t, int* flag, int* nact, unsigned char* list,
+                                           unsigned* s_bad) {
+    const bool weighting = p.rigid_contact_con_weighting != 0;
+    const bool model_joints = m.joint_count > 0;
+    const float4* rec = reinterpret_cast<const float4*>(seg.rec);
+    const int b0 = S.b0;
+    const int nb = S.nb;
+    // ---- stage bodies (body_f + joint forces go to frc, aliased on acc)
+    for (int i = t; i < nb; i += G) {
+        const int bi = b0 + i;
+        const int fl = m.body_flags[bi];
+        S.flags[i] = fl;
+        const float* q = io.body_q_in + 7 * (size_t)bi;
+        const float* qd = io.body_qd_in + 6 * (size_t)bi;
+        for (int k = 0; k < 7; ++k) S.f[k * nb + i] = q[k];
+        for (int k = 0; k < 6; ++k) S.f[(7 + k) * nb + i] = qd[k];
+        const float* fb = io.body_f_in + 6 * (size_t)bi;
+        for (int k = 0; k < 6; ++k) S.frc[k * nb + i] = fb[k];
+        if constexpr (!SB::compact) {
+            const bool kin = (fl & NB_BODY_KINEMATIC) != 0;
+            for (int k = 0; k < 3; ++k) S.c[k * nb + i] = m.body_com[3 * (size_t)bi + k];
+            S.c[3 * nb + i] = kin ? 0.0f : m.body_inv_mass[bi];
+            for (int k = 0; k < 9; ++k) {
+                S.I[k * nb + i] = m.body_inertia[9 * (size_t)bi + k];
+                S.iI[k * nb + i] = kin ? 0.0f : m.body_inv_inertia[9 * (size_t)bi + k];
+            }
+        }
+        S.cnt[i] = 0;
+    }
+    const int j0 = m.world_joint_start[w], j1 = m.world_joint_start[w + 1];
+    // bit 0: the world has a non-free enabled joint (needs a real joint pass);
+    // bit 1: some joint of the world has a non-zero joint_f entry
+    if (t == 0) flag[0] = 0;
+    group_sync<G>(g);
+    for (int j = j0 + t; j < j1; j += G) {
+        if (m.joint_type[j] != NB_JOINT_FREE && m.joint_enabled[j]) atomicOr(&flag[0], 1);
+        if (io.joint_f) {
+            const int qs = m.joint_qd_start[j];
+            const int nd = m.joint_dof_dim[2 * j] + m.joint_dof_dim[2 * j + 1];
+            for (int k = 0; k < nd; ++k)
+                if (io.joint_f[qs + k] != 0.0f) atomicOr(&flag[0], 2);
+        }
+    }
+    group_sync<G>(g);
+    // apply_joint_forces adds joint_f in joint order; all-zero forces change nothing
+    if ((flag[0] & 2) && t == 0) joint_forces(m, S, b0, j0, j1, io.joint_f);
+    group_sync<G>(g);
+    const bool world_joints = (flag[0] & 1) != 0;
+    // ---- integrate_bodies (state in registers, frc read before acc is zeroed)
+    for (int i = t; i < nb; i += G) {
+        const V3 f0{S.frc[0 * nb + i], S.frc[1 * nb + i], S.frc[2 * nb + i]};
+        const V3 t0{S.frc[3 * nb + i], S.frc[4 * nb + i], S.frc[5 * nb + i]};
+        if (!(S.flags[i] & NB_BODY_KINEMATIC)) {
+            const int bi = b0 + i;
+            int wi = m.body_world[bi];
+            if (wi < 0) wi = 0;
+            V3 gv = load_v3(m.gravity + 3 * (size_t)wi);
+            TF q = S.q(i);
+            V3 v = S.v(i), wv = S.w(i);
+            integrate_rigid_body(q, v, wv, f0, t0, S.com(i), S.inertia(i), m.body_inv_mass[bi],
+                                 load_m33(m.body_inv_inertia + 9 * (size_t)bi), gv, p.angular_damping, dt);
+            S.set(i, q, v, wv);
+        }
+    }
+    group_sync<G>(g);
+    for (int i = t; i < nb; i += G)
+        for (int k = 0; k < 6; ++k) S.acc[k * nb + i] = 0ull;
+    if (t == 0) nact[0] = nact[1] = 0;
+    group_sync<G>(g);
+    const int nc = has_contacts ? seg.world_count[w] : 0;
+    const int64_t rec_base = has_contacts ? seg.world_base[w] : 0;
+    const float4* R = rec + (size_t)rec_base * 5;
+    const bool want_imp = has_contacts && io.contact_impulse != nullptr;
+    unsigned bad = 0u;
+    for (int it = 0; it < p.iterations; ++it) {
+        if (has_contacts) {
+            contact_pass<G>(m, S, R, nc, list, nact, g, t, p.rigid_contact_relaxation, dt,
+                            weighting, &bad, want_imp ? io.impulse_scratch + (size_t)rec_base * 6 : nullptr);
+            if (want_imp) {
+                accumulate_impulses<G>(S, R, nc, rec_base, seg.rec_index, io.impulse_scratch,
+                                       io.contact_impulse, io.contact_impulse_capacity, weighting, t);
+                group_sync<G>(g);
+            }
+            for (int i = t; i < nb; i += G) {
+                V3 dl, da;
+                const bool moved = S.take(i, dl, da);
+                float weight = 1.0f;
+                if (weighting) {
+                    float iw = (float)S.cnt[i];
+                    S.cnt[i] = 0;
+                    if (iw > 0.0f) weight = 1.0f / iw;
+                }
+                TF q = S.q(i);
+                V3 v = S.v(i), wv = S.w(i);
+                const V3 com = S.com(i);
+                const float im = S.inv_m(i);
+                if (moved || world_joints) {
+                    apply_body_delta(q, v, wv, dl, da, weight, com, S.inertia(i), im, S.inv_inertia(i), dt);
+                } else {
+                    // no contact touched the body: the closed form, exact up to
+                    // the sign of zeros, which no later step of a world
+                    // without real joints can tell apart
+                    apply_zero_delta(q, v, wv, com, im);
+                }
+                if (model_joints && !world_joints) {
+                    // the joint pass of this world only renormalises (free joints)
+                    apply_zero_delta(q, v, wv, com, im);
+                }
+                S.set(i, q, v, wv);
+            }
+            group_sync<G>(g);
+        }
+        if (model_joints && (world_joints || !has_contacts)) {
+            for (int j = j0 + t; j < j1; j += G)
+                solve_joint(m, S, b0, j, io.joint_target_pos, io.joint_target_vel, p, dt, &bad);
+            group_sync<G>(g);
+            for (int i = t; i < nb; i += G) {
+                V3 dl, da;
+                S.take(i, dl, da);
+                TF q = S.q(i);
+                V3 v = S.v(i), wv = S.w(i);
+                apply_body_delta(q, v, wv, dl, da, 1.0f, S.com(i), S.inertia(i), S.inv_m(i),
+                                 S.inv_inertia(i), dt);
+                S.set(i, q, v, wv);
+            }
+            group_sync<G>(g);
+        }
+    }
+    // ---- restitution (solver_xpbd.py:685-755), after all iterations
+    if (has_contacts && p.enable_restitution) {
+        for (int k = t; k < nc; k += G)
+            restitution_contact(m, S, R + (size_t)k * 5, b0, io.body_q_in, io.body_qd_in, dt, &bad);
+        group_sync<G>(g);
+        // apply_body_delta_velocities (kernels.py:881-887)
+        for (int i = t; i < nb; i += G) {
+            V3 dl, da;
+            S.take(i, dl, da);
+            const V3 v = S.v(i), wv = S.w(i);
+            S.set(i, S.q(i), add(v, dl), add(wv, da));
+        }
+        group_sync<G>(g);
+    }
+    // ---- write back (kinematic bodies pass through unchanged)
+    for (int i = t; i < nb; i += G) {
+        const int bi = b0 + i;
+        float* qo = io.body_q_out + 7 * (size_t)bi;
+        float* qdo = io.body_qd_out + 6 * (size_t)bi;
+        if (S.flags[i] & NB_BODY_KINEMATIC) {
+            for (int k = 0; k < 7; ++k) qo[k] = io.body_q_in[7 * (size_t)bi + k];
+            for (int k = 0; k < 6; ++k) qdo[k] = io.body_qd_in[6 * (size_t)bi + k];
+            continue;
+        }
+        bool finite = true;
+        for (int k = 0; k < 7; ++k) {
+            float x = S.f[k * nb + i];
+            finite = finite && isfinite(x);
+            qo[k] = x;
+        }
+        for (int k = 0; k < 6; ++k) {
+            float x = S.f[(7 + k) * nb + i];
+            finite = finite && isfinite(x);
+            qdo[k] = x;
+        }
+        if (!finite) bad |= 2u;
+    }
+    if (bad) atomicOr(s_bad, bad);
+}
+
+// Batch mode: a CTA takes a batch of worlds (host-packed into one arena, one
+// world per group of G threads) from a device counter; the CTA waits for all
+// of a batch's worlds before the next batch reuses the arena.
 template <int G>
 __global__ void __launch_bounds__(kST, 2)
 xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, int has_contacts, float dt) {
@@ -785,11 +1019,7 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
     __shared__ unsigned char s_list[kGroups][kChunk];
     const int g = threadIdx.x / G;   // group within the CTA
     const int t = threadIdx.x % G;   // thread within the group
-    const bool weighting = p.rigid_contact_con_weighting != 0;
-    const bool model_joints = m.joint_count > 0;
-    const float4* rec = reinterpret_cast<const float4*>(seg.rec);
     if (threadIdx.x == 0) s_bad = 0u;
-
     for (;;) {
         if (threadIdx.x == 0) s_batch = atomicAdd(&seg.work_counter[4], 1);
         __syncthreads();
@@ -799,167 +1029,58 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
         if (w >= 0) {
             const int b0 = m.world_body_start[w];
             const int nb = m.world_body_start[w + 1] - b0;
-            SBodies S = sbodies_carve(arena + 4 * (size_t)m.batch_slab[b * kGroups + g], nb);
-            const int j0 = m.world_joint_start[w], j1 = m.world_joint_start[w + 1];
-            // ---- stage bodies (body_f + joint forces go to frc, aliased on acc)
-            for (int i = t; i < nb; i += G) {
-                const int bi = b0 + i;
-                const int fl = m.body_flags[bi];
-                const bool kin = (fl & NB_BODY_KINEMATIC) != 0;
-                S.flags[i] = fl;
-                const float* q = io.body_q_in + 7 * (size_t)bi;
-                const float* qd = io.body_qd_in + 6 * (size_t)bi;
-                for (int k = 0; k < 7; ++k) S.f[k * nb + i] = q[k];
-                for (int k = 0; k < 6; ++k) S.f[(7 + k) * nb + i] = qd[k];
-                const float* fb = io.body_f_in + 6 * (size_t)bi;
-                for (int k = 0; k < 6; ++k) S.frc[k * nb + i] = fb[k];
-                for (int k = 0; k < 3; ++k) S.c[k * nb + i] = m.body_com[3 * (size_t)bi + k];
-                S.c[3 * nb + i] = kin ? 0.0f : m.body_inv_mass[bi];
-                for (int k = 0; k < 9; ++k) {
-                    S.I[k * nb + i] = m.body_inertia[9 * (size_t)bi + k];
-                    S.iI[k * nb + i] = kin ? 0.0f : m.body_inv_inertia[9 * (size_t)bi + k];
-                }
-                S.cnt[i] = 0;
-            }
-            // bit 0: the world has a non-free enabled joint (needs a real joint pass);
-            // bit 1: some joint of the world has a non-zero joint_f entry
-            if (t == 0) s_flag[g] = 0;
-            group_sync<G>(g);
-            for (int j = j0 + t; j < j1; j += G) {
-                if (m.joint_type[j] != NB_JOINT_FREE && m.joint_enabled[j]) atomicOr(&s_flag[g], 1);
-                if (io.joint_f) {
-                    const int qs = m.joint_qd_start[j];
-                    const int nd = m.joint_dof_dim[2 * j] + m.joint_dof_dim[2 * j + 1];
-                    for (int k = 0; k < nd; ++k)
-                        if (io.joint_f[qs + k] != 0.0f) atomicOr(&s_flag[g], 2);
-                }
-            }
-            group_sync<G>(g);
-            // apply_joint_forces adds joint_f in joint order; all-zero forces change nothing
-            if ((s_flag[g] & 2) && t == 0) joint_forces(m, S, b0, j0, j1, io.joint_f);
-            group_sync<G>(g);
-            const bool world_joints = (s_flag[g] & 1) != 0;
-            // ---- integrate_bodies (state in registers, frc read before acc is zeroed)
-            for (int i = t; i < nb; i += G) {
-                const V3 f0{S.frc[0 * nb + i], S.frc[1 * nb + i], S.frc[2 * nb + i]};
-                const V3 t0{S.frc[3 * nb + i], S.frc[4 * nb + i], S.frc[5 * nb + i]};
-                if (!(S.flags[i] & NB_BODY_KINEMATIC)) {
-                    const int bi = b0 + i;
-                    int wi = m.body_world[bi];
-                    if (wi < 0) wi = 0;
-                    V3 gv = load_v3(m.gravity + 3 * (size_t)wi);
-                    TF q = S.q(i);
-                    V3 v = S.v(i), wv = S.w(i);
-                    integrate_rigid_body(q, v, wv, f0, t0, S.com(i), S.inertia(i), m.body_inv_mass[bi],
-                                         load_m33(m.body_inv_inertia + 9 * (size_t)bi), gv, p.angular_damping, dt);
-                    S.set(i, q, v, wv);
-                }
-            }
-            group_sync<G>(g);
-            for (int i = t; i < nb; i += G)
-                for (int k = 0; k < 6; ++k) S.acc[k * nb + i] = 0ull;
-            if (t == 0) s_nact[g][0] = s_nact[g][1] = 0;
-            group_sync<G>(g);
-            const int nc = has_contacts ? seg.world_count[w] : 0;
-            const int64_t rec_base = has_contacts ? seg.world_base[w] : 0;
-            const float4* R = rec + (size_t)rec_base * 5;
-            const bool want_imp = has_contacts && io.contact_impulse != nullptr;
-            unsigned bad = 0u;
-            for (int it = 0; it < p.iterations; ++it) {
-                if (has_contacts) {
-                    contact_pass<G>(m, S, R, nc, s_list[g], s_nact[g], g, t, p.rigid_contact_relaxation, dt,
-                                    weighting, &bad, want_imp ? io.impulse_scratch + (size_t)rec_base * 6 : nullptr);
-                    if (want_imp) {
-                        accumulate_impulses<G>(S, R, nc, rec_base, seg.rec_index, io.impulse_scratch,
-                                               io.contact_impulse, io.contact_impulse_capacity, weighting, t);
-                        group_sync<G>(g);
-                    }
-                    for (int i = t; i < nb; i += G) {
-                        V3 dl, da;
-                        const bool moved = S.take(i, dl, da);
-                        float weight = 1.0f;
-                        if (weighting) {
-                            float iw = (float)S.cnt[i];
-                            S.cnt[i] = 0;
-                            if (iw > 0.0f) weight = 1.0f / iw;
-                        }
-                        TF q = S.q(i);
-                        V3 v = S.v(i), wv = S.w(i);
-                        const V3 com = S.com(i);
-                        const float im = S.inv_m(i);
-                        if (moved || world_joints) {
-                            apply_body_delta(q, v, wv, dl, da, weight, com, S.inertia(i), im, S.inv_inertia(i), dt);
-                        } else {
-                            // no contact touched the body: the closed form, exact up to
-                            // the sign of zeros, which no later step of a world
-                            // without real joints can tell apart
-                            apply_zero_delta(q, v, wv, com, im);
-                        }
-                        if (model_joints && !world_joints) {
-                            // the joint pass of this world only renormalises (free joints)
-                            apply_zero_delta(q, v, wv, com, im);
-                        }
-                        S.set(i, q, v, wv);
-                    }
-                    group_sync<G>(g);
-                }
-                if (model_joints && (world_joints || !has_contacts)) {
-                    for (int j = j0 + t; j < j1; j += G)
-                        solve_joint(m, S, b0, j, io.joint_target_pos, io.joint_target_vel, p, dt, &bad);
-                    group_sync<G>(g);
-                    for (int i = t; i < nb; i += G) {
-                        V3 dl, da;
-                        S.take(i, dl, da);
-                        TF q = S.q(i);
-                        V3 v = S.v(i), wv = S.w(i);
-                        apply_body_delta(q, v, wv, dl, da, 1.0f, S.com(i), S.inertia(i), S.inv_m(i),
-                                         S.inv_inertia(i), dt);
-                        S.set(i, q, v, wv);
-                    }
-                    group_sync<G>(g);
-                }
-            }
-            // ---- restitution (solver_xpbd.py:685-755), after all iterations
-            if (has_contacts && p.enable_restitution) {
-                for (int k = t; k < nc; k += G)
-                    restitution_contact(m, S, R + (size_t)k * 5, b0, io.body_q_in, io.body_qd_in, dt, &bad);
-                group_sync<G>(g);
-                // apply_body_delta_velocities (kernels.py:881-887)
-                for (int i = t; i < nb; i += G) {
-                    V3 dl, da;
-                    S.take(i, dl, da);
-                    const V3 v = S.v(i), wv = S.w(i);
-                    S.set(i, S.q(i), add(v, dl), add(wv, da));
-                }
-                group_sync<G>(g);
-            }
-            // ---- write back (kinematic bodies pass through unchanged)
-            for (int i = t; i < nb; i += G) {
-                const int bi = b0 + i;
-                float* qo = io.body_q_out + 7 * (size_t)bi;
-                float* qdo = io.body_qd_out + 6 * (size_t)bi;
-                if (S.flags[i] & NB_BODY_KINEMATIC) {
-                    for (int k = 0; k < 7; ++k) qo[k] = io.body_q_in[7 * (size_t)bi + k];
-                    for (int k = 0; k < 6; ++k) qdo[k] = io.body_qd_in[6 * (size_t)bi + k];
-                    continue;
-                }
-                bool finite = true;
-                for (int k = 0; k < 7; ++k) {
-                    float x = S.f[k * nb + i];
-                    finite = finite && isfinite(x);
-                    qo[k] = x;
-                }
-                for (int k = 0; k < 6; ++k) {
-                    float x = S.f[(7 + k) * nb + i];
-                    finite = finite && isfinite(x);
-                    qdo[k] = x;
-                }
-                if (!finite) bad |= 2u;
-            }
-            if (bad) atomicOr(&s_bad, bad);
+            SBodiesT<false> S = sbodies_carve<false>(arena + 4 * (size_t)m.batch_slab[b * kGroups + g], m, b0, nb);
+            step_world<G>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g], s_list[g],
+                          &s_bad);
         }
         __syncthreads();  // every group is done with the arena before the next batch
     }
+    if (threadIdx.x == 0 && s_bad) {
+        unsigned st = 0;
+        if (s_bad & 1u) st |= NB_STATUS_FIXED_OVERFLOW;
+        if (s_bad & 2u) st |= NB_STATUS_NONFINITE;
+        atomicOr(seg.status, st);
+    }
+}
+
+// Warp mode: every warp owns a fixed share of the CTA's arena and pulls whole
+// worlds (largest first) from a device counter on its own -- no CTA-wide
+// barrier, so a warp never waits for another world.  The host picks this mode
+// when the largest world's slab fits one share (kCompact stages only the
+// mutable body state).
+template <bool kCompact>
+__global__ void __launch_bounds__(kST, 2)
+xpbd_step_warp_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, int has_contacts, float dt) {
+    extern __shared__ __align__(16) unsigned char arena[];
+    constexpr int kWarps = kST / 32;
+    __shared__ unsigned s_bad;
+    __shared__ int s_flag[kWarps];
+    __shared__ int s_nact[kWarps][2];
+    __shared__ unsigned char s_list[kWarps][kChunk];
+    const int g = threadIdx.x >> 5;
+    const int t = threadIdx.x & 31;
+    if (threadIdx.x == 0) s_bad = 0u;
+    __syncthreads();
+    const int share = (m.smem_floats_per_batch / kWarps) & ~1;  // words per warp, 8-byte aligned
+    unsigned char* region = arena + 4 * (size_t)share * g;
+    for (;;) {
+        int k = 0;
+        if (t == 0) k = atomicAdd(&seg.work_counter[4], 1);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= m.world_count) break;
+        const int w = m.world_order[k];
+        const int b0 = m.world_body_start[w];
+        const int nb = m.world_body_start[w + 1] - b0;
+        if (nb * slab_words_per_body<kCompact>() > share) {  // host guarantees this never happens
+            if (t == 0) atomicOr(seg.status, (unsigned)NB_STATUS_WORLD_TOO_LARGE);
+            continue;
+        }
+        SBodiesT<kCompact> S = sbodies_carve<kCompact>(region, m, b0, nb);
+        step_world<32>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g], s_list[g],
+                       &s_bad);
+        __syncwarp();
+    }
+    __syncthreads();
     if (threadIdx.x == 0 && s_bad) {
         unsigned st = 0;
         if (s_bad & 1u) st |= NB_STATUS_FIXED_OVERFLOW;
@@ -1014,13 +1135,33 @@ cudaError_t launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbSte
     xpbd_step_kernel<G><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
     return cudaGetLastError();
 }
+
+template <bool kCompact>
+cudaError_t launch_step_warp(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
+                             const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
+    const size_t smem = nb_step_smem_bytes(m);
+    static size_t configured = 0;
+    if (smem > configured) {
+        cudaError_t e = cudaFuncSetAttribute(xpbd_step_warp_kernel<kCompact>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = smem;
+    }
+    const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
+    xpbd_step_warp_kernel<kCompact><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
+    return cudaGetLastError();
+}
 }  // namespace
+
+int nb_step_slab_words(int compact) { return compact ? slab_words_per_body<true>() : slab_words_per_body<false>(); }
 
 cudaError_t nb_launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
                            float dt, int grid, cudaStream_t stream) {
     if (m->cta_threads != kST) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(seg->work_counter + 4, 0, sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
+    if (m->step_mode == 1) return launch_step_warp<false>(m, p, io, seg, dt, grid, stream);
+    if (m->step_mode == 2) return launch_step_warp<true>(m, p, io, seg, dt, grid, stream);
     switch (m->group_threads) {
         case 32: return launch_step<32>(m, p, io, seg, dt, grid, stream);
         case 64: return launch_step<64>(m, p, io, seg, dt, grid, stream);

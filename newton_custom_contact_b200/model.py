@@ -329,6 +329,7 @@ class Model:
             d.group_threads = int(sched.group_threads)
             d.cta_threads = int(sched.cta_threads)
             d.smem_floats_per_batch = int(sched.arena_words)
+            d.step_mode = int(sched.step_mode)
             d.batch_world = ptr(arrays["batch_world"])
             d.batch_slab = ptr(arrays["batch_slab"])
         return d

@@ -1,15 +1,20 @@
 """Work schedule and autotuner for the XPBD step kernel.
 
-The step kernel runs one world per thread group of G threads (G = 32: a warp
-per world ... G = 256: a CTA per world).  A CTA holds 256 / G groups that
-share one shared-memory arena; each world gets a slab of
-``SLAB_WORDS_PER_BODY * bodies`` 4-byte words for its body state, mass
-properties and fixed-point delta accumulators.  ``build_schedule`` packs
-worlds, largest first, into batches that fit one arena, so CTAs pulling
-batches from the device counter get similar-size worlds (little idle time at
-the batch barrier) and the biggest worlds start first.
+Two ways to map worlds to the GPU:
 
-``autotune`` times the candidate group sizes on the caller's own scene and
+* warp modes (``"warp"``, ``"warp_compact"``): every warp owns one eighth of
+  its CTA's shared-memory arena and pulls whole worlds, largest first, from a
+  device counter -- no CTA-wide barrier between worlds.  ``"warp"`` stages the
+  full body slab (49 words per body), ``"warp_compact"`` only the mutable part
+  (27 words per body; mass properties are read from the model), so worlds of
+  up to 70 / 128 bodies fit a warp's share.
+* batch mode: one world per thread group of G threads (G = 32: a warp per
+  world ... G = 256: a CTA per world); a CTA holds 256 / G groups that share
+  one arena.  Worlds are packed, largest first, into batches that fit one
+  arena; CTAs pull batches from a device counter.  Used for worlds too large
+  for a warp's share.
+
+``autotune`` times the candidate schedules on the caller's own scene and
 keeps the fastest; results are cached per world-size histogram.
 """
 
@@ -20,7 +25,10 @@ import dataclasses
 import numpy as np
 
 CTA_THREADS = 256
-SLAB_WORDS_PER_BODY = 12 + 13 + 4 + 9 + 9 + 1 + 1  # must match slab_words_per_body() in nb_xpbd.cu
+WARPS_PER_CTA = CTA_THREADS // 32
+SLAB_WORDS_PER_BODY = 12 + 13 + 4 + 9 + 9 + 1 + 1  # must match slab_words_per_body<false>() in nb_xpbd.cu
+SLAB_WORDS_COMPACT = 12 + 13 + 1 + 1  # slab_words_per_body<true>()
+STEP_MODES = {"batch": 0, "warp": 1, "warp_compact": 2}
 ARENA_WORDS_TWO_CTAS = 27 * 1024  # ~108 KB: two CTAs per SM
 ARENA_WORDS_MAX = 55 * 1024       # ~220 KB: the opt-in per-CTA maximum less the kernel's static shared memory
 GROUP_SIZES = (32, 64, 128, 256)
@@ -34,6 +42,11 @@ class StepSchedule:
     batch_count: int
     batch_world: np.ndarray   # [batch_count, groups] int32, -1 = empty group
     batch_slab: np.ndarray    # [batch_count, groups] int32 word offsets
+    mode: str = "batch"
+
+    @property
+    def step_mode(self) -> int:
+        return STEP_MODES[self.mode]
 
     @property
     def groups(self) -> int:
@@ -61,10 +74,36 @@ def default_group_threads(world_count: int, sms: int | None = None) -> int:
     return GROUP_SIZES[-1]
 
 
-def build_schedule(model, group_threads: int | None = None) -> StepSchedule:
+def warp_share_words(arena_words: int = ARENA_WORDS_TWO_CTAS) -> int:
+    """Arena words one warp owns in the warp modes (8-byte aligned)."""
+    return (arena_words // WARPS_PER_CTA) & ~1
+
+
+def default_mode(max_world_bodies: int) -> str:
+    share = warp_share_words()
+    if SLAB_WORDS_PER_BODY * max_world_bodies <= share:
+        return "warp"
+    if SLAB_WORDS_COMPACT * max_world_bodies <= share:
+        return "warp_compact"
+    return "batch"
+
+
+def build_schedule(model, group_threads: int | None = None, mode: str | None = None) -> StepSchedule:
     part = model._part
     nb = np.diff(part["world_body_start"].astype(np.int64))
     W = nb.size
+    maxb = int(nb.max()) if W else 1
+    if mode is None:
+        mode = "batch" if group_threads is not None else default_mode(maxb)
+    if mode not in STEP_MODES:
+        raise ValueError(f"mode must be one of {tuple(STEP_MODES)}")
+    if mode != "batch":
+        words = SLAB_WORDS_PER_BODY if mode == "warp" else SLAB_WORDS_COMPACT
+        if words * maxb > warp_share_words():
+            raise ValueError(f"mode {mode!r}: a world with {maxb} bodies does not fit one warp's arena share")
+        return StepSchedule(group_threads=32, cta_threads=CTA_THREADS, arena_words=ARENA_WORDS_TWO_CTAS,
+                            batch_count=0, batch_world=np.full((1, WARPS_PER_CTA), -1, np.int32),
+                            batch_slab=np.zeros((1, WARPS_PER_CTA), np.int32), mode=mode)
     g = group_threads or default_group_threads(W)
     if g not in GROUP_SIZES:
         raise ValueError(f"group_threads must be one of {GROUP_SIZES}")
@@ -97,7 +136,7 @@ def build_schedule(model, group_threads: int | None = None) -> StepSchedule:
         bw[i, : len(ws)] = ws
         bo[i, : len(os_)] = os_
     return StepSchedule(group_threads=g, cta_threads=CTA_THREADS, arena_words=int(arena), batch_count=nbatch,
-                        batch_world=bw, batch_slab=bo)
+                        batch_world=bw, batch_slab=bo, mode="batch")
 
 
 def histogram_key(model, bins=(16, 32, 64, 128, 256, 512)) -> tuple:
@@ -110,23 +149,40 @@ def histogram_key(model, bins=(16, 32, 64, 128, 256, 512)) -> tuple:
 _CACHE: dict = {}
 
 
-def autotune(pipeline, solver, state_in, state_out, contacts, dt: float, candidates=GROUP_SIZES, reps: int = 3):
-    """Time one collide + step per candidate group size on this scene; keep the fastest.
+def candidate_schedules(model) -> list:
+    """(mode, group_threads) pairs that can run this model's largest world."""
+    nb = np.diff(model._part["world_body_start"].astype(np.int64))
+    maxb = int(nb.max()) if nb.size else 1
+    share = warp_share_words()
+    out = []
+    if SLAB_WORDS_PER_BODY * maxb <= share:
+        out.append(("warp", None))
+    if SLAB_WORDS_COMPACT * maxb <= share:
+        out.append(("warp_compact", None))
+    out += [("batch", g) for g in GROUP_SIZES]
+    return out
+
+
+def autotune(pipeline, solver, state_in, state_out, contacts, dt: float, candidates=None, reps: int = 3):
+    """Time the step for every candidate schedule on this scene; keep the fastest.
 
     The state is restored after every trial, so tuning does not advance the
-    simulation.  Returns {group_threads: ms}.
+    simulation.  Returns {(mode, group_threads): ms}.
     """
     import torch
 
     key = histogram_key(pipeline.model)
     if key in _CACHE:
-        pipeline.set_step_schedule(_CACHE[key])
+        mode, g = _CACHE[key]
+        pipeline.set_step_schedule(g, mode=mode)
         return {}
+    if candidates is None:
+        candidates = candidate_schedules(pipeline.model)
     q0, qd0 = state_in.body_q.clone(), state_in.body_qd.clone()
     pipeline.collide(state_in, contacts)
     times = {}
-    for g in candidates:
-        pipeline.set_step_schedule(g)
+    for mode, g in candidates:
+        pipeline.set_step_schedule(g, mode=mode)
         solver.step(state_in, state_out, None, contacts, dt)  # warm-up / attribute setup
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -135,10 +191,10 @@ def autotune(pipeline, solver, state_in, state_out, contacts, dt: float, candida
             solver.step(state_in, state_out, None, contacts, dt)
         b.record()
         torch.cuda.synchronize()
-        times[g] = a.elapsed_time(b) / reps
+        times[(mode, g)] = a.elapsed_time(b) / reps
     best = min(times, key=times.get)
     _CACHE[key] = best
-    pipeline.set_step_schedule(best)
+    pipeline.set_step_schedule(best[1], mode=best[0])
     state_in.body_q.copy_(q0)
     state_in.body_qd.copy_(qd0)
     return times

@@ -91,12 +91,12 @@ def test_collide_all_group_sizes_and_nxn(cuda, orc):
         assert np.array_equal(pa[k], pb[k]), k
 
 
-def _run_loop(model, info, substeps, orc, iterations=None, group_threads=None):
+def _run_loop(model, info, substeps, orc, iterations=None, group_threads=None, mode=None):
     """collide + step loop on the GPU (drop-in API) and on the oracle; returns both trajectories' end states."""
     it = iterations or info["iterations"]
     pipe = CollisionPipeline(model)
-    if group_threads:
-        pipe.set_step_schedule(group_threads)
+    if group_threads or mode:
+        pipe.set_step_schedule(group_threads, mode=mode)
     solver = SolverXPBD(model, iterations=it)
     s0, s1 = model.state(), model.state()
     contacts = pipe.contacts()
@@ -129,10 +129,13 @@ def test_step_parity_c1(cuda, orc, substeps):
     assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
 
 
-@pytest.mark.parametrize("substeps,group", [(1, None), (16, None), (4, 32), (4, 64), (4, 128), (4, 256)])
-def test_step_parity_c2(cuda, orc, substeps, group):
+@pytest.mark.parametrize("substeps,group,mode", [(1, None, None), (16, None, None), (4, None, "warp"),
+                                                  (4, None, "warp_compact"), (16, None, "warp_compact"),
+                                                  (4, 32, "batch"), (4, 64, "batch"), (4, 128, "batch"),
+                                                  (4, 256, "batch")])
+def test_step_parity_c2(cuda, orc, substeps, group, mode):
     model, info = _small_c2()
-    gq, gqd, q, qd = _run_loop(model, info, substeps, orc, group_threads=group)
+    gq, gqd, q, qd = _run_loop(model, info, substeps, orc, group_threads=group, mode=mode)
     np.testing.assert_allclose(gq, q, rtol=1e-5, atol=1e-6)
     assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
 

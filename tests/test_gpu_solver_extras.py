@@ -172,3 +172,30 @@ def test_step_parity_c3_arms(cuda, orc, substeps):
     assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
     # the arms are live: joint drives moved the links
     assert not np.allclose(gq[: 7], model.host("body_q")[: 7], atol=1e-7)
+
+
+@pytest.mark.parametrize("mode", ["warp_compact", "batch"])
+def test_c3_arms_all_step_modes(cuda, orc, mode):
+    """Joint worlds through the compact warp slab and the batch kernel."""
+    model, info = scenes.scene_c3(worlds=4, device="cuda")
+    pipe_mode = (None, mode) if mode != "batch" else (64, "batch")
+    pipe = CollisionPipeline(model)
+    pipe.set_step_schedule(pipe_mode[0], mode=pipe_mode[1])
+    solver = SolverXPBD(model, iterations=info["iterations"])
+    s0, s1 = model.state(), model.state()
+    contacts = pipe.contacts()
+    dt = info["dt"] / info["substeps"]
+    q = model.host("body_q").copy()
+    qd = model.host("body_qd").copy()
+    f = np.zeros((model.body_count, 6), np.float32)
+    zeros = np.zeros(model.joint_dof_count, np.float32)
+    for _ in range(4):
+        s0.clear_forces()
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, dt)
+        segs = orc.collide(model, pipe.layout, q)
+        q, qd, _ = orc.step(model, pipe.layout, solver.params(), q, qd, f, segs, dt, joint_target_pos=zeros,
+                            joint_target_vel=zeros, joint_f=zeros)
+        s0, s1 = s1, s0
+    torch.cuda.synchronize()
+    assert _bits_equal(s0.body_q.cpu().numpy(), q) and _bits_equal(s0.body_qd.cpu().numpy(), qd)
