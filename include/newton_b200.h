@@ -155,10 +155,12 @@ typedef struct NbModelDesc {
     int32_t cta_threads;               /* threads per CTA of nb_xpbd_step */
     int32_t smem_floats_per_batch;     /* shared-memory arena of one CTA, in 4-byte words */
     int32_t step_mode;                 /* 0: batches of worlds (group_threads per world, batch_* arrays);
-                                          1: one warp per world, full body slab (49 words/body);
-                                          2: one warp per world, compact slab (27 words/body, mass
+                                          1: independent groups of group_threads (32/64/128), full
+                                             body slab (49 words/body);
+                                          2: as 1 with a compact slab (27 words/body, mass
                                              properties read from the model); modes 1-2 pull worlds
-                                             in world_order and give each warp arena/8 words */
+                                             in world_order, each group owning
+                                             arena * group_threads / cta_threads words */
     const int32_t* batch_world;        /* [batch_count, cta_threads/group_threads] world ids, -1 = none */
     const int32_t* batch_slab;         /* [batch_count, cta_threads/group_threads] arena offsets (words) */
 } NbModelDesc;

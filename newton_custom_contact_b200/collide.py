@@ -279,9 +279,9 @@ class CollisionPipeline:
         c._seg_valid = False
 
     def set_step_schedule(self, group_threads: int | None = None, mode: str | None = None) -> None:
-        """Choose how the step kernel maps worlds to warps / CTAs (see schedule.py):
-        ``mode`` "warp", "warp_compact" or "batch" (with ``group_threads``); default: the
-        first warp mode the largest world fits, else batches."""
+        """Choose how the step kernel maps worlds to thread groups (see schedule.py):
+        ``mode`` "groups", "groups_compact" or "batch", with ``group_threads``; default: the
+        smallest independent group whose arena share holds the largest world, else batches."""
         from .schedule import build_schedule
 
         sched = build_schedule(self.model, group_threads, mode)

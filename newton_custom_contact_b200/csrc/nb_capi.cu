@@ -46,8 +46,10 @@ int check_schedule(const NbModelDesc* m) {
     if (m->cta_threads != NB_STEP_THREADS) return NB_ERR_INVALID;
     if (m->smem_floats_per_batch <= 0) return NB_ERR_INVALID;
     if (m->step_mode == 1 || m->step_mode == 2) {
-        // every world's slab must fit one warp's share of the arena
-        const int share = (m->smem_floats_per_batch / (NB_STEP_THREADS / 32)) & ~1;
+        // independent groups of group_threads: every world's slab must fit one group's share
+        const int g = m->group_threads;
+        if (g != 32 && g != 64 && g != 128) return NB_ERR_INVALID;
+        const int share = (m->smem_floats_per_batch / (NB_STEP_THREADS / g)) & ~1;
         if ((int64_t)m->max_world_bodies * nb_step_slab_words(m->step_mode == 2) > share) return NB_ERR_INVALID;
         return NB_OK;
     }

@@ -1043,42 +1043,52 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
     }
 }
 
-// Warp mode: every warp owns a fixed share of the CTA's arena and pulls whole
-// worlds (largest first) from a device counter on its own -- no CTA-wide
-// barrier, so a warp never waits for another world.  The host picks this mode
-// when the largest world's slab fits one share (kCompact stages only the
+// Group mode: the CTA's threads form 256 / G independent groups of G threads;
+// every group owns a fixed share of the arena and pulls whole worlds (largest
+// first) from a device counter on its own -- no CTA-wide barrier, so a group
+// never waits for another group's world.  The host picks G and the slab
+// layout so that the largest world fits one share (kCompact stages only the
 // mutable body state).
-template <bool kCompact>
+template <int G, bool kCompact>
 __global__ void __launch_bounds__(kST, 2)
-xpbd_step_warp_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, int has_contacts, float dt) {
+xpbd_step_group_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, int has_contacts, float dt) {
     extern __shared__ __align__(16) unsigned char arena[];
-    constexpr int kWarps = kST / 32;
+    constexpr int kGroups = kST / G;
     __shared__ unsigned s_bad;
-    __shared__ int s_flag[kWarps];
-    __shared__ int s_nact[kWarps][2];
-    __shared__ unsigned char s_list[kWarps][kChunk];
-    const int g = threadIdx.x >> 5;
-    const int t = threadIdx.x & 31;
+    __shared__ int s_world[kGroups];
+    __shared__ int s_flag[kGroups];
+    __shared__ int s_nact[kGroups][2];
+    __shared__ unsigned char s_list[kGroups][kChunk];
+    const int g = threadIdx.x / G;
+    const int t = threadIdx.x % G;
     if (threadIdx.x == 0) s_bad = 0u;
     __syncthreads();
-    const int share = (m.smem_floats_per_batch / kWarps) & ~1;  // words per warp, 8-byte aligned
+    const int share = (m.smem_floats_per_batch / kGroups) & ~1;  // words per group, 8-byte aligned
     unsigned char* region = arena + 4 * (size_t)share * g;
     for (;;) {
-        int k = 0;
-        if (t == 0) k = atomicAdd(&seg.work_counter[4], 1);
-        k = __shfl_sync(0xffffffffu, k, 0);
+        int k;
+        if constexpr (G == 32) {
+            k = 0;
+            if (t == 0) k = atomicAdd(&seg.work_counter[4], 1);
+            k = __shfl_sync(0xffffffffu, k, 0);
+        } else {
+            if (t == 0) s_world[g] = atomicAdd(&seg.work_counter[4], 1);
+            group_sync<G>(g);
+            k = s_world[g];
+            group_sync<G>(g);  // everyone read it before the next pull overwrites it
+        }
         if (k >= m.world_count) break;
         const int w = m.world_order[k];
         const int b0 = m.world_body_start[w];
         const int nb = m.world_body_start[w + 1] - b0;
-        if (nb * slab_words_per_body<kCompact>() > share) {  // host guarantees this never happens
+        if (nb * slab_words_per_body<kCompact>() > share) {  // the host guarantees this never happens
             if (t == 0) atomicOr(seg.status, (unsigned)NB_STATUS_WORLD_TOO_LARGE);
             continue;
         }
         SBodiesT<kCompact> S = sbodies_carve<kCompact>(region, m, b0, nb);
-        step_world<32>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g], s_list[g],
-                       &s_bad);
-        __syncwarp();
+        step_world<G>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g], s_list[g],
+                      &s_bad);
+        group_sync<G>(g);
     }
     __syncthreads();
     if (threadIdx.x == 0 && s_bad) {
@@ -1136,20 +1146,31 @@ cudaError_t launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbSte
     return cudaGetLastError();
 }
 
-template <bool kCompact>
-cudaError_t launch_step_warp(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
-                             const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
+template <int G, bool kCompact>
+cudaError_t launch_step_group(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
+                              const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
     const size_t smem = nb_step_smem_bytes(m);
     static size_t configured = 0;
     if (smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(xpbd_step_warp_kernel<kCompact>,
+        cudaError_t e = cudaFuncSetAttribute(xpbd_step_group_kernel<G, kCompact>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         configured = smem;
     }
     const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
-    xpbd_step_warp_kernel<kCompact><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
+    xpbd_step_group_kernel<G, kCompact><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
     return cudaGetLastError();
+}
+
+template <bool kCompact>
+cudaError_t launch_step_groups(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
+                               const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
+    switch (m->group_threads) {
+        case 32: return launch_step_group<32, kCompact>(m, p, io, seg, dt, grid, stream);
+        case 64: return launch_step_group<64, kCompact>(m, p, io, seg, dt, grid, stream);
+        case 128: return launch_step_group<128, kCompact>(m, p, io, seg, dt, grid, stream);
+        default: return cudaErrorInvalidValue;
+    }
 }
 }  // namespace
 
@@ -1160,8 +1181,8 @@ cudaError_t nb_launch_step(const NbModelDesc* m, const NbXpbdParams* p, const Nb
     if (m->cta_threads != kST) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(seg->work_counter + 4, 0, sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
-    if (m->step_mode == 1) return launch_step_warp<false>(m, p, io, seg, dt, grid, stream);
-    if (m->step_mode == 2) return launch_step_warp<true>(m, p, io, seg, dt, grid, stream);
+    if (m->step_mode == 1) return launch_step_groups<false>(m, p, io, seg, dt, grid, stream);
+    if (m->step_mode == 2) return launch_step_groups<true>(m, p, io, seg, dt, grid, stream);
     switch (m->group_threads) {
         case 32: return launch_step<32>(m, p, io, seg, dt, grid, stream);
         case 64: return launch_step<64>(m, p, io, seg, dt, grid, stream);

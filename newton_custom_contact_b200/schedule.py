@@ -2,12 +2,13 @@
 
 Two ways to map worlds to the GPU:
 
-* warp modes (``"warp"``, ``"warp_compact"``): every warp owns one eighth of
+* group modes (``"groups"``, ``"groups_compact"``): the CTA's threads form
+  independent groups of G = 32, 64 or 128 threads; every group owns G / 256 of
   its CTA's shared-memory arena and pulls whole worlds, largest first, from a
-  device counter -- no CTA-wide barrier between worlds.  ``"warp"`` stages the
-  full body slab (49 words per body), ``"warp_compact"`` only the mutable part
-  (27 words per body; mass properties are read from the model), so worlds of
-  up to 70 / 128 bodies fit a warp's share.
+  device counter -- no CTA-wide barrier between worlds.  ``"groups"`` stages
+  the full body slab (49 words per body), ``"groups_compact"`` only the
+  mutable part (27 words per body; mass properties are read from the model).
+  A G = 32 share holds 70 / 128 bodies, a G = 64 share 141 / 256.
 * batch mode: one world per thread group of G threads (G = 32: a warp per
   world ... G = 256: a CTA per world); a CTA holds 256 / G groups that share
   one arena.  Worlds are packed, largest first, into batches that fit one
@@ -28,7 +29,8 @@ CTA_THREADS = 256
 WARPS_PER_CTA = CTA_THREADS // 32
 SLAB_WORDS_PER_BODY = 12 + 13 + 4 + 9 + 9 + 1 + 1  # must match slab_words_per_body<false>() in nb_xpbd.cu
 SLAB_WORDS_COMPACT = 12 + 13 + 1 + 1  # slab_words_per_body<true>()
-STEP_MODES = {"batch": 0, "warp": 1, "warp_compact": 2}
+STEP_MODES = {"batch": 0, "groups": 1, "groups_compact": 2}
+GROUP_MODE_SIZES = (32, 64, 128)
 ARENA_WORDS_TWO_CTAS = 27 * 1024  # ~108 KB: two CTAs per SM
 ARENA_WORDS_MAX = 55 * 1024       # ~220 KB: the opt-in per-CTA maximum less the kernel's static shared memory
 GROUP_SIZES = (32, 64, 128, 256)
@@ -74,18 +76,20 @@ def default_group_threads(world_count: int, sms: int | None = None) -> int:
     return GROUP_SIZES[-1]
 
 
-def warp_share_words(arena_words: int = ARENA_WORDS_TWO_CTAS) -> int:
-    """Arena words one warp owns in the warp modes (8-byte aligned)."""
-    return (arena_words // WARPS_PER_CTA) & ~1
+def group_share_words(group_threads: int, arena_words: int = ARENA_WORDS_TWO_CTAS) -> int:
+    """Arena words one group owns in the group modes (8-byte aligned)."""
+    return (arena_words // (CTA_THREADS // group_threads)) & ~1
 
 
-def default_mode(max_world_bodies: int) -> str:
-    share = warp_share_words()
-    if SLAB_WORDS_PER_BODY * max_world_bodies <= share:
-        return "warp"
-    if SLAB_WORDS_COMPACT * max_world_bodies <= share:
-        return "warp_compact"
-    return "batch"
+def default_mode(max_world_bodies: int) -> tuple:
+    """(mode, group_threads): the smallest group whose share holds the largest world, with the full
+    slab if it fits, else the compact one; else batches.  (Measured on the 4096-world drop: one
+    warp per world with the compact slab beats 64-thread groups with the full slab.)"""
+    for g in GROUP_MODE_SIZES:
+        for words, mode in ((SLAB_WORDS_PER_BODY, "groups"), (SLAB_WORDS_COMPACT, "groups_compact")):
+            if words * max_world_bodies <= group_share_words(g):
+                return mode, g
+    return "batch", None
 
 
 def build_schedule(model, group_threads: int | None = None, mode: str | None = None) -> StepSchedule:
@@ -94,16 +98,23 @@ def build_schedule(model, group_threads: int | None = None, mode: str | None = N
     W = nb.size
     maxb = int(nb.max()) if W else 1
     if mode is None:
-        mode = "batch" if group_threads is not None else default_mode(maxb)
+        if group_threads is not None:
+            mode = "batch"
+        else:
+            mode, group_threads = default_mode(maxb)
     if mode not in STEP_MODES:
         raise ValueError(f"mode must be one of {tuple(STEP_MODES)}")
     if mode != "batch":
-        words = SLAB_WORDS_PER_BODY if mode == "warp" else SLAB_WORDS_COMPACT
-        if words * maxb > warp_share_words():
-            raise ValueError(f"mode {mode!r}: a world with {maxb} bodies does not fit one warp's arena share")
-        return StepSchedule(group_threads=32, cta_threads=CTA_THREADS, arena_words=ARENA_WORDS_TWO_CTAS,
-                            batch_count=0, batch_world=np.full((1, WARPS_PER_CTA), -1, np.int32),
-                            batch_slab=np.zeros((1, WARPS_PER_CTA), np.int32), mode=mode)
+        g = group_threads or 32
+        if g not in GROUP_MODE_SIZES:
+            raise ValueError(f"group modes take group_threads in {GROUP_MODE_SIZES}")
+        words = SLAB_WORDS_PER_BODY if mode == "groups" else SLAB_WORDS_COMPACT
+        if words * maxb > group_share_words(g):
+            raise ValueError(f"mode {mode!r}: a world with {maxb} bodies does not fit a {g}-thread group's share")
+        groups = CTA_THREADS // g
+        return StepSchedule(group_threads=g, cta_threads=CTA_THREADS, arena_words=ARENA_WORDS_TWO_CTAS,
+                            batch_count=0, batch_world=np.full((1, groups), -1, np.int32),
+                            batch_slab=np.zeros((1, groups), np.int32), mode=mode)
     g = group_threads or default_group_threads(W)
     if g not in GROUP_SIZES:
         raise ValueError(f"group_threads must be one of {GROUP_SIZES}")
@@ -153,12 +164,9 @@ def candidate_schedules(model) -> list:
     """(mode, group_threads) pairs that can run this model's largest world."""
     nb = np.diff(model._part["world_body_start"].astype(np.int64))
     maxb = int(nb.max()) if nb.size else 1
-    share = warp_share_words()
     out = []
-    if SLAB_WORDS_PER_BODY * maxb <= share:
-        out.append(("warp", None))
-    if SLAB_WORDS_COMPACT * maxb <= share:
-        out.append(("warp_compact", None))
+    for words, mode in ((SLAB_WORDS_PER_BODY, "groups"), (SLAB_WORDS_COMPACT, "groups_compact")):
+        out += [(mode, g) for g in GROUP_MODE_SIZES if words * maxb <= group_share_words(g)]
     out += [("batch", g) for g in GROUP_SIZES]
     return out
 

@@ -129,8 +129,9 @@ def test_step_parity_c1(cuda, orc, substeps):
     assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
 
 
-@pytest.mark.parametrize("substeps,group,mode", [(1, None, None), (16, None, None), (4, None, "warp"),
-                                                  (4, None, "warp_compact"), (16, None, "warp_compact"),
+@pytest.mark.parametrize("substeps,group,mode", [(1, None, None), (16, None, None), (4, 32, "groups"),
+                                                  (4, 32, "groups_compact"), (16, 32, "groups_compact"),
+                                                  (4, 64, "groups"), (4, 64, "groups_compact"), (4, 128, "groups"),
                                                   (4, 32, "batch"), (4, 64, "batch"), (4, 128, "batch"),
                                                   (4, 256, "batch")])
 def test_step_parity_c2(cuda, orc, substeps, group, mode):

@@ -174,13 +174,12 @@ def test_step_parity_c3_arms(cuda, orc, substeps):
     assert not np.allclose(gq[: 7], model.host("body_q")[: 7], atol=1e-7)
 
 
-@pytest.mark.parametrize("mode", ["warp_compact", "batch"])
-def test_c3_arms_all_step_modes(cuda, orc, mode):
-    """Joint worlds through the compact warp slab and the batch kernel."""
+@pytest.mark.parametrize("mode,group", [("groups_compact", 32), ("groups", 64), ("batch", 64)])
+def test_c3_arms_all_step_modes(cuda, orc, mode, group):
+    """Joint worlds through the compact slab, 64-thread groups and the batch kernel."""
     model, info = scenes.scene_c3(worlds=4, device="cuda")
-    pipe_mode = (None, mode) if mode != "batch" else (64, "batch")
     pipe = CollisionPipeline(model)
-    pipe.set_step_schedule(pipe_mode[0], mode=pipe_mode[1])
+    pipe.set_step_schedule(group, mode=mode)
     solver = SolverXPBD(model, iterations=info["iterations"])
     s0, s1 = model.state(), model.state()
     contacts = pipe.contacts()
