@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="weak: every rank simulates its own --worlds scene; strong: the ranks split one scene")
     return ap.parse_args()
 
 
@@ -197,7 +199,13 @@ def run_ours(args, rank, world_size, local_rank):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    model, info = scenes.scene_c2(seed=args.seed + 1000 * rank, worlds=args.worlds, device=dev)
+    from newton_custom_contact_b200.distributed import max_over_ranks, shard_range
+
+    if args.scaling == "strong" and world_size > 1:
+        lo, hi = shard_range(rank, world_size, scenes.c2_world_body_counts(args.seed, args.worlds))
+        model, info = scenes.scene_c2(seed=args.seed, worlds=args.worlds, device=dev, world_range=(lo, hi))
+    else:
+        model, info = scenes.scene_c2(seed=args.seed + 1000 * rank, worlds=args.worlds, device=dev)
     substeps, iters = info["substeps"], info["iterations"]
     dt = info["dt"] / substeps
     pipe = CollisionPipeline(model)
@@ -298,12 +306,16 @@ def run_ours(args, rank, world_size, local_rank):
                 ends[k].record(stream)
         torch.cuda.synchronize()
     ms = sum(starts[k].elapsed_time(ends[k]) for k in range(args.steps))
+    # run metrics at the end of the timed steps (max over ranks)
+    from newton_custom_contact_b200.metrics import max_joint_violation, max_penetration
+
+    pipe.collide(s0, contacts)
+    pen, jv = max_penetration(model, contacts, s0.body_q), max_joint_violation(model, s0.body_q)
+    ms = max_over_ranks(ms, device=dev)
+    pen, jv = max_over_ranks([pen, jv], device=dev)
     if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    units = args.worlds * substeps * args.steps * world_size
+    units = args.worlds * substeps * args.steps * (world_size if args.scaling == "weak" else 1)
     value = units / (ms / 1e3)
     # e2e through the public API with host buffers: the host owns the state
     # between steps; each step uploads body_q / body_qd from pinned memory,
@@ -328,11 +340,7 @@ def run_ours(args, rank, world_size, local_rank):
             hqd.copy_(s0.body_qd, non_blocking=True)
             e_e[k].record(stream)
     torch.cuda.synchronize()
-    e2e_ms = sum(e_s[k].elapsed_time(e_e[k]) for k in range(args.steps))
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(sum(e_s[k].elapsed_time(e_e[k]) for k in range(args.steps)), device=dev)
     e2e_value = units / (e2e_ms / 1e3)
     status = pipe.status(contacts)
     q = s0.body_q
@@ -367,9 +375,9 @@ def run_ours(args, rank, world_size, local_rank):
     launches_per_frame = substeps * 7
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": args.scaling,
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
-        "config": {"workload": WORKLOAD, "worlds_per_gpu": args.worlds, "bodies_per_gpu": model.body_count,
+        "config": {"workload": WORKLOAD, "worlds_per_gpu": model.world_count, "bodies_per_gpu": model.body_count,
                    "substeps": substeps, "iterations": iters, "form": "plain XPBD",
                    "l2": "256 MiB buffer written between timed steps", "cuda_graph": True,
                    "frames": f"{WINDOW_START}..{WINDOW_START + WINDOW_FRAMES - 1} of the drop, cycled",
@@ -385,6 +393,7 @@ def run_ours(args, rank, world_size, local_rank):
         "gpu_launches": launches_per_frame * args.steps,
         "clocks": clk.summary(),
         "status_bits": status, "final_state_finite": finite,
+        "max_penetration_m": pen, "max_joint_violation_m": jv,
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu

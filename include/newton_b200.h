@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 4
+#define NB_ABI_VERSION 5
 
 enum {
     NB_OK = 0,
@@ -236,6 +236,9 @@ typedef struct NbStepIO {
                                     left zero-filled on return */
     int32_t contact_impulse_capacity; /* rows of contact_impulse (rigid_contact_max) */
     int32_t pad0;
+    float* body_parent_f;        /* [B,6] incoming joint wrench per body (State.body_parent_f) or NULL */
+    float* joint_impulse;        /* [J,6] zero-filled scratch, required with body_parent_f; left
+                                    zero-filled on return */
 } NbStepIO;
 
 /* ABI version of the loaded library (NB_ABI_VERSION). */

@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 4
+NB_ABI_VERSION = 5
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -207,6 +207,8 @@ class NbStepIO(C.Structure):
         ("impulse_scratch", _fp),
         ("contact_impulse_capacity", C.c_int32),
         ("pad0", C.c_int32),
+        ("body_parent_f", _fp),
+        ("joint_impulse", _fp),
     ]
 
 

@@ -255,6 +255,7 @@ class ModelBuilder:
         self.articulation_start: list[int] = []
         self.num_rigid_contacts_per_world: int | None = None
         self._requested_contact_attributes: set[str] = set()
+        self._requested_state_attributes: set[str] = set()
 
     # ------------------------------------------------------------------ counts
     @property
@@ -599,6 +600,12 @@ class ModelBuilder:
     def add_ground_plane(self, height: float = 0.0, cfg=None, label=None) -> int:
         return self.add_shape_plane(plane=(*self.up_vector, -height), width=0.0, length=0.0, cfg=cfg,
                                     label=label or "ground_plane")
+
+    def request_state_attributes(self, *attributes: str) -> None:
+        bad = sorted(set(attributes) - {"body_parent_f"})
+        if bad:
+            raise ValueError(f"Unknown state attribute(s): {', '.join(bad)}. Allowed: body_parent_f.")
+        self._requested_state_attributes.update(attributes)
 
     def request_contact_attributes(self, *attributes: str) -> None:
         allowed = {"force"}

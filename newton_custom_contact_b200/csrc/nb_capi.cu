@@ -122,6 +122,7 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
     if (params->iterations < 0) return NB_ERR_INVALID;
     if (!(dt > 0.0f)) return NB_ERR_INVALID;
     if (io->contact_impulse && (!io->impulse_scratch || io->contact_impulse_capacity < 0)) return NB_ERR_INVALID;
+    if (io->body_parent_f && model->joint_count > 0 && !io->joint_impulse) return NB_ERR_INVALID;
     if (params->enable_restitution && seg->rec && !model->shape_restitution) return NB_ERR_INVALID;
     if (model->body_count > 0 && (!io->body_q_in || !io->body_qd_in || !io->body_f_in || !io->body_q_out ||
                                   !io->body_qd_out))

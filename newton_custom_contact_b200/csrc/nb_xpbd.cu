@@ -568,9 +568,12 @@ __device__ void joint_axes(const NbModelDesc& m, int start, int count, const flo
 }
 
 // solve_body_joints for one joint (kernels.py:1441-1942)
+// imp (optional) accumulates the child-side spatial delta (joint_impulse,
+// kernels.py:1941-1942); only this thread touches joint j's row.
 template <class SB>
 __device__ __noinline__ void solve_joint(const NbModelDesc& m, SB& S, int b0, int j, const float* tpos,
-                                         const float* tvel, const NbXpbdParams& p, float dt, unsigned* bad) {
+                                         const float* tvel, const NbXpbdParams& p, float dt, unsigned* bad,
+                                         float* imp) {
     int type = m.joint_type[j];
     if (!m.joint_enabled[j]) return;
     if (type == NB_JOINT_FREE) return;
@@ -743,6 +746,11 @@ __device__ __noinline__ void solve_joint(const NbModelDesc& m, SB& S, int b0, in
     }
     if (id_p >= 0) S.add_delta(lp, ldp, adp, bad);
     if (id_c >= 0) S.add_delta(lc, ldc, adc, bad);
+    if (imp) {
+        float* r = imp + 6 * (size_t)j;
+        r[0] = r[0] + ldc.x; r[1] = r[1] + ldc.y; r[2] = r[2] + ldc.z;
+        r[3] = r[3] + adc.x; r[4] = r[4] + adc.y; r[5] = r[5] + adc.z;
+    }
 }
 
 // apply_joint_forces (kernels.py:890-1003) for the world's joints, in joint order
@@ -950,7 +958,8 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
         }
         if (model_joints && (world_joints || !has_contacts)) {
             for (int j = j0 + t; j < j1; j += G)
-                solve_joint(m, S, b0, j, io.joint_target_pos, io.joint_target_vel, p, dt, &bad);
+                solve_joint(m, S, b0, j, io.joint_target_pos, io.joint_target_vel, p, dt, &bad,
+                            io.body_parent_f ? io.joint_impulse : nullptr);
             group_sync<G>(g);
             for (int i = t; i < nb; i += G) {
                 V3 dl, da;
@@ -975,6 +984,23 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
             S.take(i, dl, da);
             const V3 v = S.v(i), wv = S.w(i);
             S.set(i, S.q(i), add(v, dl), add(wv, da));
+        }
+        group_sync<G>(g);
+    }
+    // ---- body_parent_f (solver_xpbd.py:636-655, convert_joint_impulse_to_parent_f,
+    // kernels.py:2396-2436): zero for every body of the world, then the
+    // child-side impulse / dt of each enabled non-free joint
+    if (io.body_parent_f) {
+        for (int i = t; i < nb; i += G)
+            for (int k = 0; k < 6; ++k) io.body_parent_f[6 * (size_t)(b0 + i) + k] = 0.0f;
+        group_sync<G>(g);
+        const float inv_dt = 1.0f / dt;
+        for (int j = j0 + t; j < j1; j += G) {
+            float* r = io.joint_impulse + 6 * (size_t)j;
+            const int c = m.joint_child[j];
+            if (m.joint_enabled[j] && m.joint_type[j] != NB_JOINT_FREE && c >= 0)
+                for (int k = 0; k < 6; ++k) io.body_parent_f[6 * (size_t)c + k] = r[k] * inv_dt;
+            for (int k = 0; k < 6; ++k) r[k] = 0.0f;
         }
         group_sync<G>(g);
     }

@@ -79,6 +79,7 @@ class Model:
         self.particle_count = 0
         self._collision_pipeline = None
         self._requested_contact_attributes: set[str] = set()
+        self._requested_state_attributes: set[str] = set()
         self._host: dict[str, np.ndarray] = {}
 
     # ------------------------------------------------------------ construction
@@ -140,6 +141,7 @@ class Model:
         m._init_from_host(h, world_count=W, uses_worlds=b.world_count > 0,
                           filter_pairs=set(b.shape_collision_filter_pairs),
                           requested=set(b._requested_contact_attributes))
+        m._requested_state_attributes = set(b._requested_state_attributes)
         return m
 
     @classmethod
@@ -233,11 +235,20 @@ class Model:
         self.max_world_shapes = int(cnts.max() if cnts.size else 0) + int(glob.size)
 
     # ------------------------------------------------------------ factories
+    def request_state_attributes(self, *attributes: str) -> None:
+        """Optional State arrays (model.py request_state_attributes); "body_parent_f" only."""
+        bad = sorted(set(attributes) - {"body_parent_f"})
+        if bad:
+            raise ValueError(f"Unknown state attribute(s): {', '.join(bad)}. Allowed: body_parent_f.")
+        self._requested_state_attributes.update(attributes)
+
     def state(self, requires_grad: bool | None = None) -> State:
         s = State()
         s.body_q = self.body_q.clone()
         s.body_qd = self.body_qd.clone()
         s.body_f = torch.zeros((self.body_count, 6), dtype=torch.float32, device=self.device)
+        if "body_parent_f" in self._requested_state_attributes:
+            s.body_parent_f = torch.zeros((self.body_count, 6), dtype=torch.float32, device=self.device)
         s.requires_grad = bool(requires_grad) if requires_grad is not None else self.requires_grad
         return s
 

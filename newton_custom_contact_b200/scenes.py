@@ -182,18 +182,28 @@ def _bounding_radius(t, s):
     return float(s[0] + s[1])
 
 
+def _c2_counts(rng, worlds, nmin, nmax):
+    return rng.integers(nmin, nmax + 1, size=worlds)
+
+
+def c2_world_body_counts(seed: int = 1, worlds: int = 4096, nmin: int = 8, nmax: int = 128) -> np.ndarray:
+    """Bodies per world of scene_c2(seed, worlds, nmin, nmax) without building it (for sharding)."""
+    return _c2_counts(np.random.default_rng(seed), worlds, nmin, nmax)
+
+
 def scene_c2(seed: int = 1, worlds: int = 4096, nmin: int = 8, nmax: int = 128, device=None,
-             keep_worlds: int | None = None):
+             keep_worlds: int | None = None, world_range: tuple[int, int] | None = None):
     """Uneven worlds of box / sphere / capsule bodies.  Returns (model, info).
 
     Body i of every world is placed in the same vectorised round: up to 64
     uniform draws in the 1 x 1 x 2 m column, accepting the first that keeps
     bounding spheres apart; otherwise it is raised above the world's bodies.
-    ``keep_worlds`` keeps only the first worlds of the generated scene (the
-    same bodies and poses as in the full scene), e.g. for a CPU sample.
+    ``keep_worlds`` keeps only the first worlds of the generated scene and
+    ``world_range = (a, b)`` worlds a..b-1 (the same bodies and poses as in the
+    full scene), e.g. for a CPU sample or one rank's shard.
     """
     rng = np.random.default_rng(seed)
-    counts = rng.integers(nmin, nmax + 1, size=worlds)
+    counts = _c2_counts(rng, worlds, nmin, nmax)
     kinds = np.array([int(GeoType.BOX), int(GeoType.SPHERE), int(GeoType.CAPSULE)])
     nmax_w = int(counts.max())
     types = kinds[rng.integers(0, 3, size=(worlds, nmax_w))]
@@ -238,12 +248,19 @@ def scene_c2(seed: int = 1, worlds: int = 4096, nmin: int = 8, nmax: int = 128, 
     quats = random_quats(rng, worlds * nmax_w).reshape(worlds, nmax_w, 4)
     mu_w = rng.uniform(0.3, 1.0, size=worlds)
     mask = np.arange(nmax_w)[None, :] < counts[:, None]
+    lo, hi = 0, worlds
     if keep_worlds is not None:
         if not 0 < keep_worlds <= worlds:
             raise ValueError("keep_worlds must be in [1, worlds]")
-        mask &= (np.arange(worlds) < keep_worlds)[:, None]
-        worlds = keep_worlds
-    bw = np.broadcast_to(np.arange(mask.shape[0])[:, None], mask.shape)[mask]
+        hi = keep_worlds
+    if world_range is not None:
+        lo, hi = int(world_range[0]), int(world_range[1])
+        if not 0 <= lo < hi <= worlds:
+            raise ValueError("world_range must satisfy 0 <= a < b <= worlds")
+    wid = np.arange(worlds)
+    mask &= ((wid >= lo) & (wid < hi))[:, None]
+    worlds = hi - lo
+    bw = np.broadcast_to((wid - lo)[:, None], mask.shape)[mask]
     poses = np.concatenate([pos, quats], axis=2)[mask]
     mu = np.broadcast_to(mu_w[:, None], mask.shape)[mask]
     model = assemble_free_bodies(bw, types[mask], scales[mask], poses, mu, worlds, plane_mu=0.5, device=device)

@@ -63,6 +63,7 @@ class SolverXPBD:
         self._last_dt = None
         self._contact_impulse = None
         self._contact_impulse_capacity = 0
+        self._joint_impulse = None
 
     @property
     def device(self):
@@ -139,6 +140,15 @@ class SolverXPBD:
         io.joint_target_pos = ptr(control.joint_target_pos)
         io.joint_target_vel = ptr(control.joint_target_vel)
         io.joint_f = ptr(control.joint_f)
+        if state_out.body_parent_f is not None:
+            # incoming joint wrench per body (solver_xpbd.py:294-297, 636-655)
+            self._check_state("state_out.body_parent_f", state_out.body_parent_f, (B, 6))
+            io.body_parent_f = ptr(state_out.body_parent_f)
+            if model.joint_count > 0:
+                if self._joint_impulse is None or self._joint_impulse.device != model.device:
+                    self._joint_impulse = torch.zeros((model.joint_count, 6), dtype=torch.float32,
+                                                      device=model.device)
+                io.joint_impulse = ptr(self._joint_impulse)
         impulse = None
         if contacts is not None and contacts.force is not None:
             # solver-owned accumulated impulse (solver_xpbd.py:286-291), zeroed every step

@@ -120,9 +120,10 @@ def collide(model, layout, body_q: np.ndarray) -> HostSegments:
 
 def step(model, layout, params, body_q, body_qd, body_f, segs: HostSegments | None, dt: float,
          joint_target_pos=None, joint_target_vel=None, joint_f=None, acc_mode: int = ACC_FIXED,
-         want_impulse: bool = False):
-    """One SolverXPBD.step on the CPU.  Returns (body_q_out, body_qd_out, status), plus the
-    accumulated weighted contact impulse [slot, 6] (indexed like ``segs``) when ``want_impulse``."""
+         want_impulse: bool = False, want_parent_f: bool = False):
+    """One SolverXPBD.step on the CPU.  Returns (body_q_out, body_qd_out, status), then the
+    accumulated weighted contact impulse [slot, 6] (indexed like ``segs``) when ``want_impulse``,
+    then body_parent_f [B, 6] when ``want_parent_f``."""
     from newton_custom_contact_b200._abi import NbStepIO
 
     lib = load()
@@ -143,6 +144,10 @@ def step(model, layout, params, body_q, body_qd, body_f, segs: HostSegments | No
             a = _f32(arr)
             keep.append(a)
             setattr(io, name, a.ctypes.data)
+    parent_f = None
+    if want_parent_f:
+        parent_f = np.full((q_in.shape[0], 6), np.nan, np.float32)
+        io.body_parent_f = parent_f.ctypes.data
     imp = None
     if want_impulse:
         imp = np.zeros((segs.rec[0].shape[0] if segs is not None else 1, 6), np.float32)
@@ -153,9 +158,12 @@ def step(model, layout, params, body_q, body_qd, body_f, segs: HostSegments | No
                       C.addressof(st) if st is not None else None, float(dt), int(acc_mode), C.byref(status))
     if rc != 0:
         raise RuntimeError(f"orc_step failed ({rc})")
+    out = [q_out, qd_out, int(status.value)]
     if want_impulse:
-        return q_out, qd_out, int(status.value), imp
-    return q_out, qd_out, int(status.value)
+        out.append(imp)
+    if want_parent_f:
+        out.append(parent_f)
+    return tuple(out)
 
 
 def contacts_table(model, layout, segs: HostSegments) -> np.ndarray:

@@ -359,7 +359,7 @@ static void joint_axes(const NbModelDesc* m, int start, int count, const float* 
 
 // solve_body_joints for one joint (kernels.py:1441-1942).
 static void solve_joint(World& W, int j, const float* tpos, const float* tvel, const NbXpbdParams* p, float dt,
-                        Acc& acc) {
+                        Acc& acc, float* imp = nullptr) {
     const NbModelDesc* m = W.m;
     int type = m->joint_type[j];
     if (!m->joint_enabled[j]) return;
@@ -535,6 +535,11 @@ static void solve_joint(World& W, int j, const float* tpos, const float* tvel, c
     }
     if (id_p >= 0) acc.add(lp, ldp, adp);
     if (id_c >= 0) acc.add(lc, ldc, adc);
+    if (imp) {  // joint_impulse row of joint j (kernels.py:1941-1942)
+        float* r = imp;
+        r[0] = r[0] + ldc.x; r[1] = r[1] + ldc.y; r[2] = r[2] + ldc.z;
+        r[3] = r[3] + adc.x; r[4] = r[4] + adc.y; r[5] = r[5] + adc.z;
+    }
 }
 
 // apply_joint_forces (kernels.py:890-1003), sequential in joint order.
@@ -729,6 +734,7 @@ int orc_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, co
             nc = seg->world_count[w];
         }
         int j0 = m->world_joint_start[w], j1 = m->world_joint_start[w + 1];
+        std::vector<float> jimp(io->body_parent_f ? 6 * (size_t)(j1 - j0) : 0, 0.0f);
         for (int it = 0; it < p->iterations; ++it) {
             if (seg) {
                 acc.reset(W.nb);
@@ -786,7 +792,9 @@ int orc_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, co
             }
             if (m->joint_count > 0) {
                 acc.reset(W.nb);
-                for (int j = j0; j < j1; ++j) solve_joint(W, j, io->joint_target_pos, io->joint_target_vel, p, dt, acc);
+                for (int j = j0; j < j1; ++j)
+                    solve_joint(W, j, io->joint_target_pos, io->joint_target_vel, p, dt, acc,
+                                io->body_parent_f ? jimp.data() + 6 * (size_t)(j - j0) : nullptr);
                 for (int i = 0; i < W.nb; ++i) {
                     V3 dl, da;
                     acc.get(i, dl, da);
@@ -804,6 +812,18 @@ int orc_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, co
                 acc.get(i, dl, da);
                 W.st[i].v = add(W.st[i].v, dl);
                 W.st[i].w = add(W.st[i].w, da);
+            }
+        }
+        if (io->body_parent_f) {
+            // solver_xpbd.py:636-655 with convert_joint_impulse_to_parent_f (kernels.py:2396-2436)
+            for (int i = 0; i < W.nb; ++i)
+                for (int k = 0; k < 6; ++k) io->body_parent_f[6 * (size_t)(W.b0 + i) + k] = 0.0f;
+            const float inv_dt = 1.0f / dt;
+            for (int j = j0; j < j1; ++j) {
+                const int c = m->joint_child[j];
+                if (!m->joint_enabled[j] || m->joint_type[j] == NB_JOINT_FREE || c < 0) continue;
+                for (int k = 0; k < 6; ++k)
+                    io->body_parent_f[6 * (size_t)c + k] = jimp[6 * (size_t)(j - j0) + k] * inv_dt;
             }
         }
         for (int i = 0; i < W.nb; ++i) {

@@ -198,3 +198,32 @@ def test_c3_arms_all_step_modes(cuda, orc, mode, group):
         s0, s1 = s1, s0
     torch.cuda.synchronize()
     assert _bits_equal(s0.body_q.cpu().numpy(), q) and _bits_equal(s0.body_qd.cpu().numpy(), qd)
+
+
+def test_body_parent_f_parity_c3(cuda, orc):
+    """State.body_parent_f (joint reaction per child body) equals the oracle's, bit for bit,
+    on the articulated scene; unrequested it stays None."""
+    model, info = scenes.scene_c3(worlds=4, device="cuda")
+    assert model.state().body_parent_f is None
+    model.request_state_attributes("body_parent_f")
+    pipe = CollisionPipeline(model)
+    solver = SolverXPBD(model, iterations=info["iterations"])
+    s0, s1 = model.state(), model.state()
+    contacts = pipe.contacts()
+    dt = info["dt"] / info["substeps"]
+    q, qd = model.host("body_q").copy(), model.host("body_qd").copy()
+    f = np.zeros((model.body_count, 6), np.float32)
+    zeros = np.zeros(model.joint_dof_count, np.float32)
+    for _ in range(4):
+        s0.clear_forces()
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, dt)
+        segs = orc.collide(model, pipe.layout, q)
+        q, qd, _, pf = orc.step(model, pipe.layout, solver.params(), q, qd, f, segs, dt, joint_target_pos=zeros,
+                                joint_target_vel=zeros, joint_f=zeros, want_parent_f=True)
+        torch.cuda.synchronize()
+        got = s1.body_parent_f.cpu().numpy()
+        assert _bits_equal(got, pf)
+        s0, s1 = s1, s0
+    rev = model.host("joint_child")[model.host("joint_type") == int(JointType.REVOLUTE)]
+    assert np.abs(pf[rev]).sum() > 0 and np.all(np.delete(pf, rev, axis=0) == 0.0)

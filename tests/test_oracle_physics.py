@@ -186,3 +186,84 @@ def test_shared_asin_acos_accuracy(orc):
         ulp = np.spacing(np.abs(exact).astype(np.float32)).astype(np.float64)
         assert (np.abs(got.astype(np.float64) - exact) / ulp).max() <= 2.0
     assert lib.orc_asin(1.0) == np.float32(np.pi / 2) and lib.orc_acos(1.0) == 0.0
+
+
+# ---- body_parent_f: newton/tests/test_solver_xpbd.py:752-1016 (single-body pendulums to world /
+# kinematic parent with revolute, ball and fixed joints; a two-link chain; free body).  Bodies start
+# at the pose the reference's eval_fk gives them (child 1 m below the anchor).
+
+def _pendulum(kind, parent_kinematic, gravity=9.81):
+    b = ModelBuilder(gravity=-gravity)
+    b.request_state_attributes("body_parent_f")
+    ident = (0.0, 0.0, 0.0, 1.0)
+    parent = -1
+    if parent_kinematic:
+        parent = b.add_body(xform=((0.0, 0.0, 0.0), ident), is_kinematic=True)
+        b.add_shape_box(parent, hx=0.05, hy=0.05, hz=0.05)
+    child = b.add_link(xform=((0.0, 0.0, -1.0), ident))
+    b.add_shape_box(child, hx=0.1, hy=0.1, hz=0.1)
+    pxf, cxf = ((0.0, 0.0, 0.0), ident), ((0.0, 0.0, 1.0), ident)
+    if kind == "revolute":
+        b.add_joint_revolute(parent, child, parent_xform=pxf, child_xform=cxf, axis=(0.0, 1.0, 0.0))
+    elif kind == "ball":
+        b.add_joint_ball(parent, child, parent_xform=pxf, child_xform=cxf)
+    else:
+        b.add_joint_fixed(parent, child, parent_xform=pxf, child_xform=cxf)
+    return b.finalize(device="cpu"), child
+
+
+def _parent_f_average(orc, model, iterations, settle, avg, dt=1.0 / 60.0 / 8):
+    lay = PairLayout(model, model.host("shape_contact_pairs"))
+    p = SolverXPBD(model, iterations=iterations).params()
+    q, qd = model.host("body_q").copy(), model.host("body_qd").copy()
+    f = np.zeros((model.body_count, 6), np.float32)
+    jt = model.host("joint_target_pos")
+    acc = np.zeros((model.body_count, 6))
+    for frame in range(settle + avg):
+        for _ in range(8):
+            q, qd, _, pf = orc.step(model, lay, p, q, qd, f, None, dt, joint_target_pos=jt,
+                                    joint_target_vel=np.zeros_like(jt), joint_f=np.zeros_like(jt),
+                                    want_parent_f=True)
+        if frame >= settle:
+            acc += pf
+    return acc / avg
+
+
+@pytest.mark.parametrize("kind", ["revolute", "ball", "fixed"])
+@pytest.mark.parametrize("parent_kinematic", [False, True])
+def test_oracle_parent_force_single_pendulum(orc, kind, parent_kinematic):
+    model, child = _pendulum(kind, parent_kinematic)
+    pf = _parent_f_average(orc, model, iterations=8, settle=60, avg=30)[child]
+    weight = float(model.host("body_mass")[child]) * 9.81
+    np.testing.assert_allclose(pf[2], weight, rtol=0.01)
+    np.testing.assert_allclose(pf[:2], 0.0, atol=0.1)
+    np.testing.assert_allclose(pf[3:6], 0.0, atol=0.1)
+
+
+def test_oracle_parent_force_chain_weight_propagation(orc):
+    b = ModelBuilder(gravity=-9.81)
+    b.request_state_attributes("body_parent_f")
+    ident = (0.0, 0.0, 0.0, 1.0)
+    l0 = b.add_link(xform=((0.0, 0.0, -1.0), ident))
+    b.add_shape_box(l0, hx=0.1, hy=0.1, hz=0.1)
+    b.add_joint_revolute(-1, l0, parent_xform=((0.0, 0.0, 0.0), ident), child_xform=((0.0, 0.0, 1.0), ident),
+                         axis=(0.0, 1.0, 0.0))
+    l1 = b.add_link(xform=((0.0, 0.0, -3.0), ident))
+    b.add_shape_box(l1, hx=0.1, hy=0.1, hz=0.1)
+    b.add_joint_revolute(l0, l1, parent_xform=((0.0, 0.0, -1.0), ident), child_xform=((0.0, 0.0, 1.0), ident),
+                         axis=(0.0, 1.0, 0.0))
+    model = b.finalize(device="cpu")
+    pf = _parent_f_average(orc, model, iterations=32, settle=120, avg=60)
+    m = model.host("body_mass")
+    np.testing.assert_allclose(pf[0, 2], float(m[0] + m[1]) * 9.81, rtol=0.10)
+    np.testing.assert_allclose(pf[1, 2], float(m[1]) * 9.81, rtol=0.10)
+
+
+def test_oracle_parent_force_zero_for_free_body(orc):
+    b = ModelBuilder()
+    b.request_state_attributes("body_parent_f")
+    body = b.add_body(xform=((0.0, 0.0, 0.0), (0.0, 0.0, 0.0, 1.0)))
+    b.add_shape_sphere(body, radius=0.1)
+    model = b.finalize(device="cpu")
+    pf = _parent_f_average(orc, model, iterations=2, settle=0, avg=1)
+    np.testing.assert_allclose(pf[0], 0.0, atol=1e-6)
