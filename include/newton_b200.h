@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 5
+#define NB_ABI_VERSION 6
 
 enum {
     NB_OK = 0,
@@ -206,6 +206,33 @@ typedef struct NbContactsPublic {
     int64_t* world_offset;       /* [W+1] scratch for the world scan */
 } NbContactsPublic;
 
+/* Frame-to-frame contact matching state (CollisionPipeline contact_matching,
+ * newton/_src/geometry/contact_match.py).  All arrays are device memory owned
+ * by the caller and persist between calls; prev_count must start at 0. */
+typedef struct NbMatchState {
+    int32_t capacity;            /* rigid_contact_max (rows of every per-contact array) */
+    int32_t sticky;              /* 0: "latest", 1: "sticky" (replay matched rows) */
+    float pos_threshold_sq;      /* contact_matching_pos_threshold^2 [m^2] */
+    float normal_dot_threshold;  /* contact_matching_normal_dot_threshold */
+    int32_t* prev_count;         /* [1] contacts saved from the previous call */
+    int64_t* prev_world_offset;  /* [W+1] the previous call's per-world public offsets */
+    int64_t* prev_keys;          /* [cap] previous sort keys */
+    float* prev_mid;             /* [cap,3] previous world-space contact midpoints */
+    float* prev_normal;          /* [cap,3] previous normals */
+    int64_t* prev_claim;         /* [cap] scratch */
+    int32_t* prev_was_matched;   /* [cap] scratch, required with new_indices, else NULL */
+    float* prev_point0;          /* [cap,3] sticky only (else NULL): body-frame point0 */
+    float* prev_point1;          /* [cap,3] */
+    float* prev_offset0;         /* [cap,3] */
+    float* prev_offset1;         /* [cap,3] */
+    float* prev_normal_sticky;   /* [cap,3] */
+    int32_t* match_index;        /* [cap] out: previous index, -1 not found, -2 broken */
+    int32_t* new_indices;        /* [cap] out (contact_report) or NULL */
+    int32_t* new_count;          /* [1] */
+    int32_t* broken_indices;     /* [cap] out: previous indices nobody matched */
+    int32_t* broken_count;       /* [1] */
+} NbMatchState;
+
 /* SolverXPBD constructor arguments (newton/_src/solvers/xpbd/solver_xpbd.py:95-109). */
 typedef struct NbXpbdParams {
     int32_t iterations;
@@ -276,6 +303,18 @@ int nb_publish_contacts(const NbModelDesc* model, const NbContactSeg* seg,
  */
 int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbStepIO* io,
                  const NbContactSeg* seg, float dt, int32_t grid_ctas, void* stream);
+
+/*
+ * Match the contacts nb_publish_contacts just wrote (with sort keys) against
+ * the previous call's, then (sticky) replay matched rows, build the report and
+ * save this frame for the next call.  Replaces ContactMatcher.match /
+ * replay_matched / build_report / save_sorted_state
+ * (newton/_src/geometry/contact_match.py:720-990) as called from
+ * CollisionPipeline.collide (collide.py:1083-1182).  body_q: the poses the
+ * contacts were generated at.
+ */
+int nb_match_contacts(const NbModelDesc* model, const float* body_q, const NbContactsPublic* pub,
+                      const NbContactSeg* seg, const NbMatchState* state, void* stream);
 
 /*
  * contacts.force from the impulses a step accumulated: force = impulse / dt for

@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 5
+NB_ABI_VERSION = 6
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -156,6 +156,32 @@ class NbContactSeg(C.Structure):
         ("work_counter", _fp),
         ("status", _fp),
         ("rec_index", _fp),
+    ]
+
+
+class NbMatchState(C.Structure):
+    _fields_ = [
+        ("capacity", C.c_int32),
+        ("sticky", C.c_int32),
+        ("pos_threshold_sq", C.c_float),
+        ("normal_dot_threshold", C.c_float),
+        ("prev_count", _fp),
+        ("prev_world_offset", _fp),
+        ("prev_keys", _fp),
+        ("prev_mid", _fp),
+        ("prev_normal", _fp),
+        ("prev_claim", _fp),
+        ("prev_was_matched", _fp),
+        ("prev_point0", _fp),
+        ("prev_point1", _fp),
+        ("prev_offset0", _fp),
+        ("prev_offset1", _fp),
+        ("prev_normal_sticky", _fp),
+        ("match_index", _fp),
+        ("new_indices", _fp),
+        ("new_count", _fp),
+        ("broken_indices", _fp),
+        ("broken_count", _fp),
     ]
 
 

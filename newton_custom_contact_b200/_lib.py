@@ -17,6 +17,7 @@ from ._abi import (
     NB_ERR_UNSUPPORTED,
     NbContactSeg,
     NbContactsPublic,
+    NbMatchState,
     NbModelDesc,
     NbStepIO,
     NbXpbdParams,
@@ -34,6 +35,7 @@ EXPORTS = (
     "nb_ingest_contacts",
     "nb_publish_contacts_static",
     "nb_contact_forces",
+    "nb_match_contacts",
 )
 
 _lib = None
@@ -79,6 +81,9 @@ def load(path: str | None = None) -> C.CDLL:
     lib.nb_ingest_contacts.restype = C.c_int
     lib.nb_ingest_contacts.argtypes = [C.POINTER(NbModelDesc), C.POINTER(NbContactsPublic), C.POINTER(NbContactSeg),
                                        C.c_void_p]
+    lib.nb_match_contacts.restype = C.c_int
+    lib.nb_match_contacts.argtypes = [C.POINTER(NbModelDesc), C.c_void_p, C.POINTER(NbContactsPublic),
+                                      C.POINTER(NbContactSeg), C.POINTER(NbMatchState), C.c_void_p]
     lib.nb_contact_forces.restype = C.c_int
     lib.nb_contact_forces.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_void_p, C.c_void_p]
     lib.nb_publish_contacts_static.restype = C.c_int

@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._abi import GeoType, NbContactSeg, NbContactsPublic, ShapeFlags, ptr
+from ._abi import GeoType, NbContactSeg, NbContactsPublic, NbMatchState, ShapeFlags, ptr
 from .contacts import Contacts
 
 BROAD_PHASE_MODES = ("nxn", "sap", "explicit")
@@ -187,13 +187,18 @@ class CollisionPipeline:
                  contact_matching: str = "disabled", contact_matching_pos_threshold: float = 0.0005,
                  contact_matching_normal_dot_threshold: float = 0.995, contact_report: bool = False,
                  verify_buffers: bool = True):
-        if contact_matching not in ("disabled", "latest", "sticky"):
+        if not isinstance(contact_matching, str) or contact_matching not in ("disabled", "latest", "sticky"):
             raise ValueError(
                 f"contact_matching must be one of 'disabled', 'latest', 'sticky', got {contact_matching!r}")
-        if contact_matching != "disabled":
-            raise NotImplementedError("contact matching is not implemented in this build")
-        if contact_report:
+        if contact_matching_pos_threshold < 0.0:
+            raise ValueError(f"contact_matching_pos_threshold must be non-negative, got {contact_matching_pos_threshold}")
+        if not -1.0 <= contact_matching_normal_dot_threshold <= 1.0:
+            raise ValueError("contact_matching_normal_dot_threshold must be in [-1, 1], got "
+                             f"{contact_matching_normal_dot_threshold}")
+        if contact_report and contact_matching == "disabled":
             raise ValueError('contact_report=True requires contact_matching != "disabled"')
+        if contact_matching != "disabled":
+            deterministic = True  # matching works on the sorted keys (collide.py:605-607)
         if max_triangle_pairs <= 0:
             raise ValueError("max_triangle_pairs must be > 0")
         if narrow_phase is not None or sdf_hydroelastic_config is not None:
@@ -207,6 +212,11 @@ class CollisionPipeline:
         self.device = model.device
         self.broad_phase_mode = mode
         self.deterministic = deterministic
+        self.contact_matching = contact_matching
+        self.contact_report = bool(contact_report)
+        self.contact_matching_pos_threshold = float(contact_matching_pos_threshold)
+        self.contact_matching_normal_dot_threshold = float(contact_matching_normal_dot_threshold)
+        self._match = None  # previous-frame state, allocated with the first contacts buffer
         self.requires_grad = model.requires_grad if requires_grad is None else requires_grad
         self.soft_contact_margin = soft_contact_margin
         if rigid_contact_max is None:
@@ -248,9 +258,62 @@ class CollisionPipeline:
     def contacts(self) -> Contacts:
         c = Contacts(self._rigid_contact_max, self._soft_contact_max, requires_grad=self.requires_grad,
                      device=self.device, requested_attributes=self.model.get_requested_contact_attributes(),
-                     world_count=self.model.world_count, deterministic=self.deterministic)
+                     world_count=self.model.world_count, deterministic=self.deterministic,
+                     contact_matching=self.contact_matching != "disabled", contact_report=self.contact_report)
         self.attach_segments(c)
+        if self.contact_matching != "disabled" and self._match is None:
+            self._alloc_match(c.rigid_contact_max)
         return c
+
+    # ------------------------------------------------------------ contact matching
+    def _alloc_match(self, cap: int) -> None:
+        dev = self.device
+        sticky = self.contact_matching == "sticky"
+        n = max(cap, 1)
+        f3 = lambda: torch.zeros((n, 3), dtype=torch.float32, device=dev)  # noqa: E731
+        m = {
+            "prev_count": torch.zeros(1, dtype=torch.int32, device=dev),
+            "prev_world_offset": torch.zeros(self.model.world_count + 1, dtype=torch.int64, device=dev),
+            "prev_keys": torch.zeros(n, dtype=torch.int64, device=dev),
+            "prev_mid": f3(),
+            "prev_normal": f3(),
+            "prev_claim": torch.zeros(n, dtype=torch.int64, device=dev),
+            "prev_was_matched": torch.zeros(n, dtype=torch.int32, device=dev) if self.contact_report else None,
+        }
+        for k in ("prev_point0", "prev_point1", "prev_offset0", "prev_offset1", "prev_normal_sticky"):
+            m[k] = f3() if sticky else None
+        m["capacity"] = cap
+        self._match = m
+
+    @property
+    def _prev_point0(self):
+        return None if self._match is None else self._match["prev_point0"]
+
+    def reset_contact_matching(self) -> None:
+        """Forget the previous frame (after teleporting / resetting bodies): the next
+        collide reports every contact as new (ContactMatcher.reset)."""
+        if self._match is not None:
+            self._match["prev_count"].zero_()
+
+    def _match_struct(self, c: Contacts) -> NbMatchState:
+        m = self._match
+        if m["capacity"] != c.rigid_contact_max:
+            raise ValueError("contacts buffer capacity differs from the one contact matching was set up for")
+        st = NbMatchState()
+        st.capacity = int(c.rigid_contact_max)
+        st.sticky = 1 if self.contact_matching == "sticky" else 0
+        st.pos_threshold_sq = self.contact_matching_pos_threshold ** 2
+        st.normal_dot_threshold = self.contact_matching_normal_dot_threshold
+        for k in ("prev_count", "prev_world_offset", "prev_keys", "prev_mid", "prev_normal", "prev_claim",
+                  "prev_was_matched", "prev_point0", "prev_point1", "prev_offset0", "prev_offset1",
+                  "prev_normal_sticky"):
+            setattr(st, k, ptr(m[k]))
+        st.match_index = ptr(c.rigid_contact_match_index)
+        st.new_indices = ptr(c.rigid_contact_new_indices)
+        st.new_count = ptr(c.rigid_contact_new_count)
+        st.broken_indices = ptr(c.rigid_contact_broken_indices)
+        st.broken_count = ptr(c.rigid_contact_broken_count)
+        return st
 
     def attach_segments(self, c: Contacts) -> None:
         P = max(1, self.layout.pair_count)
@@ -353,6 +416,20 @@ class CollisionPipeline:
         pub = self.public_struct(contacts)
         _lib.check("nb_publish_contacts", lib.nb_publish_contacts(C.byref(desc), C.byref(seg), C.byref(pub),
                                                                   C.c_void_p(stream)))
+        if self.contact_matching != "disabled":
+            if contacts.rigid_contact_match_index is None:
+                raise ValueError("CollisionPipeline has contact_matching enabled but the Contacts buffer was "
+                                 "created without contact_matching. Use pipeline.contacts() to create a "
+                                 "compatible buffer.")
+            if self.contact_report and contacts.rigid_contact_new_indices is None:
+                raise ValueError("CollisionPipeline has contact_report enabled but the Contacts buffer was "
+                                 "created without contact_report=True. Use pipeline.contacts() to create a "
+                                 "compatible buffer.")
+            if self._match is None:
+                self._alloc_match(contacts.rigid_contact_max)
+            st = self._match_struct(contacts)
+            _lib.check("nb_match_contacts", lib.nb_match_contacts(C.byref(desc), C.c_void_p(ptr(bq)), C.byref(pub),
+                                                                  C.byref(seg), C.byref(st), C.c_void_p(stream)))
         contacts.contact_generation.add_(1)
         contacts._seg_valid = True
 

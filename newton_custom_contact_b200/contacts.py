@@ -63,7 +63,19 @@ class Contacts:
         self.rigid_contact_damping = torch.zeros(0, **f32)
         self.rigid_contact_friction = torch.zeros(0, **f32)
         self.rigid_contact_sort_key = torch.zeros(n if deterministic else 0, dtype=torch.int64, device=dev)
+        self.contact_matching = bool(contact_matching)
+        self.contact_report = bool(contact_report)
         self.rigid_contact_match_index = torch.full((n,), -1, **i32) if contact_matching else None
+        if contact_report:
+            self.rigid_contact_new_indices = torch.zeros(n, **i32)
+            self.rigid_contact_new_count = torch.zeros(1, **i32)
+            self.rigid_contact_broken_indices = torch.zeros(n, **i32)
+            self.rigid_contact_broken_count = torch.zeros(1, **i32)
+        else:
+            self.rigid_contact_new_indices = None
+            self.rigid_contact_new_count = None
+            self.rigid_contact_broken_indices = None
+            self.rigid_contact_broken_count = None
         self.force = torch.zeros((n, 6), **f32) if requested_attributes and "force" in requested_attributes else None
         self.soft_contact_max = int(soft_contact_max)
         self.soft_contact_count = self.contact_counters[1:2]

@@ -134,6 +134,25 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
 
+int nb_match_contacts(const NbModelDesc* model, const float* body_q, const NbContactsPublic* pub,
+                      const NbContactSeg* seg, const NbMatchState* st, void* stream) {
+    int rc = check_model(model);
+    if (rc) return rc;
+    if (!body_q || !pub || !seg || !st || !seg->rec || !model->shape_body) return NB_ERR_INVALID;
+    if (!pub->count || !pub->world_offset || !pub->sort_key || pub->capacity != st->capacity) return NB_ERR_INVALID;
+    if (st->capacity < 0 || !st->prev_count || !st->prev_world_offset || !st->prev_keys || !st->prev_mid ||
+        !st->prev_normal || !st->prev_claim || !st->match_index)
+        return NB_ERR_INVALID;
+    if (st->sticky && (!st->prev_point0 || !st->prev_point1 || !st->prev_offset0 || !st->prev_offset1 ||
+                       !st->prev_normal_sticky))
+        return NB_ERR_INVALID;
+    if (st->new_indices && (!st->new_count || !st->broken_indices || !st->broken_count || !st->prev_was_matched))
+        return NB_ERR_INVALID;
+    if (st->capacity == 0) return NB_OK;
+    cudaError_t e = nb_launch_match(model, body_q, pub, seg, st, (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
 int nb_contact_forces(const float* contact_impulse, const int32_t* count, int32_t capacity, float dt, float* force,
                       void* stream) {
     if (capacity < 0 || (capacity > 0 && (!contact_impulse || !count || !force))) return NB_ERR_INVALID;

@@ -21,3 +21,5 @@ cudaError_t nb_launch_step(const NbModelDesc* m, const NbXpbdParams* p, const Nb
 cudaError_t nb_launch_contact_forces(const float* imp, const int32_t* count, int cap, float dt, float* force,
                                      cudaStream_t stream);
 int nb_step_slab_words(int compact);
+cudaError_t nb_launch_match(const NbModelDesc* m, const float* body_q, const NbContactsPublic* pub,
+                            const NbContactSeg* seg, const NbMatchState* st, cudaStream_t stream);

@@ -183,9 +183,9 @@ class Model:
             bw = h["body_world"]
             sw = h["shape_world"]
             jw = h["joint_world"]
-        else:  # every entity in world -1: one world
+        else:  # every entity in world -1: one world, static shapes included
             bw = np.zeros(self.body_count, np.int32)
-            sw = np.where(h["shape_body"] >= 0, 0, -1).astype(np.int32)
+            sw = np.zeros(self.shape_count, np.int32)
             jw = np.zeros(self.joint_count, np.int32)
         if np.any(bw < 0):
             raise ValueError("bodies in world -1 are not supported when worlds are used; add them inside a world")

@@ -39,6 +39,11 @@ def load() -> C.CDLL:
         lib.orc_step.restype = C.c_int
         lib.orc_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int,
                                  C.POINTER(C.c_uint32)]
+        lib.orc_contact_midpoints.restype = C.c_int
+        lib.orc_contact_midpoints.argtypes = [C.c_void_p, C.c_void_p, C.c_int] + [C.c_void_p] * 5
+        lib.orc_match_contacts.restype = C.c_int
+        lib.orc_match_contacts.argtypes = ([C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_int] + [C.c_void_p] * 4 +
+                                           [C.c_float, C.c_float, C.c_void_p, C.c_void_p])
         lib.orc_asin.restype = C.c_float
         lib.orc_asin.argtypes = [C.c_float]
         lib.orc_acos.restype = C.c_float
@@ -179,3 +184,65 @@ def contacts_table(model, layout, segs: HostSegments) -> np.ndarray:
             tag = int(r4[3:4].view(np.int32)[0])
             rows.append([w, s0, s1, (tag >> 24) & 0xFF, *r0[:3], *r1[:3], *r2[:3], *r3[:3], *r4[:3], r0[3], r1[3]])
     return np.asarray(rows, dtype=np.float64).reshape(-1, 21)
+
+
+class Matcher:
+    """Frame-to-frame contact matching on the CPU (oracle_match.cpp + bookkeeping).
+
+    ``step(model, body_q, pub)`` takes one frame's published contacts (dict of
+    numpy arrays in public order: count, world_offset, sort_key, point0/1,
+    offset0/1, normal, shape0/1), returns (match_index, new_indices,
+    broken_indices) and, in sticky mode, replays matched rows into ``pub`` in
+    place (ContactMatcher.match / replay_matched / build_report /
+    save_sorted_state, contact_match.py:720-990).
+    """
+
+    def __init__(self, pos_threshold=0.0005, normal_dot_threshold=0.995, sticky=False):
+        self.pos_thr_sq = np.float32(pos_threshold) * np.float32(pos_threshold)
+        self.ndot = np.float32(normal_dot_threshold)
+        self.sticky = sticky
+        self.prev = None
+
+    def step(self, model, layout, body_q, pub):
+        lib = load()
+        desc = model_desc(model, layout)
+        n = int(pub["count"])
+        W = model.world_count
+        f32 = lambda a: np.ascontiguousarray(np.asarray(a, np.float32))  # noqa: E731
+        i64 = lambda a: np.ascontiguousarray(np.asarray(a, np.int64))  # noqa: E731
+        i32 = lambda a: np.ascontiguousarray(np.asarray(a, np.int32))  # noqa: E731
+        bq = f32(body_q)
+        p0, p1, s0, s1 = f32(pub["point0"][:n]), f32(pub["point1"][:n]), i32(pub["shape0"][:n]), i32(pub["shape1"][:n])
+        mid = np.zeros((max(n, 1), 3), np.float32)
+        lib.orc_contact_midpoints(C.addressof(desc), bq.ctypes.data, n, p0.ctypes.data, p1.ctypes.data,
+                                  s0.ctypes.data, s1.ctypes.data, mid.ctypes.data)
+        keys, wo, nrm = i64(pub["sort_key"][:n]), i64(pub["world_offset"]), f32(pub["normal"][:n])
+        match = np.full(max(n, 1), -1, np.int32)
+        prev = self.prev
+        n_old = 0 if prev is None else prev["count"]
+        matched = np.zeros(max(n_old, 1), np.uint8)
+        if prev is not None:
+            lib.orc_match_contacts(W, n, wo.ctypes.data, keys.ctypes.data, mid.ctypes.data, nrm.ctypes.data, n_old,
+                                   prev["world_offset"].ctypes.data, prev["keys"].ctypes.data,
+                                   prev["mid"].ctypes.data, prev["normal"].ctypes.data, self.pos_thr_sq, self.ndot,
+                                   match.ctypes.data, matched.ctypes.data)
+        match = match[:n]
+        if self.sticky and prev is not None:
+            for i in np.nonzero(match >= 0)[0]:
+                k = match[i]
+                for f in ("point0", "point1", "offset0", "offset1", "normal"):
+                    pub[f][i] = prev[f][k]
+            p0 = f32(pub["point0"][:n])
+            p1 = f32(pub["point1"][:n])
+            nrm = f32(pub["normal"][:n])
+            lib.orc_contact_midpoints(C.addressof(desc), bq.ctypes.data, n, p0.ctypes.data, p1.ctypes.data,
+                                      s0.ctypes.data, s1.ctypes.data, mid.ctypes.data)
+        new_idx = np.nonzero(match < 0)[0].astype(np.int32)
+        broken = np.nonzero(matched[:n_old] == 0)[0].astype(np.int32) if n_old else np.zeros(0, np.int32)
+        self.prev = {"count": n, "world_offset": wo.copy(), "keys": keys.copy(), "mid": mid[:max(n, 1)].copy(),
+                     "normal": f32(pub["normal"][:max(n, 1)]).copy()}
+        if self.sticky:
+            for f in ("point0", "point1", "offset0", "offset1"):
+                self.prev[f] = f32(pub[f][:n]).copy()
+            self.prev["normal"] = f32(pub["normal"][:n]).copy() if n else self.prev["normal"]
+        return match, new_idx, broken
