@@ -83,7 +83,8 @@ int nb_collide(const NbModelDesc* model, const float* body_q, const NbContactSeg
     if (!body_q || !model->world_pair_start || !model->pair_shapes || !model->world_shape_start ||
         (model->global_shape_count > 0 && !model->global_shapes))
         return NB_ERR_INVALID;
-    if ((int64_t)nb_collide_smem_bytes(model) > smem_limit()) return NB_ERR_UNSUPPORTED;
+    if ((int64_t)(nb_collide_smem_bytes(model) + nb_collide_static_smem_bytes()) > smem_limit())
+        return NB_ERR_UNSUPPORTED;
     // grid_ctas <= 0: each narrow-phase kernel uses its own default (enough CTAs
     // to reach its register-limited occupancy)
     cudaError_t e = nb_launch_collide(model, body_q, seg, grid_ctas > 0 ? grid_ctas : 0, (cudaStream_t)stream);

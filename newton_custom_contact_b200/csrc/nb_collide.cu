@@ -81,6 +81,23 @@ __device__ __forceinline__ int warp_exclusive_scan(int v, int lane, int& total) 
     return x - v;
 }
 
+constexpr int kQB = 160;  // staged queue items per warp and class (> 128 = one chunk's maximum)
+
+// push a warp's staged items: analytic queue from the front (sign = 0), MPR/GJK
+// queue from the back (index `back - k`)
+__device__ __forceinline__ void flush_queue(const int2* buf, int n, int32_t* counter, int2* queue, long long back,
+                                            int lane) {
+    if (n == 0) return;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(counter, n);
+    base = __shfl_sync(kFull, base, 0);
+    for (int i = lane; i < n; i += 32) {
+        const long long k = (long long)base + i;
+        queue[back ? back - k : k] = buf[i];
+    }
+    __syncwarp();
+}
+
 __global__ void __launch_bounds__(kBT)
 broadphase_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
     extern __shared__ __align__(16) float4 sbox[];
@@ -93,6 +110,12 @@ broadphase_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg 
     // pairs packed as (slot_a | slot_b << 16), read four per lane with one 16-byte load
     const uint4* packed = reinterpret_cast<const uint4*>(m.pair_shapes);
     const int P = m.pair_count;
+    // narrow-phase queue items are staged per warp and pushed with one atomic per
+    // flush (queue order is free: every item writes only its own candidate's slots)
+    __shared__ int2 s_qa[kBT / 32][kQB], s_qg[kBT / 32][kQB];
+    int2* qa_buf = s_qa[warp];
+    int2* qg_buf = s_qg[warp];
+    int nqa = 0, nqg = 0;  // warp-uniform fill levels
     for (;;) {
         int k = 0;
         if (lane == 0) k = atomicAdd(&seg.work_counter[0], 1);
@@ -118,10 +141,14 @@ broadphase_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg 
         __syncwarp();
         const int p0 = m.world_pair_start[w], p1 = m.world_pair_start[w + 1];
         int ncand = 0;
-        for (int base = p0 & ~3; base < p1; base += 128) {
+        // the next chunk's pairs are loaded while this chunk is tested
+        int base = p0 & ~3;
+        uint4 nxt = make_uint4(0u, 0u, 0u, 0u);
+        if (base + 4 * lane < p1) nxt = packed[(base + 4 * lane) >> 2];
+        for (; base < p1; base += 128) {
             const int q = base + 4 * lane;  // multiple of 4: 16-byte aligned
-            uint4 pk = make_uint4(0u, 0u, 0u, 0u);
-            if (q < p1) pk = packed[q >> 2];
+            const uint4 pk = nxt;
+            if (q + 128 < p1) nxt = packed[(q + 128) >> 2];
             const unsigned pw[4] = {pk.x, pk.y, pk.z, pk.w};
             unsigned hit = 0u, easy = 0u;
 #pragma unroll
@@ -148,29 +175,36 @@ broadphase_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg 
             const int off_h = warp_exclusive_scan(nh, lane, tot_h);
             const int off_a = warp_exclusive_scan(na, lane, tot_a);
             const int off_g = off_h - off_a, tot_g = tot_h - tot_a;
-            int qa = 0, qg = 0;
-            if (lane == 0) {
-                if (tot_a) qa = atomicAdd(&seg.work_counter[2], tot_a);
-                if (tot_g) qg = atomicAdd(&seg.work_counter[3], tot_g);
+            // make room in the staging buffers (warp-uniform decisions)
+            if (nqa + tot_a > kQB) {
+                flush_queue(qa_buf, nqa, &seg.work_counter[2], queue, 0, lane);
+                nqa = 0;
             }
-            qa = __shfl_sync(kFull, qa, 0);
-            qg = __shfl_sync(kFull, qg, 0);
+            if (nqg + tot_g > kQB) {
+                flush_queue(qg_buf, nqg, &seg.work_counter[3], queue, 2 * (long long)P - 1, lane);
+                nqg = 0;
+            }
             int ih = 0, ia = 0, ig = 0;
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
                 if (!(hit >> r & 1u)) continue;
                 const int c = p0 + ncand + off_h + ih++;
                 seg.cand[c] = q + r;
-                if (easy >> r & 1u) queue[qa + off_a + ia++] = make_int2(c, w);
-                else queue[2 * (size_t)P - 1 - (qg + off_g + ig++)] = make_int2(c, w);
+                if (easy >> r & 1u) qa_buf[nqa + off_a + ia++] = make_int2(c, w);
+                else qg_buf[nqg + off_g + ig++] = make_int2(c, w);
             }
             ncand += tot_h;
+            nqa += tot_a;
+            nqg += tot_g;
+            __syncwarp();
         }
         if (lane == 0) {
             seg.cand_count[w] = ncand;
             seg.world_count[w] = 0;
         }
     }
+    flush_queue(qa_buf, nqa, &seg.work_counter[2], queue, 0, lane);
+    flush_queue(qg_buf, nqg, &seg.work_counter[3], queue, 2 * (long long)P - 1, lane);
 }
 
 struct NarrowItem {
@@ -529,6 +563,8 @@ int sm_count() {
 size_t nb_collide_smem_bytes(const NbModelDesc* m) {
     return (size_t)(kBT / 32) * 2 * (size_t)m->max_world_shapes * sizeof(float4);
 }
+
+size_t nb_collide_static_smem_bytes() { return (size_t)2 * (kBT / 32) * kQB * sizeof(int2); }
 
 cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const NbContactSeg* seg, int grid,
                               cudaStream_t stream) {

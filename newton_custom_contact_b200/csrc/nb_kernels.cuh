@@ -8,6 +8,7 @@
 #define NB_STEP_THREADS 256
 
 size_t nb_collide_smem_bytes(const NbModelDesc* m);
+size_t nb_collide_static_smem_bytes();
 size_t nb_step_smem_bytes(const NbModelDesc* m);
 
 cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const NbContactSeg* seg, int grid,
