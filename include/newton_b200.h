@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 6
+#define NB_ABI_VERSION 7
 
 enum {
     NB_OK = 0,
@@ -208,13 +208,16 @@ typedef struct NbContactsPublic {
 
 /* Frame-to-frame contact matching state (CollisionPipeline contact_matching,
  * newton/_src/geometry/contact_match.py).  All arrays are device memory owned
- * by the caller and persist between calls; prev_count must start at 0. */
+ * by the caller and persist between calls; prev_count must start at 0.
+ * match_index rows past the live count hold -1 (rows the previous call wrote
+ * are reset), so a buffer must start filled with -1. */
 typedef struct NbMatchState {
     int32_t capacity;            /* rigid_contact_max (rows of every per-contact array) */
     int32_t sticky;              /* 0: "latest", 1: "sticky" (replay matched rows) */
     float pos_threshold_sq;      /* contact_matching_pos_threshold^2 [m^2] */
     float normal_dot_threshold;  /* contact_matching_normal_dot_threshold */
-    int32_t* prev_count;         /* [1] contacts saved from the previous call */
+    int32_t* prev_count;         /* [2] contacts saved from the previous call; match_index rows
+                                    the previous call wrote (start both at 0; a reset zeroes [0]) */
     int64_t* prev_world_offset;  /* [W+1] the previous call's per-world public offsets */
     int64_t* prev_keys;          /* [cap] previous sort keys */
     float* prev_mid;             /* [cap,3] previous world-space contact midpoints */
@@ -232,6 +235,54 @@ typedef struct NbMatchState {
     int32_t* broken_indices;     /* [cap] out: previous indices nobody matched */
     int32_t* broken_count;       /* [1] */
 } NbMatchState;
+
+/* Learned warm start network (no counterpart in the reference): BF16 MLP
+ * 24 -> 128 -> 128 -> 3 with SiLU, weights row-major [out, in] as raw bf16
+ * bits; w1 is padded to 32 inputs and w3 to 16 outputs with zeros.  The
+ * network predicts ratios y of the contact's velocity correction to a prior
+ * (feature row column 26: the previous substep's correction of the matched
+ * contact, else the velocity that removes the expected depth):
+ * c = prior * y, lambda = c / w with w the generalised inverse mass along
+ * the normal (column 24) or the tangents (column 25); lambda_n >= 0 and
+ * |lambda_t| <= mu lambda_n (mu: column 17).  A feature row holds
+ * NB_WS_FEATURES floats: the 24 network inputs, then w_n, w_t, prior. */
+#define NB_WS_INPUTS 24
+#define NB_WS_FEATURES 27
+#define NB_WS_HIDDEN 128
+#define NB_WS_OUTPUTS 3
+typedef struct NbWsNet {
+    const uint16_t* w1;          /* [128, 32] */
+    const float* b1;             /* [128] */
+    const uint16_t* w2;          /* [128, 128] */
+    const float* b2;             /* [128] */
+    const uint16_t* w3;          /* [16, 128] */
+    const float* b3;             /* [16] */
+    const float* in_mean;        /* [24] feature normalisation: x' = (x - mean) * inv_std */
+    const float* in_inv_std;     /* [24] */
+    const float* out_scale;      /* [3] y = network output * out_scale */
+} NbWsNet;
+
+/* One training step's buffers (forward + backward of the MLP on `rows`
+ * samples, FP32 masters; weights row-major [out, in] without padding). */
+typedef struct NbWsTrain {
+    int32_t rows;
+    int32_t pad0;
+    const float* x;              /* [rows, 24] raw network inputs */
+    const float* t;              /* [rows, 3] target ratios y = lambda * w / prior */
+    const float* in_mean;        /* [24] */
+    const float* in_inv_std;     /* [24] */
+    const float* out_scale;      /* [3] */
+    const float* w1; const float* b1;   /* [128,24], [128] */
+    const float* w2; const float* b2;   /* [128,128], [128] */
+    const float* w3; const float* b3;   /* [3,128], [3] */
+    float* g_w1; float* g_b1; float* g_w2; float* g_b2; float* g_w3; float* g_b3;  /* gradients */
+    float* xn;                   /* [rows, 24] scratch */
+    float* z1; float* h1; float* z2; float* h2;  /* [rows, 128] scratch */
+    float* y; float* dy;         /* [rows, 3] scratch */
+    float* dh; float* dh2;       /* [rows, 128] scratch */
+    float* scratch_wq;           /* [128*24 + 128*128 + 3*128] scratch */
+    float* loss;                 /* [1] mean squared error of the normalised outputs */
+} NbWsTrain;
 
 /* SolverXPBD constructor arguments (newton/_src/solvers/xpbd/solver_xpbd.py:95-109). */
 typedef struct NbXpbdParams {
@@ -266,6 +317,11 @@ typedef struct NbStepIO {
     float* body_parent_f;        /* [B,6] incoming joint wrench per body (State.body_parent_f) or NULL */
     float* joint_impulse;        /* [J,6] zero-filled scratch, required with body_parent_f; left
                                     zero-filled on return */
+    const float* ws_lambda;      /* [ws_capacity,3] learned warm start: predicted impulse of each public
+                                    contact in its contact frame (n, t1, t2), or NULL (plain solve) */
+    int32_t ws_capacity;         /* rows of ws_lambda */
+    int32_t pad1;
+    int32_t* ws_fallback;        /* [1] worlds whose warm start was rejected (counter) or NULL */
 } NbStepIO;
 
 /* ABI version of the loaded library (NB_ABI_VERSION). */
@@ -315,6 +371,34 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
  */
 int nb_match_contacts(const NbModelDesc* model, const float* body_q, const NbContactsPublic* pub,
                       const NbContactSeg* seg, const NbMatchState* state, void* stream);
+
+/*
+ * Learned warm start (no counterpart in the reference).
+ * nb_ws_features: NB_WS_FEATURES floats per published contact from the
+ * pre-step state: matched flag, ratios to the prior of the depth estimate,
+ * the previous substep's corrections (through match_index), the relative
+ * velocity, depth, gravity and thickness; normal, inverse-mass shares,
+ * friction, body contact counts, log2 prior, direction to the other body,
+ * static side; then w_n, w_t, prior.  body_count: [B] scratch.
+ * nb_ws_targets: contact-frame lambdas of accumulated A-side impulses
+ * ([cap,6] as written by nb_xpbd_step's contact_impulse); clear_impulse != 0
+ * zeroes the live rows after reading, leaving the buffer ready for the next
+ * step.
+ * nb_ws_infer: the MLP on tensor cores (tcgen05), lambda [cap,3] for the
+ * first min(count, cap) contacts (zero where the prior is zero).
+ * nb_ws_grads / nb_ws_adam: training (gradients of the mean squared error,
+ * Adam update of an FP32 master array).
+ */
+int nb_ws_features(const NbModelDesc* model, const float* body_q, const float* body_qd,
+                   const NbContactsPublic* pub, const float* prev_lambda, const int32_t* match_index,
+                   int32_t* body_count, float dt, float* features, void* stream);
+int nb_ws_targets(const NbContactsPublic* pub, float* contact_impulse, float* lambda, int32_t clear_impulse,
+                  void* stream);
+int nb_ws_infer(const NbWsNet* net, const float* features, const int32_t* count, int32_t capacity,
+                float* lambda, uint32_t* status, void* stream);
+int nb_ws_grads(const NbWsTrain* args, void* stream);
+int nb_ws_adam(float* w, const float* grad, float* m1, float* m2, int64_t count, float lr, float beta1,
+               float beta2, float eps, float weight_decay, int32_t step, void* stream);
 
 /*
  * contacts.force from the impulses a step accumulated: force = impulse / dt for

@@ -20,6 +20,8 @@ from ._abi import (
     NbMatchState,
     NbModelDesc,
     NbStepIO,
+    NbWsNet,
+    NbWsTrain,
     NbXpbdParams,
 )
 
@@ -36,6 +38,11 @@ EXPORTS = (
     "nb_publish_contacts_static",
     "nb_contact_forces",
     "nb_match_contacts",
+    "nb_ws_features",
+    "nb_ws_targets",
+    "nb_ws_infer",
+    "nb_ws_grads",
+    "nb_ws_adam",
 )
 
 _lib = None
@@ -89,6 +96,19 @@ def load(path: str | None = None) -> C.CDLL:
     lib.nb_publish_contacts_static.restype = C.c_int
     lib.nb_publish_contacts_static.argtypes = [C.POINTER(NbModelDesc), C.POINTER(NbContactSeg),
                                                C.POINTER(NbContactsPublic), C.c_void_p]
+    lib.nb_ws_features.restype = C.c_int
+    lib.nb_ws_features.argtypes = [C.POINTER(NbModelDesc), C.c_void_p, C.c_void_p, C.POINTER(NbContactsPublic),
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p]
+    lib.nb_ws_targets.restype = C.c_int
+    lib.nb_ws_targets.argtypes = [C.POINTER(NbContactsPublic), C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+    lib.nb_ws_infer.restype = C.c_int
+    lib.nb_ws_infer.argtypes = [C.POINTER(NbWsNet), C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                C.c_void_p]
+    lib.nb_ws_grads.restype = C.c_int
+    lib.nb_ws_grads.argtypes = [C.POINTER(NbWsTrain), C.c_void_p]
+    lib.nb_ws_adam.restype = C.c_int
+    lib.nb_ws_adam.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float,
+                               C.c_float, C.c_float, C.c_float, C.c_int32, C.c_void_p]
     v = lib.nb_abi_version()
     if v != NB_ABI_VERSION:
         raise RuntimeError(f"{LIB_NAME} ABI version {v} != {NB_ABI_VERSION}; rebuild the library")

@@ -272,7 +272,8 @@ class CollisionPipeline:
         n = max(cap, 1)
         f3 = lambda: torch.zeros((n, 3), dtype=torch.float32, device=dev)  # noqa: E731
         m = {
-            "prev_count": torch.zeros(1, dtype=torch.int32, device=dev),
+            # [previous count, match_index rows written by the last call]
+            "prev_count": torch.zeros(2, dtype=torch.int32, device=dev),
             "prev_world_offset": torch.zeros(self.model.world_count + 1, dtype=torch.int64, device=dev),
             "prev_keys": torch.zeros(n, dtype=torch.int64, device=dev),
             "prev_mid": f3(),
@@ -293,7 +294,7 @@ class CollisionPipeline:
         """Forget the previous frame (after teleporting / resetting bodies): the next
         collide reports every contact as new (ContactMatcher.reset)."""
         if self._match is not None:
-            self._match["prev_count"].zero_()
+            self._match["prev_count"][:1].zero_()
 
     def _match_struct(self, c: Contacts) -> NbMatchState:
         m = self._match

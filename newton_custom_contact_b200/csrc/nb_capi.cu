@@ -124,6 +124,7 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
     if (!(dt > 0.0f)) return NB_ERR_INVALID;
     if (io->contact_impulse && (!io->impulse_scratch || io->contact_impulse_capacity < 0)) return NB_ERR_INVALID;
     if (io->body_parent_f && model->joint_count > 0 && !io->joint_impulse) return NB_ERR_INVALID;
+    if (io->ws_lambda && io->ws_capacity < 0) return NB_ERR_INVALID;
     if (params->enable_restitution && seg->rec && !model->shape_restitution) return NB_ERR_INVALID;
     if (model->body_count > 0 && (!io->body_q_in || !io->body_qd_in || !io->body_f_in || !io->body_q_out ||
                                   !io->body_qd_out))
@@ -151,6 +152,59 @@ int nb_match_contacts(const NbModelDesc* model, const float* body_q, const NbCon
         return NB_ERR_INVALID;
     if (st->capacity == 0) return NB_OK;
     cudaError_t e = nb_launch_match(model, body_q, pub, seg, st, (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+int nb_ws_features(const NbModelDesc* model, const float* body_q, const float* body_qd, const NbContactsPublic* pub,
+                   const float* prev_lambda, const int32_t* match_index, int32_t* body_count, float dt, float* features,
+                   void* stream) {
+    int rc = check_model(model);
+    if (rc) return rc;
+    if (!body_q || !body_qd || !pub || !pub->count || !body_count || !features || pub->capacity < 0 ||
+        !model->shape_body || !model->shape_mu)
+        return NB_ERR_INVALID;
+    if (pub->capacity > 0 && (!pub->shape0 || !pub->shape1 || !pub->point0 || !pub->point1 || !pub->normal ||
+                              !pub->margin0 || !pub->margin1))
+        return NB_ERR_INVALID;
+    cudaError_t e = nb_launch_ws_features(model, body_q, body_qd, pub, prev_lambda, match_index, body_count, dt,
+                                          features, (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+int nb_ws_targets(const NbContactsPublic* pub, float* impulse, float* lambda, int32_t clear_impulse, void* stream) {
+    if (!pub || !pub->count || !pub->normal || !impulse || !lambda || pub->capacity < 0) return NB_ERR_INVALID;
+    cudaError_t e = nb_launch_ws_targets(pub, impulse, lambda, clear_impulse != 0, (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+int nb_ws_infer(const NbWsNet* net, const float* features, const int32_t* count, int32_t capacity, float* lambda,
+                uint32_t* status, void* stream) {
+    if (!net || !net->w1 || !net->b1 || !net->w2 || !net->b2 || !net->w3 || !net->b3 || !net->in_mean ||
+        !net->in_inv_std || !net->out_scale || !count || !status || capacity < 0)
+        return NB_ERR_INVALID;
+    if (capacity > 0 && (!features || !lambda)) return NB_ERR_INVALID;
+    if ((reinterpret_cast<uintptr_t>(net->w1) | reinterpret_cast<uintptr_t>(net->w2) |
+         reinterpret_cast<uintptr_t>(net->w3)) & 15u)
+        return NB_ERR_INVALID;
+    cudaError_t e = nb_launch_ws_infer(net, features, count, capacity, lambda, status, (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+int nb_ws_grads(const NbWsTrain* a, void* stream) {
+    if (!a || a->rows <= 0 || !a->x || !a->t || !a->in_mean || !a->in_inv_std || !a->out_scale || !a->w1 ||
+        !a->b1 || !a->w2 || !a->b2 || !a->w3 || !a->b3 || !a->g_w1 || !a->g_b1 || !a->g_w2 || !a->g_b2 ||
+        !a->g_w3 || !a->g_b3 || !a->xn || !a->z1 || !a->h1 || !a->z2 || !a->h2 || !a->y || !a->dy || !a->dh ||
+        !a->dh2 || !a->scratch_wq || !a->loss)
+        return NB_ERR_INVALID;
+    cudaError_t e = nb_launch_ws_grads(a, (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
+int nb_ws_adam(float* w, const float* grad, float* m1, float* m2, int64_t count, float lr, float beta1, float beta2,
+               float eps, float weight_decay, int32_t step, void* stream) {
+    if (!w || !grad || !m1 || !m2 || count < 0 || step < 1) return NB_ERR_INVALID;
+    cudaError_t e = nb_launch_ws_adam(w, grad, m1, m2, (long)count, lr, beta1, beta2, eps, weight_decay, step,
+                                      (cudaStream_t)stream);
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
 

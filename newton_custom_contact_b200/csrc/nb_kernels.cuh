@@ -24,3 +24,27 @@ cudaError_t nb_launch_contact_forces(const float* imp, const int32_t* count, int
 int nb_step_slab_words(int compact);
 cudaError_t nb_launch_match(const NbModelDesc* m, const float* body_q, const NbContactsPublic* pub,
                             const NbContactSeg* seg, const NbMatchState* st, cudaStream_t stream);
+cudaError_t nb_launch_ws_features(const NbModelDesc* m, const float* q, const float* qd,
+                                  const NbContactsPublic* pub, const float* prev_lambda, const int32_t* match_index,
+                                  int32_t* body_count, float dt, float* feat, cudaStream_t s);
+cudaError_t nb_launch_ws_targets(const NbContactsPublic* pub, float* impulse, float* lam, int clear, cudaStream_t s);
+cudaError_t nb_launch_ws_infer(const NbWsNet* net, const float* feat, const int32_t* count, int cap, float* out,
+                               uint32_t* status, cudaStream_t s);
+cudaError_t nb_launch_ws_grads(const NbWsTrain* a, cudaStream_t s);
+cudaError_t nb_launch_ws_adam(float* w, const float* g, float* m1, float* m2, long count, float lr, float b1,
+                              float b2, float eps, float wd, int step, cudaStream_t s);
+
+// Grid for grid-stride loops over contact rows: enough blocks of `threads` to
+// cover `rows`, at most 8 per SM (the SM count is read once).
+inline int nb_contact_grid(long rows, int threads = 256) {
+    static int sms = 0;
+    if (sms <= 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+            sms = 148;
+    }
+    const long need = (rows + threads - 1) / threads;
+    const long cap = 8L * sms;
+    return (int)(need < 1 ? 1 : (need < cap ? need : cap));
+}

@@ -64,24 +64,27 @@ __device__ __forceinline__ int world_of(const int64_t* wo, int W, int64_t i) {
     return lo;
 }
 
+// The kernels below loop over live rows only (counts read on the device) with
+// a grid sized from the SM count: cost follows the contacts, not the capacity.
+#define FOR_ROWS(i, n) for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
+
+__device__ __forceinline__ int live_count(const NbContactsPublic& pub) {
+    return pub.count[0] < pub.capacity ? pub.count[0] : pub.capacity;
+}
+
 __global__ void clear_claims_kernel(NbMatchState st) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (st.new_count) st.new_count[0] = 0;
         if (st.broken_count) st.broken_count[0] = 0;
     }
-    if (i < st.prev_count[0]) {
+    FOR_ROWS(i, st.prev_count[0]) {
         st.prev_claim[i] = kClaimFree;
         if (st.prev_was_matched) st.prev_was_matched[i] = 0;
     }
 }
 
-__global__ void __launch_bounds__(kT) match_kernel(NbModelDesc m, const float* __restrict__ body_q,
-                                                   NbContactsPublic pub, NbMatchState st) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= st.capacity) return;
-    const int n_new = pub.count[0] < pub.capacity ? pub.count[0] : pub.capacity;
-    const int n_old = st.prev_count[0];
+__device__ void match_row(const NbModelDesc& m, const float* __restrict__ body_q, const NbContactsPublic& pub,
+                          const NbMatchState& st, int n_new, int n_old, int i) {
     if (i >= n_new || n_old == 0) {
         st.match_index[i] = kNotFound;
         return;
@@ -123,26 +126,31 @@ __global__ void __launch_bounds__(kT) match_kernel(NbModelDesc m, const float* _
     }
 }
 
+__global__ void __launch_bounds__(kT) match_kernel(NbModelDesc m, const float* __restrict__ body_q,
+                                                   NbContactsPublic pub, NbMatchState st) {
+    const int n_new = live_count(pub);
+    const int n_old = st.prev_count[0];
+    // rows past the live count that the last call wrote go back to "not found"
+    const int rows = n_new > st.prev_count[1] ? n_new : st.prev_count[1];
+    FOR_ROWS(i, rows) match_row(m, body_q, pub, st, n_new, n_old, i);
+}
+
 __global__ void resolve_kernel(NbContactsPublic pub, NbMatchState st) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n_new = pub.count[0] < pub.capacity ? pub.count[0] : pub.capacity;
-    if (i >= n_new) return;
-    const int32_t cand = st.match_index[i];
-    if (cand < 0) return;
-    const long long winner = st.prev_claim[cand] & 0xFFFFFFFFll;
-    if (winner == (pub.sort_key[i] & 0xFFFFFFFFll)) {
-        if (st.prev_was_matched) st.prev_was_matched[cand] = 1;
-    } else {
-        st.match_index[i] = kBroken;
+    FOR_ROWS(i, live_count(pub)) {
+        const int32_t cand = st.match_index[i];
+        if (cand < 0) continue;
+        const long long winner = st.prev_claim[cand] & 0xFFFFFFFFll;
+        if (winner == (pub.sort_key[i] & 0xFFFFFFFFll)) {
+            if (st.prev_was_matched) st.prev_was_matched[cand] = 1;
+        } else {
+            st.match_index[i] = kBroken;
+        }
     }
 }
 
 // sticky: matched rows take the previous frame's body-frame points, offsets
 // and normal, in the public arrays and in the solver record (same index)
-__global__ void replay_kernel(NbContactsPublic pub, NbContactSeg seg, NbMatchState st) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n_new = pub.count[0] < pub.capacity ? pub.count[0] : pub.capacity;
-    if (i >= n_new) return;
+__device__ void replay_row(const NbContactsPublic& pub, const NbContactSeg& seg, const NbMatchState& st, int i) {
     const int32_t k = st.match_index[i];
     if (k < 0) return;
     const V3 p0 = ld3(st.prev_point0, k), p1 = ld3(st.prev_point1, k);
@@ -161,16 +169,20 @@ __global__ void replay_kernel(NbContactsPublic pub, NbContactSeg seg, NbMatchSta
     r[4] = make_float4(o1.x, o1.y, o1.z, r[4].w);
 }
 
-__global__ void report_kernel(NbContactsPublic pub, NbMatchState st) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n_new = pub.count[0] < pub.capacity ? pub.count[0] : pub.capacity;
-    if (i < n_new && st.match_index[i] < 0) st.new_indices[atomicAdd(st.new_count, 1)] = i;
-    if (i < st.prev_count[0] && st.prev_was_matched[i] == 0) st.broken_indices[atomicAdd(st.broken_count, 1)] = i;
+__global__ void replay_kernel(NbContactsPublic pub, NbContactSeg seg, NbMatchState st) {
+    FOR_ROWS(i, live_count(pub)) replay_row(pub, seg, st, i);
 }
 
-__global__ void save_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactsPublic pub, NbMatchState st) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n_new = pub.count[0] < pub.capacity ? pub.count[0] : pub.capacity;
+__global__ void report_kernel(NbContactsPublic pub, NbMatchState st) {
+    const int n_new = live_count(pub), n_old = st.prev_count[0];
+    FOR_ROWS(i, n_new > n_old ? n_new : n_old) {
+        if (i < n_new && st.match_index[i] < 0) st.new_indices[atomicAdd(st.new_count, 1)] = i;
+        if (i < n_old && st.prev_was_matched[i] == 0) st.broken_indices[atomicAdd(st.broken_count, 1)] = i;
+    }
+}
+
+__device__ void save_row(const NbModelDesc& m, const float* __restrict__ body_q, const NbContactsPublic& pub,
+                         const NbMatchState& st, int n_new, int i) {
     if (i <= m.world_count) st.prev_world_offset[i] = pub.world_offset[i];
     if (i >= n_new) return;
     st.prev_keys[i] = pub.sort_key[i];
@@ -189,8 +201,14 @@ __global__ void save_kernel(NbModelDesc m, const float* __restrict__ body_q, NbC
     }
 }
 
+__global__ void save_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactsPublic pub, NbMatchState st) {
+    const int n_new = live_count(pub);
+    FOR_ROWS(i, n_new > m.world_count + 1 ? n_new : m.world_count + 1) save_row(m, body_q, pub, st, n_new, i);
+}
+
 __global__ void save_count_kernel(NbContactsPublic pub, NbMatchState st) {
-    st.prev_count[0] = pub.count[0] < pub.capacity ? pub.count[0] : pub.capacity;
+    st.prev_count[0] = live_count(pub);
+    st.prev_count[1] = live_count(pub);  // match_index rows holding values other than "not found"
 }
 
 }  // namespace
@@ -198,8 +216,8 @@ __global__ void save_count_kernel(NbContactsPublic pub, NbMatchState st) {
 cudaError_t nb_launch_match(const NbModelDesc* m, const float* body_q, const NbContactsPublic* pub,
                             const NbContactSeg* seg, const NbMatchState* st, cudaStream_t stream) {
     const int cap = st->capacity;
-    const int n = cap > m->world_count + 1 ? cap : m->world_count + 1;
-    const int blocks = (n + kT - 1) / kT;
+    const long n = cap > m->world_count + 1 ? cap : m->world_count + 1;
+    const int blocks = nb_contact_grid(n, kT);
     clear_claims_kernel<<<blocks, kT, 0, stream>>>(*st);
     match_kernel<<<blocks, kT, 0, stream>>>(*m, body_q, *pub, *st);
     resolve_kernel<<<blocks, kT, 0, stream>>>(*pub, *st);

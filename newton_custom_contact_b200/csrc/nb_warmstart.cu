@@ -1,0 +1,683 @@
+// Learned warm start of the XPBD contact solve: per-contact features, the
+// BF16 MLP 24 -> 128 -> 128 -> 3 (SiLU) that predicts each contact's total
+// impulse in its contact frame, and the MLP's training kernels.  The network
+// works relative to a physical prior: the previous substep's correction of
+// the same contact (through contact matching), else the velocity that
+// removes the depth expected after the integration.  Inputs are ratios to
+// the prior and inverse-mass shares; outputs y give the contact's velocity
+// correction c = prior * y, and the impulse is c / w with w the contact's
+// generalised inverse mass (normal / tangents), so the map the network
+// learns does not depend on the bodies' scale.
+//
+// Inference runs on the 5th-generation tensor cores: a CTA of 128 threads
+// takes 128 contacts per tile, stages the normalised features and the
+// hidden activations as BF16 in shared memory in the K-major core-matrix
+// layout (8 rows x 16 bytes per core matrix, no swizzle), issues one
+// tcgen05.mma chain per layer from a single thread with FP32 accumulators in
+// tensor memory, waits on an mbarrier signalled by tcgen05.commit, and reads
+// the accumulators back with tcgen05.ld for the bias + SiLU epilogue.  Every
+// wait is bounded; a timeout sets NB_STATUS_QUEUE_TIMEOUT and the CTA frees
+// its tensor memory and returns.
+//
+// Training (offline, ~40k multiply-adds per sample) runs on CUDA cores in
+// FP32 with straight-through BF16 rounding of weights and activations, so
+// the trained network is the one inference evaluates.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "nb_kernels.cuh"
+#include "nb_math.cuh"
+
+namespace {
+
+constexpr int kIn = NB_WS_INPUTS;     // 24 network inputs
+constexpr int kFeat = NB_WS_FEATURES; // + generalised inverse masses (normal, tangents), prior
+constexpr int kMuCol = 17;            // friction coefficient column of a feature row
+constexpr int kInPad = 32;            // K of layer 1 (two K=16 MMA steps)
+constexpr int kHid = NB_WS_HIDDEN;    // 128
+constexpr int kOut = NB_WS_OUTPUTS;   // 3
+constexpr int kOutPad = 16;           // N of layer 3 (smallest legal N for M = 128)
+constexpr int kTile = 128;            // contacts per tile = MMA M
+
+// ---------------------------------------------------------------- features
+
+__device__ __forceinline__ void contact_basis(V3 n, V3& t1, V3& t2) {
+    const V3 a = fabsf(n.x) < 0.9f ? V3{1.0f, 0.0f, 0.0f} : V3{0.0f, 1.0f, 0.0f};
+    t1 = normalize(cross(n, a));
+    t2 = cross(n, t1);
+}
+
+// Contact kernels below loop over the live contacts (count read on the device)
+// with a grid sized from the SM count, not from the buffer capacity.
+__device__ __forceinline__ int live_count(const NbContactsPublic& pub) {
+    return pub.count[0] < pub.capacity ? pub.count[0] : pub.capacity;
+}
+
+__global__ void ws_count_kernel(NbModelDesc m, NbContactsPublic pub, int32_t* body_count) {
+    const int n = live_count(pub);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int s0 = pub.shape0[i], s1 = pub.shape1[i];
+        const int b0 = s0 >= 0 ? m.shape_body[s0] : -1, b1 = s1 >= 0 ? m.shape_body[s1] : -1;
+        if (b0 >= 0) atomicAdd(body_count + b0, 1);
+        if (b1 >= 0) atomicAdd(body_count + b1, 1);
+    }
+}
+
+struct BodyView {
+    TF x;
+    V3 v, w, com_w;
+    float inv_m;
+    M33 iI;  // effective (body frame) inverse inertia
+    int count;
+};
+
+__device__ __forceinline__ BodyView body_view(const NbModelDesc& m, const float* q, const float* qd,
+                                              const int32_t* body_count, int b, V3 anchor) {
+    BodyView v;
+    if (b < 0) {
+        v.x = tf_identity();
+        v.v = v.w = V3{0.0f, 0.0f, 0.0f};
+        v.com_w = anchor;
+        v.inv_m = 0.0f;
+        v.iI = zero_m33();
+        v.count = 0;
+        return v;
+    }
+    const bool kin = (m.body_flags[b] & NB_BODY_KINEMATIC) != 0;
+    v.x = load_tf(q + 7 * (size_t)b);
+    v.v = load_v3(qd + 6 * (size_t)b);
+    v.w = load_v3(qd + 6 * (size_t)b + 3);
+    v.com_w = tf_point(v.x, load_v3(m.body_com + 3 * (size_t)b));
+    v.inv_m = kin ? 0.0f : m.body_inv_mass[b];
+    v.iI = kin ? zero_m33() : load_m33(m.body_inv_inertia + 9 * (size_t)b);
+    v.count = body_count[b];
+    return v;
+}
+
+// effective angular inverse mass of a unit impulse along u at lever r
+__device__ __forceinline__ float clip10(float x) { return fminf(10.0f, fmaxf(-10.0f, x)); }
+
+__device__ __forceinline__ float ang_inv(const BodyView& b, V3 r, V3 u) {
+    const V3 k = qrot_inv(b.x.q, cross(r, u));
+    return dot(k, mv(b.iI, k));
+}
+
+__device__ void features_row(const NbModelDesc& m, const float* __restrict__ q, const float* __restrict__ qd,
+                             const NbContactsPublic& pub, const float* __restrict__ prev_lambda,
+                             const int32_t* __restrict__ match_index, const int32_t* __restrict__ body_count,
+                             float dt, float* __restrict__ feat, int i) {
+    const int s0 = pub.shape0[i], s1 = pub.shape1[i];
+    const int ba = s0 >= 0 ? m.shape_body[s0] : -1, bb = s1 >= 0 ? m.shape_body[s1] : -1;
+    const V3 p0 = load_v3(pub.point0 + 3 * (size_t)i), p1 = load_v3(pub.point1 + 3 * (size_t)i);
+    const TF xa = ba >= 0 ? load_tf(q + 7 * (size_t)ba) : tf_identity();
+    const TF xb = bb >= 0 ? load_tf(q + 7 * (size_t)bb) : tf_identity();
+    const V3 pa = tf_point(xa, p0), pb = tf_point(xb, p1);
+    const BodyView A = body_view(m, q, qd, body_count, ba, pa);
+    const BodyView B = body_view(m, q, qd, body_count, bb, pb);
+    const V3 nrm = load_v3(pub.normal + 3 * (size_t)i);
+    V3 t1, t2;
+    contact_basis(nrm, t1, t2);
+    const float thick = pub.margin0[i] + pub.margin1[i];
+    const V3 ra = sub(pa, A.com_w), rb = sub(pb, B.com_w);
+    const V3 vrel = sub(add(B.v, cross(B.w, rb)), add(A.v, cross(A.w, ra)));
+    const V3 dcom = sub(B.com_w, A.com_w);
+    float mu = 0.0f;
+    int nz = 0;
+    if (s0 >= 0) { mu += m.shape_mu[s0]; nz += 1; }
+    if (s1 >= 0) { mu += m.shape_mu[s1]; nz += 1; }
+    if (nz) mu /= (float)nz;
+    const int bw = ba >= 0 ? ba : bb;
+    int wi = bw >= 0 ? m.body_world[bw] : 0;
+    wi = wi > 0 ? wi : 0;
+    const V3 g = load_v3(m.gravity + 3 * (size_t)wi);
+    // generalised inverse masses of a unit impulse along the normal / the tangents
+    const float lin = A.inv_m + B.inv_m;
+    const float wn = lin + ang_inv(A, ra, nrm) + ang_inv(B, rb, nrm);
+    const float wt = lin + 0.5f * (ang_inv(A, ra, t1) + ang_inv(A, ra, t2) + ang_inv(B, rb, t1) + ang_inv(B, rb, t2));
+    // features are inputs to a BF16 network: fast reciprocal / log intrinsics suffice
+    const float iwn = wn > 0.0f ? __frcp_rn(wn) : 0.0f;
+    const float idt = __frcp_rn(dt);
+    // the previous substep's solved impulse of the same contact, as a velocity correction c = lambda * w
+    float pc[3] = {0.0f, 0.0f, 0.0f};
+    if (prev_lambda && match_index) {
+        const int k = match_index[i];
+        if (k >= 0) {
+            pc[0] = prev_lambda[3 * (size_t)k] * wn;
+            pc[1] = prev_lambda[3 * (size_t)k + 1] * wt;
+            pc[2] = prev_lambda[3 * (size_t)k + 2] * wt;
+        }
+    }
+    const float d = dot(nrm, sub(pb, pa)) - thick;
+    const float vn = dot(vrel, nrm);
+    // gravity changes a dynamic body's velocity by g dt in one substep; a static side does not move
+    const float gv = dot(g, nrm) * dt;
+    const float gsep = gv * ((B.inv_m > 0.0f ? 1.0f : 0.0f) - (A.inv_m > 0.0f ? 1.0f : 0.0f));
+    // prior: the previous correction of a matched contact, else the velocity that removes the
+    // depth expected after the integration in one substep
+    const bool matched = pc[0] > 0.0f;
+    const float est = fmaxf(0.0f, -(d + (vn + gsep) * dt)) * idt;
+    const float prior = matched ? pc[0] : est;
+    float f[kFeat];
+    if (prior > 0.0f && wn > 0.0f) {
+        const float ip = __frcp_rn(prior);
+        const float dn = sqrtf(dot(dcom, dcom));
+        f[0] = matched ? 1.0f : 0.0f;
+        f[1] = clip10(est * ip);
+        f[2] = clip10(pc[0] * ip);
+        f[3] = clip10(pc[1] * ip);
+        f[4] = clip10(pc[2] * ip);
+        f[5] = clip10(dot(vrel, t1) * ip);
+        f[6] = clip10(dot(vrel, t2) * ip);
+        f[7] = clip10(vn * ip);
+        f[8] = clip10(d * idt * ip);
+        f[9] = clip10(gv * ip);
+        f[10] = nrm.x;
+        f[11] = nrm.y;
+        f[12] = nrm.z;
+        f[13] = A.inv_m * iwn;
+        f[14] = B.inv_m * iwn;
+        f[15] = (wn - lin) * iwn;
+        f[16] = wt * iwn;
+        f[17] = mu;
+        f[18] = (float)A.count;
+        f[19] = (float)B.count;
+        f[20] = __log2f(prior);
+        f[21] = clip10(thick * idt * ip);
+        f[22] = dn > 0.0f ? __fdividef(dot(dcom, nrm), dn) : 0.0f;
+        f[23] = (B.inv_m > 0.0f ? 1.0f : 0.0f) - (A.inv_m > 0.0f ? 1.0f : 0.0f);
+        f[24] = wn;
+        f[25] = wt;
+        f[26] = prior;
+    } else {
+        // nothing to predict: lambda = 0 (mu kept for the friction bound)
+        for (int j = 0; j < kFeat; ++j) f[j] = 0.0f;
+        f[17] = mu;
+        f[24] = wn;
+        f[25] = wt;
+    }
+    for (int j = 0; j < kFeat; ++j) feat[(size_t)i * kFeat + j] = f[j];
+}
+
+__global__ void ws_features_kernel(NbModelDesc m, const float* __restrict__ q, const float* __restrict__ qd,
+                                   NbContactsPublic pub, const float* __restrict__ prev_lambda,
+                                   const int32_t* __restrict__ match_index, const int32_t* __restrict__ body_count,
+                                   float dt, float* __restrict__ feat) {
+    const int n = live_count(pub);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        features_row(m, q, qd, pub, prev_lambda, match_index, body_count, dt, feat, i);
+}
+
+// contact-frame components (n, t1, t2) of accumulated A-side impulses:
+// lambda_n = -L.n (pushes the bodies apart), lambda_t = L.t; with `clear` the
+// impulse rows are zeroed after reading (the step only ever writes live rows,
+// so the whole buffer is zero again for the next step)
+__global__ void ws_targets_kernel(NbContactsPublic pub, float* __restrict__ impulse, float* __restrict__ lam,
+                                  int clear) {
+    const int n = live_count(pub);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const V3 nrm = load_v3(pub.normal + 3 * (size_t)i);
+        V3 t1, t2;
+        contact_basis(nrm, t1, t2);
+        float* row = impulse + 6 * (size_t)i;
+        const V3 L = load_v3(row);
+        lam[3 * (size_t)i] = -dot(L, nrm);
+        lam[3 * (size_t)i + 1] = dot(L, t1);
+        lam[3 * (size_t)i + 2] = dot(L, t2);
+        if (clear)
+            for (int k = 0; k < 6; ++k) row[k] = 0.0f;
+    }
+}
+
+// ---------------------------------------------------------------- tcgen05 inference
+
+constexpr uint32_t kSmW1 = 0;                                    // [128 x 32]  bf16
+constexpr uint32_t kSmW2 = kSmW1 + kHid * kInPad * 2;            // [128 x 128]
+constexpr uint32_t kSmW3 = kSmW2 + kHid * kHid * 2;              // [16 x 128]
+constexpr uint32_t kSmA1 = kSmW3 + kOutPad * kHid * 2;           // [128 x 32]
+constexpr uint32_t kSmA2 = kSmA1 + kTile * kInPad * 2;           // [128 x 128] hidden (both layers)
+constexpr uint32_t kSmF = kSmA2 + kTile * kHid * 2;              // fp32 params
+constexpr uint32_t kSmB1 = kSmF;
+constexpr uint32_t kSmB2 = kSmB1 + kHid * 4;
+constexpr uint32_t kSmB3 = kSmB2 + kHid * 4;
+constexpr uint32_t kSmMean = kSmB3 + kOutPad * 4;
+constexpr uint32_t kSmIstd = kSmMean + kInPad * 4;
+constexpr uint32_t kSmOsc = kSmIstd + kInPad * 4;
+constexpr uint32_t kSmBar = (kSmOsc + 16 + 15) & ~15u;           // mbarrier (8 B)
+constexpr uint32_t kSmTmem = kSmBar + 8;                         // tensor-memory base address
+constexpr uint32_t kSmBytes = kSmTmem + 8;
+constexpr uint32_t kTmemCols = 128;                              // one accumulator, reused by the layers
+constexpr long kWaitLimit = 1L << 26;                            // mbarrier polls before giving up
+
+// byte offset of element (row r, column k) of a K-major [rows x K] bf16 tile in
+// the no-swizzle core-matrix layout: 8 x 8 core matrices of 128 B, K-chunks
+// 128 B apart (leading byte offset), 8-row groups K/8 * 128 B apart (stride)
+__device__ __forceinline__ uint32_t cm_offset(int r, int k, int K) {
+    return (uint32_t)(((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    // start >> 4 [0,14), LBO >> 4 [16,30), SBO >> 4 [32,46), descriptor version 1 at
+    // bit 46, base offset 0, no swizzle (layout type 0 at [61,64))
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
+// K-major, N >> 3 at [17,23), M >> 4 at [24,29)
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long it = 0; it < kWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ float silu(float x) { return x / (1.0f + expf(-x)); }
+
+// inference epilogue: the fast exponential / division intrinsics (their error,
+// a few ulp, is far below the BF16 rounding the activations get next)
+__device__ __forceinline__ float silu_fast(float x) { return __fdividef(x, 1.0f + __expf(-x)); }
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// copy a row-major [rows x K] bf16 matrix from global into the core-matrix layout
+__device__ void stage_matrix(unsigned char* sm, const uint16_t* __restrict__ g, int rows, int K) {
+    const int chunks = rows * (K / 8);
+    for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
+        const int r = c / (K / 8), k = (c % (K / 8)) * 8;
+        *reinterpret_cast<uint4*>(sm + cm_offset(r, k, K)) =
+            *reinterpret_cast<const uint4*>(g + (size_t)r * K + k);
+    }
+}
+
+__global__ void __launch_bounds__(kTile, 1)
+ws_infer_kernel(NbWsNet net, const float* __restrict__ feat, const int32_t* __restrict__ count, int cap,
+                float* __restrict__ out, uint32_t* status) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int t = threadIdx.x, warp = t >> 5;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+    const uint32_t bar = sbase + kSmBar;
+    float* fb1 = reinterpret_cast<float*>(sm + kSmB1);
+    float* fb2 = reinterpret_cast<float*>(sm + kSmB2);
+    float* fb3 = reinterpret_cast<float*>(sm + kSmB3);
+    float* fmean = reinterpret_cast<float*>(sm + kSmMean);
+    float* fistd = reinterpret_cast<float*>(sm + kSmIstd);
+    float* fosc = reinterpret_cast<float*>(sm + kSmOsc);
+    // ---- weights and parameters, once per CTA
+    stage_matrix(sm + kSmW1, net.w1, kHid, kInPad);
+    stage_matrix(sm + kSmW2, net.w2, kHid, kHid);
+    stage_matrix(sm + kSmW3, net.w3, kOutPad, kHid);
+    fb1[t] = net.b1[t];
+    fb2[t] = net.b2[t];
+    if (t < kOutPad) fb3[t] = net.b3[t];
+    if (t < kInPad) {
+        fmean[t] = t < kIn ? net.in_mean[t] : 0.0f;
+        fistd[t] = t < kIn ? net.in_inv_std[t] : 0.0f;
+    }
+    if (t < 4) fosc[t] = t < kOut ? net.out_scale[t] : 0.0f;
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + kSmTmem),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kSmTmem);
+    const int n = count[0] < cap ? count[0] : cap;
+    const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+    uint32_t phase = 0;
+    bool ok = true;
+    const uint32_t id_h = idesc_bf16(kTile, kHid), id_o = idesc_bf16(kTile, kOutPad);
+    for (int base = blockIdx.x * kTile; base < n && ok; base += gridDim.x * kTile) {
+        const int row = base + t;
+        // ---- A1: normalised features of this thread's contact (zeros past n / past 24)
+        {
+            float x[kInPad];
+#pragma unroll
+            for (int j = 0; j < kInPad; ++j) {
+                const float raw = (row < n && j < kIn) ? feat[(size_t)row * kFeat + j] : 0.0f;
+                x[j] = (raw - fmean[j]) * fistd[j];
+            }
+#pragma unroll
+            for (int c = 0; c < kInPad / 8; ++c) {
+                uint4 v;
+                v.x = pack_bf16(x[8 * c], x[8 * c + 1]);
+                v.y = pack_bf16(x[8 * c + 2], x[8 * c + 3]);
+                v.z = pack_bf16(x[8 * c + 4], x[8 * c + 5]);
+                v.w = pack_bf16(x[8 * c + 6], x[8 * c + 7]);
+                *reinterpret_cast<uint4*>(sm + kSmA1 + cm_offset(t, 8 * c, kInPad)) = v;
+            }
+        }
+        // ---- three layers: MMA chain from one thread, epilogue by every thread on its row
+        for (int layer = 0; layer < 3 && ok; ++layer) {
+            fence_async_smem();
+            tc_before_sync();
+            __syncthreads();
+            if (t == 0) {
+                tc_after_sync();
+                const int K = layer == 0 ? kInPad : kHid;
+                const uint32_t a_off = layer == 0 ? kSmA1 : kSmA2;
+                const uint32_t b_off = layer == 0 ? kSmW1 : (layer == 1 ? kSmW2 : kSmW3);
+                const uint32_t idesc = layer == 2 ? id_o : id_h;
+                for (int s = 0; s < K / 16; ++s) {
+                    const uint64_t da = smem_desc(sbase + a_off + s * 256, 128, (K / 8) * 128);
+                    const uint64_t db = smem_desc(sbase + b_off + s * 256, 128, (K / 8) * 128);
+                    umma_bf16(tmem, da, db, idesc, s > 0 ? 1u : 0u);
+                }
+                umma_commit(bar);
+            }
+            ok = __syncthreads_and(mbar_wait(bar, phase)) != 0;
+            phase ^= 1u;
+            tc_after_sync();
+            if (!ok) break;
+            if (layer < 2) {
+                const float* bias = layer == 0 ? fb1 : fb2;
+#pragma unroll 1
+                for (int c0 = 0; c0 < kHid; c0 += 16) {
+                    float v[16];
+                    tmem_ld16(tmem + lane_base + (uint32_t)c0, v);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) v[j] = silu_fast(v[j] + bias[c0 + j]);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        uint4 p;
+                        p.x = pack_bf16(v[8 * h], v[8 * h + 1]);
+                        p.y = pack_bf16(v[8 * h + 2], v[8 * h + 3]);
+                        p.z = pack_bf16(v[8 * h + 4], v[8 * h + 5]);
+                        p.w = pack_bf16(v[8 * h + 6], v[8 * h + 7]);
+                        *reinterpret_cast<uint4*>(sm + kSmA2 + cm_offset(t, c0 + 8 * h, kHid)) = p;
+                    }
+                }
+            } else {
+                float v[16];
+                tmem_ld16(tmem + lane_base, v);
+                if (row < n) {
+                    // c = prior * y; lambda = c / w with lambda_n >= 0 and the tangential part inside
+                    // the friction cone |lambda_t| <= mu lambda_n; zero where there is no prior
+                    const float* fr = feat + (size_t)row * kFeat;
+                    const float wn = fr[kIn], wt = fr[kIn + 1], prior = fr[kIn + 2], mu = fr[kMuCol];
+                    float ln = 0.0f, l1 = 0.0f, l2 = 0.0f;
+                    if (prior > 0.0f && wn > 0.0f && wt > 0.0f) {
+                        ln = fmaxf(0.0f, (v[0] + fb3[0]) * fosc[0]) * prior / wn;
+                        l1 = (v[1] + fb3[1]) * fosc[1] * prior / wt;
+                        l2 = (v[2] + fb3[2]) * fosc[2] * prior / wt;
+                        const float lt = sqrtf(l1 * l1 + l2 * l2), cap = mu * ln;
+                        if (lt > cap) {
+                            const float s = lt > 0.0f ? cap / lt : 0.0f;
+                            l1 *= s;
+                            l2 *= s;
+                        }
+                    }
+                    out[(size_t)row * kOut] = ln;
+                    out[(size_t)row * kOut + 1] = l1;
+                    out[(size_t)row * kOut + 2] = l2;
+                }
+            }
+        }
+        tc_before_sync();
+        __syncthreads();  // tile done: A1 / A2 / tensor memory free for the next tile
+    }
+    if (!ok && t == 0) atomicOr(status, (unsigned)NB_STATUS_QUEUE_TIMEOUT);
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+// ---------------------------------------------------------------- training (CUDA cores, fp32)
+
+__device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+// C[M,N] = op(A)[M,K] . op(B)[K,N] (+ C if accumulate); row-major, op = transpose if flagged
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const float* __restrict__ A, int lda,
+                                                   const float* __restrict__ B, int ldb, float* __restrict__ C,
+                                                   int ldc, int accumulate) {
+    __shared__ float As[16][65], Bs[16][65];
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+    float acc[4][4] = {};
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+            const int kk = e / 64, mm = e % 64;
+            const int gm = m0 + mm, gk = k0 + kk;
+            As[kk][mm] = (gm < M && gk < K) ? (TA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk]) : 0.0f;
+            const int gn = n0 + mm;
+            Bs[kk][mm] = (gn < N && gk < K) ? (TB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn]) : 0.0f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            float a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int gm = m0 + ty * 4 + i, gn = n0 + tx * 4 + j;
+            if (gm < M && gn < N) {
+                float* c = C + (size_t)gm * ldc + gn;
+                *c = accumulate ? *c + acc[i][j] : acc[i][j];
+            }
+        }
+}
+
+template <bool TA, bool TB>
+cudaError_t gemm(int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C, int ldc, int acc,
+                 cudaStream_t s) {
+    dim3 grid((N + 63) / 64, (M + 63) / 64);
+    gemm_kernel<TA, TB><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, C, ldc, acc);
+    return cudaGetLastError();
+}
+
+// X[rows, cols]: normalise (features) or round weights, to bf16 values held in fp32
+__global__ void normalise_kernel(const float* __restrict__ x, const float* __restrict__ mean,
+                                 const float* __restrict__ istd, int rows, int cols, float* __restrict__ y) {
+    const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i >= (long)rows * cols) return;
+    const int c = (int)(i % cols);
+    y[i] = bf16_round(mean ? (x[i] - mean[c]) * istd[c] : x[i]);
+}
+
+// Z += bias; H = bf16(silu(Z))
+__global__ void bias_silu_kernel(float* __restrict__ z, const float* __restrict__ b, float* __restrict__ h, int rows,
+                                 int cols) {
+    const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i >= (long)rows * cols) return;
+    const float v = z[i] + b[i % cols];
+    z[i] = v;
+    h[i] = bf16_round(silu(v));
+}
+
+// Y += b3; loss and dY = 2 (Y - T / scale) / rows
+__global__ void out_grad_kernel(float* __restrict__ y, const float* __restrict__ b, const float* __restrict__ t,
+                                const float* __restrict__ scale, int rows, float* __restrict__ dy,
+                                float* __restrict__ loss) {
+    const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i >= (long)rows * kOut) return;
+    const int c = (int)(i % kOut);
+    const float v = y[i] + b[c];
+    y[i] = v;
+    const float e = v - t[i] / scale[c];
+    dy[i] = 2.0f * e / (float)rows;
+    atomicAdd(loss, e * e / (float)rows);
+}
+
+// dZ = dH * silu'(Z)
+__global__ void silu_grad_kernel(const float* __restrict__ z, float* __restrict__ dh, long count) {
+    const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float s = 1.0f / (1.0f + expf(-z[i]));
+    dh[i] = dh[i] * (s + z[i] * s * (1.0f - s));
+}
+
+// db[c] = sum_r dZ[r, c]
+__global__ void col_sum_kernel(const float* __restrict__ dz, int rows, int cols, float* __restrict__ db) {
+    const int c = blockIdx.x;
+    float s = 0.0f;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) s += dz[(size_t)r * cols + c];
+    __shared__ float red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) db[c] = red[0];
+}
+
+__global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m1,
+                            float* __restrict__ m2, long count, float lr, float b1, float b2, float eps, float wd,
+                            float c1, float c2) {
+    const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float gi = g[i];
+    m1[i] = b1 * m1[i] + (1.0f - b1) * gi;
+    m2[i] = b2 * m2[i] + (1.0f - b2) * gi * gi;
+    const float mh = m1[i] / c1, vh = m2[i] / c2;
+    w[i] -= lr * (mh / (sqrtf(vh) + eps) + wd * w[i]);
+}
+
+inline int blocks(long n, int t = 256) { return (int)((n + t - 1) / t); }
+
+inline int contact_grid(long capacity) { return nb_contact_grid(capacity, 256); }
+
+}  // namespace
+
+cudaError_t nb_launch_ws_features(const NbModelDesc* m, const float* q, const float* qd,
+                                  const NbContactsPublic* pub, const float* prev_lambda, const int32_t* match_index,
+                                  int32_t* body_count, float dt, float* feat, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(body_count, 0, sizeof(int32_t) * (size_t)(m->body_count > 0 ? m->body_count : 1), s);
+    if (e != cudaSuccess) return e;
+    if (pub->capacity <= 0) return cudaSuccess;
+    const int g = contact_grid(pub->capacity);
+    ws_count_kernel<<<g, 256, 0, s>>>(*m, *pub, body_count);
+    ws_features_kernel<<<g, 256, 0, s>>>(*m, q, qd, *pub, prev_lambda, match_index, body_count, dt, feat);
+    return cudaGetLastError();
+}
+
+cudaError_t nb_launch_ws_targets(const NbContactsPublic* pub, float* impulse, float* lam, int clear, cudaStream_t s) {
+    if (pub->capacity <= 0) return cudaSuccess;
+    ws_targets_kernel<<<contact_grid(pub->capacity), 256, 0, s>>>(*pub, impulse, lam, clear);
+    return cudaGetLastError();
+}
+
+cudaError_t nb_launch_ws_infer(const NbWsNet* net, const float* feat, const int32_t* count, int cap, float* out,
+                               uint32_t* status, cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(ws_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmBytes);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    if (cap <= 0) return cudaSuccess;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tiles = (cap + kTile - 1) / kTile;
+    const int grid = tiles < 2 * sms ? tiles : 2 * sms;  // shared memory fits 2 CTAs per SM
+    ws_infer_kernel<<<grid, kTile, kSmBytes, s>>>(*net, feat, count, cap, out, status);
+    return cudaGetLastError();
+}
+
+cudaError_t nb_launch_ws_grads(const NbWsTrain* a, cudaStream_t s) {
+    const int R = a->rows;
+    float* Wq[3] = {a->scratch_wq, a->scratch_wq + kHid * kIn, a->scratch_wq + kHid * kIn + kHid * kHid};
+    cudaError_t e = cudaMemsetAsync(a->loss, 0, sizeof(float), s);
+    if (e != cudaSuccess) return e;
+    // bf16-rounded weights and normalised inputs (what inference multiplies)
+    normalise_kernel<<<blocks(kHid * kIn), 256, 0, s>>>(a->w1, nullptr, nullptr, kHid, kIn, Wq[0]);
+    normalise_kernel<<<blocks(kHid * kHid), 256, 0, s>>>(a->w2, nullptr, nullptr, kHid, kHid, Wq[1]);
+    normalise_kernel<<<blocks(kOut * kHid), 256, 0, s>>>(a->w3, nullptr, nullptr, kOut, kHid, Wq[2]);
+    normalise_kernel<<<blocks((long)R * kIn), 256, 0, s>>>(a->x, a->in_mean, a->in_inv_std, R, kIn, a->xn);
+    // forward
+    if ((e = gemm<false, true>(R, kHid, kIn, a->xn, kIn, Wq[0], kIn, a->z1, kHid, 0, s))) return e;
+    bias_silu_kernel<<<blocks((long)R * kHid), 256, 0, s>>>(a->z1, a->b1, a->h1, R, kHid);
+    if ((e = gemm<false, true>(R, kHid, kHid, a->h1, kHid, Wq[1], kHid, a->z2, kHid, 0, s))) return e;
+    bias_silu_kernel<<<blocks((long)R * kHid), 256, 0, s>>>(a->z2, a->b2, a->h2, R, kHid);
+    if ((e = gemm<false, true>(R, kOut, kHid, a->h2, kHid, Wq[2], kHid, a->y, kOut, 0, s))) return e;
+    out_grad_kernel<<<blocks((long)R * kOut), 256, 0, s>>>(a->y, a->b3, a->t, a->out_scale, R, a->dy, a->loss);
+    // backward
+    if ((e = gemm<true, false>(kOut, kHid, R, a->dy, kOut, a->h2, kHid, a->g_w3, kHid, 0, s))) return e;
+    col_sum_kernel<<<kOut, 256, 0, s>>>(a->dy, R, kOut, a->g_b3);
+    if ((e = gemm<false, false>(R, kHid, kOut, a->dy, kOut, Wq[2], kHid, a->dh, kHid, 0, s))) return e;
+    silu_grad_kernel<<<blocks((long)R * kHid), 256, 0, s>>>(a->z2, a->dh, (long)R * kHid);
+    if ((e = gemm<true, false>(kHid, kHid, R, a->dh, kHid, a->h1, kHid, a->g_w2, kHid, 0, s))) return e;
+    col_sum_kernel<<<kHid, 256, 0, s>>>(a->dh, R, kHid, a->g_b2);
+    if ((e = gemm<false, false>(R, kHid, kHid, a->dh, kHid, Wq[1], kHid, a->dh2, kHid, 0, s))) return e;
+    silu_grad_kernel<<<blocks((long)R * kHid), 256, 0, s>>>(a->z1, a->dh2, (long)R * kHid);
+    if ((e = gemm<true, false>(kHid, kIn, R, a->dh2, kHid, a->xn, kIn, a->g_w1, kIn, 0, s))) return e;
+    col_sum_kernel<<<kHid, 256, 0, s>>>(a->dh2, R, kHid, a->g_b1);
+    return cudaGetLastError();
+}
+
+cudaError_t nb_launch_ws_adam(float* w, const float* g, float* m1, float* m2, long count, float lr, float b1,
+                              float b2, float eps, float wd, int step, cudaStream_t s) {
+    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    adam_kernel<<<blocks(count), 256, 0, s>>>(w, g, m1, m2, count, lr, b1, b2, eps, wd, c1, c2);
+    return cudaGetLastError();
+}

@@ -838,6 +838,132 @@ __device__ __forceinline__ void contact_pass(const NbModelDesc& m, SB& S, const 
     if (t == 0) nact[0] = nact[1] = 0;
 }
 
+// world's largest penetration max(-d, 0) over its contacts (group reduction
+// in *slot, an int holding the float's bits; non-negative floats order as ints)
+template <int G, class SB>
+__device__ __forceinline__ float world_penetration(const SB& S, const float4* __restrict__ R, int nc, int g, int t,
+                                                   int* slot) {
+    if (t == 0) *slot = 0;
+    group_sync<G>(g);
+    float worst = 0.0f;
+    for (int k = t; k < nc; k += G) {
+        const float4* r = R + (size_t)k * 5;
+        const int tag = __float_as_int(r[2].w);
+        const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
+        if (la == lb) continue;
+        TF Xa, Xb;
+        V3 bx_a, bx_b;
+        const float d = contact_depth(S, r[0], r[1], r[2], la, lb, Xa, Xb, bx_a, bx_b);
+        worst = fmaxf(worst, -d);  // NaN depths do not count
+    }
+    if (worst > 0.0f) atomicMax(slot, __float_as_int(worst));
+    group_sync<G>(g);
+    const float v = __int_as_float(*slot);
+    group_sync<G>(g);
+    return v;
+}
+
+// Learned warm start (no counterpart in the reference): before the plain
+// iterations, every contact's predicted impulse (io.ws_lambda, contact frame
+// n, t1, t2 as built by nb_ws_features) is applied to its two bodies as one
+// combined delta -- linear L on A, -L on B, angular r x L at the contact
+// points -- summed in the same exact fixed point as the solver.  Bodies that
+// receive nothing are left untouched, so an all-zero prediction reproduces
+// the plain step exactly.  The world falls back to no warm start (state
+// restored from a snapshot kept in the step's output rows) when the warm
+// start makes its largest penetration worse.
+template <int G, class SB>
+__device__ __noinline__ void warm_start(const NbModelDesc& m, const NbStepIO& io, const NbContactSeg& seg, SB& S,
+                                        const float4* __restrict__ R, int nc, int64_t rec_base, int b0, int g,
+                                        int t, int* scratch, float dt, unsigned* bad) {
+    const int nb = S.nb;
+    const float pen0 = world_penetration<G>(S, R, nc, g, t, scratch);
+    // snapshot pose + twist into this world's output rows (overwritten by the write-back)
+    for (int i = t; i < nb; i += G) {
+        float* qo = io.body_q_out + 7 * (size_t)(b0 + i);
+        float* qdo = io.body_qd_out + 6 * (size_t)(b0 + i);
+        for (int k = 0; k < 7; ++k) qo[k] = S.f[k * nb + i];
+        for (int k = 0; k < 6; ++k) qdo[k] = S.f[(7 + k) * nb + i];
+    }
+    for (int k = t; k < nc; k += G) {
+        const int64_t pub = seg.rec_index ? (int64_t)seg.rec_index[rec_base + k] : rec_base + k;
+        if (pub < 0 || pub >= io.ws_capacity) continue;
+        const float* lam = io.ws_lambda + 3 * (size_t)pub;
+        const float ln = lam[0], l1 = lam[1], l2 = lam[2];
+        if (ln == 0.0f && l1 == 0.0f && l2 == 0.0f) continue;
+        if (!(isfinite(ln) && isfinite(l1) && isfinite(l2))) continue;  // a non-finite prediction counts as none
+        const float4* r = R + (size_t)k * 5;
+        const int tag = __float_as_int(r[2].w);
+        const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
+        if (la == lb || __float_as_int(r[3].w) == __float_as_int(r[4].w)) continue;
+        const TF Xa = la >= 0 ? S.q(la) : tf_identity();
+        const TF Xb = lb >= 0 ? S.q(lb) : tf_identity();
+        const V3 nrm{r[2].x, r[2].y, r[2].z};
+        const V3 a = fabsf(nrm.x) < 0.9f ? V3{1.0f, 0.0f, 0.0f} : V3{0.0f, 1.0f, 0.0f};
+        const V3 t1 = normalize(cross(nrm, a));
+        const V3 t2 = cross(nrm, t1);
+        const V3 L = add(add(mul(nrm, -ln), mul(t1, l1)), mul(t2, l2));
+        if (la >= 0) {
+            const V3 ra = sub(tf_point(Xa, V3{r[0].x, r[0].y, r[0].z}), tf_point(Xa, S.com(la)));
+            S.add_delta(la, L, cross(ra, L), bad);
+        }
+        if (lb >= 0) {
+            const V3 Lb = neg(L);
+            const V3 rb = sub(tf_point(Xb, V3{r[1].x, r[1].y, r[1].z}), tf_point(Xb, S.com(lb)));
+            S.add_delta(lb, Lb, cross(rb, Lb), bad);
+        }
+    }
+    group_sync<G>(g);
+    for (int i = t; i < nb; i += G) {
+        V3 dl, da;
+        if (!S.take(i, dl, da)) continue;  // untouched bodies stay bit-identical
+        TF q = S.q(i);
+        V3 v = S.v(i), wv = S.w(i);
+        apply_body_delta(q, v, wv, dl, da, 1.0f, S.com(i), S.inertia(i), S.inv_m(i), S.inv_inertia(i), dt);
+        S.set(i, q, v, wv);
+    }
+    group_sync<G>(g);
+    const float pen1 = world_penetration<G>(S, R, nc, g, t, scratch);
+    if (!(pen1 <= pen0)) {
+        for (int i = t; i < nb; i += G) {
+            const float* qo = io.body_q_out + 7 * (size_t)(b0 + i);
+            const float* qdo = io.body_qd_out + 6 * (size_t)(b0 + i);
+            for (int k = 0; k < 7; ++k) S.f[k * nb + i] = qo[k];
+            for (int k = 0; k < 6; ++k) S.f[(7 + k) * nb + i] = qdo[k];
+        }
+        if (t == 0 && io.ws_fallback) atomicAdd(io.ws_fallback, 1);
+    } else if (io.contact_impulse) {
+        // the applied prediction is part of the contact's reported impulse (A side)
+        for (int k = t; k < nc; k += G) {
+            const int64_t pub = seg.rec_index ? (int64_t)seg.rec_index[rec_base + k] : rec_base + k;
+            if (pub < 0 || pub >= io.ws_capacity || pub >= io.contact_impulse_capacity) continue;
+            const float* lam = io.ws_lambda + 3 * (size_t)pub;
+            const float ln = lam[0], l1 = lam[1], l2 = lam[2];
+            if (ln == 0.0f && l1 == 0.0f && l2 == 0.0f) continue;
+            if (!(isfinite(ln) && isfinite(l1) && isfinite(l2))) continue;
+            const float4* r = R + (size_t)k * 5;
+            const int tag = __float_as_int(r[2].w);
+            const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
+            if (la == lb || __float_as_int(r[3].w) == __float_as_int(r[4].w)) continue;
+            const V3 nrm{r[2].x, r[2].y, r[2].z};
+            const V3 a = fabsf(nrm.x) < 0.9f ? V3{1.0f, 0.0f, 0.0f} : V3{0.0f, 1.0f, 0.0f};
+            const V3 t1 = normalize(cross(nrm, a));
+            const V3 t2 = cross(nrm, t1);
+            const V3 L = add(add(mul(nrm, -ln), mul(t1, l1)), mul(t2, l2));
+            V3 A{0.0f, 0.0f, 0.0f};
+            if (la >= 0) {
+                const TF Xa = S.q(la);
+                A = cross(sub(tf_point(Xa, V3{r[0].x, r[0].y, r[0].z}), tf_point(Xa, S.com(la))), L);
+            }
+            float* o = io.contact_impulse + (size_t)pub * 6;
+            o[0] += L.x; o[1] += L.y; o[2] += L.z;
+            o[3] += A.x; o[4] += A.y; o[5] += A.z;
+        }
+    }
+    if (t == 0) scratch[0] = scratch[1] = 0;  // the contact pass expects its counters at zero
+    group_sync<G>(g);
+}
+
 // One world's substep with a group of G threads: stage, joint forces,
 // integrate, `iterations` x (contacts, weighted apply, joints, apply),
 // restitution, write-back.  The caller carved the world's slab into S.
@@ -918,6 +1044,8 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
     const float4* R = rec + (size_t)rec_base * 5;
     const bool want_imp = has_contacts && io.contact_impulse != nullptr;
     unsigned bad = 0u;
+    if (has_contacts && io.ws_lambda)
+        warm_start<G>(m, io, seg, S, R, nc, rec_base, b0, g, t, nact, dt, &bad);
     for (int it = 0; it < p.iterations; ++it) {
         if (has_contacts) {
             contact_pass<G>(m, S, R, nc, list, nact, g, t, p.rigid_contact_relaxation, dt,

@@ -41,9 +41,24 @@ def _tf_mul(a, b):
 
 def max_penetration(model, contacts, body_q) -> float:
     """Largest penetration [m] among the live contacts at poses `body_q`."""
+    pen = contact_penetrations(model, contacts, body_q)
+    return float(pen.max().item()) if pen.numel() else 0.0
+
+
+def penetration_stats(model, contacts, body_q) -> dict:
+    """max, 99th percentile and mean penetration [m] over the live contacts, and their sum."""
+    pen = contact_penetrations(model, contacts, body_q)
+    if pen.numel() == 0:
+        return {"max": 0.0, "p99": 0.0, "mean": 0.0, "sum": 0.0}
+    return {"max": float(pen.max()), "p99": float(torch.quantile(pen.float()[:2**24], 0.99)),
+            "mean": float(pen.mean()), "sum": float(pen.sum())}
+
+
+def contact_penetrations(model, contacts, body_q) -> torch.Tensor:
+    """max(-d, 0) [m] per live contact at poses `body_q` (float64)."""
     n = min(int(contacts.rigid_contact_count.item()), contacts.rigid_contact_max)
     if n == 0:
-        return 0.0
+        return torch.zeros(0, dtype=torch.float64, device=body_q.device)
     dev = body_q.device
     q = body_q.to(torch.float64)
     shape_body = model.shape_body.to(dev).long()
@@ -61,7 +76,7 @@ def max_penetration(model, contacts, body_q) -> float:
     nrm = contacts.rigid_contact_normal[:n].to(torch.float64)
     thick = (contacts.rigid_contact_margin0[:n] + contacts.rigid_contact_margin1[:n]).to(torch.float64)
     d = (nrm * (pb - pa)).sum(-1) - thick
-    return float(torch.clamp(-d, min=0.0).max().item())
+    return torch.clamp(-d, min=0.0)
 
 
 def max_joint_violation(model, body_q) -> float:

@@ -8,8 +8,10 @@ reference that a caller can observe:
     solver_xpbd.py:203-257);
   * per-body constraint deltas are summed in 2^-32 fixed point, so results are
     bit-reproducible and independent of contact order;
-  * particles, springs, restitution and contact-force reporting are not part
-    of this build and raise ``NotImplementedError``.
+  * particles and springs are not part of this build and raise
+    ``NotImplementedError``;
+  * an optional learned warm start (``solver.warm_start``, warmstart.py) has
+    no counterpart in the reference; it is off by default.
 """
 
 from __future__ import annotations
@@ -64,6 +66,8 @@ class SolverXPBD:
         self._contact_impulse = None
         self._contact_impulse_capacity = 0
         self._joint_impulse = None
+        # optional learned warm start (warmstart.WarmStart); None = the plain solver
+        self.warm_start = None
 
     @property
     def device(self):
@@ -162,9 +166,16 @@ class SolverXPBD:
             io.impulse_scratch = ptr(contacts._seg["impulse_scratch"])
             io.contact_impulse_capacity = cap
         params = self.params()
+        ws = self.warm_start if contacts is not None else None
+        if ws is not None:
+            ws.before_step(model, pipe, desc, state_in, contacts, dt, io)
+            if ws.enabled() and ws.iterations is not None:
+                params.iterations = int(ws.iterations)
         grid = pipe.grid()
         _lib.check("nb_xpbd_step", lib.nb_xpbd_step(C.byref(desc), C.byref(params), C.byref(io), C.byref(seg),
                                                     float(dt), grid, C.c_void_p(stream)))
+        if ws is not None:
+            ws.after_step(contacts)
         self._contact_impulse = impulse
         self._contact_impulse_capacity = contacts.rigid_contact_max if contacts is not None else 0
         self._last_dt = dt
