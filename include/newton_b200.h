@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 7
+#define NB_ABI_VERSION 8
 
 enum {
     NB_OK = 0,
@@ -67,7 +67,8 @@ enum {
     NB_STATUS_NONFINITE = 1u << 1,        /* NaN/Inf body state after a step   */
     NB_STATUS_FIXED_OVERFLOW = 1u << 2,   /* delta accumulator saturated       */
     NB_STATUS_QUEUE_TIMEOUT = 1u << 3,    /* work-queue wait hit its bound     */
-    NB_STATUS_WORLD_TOO_LARGE = 1u << 4   /* world exceeds shared staging      */
+    NB_STATUS_WORLD_TOO_LARGE = 1u << 4,  /* world exceeds shared staging      */
+    NB_STATUS_ADJOINT_UNSUPPORTED = 1u << 5 /* adjoint skipped a world with an enabled non-free joint */
 };
 
 /* Geometry types (newton/_src/geometry/types.py:46-77). */
@@ -399,6 +400,39 @@ int nb_ws_infer(const NbWsNet* net, const float* features, const int32_t* count,
 int nb_ws_grads(const NbWsTrain* args, void* stream);
 int nb_ws_adam(float* w, const float* grad, float* m1, float* m2, int64_t count, float lr, float beta1,
                float beta2, float eps, float weight_decay, int32_t step, void* stream);
+
+/*
+ * Adjoint of one substep (no counterpart in the reference's compiled code:
+ * the reference differentiates SolverXPBD.step with wp.Tape over its Warp
+ * kernels, solver_xpbd.py).  Given the step's inputs and the cotangents of
+ * its outputs, writes the cotangents of body_q, body_qd and body_f.  Free
+ * rigid bodies with contacts: the contact records of `seg` (as the step used
+ * them) are held fixed, kinematic bodies are constants; a world with an
+ * enabled non-free joint is skipped with NB_STATUS_ADJOINT_UNSUPPORTED;
+ * restitution returns NB_ERR_UNSUPPORTED.  The forward pass is recomputed
+ * inside (optionally written to body_q_out / body_qd_out).
+ */
+typedef struct NbAdjointIO {
+    const float* body_q_in;      /* [B,7] the step's input state */
+    const float* body_qd_in;     /* [B,6] */
+    const float* body_f_in;      /* [B,6] */
+    const float* grad_q_out;     /* [B,7] cotangent of the output body_q */
+    const float* grad_qd_out;    /* [B,6] cotangent of the output body_qd */
+    float* grad_q_in;            /* [B,7] out */
+    float* grad_qd_in;           /* [B,6] out */
+    float* grad_f_in;            /* [B,6] out, or NULL */
+    float* body_q_out;           /* [B,7] out (the recomputed forward state), or NULL */
+    float* body_qd_out;          /* [B,6] out, or NULL with body_q_out */
+    float* tape_state;           /* [(iterations+1)*B*13] scratch */
+    float* tape_delta;           /* [iterations*B*6] scratch */
+    float* tape_weight;          /* [iterations*B] scratch */
+    double* grad_acc;            /* [B*13] scratch */
+    int64_t* delta_acc;          /* [B*6] scratch */
+    int32_t* count_acc;          /* [B] scratch */
+    uint32_t* status;            /* [1] NB_STATUS_* bits (sticky) */
+} NbAdjointIO;
+int nb_xpbd_step_adjoint(const NbModelDesc* model, const NbXpbdParams* params, const NbAdjointIO* io,
+                         const NbContactSeg* seg, float dt, void* stream);
 
 /*
  * contacts.force from the impulses a step accumulated: force = impulse / dt for

@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 7
+NB_ABI_VERSION = 8
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -244,6 +244,28 @@ class NbStepIO(C.Structure):
 
 class NbWsNet(C.Structure):
     _fields_ = [(k, _fp) for k in ("w1", "b1", "w2", "b2", "w3", "b3", "in_mean", "in_inv_std", "out_scale")]
+
+
+class NbAdjointIO(C.Structure):
+    _fields_ = [
+        ("body_q_in", _fp),
+        ("body_qd_in", _fp),
+        ("body_f_in", _fp),
+        ("grad_q_out", _fp),
+        ("grad_qd_out", _fp),
+        ("grad_q_in", _fp),
+        ("grad_qd_in", _fp),
+        ("grad_f_in", _fp),
+        ("body_q_out", _fp),
+        ("body_qd_out", _fp),
+        ("tape_state", _fp),
+        ("tape_delta", _fp),
+        ("tape_weight", _fp),
+        ("grad_acc", _fp),
+        ("delta_acc", _fp),
+        ("count_acc", _fp),
+        ("status", _fp),
+    ]
 
 
 class NbWsTrain(C.Structure):

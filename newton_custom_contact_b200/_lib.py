@@ -15,6 +15,7 @@ from ._abi import (
     NB_ERR_CUDA,
     NB_ERR_INVALID,
     NB_ERR_UNSUPPORTED,
+    NbAdjointIO,
     NbContactSeg,
     NbContactsPublic,
     NbMatchState,
@@ -43,6 +44,7 @@ EXPORTS = (
     "nb_ws_infer",
     "nb_ws_grads",
     "nb_ws_adam",
+    "nb_xpbd_step_adjoint",
 )
 
 _lib = None
@@ -109,6 +111,9 @@ def load(path: str | None = None) -> C.CDLL:
     lib.nb_ws_adam.restype = C.c_int
     lib.nb_ws_adam.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float,
                                C.c_float, C.c_float, C.c_float, C.c_int32, C.c_void_p]
+    lib.nb_xpbd_step_adjoint.restype = C.c_int
+    lib.nb_xpbd_step_adjoint.argtypes = [C.POINTER(NbModelDesc), C.POINTER(NbXpbdParams), C.POINTER(NbAdjointIO),
+                                         C.POINTER(NbContactSeg), C.c_float, C.c_void_p]
     v = lib.nb_abi_version()
     if v != NB_ABI_VERSION:
         raise RuntimeError(f"{LIB_NAME} ABI version {v} != {NB_ABI_VERSION}; rebuild the library")

@@ -136,6 +136,25 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
 
+int nb_xpbd_step_adjoint(const NbModelDesc* model, const NbXpbdParams* params, const NbAdjointIO* io,
+                         const NbContactSeg* seg, float dt, void* stream) {
+    int rc = check_model(model);
+    if (rc) return rc;
+    if (!params || !io || !seg || !io->status) return NB_ERR_INVALID;
+    if (params->iterations < 0 || !(dt > 0.0f)) return NB_ERR_INVALID;
+    if (params->enable_restitution) return NB_ERR_UNSUPPORTED;
+    if (!model->world_body_start || !model->world_joint_start) return NB_ERR_INVALID;
+    if (model->body_count > 0 &&
+        (!io->body_q_in || !io->body_qd_in || !io->body_f_in || !io->grad_q_out || !io->grad_qd_out ||
+         !io->grad_q_in || !io->grad_qd_in || !io->tape_state || !io->tape_delta || !io->tape_weight ||
+         !io->grad_acc || !io->delta_acc || !io->count_acc))
+        return NB_ERR_INVALID;
+    if (io->body_q_out && !io->body_qd_out) return NB_ERR_INVALID;
+    const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
+    cudaError_t e = nb_launch_xpbd_adjoint(model, params, io, seg, has_contacts, dt, (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
 int nb_match_contacts(const NbModelDesc* model, const float* body_q, const NbContactsPublic* pub,
                       const NbContactSeg* seg, const NbMatchState* st, void* stream) {
     int rc = check_model(model);

@@ -34,6 +34,9 @@ cudaError_t nb_launch_ws_grads(const NbWsTrain* a, cudaStream_t s);
 cudaError_t nb_launch_ws_adam(float* w, const float* g, float* m1, float* m2, long count, float lr, float b1,
                               float b2, float eps, float wd, int step, cudaStream_t s);
 
+cudaError_t nb_launch_xpbd_adjoint(const NbModelDesc* m, const NbXpbdParams* p, const NbAdjointIO* io,
+                                   const NbContactSeg* seg, int has_contacts, float dt, cudaStream_t s);
+
 // Grid for grid-stride loops over contact rows: enough blocks of `threads` to
 // cover `rows`, at most 8 per SM (the SM count is read once).
 inline int nb_contact_grid(long rows, int threads = 256) {
