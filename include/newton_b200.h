@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 8
+#define NB_ABI_VERSION 9
 
 enum {
     NB_OK = 0,
@@ -283,6 +283,7 @@ typedef struct NbWsTrain {
     float* dh; float* dh2;       /* [rows, 128] scratch */
     float* scratch_wq;           /* [128*24 + 128*128 + 3*128] scratch */
     float* loss;                 /* [1] mean squared error of the normalised outputs */
+    uint32_t* status;            /* [1] NB_STATUS_* bits (a tensor-core wait that timed out) */
 } NbWsTrain;
 
 /* SolverXPBD constructor arguments (newton/_src/solvers/xpbd/solver_xpbd.py:95-109). */
@@ -388,7 +389,8 @@ int nb_match_contacts(const NbModelDesc* model, const float* body_q, const NbCon
  * nb_ws_infer: the MLP on tensor cores (tcgen05), lambda [cap,3] for the
  * first min(count, cap) contacts (zero where the prior is zero).
  * nb_ws_grads / nb_ws_adam: training (gradients of the mean squared error,
- * Adam update of an FP32 master array).
+ * GEMMs on tensor cores with FP32 accumulation; Adam update of an FP32
+ * master array).
  */
 int nb_ws_features(const NbModelDesc* model, const float* body_q, const float* body_qd,
                    const NbContactsPublic* pub, const float* prev_lambda, const int32_t* match_index,

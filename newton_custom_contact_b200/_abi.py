@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 8
+NB_ABI_VERSION = 9
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -272,7 +272,7 @@ class NbWsTrain(C.Structure):
     _fields_ = [("rows", C.c_int32), ("pad0", C.c_int32)] + [
         (k, _fp) for k in ("x", "t", "in_mean", "in_inv_std", "out_scale", "w1", "b1", "w2", "b2", "w3", "b3",
                            "g_w1", "g_b1", "g_w2", "g_b2", "g_w3", "g_b3", "xn", "z1", "h1", "z2", "h2", "y", "dy",
-                           "dh", "dh2", "scratch_wq", "loss")]
+                           "dh", "dh2", "scratch_wq", "loss", "status")]
 
 
 def ptr(a) -> int | None:

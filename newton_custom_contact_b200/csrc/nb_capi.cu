@@ -213,7 +213,7 @@ int nb_ws_grads(const NbWsTrain* a, void* stream) {
     if (!a || a->rows <= 0 || !a->x || !a->t || !a->in_mean || !a->in_inv_std || !a->out_scale || !a->w1 ||
         !a->b1 || !a->w2 || !a->b2 || !a->w3 || !a->b3 || !a->g_w1 || !a->g_b1 || !a->g_w2 || !a->g_b2 ||
         !a->g_w3 || !a->g_b3 || !a->xn || !a->z1 || !a->h1 || !a->z2 || !a->h2 || !a->y || !a->dy || !a->dh ||
-        !a->dh2 || !a->scratch_wq || !a->loss)
+        !a->dh2 || !a->scratch_wq || !a->loss || !a->status)
         return NB_ERR_INVALID;
     cudaError_t e = nb_launch_ws_grads(a, (cudaStream_t)stream);
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;

@@ -19,9 +19,10 @@
 // wait is bounded; a timeout sets NB_STATUS_QUEUE_TIMEOUT and the CTA frees
 // its tensor memory and returns.
 //
-// Training (offline, ~40k multiply-adds per sample) runs on CUDA cores in
-// FP32 with straight-through BF16 rounding of weights and activations, so
-// the trained network is the one inference evaluates.
+// Training runs its GEMMs on the tensor cores too (tc_gemm: BF16 operands,
+// FP32 accumulation, gradients split into two BF16 parts), with
+// straight-through BF16 rounding of weights and activations, so the trained
+// network is the one inference evaluates.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -483,55 +484,174 @@ ws_infer_kernel(NbWsNet net, const float* __restrict__ feat, const int32_t* __re
 
 __device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
-// C[M,N] = op(A)[M,K] . op(B)[K,N] (+ C if accumulate); row-major, op = transpose if flagged
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const float* __restrict__ A, int lda,
-                                                   const float* __restrict__ B, int ldb, float* __restrict__ C,
-                                                   int ldc, int accumulate) {
-    __shared__ float As[16][65], Bs[16][65];
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-    float acc[4][4] = {};
-    for (int k0 = 0; k0 < K; k0 += 16) {
-        for (int e = threadIdx.x; e < 16 * 64; e += 256) {
-            const int kk = e / 64, mm = e % 64;
-            const int gm = m0 + mm, gk = k0 + kk;
-            As[kk][mm] = (gm < M && gk < K) ? (TA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk]) : 0.0f;
-            const int gn = n0 + mm;
-            Bs[kk][mm] = (gn < N && gk < K) ? (TB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn]) : 0.0f;
-        }
-        __syncthreads();
+// Training GEMMs on the tensor cores: C(m, n) = sum_k A(m, k) B(n, k) for FP32
+// operands in global memory with arbitrary strides (so transposed operands
+// need no copy), BF16 tcgen05.mma with an FP32 accumulator in tensor memory.
+// A CTA of 128 threads owns a 128 x nt tile of C (nt = 16 / 32 / 64 / 128)
+// and a slice of K (split-K CTAs add their partial tiles atomically into a
+// zeroed C).  Per 64-wide K chunk every thread converts 8-element runs of A
+// and B to BF16 into the K-major core-matrix layout; operands that are not
+// exactly BF16 (the gradients) are split into hi = bf16(x) and
+// lo = bf16(x - hi) and multiplied as hi.hi + hi.lo + lo.hi, which keeps the
+// products at about FP32 accuracy.
+struct TcGemm {
+    const float* A;
+    long sam, sak;
+    const float* B;
+    long sbn, sbk;
+    float* C;
+    long scm, scn;
+    int M, N, K;
+    int nt;        // tile width in n: 16, 32, 64 or 128
+    int k_per;     // K range per split (multiple of 64)
+    int split;     // > 1: atomic accumulation into C
+    int exact;     // operands are BF16 values: hi only
+};
+
+constexpr int kGemmKc = 64;
+constexpr uint32_t kGemmTileA = 128 * kGemmKc * 2;  // bytes of one 128 x 64 BF16 tile
+constexpr uint32_t kGemmTileB = 128 * kGemmKc * 2;  // at most 128 rows
+constexpr uint32_t kGemmSmem = 2 * kGemmTileA + 2 * kGemmTileB + 16;
+
+__device__ __forceinline__ void split_bf16(const float (&x)[8], uint4& hi, uint4& lo) {
+    float h[8], l[8];
 #pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-            float a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
-        }
-        __syncthreads();
+    for (int j = 0; j < 8; ++j) {
+        h[j] = __bfloat162float(__float2bfloat16_rn(x[j]));
+        l[j] = x[j] - h[j];
     }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int gm = m0 + ty * 4 + i, gn = n0 + tx * 4 + j;
-            if (gm < M && gn < N) {
-                float* c = C + (size_t)gm * ldc + gn;
-                *c = accumulate ? *c + acc[i][j] : acc[i][j];
-            }
-        }
+    hi = make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]), pack_bf16(h[6], h[7]));
+    lo = make_uint4(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]), pack_bf16(l[4], l[5]), pack_bf16(l[6], l[7]));
 }
 
-template <bool TA, bool TB>
-cudaError_t gemm(int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C, int ldc, int acc,
-                 cudaStream_t s) {
-    dim3 grid((N + 63) / 64, (M + 63) / 64);
-    gemm_kernel<TA, TB><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, C, ldc, acc);
+__global__ void __launch_bounds__(128, 1) tc_gemm_kernel(TcGemm g, uint32_t* status) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int t = threadIdx.x, warp = t >> 5;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+    const uint32_t sAh = 0, sAl = kGemmTileA, sBh = 2 * kGemmTileA, sBl = 2 * kGemmTileA + kGemmTileB;
+    const uint32_t bar = sbase + 2 * kGemmTileA + 2 * kGemmTileB;
+    const int m0 = blockIdx.x * 128, n0 = blockIdx.y * g.nt;
+    const int k_beg = blockIdx.z * g.k_per;
+    const int k_end = min(g.K, k_beg + g.k_per);
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __shared__ uint32_t s_tmem;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(&s_tmem)),
+                     "r"(128u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = idesc_bf16(128, g.nt);
+    uint32_t phase = 0;
+    bool ok = true, any = false;
+    for (int kc = k_beg; kc < k_end && ok; kc += kGemmKc) {
+        // stage A (128 rows) and B (nt rows) of this K chunk
+        for (int e = t; e < (128 + g.nt) * (kGemmKc / 8); e += 128) {
+            const bool isA = e < 128 * (kGemmKc / 8);
+            const int ee = isA ? e : e - 128 * (kGemmKc / 8);
+            const int r = ee / (kGemmKc / 8), k8 = (ee % (kGemmKc / 8)) * 8;
+            const int row = isA ? m0 + r : n0 + r;
+            const bool rin = isA ? row < g.M : row < g.N;
+            float x[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int k = kc + k8 + j;
+                x[j] = (rin && k < k_end) ? (isA ? g.A[row * g.sam + k * g.sak] : g.B[row * g.sbn + k * g.sbk])
+                                          : 0.0f;
+            }
+            uint4 hi, lo;
+            split_bf16(x, hi, lo);
+            const uint32_t off = cm_offset(r, k8, kGemmKc);
+            *reinterpret_cast<uint4*>(sm + (isA ? sAh : sBh) + off) = hi;
+            if (!g.exact) *reinterpret_cast<uint4*>(sm + (isA ? sAl : sBl) + off) = lo;
+        }
+        fence_async_smem();
+        tc_before_sync();
+        __syncthreads();
+        if (t == 0) {
+            tc_after_sync();
+            for (int s = 0; s < kGemmKc / 16; ++s) {
+                const uint32_t o = s * 256;
+                const uint32_t lbo = 128, sbo = (kGemmKc / 8) * 128;
+                umma_bf16(tmem, smem_desc(sbase + sAh + o, lbo, sbo), smem_desc(sbase + sBh + o, lbo, sbo), idesc,
+                          any ? 1u : 0u);
+                any = true;
+                if (!g.exact) {
+                    umma_bf16(tmem, smem_desc(sbase + sAh + o, lbo, sbo), smem_desc(sbase + sBl + o, lbo, sbo),
+                              idesc, 1u);
+                    umma_bf16(tmem, smem_desc(sbase + sAl + o, lbo, sbo), smem_desc(sbase + sBh + o, lbo, sbo),
+                              idesc, 1u);
+                }
+            }
+            umma_commit(bar);
+        }
+        any = true;
+        ok = __syncthreads_and(mbar_wait(bar, phase)) != 0;
+        phase ^= 1u;
+        tc_after_sync();
+    }
+    if (ok && any) {
+        const int row = m0 + t;
+        const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+        for (int c0 = 0; c0 < g.nt; c0 += 16) {
+            float v[16];
+            tmem_ld16(tmem + lane_base + (uint32_t)c0, v);
+            if (row < g.M)
+                for (int j = 0; j < 16; ++j) {
+                    const int n = n0 + c0 + j;
+                    if (n >= g.N) break;
+                    float* c = g.C + row * g.scm + n * g.scn;
+                    if (g.split > 1) atomicAdd(c, v[j]);
+                    else *c = v[j];
+                }
+        }
+    }
+    if (!ok && t == 0) atomicOr(status, (unsigned)NB_STATUS_QUEUE_TIMEOUT);
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u) : "memory");
+}
+
+cudaError_t tc_gemm(const float* A, long sam, long sak, const float* B, long sbn, long sbk, float* C, long scm,
+                    long scn, int M, int N, int K, bool exact, uint32_t* status, cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    if (M <= 0 || N <= 0 || K <= 0) return cudaSuccess;
+    TcGemm g;
+    g.A = A; g.sam = sam; g.sak = sak;
+    g.B = B; g.sbn = sbn; g.sbk = sbk;
+    g.C = C; g.scm = scm; g.scn = scn;
+    g.M = M; g.N = N; g.K = K;
+    g.nt = N <= 16 ? 16 : (N <= 32 ? 32 : (N <= 64 ? 64 : 128));
+    g.exact = exact ? 1 : 0;
+    const int mt = (M + 127) / 128, ntiles = (N + g.nt - 1) / g.nt;
+    // split K until the grid has about one CTA per SM, at least 8 chunks (512) per split
+    const int chunks = (K + kGemmKc - 1) / kGemmKc;
+    int split = 1;
+    while (mt * ntiles * split * 2 <= 148 && chunks / (split * 2) >= 8) split *= 2;
+    g.k_per = ((chunks + split - 1) / split) * kGemmKc;
+    g.split = (K + g.k_per - 1) / g.k_per;
+    if (g.split > 1) {
+        // C is dense [M, N] in one of the two orders for every split GEMM here
+        cudaError_t e = cudaMemsetAsync(C, 0, sizeof(float) * (size_t)M * N, s);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid(mt, ntiles, g.split);
+    tc_gemm_kernel<<<grid, 128, kGemmSmem, s>>>(g, status);
     return cudaGetLastError();
 }
 
@@ -654,23 +774,29 @@ cudaError_t nb_launch_ws_grads(const NbWsTrain* a, cudaStream_t s) {
     normalise_kernel<<<blocks(kHid * kHid), 256, 0, s>>>(a->w2, nullptr, nullptr, kHid, kHid, Wq[1]);
     normalise_kernel<<<blocks(kOut * kHid), 256, 0, s>>>(a->w3, nullptr, nullptr, kOut, kHid, Wq[2]);
     normalise_kernel<<<blocks((long)R * kIn), 256, 0, s>>>(a->x, a->in_mean, a->in_inv_std, R, kIn, a->xn);
-    // forward
-    if ((e = gemm<false, true>(R, kHid, kIn, a->xn, kIn, Wq[0], kIn, a->z1, kHid, 0, s))) return e;
+    uint32_t* st = a->status;
+    // forward: operands are BF16 values, one MMA per K step
+    if ((e = tc_gemm(a->xn, kIn, 1, Wq[0], kIn, 1, a->z1, kHid, 1, R, kHid, kIn, true, st, s))) return e;
     bias_silu_kernel<<<blocks((long)R * kHid), 256, 0, s>>>(a->z1, a->b1, a->h1, R, kHid);
-    if ((e = gemm<false, true>(R, kHid, kHid, a->h1, kHid, Wq[1], kHid, a->z2, kHid, 0, s))) return e;
+    if ((e = tc_gemm(a->h1, kHid, 1, Wq[1], kHid, 1, a->z2, kHid, 1, R, kHid, kHid, true, st, s))) return e;
     bias_silu_kernel<<<blocks((long)R * kHid), 256, 0, s>>>(a->z2, a->b2, a->h2, R, kHid);
-    if ((e = gemm<false, true>(R, kOut, kHid, a->h2, kHid, Wq[2], kHid, a->y, kOut, 0, s))) return e;
+    if ((e = tc_gemm(a->h2, kHid, 1, Wq[2], kHid, 1, a->y, kOut, 1, R, kOut, kHid, true, st, s))) return e;
     out_grad_kernel<<<blocks((long)R * kOut), 256, 0, s>>>(a->y, a->b3, a->t, a->out_scale, R, a->dy, a->loss);
-    // backward
-    if ((e = gemm<true, false>(kOut, kHid, R, a->dy, kOut, a->h2, kHid, a->g_w3, kHid, 0, s))) return e;
+    // backward: gradient operands split into hi + lo BF16
+    // g_w3[o, h] = sum_r dy[r, o] h2[r, h]  (m = h, n = o, k = r)
+    if ((e = tc_gemm(a->h2, 1, kHid, a->dy, 1, kOut, a->g_w3, 1, kHid, kHid, kOut, R, false, st, s))) return e;
     col_sum_kernel<<<kOut, 256, 0, s>>>(a->dy, R, kOut, a->g_b3);
-    if ((e = gemm<false, false>(R, kHid, kOut, a->dy, kOut, Wq[2], kHid, a->dh, kHid, 0, s))) return e;
+    // dh[r, h] = sum_o dy[r, o] w3[o, h]
+    if ((e = tc_gemm(a->dy, kOut, 1, Wq[2], 1, kHid, a->dh, kHid, 1, R, kHid, kOut, false, st, s))) return e;
     silu_grad_kernel<<<blocks((long)R * kHid), 256, 0, s>>>(a->z2, a->dh, (long)R * kHid);
-    if ((e = gemm<true, false>(kHid, kHid, R, a->dh, kHid, a->h1, kHid, a->g_w2, kHid, 0, s))) return e;
+    // g_w2[i, j] = sum_r dz2[r, i] h1[r, j]
+    if ((e = tc_gemm(a->dh, 1, kHid, a->h1, 1, kHid, a->g_w2, kHid, 1, kHid, kHid, R, false, st, s))) return e;
     col_sum_kernel<<<kHid, 256, 0, s>>>(a->dh, R, kHid, a->g_b2);
-    if ((e = gemm<false, false>(R, kHid, kHid, a->dh, kHid, Wq[1], kHid, a->dh2, kHid, 0, s))) return e;
+    // dh2[r, j] = sum_i dz2[r, i] w2[i, j]
+    if ((e = tc_gemm(a->dh, kHid, 1, Wq[1], 1, kHid, a->dh2, kHid, 1, R, kHid, kHid, false, st, s))) return e;
     silu_grad_kernel<<<blocks((long)R * kHid), 256, 0, s>>>(a->z1, a->dh2, (long)R * kHid);
-    if ((e = gemm<true, false>(kHid, kIn, R, a->dh2, kHid, a->xn, kIn, a->g_w1, kIn, 0, s))) return e;
+    // g_w1[i, j] = sum_r dz1[r, i] xn[r, j]
+    if ((e = tc_gemm(a->dh2, 1, kHid, a->xn, 1, kIn, a->g_w1, kIn, 1, kHid, kIn, R, false, st, s))) return e;
     col_sum_kernel<<<kHid, 256, 0, s>>>(a->dh2, R, kHid, a->g_b1);
     return cudaGetLastError();
 }

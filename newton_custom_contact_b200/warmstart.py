@@ -148,7 +148,7 @@ class WarmStartNet:
                "z2": torch.empty(R, N_HID, **f), "h2": torch.empty(R, N_HID, **f), "y": torch.empty(R, N_OUT, **f),
                "dy": torch.empty(R, N_OUT, **f), "dh": torch.empty(R, N_HID, **f), "dh2": torch.empty(R, N_HID, **f),
                "scratch_wq": torch.empty(N_HID * N_IN + N_HID * N_HID + N_OUT * N_HID, **f),
-               "loss": torch.zeros(1, **f)}
+               "loss": torch.zeros(1, **f), "status": torch.zeros(1, dtype=torch.int32, device=dev)}
         a = NbWsTrain()
         a.rows = R
         a.x, a.t = ptr(x.contiguous()), ptr(t.contiguous())
@@ -159,6 +159,8 @@ class WarmStartNet:
         for k, v in buf.items():
             setattr(a, k, ptr(v))
         _lib.check("nb_ws_grads", lib.nb_ws_grads(C.byref(a), C.c_void_p(_lib.stream_handle(dev))))
+        if int(buf["status"].item()):
+            raise RuntimeError("nb_ws_grads: a tensor-core wait timed out")
         return g, float(buf["loss"].item())
 
     def fit(self, features: torch.Tensor, lam: torch.Tensor, epochs: int = 30, batch: int = 4096,
