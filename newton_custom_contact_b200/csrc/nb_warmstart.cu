@@ -34,11 +34,14 @@ namespace {
 constexpr int kIn = NB_WS_INPUTS;     // 24 network inputs
 constexpr int kFeat = NB_WS_FEATURES; // + generalised inverse masses (normal, tangents), prior
 constexpr int kMuCol = 17;            // friction coefficient column of a feature row
+constexpr int kFeatBlock = 256;       // threads (rows) per block of the features kernel
+static_assert((kFeatBlock * kFeat * 4) % 16 == 0, "feature blocks must start on 16-byte boundaries");
 constexpr int kInPad = 32;            // K of layer 1 (two K=16 MMA steps)
 constexpr int kHid = NB_WS_HIDDEN;    // 128
 constexpr int kOut = NB_WS_OUTPUTS;   // 3
 constexpr int kOutPad = 16;           // N of layer 3 (smallest legal N for M = 128)
 constexpr int kTile = 128;            // contacts per tile = MMA M
+static_assert((kTile * kFeat * 4) % 16 == 0, "inference tiles must start on 16-byte boundaries");
 
 // ---------------------------------------------------------------- features
 
@@ -106,7 +109,7 @@ __device__ __forceinline__ float ang_inv(const BodyView& b, V3 r, V3 u) {
 __device__ void features_row(const NbModelDesc& m, const float* __restrict__ q, const float* __restrict__ qd,
                              const NbContactsPublic& pub, const float* __restrict__ prev_lambda,
                              const int32_t* __restrict__ match_index, const int32_t* __restrict__ body_count,
-                             float dt, float* __restrict__ feat, int i) {
+                             float dt, float* __restrict__ row_out, int i) {
     const int s0 = pub.shape0[i], s1 = pub.shape1[i];
     const int ba = s0 >= 0 ? m.shape_body[s0] : -1, bb = s1 >= 0 ? m.shape_body[s1] : -1;
     const V3 p0 = load_v3(pub.point0 + 3 * (size_t)i), p1 = load_v3(pub.point1 + 3 * (size_t)i);
@@ -196,16 +199,33 @@ __device__ void features_row(const NbModelDesc& m, const float* __restrict__ q, 
         f[24] = wn;
         f[25] = wt;
     }
-    for (int j = 0; j < kFeat; ++j) feat[(size_t)i * kFeat + j] = f[j];
+    for (int j = 0; j < kFeat; ++j) row_out[j] = f[j];
 }
 
 __global__ void ws_features_kernel(NbModelDesc m, const float* __restrict__ q, const float* __restrict__ qd,
                                    NbContactsPublic pub, const float* __restrict__ prev_lambda,
                                    const int32_t* __restrict__ match_index, const int32_t* __restrict__ body_count,
                                    float dt, float* __restrict__ feat) {
+    // rows are built in shared memory and written out as one contiguous block
+    // (coalesced 16-byte stores) instead of 27 strided stores per thread
+    __shared__ __align__(16) float sf[kFeatBlock * kFeat];
     const int n = live_count(pub);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        features_row(m, q, qd, pub, prev_lambda, match_index, body_count, dt, feat, i);
+    const int t = threadIdx.x;
+    for (int base = blockIdx.x * kFeatBlock; base < n; base += gridDim.x * kFeatBlock) {
+        if (base + t < n) features_row(m, q, qd, pub, prev_lambda, match_index, body_count, dt, sf + t * kFeat, base + t);
+        __syncthreads();
+        const int rows = n - base < kFeatBlock ? n - base : kFeatBlock;
+        float* dst = feat + (size_t)base * kFeat;
+        if (rows == kFeatBlock) {
+            // base is a multiple of kFeatBlock, so dst is 16-byte aligned (kFeatBlock * kFeat * 4 % 16 == 0)
+            const float4* s4 = reinterpret_cast<const float4*>(sf);
+            float4* d4 = reinterpret_cast<float4*>(dst);
+            for (int e = t; e < kFeatBlock * kFeat / 4; e += kFeatBlock) d4[e] = s4[e];
+        } else {
+            for (int e = t; e < rows * kFeat; e += kFeatBlock) dst[e] = sf[e];
+        }
+        __syncthreads();
+    }
 }
 
 // contact-frame components (n, t1, t2) of accumulated A-side impulses:
@@ -243,7 +263,8 @@ constexpr uint32_t kSmB3 = kSmB2 + kHid * 4;
 constexpr uint32_t kSmMean = kSmB3 + kOutPad * 4;
 constexpr uint32_t kSmIstd = kSmMean + kInPad * 4;
 constexpr uint32_t kSmOsc = kSmIstd + kInPad * 4;
-constexpr uint32_t kSmBar = (kSmOsc + 16 + 15) & ~15u;           // mbarrier (8 B)
+constexpr uint32_t kSmFeat = (kSmOsc + 16 + 15) & ~15u;          // [128 x 27] fp32 feature rows of the tile
+constexpr uint32_t kSmBar = kSmFeat + kTile * kFeat * 4;          // mbarrier (8 B)
 constexpr uint32_t kSmTmem = kSmBar + 8;                         // tensor-memory base address
 constexpr uint32_t kSmBytes = kSmTmem + 8;
 constexpr uint32_t kTmemCols = 128;                              // one accumulator, reused by the layers
@@ -317,11 +338,34 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
+// 64 consecutive accumulator columns of this thread's lane, load and wait in one
+// statement so no use of the registers can be scheduled before the wait
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
+    uint32_t r[64];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n\t"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int j = 0; j < 64; ++j) v[j] = __uint_as_float(r[j]);
+}
+
 __device__ __forceinline__ float silu(float x) { return x / (1.0f + expf(-x)); }
 
-// inference epilogue: the fast exponential / division intrinsics (their error,
-// a few ulp, is far below the BF16 rounding the activations get next)
-__device__ __forceinline__ float silu_fast(float x) { return __fdividef(x, 1.0f + __expf(-x)); }
+// inference epilogue: silu(u) = u sigmoid(u) = h + h tanh(h) with h = u / 2, one
+// hardware tanh (tanh.approx.f32, relative error about 2^-11) per activation --
+// far below the BF16 rounding the activations get next
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float silu_fast(float u) {
+    const float h = 0.5f * u;
+    return __fmaf_rn(h, tanh_approx(h), h);
+}
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
     const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -329,20 +373,40 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
 }
 
 // copy a row-major [rows x K] bf16 matrix from global into the core-matrix layout
+// (8 independent 16-byte loads in flight per thread before their stores)
 __device__ void stage_matrix(unsigned char* sm, const uint16_t* __restrict__ g, int rows, int K) {
     const int chunks = rows * (K / 8);
-    for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
-        const int r = c / (K / 8), k = (c % (K / 8)) * 8;
-        *reinterpret_cast<uint4*>(sm + cm_offset(r, k, K)) =
-            *reinterpret_cast<const uint4*>(g + (size_t)r * K + k);
+    for (int c0 = threadIdx.x; c0 < chunks; c0 += 8 * blockDim.x) {
+        uint4 v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int c = c0 + u * blockDim.x;
+            if (c < chunks) {
+                const int r = c / (K / 8), k = (c % (K / 8)) * 8;
+                v[u] = __ldg(reinterpret_cast<const uint4*>(g + (size_t)r * K + k));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int c = c0 + u * blockDim.x;
+            if (c < chunks) {
+                const int r = c / (K / 8), k = (c % (K / 8)) * 8;
+                *reinterpret_cast<uint4*>(sm + cm_offset(r, k, K)) = v[u];
+            }
+        }
     }
 }
 
-__global__ void __launch_bounds__(kTile, 1)
+// 256 threads per CTA: thread t owns tile row t % 128 (its tensor-memory lane)
+// and half t / 128 of the 128 hidden columns in the epilogues
+constexpr int kInferThreads = 256;
+
+__global__ void __launch_bounds__(kInferThreads, 2)
 ws_infer_kernel(NbWsNet net, const float* __restrict__ feat, const int32_t* __restrict__ count, int cap,
                 float* __restrict__ out, uint32_t* status) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int t = threadIdx.x, warp = t >> 5;
+    const int r = t & (kTile - 1), half = t >> 7;
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
     const uint32_t bar = sbase + kSmBar;
     float* fb1 = reinterpret_cast<float*>(sm + kSmB1);
@@ -355,8 +419,10 @@ ws_infer_kernel(NbWsNet net, const float* __restrict__ feat, const int32_t* __re
     stage_matrix(sm + kSmW1, net.w1, kHid, kInPad);
     stage_matrix(sm + kSmW2, net.w2, kHid, kHid);
     stage_matrix(sm + kSmW3, net.w3, kOutPad, kHid);
-    fb1[t] = net.b1[t];
-    fb2[t] = net.b2[t];
+    if (t < kHid) {
+        fb1[t] = net.b1[t];
+        fb2[t] = net.b2[t];
+    }
     if (t < kOutPad) fb3[t] = net.b3[t];
     if (t < kInPad) {
         fmean[t] = t < kIn ? net.in_mean[t] : 0.0f;
@@ -379,31 +445,49 @@ ws_infer_kernel(NbWsNet net, const float* __restrict__ feat, const int32_t* __re
     tc_after_sync();
     const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kSmTmem);
     const int n = count[0] < cap ? count[0] : cap;
-    const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+    // a warp reaches the 32 lanes 32 * (warp % 4) .. + 31: rows r of both halves
+    const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
     uint32_t phase = 0;
     bool ok = true;
     const uint32_t id_h = idesc_bf16(kTile, kHid), id_o = idesc_bf16(kTile, kOutPad);
     for (int base = blockIdx.x * kTile; base < n && ok; base += gridDim.x * kTile) {
-        const int row = base + t;
-        // ---- A1: normalised features of this thread's contact (zeros past n / past 24)
+        const int row = base + r;
+        // ---- the tile's feature rows: one contiguous block, read with coalesced 16-byte loads
+        float* sfeat = reinterpret_cast<float*>(sm + kSmFeat);
         {
-            float x[kInPad];
+            const int rows = n - base < kTile ? n - base : kTile;
+            const float* src = feat + (size_t)base * kFeat;
+            if (rows == kTile) {
+                // base is a multiple of kTile: kTile * kFeat * 4 bytes keep src 16-byte aligned
+                const float4* s4 = reinterpret_cast<const float4*>(src);
+                float4* d4 = reinterpret_cast<float4*>(sfeat);
+                for (int e = t; e < kTile * kFeat / 4; e += kInferThreads) d4[e] = s4[e];
+            } else {
+                for (int e = t; e < rows * kFeat; e += kInferThreads) sfeat[e] = src[e];
+            }
+        }
+        __syncthreads();
+        const float* fr = sfeat + r * kFeat;
+        // ---- A1: normalised features of row r, columns 16 * half .. + 15 (zeros past n / past 24)
+        {
+            float x[16];
 #pragma unroll
-            for (int j = 0; j < kInPad; ++j) {
-                const float raw = (row < n && j < kIn) ? feat[(size_t)row * kFeat + j] : 0.0f;
-                x[j] = (raw - fmean[j]) * fistd[j];
+            for (int j = 0; j < 16; ++j) {
+                const int col = 16 * half + j;
+                const float raw = (row < n && col < kIn) ? fr[col] : 0.0f;
+                x[j] = (raw - fmean[col]) * fistd[col];
             }
 #pragma unroll
-            for (int c = 0; c < kInPad / 8; ++c) {
+            for (int c = 0; c < 2; ++c) {
                 uint4 v;
                 v.x = pack_bf16(x[8 * c], x[8 * c + 1]);
                 v.y = pack_bf16(x[8 * c + 2], x[8 * c + 3]);
                 v.z = pack_bf16(x[8 * c + 4], x[8 * c + 5]);
                 v.w = pack_bf16(x[8 * c + 6], x[8 * c + 7]);
-                *reinterpret_cast<uint4*>(sm + kSmA1 + cm_offset(t, 8 * c, kInPad)) = v;
+                *reinterpret_cast<uint4*>(sm + kSmA1 + cm_offset(r, 16 * half + 8 * c, kInPad)) = v;
             }
         }
-        // ---- three layers: MMA chain from one thread, epilogue by every thread on its row
+        // ---- three layers: MMA chain from one thread, epilogue by every thread on its row and half
         for (int layer = 0; layer < 3 && ok; ++layer) {
             fence_async_smem();
             tc_before_sync();
@@ -427,29 +511,26 @@ ws_infer_kernel(NbWsNet net, const float* __restrict__ feat, const int32_t* __re
             if (!ok) break;
             if (layer < 2) {
                 const float* bias = layer == 0 ? fb1 : fb2;
-#pragma unroll 1
-                for (int c0 = 0; c0 < kHid; c0 += 16) {
-                    float v[16];
-                    tmem_ld16(tmem + lane_base + (uint32_t)c0, v);
+                const int c0 = 64 * half;
+                float v[64];
+                tmem_ld64(tmem + lane_base + (uint32_t)c0, v);
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) v[j] = silu_fast(v[j] + bias[c0 + j]);
+                for (int j = 0; j < 64; ++j) v[j] = silu_fast(v[j] + bias[c0 + j]);
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        uint4 p;
-                        p.x = pack_bf16(v[8 * h], v[8 * h + 1]);
-                        p.y = pack_bf16(v[8 * h + 2], v[8 * h + 3]);
-                        p.z = pack_bf16(v[8 * h + 4], v[8 * h + 5]);
-                        p.w = pack_bf16(v[8 * h + 6], v[8 * h + 7]);
-                        *reinterpret_cast<uint4*>(sm + kSmA2 + cm_offset(t, c0 + 8 * h, kHid)) = p;
-                    }
+                for (int h = 0; h < 8; ++h) {
+                    uint4 p;
+                    p.x = pack_bf16(v[8 * h], v[8 * h + 1]);
+                    p.y = pack_bf16(v[8 * h + 2], v[8 * h + 3]);
+                    p.z = pack_bf16(v[8 * h + 4], v[8 * h + 5]);
+                    p.w = pack_bf16(v[8 * h + 6], v[8 * h + 7]);
+                    *reinterpret_cast<uint4*>(sm + kSmA2 + cm_offset(r, c0 + 8 * h, kHid)) = p;
                 }
-            } else {
+            } else if (half == 0) {
                 float v[16];
                 tmem_ld16(tmem + lane_base, v);
                 if (row < n) {
                     // c = prior * y; lambda = c / w with lambda_n >= 0 and the tangential part inside
                     // the friction cone |lambda_t| <= mu lambda_n; zero where there is no prior
-                    const float* fr = feat + (size_t)row * kFeat;
                     const float wn = fr[kIn], wt = fr[kIn + 1], prior = fr[kIn + 2], mu = fr[kMuCol];
                     float ln = 0.0f, l1 = 0.0f, l2 = 0.0f;
                     if (prior > 0.0f && wn > 0.0f && wt > 0.0f) {
@@ -470,7 +551,7 @@ ws_infer_kernel(NbWsNet net, const float* __restrict__ feat, const int32_t* __re
             }
         }
         tc_before_sync();
-        __syncthreads();  // tile done: A1 / A2 / tensor memory free for the next tile
+        __syncthreads();  // tile done: A1 / A2 / features / tensor memory free for the next tile
     }
     if (!ok && t == 0) atomicOr(status, (unsigned)NB_STATUS_QUEUE_TIMEOUT);
     tc_before_sync();
@@ -480,7 +561,7 @@ ws_infer_kernel(NbWsNet net, const float* __restrict__ feat, const int32_t* __re
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
-// ---------------------------------------------------------------- training (CUDA cores, fp32)
+// ---------------------------------------------------------------- training
 
 __device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
@@ -760,7 +841,7 @@ cudaError_t nb_launch_ws_infer(const NbWsNet* net, const float* feat, const int3
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int tiles = (cap + kTile - 1) / kTile;
     const int grid = tiles < 2 * sms ? tiles : 2 * sms;  // shared memory fits 2 CTAs per SM
-    ws_infer_kernel<<<grid, kTile, kSmBytes, s>>>(*net, feat, count, cap, out, status);
+    ws_infer_kernel<<<grid, kInferThreads, kSmBytes, s>>>(*net, feat, count, cap, out, status);
     return cudaGetLastError();
 }
 
