@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-warm-start", action="store_true", help="skip the learned-warm-start arm")
+    ap.add_argument("--warm-start-iterations", type=int, default=2)
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="weak: every rank simulates its own --worlds scene; strong: the ranks split one scene")
     return ap.parse_args()
@@ -183,6 +185,89 @@ def algorithmic_bytes(model, layout, n_contacts: float):
     # publish: slot read (80 B), solver record (80 B) and public row + sort key (84 B) written
     publish = n_contacts * (80 + 80 + 84)
     return {"step": step, "collide": collide, "publish": publish}
+
+
+def _window_penetration(graph, stream, model, contacts, state, frames):
+    """Replay `graph` (one frame) `frames` times from the current state; per frame the penetration
+    statistics of the frame's last contacts at the frame's final poses."""
+    import torch
+
+    from newton_custom_contact_b200.metrics import penetration_stats
+
+    out = []
+    for _ in range(frames):
+        with torch.cuda.stream(stream):
+            graph.replay()
+        torch.cuda.synchronize()
+        out.append(penetration_stats(model, contacts, state.body_q))
+    return out
+
+
+def _pen_summary(stats):
+    return {k: float(np.nanmean([p[k] for p in stats]) * 1e3) for k in ("max", "p99", "mean")} | {
+        "worst": float(np.nanmax([p["max"] for p in stats]) * 1e3)}
+
+
+def warm_start_arm(model, dt, substeps, sched, stream, flush, steps, warmup, iterations):
+    """The learned-warm-start form on the same scene: contact matching ("latest", for the previous-lambda
+    feature) + warm start + `iterations` plain iterations per substep.  Timed like the plain form (CUDA
+    graph of one frame, frames WINDOW_START.., L2 flushed between steps); penetration statistics along
+    one pass of the window.  The state is not reset between timed steps: resetting would also have to
+    rewind the matching history and the previous lambdas."""
+    import torch
+
+    from newton_custom_contact_b200 import CollisionPipeline, SolverXPBD
+    from newton_custom_contact_b200.warmstart import WarmStart, WarmStartNet
+
+    net = WarmStartNet.load(os.path.join(ROOT, "newton_custom_contact_b200", "data", "warmstart_c2.npz"),
+                            device=model.device)
+    pipe = CollisionPipeline(model, contact_matching="latest")
+    pipe.set_step_schedule(sched.group_threads, sched.mode)
+    solver = SolverXPBD(model, iterations=iterations)
+    ws = WarmStart(net, iterations=iterations)
+    solver.warm_start = ws
+    a, b = model.state(), model.state()
+    c = pipe.contacts()
+
+    def frame():
+        x, y = a, b
+        for _ in range(substeps):
+            x.clear_forces()
+            pipe.collide(x, c)
+            solver.step(x, y, None, c, dt)
+            x, y = y, x
+
+    with torch.cuda.stream(stream):
+        for _ in range(WINDOW_START):
+            frame()
+    torch.cuda.synchronize()
+    snap = (a.body_q.clone(), a.body_qd.clone())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        frame()
+    torch.cuda.synchronize()
+    fb0 = ws.fallback_count
+    pen = _window_penetration(g, stream, model, c, a, WINDOW_FRAMES)
+    fb1 = ws.fallback_count
+    a.body_q.copy_(snap[0])
+    a.body_qd.copy_(snap[1])
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            g.replay()
+        for k in range(steps):
+            flush.fill_(float(k))
+            starts[k].record(stream)
+            g.replay()
+            ends[k].record(stream)
+    torch.cuda.synchronize()
+    ms = sum(starts[k].elapsed_time(ends[k]) for k in range(steps))
+    del g
+    return {"iterations": iterations, "value": model.world_count * substeps * steps / (ms / 1e3),
+            "ms_per_step": ms / steps, "penetration_mm": _pen_summary(pen),
+            "fallback_world_fraction": (fb1 - fb0) / float(model.world_count * substeps * WINDOW_FRAMES),
+            "contact_matching": "latest", "network": "newton_custom_contact_b200/data/warmstart_c2.npz"}
 
 
 def run_ours(args, rank, world_size, local_rank):
@@ -345,6 +430,15 @@ def run_ours(args, rank, world_size, local_rank):
     status = pipe.status(contacts)
     q = s0.body_q
     finite = bool(torch.isfinite(q).all().item())
+    warm = None
+    if not args.no_warm_start and world_size == 1:
+        # the plain form's penetration along one pass of the same window, then the warm-start form
+        restore()
+        plain_pen = _pen_summary(_window_penetration(g, stream, model, contacts, s0, WINDOW_FRAMES))
+        warm = warm_start_arm(model, dt, substeps, sched, stream, flush, args.steps, args.warmup,
+                              args.warm_start_iterations)
+        warm["plain_penetration_mm"] = plain_pen
+        warm["vs_plain"] = warm["value"] / value
     del g
     if dist:
         dist.barrier()
@@ -397,6 +491,8 @@ def run_ours(args, rank, world_size, local_rank):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if warm is not None:
+        line["warm_start"] = warm
     print(json.dumps(line), flush=True)
 
 
