@@ -98,6 +98,190 @@ __device__ __forceinline__ void flush_queue(const int2* buf, int n, int32_t* cou
     __syncwarp();
 }
 
+// world transform, AABB and full geometry of every shape slot of world w;
+// slot i < nloc is world shape s0 + i, slot nloc + g the global shape g
+__device__ __forceinline__ void stage_shapes(const NbModelDesc& m, const float* __restrict__ body_q, int w, int k,
+                                             float4* lo, float4* hi, float4* geom, int first, int stride) {
+    const int s0 = m.world_shape_start[w];
+    const int nloc = m.world_shape_start[w + 1] - s0;
+    const int ns = nloc + m.global_shape_count;
+    for (int i = first; i < ns; i += stride) {
+        const int s = i < nloc ? s0 + i : m.global_shapes[i - nloc];
+        const int b = m.shape_body[s];
+        TF xs = load_tf(m.shape_transform + 7 * (size_t)s);
+        TF xf = b == -1 ? xs : tf_mul(load_tf(body_q + 7 * (size_t)b), xs);
+        Geom g;
+        shape_geom(g, xf, m.shape_type[s], load_v3(m.shape_scale + 3 * (size_t)s), m.shape_margin[s],
+                   m.shape_gap[s], m.shape_radius[s], b);
+        lo[i] = make_float4(g.lo.x, g.lo.y, g.lo.z, __int_as_float(g.type));
+        hi[i] = make_float4(g.hi.x, g.hi.y, g.hi.z, 0.0f);
+        // global shapes are static: the first world processed stages them
+        if (i < nloc || k == 0) store_geom(geom + 5 * (size_t)s, g);
+    }
+}
+
+// the lane's four pairs q .. q + 3 (q a multiple of 4) of a 128-pair chunk:
+// AABB overlap bits and, among the hits, the pairs the analytic path finishes
+__device__ __forceinline__ void test_pairs(uint4 pk, int q, int p0, int p1, const float4* lo, const float4* hi, int ns,
+                                           uint32_t* status, unsigned& hit, unsigned& easy) {
+    const unsigned pw[4] = {pk.x, pk.y, pk.z, pk.w};
+    hit = 0u;
+    easy = 0u;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int p = q + r;
+        if (p < p0 || p >= p1) continue;
+        const int la = (int)(pw[r] & 0xFFFFu), lb = (int)(pw[r] >> 16);
+        // slots index shared memory: never trust them blindly
+        if (la >= ns || lb >= ns) {
+            atomicOr(status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
+            continue;
+        }
+        if (la == lb) continue;
+        const float4 al = lo[la], ah = hi[la], bl = lo[lb], bh = hi[lb];
+        const float c = 0.0f + 0.0f;
+        if (al.x <= bh.x + c && ah.x >= bl.x - c && al.y <= bh.y + c && ah.y >= bl.y - c && al.z <= bh.z + c &&
+            ah.z >= bl.z - c) {
+            hit |= 1u << r;
+            if (analytic_pair(__float_as_int(al.w), __float_as_int(bl.w))) easy |= 1u << r;
+        }
+    }
+}
+
+// per-warp staging of narrow-phase queue items (pushed with one atomic per flush;
+// queue order is free: every item writes only its own candidate's slots)
+struct QueueStage {
+    int2* qa;
+    int2* qg;
+    int nqa, nqg;  // warp-uniform fill levels
+};
+
+// writes a chunk's hits (masks of this lane, warp-wide offsets) as candidates
+// cand_base + running index, in pair order, and stages their queue items
+__device__ __forceinline__ void emit_chunk(const NbContactSeg& seg, int2* queue, long long gjk_back, QueueStage& st,
+                                           int q, unsigned hit, unsigned easy, int w, int cand_base, int lane,
+                                           int& tot_h) {
+    int tot_a;
+    const int nh = __popc(hit), na = __popc(easy);
+    const int off_h = warp_exclusive_scan(nh, lane, tot_h);
+    const int off_a = warp_exclusive_scan(na, lane, tot_a);
+    const int off_g = off_h - off_a, tot_g = tot_h - tot_a;
+    // make room in the staging buffers (warp-uniform decisions)
+    if (st.nqa + tot_a > kQB) {
+        flush_queue(st.qa, st.nqa, &seg.work_counter[2], queue, 0, lane);
+        st.nqa = 0;
+    }
+    if (st.nqg + tot_g > kQB) {
+        flush_queue(st.qg, st.nqg, &seg.work_counter[3], queue, gjk_back, lane);
+        st.nqg = 0;
+    }
+    int ih = 0, ia = 0, ig = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        if (!(hit >> r & 1u)) continue;
+        const int c = cand_base + off_h + ih++;
+        seg.cand[c] = q + r;
+        if (easy >> r & 1u) st.qa[st.nqa + off_a + ia++] = make_int2(c, w);
+        else st.qg[st.nqg + off_g + ig++] = make_int2(c, w);
+    }
+    st.nqa += tot_a;
+    st.nqg += tot_g;
+    __syncwarp();
+}
+
+// one world by one warp: shapes, then its pair chunks in order (the next chunk's
+// pairs are loaded while this chunk is tested)
+__device__ void world_by_warp(const NbModelDesc& m, const float* __restrict__ body_q, const NbContactSeg& seg, int k,
+                              float4* lo, float4* hi, QueueStage& st, int lane) {
+    const uint4* packed = reinterpret_cast<const uint4*>(m.pair_shapes);
+    int2* queue = reinterpret_cast<int2*>(seg.queue);
+    const long long gjk_back = 2 * (long long)m.pair_count - 1;
+    const int w = m.world_order[k];
+    const int ns = m.world_shape_start[w + 1] - m.world_shape_start[w] + m.global_shape_count;
+    stage_shapes(m, body_q, w, k, lo, hi, reinterpret_cast<float4*>(seg.geom), lane, 32);
+    __syncwarp();
+    const int p0 = m.world_pair_start[w], p1 = m.world_pair_start[w + 1];
+    int ncand = 0;
+    int base = p0 & ~3;
+    uint4 nxt = make_uint4(0u, 0u, 0u, 0u);
+    if (base + 4 * lane < p1) nxt = packed[(base + 4 * lane) >> 2];
+    for (; base < p1; base += 128) {
+        const int q = base + 4 * lane;  // multiple of 4: 16-byte aligned
+        const uint4 pk = nxt;
+        if (q + 128 < p1) nxt = packed[(q + 128) >> 2];
+        unsigned hit, easy;
+        test_pairs(pk, q, p0, p1, lo, hi, ns, seg.status, hit, easy);
+        int tot_h;
+        emit_chunk(seg, queue, gjk_back, st, q, hit, easy, w, p0 + ncand, lane, tot_h);
+        ncand += tot_h;
+    }
+    if (lane == 0) {
+        seg.cand_count[w] = ncand;
+        seg.world_count[w] = 0;
+    }
+    __syncwarp();
+}
+
+// one large world by the whole CTA: shapes staged once, the pair chunks split
+// into one contiguous run per warp; pass 1 counts each run's hits, a scan over
+// the warps gives every run its first candidate index, pass 2 re-tests (a few
+// comparisons per pair) and writes -- the candidates stay in pair order
+__device__ void world_by_cta(const NbModelDesc& m, const float* __restrict__ body_q, const NbContactSeg& seg, int k,
+                             float4* lo, float4* hi, QueueStage& st, int* s_run, int warp, int lane) {
+    const uint4* packed = reinterpret_cast<const uint4*>(m.pair_shapes);
+    int2* queue = reinterpret_cast<int2*>(seg.queue);
+    const long long gjk_back = 2 * (long long)m.pair_count - 1;
+    const int w = m.world_order[k];
+    const int ns = m.world_shape_start[w + 1] - m.world_shape_start[w] + m.global_shape_count;
+    stage_shapes(m, body_q, w, k, lo, hi, reinterpret_cast<float4*>(seg.geom), threadIdx.x, kBT);
+    __syncthreads();
+    const int p0 = m.world_pair_start[w], p1 = m.world_pair_start[w + 1];
+    const int cbase = p0 & ~3;
+    const int nchunks = (p1 - cbase + 127) / 128;
+    constexpr int kWarps = kBT / 32;
+    const int per = (nchunks + kWarps - 1) / kWarps;
+    const int c0 = warp * per, c1 = min(nchunks, c0 + per);
+    int count = 0;
+    for (int c = c0; c < c1; ++c) {
+        const int q = cbase + 128 * c + 4 * lane;
+        const uint4 pk = q < p1 ? packed[q >> 2] : make_uint4(0u, 0u, 0u, 0u);
+        unsigned hit, easy;
+        test_pairs(pk, q, p0, p1, lo, hi, ns, seg.status, hit, easy);
+        count += __popc(hit);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(kFull, count, o);
+    if (lane == 0) s_run[warp] = count;
+    __syncthreads();
+    int first = 0, total = 0;
+#pragma unroll
+    for (int i = 0; i < kWarps; ++i) {
+        const int v = s_run[i];
+        if (i < warp) first += v;
+        total += v;
+    }
+    int ncand = 0;
+    for (int c = c0; c < c1; ++c) {
+        const int q = cbase + 128 * c + 4 * lane;
+        const uint4 pk = q < p1 ? packed[q >> 2] : make_uint4(0u, 0u, 0u, 0u);
+        unsigned hit, easy;
+        test_pairs(pk, q, p0, p1, lo, hi, ns, seg.status, hit, easy);
+        int tot_h;
+        emit_chunk(seg, queue, gjk_back, st, q, hit, easy, w, p0 + first + ncand, lane, tot_h);
+        ncand += tot_h;
+    }
+    if (threadIdx.x == 0) {
+        seg.cand_count[w] = total;
+        seg.world_count[w] = 0;
+    }
+    __syncthreads();  // shapes and run counts are reused by the next world
+}
+
+constexpr int kCtaWorldPairs = 2048;  // worlds with at least this many pairs are shared by a whole CTA
+
+// Worlds are taken in decreasing cost.  While the next world is large, the CTA
+// takes it together (world_by_cta); from the first small world on, every warp
+// takes worlds on its own (world_by_warp).
 __global__ void __launch_bounds__(kBT)
 broadphase_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
     extern __shared__ __align__(16) float4 sbox[];
@@ -105,106 +289,37 @@ broadphase_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg 
     const int nsh = m.max_world_shapes;
     float4* lo = sbox + (size_t)warp * 2 * nsh;   // (lo.xyz, type)
     float4* hi = lo + nsh;                         // (hi.xyz, 0)
-    float4* geom = reinterpret_cast<float4*>(seg.geom);
-    int2* queue = reinterpret_cast<int2*>(seg.queue);
-    // pairs packed as (slot_a | slot_b << 16), read four per lane with one 16-byte load
-    const uint4* packed = reinterpret_cast<const uint4*>(m.pair_shapes);
-    const int P = m.pair_count;
-    // narrow-phase queue items are staged per warp and pushed with one atomic per
-    // flush (queue order is free: every item writes only its own candidate's slots)
     __shared__ int2 s_qa[kBT / 32][kQB], s_qg[kBT / 32][kQB];
-    int2* qa_buf = s_qa[warp];
-    int2* qg_buf = s_qg[warp];
-    int nqa = 0, nqg = 0;  // warp-uniform fill levels
+    __shared__ int s_k, s_run[kBT / 32];
+    QueueStage st{s_qa[warp], s_qg[warp], 0, 0};
+    int small_k = -1;  // the first small world this CTA took: warp 0 does it
     for (;;) {
-        int k = 0;
-        if (lane == 0) k = atomicAdd(&seg.work_counter[0], 1);
-        k = __shfl_sync(kFull, k, 0);
+        if (threadIdx.x == 0) s_k = atomicAdd(&seg.work_counter[0], 1);
+        __syncthreads();
+        const int k = s_k;
+        __syncthreads();
         if (k >= m.world_count) break;
         const int w = m.world_order[k];
-        const int s0 = m.world_shape_start[w];
-        const int nloc = m.world_shape_start[w + 1] - s0;
-        const int ns = nloc + m.global_shape_count;
-        for (int i = lane; i < ns; i += 32) {
-            const int s = i < nloc ? s0 + i : m.global_shapes[i - nloc];
-            const int b = m.shape_body[s];
-            TF xs = load_tf(m.shape_transform + 7 * (size_t)s);
-            TF xf = b == -1 ? xs : tf_mul(load_tf(body_q + 7 * (size_t)b), xs);
-            Geom g;
-            shape_geom(g, xf, m.shape_type[s], load_v3(m.shape_scale + 3 * (size_t)s), m.shape_margin[s],
-                       m.shape_gap[s], m.shape_radius[s], b);
-            lo[i] = make_float4(g.lo.x, g.lo.y, g.lo.z, __int_as_float(g.type));
-            hi[i] = make_float4(g.hi.x, g.hi.y, g.hi.z, 0.0f);
-            // global shapes are static: the first world processed stages them
-            if (i < nloc || k == 0) store_geom(geom + 5 * (size_t)s, g);
+        if (m.world_pair_start[w + 1] - m.world_pair_start[w] < kCtaWorldPairs) {
+            small_k = k;
+            break;
         }
-        __syncwarp();
-        const int p0 = m.world_pair_start[w], p1 = m.world_pair_start[w + 1];
-        int ncand = 0;
-        // the next chunk's pairs are loaded while this chunk is tested
-        int base = p0 & ~3;
-        uint4 nxt = make_uint4(0u, 0u, 0u, 0u);
-        if (base + 4 * lane < p1) nxt = packed[(base + 4 * lane) >> 2];
-        for (; base < p1; base += 128) {
-            const int q = base + 4 * lane;  // multiple of 4: 16-byte aligned
-            const uint4 pk = nxt;
-            if (q + 128 < p1) nxt = packed[(q + 128) >> 2];
-            const unsigned pw[4] = {pk.x, pk.y, pk.z, pk.w};
-            unsigned hit = 0u, easy = 0u;
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const int p = q + r;
-                if (p < p0 || p >= p1) continue;
-                const int la = (int)(pw[r] & 0xFFFFu), lb = (int)(pw[r] >> 16);
-                // slots index shared memory: never trust them blindly
-                if (la >= ns || lb >= ns) {
-                    atomicOr(seg.status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
-                    continue;
-                }
-                if (la == lb) continue;
-                const float4 al = lo[la], ah = hi[la], bl = lo[lb], bh = hi[lb];
-                const float c = 0.0f + 0.0f;
-                if (al.x <= bh.x + c && ah.x >= bl.x - c && al.y <= bh.y + c && ah.y >= bl.y - c &&
-                    al.z <= bh.z + c && ah.z >= bl.z - c) {
-                    hit |= 1u << r;
-                    if (analytic_pair(__float_as_int(al.w), __float_as_int(bl.w))) easy |= 1u << r;
-                }
-            }
-            int tot_h, tot_a;
-            const int nh = __popc(hit), na = __popc(easy);
-            const int off_h = warp_exclusive_scan(nh, lane, tot_h);
-            const int off_a = warp_exclusive_scan(na, lane, tot_a);
-            const int off_g = off_h - off_a, tot_g = tot_h - tot_a;
-            // make room in the staging buffers (warp-uniform decisions)
-            if (nqa + tot_a > kQB) {
-                flush_queue(qa_buf, nqa, &seg.work_counter[2], queue, 0, lane);
-                nqa = 0;
-            }
-            if (nqg + tot_g > kQB) {
-                flush_queue(qg_buf, nqg, &seg.work_counter[3], queue, 2 * (long long)P - 1, lane);
-                nqg = 0;
-            }
-            int ih = 0, ia = 0, ig = 0;
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                if (!(hit >> r & 1u)) continue;
-                const int c = p0 + ncand + off_h + ih++;
-                seg.cand[c] = q + r;
-                if (easy >> r & 1u) qa_buf[nqa + off_a + ia++] = make_int2(c, w);
-                else qg_buf[nqg + off_g + ig++] = make_int2(c, w);
-            }
-            ncand += tot_h;
-            nqa += tot_a;
-            nqg += tot_g;
-            __syncwarp();
-        }
-        if (lane == 0) {
-            seg.cand_count[w] = ncand;
-            seg.world_count[w] = 0;
+        // the CTA shares warp 0's shape arrays for this world
+        world_by_cta(m, body_q, seg, k, sbox, sbox + nsh, st, s_run, warp, lane);
+    }
+    if (small_k >= 0 && warp == 0) world_by_warp(m, body_q, seg, small_k, lo, hi, st, lane);
+    if (small_k >= 0) {
+        for (;;) {
+            int k = 0;
+            if (lane == 0) k = atomicAdd(&seg.work_counter[0], 1);
+            k = __shfl_sync(kFull, k, 0);
+            if (k >= m.world_count) break;
+            world_by_warp(m, body_q, seg, k, lo, hi, st, lane);
         }
     }
-    flush_queue(qa_buf, nqa, &seg.work_counter[2], queue, 0, lane);
-    flush_queue(qg_buf, nqg, &seg.work_counter[3], queue, 2 * (long long)P - 1, lane);
+    int2* queue = reinterpret_cast<int2*>(seg.queue);
+    flush_queue(st.qa, st.nqa, &seg.work_counter[2], queue, 0, lane);
+    flush_queue(st.qg, st.nqg, &seg.work_counter[3], queue, 2 * (long long)m.pair_count - 1, lane);
 }
 
 struct NarrowItem {
