@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 9
+#define NB_ABI_VERSION 10
 
 enum {
     NB_OK = 0,
@@ -431,6 +431,11 @@ typedef struct NbAdjointIO {
     double* grad_acc;            /* [B*13] scratch */
     int64_t* delta_acc;          /* [B*6] scratch */
     int32_t* count_acc;          /* [B] scratch */
+    int32_t* active;             /* [iterations * active_capacity * 2] scratch: (record, world) of active contacts */
+    int32_t* active_count;       /* [iterations] scratch */
+    int32_t active_capacity;     /* active contacts per iteration (>= the contact count; overflow sets
+                                    NB_STATUS_CONTACT_OVERFLOW) */
+    int32_t pad0;
     uint32_t* status;            /* [1] NB_STATUS_* bits (sticky) */
 } NbAdjointIO;
 int nb_xpbd_step_adjoint(const NbModelDesc* model, const NbXpbdParams* params, const NbAdjointIO* io,

@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 9
+NB_ABI_VERSION = 10
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -264,6 +264,10 @@ class NbAdjointIO(C.Structure):
         ("grad_acc", _fp),
         ("delta_acc", _fp),
         ("count_acc", _fp),
+        ("active", _fp),
+        ("active_count", _fp),
+        ("active_capacity", C.c_int32),
+        ("pad0", C.c_int32),
         ("status", _fp),
     ]
 

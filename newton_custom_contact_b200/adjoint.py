@@ -43,10 +43,10 @@ class SubstepAdjoint:
         self.model = solver.model
         self._bufs = None
 
-    def _alloc(self):
+    def _alloc(self, active_capacity: int = 0):
         m, K = self.model, self.solver.iterations
         B = max(m.body_count, 1)
-        key = (B, K)
+        key = (B, K, active_capacity)
         if self._bufs is None or self._bufs["key"] != key:
             dev = m.device
             f = dict(dtype=torch.float32, device=dev)
@@ -58,7 +58,11 @@ class SubstepAdjoint:
                 "grad_acc": torch.empty(B * 13, dtype=torch.float64, device=dev),
                 "delta_acc": torch.empty(B * 6, dtype=torch.int64, device=dev),
                 "count_acc": torch.empty(B, dtype=torch.int32, device=dev),
-                "status": torch.zeros(1, dtype=torch.int32, device=dev),
+                # active contacts per iteration: (record, world), at most every published contact
+                "active": torch.empty(max(K, 1) * max(active_capacity, 1) * 2, dtype=torch.int32, device=dev),
+                "active_count": torch.zeros(max(K, 1), dtype=torch.int32, device=dev),
+                "active_capacity": active_capacity,
+                "status": torch.zeros(1, dtype=torch.int32, device=dev) if self._bufs is None else self._bufs["status"],
             }
         return self._bufs
 
@@ -75,7 +79,7 @@ class SubstepAdjoint:
         for name, t, shape in (("body_q", body_q, (B, 7)), ("body_qd", body_qd, (B, 6)), ("body_f", body_f, (B, 6)),
                                ("grad_q_out", grad_q_out, (B, 7)), ("grad_qd_out", grad_qd_out, (B, 6))):
             solver._check_state(name, t, shape)
-        b = self._alloc()
+        b = self._alloc(contacts.rigid_contact_max if contacts is not None else 0)
         gq, gqd, gf = torch.empty_like(body_q), torch.empty_like(body_qd), torch.empty_like(body_f)
         io = NbAdjointIO()
         io.body_q_in, io.body_qd_in, io.body_f_in = ptr(body_q), ptr(body_qd), ptr(body_f)
@@ -83,8 +87,10 @@ class SubstepAdjoint:
         io.grad_q_in, io.grad_qd_in, io.grad_f_in = ptr(gq), ptr(gqd), ptr(gf)
         if forward_out is not None:
             io.body_q_out, io.body_qd_out = ptr(forward_out[0]), ptr(forward_out[1])
-        for k in ("tape_state", "tape_delta", "tape_weight", "grad_acc", "delta_acc", "count_acc", "status"):
+        for k in ("tape_state", "tape_delta", "tape_weight", "grad_acc", "delta_acc", "count_acc", "active",
+                  "active_count", "status"):
             setattr(io, k, ptr(b[k]))
+        io.active_capacity = b["active_capacity"]
         pipe, desc = solver._desc_for(contacts)
         if contacts is not None:
             if contacts._seg is None or not contacts._seg_valid:
@@ -143,7 +149,7 @@ class Rollout:
 
     def backward(self, checkpoints, f, substeps: int, gq, gqd):
         gf_total = torch.zeros_like(f)
-        self.adjoint._alloc()["status"].zero_()
+        self.adjoint._alloc(self.contacts.rigid_contact_max)["status"].zero_()
         n_seg = len(checkpoints)
         for s in range(n_seg - 1, -1, -1):
             start = s * self.checkpoint_every

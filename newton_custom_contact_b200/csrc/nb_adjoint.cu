@@ -8,17 +8,19 @@
 //   iteration it:  D_it(i) = sum over active contacts k of body i: C_k(S_it(a_k), S_it(b_k))
 //                  S_it+1(i) = A(S_it(i), D_it(i), w_it(i))     (apply_body_delta, weight 1/count)
 //
-// One CTA per world.  The forward pass re-runs the substep in FP32 with the
-// solver's formulas and exact fixed-point delta sums and records S_0..S_K,
-// D_it and w_it (a tape in global scratch).  The reverse pass walks the
-// iterations backwards: per body the vector-Jacobian product of A gives the
-// cotangents of S_it(i) and of D_it(i); per active contact the VJP of C_k
-// adds into the cotangents of its two bodies' poses and angular velocities;
-// finally the VJP of the integration gives d/d state_in and d/d body_f.
-// Local Jacobians (A: 19 inputs, C_k: 20, integration: 19) come from the
-// same generic code evaluated on forward-mode dual numbers, 4 directions per
-// pass; the global sweep is reverse mode.  Cotangent sums over contacts use
-// FP64 atomics.
+// The forward pass (adjoint_forward_kernel, one CTA per world) re-runs the
+// substep in FP32 with the solver's formulas and exact fixed-point delta sums
+// and records S_0..S_K, D_it, w_it and each iteration's active contacts (a
+// tape in global scratch).  The reverse pass walks the iterations backwards
+// with two flat kernels per iteration over all worlds at once:
+// adjoint_bodies_kernel (per body, the vector-Jacobian product of the body
+// update: cotangents of S_it(i) and of D_it(i)) and adjoint_contacts_kernel
+// (per active contact, the VJP of C_k added into its two bodies' pose and
+// angular-velocity cotangents with FP64 atomics); adjoint_integrate_kernel
+// finally gives d/d state_in and d/d body_f.  The body update and the
+// integration are reversed by hand; a contact's local Jacobian (20 inputs)
+// comes from the same generic code evaluated on forward-mode dual numbers,
+// 4 directions per pass.
 //
 // Held fixed (piecewise constant in the reference's own gradient as well):
 // the contact set and each record's body-frame points, offsets, normal and
@@ -235,7 +237,7 @@ struct BodyT {
 
 // integrate_bodies (newton/_src/solvers/solver.py:50-94)
 template <class T>
-__device__ void integrate_g(BodyT<T>& b, const V3T<T>& f0, const V3T<T>& t0, V3 com, const M33& I, float inv_mass,
+__device__ __forceinline__ void integrate_g(BodyT<T>& b, const V3T<T>& f0, const V3T<T>& t0, V3 com, const M33& I, float inv_mass,
                             const M33& inv_I, V3 g, float angular_damping, float dt) {
     const V3T<T> x0 = b.p, w0 = b.w, v0 = b.v;
     const Q4T<T> r0 = b.r;
@@ -259,7 +261,7 @@ __device__ void integrate_g(BodyT<T>& b, const V3T<T>& f0, const V3T<T>& t0, V3 
 
 // apply_body_deltas (newton/_src/solvers/xpbd/kernels.py:809-878), weight resolved
 template <class T>
-__device__ void apply_delta_g(BodyT<T>& b, const V3T<T>& dlin, const V3T<T>& dang, float weight, V3 com,
+__device__ __forceinline__ void apply_delta_g(BodyT<T>& b, const V3T<T>& dlin, const V3T<T>& dang, float weight, V3 com,
                               const M33& I, float inv_m, const M33& inv_I, float dt) {
     if (inv_m == 0.0f) return;
     const V3T<T> v0 = b.v, w0 = b.w, p0 = b.p;
@@ -291,7 +293,7 @@ __device__ void apply_delta_g(BodyT<T>& b, const V3T<T>& dlin, const V3T<T>& dan
 // free in a differentiated world -- the joint pass's apply of a zero delta,
 // which only renormalises (solver_xpbd.py:554-630 as the solver kernel runs it)
 template <class T>
-__device__ void body_update_g(BodyT<T>& b, const V3T<T>& dlin, const V3T<T>& dang, float weight, bool contacts,
+__device__ __forceinline__ void body_update_g(BodyT<T>& b, const V3T<T>& dlin, const V3T<T>& dang, float weight, bool contacts,
                               bool joints, V3 com, const M33& I, float inv_m, const M33& inv_I, float dt) {
     if (contacts) apply_delta_g(b, dlin, dang, weight, com, I, inv_m, inv_I, dt);
     if (joints) {
@@ -302,7 +304,7 @@ __device__ void body_update_g(BodyT<T>& b, const V3T<T>& dlin, const V3T<T>& dan
 
 // compute_contact_constraint_delta (kernels.py:1945-1979)
 template <class T>
-__device__ T constraint_delta_g(const T& err, const Q4T<T>& qa, const Q4T<T>& qb, float m_inv_a, float m_inv_b,
+__device__ __forceinline__ T constraint_delta_g(const T& err, const Q4T<T>& qa, const Q4T<T>& qb, float m_inv_a, float m_inv_b,
                                 const M33& Ia, const M33& Ib, const V3T<T>& la, const V3T<T>& lb,
                                 const V3T<T>& aa, const V3T<T>& ab, float relaxation, float dt) {
     T denom = vdot(la, la) * m_inv_a;
@@ -341,7 +343,7 @@ struct ContactC {
 // solve_body_contact_positions (kernels.py:2062-2298) for one contact:
 // deltas (linear, angular) of A and B; false when the contact is inactive
 template <class T>
-__device__ bool contact_g(const ContactC& c, const BodyT<T>& A, const BodyT<T>& B, float relaxation, float dt,
+__device__ __forceinline__ bool contact_g(const ContactC& c, const BodyT<T>& A, const BodyT<T>& B, float relaxation, float dt,
                           V3T<T>& lin_da, V3T<T>& ang_da, V3T<T>& lin_db, V3T<T>& ang_db) {
     const V3T<T> bxa0 = qrott(A.r, vc<T>(c.p0)) + A.p;
     const V3T<T> bxb0 = qrott(B.r, vc<T>(c.p1)) + B.p;
@@ -447,60 +449,202 @@ __device__ __forceinline__ Dual<N> seed(float x, int j, int j0) {
 
 // ---------------------------------------------------------------- local vector-Jacobian products
 
-// body update: inputs body (13) + dlin (3) + dang (3); outputs body (13)
+// ---- hand-written reverse mode of the per-body pieces (float)
+
+struct Q4f {
+    float x, y, z, w;
+};
+
+// cotangent of q for v' = qrot(q, v) = v (2w^2 - 1) + 2 q (q.v) + 2 w (q x v) (any q, unit or not);
+// `sgn` = -1 for qrot_inv (the cross term flips)
+__device__ __forceinline__ void qrot_vjp_q(Q4 q, V3 v, V3 g, float sgn, Q4f& gq) {
+    const V3 qv{q.x, q.y, q.z};
+    const float qdv = dot(qv, v), qdg = dot(qv, g);
+    const V3 vxg = cross(v, g);
+    gq.x += 2.0f * qdv * g.x + 2.0f * v.x * qdg + sgn * 2.0f * q.w * vxg.x;
+    gq.y += 2.0f * qdv * g.y + 2.0f * v.y * qdg + sgn * 2.0f * q.w * vxg.y;
+    gq.z += 2.0f * qdv * g.z + 2.0f * v.z * qdg + sgn * 2.0f * q.w * vxg.z;
+    gq.w += dot(g, add(mul(v, 4.0f * q.w), mul(cross(qv, v), 2.0f * sgn)));
+}
+// cotangents of a and b for m = qmul(a, b)
+__device__ __forceinline__ void qmul_vjp(Q4 a, Q4 b, Q4f g, Q4f& ga, Q4f& gb) {
+    ga.x += g.x * b.w - g.y * b.z + g.z * b.y - g.w * b.x;
+    ga.y += g.x * b.z + g.y * b.w - g.z * b.x - g.w * b.y;
+    ga.z += -g.x * b.y + g.y * b.x + g.z * b.w - g.w * b.z;
+    ga.w += g.x * b.x + g.y * b.y + g.z * b.z + g.w * b.w;
+    gb.x += g.x * a.w + g.y * a.z - g.z * a.y - g.w * a.x;
+    gb.y += -g.x * a.z + g.y * a.w + g.z * a.x - g.w * a.y;
+    gb.z += g.x * a.y - g.y * a.x + g.z * a.w - g.w * a.z;
+    gb.w += g.x * a.x + g.y * a.y + g.z * a.z + g.w * a.w;
+}
+// cotangent of u for q = normalize(u) (the solver's qnormalize; zero u maps to the identity)
+__device__ __forceinline__ Q4f qnormalize_vjp(Q4 u, Q4f g) {
+    const float l = sqrtf(qdot(u, u));
+    if (!(l > 0.0f)) return Q4f{0.0f, 0.0f, 0.0f, 0.0f};
+    const Q4 q{u.x / l, u.y / l, u.z / l, u.w / l};
+    const float d = q.x * g.x + q.y * g.y + q.z * g.z + q.w * g.w;
+    return Q4f{(g.x - q.x * d) / l, (g.y - q.y * d) / l, (g.z - q.z * d) / l, (g.w - q.w * d) / l};
+}
+// cotangents of x and y for c = x cross y
+__device__ __forceinline__ void cross_vjp(V3 x, V3 y, V3 g, V3& gx, V3& gy) {
+    gx = add(gx, cross(y, g));
+    gy = add(gy, cross(g, x));
+}
+
+// apply_delta_g(float) reversed: cotangents of the body state (13) and of the delta (6)
+__device__ void apply_delta_rev(const float* s, const float* dl, float weight, V3 com, const M33& I, float inv_m,
+                                const M33& inv_I, float dt, const float* gout, float* gs, float* gd) {
+    for (int k = 0; k < 13; ++k) gs[k] = gout[k];
+    for (int k = 0; k < 6; ++k) gd[k] = 0.0f;
+    if (inv_m == 0.0f) return;
+    // forward recomputation
+    const V3 p0{s[0], s[1], s[2]}, v0{s[7], s[8], s[9]}, w0{s[10], s[11], s[12]};
+    const Q4 q0{s[3], s[4], s[5], s[6]};
+    const float c1 = inv_m * weight;
+    const V3 dp = mul(V3{dl[0], dl[1], dl[2]}, c1);
+    const V3 dq = mul(V3{dl[3], dl[4], dl[5]}, weight);
+    const V3 wb = qrot_inv(q0, w0);
+    const V3 z = qrot_inv(q0, dq);
+    const V3 dwb = mv(inv_I, z);
+    const V3 y1 = mv(I, add(wb, dwb)), y2 = mv(I, dwb);
+    const V3 tb = add(cross(dwb, y1), cross(wb, y2));
+    const M33 dtiI = mscale(dt, inv_I);
+    const V3 u = sub(dwb, mv(dtiI, tb));
+    const V3 dw1 = qrot(q0, u);
+    const Q4 dq4{dw1.x * dt * 0.5f, dw1.y * dt * 0.5f, dw1.z * dt * 0.5f, 0.0f};
+    const Q4 mq = qmul(dq4, q0);
+    const Q4 q1u{q0.x + mq.x, q0.y + mq.y, q0.z + mq.z, q0.w + mq.w};
+    const Q4 q1 = qnormalize(q1u);
+    const V3 v1 = add(v0, dp), w1 = add(w0, dw1);
+    // reverse
+    V3 gp1{gout[0], gout[1], gout[2]}, gv1{gout[7], gout[8], gout[9]}, gw1{gout[10], gout[11], gout[12]};
+    Q4f gq1{gout[3], gout[4], gout[5], gout[6]};
+    if (length(v1) < 1e-4f) gv1 = V3{0.0f, 0.0f, 0.0f};
+    if (length(w1) < 1e-4f) gw1 = V3{0.0f, 0.0f, 0.0f};
+    V3 gv0 = gv1, gdp = gv1, gw0 = gw1, gdw1 = gw1;
+    // p1 = p0 + qrot(q0, com) + dp dt - qrot(q1, com)
+    V3 gp0 = gp1;
+    gdp = add(gdp, mul(gp1, dt));
+    Q4f gq0{0.0f, 0.0f, 0.0f, 0.0f};
+    qrot_vjp_q(q0, com, gp1, 1.0f, gq0);
+    qrot_vjp_q(q1, com, neg(gp1), 1.0f, gq1);
+    // q1 = normalize(q0 + qmul(dq4, q0))
+    const Q4f gq1u = qnormalize_vjp(q1u, gq1);
+    gq0.x += gq1u.x; gq0.y += gq1u.y; gq0.z += gq1u.z; gq0.w += gq1u.w;
+    Q4f gdq4{0.0f, 0.0f, 0.0f, 0.0f};
+    qmul_vjp(dq4, q0, gq1u, gdq4, gq0);
+    gdw1 = add(gdw1, mul(V3{gdq4.x, gdq4.y, gdq4.z}, dt * 0.5f));
+    // dw1 = qrot(q0, u), u = dwb - dt inv_I tb
+    qrot_vjp_q(q0, u, gdw1, 1.0f, gq0);
+    const V3 gu = qrot_inv(q0, gdw1);
+    V3 gdwb = gu;
+    const V3 gtb = neg(mtv(dtiI, gu));
+    // tb = dwb x (I (wb + dwb)) + wb x (I dwb)
+    V3 gwb{0.0f, 0.0f, 0.0f}, gy1{0.0f, 0.0f, 0.0f}, gy2{0.0f, 0.0f, 0.0f};
+    cross_vjp(dwb, y1, gtb, gdwb, gy1);
+    cross_vjp(wb, y2, gtb, gwb, gy2);
+    const V3 ty1 = mtv(I, gy1), ty2 = mtv(I, gy2);
+    gwb = add(gwb, ty1);
+    gdwb = add(gdwb, add(ty1, ty2));
+    // dwb = inv_I qrot_inv(q0, dq)
+    const V3 gz = mtv(inv_I, gdwb);
+    qrot_vjp_q(q0, dq, gz, -1.0f, gq0);
+    const V3 gdq = qrot(q0, gz);
+    // wb = qrot_inv(q0, w0)
+    qrot_vjp_q(q0, w0, gwb, -1.0f, gq0);
+    gw0 = add(gw0, qrot(q0, gwb));
+    gs[0] = gp0.x; gs[1] = gp0.y; gs[2] = gp0.z;
+    gs[3] = gq0.x; gs[4] = gq0.y; gs[5] = gq0.z; gs[6] = gq0.w;
+    gs[7] = gv0.x; gs[8] = gv0.y; gs[9] = gv0.z;
+    gs[10] = gw0.x; gs[11] = gw0.y; gs[12] = gw0.z;
+    gd[0] = gdp.x * c1; gd[1] = gdp.y * c1; gd[2] = gdp.z * c1;
+    gd[3] = gdq.x * weight; gd[4] = gdq.y * weight; gd[5] = gdq.z * weight;
+}
+
+// body update (body_update_g) reversed: the optional zero-delta renormalisation,
+// then the weighted apply
 __device__ void vjp_apply(const float* s, const float* dl, float weight, bool contacts, bool joints, V3 com,
                           const M33& I, float inv_m, const M33& inv_I, float dt, const float* gout, float* gs,
                           float* gd) {
-    for (int j0 = 0; j0 < 19; j0 += kDirs) {
-        BodyT<Dual<kDirs>> b;
-        Dual<kDirs> x[19];
-        for (int j = 0; j < 13; ++j) x[j] = seed<kDirs>(s[j], j, j0);
-        for (int j = 0; j < 6; ++j) x[13 + j] = seed<kDirs>(dl[j], 13 + j, j0);
-        b.p = {x[0], x[1], x[2]};
-        b.r = {x[3], x[4], x[5], x[6]};
-        b.v = {x[7], x[8], x[9]};
-        b.w = {x[10], x[11], x[12]};
-        body_update_g(b, V3T<Dual<kDirs>>{x[13], x[14], x[15]}, V3T<Dual<kDirs>>{x[16], x[17], x[18]}, weight,
-                      contacts, joints, com, I, inv_m, inv_I, dt);
-        Dual<kDirs> o[13];
-        body_out(b, o);
-        for (int k = 0; k < kDirs && j0 + k < 19; ++k) {
-            float acc = 0.0f;
-            for (int i = 0; i < 13; ++i) acc += gout[i] * o[i].d[k];
-            if (j0 + k < 13) gs[j0 + k] = acc;
-            else gd[j0 + k - 13] = acc;
-        }
+    float g[13];
+    for (int k = 0; k < 13; ++k) g[k] = gout[k];
+    float mid[13];
+    for (int k = 0; k < 13; ++k) mid[k] = s[k];
+    if (contacts) {
+        BodyT<float> b = body_from<float>(s);
+        apply_delta_g(b, V3T<float>{dl[0], dl[1], dl[2]}, V3T<float>{dl[3], dl[4], dl[5]}, weight, com, I, inv_m,
+                      inv_I, dt);
+        body_to(b, mid);
+    }
+    if (joints) {
+        const float zero[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        float gz[6];
+        apply_delta_rev(mid, zero, 1.0f, com, I, inv_m, inv_I, dt, gout, g, gz);
+    }
+    if (contacts) {
+        apply_delta_rev(s, dl, weight, com, I, inv_m, inv_I, dt, g, gs, gd);
+    } else {
+        for (int k = 0; k < 13; ++k) gs[k] = g[k];
+        for (int k = 0; k < 6; ++k) gd[k] = 0.0f;
     }
 }
 
-// integrate: inputs body (13) + force (3) + torque (3); outputs body (13)
+// integrate_g(float) reversed: cotangents of the state (13) and of the force / torque (6)
 __device__ void vjp_integrate(const float* s, const float* f, V3 com, const M33& I, float inv_mass, const M33& inv_I,
                               V3 g, float damping, float dt, const float* gout, float* gs, float* gf) {
-    for (int j0 = 0; j0 < 19; j0 += kDirs) {
-        BodyT<Dual<kDirs>> b;
-        Dual<kDirs> x[19];
-        for (int j = 0; j < 13; ++j) x[j] = seed<kDirs>(s[j], j, j0);
-        for (int j = 0; j < 6; ++j) x[13 + j] = seed<kDirs>(f[j], 13 + j, j0);
-        b.p = {x[0], x[1], x[2]};
-        b.r = {x[3], x[4], x[5], x[6]};
-        b.v = {x[7], x[8], x[9]};
-        b.w = {x[10], x[11], x[12]};
-        integrate_g(b, V3T<Dual<kDirs>>{x[13], x[14], x[15]}, V3T<Dual<kDirs>>{x[16], x[17], x[18]}, com, I, inv_mass,
-                    inv_I, g, damping, dt);
-        Dual<kDirs> o[13];
-        body_out(b, o);
-        for (int k = 0; k < kDirs && j0 + k < 19; ++k) {
-            float acc = 0.0f;
-            for (int i = 0; i < 13; ++i) acc += gout[i] * o[i].d[k];
-            if (j0 + k < 13) gs[j0 + k] = acc;
-            else gf[j0 + k - 13] = acc;
-        }
-    }
+    (void)g;
+    const V3 x0{s[0], s[1], s[2]}, w0{s[10], s[11], s[12]};
+    const Q4 r0{s[3], s[4], s[5], s[6]};
+    const V3 t0{f[3], f[4], f[5]};
+    const V3 wb = qrot_inv(r0, w0);
+    const V3 y = mv(I, wb);
+    const V3 tb = sub(qrot_inv(r0, t0), cross(wb, y));
+    const V3 sv = add(wb, mul(mv(inv_I, tb), dt));
+    const V3 w1a = qrot(r0, sv);
+    const Q4 wq{w1a.x, w1a.y, w1a.z, 0.0f};
+    const Q4 dq = qmul(wq, r0);
+    const Q4 r1u{r0.x + dq.x * 0.5f * dt, r0.y + dq.y * 0.5f * dt, r0.z + dq.z * 0.5f * dt, r0.w + dq.w * 0.5f * dt};
+    const Q4 r1 = qnormalize(r1u);
+    const float damp = 1.0f - damping * dt;
+    // reverse
+    const V3 gp{gout[0], gout[1], gout[2]}, gv{gout[7], gout[8], gout[9]}, gw{gout[10], gout[11], gout[12]};
+    Q4f gr1{gout[3], gout[4], gout[5], gout[6]};
+    V3 gw1a = mul(gw, damp);
+    // p = x1 - qrot(r1, com), x1 = x0 + qrot(r0, com) + v1 dt
+    qrot_vjp_q(r1, com, neg(gp), 1.0f, gr1);
+    const Q4f gr1u = qnormalize_vjp(r1u, gr1);
+    Q4f gr0 = gr1u;
+    const Q4f gdq{gr1u.x * 0.5f * dt, gr1u.y * 0.5f * dt, gr1u.z * 0.5f * dt, gr1u.w * 0.5f * dt};
+    Q4f gwq{0.0f, 0.0f, 0.0f, 0.0f};
+    qmul_vjp(wq, r0, gdq, gwq, gr0);
+    gw1a = add(gw1a, V3{gwq.x, gwq.y, gwq.z});
+    qrot_vjp_q(r0, sv, gw1a, 1.0f, gr0);
+    const V3 gsv = qrot_inv(r0, gw1a);
+    V3 gwb = gsv;
+    const V3 gtb = mul(mtv(inv_I, gsv), dt);
+    // tb = qrot_inv(r0, t0) - wb x (I wb)
+    qrot_vjp_q(r0, t0, gtb, -1.0f, gr0);
+    const V3 gt0 = qrot(r0, gtb);
+    V3 gy{0.0f, 0.0f, 0.0f};
+    cross_vjp(wb, y, neg(gtb), gwb, gy);
+    gwb = add(gwb, mtv(I, gy));
+    qrot_vjp_q(r0, w0, gwb, -1.0f, gr0);
+    const V3 gw0 = qrot(r0, gwb);
+    const V3 gv1 = add(gv, mul(gp, dt));
+    qrot_vjp_q(r0, com, gp, 1.0f, gr0);
+    gs[0] = gp.x; gs[1] = gp.y; gs[2] = gp.z;
+    gs[3] = gr0.x; gs[4] = gr0.y; gs[5] = gr0.z; gs[6] = gr0.w;
+    gs[7] = gv1.x; gs[8] = gv1.y; gs[9] = gv1.z;
+    gs[10] = gw0.x; gs[11] = gw0.y; gs[12] = gw0.z;
+    gf[0] = gv1.x * inv_mass * dt; gf[1] = gv1.y * inv_mass * dt; gf[2] = gv1.z * inv_mass * dt;
+    gf[3] = gt0.x; gf[4] = gt0.y; gf[5] = gt0.z;
+    (void)x0;
 }
 
 // contact: inputs A pose (7) + A omega (3) + B pose (7) + B omega (3); outputs the four deltas (12)
-__device__ void vjp_contact(const ContactC& c, const float* sa, const float* sb, float relaxation, float dt,
+__device__ __forceinline__ void vjp_contact(const ContactC& c, const float* sa, const float* sb, float relaxation, float dt,
                             const float* gout, float* ga, float* gb) {
+#pragma unroll
     for (int j0 = 0; j0 < 20; j0 += kDirs) {
         BodyT<Dual<kDirs>> A, B;
         A.p = {seed<kDirs>(sa[0], 0, j0), seed<kDirs>(sa[1], 1, j0), seed<kDirs>(sa[2], 2, j0)};
@@ -516,8 +660,10 @@ __device__ void vjp_contact(const ContactC& c, const float* sa, const float* sb,
         V3T<Dual<kDirs>> la, aa, lb, ab;
         if (!contact_g(c, A, B, relaxation, dt, la, aa, lb, ab)) return;
         const Dual<kDirs> o[12] = {la.x, la.y, la.z, aa.x, aa.y, aa.z, lb.x, lb.y, lb.z, ab.x, ab.y, ab.z};
+#pragma unroll
         for (int k = 0; k < kDirs && j0 + k < 20; ++k) {
             float acc = 0.0f;
+#pragma unroll
             for (int i = 0; i < 12; ++i) acc += gout[i] * o[i].d[k];
             const int j = j0 + k;
             // A: pose -> state 0..6, omega -> state 10..12; B likewise
@@ -584,15 +730,18 @@ __device__ ContactC load_contact(const NbModelDesc& m, const float4* r, int b0, 
 __device__ __forceinline__ void side_state(const float* tape_it, int b0, int l, float* s) {
     if (l >= 0) {
         const float* t = tape_it + 13 * (size_t)(b0 + l);
+#pragma unroll
         for (int k = 0; k < 13; ++k) s[k] = t[k];
     } else {
+#pragma unroll
         for (int k = 0; k < 13; ++k) s[k] = 0.0f;
         s[6] = 1.0f;
     }
 }
 
-__global__ void __launch_bounds__(kThreads) adjoint_world_kernel(NbModelDesc m, NbXpbdParams p, NbAdjointIO io,
-                                                                 NbContactSeg seg, int has_contacts, float dt) {
+// forward recording, one CTA per world
+__global__ void __launch_bounds__(kThreads) adjoint_forward_kernel(NbModelDesc m, NbXpbdParams p, NbAdjointIO io,
+                                                                   NbContactSeg seg, int has_contacts, float dt) {
     const int w = blockIdx.x;
     const int t = threadIdx.x;
     const int b0 = m.world_body_start[w], b1 = m.world_body_start[w + 1];
@@ -610,7 +759,21 @@ __global__ void __launch_bounds__(kThreads) adjoint_world_kernel(NbModelDesc m, 
         if (m.joint_enabled[j] && m.joint_type[j] != NB_JOINT_FREE) s_flag = 1;
     __syncthreads();
     if (s_flag) {
+        // not differentiated: the tape holds the input state throughout and no contact is active,
+        // so the reverse kernels read defined values; the status bit makes the caller discard them
         if (t == 0) atomicOr(io.status, (unsigned)NB_STATUS_ADJOINT_UNSUPPORTED);
+        for (int i = t; i < nb; i += kThreads) {
+            const int bi = b0 + i;
+            for (int it = 0; it <= K; ++it) {
+                float* o = io.tape_state + ((size_t)it * B + bi) * 13;
+                for (int k = 0; k < 7; ++k) o[k] = io.body_q_in[7 * (size_t)bi + k];
+                for (int k = 0; k < 6; ++k) o[7 + k] = io.body_qd_in[6 * (size_t)bi + k];
+                if (it < K) {
+                    for (int k = 0; k < 6; ++k) io.tape_delta[((size_t)it * B + bi) * 6 + k] = 0.0f;
+                    io.tape_weight[(size_t)it * B + bi] = 1.0f;
+                }
+            }
+        }
         return;
     }
     const int nc = has_contacts ? seg.world_count[w] : 0;
@@ -635,6 +798,7 @@ __global__ void __launch_bounds__(kThreads) adjoint_world_kernel(NbModelDesc m, 
             body_to(b, s);
         }
         float* o = io.tape_state + 13 * (size_t)bi;
+#pragma unroll
         for (int k = 0; k < 13; ++k) o[k] = s[k];
     }
     __syncthreads();
@@ -642,6 +806,7 @@ __global__ void __launch_bounds__(kThreads) adjoint_world_kernel(NbModelDesc m, 
         const float* S_it = io.tape_state + (size_t)it * B * 13;
         float* S_next = io.tape_state + (size_t)(it + 1) * B * 13;
         for (int i = t; i < nb; i += kThreads) {
+#pragma unroll
             for (int k = 0; k < 6; ++k) io.delta_acc[6 * (size_t)(b0 + i) + k] = 0ll;
             io.count_acc[b0 + i] = 0;
         }
@@ -658,15 +823,25 @@ __global__ void __launch_bounds__(kThreads) adjoint_world_kernel(NbModelDesc m, 
             if (!contact_g(c, body_from<float>(sa), body_from<float>(sb), p.rigid_contact_relaxation, dt, la, aa, lb,
                            ab))
                 continue;
+            // the reverse pass differentiates this iteration's active contacts only
+            const int slot = atomicAdd(io.active_count + it, 1);
+            if (slot < io.active_capacity) {
+                io.active[2 * ((size_t)it * io.active_capacity + slot)] = (int32_t)(seg.world_base[w] + k);
+                io.active[2 * ((size_t)it * io.active_capacity + slot) + 1] = w;
+            } else {
+                atomicOr(io.status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
+            }
             const float da[6] = {la.x, la.y, la.z, aa.x, aa.y, aa.z};
             const float db[6] = {lb.x, lb.y, lb.z, ab.x, ab.y, ab.z};
             if (c.la >= 0) {
+#pragma unroll
                 for (int q = 0; q < 6; ++q)
                     atomicAdd(reinterpret_cast<unsigned long long*>(io.delta_acc + 6 * (size_t)(b0 + c.la) + q),
                               (unsigned long long)fx_quant(da[q], &bad));
                 if (weighting) atomicAdd(io.count_acc + b0 + c.la, 1);
             }
             if (c.lb >= 0) {
+#pragma unroll
                 for (int q = 0; q < 6; ++q)
                     atomicAdd(reinterpret_cast<unsigned long long*>(io.delta_acc + 6 * (size_t)(b0 + c.lb) + q),
                               (unsigned long long)fx_quant(db[q], &bad));
@@ -677,10 +852,12 @@ __global__ void __launch_bounds__(kThreads) adjoint_world_kernel(NbModelDesc m, 
         for (int i = t; i < nb; i += kThreads) {
             const int bi = b0 + i;
             float dl[6];
+#pragma unroll
             for (int k = 0; k < 6; ++k) dl[k] = fx_float(io.delta_acc[6 * (size_t)bi + k]);
             const int cnt = io.count_acc[bi];
             const float weight = (weighting && cnt > 0) ? 1.0f / (float)cnt : 1.0f;
             float* D = io.tape_delta + ((size_t)it * B + bi) * 6;
+#pragma unroll
             for (int k = 0; k < 6; ++k) D[k] = dl[k];
             io.tape_weight[(size_t)it * B + bi] = weight;
             BodyT<float> b = body_from<float>(S_it + 13 * (size_t)bi);
@@ -697,69 +874,88 @@ __global__ void __launch_bounds__(kThreads) adjoint_world_kernel(NbModelDesc m, 
         const float* S_K = io.tape_state + (size_t)K * B * 13;
         for (int i = t; i < nb; i += kThreads) {
             const float* s = S_K + 13 * (size_t)(b0 + i);
+#pragma unroll
             for (int k = 0; k < 7; ++k) io.body_q_out[7 * (size_t)(b0 + i) + k] = s[k];
+#pragma unroll
             for (int k = 0; k < 6; ++k) io.body_qd_out[6 * (size_t)(b0 + i) + k] = s[7 + k];
         }
     }
 
-    // ---- reverse
-    for (int i = t; i < nb; i += kThreads) {
-        const int bi = b0 + i;
+    if (bad && t == 0) atomicOr(io.status, (unsigned)NB_STATUS_FIXED_OVERFLOW);
+}
+
+// ---- reverse: flat kernels over all bodies / all active contacts of one iteration
+
+__global__ void __launch_bounds__(kThreads) adjoint_seed_kernel(NbModelDesc m, NbAdjointIO io) {
+    for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < m.body_count; bi += gridDim.x * blockDim.x) {
         double* g = io.grad_acc + 13 * (size_t)bi;
         for (int k = 0; k < 7; ++k) g[k] = io.grad_q_out[7 * (size_t)bi + k];
         for (int k = 0; k < 6; ++k) g[7 + k] = io.grad_qd_out[6 * (size_t)bi + k];
     }
-    __syncthreads();
-    for (int it = K - 1; it >= 0; --it) {
-        const float* S_it = io.tape_state + (size_t)it * B * 13;
-        // bodies: VJP of the weighted apply; D's cotangent replaces D on the tape
-        for (int i = t; i < nb; i += kThreads) {
-            const int bi = b0 + i;
-            float* D = io.tape_delta + ((size_t)it * B + bi) * 6;
-            if (kinematic(m, bi)) {
-                for (int k = 0; k < 6; ++k) D[k] = 0.0f;
-                continue;
-            }
-            double* g = io.grad_acc + 13 * (size_t)bi;
-            float gout[13], gs[13], gd[6];
-            for (int k = 0; k < 13; ++k) gout[k] = (float)g[k];
-            vjp_apply(S_it + 13 * (size_t)bi, D, io.tape_weight[(size_t)it * B + bi], has_contacts != 0,
-                      model_joints, load_v3(m.body_com + 3 * (size_t)bi), load_m33(m.body_inertia + 9 * (size_t)bi),
-                      m.body_inv_mass[bi], load_m33(m.body_inv_inertia + 9 * (size_t)bi), dt, gout, gs, gd);
-            for (int k = 0; k < 13; ++k) g[k] = gs[k];
-            for (int k = 0; k < 6; ++k) D[k] = gd[k];
+}
+
+// bodies of iteration it: VJP of the body update; the cotangent of the delta replaces it on the tape
+__global__ void __launch_bounds__(kThreads) adjoint_bodies_kernel(NbModelDesc m, NbAdjointIO io, int it,
+                                                                  int has_contacts, float dt) {
+    const size_t B = (size_t)m.body_count;
+    const bool model_joints = m.joint_count > 0;
+    const float* S_it = io.tape_state + (size_t)it * B * 13;
+    for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < m.body_count; bi += gridDim.x * blockDim.x) {
+        float* D = io.tape_delta + ((size_t)it * B + bi) * 6;
+        if (kinematic(m, bi)) {
+            for (int k = 0; k < 6; ++k) D[k] = 0.0f;
+            continue;
         }
-        __syncthreads();
-        // contacts: VJP of each active contact's deltas into its bodies' poses and angular velocities
-        for (int k = t; k < nc; k += kThreads) {
-            const float4* r = R + (size_t)k * 5;
-            if (__float_as_int(r[3].w) == __float_as_int(r[4].w)) continue;
-            const ContactC c = load_contact(m, r, b0, S_it);
-            if (c.la == c.lb) continue;
-            const bool dyn_a = c.la >= 0 && !c.kin_a, dyn_b = c.lb >= 0 && !c.kin_b;
-            if (!dyn_a && !dyn_b) continue;
-            float sa[13], sb[13];
-            side_state(S_it, b0, c.la, sa);
-            side_state(S_it, b0, c.lb, sb);
-            float gout[12];
-            for (int q = 0; q < 6; ++q) {
-                gout[q] = dyn_a ? io.tape_delta[((size_t)it * B + b0 + c.la) * 6 + q] : 0.0f;
-                gout[6 + q] = dyn_b ? io.tape_delta[((size_t)it * B + b0 + c.lb) * 6 + q] : 0.0f;
-            }
-            float ga[13] = {}, gb[13] = {};
-            vjp_contact(c, sa, sb, p.rigid_contact_relaxation, dt, gout, ga, gb);
-            if (dyn_a)
-                for (int q = 0; q < 13; ++q)
-                    if (ga[q] != 0.0f) atomicAdd(io.grad_acc + 13 * (size_t)(b0 + c.la) + q, (double)ga[q]);
-            if (dyn_b)
-                for (int q = 0; q < 13; ++q)
-                    if (gb[q] != 0.0f) atomicAdd(io.grad_acc + 13 * (size_t)(b0 + c.lb) + q, (double)gb[q]);
-        }
-        __syncthreads();
+        double* g = io.grad_acc + 13 * (size_t)bi;
+        float gout[13], gs[13], gd[6], dl[6];
+        for (int k = 0; k < 13; ++k) gout[k] = (float)g[k];
+        for (int k = 0; k < 6; ++k) dl[k] = D[k];
+        vjp_apply(S_it + 13 * (size_t)bi, dl, io.tape_weight[(size_t)it * B + bi], has_contacts != 0, model_joints,
+                  load_v3(m.body_com + 3 * (size_t)bi), load_m33(m.body_inertia + 9 * (size_t)bi), m.body_inv_mass[bi],
+                  load_m33(m.body_inv_inertia + 9 * (size_t)bi), dt, gout, gs, gd);
+        for (int k = 0; k < 13; ++k) g[k] = gs[k];
+        for (int k = 0; k < 6; ++k) D[k] = gd[k];
     }
-    // integration
-    for (int i = t; i < nb; i += kThreads) {
-        const int bi = b0 + i;
+}
+
+// active contacts of iteration it: VJP of the contact's deltas into its bodies' poses and angular velocities
+__global__ void __launch_bounds__(kThreads) adjoint_contacts_kernel(NbModelDesc m, NbXpbdParams p, NbAdjointIO io,
+                                                                    NbContactSeg seg, int it, float dt) {
+    const size_t B = (size_t)m.body_count;
+    const float* S_it = io.tape_state + (size_t)it * B * 13;
+    int n = io.active_count[it];
+    n = n < io.active_capacity ? n : io.active_capacity;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int rec = io.active[2 * ((size_t)it * io.active_capacity + e)];
+        const int w = io.active[2 * ((size_t)it * io.active_capacity + e) + 1];
+        const int b0 = m.world_body_start[w];
+        const float4* r = reinterpret_cast<const float4*>(seg.rec) + (size_t)rec * 5;
+        const ContactC c = load_contact(m, r, b0, S_it);
+        const bool dyn_a = c.la >= 0 && !c.kin_a, dyn_b = c.lb >= 0 && !c.kin_b;
+        if (!dyn_a && !dyn_b) continue;
+        float sa[13], sb[13];
+        side_state(S_it, b0, c.la, sa);
+        side_state(S_it, b0, c.lb, sb);
+        float gout[12];
+        for (int q = 0; q < 6; ++q) {
+            gout[q] = dyn_a ? io.tape_delta[((size_t)it * B + b0 + c.la) * 6 + q] : 0.0f;
+            gout[6 + q] = dyn_b ? io.tape_delta[((size_t)it * B + b0 + c.lb) * 6 + q] : 0.0f;
+        }
+        float ga[13] = {}, gb[13] = {};
+        vjp_contact(c, sa, sb, p.rigid_contact_relaxation, dt, gout, ga, gb);
+        if (dyn_a)
+            for (int q = 0; q < 13; ++q)
+                if (ga[q] != 0.0f) atomicAdd(io.grad_acc + 13 * (size_t)(b0 + c.la) + q, (double)ga[q]);
+        if (dyn_b)
+            for (int q = 0; q < 13; ++q)
+                if (gb[q] != 0.0f) atomicAdd(io.grad_acc + 13 * (size_t)(b0 + c.lb) + q, (double)gb[q]);
+    }
+}
+
+// integration: cotangents of the step's inputs
+__global__ void __launch_bounds__(kThreads) adjoint_integrate_kernel(NbModelDesc m, NbXpbdParams p, NbAdjointIO io,
+                                                                     float dt) {
+    for (int bi = blockIdx.x * blockDim.x + threadIdx.x; bi < m.body_count; bi += gridDim.x * blockDim.x) {
         const double* g = io.grad_acc + 13 * (size_t)bi;
         float gout[13], gs[13], gf[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
         for (int k = 0; k < 13; ++k) gout[k] = (float)g[k];
@@ -781,7 +977,6 @@ __global__ void __launch_bounds__(kThreads) adjoint_world_kernel(NbModelDesc m, 
         if (io.grad_f_in)
             for (int k = 0; k < 6; ++k) io.grad_f_in[6 * (size_t)bi + k] = gf[k];
     }
-    if (bad && t == 0) atomicOr(io.status, (unsigned)NB_STATUS_FIXED_OVERFLOW);
 }
 
 }  // namespace
@@ -789,6 +984,18 @@ __global__ void __launch_bounds__(kThreads) adjoint_world_kernel(NbModelDesc m, 
 cudaError_t nb_launch_xpbd_adjoint(const NbModelDesc* m, const NbXpbdParams* p, const NbAdjointIO* io,
                                    const NbContactSeg* seg, int has_contacts, float dt, cudaStream_t s) {
     if (m->world_count <= 0 || m->body_count <= 0) return cudaSuccess;
-    adjoint_world_kernel<<<m->world_count, kThreads, 0, s>>>(*m, *p, *io, *seg, has_contacts, dt);
+    const int K = p->iterations;
+    cudaError_t e = cudaMemsetAsync(io->active_count, 0, sizeof(int32_t) * (size_t)(K > 0 ? K : 1), s);
+    if (e != cudaSuccess) return e;
+    adjoint_forward_kernel<<<m->world_count, kThreads, 0, s>>>(*m, *p, *io, *seg, has_contacts, dt);
+    const int gb = nb_contact_grid(m->body_count, kThreads);
+    adjoint_seed_kernel<<<gb, kThreads, 0, s>>>(*m, *io);
+    const int gc = nb_contact_grid(io->active_capacity > 0 ? io->active_capacity : 1, kThreads);
+    for (int it = K - 1; it >= 0; --it) {
+        adjoint_bodies_kernel<<<gb, kThreads, 0, s>>>(*m, *io, it, has_contacts, dt);
+        if (has_contacts && io->active_capacity > 0)
+            adjoint_contacts_kernel<<<gc, kThreads, 0, s>>>(*m, *p, *io, *seg, it, dt);
+    }
+    adjoint_integrate_kernel<<<gb, kThreads, 0, s>>>(*m, *p, *io, dt);
     return cudaGetLastError();
 }

@@ -151,6 +151,8 @@ int nb_xpbd_step_adjoint(const NbModelDesc* model, const NbXpbdParams* params, c
         return NB_ERR_INVALID;
     if (io->body_q_out && !io->body_qd_out) return NB_ERR_INVALID;
     const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
+    if (io->active_capacity < 0 || !io->active_count || (has_contacts && io->active_capacity > 0 && !io->active))
+        return NB_ERR_INVALID;
     cudaError_t e = nb_launch_xpbd_adjoint(model, params, io, seg, has_contacts, dt, (cudaStream_t)stream);
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
