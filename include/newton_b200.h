@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 10
+#define NB_ABI_VERSION 11
 
 enum {
     NB_OK = 0,
@@ -68,7 +68,8 @@ enum {
     NB_STATUS_FIXED_OVERFLOW = 1u << 2,   /* delta accumulator saturated       */
     NB_STATUS_QUEUE_TIMEOUT = 1u << 3,    /* work-queue wait hit its bound     */
     NB_STATUS_WORLD_TOO_LARGE = 1u << 4,  /* world exceeds shared staging      */
-    NB_STATUS_ADJOINT_UNSUPPORTED = 1u << 5 /* adjoint skipped a world with an enabled non-free joint */
+    NB_STATUS_ADJOINT_UNSUPPORTED = 1u << 5, /* adjoint skipped a world with an enabled non-free joint */
+    NB_STATUS_MODE_UNSUPPORTED = 1u << 6  /* flat step mode met a world with an enabled non-free joint */
 };
 
 /* Geometry types (newton/_src/geometry/types.py:46-77). */
@@ -161,7 +162,11 @@ typedef struct NbModelDesc {
                                           2: as 1 with a compact slab (27 words/body, mass
                                              properties read from the model); modes 1-2 pull worlds
                                              in world_order, each group owning
-                                             arena * group_threads / cta_threads words */
+                                             arena * group_threads / cta_threads words;
+                                          3: flat -- body state in NbStepIO.step_scratch, one
+                                             launch per phase over all worlds (models whose
+                                             joints are all free; no restitution, impulses,
+                                             body_parent_f or warm start) */
     const int32_t* batch_world;        /* [batch_count, cta_threads/group_threads] world ids, -1 = none */
     const int32_t* batch_slab;         /* [batch_count, cta_threads/group_threads] arena offsets (words) */
 } NbModelDesc;
@@ -324,6 +329,8 @@ typedef struct NbStepIO {
     int32_t ws_capacity;         /* rows of ws_lambda */
     int32_t pad1;
     int32_t* ws_fallback;        /* [1] worlds whose warm start was rejected (counter) or NULL */
+    void* step_scratch;          /* nb_step_scratch_bytes(model) bytes (16-byte aligned) for step_mode 3,
+                                    else unused */
 } NbStepIO;
 
 /* ABI version of the loaded library (NB_ABI_VERSION). */
@@ -332,6 +339,10 @@ int nb_abi_version(void);
 
 /* Number of CTAs the persistent kernels launch on the current device. */
 int32_t nb_default_grid(void);
+
+/* Bytes of NbStepIO.step_scratch nb_xpbd_step needs for this model's step_mode
+ * (0 unless step_mode is 3). */
+int64_t nb_step_scratch_size(const NbModelDesc* model);
 
 /*
  * Collision detection for all worlds: shape world transforms + AABBs

@@ -45,6 +45,7 @@ EXPORTS = (
     "nb_ws_grads",
     "nb_ws_adam",
     "nb_xpbd_step_adjoint",
+    "nb_step_scratch_size",
 )
 
 _lib = None
@@ -111,6 +112,8 @@ def load(path: str | None = None) -> C.CDLL:
     lib.nb_ws_adam.restype = C.c_int
     lib.nb_ws_adam.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float,
                                C.c_float, C.c_float, C.c_float, C.c_int32, C.c_void_p]
+    lib.nb_step_scratch_size.restype = C.c_int64
+    lib.nb_step_scratch_size.argtypes = [C.POINTER(NbModelDesc)]
     lib.nb_xpbd_step_adjoint.restype = C.c_int
     lib.nb_xpbd_step_adjoint.argtypes = [C.POINTER(NbModelDesc), C.POINTER(NbXpbdParams), C.POINTER(NbAdjointIO),
                                          C.POINTER(NbContactSeg), C.c_float, C.c_void_p]

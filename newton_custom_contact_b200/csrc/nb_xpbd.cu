@@ -1253,6 +1253,229 @@ xpbd_step_group_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg 
     }
 }
 
+// ---------------------------------------------------------------- flat mode
+// The same substep with the body state in global memory (structure of arrays
+// over all bodies, caller scratch) instead of per-world shared-memory slabs,
+// and one launch per phase over all worlds at once: flat_begin (a warp per
+// world: stage, joint forces, integrate), then per iteration flat_contacts (a
+// warp per tile of consecutive contact records of any worlds: the contact
+// pass, deltas summed with the same exact fixed-point atomics) and
+// flat_apply (a thread per body), then flat_end (write-back).  Every
+// function of the per-world path is reused on a global view of the state,
+// so the results are bit-identical; what changes is the
+// parallelism: all worlds' contacts and bodies are in flight at once instead
+// of one world's chain per thread group.  For models whose joints are all
+// free, without restitution, impulse reporting or warm start.
+
+struct FlatScratch {
+    float* f;                  // [13][B] pose + twist
+    unsigned long long* acc;   // [6][B] fixed-point deltas (the first 6 B floats hold body forces before integration)
+    int* flags;                // [B]
+    int* cnt;                  // [B]
+};
+
+__host__ __device__ inline size_t flat_acc_offset(int B) { return ((size_t)13 * B * 4 + 15) & ~(size_t)15; }
+__host__ __device__ inline size_t flat_scratch_bytes(int B) {
+    return flat_acc_offset(B) + (size_t)6 * B * 8 + (size_t)2 * B * 4;
+}
+
+__device__ __forceinline__ FlatScratch flat_scratch(void* base, int B) {
+    unsigned char* b = reinterpret_cast<unsigned char*>(base);
+    FlatScratch fs;
+    fs.f = reinterpret_cast<float*>(b);
+    fs.acc = reinterpret_cast<unsigned long long*>(b + flat_acc_offset(B));
+    fs.flags = reinterpret_cast<int*>(fs.acc + 6 * (size_t)B);
+    fs.cnt = fs.flags + B;
+    return fs;
+}
+
+// the per-world slab interface over the global arrays: local body i of a world
+// starting at b0 is global body b0 + i, arrays strided by the body count
+__device__ __forceinline__ SBodiesT<true> global_view(const NbModelDesc& m, const FlatScratch& fs, int b0) {
+    SBodiesT<true> S;
+    S.nb = m.body_count;
+    S.b0 = b0;
+    S.f = fs.f + b0;
+    S.c = S.I = S.iI = nullptr;
+    S.g_com = m.body_com;
+    S.g_inv_m = m.body_inv_mass;
+    S.g_I = m.body_inertia;
+    S.g_iI = m.body_inv_inertia;
+    S.acc = fs.acc + b0;
+    S.frc = reinterpret_cast<float*>(fs.acc) + b0;
+    S.flags = fs.flags + b0;
+    S.cnt = fs.cnt + b0;
+    return S;
+}
+
+constexpr int kFlatWarps = 8;  // warps per CTA of the per-world flat kernels
+
+__global__ void __launch_bounds__(32 * kFlatWarps)
+flat_begin_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, float dt) {
+    const FlatScratch fs = flat_scratch(io.step_scratch, m.body_count);
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    __shared__ int s_flag[kFlatWarps];
+    for (int w = blockIdx.x * kFlatWarps + wl; w < m.world_count; w += gridDim.x * kFlatWarps) {
+        const int b0 = m.world_body_start[w];
+        const int nb = m.world_body_start[w + 1] - b0;
+        SBodiesT<true> S = global_view(m, fs, b0);
+        for (int i = lane; i < nb; i += 32) {
+            const int bi = b0 + i;
+            S.flags[i] = m.body_flags[bi];
+            const float* q = io.body_q_in + 7 * (size_t)bi;
+            const float* qd = io.body_qd_in + 6 * (size_t)bi;
+            const float* fb = io.body_f_in + 6 * (size_t)bi;
+            S.set(i, TF{V3{q[0], q[1], q[2]}, Q4{q[3], q[4], q[5], q[6]}}, V3{qd[0], qd[1], qd[2]},
+                  V3{qd[3], qd[4], qd[5]});
+            for (int k = 0; k < 6; ++k) S.frc[k * S.nb + i] = fb[k];
+            S.cnt[i] = 0;
+        }
+        const int j0 = m.world_joint_start[w], j1 = m.world_joint_start[w + 1];
+        if (lane == 0) s_flag[wl] = 0;
+        __syncwarp();
+        for (int j = j0 + lane; j < j1; j += 32) {
+            if (m.joint_type[j] != NB_JOINT_FREE && m.joint_enabled[j]) atomicOr(&s_flag[wl], 1);
+            if (io.joint_f) {
+                const int qs = m.joint_qd_start[j];
+                const int nd = m.joint_dof_dim[2 * j] + m.joint_dof_dim[2 * j + 1];
+                for (int k = 0; k < nd; ++k)
+                    if (io.joint_f[qs + k] != 0.0f) atomicOr(&s_flag[wl], 2);
+            }
+        }
+        __syncwarp();
+        // an enabled non-free joint needs the per-world path (the host never selects this mode then)
+        if ((s_flag[wl] & 1) && lane == 0) atomicOr(seg.status, (unsigned)NB_STATUS_MODE_UNSUPPORTED);
+        if ((s_flag[wl] & 2) && lane == 0) joint_forces(m, S, b0, j0, j1, io.joint_f);
+        __syncwarp();
+        for (int i = lane; i < nb; i += 32) {
+            const V3 f0{S.frc[0 * S.nb + i], S.frc[1 * S.nb + i], S.frc[2 * S.nb + i]};
+            const V3 t0{S.frc[3 * S.nb + i], S.frc[4 * S.nb + i], S.frc[5 * S.nb + i]};
+            if (!(S.flags[i] & NB_BODY_KINEMATIC)) {
+                const int bi = b0 + i;
+                int wi = m.body_world[bi];
+                if (wi < 0) wi = 0;
+                const V3 gv = load_v3(m.gravity + 3 * (size_t)wi);
+                TF q = S.q(i);
+                V3 v = S.v(i), wv = S.w(i);
+                integrate_rigid_body(q, v, wv, f0, t0, S.com(i), S.inertia(i), m.body_inv_mass[bi],
+                                     load_m33(m.body_inv_inertia + 9 * (size_t)bi), gv, p.angular_damping, dt);
+                S.set(i, q, v, wv);
+            }
+        }
+        __syncwarp();
+        for (int i = lane; i < nb; i += 32)
+            for (int k = 0; k < 6; ++k) S.acc[k * S.nb + i] = 0ull;
+        __syncwarp();
+    }
+}
+
+// contact records are dense over all worlds (world w's at world_base[w] ..);
+// a record's world follows from one of its shapes: the body of shape s_a is
+// local body l_a of its world, so the world starts at shape_body[s_a] - l_a
+__device__ __forceinline__ int record_world_start(const NbModelDesc& m, const float4* r) {
+    const int tag = __float_as_int(r[2].w);
+    const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
+    if (la >= 0) return m.shape_body[__float_as_int(r[3].w)] - la;
+    if (lb >= 0) return m.shape_body[__float_as_int(r[4].w)] - lb;
+    return 0;
+}
+
+// A warp per tile of kChunk consecutive records of any worlds: test them, compact the
+// penetrating ones in shared memory, then solve those with every lane busy.
+__global__ void __launch_bounds__(32 * kFlatWarps)
+flat_contacts_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, float dt) {
+    const FlatScratch fs = flat_scratch(io.step_scratch, m.body_count);
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    __shared__ int s_nact[kFlatWarps];
+    __shared__ unsigned char s_list[kFlatWarps][kChunk];
+    const float4* rec = reinterpret_cast<const float4*>(seg.rec);
+    const bool weighting = p.rigid_contact_con_weighting != 0;
+    const int W = m.world_count;
+    const long total = W > 0 ? (long)seg.world_base[W - 1] + seg.world_count[W - 1] : 0;
+    const long tiles = (total + kChunk - 1) / kChunk;
+    unsigned bad = 0u;
+    for (long tile = blockIdx.x * (long)kFlatWarps + wl; tile < tiles; tile += (long)gridDim.x * kFlatWarps) {
+        const long base = tile * kChunk;
+        const int lim = total - base < kChunk ? (int)(total - base) : kChunk;
+        if (lane == 0) s_nact[wl] = 0;
+        __syncwarp();
+        for (int k = lane; k < lim; k += 32) {
+            const float4* r = rec + (size_t)(base + k) * 5;
+            const SBodiesT<true> S = global_view(m, fs, record_world_start(m, r));
+            if (contact_active(S, r[0], r[1], r[2])) s_list[wl][atomicAdd(&s_nact[wl], 1)] = (unsigned char)k;
+        }
+        __syncwarp();
+        const int na = s_nact[wl];
+        for (int a = lane; a < na; a += 32) {
+            const float4* r = rec + (size_t)(base + s_list[wl][a]) * 5;
+            SBodiesT<true> S = global_view(m, fs, record_world_start(m, r));
+            solve_contact(m, S, r[0], r[1], r[2], r[3], r[4], p.rigid_contact_relaxation, dt, weighting, &bad, nullptr);
+        }
+        __syncwarp();
+    }
+    if (bad && lane == 0) atomicOr(seg.status, (unsigned)NB_STATUS_FIXED_OVERFLOW);
+}
+
+// mode 0: after a contact pass (weighted apply, closed form for untouched bodies, then the free-joint
+// renormalisation when the model has joints); mode 1: the joint pass of a step without contacts
+__global__ void __launch_bounds__(256) flat_apply_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, int mode,
+                                                         float dt) {
+    const FlatScratch fs = flat_scratch(io.step_scratch, m.body_count);
+    SBodiesT<true> S = global_view(m, fs, 0);
+    const bool weighting = p.rigid_contact_con_weighting != 0;
+    const bool model_joints = m.joint_count > 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.body_count; i += gridDim.x * blockDim.x) {
+        V3 dl, da;
+        const bool moved = S.take(i, dl, da);
+        TF q = S.q(i);
+        V3 v = S.v(i), wv = S.w(i);
+        const V3 com = S.com(i);
+        const float im = S.inv_m(i);
+        if (mode == 0) {
+            float weight = 1.0f;
+            if (weighting) {
+                float iw = (float)S.cnt[i];
+                S.cnt[i] = 0;
+                if (iw > 0.0f) weight = 1.0f / iw;
+            }
+            if (moved) apply_body_delta(q, v, wv, dl, da, weight, com, S.inertia(i), im, S.inv_inertia(i), dt);
+            else apply_zero_delta(q, v, wv, com, im);
+            if (model_joints) apply_zero_delta(q, v, wv, com, im);
+        } else {
+            apply_body_delta(q, v, wv, dl, da, 1.0f, com, S.inertia(i), im, S.inv_inertia(i), dt);
+        }
+        S.set(i, q, v, wv);
+    }
+}
+
+__global__ void __launch_bounds__(256) flat_end_kernel(NbModelDesc m, NbStepIO io, NbContactSeg seg) {
+    const FlatScratch fs = flat_scratch(io.step_scratch, m.body_count);
+    SBodiesT<true> S = global_view(m, fs, 0);
+    unsigned bad = 0u;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.body_count; i += gridDim.x * blockDim.x) {
+        float* qo = io.body_q_out + 7 * (size_t)i;
+        float* qdo = io.body_qd_out + 6 * (size_t)i;
+        if (S.flags[i] & NB_BODY_KINEMATIC) {
+            for (int k = 0; k < 7; ++k) qo[k] = io.body_q_in[7 * (size_t)i + k];
+            for (int k = 0; k < 6; ++k) qdo[k] = io.body_qd_in[6 * (size_t)i + k];
+            continue;
+        }
+        bool finite = true;
+        for (int k = 0; k < 7; ++k) {
+            const float x = S.f[k * S.nb + i];
+            finite = finite && isfinite(x);
+            qo[k] = x;
+        }
+        for (int k = 0; k < 6; ++k) {
+            const float x = S.f[(7 + k) * S.nb + i];
+            finite = finite && isfinite(x);
+            qdo[k] = x;
+        }
+        if (!finite) bad = 1u;
+    }
+    if (bad) atomicOr(seg.status, (unsigned)NB_STATUS_NONFINITE);
+}
+
 }  // namespace
 
 size_t nb_step_smem_bytes(const NbModelDesc* m) { return (size_t)m->smem_floats_per_batch * 4; }
@@ -1330,11 +1553,39 @@ cudaError_t launch_step_groups(const NbModelDesc* m, const NbXpbdParams* p, cons
 
 int nb_step_slab_words(int compact) { return compact ? slab_words_per_body<true>() : slab_words_per_body<false>(); }
 
+size_t nb_step_scratch_bytes(const NbModelDesc* m) {
+    return m->step_mode == 3 && m->body_count > 0 ? flat_scratch_bytes(m->body_count) : 0;
+}
+
+namespace {
+cudaError_t launch_flat(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
+                        float dt, cudaStream_t stream) {
+    if (m->body_count <= 0) return cudaSuccess;
+    const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
+    const int gw = nb_contact_grid((long)m->world_count * 32, 32 * kFlatWarps);
+    const int gb = nb_contact_grid(m->body_count, 256);
+    // contact tiles: one warp per kChunk records, records at most 5 per candidate pair
+    const int gc = nb_contact_grid((long)m->contact_capacity / kChunk * 32 + 32, 32 * kFlatWarps);
+    flat_begin_kernel<<<gw, 32 * kFlatWarps, 0, stream>>>(*m, *p, *io, *seg, dt);
+    for (int it = 0; it < p->iterations; ++it) {
+        if (has_contacts) {
+            flat_contacts_kernel<<<gc, 32 * kFlatWarps, 0, stream>>>(*m, *p, *io, *seg, dt);
+            flat_apply_kernel<<<gb, 256, 0, stream>>>(*m, *p, *io, 0, dt);
+        } else if (m->joint_count > 0) {
+            flat_apply_kernel<<<gb, 256, 0, stream>>>(*m, *p, *io, 1, dt);
+        }
+    }
+    flat_end_kernel<<<gb, 256, 0, stream>>>(*m, *io, *seg);
+    return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t nb_launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
                            float dt, int grid, cudaStream_t stream) {
     if (m->cta_threads != kST) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(seg->work_counter + 4, 0, sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
+    if (m->step_mode == 3) return launch_flat(m, p, io, seg, dt, stream);
     if (m->step_mode == 1) return launch_step_groups<false>(m, p, io, seg, dt, grid, stream);
     if (m->step_mode == 2) return launch_step_groups<true>(m, p, io, seg, dt, grid, stream);
     switch (m->group_threads) {

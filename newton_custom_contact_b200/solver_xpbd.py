@@ -68,6 +68,7 @@ class SolverXPBD:
         self._joint_impulse = None
         # optional learned warm start (warmstart.WarmStart); None = the plain solver
         self.warm_start = None
+        self._step_scratch = None
 
     @property
     def device(self):
@@ -166,6 +167,17 @@ class SolverXPBD:
             io.impulse_scratch = ptr(contacts._seg["impulse_scratch"])
             io.contact_impulse_capacity = cap
         params = self.params()
+        if desc.step_mode == 3:
+            # flat schedule: the body state lives in a caller-owned scratch buffer
+            if (self.enable_restitution or io.contact_impulse or io.body_parent_f
+                    or (self.warm_start is not None and contacts is not None)):
+                raise ValueError("the 'flat' step schedule runs the plain solve only (no restitution, contact "
+                                 "forces, body_parent_f or warm start); choose another schedule with "
+                                 "pipeline.set_step_schedule")
+            nbytes = int(lib.nb_step_scratch_size(C.byref(desc)))
+            if self._step_scratch is None or self._step_scratch.numel() < nbytes:
+                self._step_scratch = torch.empty(nbytes, dtype=torch.uint8, device=model.device)
+            io.step_scratch = ptr(self._step_scratch)
         ws = self.warm_start if contacts is not None else None
         if ws is not None:
             ws.before_step(model, pipe, desc, state_in, contacts, dt, io)
