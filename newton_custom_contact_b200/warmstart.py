@@ -57,6 +57,36 @@ def ratio_targets(features: torch.Tensor, lam: torch.Tensor) -> tuple[torch.Tens
     return f[:, :N_IN].contiguous(), y.contiguous()
 
 
+def moments(x: torch.Tensor, group=None) -> tuple[torch.Tensor, torch.Tensor]:
+    """Per-column mean and standard deviation (unbiased) of x [R, C]; with a process group, of the
+    rows of every rank (sums all-reduced in float64)."""
+    s = torch.stack([torch.full((x.shape[1],), float(x.shape[0]), dtype=torch.float64, device=x.device),
+                     x.double().sum(0), (x.double() ** 2).sum(0)])
+    if group is not None:
+        import torch.distributed as dist
+
+        dist.all_reduce(s, op=dist.ReduceOp.SUM, group=group)
+    n, sx, sxx = s[0], s[1], s[2]
+    mean = sx / n
+    var = (sxx - n * mean * mean) / (n - 1).clamp_min(1.0)
+    return mean.float(), var.clamp_min(0.0).sqrt().float()
+
+
+def allreduce_mean(grads: dict, group) -> None:
+    """Average gradient tensors over the ranks of `group`, in place (one flat all-reduce)."""
+    import torch.distributed as dist
+
+    keys = sorted(grads)
+    flat = torch.cat([grads[k].reshape(-1) for k in keys])
+    dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+    flat /= dist.get_world_size(group)
+    o = 0
+    for k in keys:
+        n = grads[k].numel()
+        grads[k].copy_(flat[o:o + n].view_as(grads[k]))
+        o += n
+
+
 def _bf16_bits(t: torch.Tensor) -> torch.Tensor:
     return t.to(torch.bfloat16).view(torch.int16).contiguous()
 
@@ -129,10 +159,13 @@ class WarmStartNet:
                                                   C.c_void_p(ptr(status)), C.c_void_p(_lib.stream_handle(self.device))))
 
     # ------------------------------------------------------------ training
-    def set_normalisation(self, x: torch.Tensor, t: torch.Tensor) -> None:
-        self.in_mean = x.mean(0).contiguous()
-        self.in_inv_std = 1.0 / torch.maximum(x.std(0), 1e-4 + 1e-3 * self.in_mean.abs())
-        self.out_scale = t.std(0).clamp_min(1e-8).contiguous()
+    def set_normalisation(self, x: torch.Tensor, t: torch.Tensor, group=None) -> None:
+        """Input mean / inverse std and output scale of the samples (over every rank's shard with a
+        process group)."""
+        (xm, xs), (_, ts) = moments(x, group), moments(t, group)
+        self.in_mean = xm.contiguous()
+        self.in_inv_std = 1.0 / torch.maximum(xs, 1e-4 + 1e-3 * xm.abs())
+        self.out_scale = ts.clamp_min(1e-8).contiguous()
         self._packed = None
 
     def grads(self, x: torch.Tensor, t: torch.Tensor) -> tuple[dict, float]:
@@ -164,14 +197,23 @@ class WarmStartNet:
         return g, float(buf["loss"].item())
 
     def fit(self, features: torch.Tensor, lam: torch.Tensor, epochs: int = 30, batch: int = 4096,
-            lr: float = 2e-3, weight_decay: float = 1e-5, seed: int = 0, log=None) -> list[float]:
+            lr: float = 2e-3, weight_decay: float = 1e-5, seed: int = 0, log=None, group=None) -> list[float]:
         """Adam on minibatches (nb_ws_grads + nb_ws_adam) of (features [R, 27], lambda [R, 3]) samples,
         regressing the ratios y = lambda * w / prior of the rows with a prior; normalisation from the
-        data."""
+        data.  With a torch.distributed process group every rank holds its own shard of the samples
+        (the same number of minibatches per epoch on every rank) and the gradients are averaged over
+        the ranks before each update (data parallel; NCCL over NVLink on GPUs)."""
         lib = _lib.load()
         x, t = ratio_targets(features, lam)
         batch = max(1, min(batch, x.shape[0]))
-        self.set_normalisation(x, t)
+        self.set_normalisation(x, t, group)
+        n_batches = x.shape[0] // batch
+        if group is not None:
+            import torch.distributed as dist
+
+            nbt = torch.tensor([n_batches], device=x.device)
+            dist.all_reduce(nbt, op=dist.ReduceOp.MIN, group=group)
+            n_batches = int(nbt.item())
         m1 = {k: torch.zeros_like(v) for k, v in self.params.items()}
         m2 = {k: torch.zeros_like(v) for k, v in self.params.items()}
         gen = torch.Generator(device=x.device).manual_seed(seed)
@@ -180,9 +222,11 @@ class WarmStartNet:
         for ep in range(epochs):
             perm = torch.randperm(x.shape[0], generator=gen, device=x.device)
             tot, nb = 0.0, 0
-            for s0 in range(0, x.shape[0] - batch + 1, batch):
-                idx = perm[s0:s0 + batch]
+            for bi in range(n_batches):
+                idx = perm[bi * batch:(bi + 1) * batch]
                 g, loss = self.grads(x[idx], t[idx])
+                if group is not None:
+                    allreduce_mean(g, group)
                 step += 1
                 cur_lr = lr * 0.5 * (1.0 + np.cos(np.pi * ep / max(epochs, 1)))
                 for k, w in self.params.items():

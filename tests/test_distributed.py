@@ -80,3 +80,38 @@ def test_partition_edge_cases():
     with pytest.raises(ValueError):
         partition_worlds([1.0], 2)
     assert max_over_ranks(3.5) == 3.5  # no process group: identity
+
+
+def _ws_worker(rank, world_size, port, out_dir):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+
+    from newton_custom_contact_b200.warmstart import allreduce_mean, moments
+
+    dist.init_process_group("gloo", rank=rank, world_size=world_size, timeout=datetime.timedelta(seconds=60))
+    try:
+        g = torch.Generator().manual_seed(0)
+        x = torch.randn(1000, 5, generator=g) * torch.tensor([1.0, 2.0, 0.5, 3.0, 1.5]) + 0.3
+        shard = x[rank::world_size]
+        mean, std = moments(shard, dist.group.WORLD)
+        grads = {"w": torch.full((3, 2), float(rank + 1)), "b": torch.tensor([10.0 * rank, 1.0])}
+        allreduce_mean(grads, dist.group.WORLD)
+        np.save(os.path.join(out_dir, f"ws{rank}.npy"),
+                np.array([mean.numpy(), std.numpy(), grads["w"].numpy(), grads["b"].numpy(),
+                          x.mean(0).numpy(), x.std(0).numpy()], dtype=object), allow_pickle=True)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_warm_start_training_reductions_over_two_ranks(tmp_path):
+    """Data-parallel warm-start training: normalisation moments over all ranks' samples and the
+    gradient average, on two gloo ranks."""
+    port = _free_port()
+    mp.start_processes(_ws_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    for r in range(2):
+        mean, std, w, b, full_mean, full_std = np.load(tmp_path / f"ws{r}.npy", allow_pickle=True)
+        np.testing.assert_allclose(mean, full_mean, rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(std, full_std, rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(w, np.full((3, 2), 1.5))
+        np.testing.assert_allclose(b, np.array([5.0, 1.0]))

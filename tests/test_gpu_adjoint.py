@@ -221,3 +221,69 @@ def test_restitution_is_refused():
         SubstepAdjoint(solver)(c, a.body_q, a.body_qd, a.body_f, z(a.body_q), z(a.body_qd), DT)
     with pytest.raises(NotImplementedError):
         Rollout(CollisionPipeline(m, contact_matching="latest"), SolverXPBD(m), DT)
+
+
+def test_c5_stack_com_gradient():
+    """The differentiation workload: 16-box stacks, 64 substeps at dt = 1/600 with 8 iterations,
+    loss = sum over worlds of |COM_final - target|^2, gradient with respect to the initial twists
+    through the checkpointed rollout (every 16 substeps); central differences of rollouts that replay
+    the nominal rollout's contacts agree (best of three step sizes, relative 1e-1)."""
+    m, info = scenes.scene_c5(worlds=3, device=DEV)
+    pipe = CollisionPipeline(m)
+    solver = SolverXPBD(m, iterations=info["iterations"])
+    dt, n_sub = info["dt"], info["substeps"]
+    B, W = m.body_count, m.world_count
+    s0 = m.state()
+    q0, qd0 = s0.body_q.clone(), s0.body_qd.clone()
+    f = torch.zeros(B, 6, device=DEV)
+    world = torch.repeat_interleave(torch.arange(W, device=DEV), B // W)
+    target = torch.zeros(W, 3, device=DEV)
+    target.index_add_(0, world, q0[:, :3])
+    target = target / (B // W) + torch.tensor([0.05, -0.02, 0.0], device=DEV)
+
+    def com_loss(q):
+        com = torch.zeros(W, 3, dtype=q.dtype, device=DEV)
+        com.index_add_(0, world, q[:, :3])
+        com = com / (B // W)
+        return ((com - target.to(q.dtype)) ** 2).sum()
+
+    qv, qdv = q0.clone().requires_grad_(True), qd0.clone().requires_grad_(True)
+    q1, _ = simulate(pipe, solver, qv, qdv, f, substeps=n_sub, dt=dt, checkpoint_every=16)
+    com_loss(q1).backward()
+    assert bool(torch.isfinite(qdv.grad).all()) and float(qdv.grad.abs().max()) > 0.0
+
+    a, b = m.state(), m.state()
+    c = pipe.contacts()
+    a.body_q.copy_(q0)
+    a.body_qd.copy_(qd0)
+    recs = []
+    for _ in range(n_sub):
+        a.body_f.zero_()
+        pipe.collide(a, c)
+        recs.append({k: c._seg[k].clone() for k in ("rec", "world_base", "world_count")})
+        solver.step(a, b, None, c, dt)
+        a, b = b, a
+    torch.testing.assert_close(a.body_q, q1.detach(), rtol=0, atol=0)
+
+    def loss(q, qd, ff):
+        qq, _ = _replay_dt(solver, m, c, recs, q, qd, ff, dt)
+        return float(com_loss(qq.double()))
+
+    checks = [("qd", 0, 0), ("qd", 5, 1), ("qd", 15, 3), ("qd", 20, 5), ("q", 3, 0), ("q", 40, 1)]
+    bad = _fd_mismatches(loss, {"q": q0, "qd": qd0, "f": f}, {"q": qv.grad, "qd": qdv.grad, "f": torch.zeros_like(f)},
+                         checks, rel=1e-1, abs_=1e-4)
+    assert not bad, bad
+
+
+def _replay_dt(solver, m, c, recs, q, qd, f, dt):
+    a, b = m.state(), m.state()
+    a.body_q.copy_(q)
+    a.body_qd.copy_(qd)
+    for r in recs:
+        a.body_f.copy_(f)
+        for k, v in r.items():
+            c._seg[k].copy_(v)
+        c._seg_valid = True
+        solver.step(a, b, None, c, dt)
+        a, b = b, a
+    return a.body_q, a.body_qd
