@@ -471,7 +471,7 @@ gjk_prefilter_kernel(NbModelDesc m, NbContactSeg seg) {
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n1; base += stride) {
         const int i = base + lane;
-        bool keep = false, boxes = false;
+        bool keep = false;
         int2 e = make_int2(0, 0);
         if (i < n1) {
             e = queue[2 * (size_t)P - 1 - i];
@@ -481,36 +481,25 @@ gjk_prefilter_kernel(NbModelDesc m, NbContactSeg seg) {
             const int nloc = m.world_shape_start[e.y + 1] - s0;
             const int sa = la < nloc ? s0 + la : m.global_shapes[la - nloc];
             const int sb = lb < nloc ? s0 + lb : m.global_shapes[lb - nloc];
-            const Geom ga = load_geom(geom + 5 * (size_t)sa, sa), gb = load_geom(geom + 5 * (size_t)sb, sb);
-            keep = !gjk_pair_separated(ga, gb);
-            boxes = ga.type == NB_GEO_BOX && gb.type == NB_GEO_BOX;
+            keep = !gjk_pair_separated(load_geom(geom + 5 * (size_t)sa, sa), load_geom(geom + 5 * (size_t)sb, sb));
             if (!keep) seg.counts[e.x] = 0;
         }
-        // survivors are binned by shape pair so that the MPR/GJK warps run one
-        // support-function mix: box-box from the queue front up, every other
-        // pair down from just below the unread back part of the queue
-        const unsigned bal_b = __ballot_sync(kFull, keep && boxes), bal_o = __ballot_sync(kFull, keep && !boxes);
-        int off_b = 0, off_o = 0;
-        if (lane == 0 && bal_b) off_b = atomicAdd(&seg.work_counter[5], __popc(bal_b));
-        if (lane == 0 && bal_o) off_o = atomicAdd(&seg.work_counter[6], __popc(bal_o));
-        off_b = __shfl_sync(kFull, off_b, 0);
-        off_o = __shfl_sync(kFull, off_o, 0);
-        const unsigned below = (1u << lane) - 1u;
-        if (keep && boxes) queue[off_b + __popc(bal_b & below)] = e;
-        if (keep && !boxes) queue[2 * (size_t)P - 1 - n1 - (off_o + __popc(bal_o & below))] = e;
+        const unsigned bal = __ballot_sync(kFull, keep);
+        int off = 0;
+        if (lane == 0 && bal) off = atomicAdd(&seg.work_counter[5], __popc(bal));
+        off = __shfl_sync(kFull, off, 0);
+        if (keep) queue[off + __popc(bal & ((1u << lane) - 1u))] = e;
     }
 }
 
 // MPR / GJK / manifold on the items that survived the prefilter
 __global__ void __launch_bounds__(kNT)
 narrow_gjk_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
-    // box-box survivors at [0, nb), the others at 2P - 1 - n1 - [0, no) (see gjk_prefilter_kernel)
-    const int nbx = seg.work_counter[5], no = seg.work_counter[6], n1 = seg.work_counter[3];
-    const size_t top = 2 * (size_t)m.pair_count - 1 - n1;
+    const int n = seg.work_counter[5];
     const int2* queue = reinterpret_cast<const int2*>(seg.queue);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nbx + no; i += gridDim.x * blockDim.x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         NarrowItem it;
-        narrow_setup(m, seg, body_q, i < nbx ? queue[i] : queue[top - (i - nbx)], it);
+        narrow_setup(m, seg, body_q, queue[i], it);
         gjk_pair(it.wr, it.ga, it.gb);
         narrow_finish(seg, it);
     }
@@ -706,7 +695,7 @@ cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const N
     }
     e = cudaMemsetAsync(seg->work_counter, 0, 4 * sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(seg->work_counter + 5, 0, 2 * sizeof(int32_t), stream);
+    e = cudaMemsetAsync(seg->work_counter + 5, 0, sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
     const int sms = sm_count();
     broadphase_kernel<<<sms * 4, kBT, smem, stream>>>(*m, body_q, *seg);
