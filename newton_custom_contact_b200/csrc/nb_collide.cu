@@ -2,7 +2,8 @@
 //
 // Kernels per substep:
 //   1. broadphase_kernel -- one warp per world (worlds pulled from a device
-//      counter, largest first).  The warp computes every shape's world
+//      counter, largest first; worlds with 2048+ candidate pairs are shared
+//      by the whole CTA).  The warp computes every shape's world
 //      transform and AABB (compute_shape_aabbs, newton/_src/sim/collide.py:150-275),
 //      stages the AABBs in shared memory and the full geometry in global
 //      memory, then tests the world's candidate pairs (explicit pair list
