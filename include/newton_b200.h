@@ -374,6 +374,21 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
                  const NbContactSeg* seg, float dt, int32_t grid_ctas, void* stream);
 
 /*
+ * n_substeps x (nb_collide, nb_publish_contacts, nb_xpbd_step) in one call --
+ * the frame loop of the reference's examples (collide + SolverXPBD.step per
+ * substep, e.g. newton/examples/contacts/example_pyramid.py:155-161) without a host round
+ * trip per substep.  The state ping-pongs between io's input and output
+ * buffers: body_q_in / body_qd_in hold the initial state and are overwritten
+ * (as the reference's state_in is), body_q_out / body_qd_out receive the
+ * final state; body_f_in is applied at every substep.  The plain solve only:
+ * contact_impulse, body_parent_f and ws_lambda must be NULL
+ * (NB_ERR_UNSUPPORTED).  pub receives the last substep's contacts.
+ */
+int nb_xpbd_substeps(const NbModelDesc* model, const NbXpbdParams* params, const NbStepIO* io,
+                     const NbContactSeg* seg, const NbContactsPublic* pub, float dt, int32_t n_substeps,
+                     int32_t grid_ctas, void* stream);
+
+/*
  * Match the contacts nb_publish_contacts just wrote (with sort keys) against
  * the previous call's, then (sticky) replay matched rows, build the report and
  * save this frame for the next call.  Replaces ContactMatcher.match /

@@ -170,6 +170,39 @@ int nb_xpbd_step_adjoint(const NbModelDesc* model, const NbXpbdParams* params, c
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
 
+int nb_xpbd_substeps(const NbModelDesc* model, const NbXpbdParams* params, const NbStepIO* io,
+                     const NbContactSeg* seg, const NbContactsPublic* pub, float dt, int32_t n_substeps,
+                     int32_t grid_ctas, void* stream) {
+    if (!io || n_substeps < 0) return NB_ERR_INVALID;
+    // the plain solve only: per-step outputs (impulses, parent forces) and per-step inputs (warm start)
+    // have no meaning across several substeps of one call
+    if (io->contact_impulse || io->body_parent_f || io->ws_lambda) return NB_ERR_UNSUPPORTED;
+    if (n_substeps == 0) return NB_OK;
+    // substep k reads one pair of state buffers and writes the other (the step leaves its input unchanged)
+    NbStepIO cur = *io;
+    int rc = NB_OK;
+    for (int k = 0; k < n_substeps; ++k) {
+        const bool odd = (k & 1) != 0;
+        cur.body_q_in = odd ? io->body_q_out : io->body_q_in;
+        cur.body_qd_in = odd ? io->body_qd_out : io->body_qd_in;
+        cur.body_q_out = odd ? const_cast<float*>(io->body_q_in) : io->body_q_out;
+        cur.body_qd_out = odd ? const_cast<float*>(io->body_qd_in) : io->body_qd_out;
+        if ((rc = nb_collide(model, cur.body_q_in, seg, grid_ctas, stream))) return rc;
+        if ((rc = nb_publish_contacts(model, seg, pub, stream))) return rc;
+        if ((rc = nb_xpbd_step(model, params, &cur, seg, dt, grid_ctas, stream))) return rc;
+    }
+    if ((n_substeps & 1) == 0 && model->body_count > 0) {
+        // an even count ends in the input buffers: one copy per array into the outputs
+        cudaStream_t s = (cudaStream_t)stream;
+        if (cudaMemcpyAsync(io->body_q_out, io->body_q_in, sizeof(float) * 7 * (size_t)model->body_count,
+                            cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(io->body_qd_out, io->body_qd_in, sizeof(float) * 6 * (size_t)model->body_count,
+                            cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            return NB_ERR_CUDA;
+    }
+    return NB_OK;
+}
+
 int nb_match_contacts(const NbModelDesc* model, const float* body_q, const NbContactsPublic* pub,
                       const NbContactSeg* seg, const NbMatchState* st, void* stream) {
     int rc = check_model(model);

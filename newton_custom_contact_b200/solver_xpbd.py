@@ -192,6 +192,58 @@ class SolverXPBD:
         self._contact_impulse_capacity = contacts.rigid_contact_max if contacts is not None else 0
         self._last_dt = dt
 
+    def step_substeps(self, state_in, state_out, contacts: Contacts, dt: float, substeps: int) -> None:
+        """`substeps` x (collide, step) in one library call (``nb_xpbd_substeps``; no counterpart in the
+        reference, whose examples loop ``model.collide`` + ``solver.step`` on the host): the pipeline that
+        made `contacts` collides at every substep, ``state_in.body_f`` is applied at every substep,
+        ``state_out`` receives the final state and ``state_in`` is overwritten (ping-pong buffer).
+        The plain solve only: no contact forces, ``body_parent_f`` or warm start."""
+        model = self.model
+        _lib.require_cuda(model.device)
+        if substeps < 0:
+            raise ValueError("substeps must be non-negative")
+        if model.body_count == 0 or substeps == 0:
+            return
+        if contacts.force is not None or state_out.body_parent_f is not None or self.warm_start is not None:
+            raise ValueError("step_substeps runs the plain solve only (no contact forces, body_parent_f or warm "
+                             "start)")
+        B = model.body_count
+        for name, t, shape in (("state_in.body_q", state_in.body_q, (B, 7)), ("state_in.body_qd", state_in.body_qd, (B, 6)),
+                               ("state_in.body_f", state_in.body_f, (B, 6)), ("state_out.body_q", state_out.body_q, (B, 7)),
+                               ("state_out.body_qd", state_out.body_qd, (B, 6))):
+            self._check_state(name, t, shape)
+        pipe = contacts._layout
+        if pipe is None:
+            raise ValueError("contacts must come from a CollisionPipeline (pipeline.contacts())")
+        if getattr(pipe, "contact_matching", "disabled") != "disabled":
+            raise ValueError("step_substeps does not run contact matching; call collide and step per substep")
+        if contacts._seg is None:
+            pipe.attach_segments(contacts)
+        if contacts._world_offset.numel() != model.world_count + 1:
+            contacts._world_offset = torch.zeros(model.world_count + 1, dtype=torch.int64, device=model.device)
+        lib = _lib.load()
+        desc = pipe.desc()
+        control = model.control(clone_variables=False)
+        io = NbStepIO()
+        io.body_q_in, io.body_qd_in, io.body_f_in = ptr(state_in.body_q), ptr(state_in.body_qd), ptr(state_in.body_f)
+        io.body_q_out, io.body_qd_out = ptr(state_out.body_q), ptr(state_out.body_qd)
+        io.joint_target_pos = ptr(control.joint_target_pos)
+        io.joint_target_vel = ptr(control.joint_target_vel)
+        io.joint_f = ptr(control.joint_f)
+        if desc.step_mode == 3:
+            nbytes = int(lib.nb_step_scratch_size(C.byref(desc)))
+            if self._step_scratch is None or self._step_scratch.numel() < nbytes:
+                self._step_scratch = torch.empty(nbytes, dtype=torch.uint8, device=model.device)
+            io.step_scratch = ptr(self._step_scratch)
+        params = self.params()
+        _lib.check("nb_xpbd_substeps", lib.nb_xpbd_substeps(
+            C.byref(desc), C.byref(params), C.byref(io), C.byref(pipe.seg_struct(contacts)),
+            C.byref(pipe.public_struct(contacts)), float(dt), int(substeps), pipe.grid(),
+            C.c_void_p(_lib.stream_handle(model.device))))
+        contacts.contact_generation.add_(int(substeps))
+        contacts._seg_valid = True
+        self._last_dt = dt
+
     def update_contacts(self, contacts: Contacts, state=None) -> None:
         """Populate ``contacts.force`` (force [N], torque [N m] per contact) from the impulses the last
         ``step`` accumulated (solver_xpbd.py:766-821); same errors as the reference."""

@@ -234,3 +234,31 @@ def test_collide_bit_exact_in_piled_state(cuda, orc):
     segs = orc.collide(model, pipe.layout, s0.body_q.cpu().numpy())
     table = _assert_contacts_equal(model, pipe, contacts, segs, orc)
     assert table.shape[0] > 5000
+
+
+@pytest.mark.parametrize("n", [1, 4, 5])
+def test_substeps_entry_matches_host_loop(cuda, n):
+    """nb_xpbd_substeps (SolverXPBD.step_substeps) against the host loop of collide + step, bit for bit,
+    for odd and even substep counts (the state ping-pongs between the two buffers)."""
+    model, info = _small_c2(worlds=24)
+    dt = info["dt"] / info["substeps"]
+    pipe = CollisionPipeline(model)
+    solver = SolverXPBD(model, iterations=info["iterations"])
+    s0, s1 = model.state(), model.state()
+    c = pipe.contacts()
+    for _ in range(n):
+        s0.clear_forces()
+        pipe.collide(s0, c)
+        solver.step(s0, s1, None, c, dt)
+        s0, s1 = s1, s0
+    torch.cuda.synchronize()
+    ref_q, ref_qd = s0.body_q.cpu().numpy(), s0.body_qd.cpu().numpy()
+    ref_count = int(c.rigid_contact_count.item())
+    a, b = model.state(), model.state()
+    c2 = pipe.contacts()
+    a.clear_forces()
+    solver.step_substeps(a, b, c2, dt, n)
+    torch.cuda.synchronize()
+    assert _bits_equal(b.body_q.cpu().numpy(), ref_q) and _bits_equal(b.body_qd.cpu().numpy(), ref_qd)
+    assert int(c2.rigid_contact_count.item()) == ref_count
+    assert pipe.status(c2) == 0
