@@ -1,6 +1,6 @@
 """Train the learned warm start on the uneven-worlds scene and evaluate its gain.
 
-    python -m newton_custom_contact_b200.train_warmstart --out newton_custom_contact_b200/data/warmstart_c2.npz
+    python -m newton_custom_contact_b200.train_warmstart [--scene c2|c5]
 
 Samples are (features, lambda) pairs of the plain solver with the teacher's
 iteration count: first along plain rollouts, then (DAgger rounds) at the
@@ -28,10 +28,23 @@ from .metrics import penetration_stats
 from .warmstart import WarmStart, WarmStartNet, corrections
 
 DT = 1.0 / 480.0
+SCENE = "c2"  # "c2": uneven worlds of boxes / spheres / capsules; "c5": 16-box stacks (dt 1/600)
+
+
+def set_scene(kind: str) -> None:
+    """Scene family the training / evaluation helpers build (and its substep)."""
+    global SCENE, DT
+    if kind not in ("c2", "c5"):
+        raise ValueError("scene must be 'c2' or 'c5'")
+    SCENE = kind
+    DT = 1.0 / 480.0 if kind == "c2" else 1.0 / 600.0
 
 
 def make_scene(seed: int, worlds: int, device):
-    m, _ = scenes.scene_c2(seed=seed, worlds=worlds, device=device)
+    if SCENE == "c5":
+        m, _ = scenes.scene_c5(seed=seed, worlds=worlds, device=device)
+    else:
+        m, _ = scenes.scene_c2(seed=seed, worlds=worlds, device=device)
     pipe = CollisionPipeline(m, contact_matching="latest")
     return m, pipe
 
@@ -187,7 +200,10 @@ def evaluate(net: WarmStartNet, device="cuda", worlds: int = 1024, seed: int = 1
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "data", "warmstart_c2.npz"))
+    ap.add_argument("--scene", default="c2", choices=["c2", "c5"])
+    ap.add_argument("--out", default=None, help="network file (default: data/warmstart_<scene>.npz)")
+    ap.add_argument("--train-seed", type=int, default=None)
+    ap.add_argument("--eval-seed", type=int, default=None)
     ap.add_argument("--worlds", type=int, default=1024)
     ap.add_argument("--substeps", type=int, default=240)
     ap.add_argument("--dagger", type=int, default=1)
@@ -197,17 +213,24 @@ def main():
     ap.add_argument("--report", default=None)
     ap.add_argument("--eval-only", action="store_true", help="evaluate the network saved at --out")
     a = ap.parse_args()
+    set_scene(a.scene)
+    if a.out is None:
+        a.out = os.path.join(os.path.dirname(__file__), "data", f"warmstart_{a.scene}.npz")
+    # training and evaluation scenes differ (unseen seed at evaluation)
+    train_seed = a.train_seed if a.train_seed is not None else (2 if a.scene == "c2" else 6)
+    eval_seed = a.eval_seed if a.eval_seed is not None else (1 if a.scene == "c2" else 5)
     t0 = time.time()
     if a.eval_only:
         net = WarmStartNet.load(a.out)
         res = {}
     else:
-        net, info = train(worlds=a.worlds, substeps=a.substeps, dagger_rounds=a.dagger, epochs=a.epochs,
-                          student_iterations=a.student_iterations, fraction=a.fraction)
+        net, info = train(worlds=a.worlds, seed=train_seed, substeps=a.substeps, dagger_rounds=a.dagger,
+                          epochs=a.epochs, student_iterations=a.student_iterations, fraction=a.fraction)
         os.makedirs(os.path.dirname(a.out), exist_ok=True)
         net.save(a.out)
         res = {"train": info, "train_s": time.time() - t0}
-    res["eval"] = evaluate(net, worlds=a.worlds, student_iterations=(a.student_iterations, 4))
+    res["scene"] = a.scene
+    res["eval"] = evaluate(net, worlds=a.worlds, seed=eval_seed, student_iterations=(a.student_iterations, 4))
     print(json.dumps(res, indent=1))
     if a.report:
         with open(a.report, "w") as f:
