@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 11
+#define NB_ABI_VERSION 12
 
 enum {
     NB_OK = 0,
@@ -97,7 +97,8 @@ typedef struct NbModelDesc {
     int32_t max_world_shapes;     /* max world shapes + global shapes */
     int32_t max_world_joints;
     int32_t max_world_pairs;
-    int32_t pad0;
+    int32_t all_joints_free;      /* 1: every joint is FREE (no joint constraints: the step may use its
+                                     lean kernel); 0: unknown or not */
     int64_t contact_capacity;     /* contact slots = 5 * pair_count */
 
     /* bodies [B] */

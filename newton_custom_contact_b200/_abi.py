@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 11
+NB_ABI_VERSION = 12
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -90,7 +90,7 @@ class NbModelDesc(C.Structure):
         ("max_world_shapes", C.c_int32),
         ("max_world_joints", C.c_int32),
         ("max_world_pairs", C.c_int32),
-        ("pad0", C.c_int32),
+        ("all_joints_free", C.c_int32),
         ("contact_capacity", C.c_int64),
         ("body_com", _fp),
         ("body_mass", _fp),

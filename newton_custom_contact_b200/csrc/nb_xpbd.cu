@@ -967,7 +967,12 @@ __device__ __noinline__ void warm_start(const NbModelDesc& m, const NbStepIO& io
 // One world's substep with a group of G threads: stage, joint forces,
 // integrate, `iterations` x (contacts, weighted apply, joints, apply),
 // restitution, write-back.  The caller carved the world's slab into S.
-template <int G, class SB>
+// kLean: the variant for models whose joints are all FREE, called without
+// restitution, warm start or per-contact impulses.  It drops those passes and
+// the joint solve at compile time (each of them would be a no-op for such a
+// call), which keeps the world's shared-memory view in registers instead of
+// on the stack; the arithmetic of what remains is the same code.
+template <int G, bool kLean, class SB>
 __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdParams& p, const NbStepIO& io,
                                            const NbContactSeg& seg, bool has_contacts, float dt, int w, SB& S,
                                            int g, int t, int* flag, int* nact, unsigned char* list,
@@ -1042,18 +1047,22 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
     const int nc = has_contacts ? seg.world_count[w] : 0;
     const int64_t rec_base = has_contacts ? seg.world_base[w] : 0;
     const float4* R = rec + (size_t)rec_base * 5;
-    const bool want_imp = has_contacts && io.contact_impulse != nullptr;
+    const bool want_imp = !kLean && has_contacts && io.contact_impulse != nullptr;
     unsigned bad = 0u;
-    if (has_contacts && io.ws_lambda)
-        warm_start<G>(m, io, seg, S, R, nc, rec_base, b0, g, t, nact, dt, &bad);
+    if constexpr (!kLean) {
+        if (has_contacts && io.ws_lambda)
+            warm_start<G>(m, io, seg, S, R, nc, rec_base, b0, g, t, nact, dt, &bad);
+    }
     for (int it = 0; it < p.iterations; ++it) {
         if (has_contacts) {
             contact_pass<G>(m, S, R, nc, list, nact, g, t, p.rigid_contact_relaxation, dt,
                             weighting, &bad, want_imp ? io.impulse_scratch + (size_t)rec_base * 6 : nullptr);
-            if (want_imp) {
-                accumulate_impulses<G>(S, R, nc, rec_base, seg.rec_index, io.impulse_scratch,
-                                       io.contact_impulse, io.contact_impulse_capacity, weighting, t);
-                group_sync<G>(g);
+            if constexpr (!kLean) {
+                if (want_imp) {
+                    accumulate_impulses<G>(S, R, nc, rec_base, seg.rec_index, io.impulse_scratch,
+                                           io.contact_impulse, io.contact_impulse_capacity, weighting, t);
+                    group_sync<G>(g);
+                }
             }
             for (int i = t; i < nb; i += G) {
                 V3 dl, da;
@@ -1085,9 +1094,11 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
             group_sync<G>(g);
         }
         if (model_joints && (world_joints || !has_contacts)) {
-            for (int j = j0 + t; j < j1; j += G)
-                solve_joint(m, S, b0, j, io.joint_target_pos, io.joint_target_vel, p, dt, &bad,
-                            io.body_parent_f ? io.joint_impulse : nullptr);
+            if constexpr (!kLean) {  // solve_joint returns at once for FREE joints
+                for (int j = j0 + t; j < j1; j += G)
+                    solve_joint(m, S, b0, j, io.joint_target_pos, io.joint_target_vel, p, dt, &bad,
+                                io.body_parent_f ? io.joint_impulse : nullptr);
+            }
             group_sync<G>(g);
             for (int i = t; i < nb; i += G) {
                 V3 dl, da;
@@ -1102,9 +1113,11 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
         }
     }
     // ---- restitution (solver_xpbd.py:685-755), after all iterations
-    if (has_contacts && p.enable_restitution) {
-        for (int k = t; k < nc; k += G)
-            restitution_contact(m, S, R + (size_t)k * 5, b0, io.body_q_in, io.body_qd_in, dt, &bad);
+    if (!kLean && has_contacts && p.enable_restitution) {
+        if constexpr (!kLean) {
+            for (int k = t; k < nc; k += G)
+                restitution_contact(m, S, R + (size_t)k * 5, b0, io.body_q_in, io.body_qd_in, dt, &bad);
+        }
         group_sync<G>(g);
         // apply_body_delta_velocities (kernels.py:881-887)
         for (int i = t; i < nb; i += G) {
@@ -1161,7 +1174,7 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
 // Batch mode: a CTA takes a batch of worlds (host-packed into one arena, one
 // world per group of G threads) from a device counter; the CTA waits for all
 // of a batch's worlds before the next batch reuses the arena.
-template <int G>
+template <int G, bool kLean>
 __global__ void __launch_bounds__(kST, 2)
 xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, int has_contacts, float dt) {
     extern __shared__ __align__(16) unsigned char arena[];
@@ -1184,7 +1197,7 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
             const int b0 = m.world_body_start[w];
             const int nb = m.world_body_start[w + 1] - b0;
             SBodiesT<false> S = sbodies_carve<false>(arena + 4 * (size_t)m.batch_slab[b * kGroups + g], m, b0, nb);
-            step_world<G>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g], s_list[g],
+            step_world<G, kLean>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g], s_list[g],
                           &s_bad);
         }
         __syncthreads();  // every group is done with the arena before the next batch
@@ -1203,7 +1216,7 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
 // never waits for another group's world.  The host picks G and the slab
 // layout so that the largest world fits one share (kCompact stages only the
 // mutable body state).
-template <int G, bool kCompact>
+template <int G, bool kCompact, bool kLean>
 __global__ void __launch_bounds__(kST, 2)
 xpbd_step_group_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, int has_contacts, float dt) {
     extern __shared__ __align__(16) unsigned char arena[];
@@ -1240,7 +1253,7 @@ xpbd_step_group_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg 
             continue;
         }
         SBodiesT<kCompact> S = sbodies_carve<kCompact>(region, m, b0, nb);
-        step_world<G>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g], s_list[g],
+        step_world<G, kLean>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g], s_list[g],
                       &s_bad);
         group_sync<G>(g);
     }
@@ -1507,36 +1520,57 @@ cudaError_t nb_launch_contact_forces(const float* imp, const int32_t* count, int
 }
 
 namespace {
-template <int G>
-cudaError_t launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
-                        float dt, int grid, cudaStream_t stream) {
+// the lean step kernel applies: every joint is FREE and the call asks for
+// none of restitution, warm start and per-contact impulses
+bool step_is_lean(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io) {
+    return m->all_joints_free == 1 && p->enable_restitution == 0 && io->ws_lambda == nullptr &&
+           io->contact_impulse == nullptr;
+}
+
+template <int G, bool kLean>
+cudaError_t launch_step_variant(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
+                                const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
     const size_t smem = nb_step_smem_bytes(m);
     static size_t configured = 0;
     if (smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(xpbd_step_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(xpbd_step_kernel<G, kLean>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         configured = smem;
     }
     const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
-    xpbd_step_kernel<G><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
+    xpbd_step_kernel<G, kLean><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
+    return cudaGetLastError();
+}
+
+template <int G>
+cudaError_t launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
+                        float dt, int grid, cudaStream_t stream) {
+    return step_is_lean(m, p, io) ? launch_step_variant<G, true>(m, p, io, seg, dt, grid, stream)
+                                  : launch_step_variant<G, false>(m, p, io, seg, dt, grid, stream);
+}
+
+template <int G, bool kCompact, bool kLean>
+cudaError_t launch_step_group_variant(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
+                                      const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
+    const size_t smem = nb_step_smem_bytes(m);
+    static size_t configured = 0;
+    if (smem > configured) {
+        cudaError_t e = cudaFuncSetAttribute(xpbd_step_group_kernel<G, kCompact, kLean>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = smem;
+    }
+    const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
+    xpbd_step_group_kernel<G, kCompact, kLean><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
     return cudaGetLastError();
 }
 
 template <int G, bool kCompact>
 cudaError_t launch_step_group(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
                               const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
-    const size_t smem = nb_step_smem_bytes(m);
-    static size_t configured = 0;
-    if (smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(xpbd_step_group_kernel<G, kCompact>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = smem;
-    }
-    const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
-    xpbd_step_group_kernel<G, kCompact><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
-    return cudaGetLastError();
+    return step_is_lean(m, p, io) ? launch_step_group_variant<G, kCompact, true>(m, p, io, seg, dt, grid, stream)
+                                  : launch_step_group_variant<G, kCompact, false>(m, p, io, seg, dt, grid, stream);
 }
 
 template <bool kCompact>

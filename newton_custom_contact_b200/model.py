@@ -12,7 +12,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from ._abi import NbModelDesc, ptr
+from ._abi import JointType, NbModelDesc, ptr
 
 
 def _dev(device) -> torch.device:
@@ -308,6 +308,8 @@ class Model:
         d.max_world_bodies = self.max_world_bodies
         d.max_world_shapes = self.max_world_shapes
         d.max_world_joints = self.max_world_joints
+        jt = np.asarray(self._host["joint_type"])
+        d.all_joints_free = int(bool(np.all(jt == int(JointType.FREE))))
         names = {
             "body_com": "body_com", "body_mass": "body_mass", "body_inv_mass": "body_inv_mass",
             "body_inertia": "body_inertia", "body_inv_inertia": "body_inv_inertia", "body_flags": "body_flags",
