@@ -36,6 +36,7 @@ using namespace nbg;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kBT = 256;             // broad phase: threads per CTA (8 worlds in flight)
 constexpr int kNT = 128;             // narrow phase: threads per CTA
+constexpr int kGjkMinBlocks = 12;     // MPR/GJK kernel: resident CTAs per SM the registers are fitted to
 constexpr int kSlotF4 = 25;          // 5 contacts x 5 float4 per candidate
 
 __device__ __forceinline__ void store_geom(float4* g, const Geom& x) {
@@ -493,8 +494,11 @@ gjk_prefilter_kernel(NbModelDesc m, NbContactSeg seg) {
     }
 }
 
-// MPR / GJK / manifold on the items that survived the prefilter
-__global__ void __launch_bounds__(kNT)
+// MPR / GJK / manifold on the items that survived the prefilter.  Latency
+// and divergence bound: 12 CTAs per SM (48 warps, 40 registers, a few bytes
+// of spills) hide more of it than the unconstrained 122 registers at 4 CTAs
+// (collide 0.57 vs 0.72 ms per substep on 4096 uneven worlds).
+__global__ void __launch_bounds__(kNT, kGjkMinBlocks)
 narrow_gjk_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
     const int n = seg.work_counter[5];
     const int2* queue = reinterpret_cast<const int2*>(seg.queue);
@@ -554,7 +558,11 @@ __global__ void __launch_bounds__(1024) world_scan_kernel(int W, const int32_t* 
 }
 
 // Dense public Contacts arrays ordered by (world, key), and the same contacts
-// as solver records (rec), contiguous per world; one warp per world.
+// as solver records (rec), contiguous per world; one warp per world.  The
+// warp scans the contact counts of 32 candidates at a time, then its lanes
+// take the chunk's outputs in order (lane k writes output k, k + 32, ...),
+// each finding its candidate among the 32 scanned counts, so consecutive
+// lanes store to consecutive rows of every array.
 __global__ void __launch_bounds__(256) publish_kernel(NbModelDesc m, NbContactSeg seg, NbContactsPublic pub) {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -569,17 +577,26 @@ __global__ void __launch_bounds__(256) publish_kernel(NbModelDesc m, NbContactSe
         for (int base = 0; base < nc; base += 32) {
             const int i = base + lane;
             const int n = i < nc ? (int)seg.counts[c0 + i] : 0;
-            int x = n;
+            int x = n;  // inclusive scan of the chunk's counts
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 int y = __shfl_up_sync(kFull, x, o);
                 if (lane >= o) x += y;
             }
             const int tot = __shfl_sync(kFull, x, 31);
-            const int excl = x - n;
-            for (int j = 0; j < n; ++j) {
-                const int64_t d = dst0 + running + excl + j;
-                const float4* sl = slots + ((size_t)(c0 + i) * 5 + j) * 5;
+            for (int o0 = 0; o0 < tot; o0 += 32) {
+                const int o = o0 + lane;
+                // source lane: the number of lanes whose inclusive sum is <= o
+                int src = 0;
+#pragma unroll
+                for (int k = 0; k < 32; ++k) src += __shfl_sync(kFull, x, k) <= o ? 1 : 0;
+                const int src_c = src < 31 ? src : 31;
+                const int x_src = __shfl_sync(kFull, x, src_c);
+                const int n_src = __shfl_sync(kFull, n, src_c);
+                if (o >= tot) continue;
+                const int j = o - (x_src - n_src);
+                const int64_t d = dst0 + running + o;
+                const float4* sl = slots + ((size_t)(c0 + base + src) * 5 + j) * 5;
                 const float4 a = sl[0], b = sl[1], c = sl[2], e = sl[3], f = sl[4];
                 // solver record: the tag moves next to the normal so the
                 // penetration test reads the first 48 bytes only
