@@ -72,17 +72,6 @@ __device__ __forceinline__ bool analytic_pair(int ta, int tb) {
     return false;
 }
 
-__device__ __forceinline__ int warp_exclusive_scan(int v, int lane, int& total) {
-    int x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(kFull, x, o);
-        if (lane >= o) x += y;
-    }
-    total = __shfl_sync(kFull, x, 31);
-    return x - v;
-}
-
 constexpr int kQB = 160;  // staged queue items per warp and class (> 128 = one chunk's maximum)
 
 // push a warp's staged items: analytic queue from the front (sign = 0), MPR/GJK
@@ -122,17 +111,18 @@ __device__ __forceinline__ void stage_shapes(const NbModelDesc& m, const float* 
     }
 }
 
-// the lane's four pairs q .. q + 3 (q a multiple of 4) of a 128-pair chunk:
-// AABB overlap bits and, among the hits, the pairs the analytic path finishes
-__device__ __forceinline__ void test_pairs(uint4 pk, int q, int p0, int p1, const float4* lo, const float4* hi, int ns,
-                                           uint32_t* status, unsigned& hit, unsigned& easy) {
-    const unsigned pw[4] = {pk.x, pk.y, pk.z, pk.w};
+// the lane's four pairs q + 32 r (r = 0..3) of a 128-pair chunk (q = chunk
+// start + lane, so neighbouring lanes read neighbouring shape slots: no bank
+// conflicts): AABB overlap bits and, among the hits, the pairs the analytic
+// path finishes
+__device__ __forceinline__ void test_pairs(const unsigned (&pw)[4], int q, int p1, const float4* lo, const float4* hi,
+                                           int ns, uint32_t* status, unsigned& hit, unsigned& easy) {
     hit = 0u;
     easy = 0u;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const int p = q + r;
-        if (p < p0 || p >= p1) continue;
+        const int p = q + 32 * r;
+        if (p >= p1) continue;
         const int la = (int)(pw[r] & 0xFFFFu), lb = (int)(pw[r] >> 16);
         // slots index shared memory: never trust them blindly
         if (la >= ns || lb >= ns) {
@@ -158,16 +148,23 @@ struct QueueStage {
     int nqa, nqg;  // warp-uniform fill levels
 };
 
-// writes a chunk's hits (masks of this lane, warp-wide offsets) as candidates
+// writes a chunk's hits (bit r of this lane = pair q + 32 r) as candidates
 // cand_base + running index, in pair order, and stages their queue items
 __device__ __forceinline__ void emit_chunk(const NbContactSeg& seg, int2* queue, long long gjk_back, QueueStage& st,
                                            int q, unsigned hit, unsigned easy, int w, int cand_base, int lane,
                                            int& tot_h) {
-    int tot_a;
-    const int nh = __popc(hit), na = __popc(easy);
-    const int off_h = warp_exclusive_scan(nh, lane, tot_h);
-    const int off_a = warp_exclusive_scan(na, lane, tot_a);
-    const int off_g = off_h - off_a, tot_g = tot_h - tot_a;
+    const unsigned below = (1u << lane) - 1u;
+    unsigned bh[4], ba[4];
+    int tot_a = 0;
+    tot_h = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        bh[r] = __ballot_sync(kFull, (hit >> r) & 1u);
+        ba[r] = __ballot_sync(kFull, (easy >> r) & 1u);
+        tot_h += __popc(bh[r]);
+        tot_a += __popc(ba[r]);
+    }
+    const int tot_g = tot_h - tot_a;
     // make room in the staging buffers (warp-uniform decisions)
     if (st.nqa + tot_a > kQB) {
         flush_queue(st.qa, st.nqa, &seg.work_counter[2], queue, 0, lane);
@@ -177,14 +174,17 @@ __device__ __forceinline__ void emit_chunk(const NbContactSeg& seg, int2* queue,
         flush_queue(st.qg, st.nqg, &seg.work_counter[3], queue, gjk_back, lane);
         st.nqg = 0;
     }
-    int ih = 0, ia = 0, ig = 0;
+    int oh = 0, oa = 0;  // hits and analytic items of the rounds before r
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        if (!(hit >> r & 1u)) continue;
-        const int c = cand_base + off_h + ih++;
-        seg.cand[c] = q + r;
-        if (easy >> r & 1u) st.qa[st.nqa + off_a + ia++] = make_int2(c, w);
-        else st.qg[st.nqg + off_g + ig++] = make_int2(c, w);
+        if ((hit >> r) & 1u) {
+            const int c = cand_base + oh + __popc(bh[r] & below);
+            seg.cand[c] = q + 32 * r;
+            if ((easy >> r) & 1u) st.qa[st.nqa + oa + __popc(ba[r] & below)] = make_int2(c, w);
+            else st.qg[st.nqg + (oh - oa) + __popc(bh[r] & ~ba[r] & below)] = make_int2(c, w);
+        }
+        oh += __popc(bh[r]);
+        oa += __popc(ba[r]);
     }
     st.nqa += tot_a;
     st.nqg += tot_g;
@@ -195,7 +195,7 @@ __device__ __forceinline__ void emit_chunk(const NbContactSeg& seg, int2* queue,
 // pairs are loaded while this chunk is tested)
 __device__ void world_by_warp(const NbModelDesc& m, const float* __restrict__ body_q, const NbContactSeg& seg, int k,
                               float4* lo, float4* hi, QueueStage& st, int lane) {
-    const uint4* packed = reinterpret_cast<const uint4*>(m.pair_shapes);
+    const unsigned* pairs = m.pair_shapes;
     int2* queue = reinterpret_cast<int2*>(seg.queue);
     const long long gjk_back = 2 * (long long)m.pair_count - 1;
     const int w = m.world_order[k];
@@ -204,15 +204,19 @@ __device__ void world_by_warp(const NbModelDesc& m, const float* __restrict__ bo
     __syncwarp();
     const int p0 = m.world_pair_start[w], p1 = m.world_pair_start[w + 1];
     int ncand = 0;
-    int base = p0 & ~3;
-    uint4 nxt = make_uint4(0u, 0u, 0u, 0u);
-    if (base + 4 * lane < p1) nxt = packed[(base + 4 * lane) >> 2];
-    for (; base < p1; base += 128) {
-        const int q = base + 4 * lane;  // multiple of 4: 16-byte aligned
-        const uint4 pk = nxt;
-        if (q + 128 < p1) nxt = packed[(q + 128) >> 2];
+    unsigned nxt[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) nxt[r] = p0 + lane + 32 * r < p1 ? pairs[p0 + lane + 32 * r] : 0u;
+    for (int base = p0; base < p1; base += 128) {
+        const int q = base + lane;
+        unsigned pw[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            pw[r] = nxt[r];
+            nxt[r] = q + 128 + 32 * r < p1 ? pairs[q + 128 + 32 * r] : 0u;
+        }
         unsigned hit, easy;
-        test_pairs(pk, q, p0, p1, lo, hi, ns, seg.status, hit, easy);
+        test_pairs(pw, q, p1, lo, hi, ns, seg.status, hit, easy);
         int tot_h;
         emit_chunk(seg, queue, gjk_back, st, q, hit, easy, w, p0 + ncand, lane, tot_h);
         ncand += tot_h;
@@ -230,7 +234,7 @@ __device__ void world_by_warp(const NbModelDesc& m, const float* __restrict__ bo
 // comparisons per pair) and writes -- the candidates stay in pair order
 __device__ void world_by_cta(const NbModelDesc& m, const float* __restrict__ body_q, const NbContactSeg& seg, int k,
                              float4* lo, float4* hi, QueueStage& st, int* s_run, int warp, int lane) {
-    const uint4* packed = reinterpret_cast<const uint4*>(m.pair_shapes);
+    const unsigned* pairs = m.pair_shapes;
     int2* queue = reinterpret_cast<int2*>(seg.queue);
     const long long gjk_back = 2 * (long long)m.pair_count - 1;
     const int w = m.world_order[k];
@@ -238,17 +242,19 @@ __device__ void world_by_cta(const NbModelDesc& m, const float* __restrict__ bod
     stage_shapes(m, body_q, w, k, lo, hi, reinterpret_cast<float4*>(seg.geom), threadIdx.x, kBT);
     __syncthreads();
     const int p0 = m.world_pair_start[w], p1 = m.world_pair_start[w + 1];
-    const int cbase = p0 & ~3;
+    const int cbase = p0;
     const int nchunks = (p1 - cbase + 127) / 128;
     constexpr int kWarps = kBT / 32;
     const int per = (nchunks + kWarps - 1) / kWarps;
     const int c0 = warp * per, c1 = min(nchunks, c0 + per);
     int count = 0;
     for (int c = c0; c < c1; ++c) {
-        const int q = cbase + 128 * c + 4 * lane;
-        const uint4 pk = q < p1 ? packed[q >> 2] : make_uint4(0u, 0u, 0u, 0u);
+        const int q = cbase + 128 * c + lane;
+        unsigned pw[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) pw[r] = q + 32 * r < p1 ? pairs[q + 32 * r] : 0u;
         unsigned hit, easy;
-        test_pairs(pk, q, p0, p1, lo, hi, ns, seg.status, hit, easy);
+        test_pairs(pw, q, p1, lo, hi, ns, seg.status, hit, easy);
         count += __popc(hit);
     }
 #pragma unroll
@@ -264,10 +270,12 @@ __device__ void world_by_cta(const NbModelDesc& m, const float* __restrict__ bod
     }
     int ncand = 0;
     for (int c = c0; c < c1; ++c) {
-        const int q = cbase + 128 * c + 4 * lane;
-        const uint4 pk = q < p1 ? packed[q >> 2] : make_uint4(0u, 0u, 0u, 0u);
+        const int q = cbase + 128 * c + lane;
+        unsigned pw[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) pw[r] = q + 32 * r < p1 ? pairs[q + 32 * r] : 0u;
         unsigned hit, easy;
-        test_pairs(pk, q, p0, p1, lo, hi, ns, seg.status, hit, easy);
+        test_pairs(pw, q, p1, lo, hi, ns, seg.status, hit, easy);
         int tot_h;
         emit_chunk(seg, queue, gjk_back, st, q, hit, easy, w, p0 + first + ncand, lane, tot_h);
         ncand += tot_h;
