@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned-warm-start arm")
     ap.add_argument("--warm-start-iterations", type=int, default=2)
+    ap.add_argument("--step-schedule", default=None, metavar="MODE/G",
+                    help="fix the step schedule (e.g. groups_compact/32) instead of autotuning it; a run "
+                         "under a profiler serialises launches, so its autotuner may pick another schedule")
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="weak: every rank simulates its own --worlds scene; strong: the ranks split one scene")
     return ap.parse_args()
@@ -317,9 +320,14 @@ def run_ours(args, rank, world_size, local_rank):
     # trials restore the state, so the trajectory does not move
     from newton_custom_contact_b200.schedule import autotune
 
-    with torch.cuda.stream(stream):
-        s0.clear_forces()
-        tune_ms = autotune(pipe, solver, s0, s1, contacts, dt, reps=3)
+    if args.step_schedule:
+        mode, g_threads = args.step_schedule.split("/")
+        pipe.set_step_schedule(int(g_threads), mode)
+        tune_ms = {}
+    else:
+        with torch.cuda.stream(stream):
+            s0.clear_forces()
+            tune_ms = autotune(pipe, solver, s0, s1, contacts, dt, reps=3)
     torch.cuda.synchronize()
     sched = pipe._schedule
 
