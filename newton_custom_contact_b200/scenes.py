@@ -20,6 +20,9 @@ the infinite-plane bounding radius 1e6 (geometry/utils.py:98-102), gap 0.1
       8..48 loose boxes (half-extent U[0.03,0.08]) on a table plane.
   C5  1024 worlds of 16-box stacks (half-extent 0.1, lateral jitter +-1 cm,
       mu U[0.4,0.8]), initial twists N(0, 0.1).
+  falling shapes  the scene of newton/tests/test_shapes_no_bounce.py with the
+      shapes this solver collides (spheres, boxes, capsules in turn), every
+      world the same grid.
 """
 
 from __future__ import annotations
@@ -330,3 +333,36 @@ def scene_c3(seed: int = 3, worlds: int = 4096, device=None):
     phases = np.asarray(phases)
     return model, dict(dt=1.0 / 120.0, substeps=4, iterations=8, phases=phases,
                        name=f"C3: {worlds} arm worlds")
+
+
+def scene_falling_shapes(worlds: int = 1, device=None):
+    """The falling-shapes scene of newton/tests/test_shapes_no_bounce.py:32-184 with the
+    shapes this solver collides: a 4 x 4 x 8 grid (spacing 1.5 m, offset (-5, -5, 1),
+    +-0.2 m jitter from default_rng(42)) of spheres (r 0.3), boxes (half 0.3) and capsules
+    (r 0.2, half height 0.4) in turn, each a free body (add_body's own free joint), above a
+    ground plane at z = -0.5 (the reference's 2-triangle ground mesh at that height).  Every
+    world holds the same grid.  Returns (model, initial z of every body as float32)."""
+    b = ModelBuilder()
+    b.add_ground_plane(height=-0.5)
+    z0 = []
+    for _ in range(worlds):
+        rng = np.random.default_rng(42)
+        b.begin_world()
+        k = 0
+        for ix in range(4):
+            for iy in range(4):
+                for iz in range(8):
+                    base = np.array([-5.0 + 1.5 * ix, -5.0 + 1.5 * iy, 1.0 + 1.5 * iz])
+                    pos = base + np.array([(rng.random() - 0.5) * 0.4 for _ in range(3)])
+                    z0.append(np.float32(pos[2]))
+                    body = b.add_body(xform=np.concatenate([pos, [0.0, 0.0, 0.0, 1.0]]))
+                    kind = k % 3
+                    k += 1
+                    if kind == 0:
+                        b.add_shape_sphere(body, radius=0.3)
+                    elif kind == 1:
+                        b.add_shape_box(body, hx=0.3, hy=0.3, hz=0.3)
+                    else:
+                        b.add_shape_capsule(body, radius=0.2, half_height=0.4)
+        b.end_world()
+    return b.finalize(device=device), np.asarray(z0, np.float32)

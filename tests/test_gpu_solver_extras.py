@@ -229,46 +229,13 @@ def test_body_parent_f_parity_c3(cuda, orc):
     assert np.abs(pf[rev]).sum() > 0 and np.all(np.delete(pf, rev, axis=0) == 0.0)
 
 
-def _no_bounce_model(worlds):
-    """The falling-shapes scene of newton/tests/test_shapes_no_bounce.py:32-184 with the
-    shapes this solver collides: a 4 x 4 x 8 grid (spacing 1.5 m, offset (-5, -5, 1),
-    +-0.2 m jitter from default_rng(42)) of spheres (r 0.3), boxes (half 0.3) and capsules
-    (r 0.2, half height 0.4) in turn, each a free body (add_body's own free joint), above a ground plane at
-    z = -0.5 (the reference's 2-triangle ground mesh at that height).  Every world holds
-    the same grid."""
-    b = ModelBuilder()
-    b.add_ground_plane(height=-0.5)
-    z0 = []
-    for _ in range(worlds):
-        rng = np.random.default_rng(42)
-        b.begin_world()
-        k = 0
-        for ix in range(4):
-            for iy in range(4):
-                for iz in range(8):
-                    base = np.array([-5.0 + 1.5 * ix, -5.0 + 1.5 * iy, 1.0 + 1.5 * iz])
-                    pos = base + np.array([(rng.random() - 0.5) * 0.4 for _ in range(3)])
-                    z0.append(np.float32(pos[2]))
-                    body = b.add_body(xform=np.concatenate([pos, [0.0, 0.0, 0.0, 1.0]]))
-                    kind = k % 3
-                    k += 1
-                    if kind == 0:
-                        b.add_shape_sphere(body, radius=0.3)
-                    elif kind == 1:
-                        b.add_shape_box(body, hx=0.3, hy=0.3, hz=0.3)
-                    else:
-                        b.add_shape_capsule(body, radius=0.2, half_height=0.4)
-        b.end_world()
-    return b.finalize(device="cuda"), np.asarray(z0, np.float32)
-
-
 def test_shapes_never_exceed_initial_z(cuda):
     """No shape dropped on the ground ever rises above max(2 m, its initial z) over 200
     frames at 100 fps with 10 substeps, 2 iterations, relaxation 0.8 and no angular
     damping (the reference's settings, test_shapes_no_bounce.py:186-226); the replicated
     worlds stay bit-identical to one another throughout."""
     worlds = 4
-    model, z0 = _no_bounce_model(worlds)
+    model, z0 = scenes.scene_falling_shapes(worlds, device="cuda")
     pipe = CollisionPipeline(model)
     solver = SolverXPBD(model, iterations=2, rigid_contact_relaxation=0.8, angular_damping=0.0)
     s0, s1 = model.state(), model.state()

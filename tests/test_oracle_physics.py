@@ -10,6 +10,9 @@ Scenes and assertions are those of the reference's own tests:
     equilibrium of a small sphere, a heavy sphere, a box and a three-cube
     pyramid; iterations=32, rigid_contact_con_weighting=True) and :658-726
     (zero force in free fall and for a pair inside the gap).
+  * no bounce: newton/tests/test_shapes_no_bounce.py:21-226 (a grid of shapes
+    dropped on the ground never rises above max(2 m, its start) in 200 frames),
+    with the sphere / box / capsule shapes of the grid.
 The CUDA path is compared with the oracle bit for bit in test_gpu_solver_extras.py.
 """
 
@@ -267,3 +270,26 @@ def test_oracle_parent_force_zero_for_free_body(orc):
     model = b.finalize(device="cpu")
     pf = _parent_f_average(orc, model, iterations=2, settle=0, avg=1)
     np.testing.assert_allclose(pf[0], 0.0, atol=1e-6)
+
+
+def test_oracle_shapes_never_exceed_initial_z(orc):
+    """newton/tests/test_shapes_no_bounce.py:186-226 on the oracle: spheres, boxes and
+    capsules dropped on a plane never rise above max(2 m, their initial z) over 200 frames
+    at 100 fps with 10 substeps, XPBD with 2 iterations, relaxation 0.8, no angular
+    damping; by the last frame every body has landed below its start."""
+    from newton_custom_contact_b200 import scenes
+
+    model, z0 = scenes.scene_falling_shapes(1, device="cpu")
+    solver = SolverXPBD(model, iterations=2, rigid_contact_relaxation=0.8, angular_damping=0.0)
+    limit = np.maximum(np.float32(2.0), z0)
+    frames = {"n": 0, "contacts": 0}
+
+    def check(i, q, qd, segs, lay, imp):
+        frames["contacts"] = max(frames["contacts"], int(np.sum(segs.world_count)))
+        if (i + 1) % 10 == 0:
+            frames["n"] += 1
+            assert np.all(q[:, 2] <= limit), f"frame {frames['n']}: max excess {float((q[:, 2] - limit).max()):.4f} m"
+
+    q, _ = _sim(orc, model, solver, 1.0 / 100.0 / 10, 2000, on_step=check)
+    assert frames["n"] == 200 and np.all(np.isfinite(q))
+    assert frames["contacts"] >= 16 and np.all(q[:, 2] < z0)
