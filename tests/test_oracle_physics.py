@@ -13,6 +13,8 @@ Scenes and assertions are those of the reference's own tests:
   * no bounce: newton/tests/test_shapes_no_bounce.py:21-226 (a grid of shapes
     dropped on the ground never rises above max(2 m, its start) in 200 frames),
     with the sphere / box / capsule shapes of the grid.
+  * shapes at rest on a plane and a two-box drop: newton/tests/test_rigid_contact.py:
+    28-227 and 766-831 with SolverXPBD(iterations=2) (:841).
 The CUDA path is compared with the oracle bit for bit in test_gpu_solver_extras.py.
 """
 
@@ -293,3 +295,84 @@ def test_oracle_shapes_never_exceed_initial_z(orc):
     q, _ = _sim(orc, model, solver, 1.0 / 100.0 / 10, 2000, on_step=check)
     assert frames["n"] == 200 and np.all(np.isfinite(q))
     assert frames["contacts"] >= 16 and np.all(q[:, 2] < z0)
+
+
+def _frames(orc, model, solver, frame_dt, substeps, frames, on_frame=None):
+    """`frames` frames of `substeps` substeps (collide + step each) on the oracle."""
+    lay = PairLayout(model, model.host("shape_contact_pairs"))
+    p = solver.params()
+    q = model.host("body_q").copy()
+    qd = model.host("body_qd").copy()
+    f = np.zeros((model.body_count, 6), np.float32)
+    dt = frame_dt / substeps
+    for k in range(frames):
+        for _ in range(substeps):
+            segs = orc.collide(model, lay, q)
+            q, qd = orc.step(model, lay, p, q, qd, f, segs, dt)[:2]
+        if on_frame is not None:
+            on_frame(k, q, qd)
+    return q, qd
+
+
+def test_oracle_shapes_on_plane(orc):
+    """newton/tests/test_rigid_contact.py:28-227 with SolverXPBD(iterations=2) (:841):
+    spheres (r 0.1 s), Y-lying capsules (r 0.1 s, half height 0.3 s) and boxes
+    (0.2 s, 0.25 s, 0.3 s) for s in (0.5, 1) dropped from 0.5 m come to rest on the
+    plane after 120 frames of 30 substeps at 60 fps: |v|, |w| < 0.2, positions within
+    0.25 of resting on the plane, orientations within 0.1 of identity.  The reference's
+    cylinder and mesh bodies are left out (shapes this solver does not collide)."""
+    from newton_custom_contact_b200.builder import quat_from_axis_angle
+
+    b = ModelBuilder()
+    expected = []
+    for i, s in enumerate((0.5, 1.0)):
+        y = i * 1.5
+        body = b.add_body(xform=[0.0, y, 0.5, 0.0, 0.0, 0.0, 1.0])
+        b.add_shape_sphere(body, radius=0.1 * s)
+        expected.append((0.0, y, 0.1 * s))
+        body = b.add_body(xform=[2.0, y, 0.5, 0.0, 0.0, 0.0, 1.0])
+        z_to_y = quat_from_axis_angle((1.0, 0.0, 0.0), -0.5 * np.pi)
+        b.add_shape_capsule(body, xform=np.concatenate([[0.0, 0.0, 0.0], z_to_y]), radius=0.1 * s,
+                            half_height=0.3 * s)
+        expected.append((2.0, y, 0.1 * s))
+        body = b.add_body(xform=[4.0, y, 0.5, 0.0, 0.0, 0.0, 1.0])
+        b.add_shape_box(body, hx=0.2 * s, hy=0.25 * s, hz=0.3 * s)
+        expected.append((4.0, y, 0.3 * s))
+    b.add_ground_plane()
+    model = b.finalize(device="cpu")
+    solver = SolverXPBD(model, iterations=2)
+    q, qd = _frames(orc, model, solver, 1.0 / 60.0, 30, 120)
+    assert np.all(np.isfinite(q)) and np.all(np.isfinite(qd))
+    assert np.abs(qd[:, :3]).max() < 0.2 and np.abs(qd[:, 3:]).max() < 0.2
+    assert np.abs(q[:, :3] - np.asarray(expected)).max() < 0.25
+    assert np.abs(q[:, 3:] - np.array([0.0, 0.0, 0.0, 1.0])).max() < 0.1
+
+
+def test_oracle_box_drop(orc):
+    """newton/tests/test_rigid_contact.py:766-831 with SolverXPBD(iterations=2): a box
+    (half 0.5) resting 0.1 above the plane and a second one tilted 0.5 rad about x
+    dropped from 2.1 m onto it; over 60 frames of 8 substeps the vertical speed never
+    exceeds free fall from the drop height, and both end near the origin, above the
+    ground and nearly at rest."""
+    from newton_custom_contact_b200.builder import quat_from_axis_angle
+
+    h = 0.5
+    b = ModelBuilder()
+    b.add_ground_plane()
+    body = b.add_body(xform=[0.0, 0.0, h * 1.2, 0.0, 0.0, 0.0, 1.0])
+    b.add_shape_box(body, hx=h, hy=h, hz=h)
+    body = b.add_body(xform=np.concatenate([[0.0, 0.0, h * 4.2], quat_from_axis_angle((1.0, 0.0, 0.0), 0.5)]))
+    b.add_shape_box(body, hx=h, hy=h, hz=h)
+    model = b.finalize(device="cpu")
+    solver = SolverXPBD(model, iterations=2)
+    v_max = np.sqrt(2.0 * 9.81 * h * 3.2)
+    seen = {"v": 0.0}
+
+    def track(k, q, qd):
+        seen["v"] = max(seen["v"], float(np.abs(qd[:, 2]).max()))
+
+    q, qd = _frames(orc, model, solver, 1.0 / 60.0, 8, 60, on_frame=track)
+    assert seen["v"] < v_max
+    assert np.all(np.abs(q[:, 0]) < 1.0) and np.all(np.abs(q[:, 1]) < 1.0)
+    assert np.all(q[:, 2] > 0.5 * h)
+    assert np.all(np.linalg.norm(qd[:, :3], axis=1) < 1.0)
