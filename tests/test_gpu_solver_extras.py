@@ -258,3 +258,59 @@ def test_shapes_never_exceed_initial_z(cuda):
     assert np.all(np.isfinite(q))
     # the grid has landed: every body below its start, contacts live in every world
     assert in_contact >= worlds * 16 and np.all(z < z0)
+
+
+def _shapes_on_plane_model():
+    """newton/tests/test_rigid_contact.py:28-227 without its cylinder and mesh bodies."""
+    from newton_custom_contact_b200.builder import quat_from_axis_angle
+
+    b = ModelBuilder()
+    expected = []
+    for i, s in enumerate((0.5, 1.0)):
+        y = i * 1.5
+        body = b.add_body(xform=[0.0, y, 0.5, 0.0, 0.0, 0.0, 1.0])
+        b.add_shape_sphere(body, radius=0.1 * s)
+        expected.append((0.0, y, 0.1 * s))
+        body = b.add_body(xform=[2.0, y, 0.5, 0.0, 0.0, 0.0, 1.0])
+        z_to_y = quat_from_axis_angle((1.0, 0.0, 0.0), -0.5 * np.pi)
+        b.add_shape_capsule(body, xform=np.concatenate([[0.0, 0.0, 0.0], z_to_y]), radius=0.1 * s,
+                            half_height=0.3 * s)
+        expected.append((2.0, y, 0.1 * s))
+        body = b.add_body(xform=[4.0, y, 0.5, 0.0, 0.0, 0.0, 1.0])
+        b.add_shape_box(body, hx=0.2 * s, hy=0.25 * s, hz=0.3 * s)
+        expected.append((4.0, y, 0.3 * s))
+    b.add_ground_plane()
+    return b.finalize(device="cuda"), np.asarray(expected)
+
+
+def test_shapes_on_plane_parity(cuda, orc):
+    """The reference's shapes-on-plane rest test (test_rigid_contact.py:28-227, XPBD with
+    2 iterations) through the CUDA path: 120 frames of 30 substeps agree with the oracle
+    bit for bit, and the bodies rest on the plane (|v|, |w| < 0.2, positions within 0.25,
+    orientations within 0.1 of identity)."""
+    model, expected = _shapes_on_plane_model()
+    gq, gqd, q, qd, _ = _run(model, 120 * 30, 1.0 / 60.0 / 30, 2, orc)
+    assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
+    assert np.abs(gqd[:, :3]).max() < 0.2 and np.abs(gqd[:, 3:]).max() < 0.2
+    assert np.abs(gq[:, :3] - expected).max() < 0.25
+    assert np.abs(gq[:, 3:] - np.array([0.0, 0.0, 0.0, 1.0])).max() < 0.1
+
+
+def test_box_drop_parity(cuda, orc):
+    """The reference's two-box drop (test_rigid_contact.py:766-831, XPBD with 2 iterations)
+    through the CUDA path: 60 frames of 8 substeps agree with the oracle bit for bit; both
+    boxes end near the origin, above the ground and nearly at rest."""
+    from newton_custom_contact_b200.builder import quat_from_axis_angle
+
+    h = 0.5
+    b = ModelBuilder()
+    b.add_ground_plane()
+    body = b.add_body(xform=[0.0, 0.0, h * 1.2, 0.0, 0.0, 0.0, 1.0])
+    b.add_shape_box(body, hx=h, hy=h, hz=h)
+    body = b.add_body(xform=np.concatenate([[0.0, 0.0, h * 4.2], quat_from_axis_angle((1.0, 0.0, 0.0), 0.5)]))
+    b.add_shape_box(body, hx=h, hy=h, hz=h)
+    model = b.finalize(device="cuda")
+    gq, gqd, q, qd, _ = _run(model, 60 * 8, 1.0 / 60.0 / 8, 2, orc)
+    assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
+    assert np.all(np.abs(gq[:, :2]) < 1.0) and np.all(gq[:, 2] > 0.5 * h)
+    assert np.all(np.linalg.norm(gqd[:, :3], axis=1) < 1.0)
