@@ -873,7 +873,7 @@ __device__ __forceinline__ float world_penetration(const SB& S, const float4* __
 // restored from a snapshot kept in the step's output rows) when the warm
 // start makes its largest penetration worse.
 template <int G, class SB>
-__device__ __noinline__ void warm_start(const NbModelDesc& m, const NbStepIO& io, const NbContactSeg& seg, SB& S,
+__device__ __forceinline__ void warm_start(const NbModelDesc& m, const NbStepIO& io, const NbContactSeg& seg, SB& S,
                                         const float4* __restrict__ R, int nc, int64_t rec_base, int b0, int g,
                                         int t, int* scratch, float dt, unsigned* bad) {
     const int nb = S.nb;
@@ -968,10 +968,11 @@ __device__ __noinline__ void warm_start(const NbModelDesc& m, const NbStepIO& io
 // integrate, `iterations` x (contacts, weighted apply, joints, apply),
 // restitution, write-back.  The caller carved the world's slab into S.
 // kLean: the variant for models whose joints are all FREE, called without
-// restitution, warm start or per-contact impulses.  It drops those passes and
-// the joint solve at compile time (each of them would be a no-op for such a
-// call), which keeps the world's shared-memory view in registers instead of
-// on the stack; the arithmetic of what remains is the same code.
+// restitution or per-contact impulses.  It drops those passes and the joint
+// solve at compile time (each of them would be a no-op for such a call),
+// which keeps the world's shared-memory view in registers instead of on the
+// stack; the arithmetic of what remains is the same code.  The warm-start
+// pass is inlined, so it runs in either variant.
 template <int G, bool kLean, class SB>
 __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdParams& p, const NbStepIO& io,
                                            const NbContactSeg& seg, bool has_contacts, float dt, int w, SB& S,
@@ -1049,10 +1050,8 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
     const float4* R = rec + (size_t)rec_base * 5;
     const bool want_imp = !kLean && has_contacts && io.contact_impulse != nullptr;
     unsigned bad = 0u;
-    if constexpr (!kLean) {
-        if (has_contacts && io.ws_lambda)
-            warm_start<G>(m, io, seg, S, R, nc, rec_base, b0, g, t, nact, dt, &bad);
-    }
+    if (has_contacts && io.ws_lambda)
+        warm_start<G>(m, io, seg, S, R, nc, rec_base, b0, g, t, nact, dt, &bad);
     for (int it = 0; it < p.iterations; ++it) {
         if (has_contacts) {
             contact_pass<G>(m, S, R, nc, list, nact, g, t, p.rigid_contact_relaxation, dt,
@@ -1521,10 +1520,9 @@ cudaError_t nb_launch_contact_forces(const float* imp, const int32_t* count, int
 
 namespace {
 // the lean step kernel applies: every joint is FREE and the call asks for
-// none of restitution, warm start and per-contact impulses
+// neither restitution nor per-contact impulses
 bool step_is_lean(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io) {
-    return m->all_joints_free == 1 && p->enable_restitution == 0 && io->ws_lambda == nullptr &&
-           io->contact_impulse == nullptr;
+    return m->all_joints_free == 1 && p->enable_restitution == 0 && io->contact_impulse == nullptr;
 }
 
 template <int G, bool kLean>
