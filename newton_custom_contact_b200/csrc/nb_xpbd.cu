@@ -971,9 +971,10 @@ __device__ __forceinline__ void warm_start(const NbModelDesc& m, const NbStepIO&
 // restitution or per-contact impulses.  It drops those passes and the joint
 // solve at compile time (each of them would be a no-op for such a call),
 // which keeps the world's shared-memory view in registers instead of on the
-// stack; the arithmetic of what remains is the same code.  The warm-start
-// pass is inlined, so it runs in either variant.
-template <int G, bool kLean, class SB>
+// stack; the arithmetic of what remains is the same code.  kWarm: the
+// warm-start pass (inlined) is compiled in; the lean variant is built with
+// and without it, so that plain calls do not carry its code.
+template <int G, bool kLean, bool kWarm, class SB>
 __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdParams& p, const NbStepIO& io,
                                            const NbContactSeg& seg, bool has_contacts, float dt, int w, SB& S,
                                            int g, int t, int* flag, int* nact, unsigned char* list,
@@ -1050,8 +1051,10 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
     const float4* R = rec + (size_t)rec_base * 5;
     const bool want_imp = !kLean && has_contacts && io.contact_impulse != nullptr;
     unsigned bad = 0u;
-    if (has_contacts && io.ws_lambda)
-        warm_start<G>(m, io, seg, S, R, nc, rec_base, b0, g, t, nact, dt, &bad);
+    if constexpr (kWarm) {
+        if (has_contacts && io.ws_lambda)
+            warm_start<G>(m, io, seg, S, R, nc, rec_base, b0, g, t, nact, dt, &bad);
+    }
     for (int it = 0; it < p.iterations; ++it) {
         if (has_contacts) {
             contact_pass<G>(m, S, R, nc, list, nact, g, t, p.rigid_contact_relaxation, dt,
@@ -1173,7 +1176,7 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
 // Batch mode: a CTA takes a batch of worlds (host-packed into one arena, one
 // world per group of G threads) from a device counter; the CTA waits for all
 // of a batch's worlds before the next batch reuses the arena.
-template <int G, bool kLean>
+template <int G, bool kLean, bool kWarm>
 __global__ void __launch_bounds__(kST, 2)
 xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, int has_contacts, float dt) {
     extern __shared__ __align__(16) unsigned char arena[];
@@ -1196,8 +1199,8 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
             const int b0 = m.world_body_start[w];
             const int nb = m.world_body_start[w + 1] - b0;
             SBodiesT<false> S = sbodies_carve<false>(arena + 4 * (size_t)m.batch_slab[b * kGroups + g], m, b0, nb);
-            step_world<G, kLean>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g], s_list[g],
-                          &s_bad);
+            step_world<G, kLean, kWarm>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g],
+                                        s_list[g], &s_bad);
         }
         __syncthreads();  // every group is done with the arena before the next batch
     }
@@ -1215,7 +1218,7 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
 // never waits for another group's world.  The host picks G and the slab
 // layout so that the largest world fits one share (kCompact stages only the
 // mutable body state).
-template <int G, bool kCompact, bool kLean>
+template <int G, bool kCompact, bool kLean, bool kWarm>
 __global__ void __launch_bounds__(kST, 2)
 xpbd_step_group_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, int has_contacts, float dt) {
     extern __shared__ __align__(16) unsigned char arena[];
@@ -1252,8 +1255,8 @@ xpbd_step_group_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg 
             continue;
         }
         SBodiesT<kCompact> S = sbodies_carve<kCompact>(region, m, b0, nb);
-        step_world<G, kLean>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g], s_list[g],
-                      &s_bad);
+        step_world<G, kLean, kWarm>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g],
+                                    s_list[g], &s_bad);
         group_sync<G>(g);
     }
     __syncthreads();
@@ -1525,50 +1528,54 @@ bool step_is_lean(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* i
     return m->all_joints_free == 1 && p->enable_restitution == 0 && io->contact_impulse == nullptr;
 }
 
-template <int G, bool kLean>
+template <int G, bool kLean, bool kWarm>
 cudaError_t launch_step_variant(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
                                 const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
     const size_t smem = nb_step_smem_bytes(m);
     static size_t configured = 0;
     if (smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(xpbd_step_kernel<G, kLean>,
+        cudaError_t e = cudaFuncSetAttribute(xpbd_step_kernel<G, kLean, kWarm>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         configured = smem;
     }
     const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
-    xpbd_step_kernel<G, kLean><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
+    xpbd_step_kernel<G, kLean, kWarm><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
     return cudaGetLastError();
 }
 
 template <int G>
 cudaError_t launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
                         float dt, int grid, cudaStream_t stream) {
-    return step_is_lean(m, p, io) ? launch_step_variant<G, true>(m, p, io, seg, dt, grid, stream)
-                                  : launch_step_variant<G, false>(m, p, io, seg, dt, grid, stream);
+    if (!step_is_lean(m, p, io)) return launch_step_variant<G, false, true>(m, p, io, seg, dt, grid, stream);
+    return io->ws_lambda ? launch_step_variant<G, true, true>(m, p, io, seg, dt, grid, stream)
+                         : launch_step_variant<G, true, false>(m, p, io, seg, dt, grid, stream);
 }
 
-template <int G, bool kCompact, bool kLean>
+template <int G, bool kCompact, bool kLean, bool kWarm>
 cudaError_t launch_step_group_variant(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
                                       const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
     const size_t smem = nb_step_smem_bytes(m);
     static size_t configured = 0;
     if (smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(xpbd_step_group_kernel<G, kCompact, kLean>,
+        cudaError_t e = cudaFuncSetAttribute(xpbd_step_group_kernel<G, kCompact, kLean, kWarm>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         configured = smem;
     }
     const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
-    xpbd_step_group_kernel<G, kCompact, kLean><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
+    xpbd_step_group_kernel<G, kCompact, kLean, kWarm><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts,
+                                                                                 dt);
     return cudaGetLastError();
 }
 
 template <int G, bool kCompact>
 cudaError_t launch_step_group(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
                               const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
-    return step_is_lean(m, p, io) ? launch_step_group_variant<G, kCompact, true>(m, p, io, seg, dt, grid, stream)
-                                  : launch_step_group_variant<G, kCompact, false>(m, p, io, seg, dt, grid, stream);
+    if (!step_is_lean(m, p, io))
+        return launch_step_group_variant<G, kCompact, false, true>(m, p, io, seg, dt, grid, stream);
+    return io->ws_lambda ? launch_step_group_variant<G, kCompact, true, true>(m, p, io, seg, dt, grid, stream)
+                         : launch_step_group_variant<G, kCompact, true, false>(m, p, io, seg, dt, grid, stream);
 }
 
 template <bool kCompact>
