@@ -80,3 +80,20 @@ def test_fixed_joint_to_world_filters_ground():
     b.add_shape_sphere(other, radius=0.1)
     pairs = {tuple(p) for p in b.find_shape_contact_pairs().tolist()}
     assert (0, 1) not in pairs and (0, 2) in pairs and (1, 2) in pairs
+
+
+def test_desc_all_joints_free():
+    """NbModelDesc.all_joints_free (which lets the step use its lean kernel) is 1 only when
+    every joint is FREE: the free-body scenes, not the revolute arms."""
+    bw, types, scales, poses, mu, W = _random_bodies(3)
+    free = scenes.assemble_free_bodies(bw, types, scales, poses, mu, W, plane_mu=0.5, device="cpu")
+    assert free.make_desc(free.host_arrays()).all_joints_free == 1
+    arms, _ = scenes.scene_c3(worlds=2, device="cpu")
+    assert arms.make_desc(arms.host_arrays()).all_joints_free == 0
+    b = ModelBuilder()
+    b.add_ground_plane()
+    body = b.add_link(xform=((0.0, 0.0, 1.0), (0.0, 0.0, 0.0, 1.0)))
+    b.add_shape_sphere(body, radius=0.1)
+    b.add_joint_fixed(-1, body)
+    fixed = b.finalize(device="cpu")
+    assert fixed.make_desc(fixed.host_arrays()).all_joints_free == 0
