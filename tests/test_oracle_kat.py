@@ -2,7 +2,9 @@
 
 Expected values are the assertions of the reference's own tests:
 newton/tests/test_collision_primitives.py (plane-sphere :429, sphere-sphere :505,
-sphere-box :1136, plane-box :1335, box-box :1529, box-box depths :1881) and
+sphere-capsule :587, capsule-capsule :696, sphere-box :1136, plane-capsule :1251,
+plane-box :1335, box-box :1529, box-box with margin :1613, capsule-box :1749,
+box-box depths :1881) and
 newton/tests/test_narrow_phase.py (box-box face :635, edge :708, capsules
 :801-895, plane-capsule :1083).  Contacts here run the full pipeline path
 (primitive routing, MPR/GJK, manifold, write_contact gap test) with gap 0 on
@@ -142,3 +144,80 @@ def test_sort_sub_keys(orc):
     rows = run(orc, B, [0, 0, 0], [0.5, 0.5, 0.5], B, [0, 0, 0.95], [0.5, 0.5, 0.5], gap=0.1)
     subs = rows[:, 12].astype(int)
     assert np.all(np.diff(subs) > 0) and subs.max() <= 4
+
+
+# ---- more of newton/tests/test_collision_primitives.py: sphere-capsule :587,
+# capsule-capsule :696, plane-capsule :1251, box-box with margin :1613,
+# capsule-box :1749 (the reference's distances are checked within its own
+# tolerances; separated cases need a summed gap larger than the distance)
+
+QY90 = [0.0, math.sin(math.pi / 4), 0.0, math.cos(math.pi / 4)]   # local z -> world x
+QX90 = [math.sin(math.pi / 4), 0.0, 0.0, math.cos(math.pi / 4)]   # local z -> world -y
+
+
+def _dist_to_capsule(p, c, axis, r, hh):
+    p, c, axis = np.asarray(p, float), np.asarray(c, float), np.asarray(axis, float)
+    t = np.clip(np.dot(p - c, axis), -hh, hh)
+    return abs(np.linalg.norm(p - (c + t * axis)) - r)
+
+
+@pytest.mark.parametrize("p,dist", [([0, 1.5, 0], 0.5), ([0, 1.0, 0], 0.0), ([0, 0.9, 0], -0.1), ([0, 0.8, 0], -0.2),
+                                    ([0, 0, 2.5], 0.5), ([0, 0, 2.0], 0.0), ([0, 0, 1.9], -0.1), ([0, 0, 1.8], -0.2)])
+def test_sphere_capsule(orc, p, dist):
+    gap = 0.3 if dist > 0 else 0.0
+    rows = run(orc, S, p, [0.5, 0, 0], C, [0, 0, 0], [0.5, 1.0, 0], gap=gap)
+    assert rows.shape[0] == 1
+    r = rows[0]
+    assert r[11] == pytest.approx(dist, abs=0.01)
+    n = r[6:9]
+    assert np.dot(n, -np.asarray(p, float)) > 0.99 * np.linalg.norm(p)  # from the sphere into the capsule
+    if dist < 0:
+        on_sphere = r[0:3] + n * r[9]
+        on_capsule = r[3:6] - n * r[10]
+        assert abs(np.linalg.norm(on_sphere - np.asarray(p, float)) - 0.5) < 0.05
+        assert _dist_to_capsule(on_capsule, [0, 0, 0], [0, 0, 1], 0.5, 1.0) < 0.05
+    assert run(orc, S, p, [0.5, 0, 0], C, [0, 0, 0], [0.5, 1.0, 0]).shape[0] == (0 if dist > 0 else 1)
+
+
+@pytest.mark.parametrize("y,dist", [(2.0, 1.0), (1.5, 0.5), (1.0, 0.0), (0.9, -0.1), (0.8, -0.2), (0.6, -0.4)])
+def test_capsule_capsule_parallel(orc, y, dist):
+    gap = 0.6 if dist > 0 else 0.0
+    rows = run(orc, C, [0, 0, 0], [0.5, 1.0, 0], C, [0, y, 0], [0.5, 1.0, 0], gap=gap, qa=QY90, qb=QY90)
+    assert rows.shape[0] >= 1
+    assert np.allclose(rows[:, 11], dist, atol=0.01)
+    assert np.all(rows[:, 7] > 0.99)  # normal along +y, from the first capsule into the second
+
+
+def test_capsule_capsule_perpendicular_through_centre(orc):
+    rows = run(orc, C, [0, 0, 0], [0.5, 1.0, 0], C, [0, 0, 0], [0.5, 1.0, 0], qa=QY90, qb=QX90)
+    assert rows.shape[0] >= 1
+    assert rows[0, 11] == pytest.approx(-1.0, abs=0.01)
+
+
+@pytest.mark.parametrize("z,dist", [(2.0, 1.5), (1.5, 1.0), (1.0, 0.5), (0.5, 0.0), (0.4, -0.1), (0.3, -0.2),
+                                    (0.2, -0.3)])
+def test_plane_capsule_horizontal(orc, z, dist):
+    gap = 0.8 if dist > 0 else 0.0
+    rows = run(orc, P, [0, 0, 0], [0, 0, 0], C, [0, 0, z], [0.5, 1.0, 0], gap=gap, qb=QY90)
+    assert rows.shape[0] == 2  # one contact per end of the horizontal capsule
+    assert np.allclose(rows[:, 11], dist, atol=0.01)
+    assert np.all(rows[:, 8] > 0.99)
+
+
+@pytest.mark.parametrize("gap_sum,contacts", [(0.0, False), (0.3, True), (0.1, False)])
+def test_box_box_margin(orc, gap_sum, contacts):
+    # stacked boxes 0.2 apart: a contact only when the contact threshold exceeds the gap
+    rows = run(orc, B, [0, 0, 0], [0.5, 0.5, 0.5], B, [0, 0, 1.2], [0.5, 0.5, 0.5], gap=0.5 * gap_sum)
+    assert (rows.shape[0] > 0) == contacts
+    if contacts:
+        assert np.allclose(rows[:, 11], 0.2, atol=0.01)
+        assert np.all(rows[:, 8] > 0.99)
+
+
+@pytest.mark.parametrize("z,dist", [(3.0, 0.5), (2.5, 0.0), (2.4, -0.1), (2.3, -0.2), (2.2, -0.3)])
+def test_capsule_box_upright(orc, z, dist):
+    gap = 0.3 if dist > 0 else 0.0
+    rows = run(orc, C, [0, 0, z], [0.5, 1.0, 0], B, [0, 0, 0], [1, 1, 1], gap=gap)
+    assert rows.shape[0] >= 1
+    assert rows[:, 11].min() == pytest.approx(dist, abs=0.05)
+    assert np.all(rows[:, 8] < -0.99)  # from the capsule down into the box
