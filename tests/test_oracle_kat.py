@@ -5,8 +5,8 @@ newton/tests/test_collision_primitives.py (plane-sphere :429, sphere-sphere :505
 sphere-capsule :587, capsule-capsule :696, sphere-box :1136, plane-capsule :1251,
 plane-box :1335, box-box :1529, box-box with margin :1613, capsule-box :1749,
 box-box depths :1881) and
-newton/tests/test_narrow_phase.py (box-box face :635, edge :708, capsules
-:801-895, plane-capsule :1083).  Contacts here run the full pipeline path
+newton/tests/test_narrow_phase.py (sphere-box corner :591, box-box face :635,
+edge :708, capsules :801-895, plane-capsule :1083, per-shape gap :1271).  Contacts here run the full pipeline path
 (primitive routing, MPR/GJK, manifold, write_contact gap test) with gap 0 on
 both shapes, i.e. the reference primitive with margin 0.
 """
@@ -221,3 +221,37 @@ def test_capsule_box_upright(orc, z, dist):
     assert rows.shape[0] >= 1
     assert rows[:, 11].min() == pytest.approx(dist, abs=0.05)
     assert np.all(rows[:, 8] < -0.99)  # from the capsule down into the box
+
+
+# ---- newton/tests/test_narrow_phase.py: sphere-box corner :591, per-shape gap :1271
+
+def _dist_to_box(p, half):
+    q = np.abs(np.asarray(p, float)) - np.asarray(half, float)
+    outside = np.linalg.norm(np.maximum(q, 0.0))
+    return outside if outside > 0.0 else -q.max()  # inside: distance to the nearest face
+
+
+def test_sphere_box_corner(orc):
+    c = np.ones(3) / np.sqrt(3.0) * 1.5
+    rows = run(orc, S, c, [0.5, 0, 0], B, [0, 0, 0], [1, 1, 1])
+    assert rows.shape[0] == 1
+    r = rows[0]
+    n = r[6:9]
+    assert np.linalg.norm(n) == pytest.approx(1.0, abs=0.01)
+    # the centre (0.866, 0.866, 0.866) lies inside the box: pushed out through the nearest
+    # face, depth -(1 - 0.866 + r)
+    assert r[11] == pytest.approx(-(1.0 - c[0] + 0.5), abs=0.01)
+    on_sphere = r[0:3] + n * r[9]
+    on_box = r[3:6] - n * r[10]
+    assert abs(np.linalg.norm(on_sphere - c) - 0.5) < 0.05
+    assert abs(_dist_to_box(on_box, [1, 1, 1])) < 0.05
+
+
+@pytest.mark.parametrize("z,gap_sphere,contact", [(0.25, 0.02, False), (0.15, 0.02, True), (0.23, 0.06, True)])
+def test_per_shape_gap(orc, z, gap_sphere, contact):
+    # plane gap 0.01; a sphere of radius 0.2 has a contact only within the summed gap
+    rows = orc.collide_pair(P, xf([0, 0, 0]), [0, 0, 0], S, xf([0, 0, z]), [0.2, 0, 0], gap_a=0.01,
+                            gap_b=gap_sphere)
+    assert (rows.shape[0] == 1) == contact
+    if contact:
+        assert rows[0, 11] == pytest.approx(z - 0.2, abs=1e-5)
