@@ -1,0 +1,94 @@
+"""Host-side logic of CollisionPipeline, checked on CPU against the reference's own tests.
+
+* Contact capacity estimate: newton/tests/test_collision_pipeline.py:796-865
+  (TestContactEstimator, the cases with primitive shapes only; the estimate
+  follows newton/_src/sim/collide.py:278-376).
+* Candidate-pair count per world: :866-979 (TestShapePairsMaxScaling: the
+  pair set grows linearly with the world count, global shapes join every
+  world's segment).
+* Constructor errors: newton/_src/sim/collide.py:587-603.
+"""
+
+import numpy as np
+import pytest
+
+from newton_custom_contact_b200 import CollisionPipeline, GeoType, ModelBuilder
+from newton_custom_contact_b200.collide import _estimate_rigid_contact_max
+
+
+class _Shapes:
+    """The fields the estimate reads: shape types and worlds, world count, pair count."""
+
+    def __init__(self, shape_type, shape_world, world_count, pair_count):
+        self._h = {"shape_type": np.asarray(shape_type, np.int32), "shape_world": np.asarray(shape_world, np.int32)}
+        self.world_count = world_count
+        self.shape_contact_pair_count = pair_count
+
+    def host_arrays(self):
+        return self._h
+
+
+def test_estimate_world_aware_planes():
+    # 4 worlds of 10 boxes and 10 planes: 40*20*5 // 2 = 2000 box contacts and
+    # 4 * (10 * 10) plane pairs * 5 = 2000 plane contacts, not a cross-world square
+    st = ([int(GeoType.BOX)] * 10 + [int(GeoType.PLANE)] * 10) * 4
+    sw = np.repeat(np.arange(4), 20)
+    assert _estimate_rigid_contact_max(_Shapes(st, sw, 4, 0)) == 4000
+
+
+def test_estimate_pair_count_tighter_than_heuristic():
+    # 40 boxes in 4 worlds: heuristic 2000, 300 known pairs * 5 = 1500
+    st = [int(GeoType.BOX)] * 40
+    sw = np.repeat(np.arange(4), 10)
+    assert _estimate_rigid_contact_max(_Shapes(st, sw, 4, 300)) == 1500
+
+
+def test_estimate_floor_and_no_shapes():
+    assert _estimate_rigid_contact_max(_Shapes([], [], 1, 0)) == 1000
+    assert _estimate_rigid_contact_max(_Shapes([int(GeoType.SPHERE)] * 3, [0, 0, 0], 1, 0)) == 1000
+
+
+def _worlds_of_boxes(worlds, per_world, ground=False):
+    rb = ModelBuilder()
+    for _ in range(per_world):
+        b = rb.add_body()
+        rb.add_shape_box(body=b, hx=0.1, hy=0.1, hz=0.1)
+    mb = ModelBuilder()
+    if ground:
+        mb.add_ground_plane()
+    for _ in range(worlds):
+        mb.add_world(rb)
+    return mb.finalize(device="cpu")
+
+
+@pytest.mark.parametrize("broad_phase", ["explicit", "nxn", "sap"])
+def test_shape_pairs_scale_linearly_with_worlds(broad_phase):
+    for worlds in (1, 2, 4, 64):
+        model = _worlds_of_boxes(worlds, 5)
+        pipe = CollisionPipeline(model, broad_phase=broad_phase)
+        assert pipe.shape_pairs_max == worlds * (5 * 4 // 2)
+    n = model.shape_count
+    assert pipe.shape_pairs_max < n * (n - 1) // 2 / 10
+
+
+@pytest.mark.parametrize("broad_phase", ["explicit", "nxn", "sap"])
+def test_global_shape_joins_every_world(broad_phase):
+    # each world: 3 boxes + the global ground plane -> 3 box pairs + 3 plane pairs
+    model = _worlds_of_boxes(2, 3, ground=True)
+    assert CollisionPipeline(model, broad_phase=broad_phase).shape_pairs_max == 2 * 6
+
+
+def test_constructor_errors():
+    model = _worlds_of_boxes(1, 2)
+    with pytest.raises(ValueError):
+        CollisionPipeline(model, broad_phase="octree")
+    with pytest.raises(ValueError):
+        CollisionPipeline(model, shape_pairs_max=0)
+    with pytest.raises(ValueError):
+        CollisionPipeline(model, max_triangle_pairs=0)
+    with pytest.raises(ValueError):
+        CollisionPipeline(model, contact_matching="always")
+    with pytest.raises(ValueError):
+        CollisionPipeline(model, contact_report=True)
+    with pytest.raises(NotImplementedError):
+        CollisionPipeline(model, sdf_hydroelastic_config=object())
