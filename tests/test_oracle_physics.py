@@ -15,6 +15,9 @@ Scenes and assertions are those of the reference's own tests:
     with the sphere / box / capsule shapes of the grid.
   * shapes at rest on a plane and a two-box drop: newton/tests/test_rigid_contact.py:
     28-227 and 766-831 with SolverXPBD(iterations=2) (:841).
+  * static and dynamic friction, free fall, projectile motion and momentum
+    conservation: newton/tests/test_physics_validation.py:505-641, :21-80,
+    :256-318, :413-498 with the XPBD settings those tests register.
 The CUDA path is compared with the oracle bit for bit in test_gpu_solver_extras.py.
 """
 
@@ -376,3 +379,159 @@ def test_oracle_box_drop(orc):
     assert np.all(np.abs(q[:, 0]) < 1.0) and np.all(np.abs(q[:, 1]) < 1.0)
     assert np.all(q[:, 2] > 0.5 * h)
     assert np.all(np.linalg.norm(qd[:, :3], axis=1) < 1.0)
+
+
+# ---- friction: newton/tests/test_physics_validation.py:505-563 (static) and :571-641
+# (dynamic), SolverXPBD(iterations=10, angular_damping=0) (:1619-1622).  The reference's
+# builder is Y-up; this one is Z-up, so the box rests along Z and slides along X.
+
+def _friction_loop(orc, model, solver, dt, steps, force_fn=None, qd0=None):
+    lay = PairLayout(model, model.host("shape_contact_pairs"))
+    p = solver.params()
+    q = model.host("body_q").copy()
+    qd = model.host("body_qd").copy() if qd0 is None else np.asarray(qd0, np.float32).copy()
+    zero = np.zeros((model.body_count, 6), np.float32)
+    for i in range(steps):
+        f = zero if force_fn is None else force_fn(i)
+        segs = orc.collide(model, lay, q)
+        q, qd = orc.step(model, lay, p, q, qd, f, segs, dt)[:2]
+    return q, qd
+
+
+def _box_on_ground(mu, boxes_x):
+    cfg = ModelBuilder.ShapeConfig(mu=mu, gap=0.1)
+    b = ModelBuilder(up_axis="Z", gravity=-10.0)
+    b.add_ground_plane(cfg=cfg)
+    h = 0.25
+    for y in boxes_x:
+        body = b.add_body(xform=[0.0, y, h + 0.001, 0.0, 0.0, 0.0, 1.0])
+        b.add_shape_box(body, hx=h, hy=h, hz=h, cfg=cfg)
+    return b.finalize(device="cpu"), h
+
+
+def test_oracle_static_friction(orc):
+    """A push of 0.3 mu m g leaves the box in place; 2 mu m g slides it (after 20 settling steps)."""
+    mu = 0.5
+    model, h = _box_on_ground(mu, [0.0, 5.0])
+    mass = 1000.0 * (2 * h) ** 3
+    push = np.zeros((2, 6), np.float32)
+    push[0, 0] = 0.3 * mu * mass * 10.0
+    push[1, 0] = 2.0 * mu * mass * 10.0
+    zero = np.zeros_like(push)
+    solver = SolverXPBD(model, iterations=10, angular_damping=0.0)
+    q, _ = _friction_loop(orc, model, solver, 1e-3, 200, force_fn=lambda i: push if i > 20 else zero)
+    assert abs(q[0, 0]) < 0.01 and q[0, 2] == pytest.approx(h, abs=0.01)
+    assert q[1, 0] > 0.05 and q[1, 2] == pytest.approx(h, abs=0.01)
+
+
+def test_oracle_dynamic_friction(orc):
+    """A box sliding at 2 m/s stops after v0^2 / (2 mu g) = 0.5 m (within 1 %)."""
+    mu, v0, g = 0.4, 2.0, 10.0
+    model, h = _box_on_ground(mu, [0.0])
+    qd0 = model.host("body_qd").copy()
+    qd0[0, 0] = v0
+    solver = SolverXPBD(model, iterations=10, angular_damping=0.0)
+    t_stop = v0 / (mu * g)
+    q, qd = _friction_loop(orc, model, solver, 1e-3, int(1.5 * t_stop / 1e-3), qd0=qd0)
+    d_stop = v0 ** 2 / (2.0 * mu * g)
+    assert q[0, 0] == pytest.approx(d_stop, abs=0.01 * d_stop)
+    assert abs(qd[0, 0]) < 0.01 and q[0, 2] == pytest.approx(h, abs=0.01)
+
+
+# ---- integration without contacts: newton/tests/test_physics_validation.py free fall
+# :21-80, projectile :256-318, momentum conservation :413-498, with
+# SolverXPBD(angular_damping=0) (:1509-1512).  Z-up here (the reference is Y-up).
+
+def _free_loop(orc, model, dt, steps, qd0=None, on_step=None):
+    solver = SolverXPBD(model, angular_damping=0.0)
+    lay = PairLayout(model, model.host("shape_contact_pairs"))
+    p = solver.params()
+    q = model.host("body_q").copy()
+    qd = model.host("body_qd").copy() if qd0 is None else np.asarray(qd0, np.float32).copy()
+    f = np.zeros((model.body_count, 6), np.float32)
+    for i in range(1, steps + 1):
+        q, qd = orc.step(model, lay, p, q, qd, f, None, dt)[:2]
+        if on_step is not None:
+            on_step(i, q, qd)
+    return q, qd
+
+
+def _tolerances(g, dt, t):
+    return max(2.0 * 0.5 * abs(g) * dt * t, 1e-3), max(abs(g) * dt, 1e-3)
+
+
+def test_oracle_free_fall(orc):
+    g, h0, dt = -10.0, 5.0, 1e-3
+    b = ModelBuilder(up_axis="Z", gravity=g)
+    b.add_shape_sphere(b.add_body(xform=[0.0, 0.0, h0, 0.0, 0.0, 0.0, 1.0]), radius=0.1)
+    model = b.finalize(device="cpu")
+
+    def check(i, q, qd):
+        if i % 100 == 0:
+            t = i * dt
+            pos_tol, vel_tol = _tolerances(g, dt, t)
+            assert q[0, 2] == pytest.approx(h0 + 0.5 * g * t * t, abs=pos_tol)
+            assert qd[0, 2] == pytest.approx(g * t, abs=vel_tol)
+            assert abs(q[0, 0]) < 1e-4 and abs(q[0, 1]) < 1e-4
+
+    _free_loop(orc, model, dt, 500, on_step=check)
+
+
+def test_oracle_projectile(orc):
+    g, dt = -10.0, 1e-3
+    p0, v0 = np.array([0.0, 0.0, 10.0]), np.array([5.0, 0.0, 10.0])
+    b = ModelBuilder(up_axis="Z", gravity=g)
+    b.add_shape_sphere(b.add_body(xform=list(p0) + [0.0, 0.0, 0.0, 1.0]), radius=0.1)
+    model = b.finalize(device="cpu")
+    qd0 = np.zeros((1, 6), np.float32)
+    qd0[0, :3] = v0
+
+    def check(i, q, qd):
+        if i in (10, 20, 30, 50, 70, 100):
+            t = i * dt
+            pos_tol, vel_tol = _tolerances(g, dt, t)
+            want_p = p0 + v0 * t + np.array([0.0, 0.0, 0.5 * g * t * t])
+            want_v = v0 + np.array([0.0, 0.0, g * t])
+            assert np.all(np.abs(q[0, :3] - want_p) <= pos_tol)
+            assert np.all(np.abs(qd[0, :3] - want_v) <= vel_tol)
+
+    _free_loop(orc, model, dt, 100, qd0=qd0, on_step=check)
+
+
+def _rot(qxyzw):
+    x, y, z, w = (float(v) for v in qxyzw)
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+
+
+def test_oracle_momentum_conservation(orc):
+    """Four separated free boxes without gravity: linear and angular momentum drift below
+    5e-4 (relative) over 1000 steps, and the bodies move."""
+    pos = [(0.0, 0.0, 0.0), (100.0, 0.0, 0.0), (0.0, 100.0, 0.0), (0.0, 0.0, 100.0)]
+    vel = [(1.0, 0.0, 0.0, 0.0, 0.0, 0.5), (0.0, -1.0, 0.0, 0.3, 0.0, 0.0), (0.0, 0.0, 1.5, 0.0, -0.2, 0.0),
+           (-0.5, 0.5, -0.5, 0.0, 0.0, -0.3)]
+    b = ModelBuilder(up_axis="Z", gravity=0.0)
+    for p in pos:
+        b.add_shape_box(b.add_body(xform=list(p) + [0.0, 0.0, 0.0, 1.0]), hx=0.5, hy=0.5, hz=0.5)
+    model = b.finalize(device="cpu")
+    m = model.host("body_mass")
+    inertia = model.host("body_inertia").reshape(-1, 3, 3)
+
+    def momenta(q, qd):
+        p_tot, l_tot = np.zeros(3), np.zeros(3)
+        for i in range(4):
+            p_tot += m[i] * qd[i, :3]
+            l_tot += np.cross(q[i, :3], m[i] * qd[i, :3])
+            r = _rot(q[i, 3:7])
+            l_tot += r @ inertia[i] @ r.T @ qd[i, 3:6]
+        return p_tot, l_tot
+
+    qd0 = np.asarray(vel, np.float32)
+    q0 = model.host("body_q").copy()
+    p_a, l_a = momenta(q0, qd0)
+    q, qd = _free_loop(orc, model, 1e-3, 1000, qd0=qd0)
+    p_b, l_b = momenta(q, qd)
+    assert np.linalg.norm(p_b - p_a) / np.linalg.norm(p_a) < 5e-4
+    assert np.linalg.norm(l_b - l_a) / np.linalg.norm(l_a) < 5e-4
+    assert np.linalg.norm(q[:, :3] - np.asarray(pos)) > 0.1
