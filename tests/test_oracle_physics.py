@@ -17,9 +17,12 @@ Scenes and assertions are those of the reference's own tests:
     28-227 and 766-831 with SolverXPBD(iterations=2) (:841).
   * static and dynamic friction, free fall, projectile motion and momentum
     conservation: newton/tests/test_physics_validation.py:505-641, :21-80,
-    :256-318, :413-498 with the XPBD settings those tests register.
+    :256-318, :413-498 with the XPBD settings those tests register; the
+    revolute pendulum's period (:83-158, 20 iterations, dt 3e-4).
 The CUDA path is compared with the oracle bit for bit in test_gpu_solver_extras.py.
 """
+
+import math
 
 import numpy as np
 import pytest
@@ -535,3 +538,40 @@ def test_oracle_momentum_conservation(orc):
     assert np.linalg.norm(p_b - p_a) / np.linalg.norm(p_a) < 5e-4
     assert np.linalg.norm(l_b - l_a) / np.linalg.norm(l_a) < 5e-4
     assert np.linalg.norm(q[:, :3] - np.asarray(pos)) > 0.1
+
+
+def test_oracle_pendulum_period(orc):
+    """newton/tests/test_physics_validation.py:83-158 with SolverXPBD(iterations=20,
+    angular_damping=0) and dt 3e-4 (:1579-1591): a point-like sphere (r 0.01) on a 1 m
+    revolute pendulum released at 0.05 rad follows theta0 cos(omega t) with
+    T = 2 pi sqrt(I_pivot / (m g L)) within 1 % of the amplitude (mean error over 3.5
+    periods).  Z-up here, swinging about y; the body starts at the pose forward
+    kinematics gives the initial angle."""
+    g, L, theta0, dt = 10.0, 1.0, 0.05, 3e-4
+    b = ModelBuilder(gravity=-g)
+    s, c = math.sin(theta0), math.cos(theta0)
+    q_link = (0.0, math.sin(0.5 * theta0), 0.0, math.cos(0.5 * theta0))  # theta0 about +y
+    link = b.add_link(xform=((-L * s, 0.0, -L * c), q_link))
+    b.add_shape_sphere(link, radius=0.01)
+    ident = (0.0, 0.0, 0.0, 1.0)
+    b.add_joint_revolute(-1, link, parent_xform=((0.0, 0.0, 0.0), ident), child_xform=((0.0, 0.0, L), ident),
+                         axis=(0.0, 1.0, 0.0))
+    model = b.finalize(device="cpu")
+    m = float(model.host("body_mass")[0])
+    i_pivot = float(model.host("body_inertia").reshape(-1, 3, 3)[0, 1, 1]) + m * L * L
+    period = 2.0 * math.pi * math.sqrt(i_pivot / (m * g * L))
+    lay = PairLayout(model, model.host("shape_contact_pairs"))
+    p = SolverXPBD(model, iterations=20, angular_damping=0.0).params()
+    q, qd = model.host("body_q").copy(), model.host("body_qd").copy()
+    f = np.zeros((1, 6), np.float32)
+    jt = model.host("joint_target_pos")
+    zeros = np.zeros_like(jt)
+    steps = int(3.5 * period / dt)
+    angles = np.empty(steps)
+    for i in range(steps):
+        q, qd = orc.step(model, lay, p, q, qd, f, None, dt, joint_target_pos=jt, joint_target_vel=zeros,
+                         joint_f=zeros)[:2]
+        angles[i] = math.atan2(-q[0, 0], -q[0, 2])  # +theta swings the body towards -x
+    t = np.arange(1, steps + 1) * dt
+    err = np.mean(np.abs(angles - theta0 * np.cos(2.0 * math.pi / period * t))) / theta0
+    assert err < 0.01, err
