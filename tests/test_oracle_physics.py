@@ -18,7 +18,8 @@ Scenes and assertions are those of the reference's own tests:
   * static and dynamic friction, free fall, projectile motion and momentum
     conservation: newton/tests/test_physics_validation.py:505-641, :21-80,
     :256-318, :413-498 with the XPBD settings those tests register; the
-    revolute pendulum's period (:83-158, 20 iterations, dt 3e-4).
+    revolute pendulum's period (:83-158, 20 iterations, dt 3e-4) and joint
+    actuation by joint forces (:321-409).
 The CUDA path is compared with the oracle bit for bit in test_gpu_solver_extras.py.
 """
 
@@ -575,3 +576,41 @@ def test_oracle_pendulum_period(orc):
     t = np.arange(1, steps + 1) * dt
     err = np.mean(np.abs(angles - theta0 * np.cos(2.0 * math.pi / period * t))) / theta0
     assert err < 0.01, err
+
+
+def test_oracle_joint_actuation(orc):
+    """newton/tests/test_physics_validation.py:321-409 with SolverXPBD(iterations=20,
+    angular_damping=0): without gravity, a joint torque of 5 N m on a revolute link and a
+    force of 5 N on a prismatic link accelerate them as tau / I and F / m over 300 steps
+    of 1 ms.  Measured on the bodies' twists (the joint coordinates of the reference
+    follow from them)."""
+    tau, force, dt, steps = 5.0, 5.0, 1e-3, 300
+    b = ModelBuilder(gravity=0.0)
+    ident = (0.0, 0.0, 0.0, 1.0)
+    rev = b.add_link(xform=((0.0, 0.0, 0.0), ident))
+    b.add_shape_box(rev, hx=0.2, hy=0.2, hz=0.2)
+    b.add_joint_revolute(-1, rev, parent_xform=((0.0, 0.0, 0.0), ident), child_xform=((0.0, 0.0, 0.0), ident),
+                         axis=(0.0, 0.0, 1.0))
+    pri = b.add_link(xform=((0.0, 0.0, 5.0), ident))
+    b.add_shape_sphere(pri, radius=0.1)
+    b.add_joint_prismatic(-1, pri, parent_xform=((0.0, 0.0, 5.0), ident), child_xform=((0.0, 0.0, 0.0), ident),
+                          axis=(1.0, 0.0, 0.0))
+    model = b.finalize(device="cpu")
+    i_zz = float(model.host("body_inertia").reshape(-1, 3, 3)[rev, 2, 2])
+    m_pri = float(model.host("body_mass")[pri])
+    qd_start = model.host("joint_qd_start")
+    jf = np.zeros(model.joint_dof_count, np.float32)
+    jf[qd_start[0]] = tau
+    jf[qd_start[1]] = force
+    lay = PairLayout(model, model.host("shape_contact_pairs"))
+    p = SolverXPBD(model, iterations=20, angular_damping=0.0).params()
+    q, qd = model.host("body_q").copy(), model.host("body_qd").copy()
+    f = np.zeros((model.body_count, 6), np.float32)
+    zeros = np.zeros(model.joint_dof_count, np.float32)
+    for _ in range(steps):
+        q, qd = orc.step(model, lay, p, q, qd, f, None, dt, joint_target_pos=zeros, joint_target_vel=zeros,
+                         joint_f=jf)[:2]
+    t = steps * dt
+    assert qd[rev, 5] == pytest.approx(tau * t / i_zz, abs=max(tau / i_zz * dt, 1e-3))
+    assert qd[pri, 0] == pytest.approx(force * t / m_pri, abs=max(force / m_pri * dt, 1e-3))
+    assert qd[rev, 5] > 0.0 and qd[pri, 0] > 0.0
