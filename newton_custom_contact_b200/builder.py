@@ -229,7 +229,9 @@ class ModelBuilder:
         self.shape_collision_group: list[int] = []
         self.shape_world: list[int] = []
         self.shape_label: list[str] = []
-        self.shape_collision_filter_pairs: set[tuple[int, int]] = set()
+        # a list, as in the reference builder (builder.py:966), so that callers may append;
+        # the pair list canonicalises and de-duplicates it
+        self.shape_collision_filter_pairs: list[tuple[int, int]] = []
         # joints
         self.joint_type: list[int] = []
         self.joint_enabled: list[bool] = []
@@ -355,7 +357,7 @@ class ModelBuilder:
             self.shape_world.append(self._current_world)
             self.shape_label.append(builder.shape_label[s])
         for a, b in builder.shape_collision_filter_pairs:
-            self.shape_collision_filter_pairs.add((a + s_off, b + s_off))
+            self.shape_collision_filter_pairs.append((a + s_off, b + s_off))
         for j in range(builder.joint_count):
             p = builder.joint_parent[j]
             c = builder.joint_child[j]
@@ -506,7 +508,7 @@ class ModelBuilder:
     # ------------------------------------------------------------------ shapes
     def add_shape_collision_filter_pair(self, shape_a: int, shape_b: int) -> None:
         a, b = (shape_a, shape_b) if shape_a < shape_b else (shape_b, shape_a)
-        self.shape_collision_filter_pairs.add((a, b))
+        self.shape_collision_filter_pairs.append((a, b))
 
     def add_shape(self, *, body: int, type: int, xform=None, cfg=None, scale=None, is_static: bool = False,
                   label=None) -> int:
@@ -634,7 +636,7 @@ class ModelBuilder:
         colliding = [i for i in range(self.shape_count) if flags[i] & ShapeFlags.COLLIDE_SHAPES]
         order = sorted(colliding, key=lambda i: self.shape_world[i])
         pairs = []
-        filters = self.shape_collision_filter_pairs
+        filters = {(min(a, b), max(a, b)) for a, b in self.shape_collision_filter_pairs}
         for i1 in range(len(order)):
             s1 = order[i1]
             w1 = self.shape_world[s1]

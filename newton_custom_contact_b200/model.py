@@ -139,7 +139,7 @@ class Model:
         h["gravity"] = np.asarray(grav, dtype=f32).reshape(W, 3)
         h["shape_contact_pairs"] = b.find_shape_contact_pairs()
         m._init_from_host(h, world_count=W, uses_worlds=b.world_count > 0,
-                          filter_pairs=set(b.shape_collision_filter_pairs),
+                          filter_pairs={(min(x, y), max(x, y)) for x, y in b.shape_collision_filter_pairs},
                           requested=set(b._requested_contact_attributes))
         m._requested_state_attributes = set(b._requested_state_attributes)
         return m

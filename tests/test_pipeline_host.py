@@ -7,6 +7,8 @@
   pair set grows linearly with the world count, global shapes join every
   world's segment).
 * Constructor errors: newton/_src/sim/collide.py:587-603.
+* Shape collision filter pairs: :460-573 (an excluded pair makes no contacts; the
+  explicit, NxN and SAP modes report the same pairs).
 """
 
 import numpy as np
@@ -92,3 +94,41 @@ def test_constructor_errors():
         CollisionPipeline(model, contact_report=True)
     with pytest.raises(NotImplementedError):
         CollisionPipeline(model, sdf_hydroelastic_config=object())
+
+
+# ---- newton/tests/test_collision_pipeline.py:460-573: excluded shape pairs make no
+# contacts, and every broad-phase mode reports the same contacting pairs (the
+# contacts come from the CPU oracle of the pipeline here)
+
+def _overlapping_spheres(n, exclude):
+    b = ModelBuilder(gravity=0.0)
+    b.rigid_gap = 0.01
+    shapes = []
+    for _ in range(n):
+        body = b.add_body(xform=[0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0])
+        shapes.append(b.add_shape_sphere(body=body, radius=0.5))
+    a, c = shapes[exclude[0]], shapes[exclude[1]]
+    b.shape_collision_filter_pairs.append((min(a, c), max(a, c)))  # appended, as the reference test does
+    return b.finalize(device="cpu"), (min(a, c), max(a, c))
+
+
+def _contact_pairs(orc, model, broad_phase):
+    pipe = CollisionPipeline(model, broad_phase=broad_phase)
+    segs = orc.collide(model, pipe.layout, model.host("body_q"))
+    tab = orc.contacts_table(model, pipe.layout, segs)
+    return {(min(int(r[1]), int(r[2])), max(int(r[1]), int(r[2]))) for r in tab}
+
+
+@pytest.mark.parametrize("broad_phase", ["nxn", "sap", "explicit"])
+def test_filtered_pair_makes_no_contacts(orc, broad_phase):
+    model, _ = _overlapping_spheres(2, (0, 1))
+    assert _contact_pairs(orc, model, broad_phase) == set()
+
+
+def test_filter_consistent_across_broad_phases(orc):
+    model, excluded = _overlapping_spheres(3, (0, 1))
+    sets = {bp: _contact_pairs(orc, model, bp) for bp in ("explicit", "nxn", "sap")}
+    for pairs in sets.values():
+        assert excluded not in pairs
+        assert len(pairs) == 2
+    assert sets["explicit"] == sets["nxn"] == sets["sap"]
