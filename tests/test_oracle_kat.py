@@ -6,7 +6,9 @@ sphere-capsule :587, capsule-capsule :696, sphere-box :1136, plane-capsule :1251
 plane-box :1335, box-box :1529, box-box with margin :1613, capsule-box :1749,
 box-box depths :1881) and
 newton/tests/test_narrow_phase.py (sphere-box corner :591, box-box face :635,
-edge :708, capsules :801-895, plane-capsule :1083, per-shape gap :1271).  Contacts here run the full pipeline path
+edge :708, capsules :801-895, plane-capsule :1083, per-shape gap :1271) and
+newton/tests/test_collision_pipeline.py (sphere-pair normal direction :590,
+box-box quaternion perturbation :720).  Contacts here run the full pipeline path
 (primitive routing, MPR/GJK, manifold, write_contact gap test) with gap 0 on
 both shapes, i.e. the reference primitive with margin 0.
 """
@@ -255,3 +257,64 @@ def test_per_shape_gap(orc, z, gap_sphere, contact):
     assert (rows.shape[0] == 1) == contact
     if contact:
         assert rows[0, 11] == pytest.approx(z - 0.2, abs=1e-5)
+
+
+# ---- newton/tests/test_collision_pipeline.py:590-717 (contact normal direction for
+# sphere pairs) and :720-771 (box-box under a 1e-14 quaternion perturbation), through
+# the pipeline's oracle with a model of free bodies
+
+def _model_contacts(orc, model):
+    from newton_custom_contact_b200 import CollisionPipeline
+
+    pipe = CollisionPipeline(model)
+    segs = orc.collide(model, pipe.layout, model.host("body_q"))
+    return orc.contacts_table(model, pipe.layout, segs)
+
+
+def test_sphere_pair_normals_point_from_shape0_to_shape1(orc):
+    from newton_custom_contact_b200 import ModelBuilder
+
+    half_dists, ys, expect = [0.3, 0.5, 0.54, 0.75], [0.0, 3.0, 6.0, 9.0], [True, True, True, False]
+    b = ModelBuilder(gravity=0.0)
+    b.rigid_gap = 0.05
+    centres = []
+    for hd, y in zip(half_dists, ys):
+        for x in (-hd, hd):
+            centres.append((x, y, 0.0))
+            b.add_shape_sphere(b.add_body(xform=[x, y, 0.0, 0.0, 0.0, 0.0, 1.0]), radius=0.5)
+    model = b.finalize(device="cpu")
+    tab = _model_contacts(orc, model)
+    centres = np.asarray(centres)
+    per_pair = {k: [r for r in tab if int(r[1]) // 2 == k] for k in range(4)}
+    for k in range(4):
+        assert (len(per_pair[k]) > 0) == expect[k]
+        for r in per_pair[k]:
+            s0, s1 = int(r[1]), int(r[2])
+            n = r[10:13]
+            assert np.linalg.norm(n) == pytest.approx(1.0, abs=1e-3)
+            d = centres[s1] - centres[s0]
+            assert np.dot(n, d / np.linalg.norm(d)) > 0.95
+            mid = 0.5 * ((r[4:7] + centres[s0]) + (r[7:10] + centres[s1]))
+            lo, hi = min(centres[s0, 0], centres[s1, 0]), max(centres[s0, 0], centres[s1, 0])
+            assert lo - 1e-3 <= mid[0] <= hi + 1e-3
+
+
+def test_box_box_quaternion_perturbation(orc):
+    """Face-to-face cubes rotated 30 deg about x, the second with a 1e-14 quaternion
+    perturbation: four face-corner contacts, body-frame points inside the cube, normals
+    along x (the support deadband of support_function.py:39)."""
+    from newton_custom_contact_b200 import ModelBuilder
+
+    half = 0.495
+    q_clean = [0.2588233343021173, 0.0, 0.0, 0.9659246769912934]
+    q_noisy = [0.2588233343021173, -2.27e-14, 9.25e-15, 0.9659246769912934]
+    y, z = 6.680443286895752, 4.4285125732421875
+    b = ModelBuilder()
+    b.add_shape_box(b.add_body(xform=[half, y, z] + q_clean), hx=half, hy=half, hz=half)
+    b.add_shape_box(b.add_body(xform=[-half, y, z] + q_noisy), hx=half, hy=half, hz=half)
+    model = b.finalize(device="cpu")
+    tab = _model_contacts(orc, model)
+    assert tab.shape[0] == 4
+    for r in tab:
+        assert np.all(np.abs(r[4:7]) <= half * 1.01)
+        assert abs(r[10]) == pytest.approx(1.0, abs=0.01)
