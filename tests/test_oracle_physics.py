@@ -13,8 +13,9 @@ Scenes and assertions are those of the reference's own tests:
   * no bounce: newton/tests/test_shapes_no_bounce.py:21-226 (a grid of shapes
     dropped on the ground never rises above max(2 m, its start) in 200 frames),
     with the sphere / box / capsule shapes of the grid.
-  * shapes at rest on a plane and a two-box drop: newton/tests/test_rigid_contact.py:
-    28-227 and 766-831 with SolverXPBD(iterations=2) (:841).
+  * shapes at rest on a plane, a two-box drop and boxes / spheres / a capsule held on
+    a ramp by an end wall: newton/tests/test_rigid_contact.py:28-227, 766-831 and
+    230-503 with SolverXPBD(iterations=2) (:841).
   * static and dynamic friction, free fall, projectile motion and momentum
     conservation: newton/tests/test_physics_validation.py:505-641, :21-80,
     :256-318, :413-498 with the XPBD settings those tests register; the
@@ -614,3 +615,54 @@ def test_oracle_joint_actuation(orc):
     assert qd[rev, 5] == pytest.approx(tau * t / i_zz, abs=max(tau / i_zz * dt, 1e-3))
     assert qd[pri, 0] == pytest.approx(force * t / m_pri, abs=max(force / m_pri * dt, 1e-3))
     assert qd[rev, 5] > 0.0 and qd[pri, 0] > 0.0
+
+
+def _qmul(a, b):
+    ax, ay, az, aw = a
+    bx, by, bz, bw = b
+    return [aw * bx + ax * bw + ay * bz - az * by, aw * by - ax * bz + ay * bw + az * bx,
+            aw * bz + ax * by - ay * bx + az * bw, aw * bw - ax * bx - ay * by - az * bz]
+
+
+def test_oracle_ramp_multicontact_stays_put(orc):
+    """newton/tests/test_rigid_contact.py:230-503 (a 30 degree ramp plane with guide walls
+    and an end wall, XPBD with 2 iterations, 100 frames of 10 substeps at 60 fps): every
+    body moves less than 0.15 cube sizes and turns less than 10 degrees.  The bodies are
+    the reference's contiguous run of in-scope shapes from the wall up (two cubes, two
+    spheres, the capsule); its cylinder, cones and convex hulls, which rest further up the
+    run, are left out with everything behind them."""
+    from newton_custom_contact_b200.builder import quat_from_axis_angle
+
+    length, thick, angle, wall_h = 10.0, 0.5, np.radians(30.0), 2.0
+    cube = 0.99
+    width = cube * 2.01
+    ramp_c = np.array([0.0, length / 2 * np.cos(angle), length / 2 * np.sin(angle)])
+    rq = list(quat_from_axis_angle((1.0, 0.0, 0.0), float(angle)))
+    r = _rot(rq)
+    fwd, up, right = r @ [0.0, -1.0, 0.0], r @ [0.0, 0.0, 1.0], r @ [1.0, 0.0, 0.0]
+    b = ModelBuilder()
+    b.add_shape_plane(body=-1, xform=list(ramp_c) + rq, width=0.0, length=0.0)
+    for side in (1.0, -1.0):
+        c = ramp_c + side * (width / 2 + 0.05) * right + 0.15 * up
+        b.add_shape_box(-1, xform=list(c) + rq, hx=0.05, hy=length / 2, hz=0.15)
+    shift = 0.6 * length
+    tmp = ramp_c + 0.5 * cube * (up + shift * fwd)
+    b.add_shape_box(-1, xform=[0.0, tmp[1] - cube / 2 * 1.4 - thick / 2, tmp[2], 0.0, 0.0, 0.0, 1.0],
+                    hx=width / 2, hy=thick / 2, hz=wall_h / 2)
+    for side in (1.0, -1.0):
+        p = ramp_c + 0.5 * cube * (up + side * right + shift * fwd)
+        b.add_shape_box(b.add_body(xform=list(p) + rq), hx=cube / 2, hy=cube / 2, hz=cube / 2)
+    for side in (1.0, -1.0):
+        p = ramp_c + 0.5 * cube * (up + side * right + (shift - 2.01) * fwd)
+        b.add_shape_sphere(b.add_body(xform=list(p) + rq), radius=cube / 2)
+    p = ramp_c + 0.5 * cube * (up + (shift - 4.02) * fwd)
+    z_to_x = [0.0, math.sin(math.pi / 4), 0.0, math.cos(math.pi / 4)]
+    b.add_shape_capsule(b.add_body(xform=list(p) + _qmul(rq, z_to_x)), radius=cube / 2, half_height=cube / 2)
+    b.add_ground_plane()
+    model = b.finalize(device="cpu")
+    q0 = model.host("body_q").copy()
+    q, _ = _sim(orc, model, SolverXPBD(model, iterations=2), 1.0 / 60.0 / 10, 1000)
+    for i in range(model.body_count):
+        assert np.linalg.norm(q[i, :3] - q0[i, :3]) < 0.15 * cube, i
+        dot = min(1.0, abs(float(np.dot(q[i, 3:], q0[i, 3:]))))
+        assert 2.0 * math.acos(dot) < math.radians(10.0), i
