@@ -16,6 +16,8 @@ Scenes and assertions are those of the reference's own tests:
   * shapes at rest on a plane, a two-box drop and boxes / spheres / a capsule held on
     a ramp by an end wall: newton/tests/test_rigid_contact.py:28-227, 766-831 and
     230-503 with SolverXPBD(iterations=2) (:841).
+  * head-on collisions of sphere / box / capsule pairs:
+    newton/tests/test_collision_pipeline.py:46-262.
   * static and dynamic friction, free fall, projectile motion and momentum
     conservation: newton/tests/test_physics_validation.py:505-641, :21-80,
     :256-318, :413-498 with the XPBD settings those tests register; the
@@ -666,3 +668,48 @@ def test_oracle_ramp_multicontact_stays_put(orc):
         assert np.linalg.norm(q[i, :3] - q0[i, :3]) < 0.15 * cube, i
         dot = min(1.0, abs(float(np.dot(q[i, 3:], q0[i, 3:]))))
         assert 2.0 * math.acos(dot) < math.radians(10.0), i
+
+
+# ---- newton/tests/test_collision_pipeline.py:46-262: body A (x = -1) thrown at 5 m/s
+# into body B (x = +1) without gravity; contacts found once per frame and reused for its
+# 10 substeps, XPBD defaults, 100 frames at 60 fps.  Afterwards A has no sideways
+# velocity, and B moves forward (0.03 < vx <= 5) without sideways (and, where the
+# reference asks, angular) velocity.  The pairs of shapes this solver collides:
+
+_HEAD_ON = [("sphere", "sphere", True), ("sphere", "box", True), ("sphere", "capsule", True),
+            ("box", "box", False), ("capsule", "capsule", False)]
+
+
+def _add_default_shape(b, kind, body):
+    if kind == "box":
+        b.add_shape_box(body)            # builder defaults: half extents 0.5
+    elif kind == "sphere":
+        b.add_shape_sphere(body, radius=0.5)
+    else:
+        b.add_shape_capsule(body, radius=0.25, half_height=0.3)
+
+
+@pytest.mark.parametrize("kind_a,kind_b,strict_b", _HEAD_ON)
+def test_oracle_head_on_collision(orc, kind_a, kind_b, strict_b):
+    b = ModelBuilder(gravity=0.0)
+    b.rigid_gap = 0.005
+    _add_default_shape(b, kind_a, b.add_body(xform=[-1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0]))
+    _add_default_shape(b, kind_b, b.add_body(xform=[1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0]))
+    model = b.finalize(device="cpu")
+    lay = PairLayout(model, model.host("shape_contact_pairs"))
+    p = SolverXPBD(model).params()
+    q = model.host("body_q").copy()
+    qd = model.host("body_qd").copy()
+    qd[0, 0] = 5.0
+    f = np.zeros((2, 6), np.float32)
+    dt = 1.0 / 60.0 / 10
+    for _ in range(100):
+        segs = orc.collide(model, lay, q)
+        for _ in range(10):
+            q, qd = orc.step(model, lay, p, q, qd, f, segs, dt)[:2]
+    tol = 3e-3
+    assert abs(qd[0, 1]) < tol and abs(qd[0, 2]) < tol
+    assert 0.03 < qd[1, 0] <= 5.0
+    assert abs(qd[1, 1]) < tol and abs(qd[1, 2]) < tol
+    if strict_b:
+        assert np.all(np.abs(qd[1, 3:6]) < tol)
