@@ -9,6 +9,8 @@
 * Constructor errors: newton/_src/sim/collide.py:587-603.
 * Shape collision filter pairs: :460-573 (an excluded pair makes no contacts; the
   explicit, NxN and SAP modes report the same pairs).
+* Candidate pairs across worlds and collision groups: newton/tests/test_broad_phase.py:
+  22-68, 271-428 (the builder's explicit list and the NxN list against the rule).
 """
 
 import numpy as np
@@ -132,3 +134,64 @@ def test_filter_consistent_across_broad_phases(orc):
         assert excluded not in pairs
         assert len(pairs) == 2
     assert sets["explicit"] == sets["nxn"] == sets["sap"]
+
+
+# ---- newton/tests/test_broad_phase.py:22-68 and :271-428: the candidate pairs across
+# worlds and collision groups (positive groups collide with themselves and with
+# negative groups, a negative group with everything but itself, group 0 with nothing;
+# world -1 shapes with every world; shapes of one body, the static ones included,
+# never pair: builder.py:5539-5542)
+
+def _group_pair(a, b):
+    if a == 0 or b == 0:
+        return False
+    return (a == b or b < 0) if a > 0 else a != b
+
+
+def _world_group_pair(wa, wb, ga, gb):
+    if wa != -1 and wb != -1 and wa != wb:
+        return False
+    return _group_pair(ga, gb)
+
+
+@pytest.mark.parametrize("seed", [123, 7])
+def test_pairs_follow_world_and_group_rules(seed):
+    from newton_custom_contact_b200.collide import nxn_pairs
+
+    rng = np.random.Generator(np.random.PCG64(seed))
+    worlds, per_world, n_global = 4, 10, 5
+    groups = rng.integers(1, 6, size=worlds * per_world + n_global)
+    groups[rng.choice(groups.size, size=int(np.sqrt(groups.size)), replace=False)] = -1
+    groups[rng.choice(groups.size, size=2, replace=False)] = 0
+    b = ModelBuilder()
+    meta = []  # (shape, world, group, body)
+    k = 0
+    for _ in range(n_global):  # static shapes outside any world
+        g = int(groups[k])
+        k += 1
+        s = b.add_shape_box(-1, xform=list(rng.random(3) * 5.0) + [0.0, 0.0, 0.0, 1.0], hx=0.2, hy=0.2, hz=0.2,
+                            cfg=ModelBuilder.ShapeConfig(collision_group=g))
+        meta.append((s, -1, g, -1))
+    for w in range(worlds):
+        b.begin_world()
+        for _ in range(per_world):
+            g = int(groups[k])
+            k += 1
+            body = b.add_body(xform=list(rng.random(3) * 5.0) + [0.0, 0.0, 0.0, 1.0])
+            s = b.add_shape_sphere(body, radius=0.2, cfg=ModelBuilder.ShapeConfig(collision_group=g))
+            meta.append((s, w, g, body))
+        b.end_world()
+    want = set()
+    for i in range(len(meta)):
+        for j in range(i + 1, len(meta)):
+            (sa, wa, ga, ba), (sb, wb, gb, bb) = meta[i], meta[j]
+            if ba != bb and _world_group_pair(wa, wb, ga, gb):
+                want.add((min(sa, sb), max(sa, sb)))
+    model = b.finalize(device="cpu")
+    explicit = {tuple(p) for p in model.host("shape_contact_pairs").tolist()}
+    nxn = {tuple(p) for p in np.asarray(nxn_pairs(model)).reshape(-1, 2).tolist()}
+    assert explicit == want
+    assert nxn == want
+    # the draw exercises every rule: global-world pairs, negative and zero groups
+    assert any(-1 in (meta[a][1], meta[b][1]) for a, b in [(0, len(meta) - 1)])
+    assert (groups < 0).any() and (groups == 0).any()
