@@ -11,6 +11,7 @@
   explicit, NxN and SAP modes report the same pairs).
 * Candidate pairs across worlds and collision groups: newton/tests/test_broad_phase.py:
   22-68, 271-428 (the builder's explicit list and the NxN list against the rule).
+* Per-shape gaps in the broad and narrow phase: test_broad_phase.py:2024-2130.
 """
 
 import numpy as np
@@ -195,3 +196,28 @@ def test_pairs_follow_world_and_group_rules(seed):
     # the draw exercises every rule: global-world pairs, negative and zero groups
     assert any(-1 in (meta[a][1], meta[b][1]) for a, b in [(0, len(meta) - 1)])
     assert (groups < 0).any() and (groups == 0).any()
+
+
+def test_per_shape_gap_through_the_pipeline(orc):
+    """newton/tests/test_broad_phase.py:2024-2130: two spheres (r 0.2) hover 0.04 above the
+    ground (gap 0.01); A with gap 0.02 (summed 0.03) gets no contact, B with gap 0.06
+    (summed 0.07) does, with separation 0.04 -- the broad phase and the narrow phase
+    of the pipeline both apply each shape's own gap."""
+    b = ModelBuilder(gravity=0.0)
+    b.add_ground_plane(cfg=ModelBuilder.ShapeConfig(gap=0.01))
+    a = b.add_shape_sphere(b.add_body(xform=[0.0, 0.0, 0.24, 0.0, 0.0, 0.0, 1.0]), radius=0.2,
+                           cfg=ModelBuilder.ShapeConfig(gap=0.02))
+    c = b.add_shape_sphere(b.add_body(xform=[10.0, 0.0, 0.24, 0.0, 0.0, 0.0, 1.0]), radius=0.2,
+                           cfg=ModelBuilder.ShapeConfig(gap=0.06))
+    model = b.finalize(device="cpu")
+    pipe = CollisionPipeline(model)
+    segs = orc.collide(model, pipe.layout, model.host("body_q"))
+    tab = orc.contacts_table(model, pipe.layout, segs)
+    shapes = {int(r[1]) for r in tab} | {int(r[2]) for r in tab}
+    assert c in shapes and a not in shapes
+    row = [r for r in tab if c in (int(r[1]), int(r[2]))][0]
+    n, p0, p1 = row[10:13], row[4:7], row[7:10]
+    # ground point in world space (static: body frame = world) and sphere centre offset
+    centre = np.array([10.0, 0.0, 0.24])
+    sep = abs(float(np.dot(n, (p1 + centre if int(row[2]) == c else p1) - (p0 + centre if int(row[1]) == c else p0))))
+    assert sep - (row[19] + row[20]) == pytest.approx(0.04, abs=1e-5)
