@@ -370,6 +370,9 @@ int nb_publish_contacts(const NbModelDesc* model, const NbContactSeg* seg,
  * `iterations` x (solve_body_contact_positions, apply_body_deltas,
  * solve_body_joints, apply_body_deltas), optional restitution and the
  * kinematic pass-through.  Replaces SolverXPBD.step (solver_xpbd.py:259-764).
+ * With model->all_joints_free == 1 and neither restitution nor per-contact
+ * impulses requested, a lean kernel without the joint solve runs (same
+ * results); 0 always selects the full kernel.
  */
 int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbStepIO* io,
                  const NbContactSeg* seg, float dt, int32_t grid_ctas, void* stream);
