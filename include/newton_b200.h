@@ -501,7 +501,12 @@ int nb_ingest_contacts(const NbModelDesc* model, const NbContactsPublic* pub,
  * device: calls that may overlap in time on one device race; calls on one
  * stream are ordered.  Nothing in the scratch must start at zero.  The first
  * call on a device looks up the array's address (cudaGetSymbolAddress); make
- * it before any stream capture.
+ * it before any stream capture.  The address is kept for the life of the
+ * process: cudaDeviceReset between calls is not supported (the next call
+ * would write through the address of the destroyed context).
+ * The caller's pub->world_offset is neither read nor written, so this call
+ * cannot feed the consumer of per-world offsets: nb_match_contacts (contact
+ * matching) reads pub->world_offset and needs nb_publish_contacts.
  */
 #define NB_PUBLISH_STATIC_MAX_WORLDS 65536
 int nb_publish_contacts_static(const NbModelDesc* model, const NbContactSeg* seg,

@@ -1,11 +1,22 @@
-"""Loader for the in-tree CUDA library libnewton_b200.so (C ABI in include/newton_b200.h).
+"""Loader for the in-tree CUDA library (C ABI in include/newton_b200.h).
 
-There is no fallback: if the library or a CUDA device is missing, every entry
-point raises.
+Two builds of the same sources export the same ABI:
+
+* ``libnewton_b200.so`` -- the product build (the compiler contracts a*b+c
+  into fused multiply-adds); used unless another build is selected;
+* ``libnewton_b200_exact.so`` -- the parity build (``--fmad=false``): every
+  fp32 expression rounds in source order, exactly like the CPU oracle, so the
+  two agree bit for bit.
+
+``use_build("exact")`` / ``with build("exact"):`` select the parity build for
+the calls that follow (the environment variable ``NEWTON_B200_BUILD`` sets the
+initial choice).  There is no fallback: if the library or a CUDA device is
+missing, every entry point raises.
 """
 
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 
@@ -26,8 +37,10 @@ from ._abi import (
     NbXpbdParams,
 )
 
+_HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_NAME = "libnewton_b200.so"
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+LIB_PATH = os.path.join(_HERE, LIB_NAME)
+BUILDS = {"product": LIB_PATH, "exact": os.path.join(_HERE, "libnewton_b200_exact.so")}
 
 EXPORTS = (
     "nb_abi_version",
@@ -49,7 +62,33 @@ EXPORTS = (
     "nb_xpbd_substeps",
 )
 
-_lib = None
+_libs: dict = {}
+_active = os.environ.get("NEWTON_B200_BUILD", "product")
+if _active not in BUILDS:
+    raise ValueError(f"NEWTON_B200_BUILD must be one of {sorted(BUILDS)}, got {_active!r}")
+
+
+def use_build(name: str) -> str:
+    """Select the build ("product" or "exact") that load() returns from now on; returns the previous one."""
+    global _active
+    if name not in BUILDS:
+        raise ValueError(f"unknown build {name!r}; expected one of {sorted(BUILDS)}")
+    prev, _active = _active, name
+    return prev
+
+
+def active_build() -> str:
+    return _active
+
+
+@contextlib.contextmanager
+def build(name: str):
+    """Run the enclosed calls on one build of the library."""
+    prev = use_build(name)
+    try:
+        yield load()
+    finally:
+        use_build(prev)
 
 
 class NbError(RuntimeError):
@@ -68,15 +107,14 @@ class NbError(RuntimeError):
 
 
 def load(path: str | None = None) -> C.CDLL:
-    """Load (once) and type the library; raises if it is missing."""
-    global _lib
-    if _lib is not None and path is None:
-        return _lib
-    p = path or LIB_PATH
+    """Load (once per build) and type the active build of the library; raises if it is missing."""
+    if path is None and _active in _libs:
+        return _libs[_active]
+    p = path or BUILDS[_active]
     if not os.path.exists(p):
         raise RuntimeError(
-            f"{LIB_NAME} not found at {p}; build it with `python -c 'import __graft_entry__ as g; g.build()'` "
-            "or `make -C newton_custom_contact_b200/csrc`"
+            f"{os.path.basename(p)} not found at {p}; build it with "
+            "`python -c 'import __graft_entry__ as g; g.build()'` or `make -j -C newton_custom_contact_b200/csrc`"
         )
     lib = C.CDLL(p)
     lib.nb_abi_version.restype = C.c_int
@@ -126,7 +164,7 @@ def load(path: str | None = None) -> C.CDLL:
     if v != NB_ABI_VERSION:
         raise RuntimeError(f"{LIB_NAME} ABI version {v} != {NB_ABI_VERSION}; rebuild the library")
     if path is None:
-        _lib = lib
+        _libs[_active] = lib
     return lib
 
 

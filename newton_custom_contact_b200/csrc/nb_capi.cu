@@ -1,9 +1,18 @@
 // extern "C" entry points of libnewton_b200.so (declared in include/newton_b200.h).
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <utility>
+#include <vector>
+
 #include "nb_kernels.cuh"
 
 namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_smem_mutex;
+// per device: (kernel, dynamic shared-memory bytes already allowed)
+std::vector<std::pair<const void*, size_t>> g_smem_raised[kMaxDevices];
 
 int grid_for(int requested) {
     if (requested > 0) return requested;
@@ -69,6 +78,29 @@ int smem_limit() {
 }
 
 }  // namespace
+
+cudaError_t nb_raise_dynamic_smem(const void* kernel, size_t bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_smem_mutex);
+    for (auto& kv : g_smem_raised[dev]) {
+        if (kv.first != kernel) continue;
+        if (bytes <= kv.second) return cudaSuccess;
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e == cudaSuccess) kv.second = bytes;
+        return e;
+    }
+    if (bytes <= 48 * 1024) {
+        // within the default limit: nothing to raise, remember that
+        g_smem_raised[dev].emplace_back(kernel, (size_t)48 * 1024);
+        return cudaSuccess;
+    }
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) g_smem_raised[dev].emplace_back(kernel, bytes);
+    return e;
+}
 
 extern "C" {
 

@@ -26,6 +26,8 @@
 //      (ContactSorter, contact_sort.py:194-445).
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "nb_geom.cuh"
 #include "nb_kernels.cuh"
 
@@ -707,18 +709,48 @@ size_t nb_collide_smem_bytes(const NbModelDesc* m) {
 
 size_t nb_collide_static_smem_bytes() { return (size_t)2 * (kBT / 32) * kQB * sizeof(int2); }
 
+namespace {
+
+// Occupancy of the narrow-phase kernels per device ordinal (a process may
+// drive several GPUs; the mutex orders first calls from several host threads).
+constexpr int kMaxCollideDevices = 64;
+struct NarrowOccupancy {
+    int analytic = 0, prefilter = 0, gjk = 0;
+};
+std::mutex g_occ_mutex;
+NarrowOccupancy g_occ[kMaxCollideDevices];
+
+cudaError_t narrow_occupancy(NarrowOccupancy* out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxCollideDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_occ_mutex);
+    NarrowOccupancy& c = g_occ[dev];
+    if (!c.gjk) {
+        // default grids: one wave at each kernel's occupancy (grid-stride loops)
+        int a = 0, p = 0, g = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, narrow_analytic_kernel, kNT, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, gjk_prefilter_kernel, kNT, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g, narrow_gjk_kernel, kNT, 0);
+        c.analytic = a > 0 ? a : 4;
+        c.prefilter = p > 0 ? p : 4;
+        c.gjk = g > 0 ? g : 4;
+    }
+    *out = c;
+    return cudaSuccess;
+}
+
+}  // namespace
+
 cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const NbContactSeg* seg, int grid,
                               cudaStream_t stream) {
-    size_t smem = nb_collide_smem_bytes(m);
-    // raise the dynamic shared-memory limit only when needed, so calls made
-    // during CUDA-graph capture (after a first eager call) touch no attributes
-    static size_t configured = 0;
-    cudaError_t e;
-    if (smem > configured) {
-        e = cudaFuncSetAttribute(broadphase_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = smem;
-    }
+    const size_t smem = nb_collide_smem_bytes(m);
+    cudaError_t e = nb_raise_dynamic_smem((const void*)broadphase_kernel, smem);
+    if (e != cudaSuccess) return e;
+    NarrowOccupancy occ;
+    e = narrow_occupancy(&occ);
+    if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(seg->work_counter, 0, 4 * sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(seg->work_counter + 5, 0, sizeof(int32_t), stream);
@@ -727,23 +759,13 @@ cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const N
     broadphase_kernel<<<sms * 4, kBT, smem, stream>>>(*m, body_q, *seg);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    // default grids: one wave at the kernel's occupancy (grid-stride loops)
-    static int occ_analytic = 0, occ_prefilter = 0, occ_gjk = 0;
-    if (!occ_gjk) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_analytic, narrow_analytic_kernel, kNT, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_prefilter, gjk_prefilter_kernel, kNT, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_gjk, narrow_gjk_kernel, kNT, 0);
-        occ_analytic = occ_analytic > 0 ? occ_analytic : 4;
-        occ_prefilter = occ_prefilter > 0 ? occ_prefilter : 4;
-        occ_gjk = occ_gjk > 0 ? occ_gjk : 4;
-    }
-    narrow_analytic_kernel<<<grid > 0 ? grid : sms * occ_analytic, kNT, 0, stream>>>(*m, body_q, *seg);
+    narrow_analytic_kernel<<<grid > 0 ? grid : sms * occ.analytic, kNT, 0, stream>>>(*m, body_q, *seg);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    gjk_prefilter_kernel<<<grid > 0 ? grid : sms * occ_prefilter, kNT, 0, stream>>>(*m, *seg);
+    gjk_prefilter_kernel<<<grid > 0 ? grid : sms * occ.prefilter, kNT, 0, stream>>>(*m, *seg);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    narrow_gjk_kernel<<<grid > 0 ? grid : sms * occ_gjk, kNT, 0, stream>>>(*m, body_q, *seg);
+    narrow_gjk_kernel<<<grid > 0 ? grid : sms * occ.gjk, kNT, 0, stream>>>(*m, body_q, *seg);
     return cudaGetLastError();
 }
 

@@ -35,19 +35,24 @@ cudaError_t nb_launch_ws_grads(const NbWsTrain* a, cudaStream_t s);
 cudaError_t nb_launch_ws_adam(float* w, const float* g, float* m1, float* m2, long count, float lr, float b1,
                               float b2, float eps, float wd, int step, cudaStream_t s);
 
+// Raises `kernel`'s dynamic shared-memory limit on the current device to at
+// least `bytes` (cudaFuncSetAttribute) unless an earlier call on this device
+// already did.  Attributes belong to a device, so the record is kept per
+// (kernel, device ordinal); a mutex orders first calls from several host
+// threads.  Calls that need no raise touch no attribute, which keeps them
+// legal inside CUDA-graph capture.
+cudaError_t nb_raise_dynamic_smem(const void* kernel, size_t bytes);
+
 cudaError_t nb_launch_xpbd_adjoint(const NbModelDesc* m, const NbXpbdParams* p, const NbAdjointIO* io,
                                    const NbContactSeg* seg, int has_contacts, float dt, cudaStream_t s);
 
 // Grid for grid-stride loops over contact rows: enough blocks of `threads` to
-// cover `rows`, at most 8 per SM (the SM count is read once).
+// cover `rows`, at most 8 per SM of the current device.
 inline int nb_contact_grid(long rows, int threads = 256) {
-    static int sms = 0;
-    if (sms <= 0) {
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
-            sms = 148;
-    }
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+        sms = 148;
     const long need = (rows + threads - 1) / threads;
     const long cap = 8L * sms;
     return (int)(need < 1 ? 1 : (need < cap ? need : cap));

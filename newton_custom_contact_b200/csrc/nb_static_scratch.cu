@@ -20,7 +20,12 @@
 //     order their streams) race on it; calls on one stream are ordered;
 //   * the first call on a device looks the array's address up with
 //     cudaGetSymbolAddress (which may load the module); make that first call
-//     before any stream capture.
+//     before any stream capture.  The address is cached per device ordinal
+//     for the life of the process: a cudaDeviceReset between calls is not
+//     supported;
+//   * pub->world_offset is neither read nor written, so the per-world
+//     offsets that nb_match_contacts reads are not produced here: callers
+//     that match contacts use nb_publish_contacts.
 #include <cuda_runtime.h>
 
 #include <mutex>

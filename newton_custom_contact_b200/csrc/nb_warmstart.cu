@@ -705,12 +705,8 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(TcGemm g, uint32_t* sta
 
 cudaError_t tc_gemm(const float* A, long sam, long sak, const float* B, long sbn, long sbk, float* C, long scm,
                     long scn, int M, int N, int K, bool exact, uint32_t* status, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    cudaError_t e = nb_raise_dynamic_smem((const void*)tc_gemm_kernel, kGemmSmem);
+    if (e != cudaSuccess) return e;
     if (M <= 0 || N <= 0 || K <= 0) return cudaSuccess;
     TcGemm g;
     g.A = A; g.sam = sam; g.sak = sak;
@@ -830,12 +826,8 @@ cudaError_t nb_launch_ws_targets(const NbContactsPublic* pub, float* impulse, fl
 
 cudaError_t nb_launch_ws_infer(const NbWsNet* net, const float* feat, const int32_t* count, int cap, float* out,
                                uint32_t* status, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(ws_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmBytes);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    cudaError_t e = nb_raise_dynamic_smem((const void*)ws_infer_kernel, kSmBytes);
+    if (e != cudaSuccess) return e;
     if (cap <= 0) return cudaSuccess;
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

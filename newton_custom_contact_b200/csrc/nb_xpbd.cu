@@ -1532,13 +1532,8 @@ template <int G, bool kLean, bool kWarm>
 cudaError_t launch_step_variant(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
                                 const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
     const size_t smem = nb_step_smem_bytes(m);
-    static size_t configured = 0;
-    if (smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(xpbd_step_kernel<G, kLean, kWarm>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = smem;
-    }
+    cudaError_t e = nb_raise_dynamic_smem((const void*)xpbd_step_kernel<G, kLean, kWarm>, smem);
+    if (e != cudaSuccess) return e;
     const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
     xpbd_step_kernel<G, kLean, kWarm><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
     return cudaGetLastError();
@@ -1556,13 +1551,8 @@ template <int G, bool kCompact, bool kLean, bool kWarm>
 cudaError_t launch_step_group_variant(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
                                       const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
     const size_t smem = nb_step_smem_bytes(m);
-    static size_t configured = 0;
-    if (smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(xpbd_step_group_kernel<G, kCompact, kLean, kWarm>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = smem;
-    }
+    cudaError_t e = nb_raise_dynamic_smem((const void*)xpbd_step_group_kernel<G, kCompact, kLean, kWarm>, smem);
+    if (e != cudaSuccess) return e;
     const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
     xpbd_step_group_kernel<G, kCompact, kLean, kWarm><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts,
                                                                                  dt);

@@ -10,6 +10,20 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and libnewton_b200.so")
+    config.addinivalue_line("markers", "product_build: runs on the product build (FMA contraction) of the library "
+                                       "and compares at a stated tolerance; every other test runs on the parity "
+                                       "build, which agrees with the oracle bit for bit")
+
+
+@pytest.fixture(autouse=True)
+def _library_build(request):
+    """Bit-exact comparisons with the oracle use the parity build (--fmad=false); tests marked
+    product_build check the product build at tolerance."""
+    from newton_custom_contact_b200 import _lib
+
+    prev = _lib.use_build("product" if request.node.get_closest_marker("product_build") else "exact")
+    yield
+    _lib.use_build(prev)
 
 
 @pytest.fixture(scope="session")

@@ -12,11 +12,13 @@ from newton_custom_contact_b200 import _abi, _lib
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-@pytest.fixture(scope="module")
-def lib():
-    if not os.path.exists(_lib.LIB_PATH):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "newton_custom_contact_b200", "csrc")], check=True)
-    return _lib.load()
+@pytest.fixture(scope="module", params=sorted(_lib.BUILDS))
+def lib(request):
+    """Both builds of the library (product and parity) export the same ABI."""
+    if not all(os.path.exists(p) for p in _lib.BUILDS.values()):
+        subprocess.run(["make", "-s", "-j", "8", "-C", os.path.join(ROOT, "newton_custom_contact_b200", "csrc")],
+                       check=True)
+    return _lib.load(_lib.BUILDS[request.param])
 
 
 def declared_functions():

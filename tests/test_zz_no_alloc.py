@@ -60,13 +60,17 @@ def test_static_publish_matches_publish(cuda):
     stream = C.c_void_p(_lib.stream_handle(model.device))
     got_c = pipe.contacts()
     seg = pipe.seg_struct(got_c)
+    sentinel = torch.full_like(got_c._world_offset, -5)
     for call in range(2):
         _poison(got_c)
         assert lib.nb_collide(C.byref(desc), C.c_void_p(ptr(state.body_q)), C.byref(seg), 0, stream) == 0
         pub = pipe.public_struct(got_c)
-        pub.world_offset = None  # the static entry point needs no scan buffer
+        # the static entry point needs no scan buffer: the first call passes none, the second a
+        # sentinel buffer that must come back untouched
+        pub.world_offset = None if call == 0 else ptr(sentinel)
         assert lib.nb_publish_contacts_static(C.byref(desc), C.byref(seg), C.byref(pub), stream) == 0
         got = _snapshot(pipe, got_c)
+        assert bool((sentinel == -5).all().item()), f"call {call}: caller's world_offset was written"
         assert got["count"] == want["count"], f"call {call}"
         for k in _INT + ("world_count", "world_base", "rec"):
             assert np.array_equal(got[k], want[k]), f"call {call}: {k}"
