@@ -533,9 +533,7 @@ def run_ours(args, rank, world_size, local_rank):
         cpu = cpu_baseline(args.seed, args.cpu_sample_seconds, args.worlds)
     # own kernels per substep: broad phase, analytic narrow phase, MPR/GJK
     # prefilter, MPR/GJK narrow phase, world scan, publish, and the XPBD step
-    # (one kernel, or with the flat schedule begin + iterations x (contacts, apply) + end)
-    step_launches = 2 + 2 * iters if sched.mode == "flat" else 1
-    launches_per_frame = substeps * (6 + step_launches)
+    launches_per_frame = substeps * 7
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": args.scaling,

@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 12
+#define NB_ABI_VERSION 13
 
 enum {
     NB_OK = 0,
@@ -65,11 +65,11 @@ enum {
 enum {
     NB_STATUS_CONTACT_OVERFLOW = 1u << 0, /* public contact buffer too small   */
     NB_STATUS_NONFINITE = 1u << 1,        /* NaN/Inf body state after a step   */
-    NB_STATUS_FIXED_OVERFLOW = 1u << 2,   /* delta accumulator saturated       */
+    NB_STATUS_FIXED_OVERFLOW = 1u << 2,   /* reserved (no longer produced)     */
     NB_STATUS_QUEUE_TIMEOUT = 1u << 3,    /* work-queue wait hit its bound     */
     NB_STATUS_WORLD_TOO_LARGE = 1u << 4,  /* world exceeds shared staging      */
     NB_STATUS_ADJOINT_UNSUPPORTED = 1u << 5, /* adjoint skipped a world with an enabled non-free joint */
-    NB_STATUS_MODE_UNSUPPORTED = 1u << 6  /* flat step mode met a world with an enabled non-free joint */
+    NB_STATUS_MODE_UNSUPPORTED = 1u << 6  /* reserved (no longer produced)     */
 };
 
 /* Geometry types (newton/_src/geometry/types.py:46-77). */
@@ -159,15 +159,11 @@ typedef struct NbModelDesc {
     int32_t smem_floats_per_batch;     /* shared-memory arena of one CTA, in 4-byte words */
     int32_t step_mode;                 /* 0: batches of worlds (group_threads per world, batch_* arrays);
                                           1: independent groups of group_threads (32/64/128), full
-                                             body slab (49 words/body);
-                                          2: as 1 with a compact slab (27 words/body, mass
+                                             body slab (43 words/body);
+                                          2: as 1 with a compact slab (21 words/body, mass
                                              properties read from the model); modes 1-2 pull worlds
                                              in world_order, each group owning
-                                             arena * group_threads / cta_threads words;
-                                          3: flat -- body state in NbStepIO.step_scratch, one
-                                             launch per phase over all worlds (models whose
-                                             joints are all free; no restitution, impulses,
-                                             body_parent_f or warm start) */
+                                             arena * group_threads / cta_threads words */
     const int32_t* batch_world;        /* [batch_count, cta_threads/group_threads] world ids, -1 = none */
     const int32_t* batch_slab;         /* [batch_count, cta_threads/group_threads] arena offsets (words) */
 } NbModelDesc;
@@ -330,8 +326,6 @@ typedef struct NbStepIO {
     int32_t ws_capacity;         /* rows of ws_lambda */
     int32_t pad1;
     int32_t* ws_fallback;        /* [1] worlds whose warm start was rejected (counter) or NULL */
-    void* step_scratch;          /* nb_step_scratch_bytes(model) bytes (16-byte aligned) for step_mode 3,
-                                    else unused */
 } NbStepIO;
 
 /* ABI version of the loaded library (NB_ABI_VERSION). */
@@ -340,10 +334,6 @@ int nb_abi_version(void);
 
 /* Number of CTAs the persistent kernels launch on the current device. */
 int32_t nb_default_grid(void);
-
-/* Bytes of NbStepIO.step_scratch nb_xpbd_step needs for this model's step_mode
- * (0 unless step_mode is 3). */
-int64_t nb_step_scratch_size(const NbModelDesc* model);
 
 /*
  * Collision detection for all worlds: shape world transforms + AABBs
@@ -459,7 +449,7 @@ typedef struct NbAdjointIO {
     float* tape_delta;           /* [iterations*B*6] scratch */
     float* tape_weight;          /* [iterations*B] scratch */
     double* grad_acc;            /* [B*13] scratch */
-    int64_t* delta_acc;          /* [B*6] scratch */
+    float* delta_acc;            /* [B*6] scratch */
     int32_t* count_acc;          /* [B] scratch */
     int32_t* active;             /* [iterations * active_capacity * 2] scratch: (record, world) of active contacts */
     int32_t* active_count;       /* [iterations] scratch */

@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 12
+NB_ABI_VERSION = 13
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -239,7 +239,6 @@ class NbStepIO(C.Structure):
         ("ws_capacity", C.c_int32),
         ("pad1", C.c_int32),
         ("ws_fallback", _fp),
-        ("step_scratch", _fp),
     ]
 
 

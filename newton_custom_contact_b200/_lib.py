@@ -58,7 +58,6 @@ EXPORTS = (
     "nb_ws_grads",
     "nb_ws_adam",
     "nb_xpbd_step_adjoint",
-    "nb_step_scratch_size",
     "nb_xpbd_substeps",
 )
 
@@ -155,8 +154,6 @@ def load(path: str | None = None) -> C.CDLL:
     lib.nb_xpbd_substeps.argtypes = [C.POINTER(NbModelDesc), C.POINTER(NbXpbdParams), C.POINTER(NbStepIO),
                                      C.POINTER(NbContactSeg), C.POINTER(NbContactsPublic), C.c_float, C.c_int32,
                                      C.c_int32, C.c_void_p]
-    lib.nb_step_scratch_size.restype = C.c_int64
-    lib.nb_step_scratch_size.argtypes = [C.POINTER(NbModelDesc)]
     lib.nb_xpbd_step_adjoint.restype = C.c_int
     lib.nb_xpbd_step_adjoint.argtypes = [C.POINTER(NbModelDesc), C.POINTER(NbXpbdParams), C.POINTER(NbAdjointIO),
                                          C.POINTER(NbContactSeg), C.c_float, C.c_void_p]

@@ -56,7 +56,7 @@ class SubstepAdjoint:
                 "tape_delta": torch.empty(max(K, 1) * B * 6, **f),
                 "tape_weight": torch.empty(max(K, 1) * B, **f),
                 "grad_acc": torch.empty(B * 13, dtype=torch.float64, device=dev),
-                "delta_acc": torch.empty(B * 6, dtype=torch.int64, device=dev),
+                "delta_acc": torch.empty(B * 6, dtype=torch.float32, device=dev),
                 "count_acc": torch.empty(B, dtype=torch.int32, device=dev),
                 # active contacts per iteration: (record, world), at most every published contact
                 "active": torch.empty(max(K, 1) * max(active_capacity, 1) * 2, dtype=torch.int32, device=dev),
@@ -170,7 +170,7 @@ class Rollout:
         st = self.adjoint.status()
         if st:
             raise RuntimeError(f"adjoint status bits 0x{st:x} (a world with an enabled non-free joint, or "
-                               "fixed-point saturation)")
+                               "active-contact overflow)")
         return gq, gqd, gf_total
 
 

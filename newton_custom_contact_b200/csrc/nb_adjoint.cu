@@ -9,8 +9,8 @@
 //                  S_it+1(i) = A(S_it(i), D_it(i), w_it(i))     (apply_body_delta, weight 1/count)
 //
 // The forward pass (adjoint_forward_kernel, one CTA per world) re-runs the
-// substep in FP32 with the solver's formulas and exact fixed-point delta sums
-// and records S_0..S_K, D_it, w_it and each iteration's active contacts (a
+// substep in FP32 with the solver's formulas and its ordered float delta sums
+// (nb_ordered.cuh) and records S_0..S_K, D_it, w_it and each iteration's active contacts (a
 // tape in global scratch).  The reverse pass walks the iterations backwards
 // with two flat kernels per iteration over all worlds at once:
 // adjoint_bodies_kernel (per body, the vector-Jacobian product of the body
@@ -32,6 +32,7 @@
 
 #include "nb_kernels.cuh"
 #include "nb_math.cuh"
+#include "nb_ordered.cuh"
 
 namespace {
 
@@ -753,6 +754,7 @@ __global__ void __launch_bounds__(kThreads) adjoint_forward_kernel(NbModelDesc m
     const bool model_joints = m.joint_count > 0;
     // enabled non-free joints are not differentiated
     __shared__ int s_flag;
+    __shared__ nb::OrderedBatch<kThreads> s_batch;
     if (t == 0) s_flag = 0;
     __syncthreads();
     for (int j = m.world_joint_start[w] + t; j < m.world_joint_start[w + 1]; j += kThreads)
@@ -778,7 +780,6 @@ __global__ void __launch_bounds__(kThreads) adjoint_forward_kernel(NbModelDesc m
     }
     const int nc = has_contacts ? seg.world_count[w] : 0;
     const float4* R = has_contacts ? reinterpret_cast<const float4*>(seg.rec) + (size_t)seg.world_base[w] * 5 : nullptr;
-    unsigned bad = 0u;
 
     // ---- forward: integrate, then K iterations, recording the tape
     for (int i = t; i < nb; i += kThreads) {
@@ -807,22 +808,35 @@ __global__ void __launch_bounds__(kThreads) adjoint_forward_kernel(NbModelDesc m
         float* S_next = io.tape_state + (size_t)(it + 1) * B * 13;
         for (int i = t; i < nb; i += kThreads) {
 #pragma unroll
-            for (int k = 0; k < 6; ++k) io.delta_acc[6 * (size_t)(b0 + i) + k] = 0ll;
+            for (int k = 0; k < 6; ++k) io.delta_acc[6 * (size_t)(b0 + i) + k] = 0.0f;
             io.count_acc[b0 + i] = 0;
         }
         __syncthreads();
-        for (int k = t; k < nc; k += kThreads) {
+        // the solver's contact pass: each body's delta is the float sum of its active contacts'
+        // deltas in record order (nb_ordered.cuh), as in nb_xpbd_step
+        auto test = [&](int k, int& ends) -> bool {
             const float4* r = R + (size_t)k * 5;
-            if (__float_as_int(r[3].w) == __float_as_int(r[4].w)) continue;
+            if (__float_as_int(r[3].w) == __float_as_int(r[4].w)) return false;
             const ContactC c = load_contact(m, r, b0, S_it);
-            if (c.la == c.lb) continue;
+            if (c.la == c.lb) return false;
             float sa[13], sb[13];
             side_state(S_it, b0, c.la, sa);
             side_state(S_it, b0, c.lb, sb);
             V3T<float> la, aa, lb, ab;
             if (!contact_g(c, body_from<float>(sa), body_from<float>(sb), p.rigid_contact_relaxation, dt, la, aa, lb,
                            ab))
-                continue;
+                return false;
+            ends = nb::ends_pack(c.la, c.lb);
+            return true;
+        };
+        auto solve = [&](int k, float* d12) {
+            const float4* r = R + (size_t)k * 5;
+            const ContactC c = load_contact(m, r, b0, S_it);
+            float sa[13], sb[13];
+            side_state(S_it, b0, c.la, sa);
+            side_state(S_it, b0, c.lb, sb);
+            V3T<float> la, aa, lb, ab;
+            contact_g(c, body_from<float>(sa), body_from<float>(sb), p.rigid_contact_relaxation, dt, la, aa, lb, ab);
             // the reverse pass differentiates this iteration's active contacts only
             const int slot = atomicAdd(io.active_count + it, 1);
             if (slot < io.active_capacity) {
@@ -831,29 +845,22 @@ __global__ void __launch_bounds__(kThreads) adjoint_forward_kernel(NbModelDesc m
             } else {
                 atomicOr(io.status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
             }
-            const float da[6] = {la.x, la.y, la.z, aa.x, aa.y, aa.z};
-            const float db[6] = {lb.x, lb.y, lb.z, ab.x, ab.y, ab.z};
-            if (c.la >= 0) {
+            d12[0] = la.x; d12[1] = la.y; d12[2] = la.z; d12[3] = aa.x; d12[4] = aa.y; d12[5] = aa.z;
+            d12[6] = lb.x; d12[7] = lb.y; d12[8] = lb.z; d12[9] = ab.x; d12[10] = ab.y; d12[11] = ab.z;
+        };
+        auto add = [&](int i, int, const float* d6) {
+            float* acc = io.delta_acc + 6 * (size_t)(b0 + i);
 #pragma unroll
-                for (int q = 0; q < 6; ++q)
-                    atomicAdd(reinterpret_cast<unsigned long long*>(io.delta_acc + 6 * (size_t)(b0 + c.la) + q),
-                              (unsigned long long)fx_quant(da[q], &bad));
-                if (weighting) atomicAdd(io.count_acc + b0 + c.la, 1);
-            }
-            if (c.lb >= 0) {
-#pragma unroll
-                for (int q = 0; q < 6; ++q)
-                    atomicAdd(reinterpret_cast<unsigned long long*>(io.delta_acc + 6 * (size_t)(b0 + c.lb) + q),
-                              (unsigned long long)fx_quant(db[q], &bad));
-                if (weighting) atomicAdd(io.count_acc + b0 + c.lb, 1);
-            }
-        }
+            for (int q = 0; q < 6; ++q) acc[q] = acc[q] + d6[q];
+            if (weighting) io.count_acc[b0 + i] += 1;
+        };
+        nb::ordered_pass<kThreads, kThreads>(s_batch, nc, 0, t, test, solve, add);
         __syncthreads();
         for (int i = t; i < nb; i += kThreads) {
             const int bi = b0 + i;
             float dl[6];
 #pragma unroll
-            for (int k = 0; k < 6; ++k) dl[k] = fx_float(io.delta_acc[6 * (size_t)bi + k]);
+            for (int k = 0; k < 6; ++k) dl[k] = io.delta_acc[6 * (size_t)bi + k];
             const int cnt = io.count_acc[bi];
             const float weight = (weighting && cnt > 0) ? 1.0f / (float)cnt : 1.0f;
             float* D = io.tape_delta + ((size_t)it * B + bi) * 6;
@@ -881,7 +888,6 @@ __global__ void __launch_bounds__(kThreads) adjoint_forward_kernel(NbModelDesc m
         }
     }
 
-    if (bad && t == 0) atomicOr(io.status, (unsigned)NB_STATUS_FIXED_OVERFLOW);
 }
 
 // ---- reverse: flat kernels over all bodies / all active contacts of one iteration

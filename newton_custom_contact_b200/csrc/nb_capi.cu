@@ -62,7 +62,6 @@ int check_schedule(const NbModelDesc* m) {
         if ((int64_t)m->max_world_bodies * nb_step_slab_words(m->step_mode == 2) > share) return NB_ERR_INVALID;
         return NB_OK;
     }
-    if (m->step_mode == 3) return NB_OK;  // flat: no shared-memory arena
     if (m->step_mode != 0) return NB_ERR_INVALID;
     const int g = m->group_threads;
     if (g != 32 && g != 64 && g != 128 && g != 256) return NB_ERR_INVALID;
@@ -124,11 +123,6 @@ int nb_collide(const NbModelDesc* model, const float* body_q, const NbContactSeg
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }
 
-int64_t nb_step_scratch_size(const NbModelDesc* model) {
-    if (!model) return 0;
-    return (int64_t)nb_step_scratch_bytes(model);
-}
-
 int nb_publish_contacts(const NbModelDesc* model, const NbContactSeg* seg, const NbContactsPublic* pub,
                         void* stream) {
     int rc = check_model(model);
@@ -169,14 +163,7 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
         return NB_ERR_INVALID;
     if ((rc = check_schedule(model))) return rc;
     if (seg->rec && (rc = check_step_seg(seg))) return rc;
-    if (model->step_mode == 3) {
-        // flat mode: the plain solve of free bodies only
-        if (!io->step_scratch || (reinterpret_cast<uintptr_t>(io->step_scratch) & 15u)) return NB_ERR_INVALID;
-        if (params->enable_restitution || io->contact_impulse || io->body_parent_f || io->ws_lambda)
-            return NB_ERR_UNSUPPORTED;
-    } else if ((int64_t)nb_step_smem_bytes(model) > smem_limit()) {
-        return NB_ERR_UNSUPPORTED;
-    }
+    if ((int64_t)nb_step_smem_bytes(model) > smem_limit()) return NB_ERR_UNSUPPORTED;
     cudaError_t e = nb_launch_step(model, params, io, seg, dt, grid_for(grid_ctas), (cudaStream_t)stream);
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }

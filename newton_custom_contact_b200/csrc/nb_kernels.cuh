@@ -22,7 +22,6 @@ cudaError_t nb_launch_step(const NbModelDesc* m, const NbXpbdParams* p, const Nb
 cudaError_t nb_launch_contact_forces(const float* imp, const int32_t* count, int cap, float dt, float* force,
                                      cudaStream_t stream);
 int nb_step_slab_words(int compact);
-size_t nb_step_scratch_bytes(const NbModelDesc* m);
 cudaError_t nb_launch_match(const NbModelDesc* m, const float* body_q, const NbContactsPublic* pub,
                             const NbContactSeg* seg, const NbMatchState* st, cudaStream_t stream);
 cudaError_t nb_launch_ws_features(const NbModelDesc* m, const float* q, const float* qd,

@@ -8,29 +8,40 @@
 // constraint-projection passes never touch HBM for body state (the reference
 // re-reads body arrays in ~7 launches per iteration,
 // newton/_src/solvers/xpbd/solver_xpbd.py:371-630).  Per iteration:
-//   contacts: the group's threads test the world's dense contact records,
-//             compact the penetrating ones and solve those
+//   contacts: the group tests the world's dense contact records in order,
+//             compacts the penetrating ones in order and solves them
 //             (solve_body_contact_positions, newton/_src/solvers/xpbd/kernels.py:2062-2298);
-//             per-body deltas and contact counts are summed with shared-memory
-//             int64 fixed-point atomics -- exact, so the result does not depend
-//             on thread or contact order;
+//             each body's delta is the float sum of its contacts' deltas in
+//             contact order (nb_ordered.cuh) -- the reference's sum run
+//             sequentially, deterministic on the GPU;
 //   bodies:   weighted apply_body_deltas (kernels.py:809-878), then the joint
-//             pass (solve_body_joints, kernels.py:1441-1942) and the unweighted
-//             apply of solver_xpbd.py:590-630.
+//             pass (solve_body_joints, kernels.py:1441-1942, summed in joint
+//             order the same way) and the unweighted apply of
+//             solver_xpbd.py:590-630.
 // Group barriers are __syncwarp (G = 32), named barriers (G = 64, 128) or
 // __syncthreads (G = 256).
 #include <cuda_runtime.h>
 
 #include "nb_kernels.cuh"
 #include "nb_math.cuh"
+#include "nb_ordered.cuh"
 
 namespace {
 
 constexpr int kST = NB_STEP_THREADS;  // threads per CTA
 
+// entries of one ordered batch per group: at least one test round of G items,
+// sized so that 8 warp groups' batches (21.5 KB) leave room for two CTAs' arenas per SM
+template <int G>
+struct BatchCap {
+    static constexpr int value = G == 32 ? 48 : (G == 256 ? 256 : 128);
+};
+template <int G>
+using Batch = nb::OrderedBatch<BatchCap<G>::value>;
+
 // Per-world body state in shared memory.  kCompact = false: everything the
-// substep touches is staged (49 words per body); kCompact = true: only the
-// mutable part (pose, twist, delta accumulators, flags, contact count: 27
+// substep touches is staged (43 words per body); kCompact = true: only the
+// mutable part (pose, twist, delta accumulators, flags, contact count: 21
 // words per body) is staged and the static mass properties are read from the
 // model (read-only path), so worlds of up to 128 bodies fit one warp's share
 // of the arena.
@@ -49,8 +60,8 @@ struct SBodiesT {
     const float* g_iI;
     float* frc;                // [6][nb]  body_f + joint forces (aliases acc before integration)
     int* flags;                // [nb]
-    unsigned long long* acc;   // [6][nb]
-    int* cnt;                  // [nb]
+    float* acc;                // [6][nb]  delta accumulators (linear 3, angular 3)
+    int* cnt;                  // [nb]     active contacts of the iteration
 
     __device__ TF q(int i) const {
         return TF{V3{f[0 * nb + i], f[1 * nb + i], f[2 * nb + i]},
@@ -102,47 +113,41 @@ struct SBodiesT {
         }
         return r;
     }
-    __device__ void add_delta(int i, V3 lin, V3 ang, unsigned* bad) {
-        acc_add(i, 0, fx_quant(lin.x, bad));
-        acc_add(i, 1, fx_quant(lin.y, bad));
-        acc_add(i, 2, fx_quant(lin.z, bad));
-        acc_add(i, 3, fx_quant(ang.x, bad));
-        acc_add(i, 4, fx_quant(ang.y, bad));
-        acc_add(i, 5, fx_quant(ang.z, bad));
+    // the reference's atomic_add(deltas, i, spatial_vector(lin, ang)): old + value, per component
+    // (only body i's owner thread of the ordered pass calls this)
+    __device__ __forceinline__ void add(int i, const float* d6) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) acc[k * nb + i] = acc[k * nb + i] + d6[k];
     }
-    __device__ void acc_add(int i, int k, long long v) {
-        if (v != 0) atomicAdd(&acc[k * nb + i], (unsigned long long)v);
-    }
-    // read and clear the accumulated delta of body i; false when it is all zero
+    // read and clear the accumulated delta of body i; false when nothing was added
     __device__ bool take(int i, V3& lin, V3& ang) {
-        long long v[6];
-        unsigned long long any = 0ull;
+        float v[6];
+        unsigned any = 0u;
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            v[k] = (long long)acc[k * nb + i];
-            any |= (unsigned long long)v[k];
-            acc[k * nb + i] = 0ull;
+            v[k] = acc[k * nb + i];
+            any |= __float_as_uint(v[k]);
+            acc[k * nb + i] = 0.0f;
         }
-        lin = V3{fx_float(v[0]), fx_float(v[1]), fx_float(v[2])};
-        ang = V3{fx_float(v[3]), fx_float(v[4]), fx_float(v[5])};
-        return any != 0ull;
+        lin = V3{v[0], v[1], v[2]};
+        ang = V3{v[3], v[4], v[5]};
+        return any != 0u;
     }
 };
 
-// 4-byte words of one world's slab: acc (12 words/body, 8-byte aligned first),
-// f 13, [c 4, I 9, iI 9,] flags 1, cnt 1
+// 4-byte words of one world's slab: acc 6, f 13, [c 4, I 9, iI 9,] flags 1, cnt 1
 template <bool kCompact>
-__host__ __device__ constexpr int slab_words_per_body() { return kCompact ? 12 + 13 + 1 + 1 : 12 + 13 + 4 + 9 + 9 + 1 + 1; }
+__host__ __device__ constexpr int slab_words_per_body() { return kCompact ? 6 + 13 + 1 + 1 : 6 + 13 + 4 + 9 + 9 + 1 + 1; }
 
 template <bool kCompact>
 __device__ SBodiesT<kCompact> sbodies_carve(unsigned char* slab, const NbModelDesc& m, int b0, int nb) {
     SBodiesT<kCompact> s;
     s.nb = nb;
     s.b0 = b0;
-    unsigned long long* a = reinterpret_cast<unsigned long long*>(slab);
+    float* a = reinterpret_cast<float*>(slab);
     s.acc = a;
-    s.frc = reinterpret_cast<float*>(a);  // used only before integration
-    float* fl = reinterpret_cast<float*>(a + 6 * (size_t)nb);
+    s.frc = a;  // used only before integration
+    float* fl = a + 6 * (size_t)nb;
     s.f = fl;
     s.g_com = m.body_com;
     s.g_inv_m = m.body_inv_mass;
@@ -223,21 +228,6 @@ __device__ void apply_body_delta(TF& q, V3& v, V3& w, V3 dlin, V3 dang, float we
     w = w1;
 }
 
-// apply_body_delta with an all-zero delta in closed form.  With dlin = dang = 0
-// every intermediate of the general path (dp, dwb, tb, dw1) is a signed zero,
-// so q1 = normalize(q0), p1 = (p0 + R(q0) com) - R(q1) com, and v, w only
-// pass the |x| < 1e-4 test; results equal the general path's up to the sign
-// of zero components.
-__device__ __forceinline__ void apply_zero_delta(TF& q, V3& v, V3& w, V3 com, float inv_m) {
-    if (inv_m == 0.0f) return;
-    const Q4 q0 = q.q;
-    const Q4 q1 = qnormalize(q0);
-    const V3 x_com = add(q.p, qrot(q0, com));
-    q = TF{sub(x_com, qrot(q1, com)), q1};
-    if (length(v) < 1e-4f) v = V3{0.0f, 0.0f, 0.0f};
-    if (length(w) < 1e-4f) w = V3{0.0f, 0.0f, 0.0f};
-}
-
 // kernels.py:1945-1979
 __device__ float contact_constraint_delta(float err, Q4 qa, Q4 qb, float m_inv_a, float m_inv_b, const M33& Ia,
                                           const M33& Ib, V3 la, V3 lb, V3 aa, V3 ab, float relaxation, float dt) {
@@ -299,33 +289,36 @@ __device__ __forceinline__ float contact_depth(const SB& S, float4 r0, float4 r1
     return dot(V3{r2.x, r2.y, r2.z}, sub(bx_b, bx_a)) - thickness;
 }
 
-// true when solve_contact would move a body (NaN depths count, so they
-// propagate exactly as in the reference)
+// true when the reference's solve_body_contact_positions adds deltas for this
+// record: distinct bodies (equal shapes imply equal bodies) and depth < 0 (NaN
+// depths count, so they propagate exactly as in the reference); ends receives
+// the two world-local bodies for the ordered accumulation
 template <class SB>
-__device__ __forceinline__ bool contact_active(const SB& S, float4 r0, float4 r1, float4 r2) {
+__device__ __forceinline__ bool contact_active(const SB& S, float4 r0, float4 r1, float4 r2, int& ends) {
     const int tag = __float_as_int(r2.w);
     const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
     if (la == lb) return false;
     TF Xa, Xb;
     V3 bx_a, bx_b;
+    ends = nb::ends_pack(la, lb);
     return !(contact_depth(S, r0, r1, r2, la, lb, Xa, Xb, bx_a, bx_b) >= 0.0f);
 }
 
-// solve_body_contact_positions for one contact (kernels.py:2062-2298)
-// imp (optional) receives the A-side spatial delta (the contact_impulse_iter
-// entry of the reference) of an active contact.
+// solve_body_contact_positions for one active contact (kernels.py:2062-2298):
+// d12 receives the deltas the reference adds to body A (linear, angular) and
+// body B; imp (optional) the A-side spatial delta (the contact_impulse_iter
+// entry of the reference).  The caller has established that the contact is
+// active (contact_active: distinct bodies, depth < 0 or NaN; equal shapes
+// imply equal bodies).
 template <class SB>
-__device__ void solve_contact(const NbModelDesc& m, SB& S, float4 r0, float4 r1, float4 r2, float4 r3, float4 r4,
-                              float relaxation, float dt, bool weighting, unsigned* bad, float* imp) {
+__device__ void solve_contact(const NbModelDesc& m, const SB& S, float4 r0, float4 r1, float4 r2, float4 r3,
+                              float4 r4, float relaxation, float dt, float* d12, float* imp) {
     const int sa = __float_as_int(r3.w), sb = __float_as_int(r4.w);
-    if (sa == sb) return;
     const int tag = __float_as_int(r2.w);
     const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
-    if (la == lb) return;
     TF Xa, Xb;
     V3 bx_a, bx_b;
     const float d = contact_depth(S, r0, r1, r2, la, lb, Xa, Xb, bx_a, bx_b);
-    if (d >= 0.0f) return;
     const V3 n{r2.x, r2.y, r2.z};
     float m_inv_a = 0.0f, m_inv_b = 0.0f;
     M33 Ia = zero_m33(), Ib = zero_m33();
@@ -343,10 +336,6 @@ __device__ void solve_contact(const NbModelDesc& m, SB& S, float4 r0, float4 r1,
     V3 r_b = sub(bx_b, tf_point(Xb, com_b));
     V3 ang_a = neg(cross(r_a, n));
     V3 ang_b = cross(r_b, n);
-    if (weighting) {
-        if (la >= 0) atomicAdd(&S.cnt[la], 1);
-        if (lb >= 0) atomicAdd(&S.cnt[lb], 1);
-    }
     float lambda_n = contact_constraint_delta(d, Xa.q, Xb.q, m_inv_a, m_inv_b, Ia, Ib, neg(n), n, ang_a, ang_b,
                                               relaxation, dt);
     V3 lin_da = mul(neg(n), lambda_n);
@@ -409,8 +398,10 @@ __device__ void solve_contact(const NbModelDesc& m, SB& S, float4 r0, float4 r1,
             ang_db = add(ang_db, mul(rn, lr));
         }
     }
-    if (la >= 0) S.add_delta(la, lin_da, ang_da, bad);
-    if (lb >= 0) S.add_delta(lb, lin_db, ang_db, bad);
+    d12[0] = lin_da.x; d12[1] = lin_da.y; d12[2] = lin_da.z;
+    d12[3] = ang_da.x; d12[4] = ang_da.y; d12[5] = ang_da.z;
+    d12[6] = lin_db.x; d12[7] = lin_db.y; d12[8] = lin_db.z;
+    d12[9] = ang_db.x; d12[10] = ang_db.y; d12[11] = ang_db.z;
     if (imp) {
         imp[0] = lin_da.x; imp[1] = lin_da.y; imp[2] = lin_da.z;
         imp[3] = ang_da.x; imp[4] = ang_da.y; imp[5] = ang_da.z;
@@ -422,14 +413,16 @@ __device__ __forceinline__ V3 velocity_at(V3 v, V3 w, V3 r) { return add(cross(w
 
 // apply_rigid_restitution (kernels.py:2471-2620) for one solver record:
 // pre-step poses / twists from the step's inputs, current twists from the
-// slab; velocity deltas go to the fixed-point accumulators.
+// slab.  Returns whether the reference adds velocity deltas for the record;
+// if so, d12 receives them (body A linear, angular; body B linear, angular)
+// and ends the two bodies.
 template <class SB>
-__device__ __noinline__ void restitution_contact(const NbModelDesc& m, SB& S, const float4* r, int b0,
+__device__ __noinline__ bool restitution_contact(const NbModelDesc& m, const SB& S, const float4* r, int b0,
                                                  const float* __restrict__ q_prev, const float* __restrict__ qd_prev,
-                                                 float dt, unsigned* bad) {
+                                                 float dt, float* d12, int& ends) {
     const float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3], r4 = r[4];
     const int sa = __float_as_int(r3.w), sb = __float_as_int(r4.w);
-    if (sa == sb) return;
+    if (sa == sb) return false;
     int nz = 0;
     float rest = 0.0f;
     if (sa >= 0) { nz += 1; rest += __ldg(m.shape_restitution + sa); }
@@ -437,7 +430,7 @@ __device__ __noinline__ void restitution_contact(const NbModelDesc& m, SB& S, co
     if (nz > 0) rest /= (float)nz;
     const int tag = __float_as_int(r2.w);
     const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
-    if (la == lb) return;
+    if (la == lb) return false;
     float m_inv_a = 0.0f, m_inv_b = 0.0f;
     M33 Ia = zero_m33(), Ib = zero_m33();
     TF Xa = tf_identity(), Xb = tf_identity();
@@ -451,7 +444,7 @@ __device__ __noinline__ void restitution_contact(const NbModelDesc& m, SB& S, co
     V3 bx_b = tf_point(Xb, add(V3{r1.x, r1.y, r1.z}, V3{r4.x, r4.y, r4.z}));
     const float thickness = r0.w + r1.w;
     const float d = dot(n, sub(bx_b, bx_a)) - thickness;
-    if (d >= 0.0f) return;
+    if (d >= 0.0f) return false;
     V3 r_a = sub(bx_a, tf_point(Xa, com_a));
     V3 r_b = sub(bx_b, tf_point(Xb, com_b));
     V3 rxn_a{0, 0, 0}, rxn_b{0, 0, 0};
@@ -473,19 +466,26 @@ __device__ __noinline__ void restitution_contact(const NbModelDesc& m, SB& S, co
         rxn_b = qrot_inv(Xb.q, cross(r_b, n));
         inv_mass += m_inv_b + dot(rxn_b, mv(Ib, rxn_b));
     }
-    if (inv_mass == 0.0f) return;
+    if (inv_mass == 0.0f) return false;
     const float rel_old = dot(n, sub(v_b, v_a));
     const float rel_new = dot(n, sub(v_b_new, v_a_new));
-    if (rel_old >= 0.0f) return;
+    if (rel_old >= 0.0f) return false;
     const float dv = (-rel_new - rest * rel_old) / inv_mass;
+    V3 la_v{0, 0, 0}, aa_v{0, 0, 0}, lb_v{0, 0, 0}, ab_v{0, 0, 0};
     if (la >= 0) {
         const float dva = -dv;
-        S.add_delta(la, mul(mul(n, m_inv_a), dva), qrot(Xa.q, mul(mv(Ia, rxn_a), dva)), bad);
+        la_v = mul(mul(n, m_inv_a), dva);
+        aa_v = qrot(Xa.q, mul(mv(Ia, rxn_a), dva));
     }
     if (lb >= 0) {
         const float dvb = dv;
-        S.add_delta(lb, mul(mul(n, m_inv_b), dvb), qrot(Xb.q, mul(mv(Ib, rxn_b), dvb)), bad);
+        lb_v = mul(mul(n, m_inv_b), dvb);
+        ab_v = qrot(Xb.q, mul(mv(Ib, rxn_b), dvb));
     }
+    d12[0] = la_v.x; d12[1] = la_v.y; d12[2] = la_v.z; d12[3] = aa_v.x; d12[4] = aa_v.y; d12[5] = aa_v.z;
+    d12[6] = lb_v.x; d12[7] = lb_v.y; d12[8] = lb_v.z; d12[9] = ab_v.x; d12[10] = ab_v.y; d12[11] = ab_v.z;
+    ends = nb::ends_pack(la, lb);
+    return true;
 }
 
 // accumulate_weighted_contact_impulse (kernels.py:2301-2360) for the world's
@@ -567,16 +567,32 @@ __device__ void joint_axes(const NbModelDesc& m, int start, int count, const flo
         if (comp(damp, i) > 0.0f) set_comp(tv, i, comp(tv, i) / comp(damp, i));
 }
 
-// solve_body_joints for one joint (kernels.py:1441-1942)
-// imp (optional) accumulates the child-side spatial delta (joint_impulse,
+// Whether the reference's solve_body_joints adds deltas for joint j
+// (kernels.py:1441-1942: enabled, not FREE, some body moves); ends receives
+// the parent (side A) and child (side B) bodies.
+template <class SB>
+__device__ __forceinline__ bool joint_active(const NbModelDesc& m, const SB& S, int b0, int j, int& ends) {
+    if (!m.joint_enabled[j] || m.joint_type[j] == NB_JOINT_FREE) return false;
+    const int id_c = m.joint_child[j], id_p = m.joint_parent[j];
+    const int lc = id_c - b0, lp = id_p < 0 ? -1 : id_p - b0;
+    if ((id_p < 0 || S.inv_m(lp) == 0.0f) && S.inv_m(lc) == 0.0f) return false;
+    ends = nb::ends_pack(lp, lc);
+    return true;
+}
+
+// solve_body_joints for one active joint (kernels.py:1441-1942): d12
+// receives the parent's delta (linear, angular) and the child's.  imp
+// (optional) accumulates the child-side spatial delta (joint_impulse,
 // kernels.py:1941-1942); only this thread touches joint j's row.
 template <class SB>
-__device__ __noinline__ void solve_joint(const NbModelDesc& m, SB& S, int b0, int j, const float* tpos,
-                                         const float* tvel, const NbXpbdParams& p, float dt, unsigned* bad,
+__device__ __noinline__ void solve_joint(const NbModelDesc& m, const SB& S, int b0, int j, const float* tpos,
+                                         const float* tvel, const NbXpbdParams& p, float dt, float* d12,
                                          float* imp) {
+    // a joint that returns before its deltas contributes zeros: adding +0 leaves every accumulator
+    // unchanged (an accumulator that starts at +0 never holds -0)
+#pragma unroll
+    for (int k = 0; k < 12; ++k) d12[k] = 0.0f;
     int type = m.joint_type[j];
-    if (!m.joint_enabled[j]) return;
-    if (type == NB_JOINT_FREE) return;
     int id_c = m.joint_child[j], id_p = m.joint_parent[j];
     int lc = id_c - b0, lp = id_p < 0 ? -1 : id_p - b0;
     TF X_pj = load_tf(m.joint_X_p + 7 * (size_t)j);
@@ -601,7 +617,6 @@ __device__ __noinline__ void solve_joint(const NbModelDesc& m, SB& S, int b0, in
     float m_inv_c = S.inv_m(lc);
     M33 I_inv_c = S.inv_inertia(lc);
     V3 vel_c = S.v(lc), om_c = S.w(lc);
-    if (m_inv_p == 0.0f && m_inv_c == 0.0f) return;
     V3 ldp{0, 0, 0}, adp{0, 0, 0}, ldc{0, 0, 0}, adc{0, 0, 0};
     TF rel = tf_mul(tf_inverse(X_wp), X_wc);
     V3 rel_p = rel.p;
@@ -744,8 +759,8 @@ __device__ __noinline__ void solve_joint(const NbModelDesc& m, SB& S, int b0, in
             adc = add(adc, mul(ang_c, dl));
         }
     }
-    if (id_p >= 0) S.add_delta(lp, ldp, adp, bad);
-    if (id_c >= 0) S.add_delta(lc, ldc, adc, bad);
+    d12[0] = ldp.x; d12[1] = ldp.y; d12[2] = ldp.z; d12[3] = adp.x; d12[4] = adp.y; d12[5] = adp.z;
+    d12[6] = ldc.x; d12[7] = ldc.y; d12[8] = ldc.z; d12[9] = adc.x; d12[10] = adc.y; d12[11] = adc.z;
     if (imp) {
         float* r = imp + 6 * (size_t)j;
         r[0] = r[0] + ldc.x; r[1] = r[1] + ldc.y; r[2] = r[2] + ldc.z;
@@ -803,39 +818,31 @@ __device__ void joint_forces(const NbModelDesc& m, SB& S, int b0, int j0, int j1
     }
 }
 
-// contacts examined per compaction round of the contact pass
-constexpr int kChunk = 256;
-
-// Contact pass of one iteration for one world.  Few contacts penetrate at any
-// time, so the group first tests a chunk of records (one per thread, 48-byte
-// reads), compacts the penetrating ones into a shared list and then solves the
-// list with every thread busy.  Order does not matter: deltas are summed
-// exactly.  nact[2] alternates between chunks so that resetting one counter
-// never races with the next chunk's appends; both are zero on entry and on
-// return (visible to the group after its next barrier).
+// Contact pass of one iteration for one world (solve_body_contact_positions
+// over the world's records, kernels.py:2062-2298): the group tests the
+// records in order (48-byte reads), solves the penetrating ones in batches
+// with every thread busy, and each body's owner adds its contacts' deltas in
+// record order (nb_ordered.cuh); with weighting, the owner also counts them
+// (the reference's contact_inv_weight).  imp_scratch (optional) receives each
+// active record's A-side delta.
 template <int G, class SB>
 __device__ __forceinline__ void contact_pass(const NbModelDesc& m, SB& S, const float4* __restrict__ R, int nc,
-                                             unsigned char* list, int* nact, int g, int t, float relaxation, float dt,
-                                             bool weighting, unsigned* bad, float* imp_scratch) {
-    int parity = 0;
-    for (int base = 0; base < nc; base += kChunk, parity ^= 1) {
-        const int lim = nc - base < kChunk ? nc - base : kChunk;
-        for (int k = t; k < lim; k += G) {
-            const float4* r = R + (size_t)(base + k) * 5;
-            if (contact_active(S, r[0], r[1], r[2])) list[atomicAdd(&nact[parity], 1)] = (unsigned char)k;
-        }
-        group_sync<G>(g);
-        if (t == 0) nact[parity ^ 1] = 0;
-        const int na = nact[parity];
-        for (int a = t; a < na; a += G) {
-            const int k = base + list[a];
-            const float4* r = R + (size_t)k * 5;
-            solve_contact(m, S, r[0], r[1], r[2], r[3], r[4], relaxation, dt, weighting, bad,
-                          imp_scratch ? imp_scratch + (size_t)k * 6 : nullptr);
-        }
-        group_sync<G>(g);
-    }
-    if (t == 0) nact[0] = nact[1] = 0;
+                                             Batch<G>& B, int g, int t, float relaxation, float dt, bool weighting,
+                                             float* imp_scratch) {
+    auto test = [&](int k, int& ends) -> bool {
+        const float4* r = R + (size_t)k * 5;
+        return contact_active(S, r[0], r[1], r[2], ends);
+    };
+    auto solve = [&](int k, float* d12) {
+        const float4* r = R + (size_t)k * 5;
+        solve_contact(m, S, r[0], r[1], r[2], r[3], r[4], relaxation, dt, d12,
+                      imp_scratch ? imp_scratch + (size_t)k * 6 : nullptr);
+    };
+    auto add = [&](int i, int, const float* d6) {
+        S.add(i, d6);
+        if (weighting) S.cnt[i] += 1;
+    };
+    nb::ordered_pass<G, kST>(B, nc, g, t, test, solve, add);
 }
 
 // world's largest penetration max(-d, 0) over its contacts (group reduction
@@ -867,15 +874,15 @@ __device__ __forceinline__ float world_penetration(const SB& S, const float4* __
 // iterations, every contact's predicted impulse (io.ws_lambda, contact frame
 // n, t1, t2 as built by nb_ws_features) is applied to its two bodies as one
 // combined delta -- linear L on A, -L on B, angular r x L at the contact
-// points -- summed in the same exact fixed point as the solver.  Bodies that
-// receive nothing are left untouched, so an all-zero prediction reproduces
-// the plain step exactly.  The world falls back to no warm start (state
-// restored from a snapshot kept in the step's output rows) when the warm
-// start makes its largest penetration worse.
+// points -- summed per body in record order like the solver's deltas.
+// Bodies that receive nothing are left untouched, so an all-zero prediction
+// reproduces the plain step exactly.  The world falls back to no warm start
+// (state restored from a snapshot kept in the step's output rows) when the
+// warm start makes its largest penetration worse.
 template <int G, class SB>
 __device__ __forceinline__ void warm_start(const NbModelDesc& m, const NbStepIO& io, const NbContactSeg& seg, SB& S,
                                         const float4* __restrict__ R, int nc, int64_t rec_base, int b0, int g,
-                                        int t, int* scratch, float dt, unsigned* bad) {
+                                        int t, int* scratch, Batch<G>& B, float dt) {
     const int nb = S.nb;
     const float pen0 = world_penetration<G>(S, R, nc, g, t, scratch);
     // snapshot pose + twist into this world's output rows (overwritten by the write-back)
@@ -885,34 +892,52 @@ __device__ __forceinline__ void warm_start(const NbModelDesc& m, const NbStepIO&
         for (int k = 0; k < 7; ++k) qo[k] = S.f[k * nb + i];
         for (int k = 0; k < 6; ++k) qdo[k] = S.f[(7 + k) * nb + i];
     }
-    for (int k = t; k < nc; k += G) {
+    auto prediction = [&](int k, float& ln, float& l1, float& l2) -> bool {
         const int64_t pub = seg.rec_index ? (int64_t)seg.rec_index[rec_base + k] : rec_base + k;
-        if (pub < 0 || pub >= io.ws_capacity) continue;
+        if (pub < 0 || pub >= io.ws_capacity) return false;
         const float* lam = io.ws_lambda + 3 * (size_t)pub;
-        const float ln = lam[0], l1 = lam[1], l2 = lam[2];
-        if (ln == 0.0f && l1 == 0.0f && l2 == 0.0f) continue;
-        if (!(isfinite(ln) && isfinite(l1) && isfinite(l2))) continue;  // a non-finite prediction counts as none
+        ln = lam[0];
+        l1 = lam[1];
+        l2 = lam[2];
+        if (ln == 0.0f && l1 == 0.0f && l2 == 0.0f) return false;
+        return isfinite(ln) && isfinite(l1) && isfinite(l2);  // a non-finite prediction counts as none
+    };
+    auto test = [&](int k, int& ends) -> bool {
+        float ln, l1, l2;
+        if (!prediction(k, ln, l1, l2)) return false;
         const float4* r = R + (size_t)k * 5;
         const int tag = __float_as_int(r[2].w);
         const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
-        if (la == lb || __float_as_int(r[3].w) == __float_as_int(r[4].w)) continue;
-        const TF Xa = la >= 0 ? S.q(la) : tf_identity();
-        const TF Xb = lb >= 0 ? S.q(lb) : tf_identity();
+        if (la == lb || __float_as_int(r[3].w) == __float_as_int(r[4].w)) return false;
+        ends = nb::ends_pack(la, lb);
+        return true;
+    };
+    auto solve = [&](int k, float* d12) {
+        float ln, l1, l2;
+        prediction(k, ln, l1, l2);
+        const float4* r = R + (size_t)k * 5;
+        const int tag = __float_as_int(r[2].w);
+        const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
         const V3 nrm{r[2].x, r[2].y, r[2].z};
         const V3 a = fabsf(nrm.x) < 0.9f ? V3{1.0f, 0.0f, 0.0f} : V3{0.0f, 1.0f, 0.0f};
         const V3 t1 = normalize(cross(nrm, a));
         const V3 t2 = cross(nrm, t1);
         const V3 L = add(add(mul(nrm, -ln), mul(t1, l1)), mul(t2, l2));
+        V3 aa{0, 0, 0}, ab{0, 0, 0};
         if (la >= 0) {
-            const V3 ra = sub(tf_point(Xa, V3{r[0].x, r[0].y, r[0].z}), tf_point(Xa, S.com(la)));
-            S.add_delta(la, L, cross(ra, L), bad);
+            const TF Xa = S.q(la);
+            aa = cross(sub(tf_point(Xa, V3{r[0].x, r[0].y, r[0].z}), tf_point(Xa, S.com(la))), L);
         }
+        const V3 Lb = neg(L);
         if (lb >= 0) {
-            const V3 Lb = neg(L);
-            const V3 rb = sub(tf_point(Xb, V3{r[1].x, r[1].y, r[1].z}), tf_point(Xb, S.com(lb)));
-            S.add_delta(lb, Lb, cross(rb, Lb), bad);
+            const TF Xb = S.q(lb);
+            ab = cross(sub(tf_point(Xb, V3{r[1].x, r[1].y, r[1].z}), tf_point(Xb, S.com(lb))), Lb);
         }
-    }
+        d12[0] = L.x; d12[1] = L.y; d12[2] = L.z; d12[3] = aa.x; d12[4] = aa.y; d12[5] = aa.z;
+        d12[6] = Lb.x; d12[7] = Lb.y; d12[8] = Lb.z; d12[9] = ab.x; d12[10] = ab.y; d12[11] = ab.z;
+    };
+    auto add_row = [&](int i, int, const float* d6) { S.add(i, d6); };
+    nb::ordered_pass<G, kST>(B, nc, g, t, test, solve, add_row);
     group_sync<G>(g);
     for (int i = t; i < nb; i += G) {
         V3 dl, da;
@@ -960,7 +985,6 @@ __device__ __forceinline__ void warm_start(const NbModelDesc& m, const NbStepIO&
             o[3] += A.x; o[4] += A.y; o[5] += A.z;
         }
     }
-    if (t == 0) scratch[0] = scratch[1] = 0;  // the contact pass expects its counters at zero
     group_sync<G>(g);
 }
 
@@ -977,7 +1001,7 @@ __device__ __forceinline__ void warm_start(const NbModelDesc& m, const NbStepIO&
 template <int G, bool kLean, bool kWarm, class SB>
 __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdParams& p, const NbStepIO& io,
                                            const NbContactSeg& seg, bool has_contacts, float dt, int w, SB& S,
-                                           int g, int t, int* flag, int* nact, unsigned char* list,
+                                           int g, int t, int* flag, int* pen_slot, Batch<G>& B,
                                            unsigned* s_bad) {
     const bool weighting = p.rigid_contact_con_weighting != 0;
     const bool model_joints = m.joint_count > 0;
@@ -1043,8 +1067,7 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
     }
     group_sync<G>(g);
     for (int i = t; i < nb; i += G)
-        for (int k = 0; k < 6; ++k) S.acc[k * nb + i] = 0ull;
-    if (t == 0) nact[0] = nact[1] = 0;
+        for (int k = 0; k < 6; ++k) S.acc[k * nb + i] = 0.0f;
     group_sync<G>(g);
     const int nc = has_contacts ? seg.world_count[w] : 0;
     const int64_t rec_base = has_contacts ? seg.world_base[w] : 0;
@@ -1052,13 +1075,13 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
     const bool want_imp = !kLean && has_contacts && io.contact_impulse != nullptr;
     unsigned bad = 0u;
     if constexpr (kWarm) {
-        if (has_contacts && io.ws_lambda)
-            warm_start<G>(m, io, seg, S, R, nc, rec_base, b0, g, t, nact, dt, &bad);
+        if (has_contacts && io.ws_lambda) warm_start<G>(m, io, seg, S, R, nc, rec_base, b0, g, t, pen_slot, B, dt);
     }
+    const V3 zero3{0.0f, 0.0f, 0.0f};
     for (int it = 0; it < p.iterations; ++it) {
         if (has_contacts) {
-            contact_pass<G>(m, S, R, nc, list, nact, g, t, p.rigid_contact_relaxation, dt,
-                            weighting, &bad, want_imp ? io.impulse_scratch + (size_t)rec_base * 6 : nullptr);
+            contact_pass<G>(m, S, R, nc, B, g, t, p.rigid_contact_relaxation, dt, weighting,
+                            want_imp ? io.impulse_scratch + (size_t)rec_base * 6 : nullptr);
             if constexpr (!kLean) {
                 if (want_imp) {
                     accumulate_impulses<G>(S, R, nc, rec_base, seg.rec_index, io.impulse_scratch,
@@ -1066,12 +1089,15 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
                     group_sync<G>(g);
                 }
             }
+            // apply_body_deltas over every body (kernels.py:809-878), weighted by the contact count;
+            // in a world whose joints are all free the joint pass that follows adds nothing, so its
+            // apply (again every body, zero delta) is fused here
             for (int i = t; i < nb; i += G) {
                 V3 dl, da;
-                const bool moved = S.take(i, dl, da);
+                S.take(i, dl, da);
                 float weight = 1.0f;
                 if (weighting) {
-                    float iw = (float)S.cnt[i];
+                    const float iw = (float)S.cnt[i];
                     S.cnt[i] = 0;
                     if (iw > 0.0f) weight = 1.0f / iw;
                 }
@@ -1079,29 +1105,25 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
                 V3 v = S.v(i), wv = S.w(i);
                 const V3 com = S.com(i);
                 const float im = S.inv_m(i);
-                if (moved || world_joints) {
-                    apply_body_delta(q, v, wv, dl, da, weight, com, S.inertia(i), im, S.inv_inertia(i), dt);
-                } else {
-                    // no contact touched the body: the closed form, exact up to
-                    // the sign of zeros, which no later step of a world
-                    // without real joints can tell apart
-                    apply_zero_delta(q, v, wv, com, im);
-                }
-                if (model_joints && !world_joints) {
-                    // the joint pass of this world only renormalises (free joints)
-                    apply_zero_delta(q, v, wv, com, im);
-                }
+                const M33 I = S.inertia(i), iI = S.inv_inertia(i);
+                apply_body_delta(q, v, wv, dl, da, weight, com, I, im, iI, dt);
+                if (model_joints && !world_joints) apply_body_delta(q, v, wv, zero3, zero3, 1.0f, com, I, im, iI, dt);
                 S.set(i, q, v, wv);
             }
             group_sync<G>(g);
         }
         if (model_joints && (world_joints || !has_contacts)) {
-            if constexpr (!kLean) {  // solve_joint returns at once for FREE joints
-                for (int j = j0 + t; j < j1; j += G)
-                    solve_joint(m, S, b0, j, io.joint_target_pos, io.joint_target_vel, p, dt, &bad,
-                                io.body_parent_f ? io.joint_impulse : nullptr);
+            if constexpr (!kLean) {
+                if (world_joints) {
+                    float* jimp = io.body_parent_f ? io.joint_impulse : nullptr;
+                    auto jtest = [&](int k, int& ends) -> bool { return joint_active(m, S, b0, j0 + k, ends); };
+                    auto jsolve = [&](int k, float* d12) {
+                        solve_joint(m, S, b0, j0 + k, io.joint_target_pos, io.joint_target_vel, p, dt, d12, jimp);
+                    };
+                    auto jadd = [&](int i, int, const float* d6) { S.add(i, d6); };
+                    nb::ordered_pass<G, kST>(B, j1 - j0, g, t, jtest, jsolve, jadd);
+                }
             }
-            group_sync<G>(g);
             for (int i = t; i < nb; i += G) {
                 V3 dl, da;
                 S.take(i, dl, da);
@@ -1115,20 +1137,27 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
         }
     }
     // ---- restitution (solver_xpbd.py:685-755), after all iterations
-    if (!kLean && has_contacts && p.enable_restitution) {
-        if constexpr (!kLean) {
-            for (int k = t; k < nc; k += G)
-                restitution_contact(m, S, R + (size_t)k * 5, b0, io.body_q_in, io.body_qd_in, dt, &bad);
+    if constexpr (!kLean) {
+        if (has_contacts && p.enable_restitution) {
+            auto rtest = [&](int k, int& ends) -> bool {
+                float tmp[12];
+                return restitution_contact(m, S, R + (size_t)k * 5, b0, io.body_q_in, io.body_qd_in, dt, tmp, ends);
+            };
+            auto rsolve = [&](int k, float* d12) {
+                int ends;
+                restitution_contact(m, S, R + (size_t)k * 5, b0, io.body_q_in, io.body_qd_in, dt, d12, ends);
+            };
+            auto radd = [&](int i, int, const float* d6) { S.add(i, d6); };
+            nb::ordered_pass<G, kST>(B, nc, g, t, rtest, rsolve, radd);
+            // apply_body_delta_velocities (kernels.py:881-887) over every body
+            for (int i = t; i < nb; i += G) {
+                V3 dl, da;
+                S.take(i, dl, da);
+                const V3 v = S.v(i), wv = S.w(i);
+                S.set(i, S.q(i), add(v, dl), add(wv, da));
+            }
+            group_sync<G>(g);
         }
-        group_sync<G>(g);
-        // apply_body_delta_velocities (kernels.py:881-887)
-        for (int i = t; i < nb; i += G) {
-            V3 dl, da;
-            S.take(i, dl, da);
-            const V3 v = S.v(i), wv = S.w(i);
-            S.set(i, S.q(i), add(v, dl), add(wv, da));
-        }
-        group_sync<G>(g);
     }
     // ---- body_parent_f (solver_xpbd.py:636-655, convert_joint_impulse_to_parent_f,
     // kernels.py:2396-2436): zero for every body of the world, then the
@@ -1184,8 +1213,8 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
     __shared__ int s_batch;
     __shared__ unsigned s_bad;
     __shared__ int s_flag[kGroups];
-    __shared__ int s_nact[kGroups][2];
-    __shared__ unsigned char s_list[kGroups][kChunk];
+    __shared__ int s_pen[kGroups];
+    __shared__ Batch<G> s_ob[kGroups];
     const int g = threadIdx.x / G;   // group within the CTA
     const int t = threadIdx.x % G;   // thread within the group
     if (threadIdx.x == 0) s_bad = 0u;
@@ -1199,17 +1228,12 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
             const int b0 = m.world_body_start[w];
             const int nb = m.world_body_start[w + 1] - b0;
             SBodiesT<false> S = sbodies_carve<false>(arena + 4 * (size_t)m.batch_slab[b * kGroups + g], m, b0, nb);
-            step_world<G, kLean, kWarm>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g],
-                                        s_list[g], &s_bad);
+            step_world<G, kLean, kWarm>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], &s_pen[g],
+                                        s_ob[g], &s_bad);
         }
         __syncthreads();  // every group is done with the arena before the next batch
     }
-    if (threadIdx.x == 0 && s_bad) {
-        unsigned st = 0;
-        if (s_bad & 1u) st |= NB_STATUS_FIXED_OVERFLOW;
-        if (s_bad & 2u) st |= NB_STATUS_NONFINITE;
-        atomicOr(seg.status, st);
-    }
+    if (threadIdx.x == 0 && s_bad) atomicOr(seg.status, (unsigned)NB_STATUS_NONFINITE);
 }
 
 // Group mode: the CTA's threads form 256 / G independent groups of G threads;
@@ -1226,8 +1250,8 @@ xpbd_step_group_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg 
     __shared__ unsigned s_bad;
     __shared__ int s_world[kGroups];
     __shared__ int s_flag[kGroups];
-    __shared__ int s_nact[kGroups][2];
-    __shared__ unsigned char s_list[kGroups][kChunk];
+    __shared__ int s_pen[kGroups];
+    __shared__ Batch<G> s_ob[kGroups];
     const int g = threadIdx.x / G;
     const int t = threadIdx.x % G;
     if (threadIdx.x == 0) s_bad = 0u;
@@ -1255,240 +1279,12 @@ xpbd_step_group_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg 
             continue;
         }
         SBodiesT<kCompact> S = sbodies_carve<kCompact>(region, m, b0, nb);
-        step_world<G, kLean, kWarm>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], s_nact[g],
-                                    s_list[g], &s_bad);
+        step_world<G, kLean, kWarm>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], &s_pen[g],
+                                    s_ob[g], &s_bad);
         group_sync<G>(g);
     }
     __syncthreads();
-    if (threadIdx.x == 0 && s_bad) {
-        unsigned st = 0;
-        if (s_bad & 1u) st |= NB_STATUS_FIXED_OVERFLOW;
-        if (s_bad & 2u) st |= NB_STATUS_NONFINITE;
-        atomicOr(seg.status, st);
-    }
-}
-
-// ---------------------------------------------------------------- flat mode
-// The same substep with the body state in global memory (structure of arrays
-// over all bodies, caller scratch) instead of per-world shared-memory slabs,
-// and one launch per phase over all worlds at once: flat_begin (a warp per
-// world: stage, joint forces, integrate), then per iteration flat_contacts (a
-// warp per tile of consecutive contact records of any worlds: the contact
-// pass, deltas summed with the same exact fixed-point atomics) and
-// flat_apply (a thread per body), then flat_end (write-back).  Every
-// function of the per-world path is reused on a global view of the state,
-// so the results are bit-identical; what changes is the
-// parallelism: all worlds' contacts and bodies are in flight at once instead
-// of one world's chain per thread group.  For models whose joints are all
-// free, without restitution, impulse reporting or warm start.
-
-struct FlatScratch {
-    float* f;                  // [13][B] pose + twist
-    unsigned long long* acc;   // [6][B] fixed-point deltas (the first 6 B floats hold body forces before integration)
-    int* flags;                // [B]
-    int* cnt;                  // [B]
-};
-
-__host__ __device__ inline size_t flat_acc_offset(int B) { return ((size_t)13 * B * 4 + 15) & ~(size_t)15; }
-__host__ __device__ inline size_t flat_scratch_bytes(int B) {
-    return flat_acc_offset(B) + (size_t)6 * B * 8 + (size_t)2 * B * 4;
-}
-
-__device__ __forceinline__ FlatScratch flat_scratch(void* base, int B) {
-    unsigned char* b = reinterpret_cast<unsigned char*>(base);
-    FlatScratch fs;
-    fs.f = reinterpret_cast<float*>(b);
-    fs.acc = reinterpret_cast<unsigned long long*>(b + flat_acc_offset(B));
-    fs.flags = reinterpret_cast<int*>(fs.acc + 6 * (size_t)B);
-    fs.cnt = fs.flags + B;
-    return fs;
-}
-
-// the per-world slab interface over the global arrays: local body i of a world
-// starting at b0 is global body b0 + i, arrays strided by the body count
-__device__ __forceinline__ SBodiesT<true> global_view(const NbModelDesc& m, const FlatScratch& fs, int b0) {
-    SBodiesT<true> S;
-    S.nb = m.body_count;
-    S.b0 = b0;
-    S.f = fs.f + b0;
-    S.c = S.I = S.iI = nullptr;
-    S.g_com = m.body_com;
-    S.g_inv_m = m.body_inv_mass;
-    S.g_I = m.body_inertia;
-    S.g_iI = m.body_inv_inertia;
-    S.acc = fs.acc + b0;
-    S.frc = reinterpret_cast<float*>(fs.acc) + b0;
-    S.flags = fs.flags + b0;
-    S.cnt = fs.cnt + b0;
-    return S;
-}
-
-constexpr int kFlatWarps = 8;  // warps per CTA of the per-world flat kernels
-
-__global__ void __launch_bounds__(32 * kFlatWarps)
-flat_begin_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, float dt) {
-    const FlatScratch fs = flat_scratch(io.step_scratch, m.body_count);
-    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-    __shared__ int s_flag[kFlatWarps];
-    for (int w = blockIdx.x * kFlatWarps + wl; w < m.world_count; w += gridDim.x * kFlatWarps) {
-        const int b0 = m.world_body_start[w];
-        const int nb = m.world_body_start[w + 1] - b0;
-        SBodiesT<true> S = global_view(m, fs, b0);
-        for (int i = lane; i < nb; i += 32) {
-            const int bi = b0 + i;
-            S.flags[i] = m.body_flags[bi];
-            const float* q = io.body_q_in + 7 * (size_t)bi;
-            const float* qd = io.body_qd_in + 6 * (size_t)bi;
-            const float* fb = io.body_f_in + 6 * (size_t)bi;
-            S.set(i, TF{V3{q[0], q[1], q[2]}, Q4{q[3], q[4], q[5], q[6]}}, V3{qd[0], qd[1], qd[2]},
-                  V3{qd[3], qd[4], qd[5]});
-            for (int k = 0; k < 6; ++k) S.frc[k * S.nb + i] = fb[k];
-            S.cnt[i] = 0;
-        }
-        const int j0 = m.world_joint_start[w], j1 = m.world_joint_start[w + 1];
-        if (lane == 0) s_flag[wl] = 0;
-        __syncwarp();
-        for (int j = j0 + lane; j < j1; j += 32) {
-            if (m.joint_type[j] != NB_JOINT_FREE && m.joint_enabled[j]) atomicOr(&s_flag[wl], 1);
-            if (io.joint_f) {
-                const int qs = m.joint_qd_start[j];
-                const int nd = m.joint_dof_dim[2 * j] + m.joint_dof_dim[2 * j + 1];
-                for (int k = 0; k < nd; ++k)
-                    if (io.joint_f[qs + k] != 0.0f) atomicOr(&s_flag[wl], 2);
-            }
-        }
-        __syncwarp();
-        // an enabled non-free joint needs the per-world path (the host never selects this mode then)
-        if ((s_flag[wl] & 1) && lane == 0) atomicOr(seg.status, (unsigned)NB_STATUS_MODE_UNSUPPORTED);
-        if ((s_flag[wl] & 2) && lane == 0) joint_forces(m, S, b0, j0, j1, io.joint_f);
-        __syncwarp();
-        for (int i = lane; i < nb; i += 32) {
-            const V3 f0{S.frc[0 * S.nb + i], S.frc[1 * S.nb + i], S.frc[2 * S.nb + i]};
-            const V3 t0{S.frc[3 * S.nb + i], S.frc[4 * S.nb + i], S.frc[5 * S.nb + i]};
-            if (!(S.flags[i] & NB_BODY_KINEMATIC)) {
-                const int bi = b0 + i;
-                int wi = m.body_world[bi];
-                if (wi < 0) wi = 0;
-                const V3 gv = load_v3(m.gravity + 3 * (size_t)wi);
-                TF q = S.q(i);
-                V3 v = S.v(i), wv = S.w(i);
-                integrate_rigid_body(q, v, wv, f0, t0, S.com(i), S.inertia(i), m.body_inv_mass[bi],
-                                     load_m33(m.body_inv_inertia + 9 * (size_t)bi), gv, p.angular_damping, dt);
-                S.set(i, q, v, wv);
-            }
-        }
-        __syncwarp();
-        for (int i = lane; i < nb; i += 32)
-            for (int k = 0; k < 6; ++k) S.acc[k * S.nb + i] = 0ull;
-        __syncwarp();
-    }
-}
-
-// contact records are dense over all worlds (world w's at world_base[w] ..);
-// a record's world follows from one of its shapes: the body of shape s_a is
-// local body l_a of its world, so the world starts at shape_body[s_a] - l_a
-__device__ __forceinline__ int record_world_start(const NbModelDesc& m, const float4* r) {
-    const int tag = __float_as_int(r[2].w);
-    const int la = (tag & 0xFFF) - 1, lb = ((tag >> 12) & 0xFFF) - 1;
-    if (la >= 0) return m.shape_body[__float_as_int(r[3].w)] - la;
-    if (lb >= 0) return m.shape_body[__float_as_int(r[4].w)] - lb;
-    return 0;
-}
-
-// A warp per tile of kChunk consecutive records of any worlds: test them, compact the
-// penetrating ones in shared memory, then solve those with every lane busy.
-__global__ void __launch_bounds__(32 * kFlatWarps)
-flat_contacts_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, float dt) {
-    const FlatScratch fs = flat_scratch(io.step_scratch, m.body_count);
-    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-    __shared__ int s_nact[kFlatWarps];
-    __shared__ unsigned char s_list[kFlatWarps][kChunk];
-    const float4* rec = reinterpret_cast<const float4*>(seg.rec);
-    const bool weighting = p.rigid_contact_con_weighting != 0;
-    const int W = m.world_count;
-    const long total = W > 0 ? (long)seg.world_base[W - 1] + seg.world_count[W - 1] : 0;
-    const long tiles = (total + kChunk - 1) / kChunk;
-    unsigned bad = 0u;
-    for (long tile = blockIdx.x * (long)kFlatWarps + wl; tile < tiles; tile += (long)gridDim.x * kFlatWarps) {
-        const long base = tile * kChunk;
-        const int lim = total - base < kChunk ? (int)(total - base) : kChunk;
-        if (lane == 0) s_nact[wl] = 0;
-        __syncwarp();
-        for (int k = lane; k < lim; k += 32) {
-            const float4* r = rec + (size_t)(base + k) * 5;
-            const SBodiesT<true> S = global_view(m, fs, record_world_start(m, r));
-            if (contact_active(S, r[0], r[1], r[2])) s_list[wl][atomicAdd(&s_nact[wl], 1)] = (unsigned char)k;
-        }
-        __syncwarp();
-        const int na = s_nact[wl];
-        for (int a = lane; a < na; a += 32) {
-            const float4* r = rec + (size_t)(base + s_list[wl][a]) * 5;
-            SBodiesT<true> S = global_view(m, fs, record_world_start(m, r));
-            solve_contact(m, S, r[0], r[1], r[2], r[3], r[4], p.rigid_contact_relaxation, dt, weighting, &bad, nullptr);
-        }
-        __syncwarp();
-    }
-    if (bad && lane == 0) atomicOr(seg.status, (unsigned)NB_STATUS_FIXED_OVERFLOW);
-}
-
-// mode 0: after a contact pass (weighted apply, closed form for untouched bodies, then the free-joint
-// renormalisation when the model has joints); mode 1: the joint pass of a step without contacts
-__global__ void __launch_bounds__(256) flat_apply_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, int mode,
-                                                         float dt) {
-    const FlatScratch fs = flat_scratch(io.step_scratch, m.body_count);
-    SBodiesT<true> S = global_view(m, fs, 0);
-    const bool weighting = p.rigid_contact_con_weighting != 0;
-    const bool model_joints = m.joint_count > 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.body_count; i += gridDim.x * blockDim.x) {
-        V3 dl, da;
-        const bool moved = S.take(i, dl, da);
-        TF q = S.q(i);
-        V3 v = S.v(i), wv = S.w(i);
-        const V3 com = S.com(i);
-        const float im = S.inv_m(i);
-        if (mode == 0) {
-            float weight = 1.0f;
-            if (weighting) {
-                float iw = (float)S.cnt[i];
-                S.cnt[i] = 0;
-                if (iw > 0.0f) weight = 1.0f / iw;
-            }
-            if (moved) apply_body_delta(q, v, wv, dl, da, weight, com, S.inertia(i), im, S.inv_inertia(i), dt);
-            else apply_zero_delta(q, v, wv, com, im);
-            if (model_joints) apply_zero_delta(q, v, wv, com, im);
-        } else {
-            apply_body_delta(q, v, wv, dl, da, 1.0f, com, S.inertia(i), im, S.inv_inertia(i), dt);
-        }
-        S.set(i, q, v, wv);
-    }
-}
-
-__global__ void __launch_bounds__(256) flat_end_kernel(NbModelDesc m, NbStepIO io, NbContactSeg seg) {
-    const FlatScratch fs = flat_scratch(io.step_scratch, m.body_count);
-    SBodiesT<true> S = global_view(m, fs, 0);
-    unsigned bad = 0u;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.body_count; i += gridDim.x * blockDim.x) {
-        float* qo = io.body_q_out + 7 * (size_t)i;
-        float* qdo = io.body_qd_out + 6 * (size_t)i;
-        if (S.flags[i] & NB_BODY_KINEMATIC) {
-            for (int k = 0; k < 7; ++k) qo[k] = io.body_q_in[7 * (size_t)i + k];
-            for (int k = 0; k < 6; ++k) qdo[k] = io.body_qd_in[6 * (size_t)i + k];
-            continue;
-        }
-        bool finite = true;
-        for (int k = 0; k < 7; ++k) {
-            const float x = S.f[k * S.nb + i];
-            finite = finite && isfinite(x);
-            qo[k] = x;
-        }
-        for (int k = 0; k < 6; ++k) {
-            const float x = S.f[(7 + k) * S.nb + i];
-            finite = finite && isfinite(x);
-            qdo[k] = x;
-        }
-        if (!finite) bad = 1u;
-    }
-    if (bad) atomicOr(seg.status, (unsigned)NB_STATUS_NONFINITE);
+    if (threadIdx.x == 0 && s_bad) atomicOr(seg.status, (unsigned)NB_STATUS_NONFINITE);
 }
 
 }  // namespace
@@ -1582,39 +1378,11 @@ cudaError_t launch_step_groups(const NbModelDesc* m, const NbXpbdParams* p, cons
 
 int nb_step_slab_words(int compact) { return compact ? slab_words_per_body<true>() : slab_words_per_body<false>(); }
 
-size_t nb_step_scratch_bytes(const NbModelDesc* m) {
-    return m->step_mode == 3 && m->body_count > 0 ? flat_scratch_bytes(m->body_count) : 0;
-}
-
-namespace {
-cudaError_t launch_flat(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
-                        float dt, cudaStream_t stream) {
-    if (m->body_count <= 0) return cudaSuccess;
-    const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
-    const int gw = nb_contact_grid((long)m->world_count * 32, 32 * kFlatWarps);
-    const int gb = nb_contact_grid(m->body_count, 256);
-    // contact tiles: one warp per kChunk records, records at most 5 per candidate pair
-    const int gc = nb_contact_grid((long)m->contact_capacity / kChunk * 32 + 32, 32 * kFlatWarps);
-    flat_begin_kernel<<<gw, 32 * kFlatWarps, 0, stream>>>(*m, *p, *io, *seg, dt);
-    for (int it = 0; it < p->iterations; ++it) {
-        if (has_contacts) {
-            flat_contacts_kernel<<<gc, 32 * kFlatWarps, 0, stream>>>(*m, *p, *io, *seg, dt);
-            flat_apply_kernel<<<gb, 256, 0, stream>>>(*m, *p, *io, 0, dt);
-        } else if (m->joint_count > 0) {
-            flat_apply_kernel<<<gb, 256, 0, stream>>>(*m, *p, *io, 1, dt);
-        }
-    }
-    flat_end_kernel<<<gb, 256, 0, stream>>>(*m, *io, *seg);
-    return cudaGetLastError();
-}
-}  // namespace
-
 cudaError_t nb_launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
                            float dt, int grid, cudaStream_t stream) {
     if (m->cta_threads != kST) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(seg->work_counter + 4, 0, sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
-    if (m->step_mode == 3) return launch_flat(m, p, io, seg, dt, stream);
     if (m->step_mode == 1) return launch_step_groups<false>(m, p, io, seg, dt, grid, stream);
     if (m->step_mode == 2) return launch_step_groups<true>(m, p, io, seg, dt, grid, stream);
     switch (m->group_threads) {

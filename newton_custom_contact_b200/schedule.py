@@ -6,9 +6,9 @@ Two ways to map worlds to the GPU:
   independent groups of G = 32, 64 or 128 threads; every group owns G / 256 of
   its CTA's shared-memory arena and pulls whole worlds, largest first, from a
   device counter -- no CTA-wide barrier between worlds.  ``"groups"`` stages
-  the full body slab (49 words per body), ``"groups_compact"`` only the
-  mutable part (27 words per body; mass properties are read from the model).
-  A G = 32 share holds 70 / 128 bodies, a G = 64 share 141 / 256.
+  the full body slab (43 words per body), ``"groups_compact"`` only the
+  mutable part (21 words per body; mass properties are read from the model).
+  A G = 32 share holds 62 / 128 bodies, a G = 64 share 125 / 256.
 * batch mode: one world per thread group of G threads (G = 32: a warp per
   world ... G = 256: a CTA per world); a CTA holds 256 / G groups that share
   one arena.  Worlds are packed, largest first, into batches that fit one
@@ -27,12 +27,15 @@ import numpy as np
 
 CTA_THREADS = 256
 WARPS_PER_CTA = CTA_THREADS // 32
-SLAB_WORDS_PER_BODY = 12 + 13 + 4 + 9 + 9 + 1 + 1  # must match slab_words_per_body<false>() in nb_xpbd.cu
-SLAB_WORDS_COMPACT = 12 + 13 + 1 + 1  # slab_words_per_body<true>()
-STEP_MODES = {"batch": 0, "groups": 1, "groups_compact": 2, "flat": 3}
+SLAB_WORDS_PER_BODY = 6 + 13 + 4 + 9 + 9 + 1 + 1  # must match slab_words_per_body<false>() in nb_xpbd.cu
+SLAB_WORDS_COMPACT = 6 + 13 + 1 + 1  # slab_words_per_body<true>()
+STEP_MODES = {"batch": 0, "groups": 1, "groups_compact": 2}
 GROUP_MODE_SIZES = (32, 64, 128)
-ARENA_WORDS_TWO_CTAS = 27 * 1024  # ~108 KB: two CTAs per SM
-ARENA_WORDS_MAX = 55 * 1024       # ~220 KB: the opt-in per-CTA maximum less the kernel's static shared memory
+# The step kernel's static shared memory (the groups' ordered-accumulation batches) is 21.8 KB for
+# 32-thread groups and up to 28.9 KB for 64-thread groups; with the dynamic arena below, two CTAs
+# still fit one SM's 228 KB.
+ARENA_WORDS_TWO_CTAS = 21 * 1024  # 84 KB: two CTAs per SM
+ARENA_WORDS_MAX = 48 * 1024       # 192 KB: the opt-in per-CTA maximum less the kernel's static shared memory
 GROUP_SIZES = (32, 64, 128, 256)
 
 
@@ -104,12 +107,6 @@ def build_schedule(model, group_threads: int | None = None, mode: str | None = N
             mode, group_threads = default_mode(maxb)
     if mode not in STEP_MODES:
         raise ValueError(f"mode must be one of {tuple(STEP_MODES)}")
-    if mode == "flat":
-        if not flat_applicable(model):
-            raise ValueError("mode 'flat' needs a model whose enabled joints are all free joints")
-        return StepSchedule(group_threads=32, cta_threads=CTA_THREADS, arena_words=ARENA_WORDS_TWO_CTAS,
-                            batch_count=0, batch_world=np.full((1, CTA_THREADS // 32), -1, np.int32),
-                            batch_slab=np.zeros((1, CTA_THREADS // 32), np.int32), mode=mode)
     if mode != "batch":
         g = group_threads or 32
         if g not in GROUP_MODE_SIZES:
@@ -166,24 +163,11 @@ def histogram_key(model, bins=(16, 32, 64, 128, 256, 512)) -> tuple:
 _CACHE: dict = {}
 
 
-def flat_applicable(model) -> bool:
-    """The flat mode (body state in global memory, one launch per phase over all worlds) handles free
-    bodies only: every enabled joint must be a free joint."""
-    from ._abi import JointType
-
-    if model.joint_count == 0:
-        return True
-    jt = model.host("joint_type")
-    en = model.host("joint_enabled")
-    return bool(np.all((jt == int(JointType.FREE)) | (en == 0)))
-
-
-def candidate_schedules(model, flat: bool = True) -> list:
-    """(mode, group_threads) pairs that can run this model's largest world (plus the flat mode when it
-    applies and `flat`)."""
+def candidate_schedules(model) -> list:
+    """(mode, group_threads) pairs that can run this model's largest world."""
     nb = np.diff(model._part["world_body_start"].astype(np.int64))
     maxb = int(nb.max()) if nb.size else 1
-    out = [("flat", 32)] if flat and flat_applicable(model) else []
+    out = []
     for words, mode in ((SLAB_WORDS_PER_BODY, "groups"), (SLAB_WORDS_COMPACT, "groups_compact")):
         out += [(mode, g) for g in GROUP_MODE_SIZES if words * maxb <= group_share_words(g)]
     out += [("batch", g) for g in GROUP_SIZES]
@@ -204,10 +188,7 @@ def autotune(pipeline, solver, state_in, state_out, contacts, dt: float, candida
         pipeline.set_step_schedule(g, mode=mode)
         return {}
     if candidates is None:
-        # the flat mode runs the plain solve only
-        plain = (not solver.enable_restitution and getattr(solver, "warm_start", None) is None
-                 and contacts.force is None and state_out.body_parent_f is None)
-        candidates = candidate_schedules(pipeline.model, flat=plain)
+        candidates = candidate_schedules(pipeline.model)
     q0, qd0 = state_in.body_q.clone(), state_in.body_qd.clone()
     pipeline.collide(state_in, contacts)
     times = {}

@@ -6,8 +6,9 @@ projection, delta application) from libnewton_b200.so.  Differences from the
 reference that a caller can observe:
   * ``state_in`` is left unchanged (the reference ping-pongs through it,
     solver_xpbd.py:203-257);
-  * per-body constraint deltas are summed in 2^-32 fixed point, so results are
-    bit-reproducible and independent of contact order;
+  * per-body constraint deltas are summed in float in contact (joint) order --
+    the reference's sums run sequentially -- so results are bit-reproducible
+    where the reference's atomic order is unspecified;
   * particles and springs are not part of this build and raise
     ``NotImplementedError``;
   * an optional learned warm start (``solver.warm_start``, warmstart.py) has
@@ -68,7 +69,6 @@ class SolverXPBD:
         self._joint_impulse = None
         # optional learned warm start (warmstart.WarmStart); None = the plain solver
         self.warm_start = None
-        self._step_scratch = None
 
     @property
     def device(self):
@@ -167,17 +167,6 @@ class SolverXPBD:
             io.impulse_scratch = ptr(contacts._seg["impulse_scratch"])
             io.contact_impulse_capacity = cap
         params = self.params()
-        if desc.step_mode == 3:
-            # flat schedule: the body state lives in a caller-owned scratch buffer
-            if (self.enable_restitution or io.contact_impulse or io.body_parent_f
-                    or (self.warm_start is not None and contacts is not None)):
-                raise ValueError("the 'flat' step schedule runs the plain solve only (no restitution, contact "
-                                 "forces, body_parent_f or warm start); choose another schedule with "
-                                 "pipeline.set_step_schedule")
-            nbytes = int(lib.nb_step_scratch_size(C.byref(desc)))
-            if self._step_scratch is None or self._step_scratch.numel() < nbytes:
-                self._step_scratch = torch.empty(nbytes, dtype=torch.uint8, device=model.device)
-            io.step_scratch = ptr(self._step_scratch)
         ws = self.warm_start if contacts is not None else None
         if ws is not None:
             ws.before_step(model, pipe, desc, state_in, contacts, dt, io)
@@ -230,11 +219,6 @@ class SolverXPBD:
         io.joint_target_pos = ptr(control.joint_target_pos)
         io.joint_target_vel = ptr(control.joint_target_vel)
         io.joint_f = ptr(control.joint_f)
-        if desc.step_mode == 3:
-            nbytes = int(lib.nb_step_scratch_size(C.byref(desc)))
-            if self._step_scratch is None or self._step_scratch.numel() < nbytes:
-                self._step_scratch = torch.empty(nbytes, dtype=torch.uint8, device=model.device)
-            io.step_scratch = ptr(self._step_scratch)
         params = self.params()
         _lib.check("nb_xpbd_substeps", lib.nb_xpbd_substeps(
             C.byref(desc), C.byref(params), C.byref(io), C.byref(pipe.seg_struct(contacts)),

@@ -124,9 +124,10 @@ def collide(model, layout, body_q: np.ndarray) -> HostSegments:
 
 
 def step(model, layout, params, body_q, body_qd, body_f, segs: HostSegments | None, dt: float,
-         joint_target_pos=None, joint_target_vel=None, joint_f=None, acc_mode: int = ACC_FIXED,
+         joint_target_pos=None, joint_target_vel=None, joint_f=None, acc_mode: int = ACC_FLOAT,
          want_impulse: bool = False, want_parent_f: bool = False):
-    """One SolverXPBD.step on the CPU.  Returns (body_q_out, body_qd_out, status), then the
+    """One SolverXPBD.step on the CPU (per-body deltas summed in float in contact / joint order, like the
+    CUDA kernels, unless ``acc_mode`` is ACC_FIXED).  Returns (body_q_out, body_qd_out, status), then the
     accumulated weighted contact impulse [slot, 6] (indexed like ``segs``) when ``want_impulse``,
     then body_parent_f [B, 6] when ``want_parent_f``."""
     from newton_custom_contact_b200._abi import NbStepIO

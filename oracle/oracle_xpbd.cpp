@@ -15,12 +15,15 @@
 //   SolverXPBD.step orchestration             newton/_src/solvers/xpbd/solver_xpbd.py:259-764
 //
 // The reference sums per-body deltas with float atomics, i.e. in an unspecified
-// order.  This oracle offers two accumulation modes:
+// order on a GPU.  This oracle offers two accumulation modes:
+//   ORC_ACC_FLOAT  -- plain fp32 sums in contact-index (joint-index) order: the
+//                     reference run sequentially, and what the CUDA kernels
+//                     compute (their ordered accumulation), so the two agree
+//                     bit for bit;
 //   ORC_ACC_FIXED  -- each contribution is rounded to a 2^-32 fixed-point
-//                     int64 and summed exactly (order-independent); the CUDA
-//                     kernels use the same rule, so the two agree bit for bit.
-//   ORC_ACC_FLOAT  -- plain fp32 sums in contact-index order (the reference
-//                     semantics with one particular atomic order).
+//                     int64 and summed exactly (order-independent); kept to
+//                     measure how far another summation rule lands from the
+//                     reference.
 #include "oracle_math.h"
 #include "../include/newton_b200.h"
 

@@ -1,9 +1,9 @@
 """CUDA path vs the CPU oracle on identical seeded scenes.
 
-Both sides are compiled without fp contraction and sum per-body deltas in
-the same 2^-32 fixed point, so contacts and body states are compared for
-exact equality (the parity bar of 1e-5 rel / 1e-6 m is asserted as well, to
-report the size of any difference).
+Both sides are compiled without fp contraction (the library's parity build)
+and sum per-body deltas in float in contact / joint order, so contacts and
+body states are compared for exact equality (the parity bar of 1e-5 rel /
+1e-6 m is asserted as well, to report the size of any difference).
 """
 
 import numpy as np
@@ -133,7 +133,7 @@ def test_step_parity_c1(cuda, orc, substeps):
                                                   (4, 32, "groups_compact"), (16, 32, "groups_compact"),
                                                   (4, 64, "groups"), (4, 64, "groups_compact"), (4, 128, "groups"),
                                                   (4, 32, "batch"), (4, 64, "batch"), (4, 128, "batch"),
-                                                  (4, 256, "batch"), (4, 32, "flat"), (16, 32, "flat")])
+                                                  (4, 256, "batch")])
 def test_step_parity_c2(cuda, orc, substeps, group, mode):
     model, info = _small_c2()
     gq, gqd, q, qd = _run_loop(model, info, substeps, orc, group_threads=group, mode=mode)
@@ -141,38 +141,8 @@ def test_step_parity_c2(cuda, orc, substeps, group, mode):
     assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
 
 
-def test_step_parity_c1_flat(cuda, orc):
-    """One 64-body world through the flat schedule (one warp for all its contacts)."""
-    model, info = scenes.scene_c1(device="cuda")
-    gq, gqd, q, qd = _run_loop(model, info, 16, orc, group_threads=32, mode="flat")
-    assert _bits_equal(gq, q) and _bits_equal(gqd, qd)
-
-
-def test_flat_schedule_limits(cuda):
-    """The flat schedule runs free bodies' plain solve only."""
-    model, info = scenes.scene_c3(worlds=2, device="cuda")
-    with pytest.raises(ValueError):
-        CollisionPipeline(model).set_step_schedule(32, mode="flat")
-    model, info = _small_c2(worlds=4)
-    model.request_contact_attributes("force")
-    pipe = CollisionPipeline(model)
-    pipe.set_step_schedule(32, mode="flat")
-    solver = SolverXPBD(model, iterations=2)
-    s0, s1 = model.state(), model.state()
-    contacts = pipe.contacts()
-    pipe.collide(s0, contacts)
-    with pytest.raises(ValueError):
-        solver.step(s0, s1, None, contacts, 1.0 / 480.0)
-
-
-@pytest.mark.parametrize("mode", [None, "flat"])
-def test_step_without_contacts(cuda, orc, mode):
-    if mode:
-        scenes_model, _ = scenes.scene_c1(device="cuda")
-        scenes_model._default_pipeline().set_step_schedule(32, mode=mode)
-        _check_step_without_contacts(scenes_model, orc)
-    else:
-        _check_step_without_contacts(scenes.scene_c1(device="cuda")[0], orc)
+def test_step_without_contacts(cuda, orc):
+    _check_step_without_contacts(scenes.scene_c1(device="cuda")[0], orc)
 
 
 def _check_step_without_contacts(model, orc):
