@@ -207,6 +207,8 @@ typedef struct NbContactsPublic {
     float* margin1;              /* [cap] */
     int64_t* sort_key;           /* [cap] or NULL */
     int64_t* world_offset;       /* [W+1] scratch for the world scan */
+    int32_t* generation;         /* [1] Contacts.contact_generation, bumped by every publish (wraps to 0 after
+                                    INT32_MAX, as compute_shape_aabbs does, collide.py:211-218), or NULL */
 } NbContactsPublic;
 
 /* Frame-to-frame contact matching state (CollisionPipeline contact_matching,
@@ -334,6 +336,12 @@ int nb_abi_version(void);
 
 /* Number of CTAs the persistent kernels launch on the current device. */
 int32_t nb_default_grid(void);
+
+/*
+ * State.clear_forces (newton/_src/sim/state.py:156): zero body_f [n_bodies, 6]
+ * with a memset on the stream (no kernel launch).
+ */
+int nb_clear_forces(float* body_f, int32_t n_bodies, void* stream);
 
 /*
  * Collision detection for all worlds: shape world transforms + AABBs

@@ -201,6 +201,7 @@ class NbContactsPublic(C.Structure):
         ("margin1", _fp),
         ("sort_key", _fp),
         ("world_offset", _fp),
+        ("generation", _fp),
     ]
 
 

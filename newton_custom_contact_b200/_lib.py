@@ -45,6 +45,7 @@ BUILDS = {"product": LIB_PATH, "exact": os.path.join(_HERE, "libnewton_b200_exac
 EXPORTS = (
     "nb_abi_version",
     "nb_default_grid",
+    "nb_clear_forces",
     "nb_collide",
     "nb_publish_contacts",
     "nb_xpbd_step",
@@ -118,6 +119,8 @@ def load(path: str | None = None) -> C.CDLL:
     lib = C.CDLL(p)
     lib.nb_abi_version.restype = C.c_int
     lib.nb_default_grid.restype = C.c_int32
+    lib.nb_clear_forces.restype = C.c_int
+    lib.nb_clear_forces.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
     lib.nb_collide.restype = C.c_int
     lib.nb_collide.argtypes = [C.POINTER(NbModelDesc), C.c_void_p, C.POINTER(NbContactSeg), C.c_int32, C.c_void_p]
     lib.nb_publish_contacts.restype = C.c_int

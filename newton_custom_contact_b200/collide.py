@@ -395,6 +395,7 @@ class CollisionPipeline:
         p.margin1 = ptr(c.rigid_contact_margin1)
         p.sort_key = ptr(c.rigid_contact_sort_key) if c.rigid_contact_sort_key.numel() else None
         p.world_offset = ptr(c._world_offset)
+        p.generation = ptr(c.contact_generation)
         return p
 
     # ------------------------------------------------------------ collide
@@ -431,7 +432,6 @@ class CollisionPipeline:
             st = self._match_struct(contacts)
             _lib.check("nb_match_contacts", lib.nb_match_contacts(C.byref(desc), C.c_void_p(ptr(bq)), C.byref(pub),
                                                                   C.byref(seg), C.byref(st), C.c_void_p(stream)))
-        contacts.contact_generation.add_(1)
         contacts._seg_valid = True
 
     def status(self, contacts: Contacts) -> int:

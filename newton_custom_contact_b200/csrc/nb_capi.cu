@@ -107,6 +107,13 @@ int nb_abi_version(void) { return NB_ABI_VERSION; }
 
 int32_t nb_default_grid(void) { return grid_for(0); }
 
+int nb_clear_forces(float* body_f, int32_t n_bodies, void* stream) {
+    if (n_bodies < 0 || (n_bodies > 0 && !body_f)) return NB_ERR_INVALID;
+    if (n_bodies == 0) return NB_OK;
+    const cudaError_t e = cudaMemsetAsync(body_f, 0, sizeof(float) * 6 * (size_t)n_bodies, (cudaStream_t)stream);
+    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+}
+
 int nb_collide(const NbModelDesc* model, const float* body_q, const NbContactSeg* seg, int32_t grid_ctas,
                void* stream) {
     int rc = check_model(model);

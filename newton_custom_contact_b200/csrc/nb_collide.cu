@@ -525,7 +525,8 @@ narrow_gjk_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg 
 // = total (may exceed the public capacity, as in the reference).
 __global__ void __launch_bounds__(1024) world_scan_kernel(int W, const int32_t* __restrict__ world_count,
                                                           int64_t* world_offset, int64_t* world_base,
-                                                          int32_t* count_out, int cap, uint32_t* status) {
+                                                          int32_t* count_out, int cap, uint32_t* status,
+                                                          int32_t* generation) {
     __shared__ int64_t warp_sums[32];
     __shared__ int64_t carry;
     if (threadIdx.x == 0) carry = 0;
@@ -564,6 +565,12 @@ __global__ void __launch_bounds__(1024) world_scan_kernel(int W, const int32_t* 
         world_offset[W] = carry;
         count_out[0] = carry > 0x7fffffff ? 0x7fffffff : (int32_t)carry;
         if (carry > cap) atomicOr(status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
+        if (generation) {
+            // Contacts.contact_generation, bumped once per collide with the wraparound of
+            // compute_shape_aabbs (collide.py:211-218)
+            const int32_t g = generation[0];
+            generation[0] = g == 2147483647 ? 0 : g + 1;
+        }
     }
 }
 
@@ -772,8 +779,7 @@ cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const N
 cudaError_t nb_launch_publish(const NbModelDesc* m, const NbContactSeg* seg, const NbContactsPublic* pub,
                               cudaStream_t stream) {
     world_scan_kernel<<<1, 1024, 0, stream>>>(m->world_count, seg->world_count, pub->world_offset, seg->world_base,
-                                              pub->count,
-                                              pub->capacity, seg->status);
+                                              pub->count, pub->capacity, seg->status, pub->generation);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const int blocks = (m->world_count * 32 + 255) / 256;

@@ -35,8 +35,17 @@ class State:
         self.requires_grad = False
 
     def clear_forces(self) -> None:
-        """Zero body_f (state.py:156)."""
-        if self.body_f is not None:
+        """Zero body_f (state.py:156): a memset on the current stream through the library when body_f is a
+        CUDA tensor."""
+        if self.body_f is None:
+            return
+        if self.body_f.is_cuda and self.body_f.is_contiguous() and self.body_f.dtype == torch.float32:
+            from . import _lib
+
+            lib = _lib.load()
+            _lib.check("nb_clear_forces", lib.nb_clear_forces(self.body_f.data_ptr(), int(self.body_f.shape[0]),
+                                                               _lib.stream_handle(self.body_f.device)))
+        else:
             self.body_f.zero_()
 
     def assign(self, other: "State") -> None:

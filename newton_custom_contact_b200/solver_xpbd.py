@@ -224,7 +224,6 @@ class SolverXPBD:
             C.byref(desc), C.byref(params), C.byref(io), C.byref(pipe.seg_struct(contacts)),
             C.byref(pipe.public_struct(contacts)), float(dt), int(substeps), pipe.grid(),
             C.c_void_p(_lib.stream_handle(model.device))))
-        contacts.contact_generation.add_(int(substeps))
         contacts._seg_valid = True
         self._last_dt = dt
 

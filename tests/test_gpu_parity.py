@@ -232,3 +232,28 @@ def test_substeps_entry_matches_host_loop(cuda, n):
     assert _bits_equal(b.body_q.cpu().numpy(), ref_q) and _bits_equal(b.body_qd.cpu().numpy(), ref_qd)
     assert int(c2.rigid_contact_count.item()) == ref_count
     assert pipe.status(c2) == 0
+
+
+def test_contact_generation_bumped_by_collide(cuda):
+    """Contacts.contact_generation advances once per collide inside the library's publish, with the
+    reference's wraparound after INT32_MAX (compute_shape_aabbs, collide.py:211-218)."""
+    model, _ = _small_c2(worlds=4)
+    pipe = CollisionPipeline(model)
+    c = pipe.contacts()
+    s = model.state()
+    g0 = int(c.contact_generation.item())
+    for _ in range(3):
+        pipe.collide(s, c)
+    assert int(c.contact_generation.item()) == g0 + 3
+    c.contact_generation.fill_(2147483647)
+    pipe.collide(s, c)
+    assert int(c.contact_generation.item()) == 0
+
+
+def test_clear_forces_zeroes_body_f(cuda):
+    model, _ = _small_c2(worlds=4)
+    s = model.state()
+    s.body_f.fill_(3.0)
+    s.clear_forces()
+    torch.cuda.synchronize()
+    assert bool((s.body_f == 0).all().item())

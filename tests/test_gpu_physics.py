@@ -155,3 +155,54 @@ def test_joint_actuation(cuda, orc):
     t = steps * dt
     assert qd[rev, 5] == pytest.approx(tau * t / i_zz, abs=max(tau / i_zz * dt, 1e-3))
     assert qd[pri, 0] == pytest.approx(force * t / m_pri, abs=max(force / m_pri * dt, 1e-3))
+
+
+def test_kinematic_platform_drags_boxes(cuda, orc):
+    """Kinematic bodies through the CUDA path, bit for bit against the oracle: a kinematic platform
+    (effective inverse mass and inertia zero, solver.py:160-174) that the caller moves every substep
+    at 0.5 m/s carries boxes resting on it through the contacts' kinematic friction term
+    (kernels.py:2220-2225); the step passes the platform's own state through unchanged
+    (copy_kinematic_body_state_kernel, kernels.py:18-31)."""
+    cfg = ModelBuilder.ShapeConfig(mu=0.8, gap=0.05)
+    b = ModelBuilder(up_axis="Z", gravity=-9.81)
+    platform = b.add_body(xform=[0.0, 0.0, 0.1, 0.0, 0.0, 0.0, 1.0], is_kinematic=True)
+    b.add_shape_box(platform, hx=1.0, hy=1.0, hz=0.1, cfg=cfg)
+    h = 0.1
+    for x in (-0.5, 0.0, 0.5):
+        body = b.add_body(xform=[x, 0.0, 0.2 + h + 0.002, 0.0, 0.0, 0.0, 1.0])
+        b.add_shape_box(body, hx=h, hy=h, hz=h, cfg=cfg)
+    model = b.finalize(device="cuda")
+    dt = 1.0 / 60.0 / 8
+    speed = 0.5
+    solver = SolverXPBD(model, iterations=8)
+    pipe = CollisionPipeline(model)
+    contacts = pipe.contacts()
+    s0, s1 = model.state(), model.state()
+    q = model.host("body_q").copy()
+    qd = model.host("body_qd").copy()
+    qd[platform, 0] = np.float32(speed)
+    s0.body_qd.copy_(torch.from_numpy(qd))
+    zero = np.zeros((model.body_count, 6), np.float32)
+    p = solver.params()
+    for i in range(240):
+        # the caller drives the kinematic platform: its pose before substep i
+        q[platform, 0] = np.float32(speed * dt * i)
+        s0.body_q[platform, 0] = float(q[platform, 0])
+        s0.clear_forces()
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, dt)
+        segs = orc.collide(model, pipe.layout, q)
+        q_in = q.copy()
+        q, qd = orc.step(model, pipe.layout, p, q, qd, zero, segs, dt)[:2]
+        # kinematic pass-through: the step leaves the platform as it got it
+        assert np.array_equal(q[platform], q_in[platform])
+        s0, s1 = s1, s0
+        if i in (0, 15, 239):
+            torch.cuda.synchronize()
+            gq, gqd = s0.body_q.cpu().numpy(), s0.body_qd.cpu().numpy()
+            assert _bits_equal(gq, q) and _bits_equal(gqd, qd), f"substep {i}"
+    # after 0.5 s the boxes ride the platform: they move along +x at close to its speed and stay on it
+    boxes = [i for i in range(model.body_count) if i != platform]
+    vx = qd[boxes, 0]
+    assert np.all(vx > 0.8 * speed) and np.all(vx < 1.2 * speed), vx
+    assert np.all(np.abs(q[boxes, 2] - (0.2 + h)) < 0.01)
