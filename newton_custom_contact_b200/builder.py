@@ -21,12 +21,17 @@ import numpy as np
 from ._abi import BodyFlags, GeoType, JointType, ShapeFlags
 
 
+def _cross(a, b):
+    # the component formulas of np.cross for 3-vectors, without its axis handling
+    return np.array([a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]])
+
+
 def _quat_rotate(q, v):
     q = np.asarray(q, dtype=np.float64)
     v = np.asarray(v, dtype=np.float64)
     u = q[:3]
     w = q[3]
-    return v * (2.0 * w * w - 1.0) + u * (2.0 * np.dot(u, v)) + np.cross(u, v) * (2.0 * w)
+    return v * (2.0 * w * w - 1.0) + u * (2.0 * np.dot(u, v)) + _cross(u, v) * (2.0 * w)
 
 
 def _quat_to_matrix(q):
