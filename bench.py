@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned-warm-start arm")
     ap.add_argument("--warm-start-iterations", type=int, default=2)
+    ap.add_argument("--no-articulated", action="store_true", help="skip the articulated (C3) batch")
     ap.add_argument("--step-schedule", default=None, metavar="MODE/G",
                     help="fix the step schedule (e.g. groups_compact/32) instead of autotuning it; a run "
                          "under a profiler serialises launches, so its autotuner may pick another schedule")
@@ -336,6 +337,104 @@ def warm_start_arm(model, dt, substeps, sched, stream, flush, steps, warmup, ite
             "contact_matching": "latest", "network": "newton_custom_contact_b200/data/warmstart_c2.npz"}
 
 
+ARM_AMPLITUDE = 0.5               # rad, joint target amplitude of the articulated batch
+ARM_FREQUENCY = 0.5               # Hz
+
+
+def articulated_arm(dev, stream, flush, steps, warmup):
+    """The articulated batch (4096 worlds of a 7-link revolute arm among 8..48 loose boxes on a table
+    plane; dt 1/120 s, 4 substeps x 8 iterations): joint targets A sin(2 pi f t + phase) with a random
+    phase per joint, written into Control.joint_target_pos before every frame (inside the timed
+    region).  Timed like the main workload: each step is frames 6..35 from the same frame-6 state."""
+    import torch
+
+    from newton_custom_contact_b200 import CollisionPipeline, JointType, SolverXPBD, scenes
+    from newton_custom_contact_b200.metrics import max_joint_violation, max_penetration
+    from newton_custom_contact_b200.schedule import autotune
+
+    t0 = time.perf_counter()
+    model, info = scenes.scene_c3(worlds=4096, device=dev)
+    build_s = time.perf_counter() - t0
+    substeps, iters = info["substeps"], info["iterations"]
+    dt = info["dt"] / substeps
+    pipe = CollisionPipeline(model)
+    solver = SolverXPBD(model, iterations=iters)
+    s0, s1 = model.state(), model.state()
+    contacts = pipe.contacts()
+    control = model.control()
+    # joint target table: frame f sets the targets of time f * frame_dt
+    jt = model.host("joint_type")
+    rev = np.nonzero(jt == int(JointType.REVOLUTE))[0]
+    dof = model.host("joint_qd_start")[rev]
+    phases = np.asarray(info["phases"], np.float64).reshape(-1)
+    n_frames = WINDOW_START + WINDOW_FRAMES
+    table = np.zeros((n_frames, model.joint_dof_count), np.float32)
+    for f in range(n_frames):
+        table[f, dof] = ARM_AMPLITUDE * np.sin(2.0 * np.pi * ARM_FREQUENCY * f * info["dt"] + phases)
+    table_d = torch.from_numpy(table).to(dev)
+
+    def frame():
+        a, b = s0, s1
+        for _ in range(substeps):
+            a.clear_forces()
+            pipe.collide(a, contacts)
+            solver.step(a, b, control, contacts, dt)
+            a, b = b, a
+
+    with torch.cuda.stream(stream):
+        for f in range(WINDOW_START):
+            control.joint_target_pos.copy_(table_d[f])
+            frame()
+    torch.cuda.synchronize()
+    snap = (s0.body_q.clone(), s0.body_qd.clone())
+    with torch.cuda.stream(stream):
+        s0.clear_forces()
+        tune_ms = autotune(pipe, solver, s0, s1, contacts, dt, reps=3)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        frame()
+    torch.cuda.synchronize()
+
+    def window():
+        for f in range(WINDOW_START, n_frames):
+            control.joint_target_pos.copy_(table_d[f])
+            g.replay()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for k in range(warmup + steps):
+            s0.body_q.copy_(snap[0])
+            s0.body_qd.copy_(snap[1])
+            flush.fill_(float(k))
+            if k >= warmup:
+                starts[k - warmup].record(stream)
+            window()
+            if k >= warmup:
+                ends[k - warmup].record(stream)
+    torch.cuda.synchronize()
+    ms = sum(starts[k].elapsed_time(ends[k]) for k in range(steps))
+    with torch.cuda.stream(stream):
+        pipe.collide(s0, contacts)
+    torch.cuda.synchronize()
+    pen, jv = max_penetration(model, contacts, s0.body_q), max_joint_violation(model, s0.body_q)
+    finite = bool(torch.isfinite(s0.body_q).all().item())
+    del g
+    units = model.world_count * substeps * WINDOW_FRAMES * steps
+    sched = pipe._schedule
+    return {"workload": "C3: 4096 worlds of a 7-link revolute arm (capsules r 0.04 m, 0.3 m, 1 kg, limits "
+                        "+-2.5 rad, drive ke 500 kd 20) among 8..48 boxes on a table plane; dt 1/120, 4 substeps "
+                        "x 8 iterations",
+            "value": units / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "frames": FRAMES,
+            "bodies": model.body_count, "joints": model.joint_count,
+            "joint_targets": f"{ARM_AMPLITUDE} rad x sin(2 pi {ARM_FREQUENCY} Hz t + phase), set every frame",
+            "max_joint_violation_m": jv, "max_penetration_m": pen, "final_state_finite": finite,
+            "step_schedule": {"mode": sched.mode, "group_threads": sched.group_threads,
+                              "autotune_ms": {f"{m}/{g_}": round(v, 4) for (m, g_), v in tune_ms.items()}},
+            "scene_build_s": round(build_s, 1)}
+
+
 def run_ours(args, rank, world_size, local_rank):
     import torch
 
@@ -506,6 +605,9 @@ def run_ours(args, rank, world_size, local_rank):
                               args.warm_start_iterations)
         warm["plain_penetration_mm"] = plain_pen
         warm["vs_plain"] = warm["value"] / value
+    arm = None
+    if not args.no_articulated and world_size == 1:
+        arm = articulated_arm(dev, stream, flush, args.steps, args.warmup)
     del g
     if dist:
         dist.barrier()
@@ -564,6 +666,8 @@ def run_ours(args, rank, world_size, local_rank):
         line["cpu_baseline"] = cpu
     if warm is not None:
         line["warm_start"] = warm
+    if arm is not None:
+        line["articulated"] = arm
     print(json.dumps(line), flush=True)
 
 

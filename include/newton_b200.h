@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 13
+#define NB_ABI_VERSION 14
 
 enum {
     NB_OK = 0,
@@ -465,6 +465,8 @@ typedef struct NbAdjointIO {
                                     NB_STATUS_CONTACT_OVERFLOW) */
     int32_t pad0;
     uint32_t* status;            /* [1] NB_STATUS_* bits (sticky) */
+    double* grad_shape_mu;       /* [S] accumulated (+=) cotangent of shape_mu (the friction coefficient a
+                                    contact uses is the mean of its shapes'), or NULL */
 } NbAdjointIO;
 int nb_xpbd_step_adjoint(const NbModelDesc* model, const NbXpbdParams* params, const NbAdjointIO* io,
                          const NbContactSeg* seg, float dt, void* stream);

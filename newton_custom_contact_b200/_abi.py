@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 13
+NB_ABI_VERSION = 14
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -270,6 +270,7 @@ class NbAdjointIO(C.Structure):
         ("active_capacity", C.c_int32),
         ("pad0", C.c_int32),
         ("status", _fp),
+        ("grad_shape_mu", _fp),
     ]
 
 

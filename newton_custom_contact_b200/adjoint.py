@@ -16,8 +16,12 @@ substep at a time:
   runs the adjoint kernel over the segment's substeps in reverse.
 
 What is differentiated: free rigid bodies with contacts; gradients with
-respect to the initial ``body_q``, ``body_qd`` and a constant ``body_f``
-(applied at every substep).  Within a substep the contact set and the
+respect to the initial ``body_q``, ``body_qd``, a constant ``body_f``
+(applied at every substep) and, optionally, the shapes' friction
+coefficients ``shape_mu`` (a contact's coefficient is the mean of its two
+shapes', newton/_src/solvers/xpbd/kernels.py:2160-2178; a per-world friction
+is a differentiable map from world to shape coefficients that the caller
+builds in torch).  Within a substep the contact set and the
 contacts' body-frame points, offsets, normals and margins are held fixed,
 as are which contacts are active, the contact counts of the weighting and
 the friction-cone / velocity-threshold branches.  Not differentiated
@@ -67,10 +71,11 @@ class SubstepAdjoint:
         return self._bufs
 
     def __call__(self, contacts, body_q, body_qd, body_f, grad_q_out, grad_qd_out, dt: float,
-                 forward_out: tuple | None = None):
+                 forward_out: tuple | None = None, grad_shape_mu: torch.Tensor | None = None):
         """Cotangents (grad_body_q, grad_body_qd, grad_body_f) of one substep's inputs given those of its
         outputs; `contacts` as the step used them (after collide).  With `forward_out = (q, qd)` the
-        recomputed forward state is written there."""
+        recomputed forward state is written there; with `grad_shape_mu` (float64 [shape_count]) the
+        cotangent of the shapes' friction coefficients is added to it."""
         solver, m = self.solver, self.model
         _lib.require_cuda(m.device)
         if solver.enable_restitution:
@@ -91,6 +96,12 @@ class SubstepAdjoint:
                   "active_count", "status"):
             setattr(io, k, ptr(b[k]))
         io.active_capacity = b["active_capacity"]
+        if grad_shape_mu is not None:
+            if (grad_shape_mu.dtype != torch.float64 or not grad_shape_mu.is_contiguous()
+                    or grad_shape_mu.numel() != m.shape_count or grad_shape_mu.device != body_q.device):
+                raise TypeError("grad_shape_mu must be a contiguous float64 tensor of shape_count entries on the "
+                                "model device")
+            io.grad_shape_mu = ptr(grad_shape_mu)
         pipe, desc = solver._desc_for(contacts)
         if contacts is not None:
             if contacts._seg is None or not contacts._seg_valid:
@@ -147,8 +158,9 @@ class Rollout:
                 checkpoints.append((q.clone(), qd.clone()))
         return q, qd, checkpoints
 
-    def backward(self, checkpoints, f, substeps: int, gq, gqd):
+    def backward(self, checkpoints, f, substeps: int, gq, gqd, want_mu: bool = False):
         gf_total = torch.zeros_like(f)
+        gmu = torch.zeros(self.model.shape_count, dtype=torch.float64, device=f.device) if want_mu else None
         self.adjoint._alloc(self.contacts.rigid_contact_max)["status"].zero_()
         n_seg = len(checkpoints)
         for s in range(n_seg - 1, -1, -1):
@@ -165,41 +177,53 @@ class Rollout:
                 a.body_f.copy_(f)
                 self.pipe.collide(a, self.contacts)
                 gq, gqd, gf = self.adjoint(self.contacts, a.body_q, a.body_qd, a.body_f, gq.contiguous(),
-                                           gqd.contiguous(), self.dt)
+                                           gqd.contiguous(), self.dt, grad_shape_mu=gmu)
                 gf_total += gf
         st = self.adjoint.status()
         if st:
             raise RuntimeError(f"adjoint status bits 0x{st:x} (a world with an enabled non-free joint, or "
                                "active-contact overflow)")
-        return gq, gqd, gf_total
+        return gq, gqd, gf_total, gmu
 
 
 class _RolloutFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, body_q, body_qd, body_f, rollout, substeps):
+    def forward(ctx, body_q, body_qd, body_f, shape_mu, rollout, substeps):
+        if shape_mu is not None:
+            # the rollout runs with these coefficients: they become the model's
+            rollout.model.shape_material_mu.copy_(shape_mu.detach().to(torch.float32))
         q, qd, checkpoints = rollout.forward(body_q.detach().contiguous(), body_qd.detach().contiguous(),
                                              body_f.detach().contiguous(), substeps)
         ctx.rollout, ctx.substeps, ctx.checkpoints = rollout, substeps, checkpoints
         ctx.body_f = body_f.detach().contiguous()
+        ctx.want_mu = shape_mu is not None and shape_mu.requires_grad
+        ctx.mu_dtype = shape_mu.dtype if shape_mu is not None else None
         return q, qd
 
     @staticmethod
     def backward(ctx, gq, gqd):
         gq = torch.zeros_like(ctx.checkpoints[0][0]) if gq is None else gq
         gqd = torch.zeros_like(ctx.checkpoints[0][1]) if gqd is None else gqd
-        g_q, g_qd, g_f = ctx.rollout.backward(ctx.checkpoints, ctx.body_f, ctx.substeps, gq.float(), gqd.float())
-        return g_q, g_qd, g_f, None, None
+        g_q, g_qd, g_f, g_mu = ctx.rollout.backward(ctx.checkpoints, ctx.body_f, ctx.substeps, gq.float(), gqd.float(),
+                                                    want_mu=ctx.want_mu)
+        if g_mu is not None:
+            g_mu = g_mu.to(ctx.mu_dtype)
+        return g_q, g_qd, g_f, g_mu, None, None
 
 
 def simulate(pipeline, solver, body_q: torch.Tensor, body_qd: torch.Tensor, body_f: torch.Tensor | None = None,
              substeps: int = 1, dt: float = 1.0 / 480.0, checkpoint_every: int = 16,
-             rollout: Rollout | None = None):
+             rollout: Rollout | None = None, shape_mu: torch.Tensor | None = None):
     """`substeps` substeps of collide + ``solver.step`` from (body_q, body_qd) with the constant body
     force `body_f`; returns (body_q, body_qd) after the last substep, differentiable with respect to
-    the three inputs."""
+    the three inputs.  With `shape_mu` ([shape_count]), the rollout uses those friction coefficients
+    (they are copied into ``model.shape_material_mu``) and the result is differentiable with respect
+    to them too."""
     m = solver.model
     if body_f is None:
         body_f = torch.zeros((m.body_count, 6), dtype=torch.float32, device=body_q.device)
+    if shape_mu is not None and shape_mu.shape != (m.shape_count,):
+        raise ValueError(f"shape_mu must have shape ({m.shape_count},)")
     if rollout is None:
         rollout = Rollout(pipeline, solver, dt, checkpoint_every)
-    return _RolloutFn.apply(body_q, body_qd, body_f, rollout, int(substeps))
+    return _RolloutFn.apply(body_q, body_qd, body_f, shape_mu, rollout, int(substeps))

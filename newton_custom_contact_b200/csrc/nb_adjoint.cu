@@ -343,9 +343,10 @@ struct ContactC {
 
 // solve_body_contact_positions (kernels.py:2062-2298) for one contact:
 // deltas (linear, angular) of A and B; false when the contact is inactive
+// (mu: the contact's friction coefficient c.mu, as a T so that its derivative can be carried)
 template <class T>
 __device__ __forceinline__ bool contact_g(const ContactC& c, const BodyT<T>& A, const BodyT<T>& B, float relaxation, float dt,
-                          V3T<T>& lin_da, V3T<T>& ang_da, V3T<T>& lin_db, V3T<T>& ang_db) {
+                          V3T<T>& lin_da, V3T<T>& ang_da, V3T<T>& lin_db, V3T<T>& ang_db, const T& mu) {
     const V3T<T> bxa0 = qrott(A.r, vc<T>(c.p0)) + A.p;
     const V3T<T> bxb0 = qrott(B.r, vc<T>(c.p1)) + B.p;
     const V3T<T> n = vc<T>(c.n);
@@ -387,7 +388,7 @@ __device__ __forceinline__ bool contact_g(const ContactC& c, const BodyT<T>& A, 
         if (val(err) > 0.0f) {
             T lf = constraint_delta_g(err, A.r, B.r, c.m_inv_a, c.m_inv_b, c.Ia, c.Ib, -perp, perp, ang_a, ang_b,
                                       relaxation, dt);
-            lf = maxv(lf, -lambda_n * c.mu);
+            lf = maxv(lf, -lambda_n * mu);
             lin_da = lin_da - vmul(perp, lf);
             lin_db = lin_db + vmul(perp, lf);
             ang_da = ang_da + vmul(ang_a, lf);
@@ -659,7 +660,7 @@ __device__ __forceinline__ void vjp_contact(const ContactC& c, const float* sa, 
         B.v = {Dual<kDirs>(sb[7]), Dual<kDirs>(sb[8]), Dual<kDirs>(sb[9])};
         B.w = {seed<kDirs>(sb[10], 17, j0), seed<kDirs>(sb[11], 18, j0), seed<kDirs>(sb[12], 19, j0)};
         V3T<Dual<kDirs>> la, aa, lb, ab;
-        if (!contact_g(c, A, B, relaxation, dt, la, aa, lb, ab)) return;
+        if (!contact_g(c, A, B, relaxation, dt, la, aa, lb, ab, Dual<kDirs>(c.mu))) return;
         const Dual<kDirs> o[12] = {la.x, la.y, la.z, aa.x, aa.y, aa.z, lb.x, lb.y, lb.z, ab.x, ab.y, ab.z};
 #pragma unroll
         for (int k = 0; k < kDirs && j0 + k < 20; ++k) {
@@ -674,6 +675,22 @@ __device__ __forceinline__ void vjp_contact(const ContactC& c, const float* sa, 
             else gb[j - 7] += acc;
         }
     }
+}
+
+// contact: the derivative of the four deltas along the contact's friction coefficient, contracted with
+// their cotangents (one forward-mode direction; nonzero where the friction cone clamps)
+__device__ __forceinline__ float vjp_contact_mu(const ContactC& c, const float* sa, const float* sb, float relaxation,
+                                                float dt, const float* gout) {
+    const BodyT<Dual<1>> A = body_from<Dual<1>>(sa), B = body_from<Dual<1>>(sb);
+    Dual<1> mu(c.mu);
+    mu.d[0] = 1.0f;
+    V3T<Dual<1>> la, aa, lb, ab;
+    if (!contact_g(c, A, B, relaxation, dt, la, aa, lb, ab, mu)) return 0.0f;
+    const Dual<1> o[12] = {la.x, la.y, la.z, aa.x, aa.y, aa.z, lb.x, lb.y, lb.z, ab.x, ab.y, ab.z};
+    float acc = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) acc += gout[i] * o[i].d[0];
+    return acc;
 }
 
 // ---------------------------------------------------------------- the per-world kernel
@@ -824,7 +841,7 @@ __global__ void __launch_bounds__(kThreads) adjoint_forward_kernel(NbModelDesc m
             side_state(S_it, b0, c.lb, sb);
             V3T<float> la, aa, lb, ab;
             if (!contact_g(c, body_from<float>(sa), body_from<float>(sb), p.rigid_contact_relaxation, dt, la, aa, lb,
-                           ab))
+                           ab, c.mu))
                 return false;
             ends = nb::ends_pack(c.la, c.lb);
             return true;
@@ -836,7 +853,8 @@ __global__ void __launch_bounds__(kThreads) adjoint_forward_kernel(NbModelDesc m
             side_state(S_it, b0, c.la, sa);
             side_state(S_it, b0, c.lb, sb);
             V3T<float> la, aa, lb, ab;
-            contact_g(c, body_from<float>(sa), body_from<float>(sb), p.rigid_contact_relaxation, dt, la, aa, lb, ab);
+            contact_g(c, body_from<float>(sa), body_from<float>(sb), p.rigid_contact_relaxation, dt, la, aa, lb, ab,
+                      c.mu);
             // the reverse pass differentiates this iteration's active contacts only
             const int slot = atomicAdd(io.active_count + it, 1);
             if (slot < io.active_capacity) {
@@ -949,6 +967,16 @@ __global__ void __launch_bounds__(kThreads) adjoint_contacts_kernel(NbModelDesc 
         }
         float ga[13] = {}, gb[13] = {};
         vjp_contact(c, sa, sb, p.rigid_contact_relaxation, dt, gout, ga, gb);
+        if (io.grad_shape_mu && c.mu > 0.0f) {
+            // the contact's mu is the mean of its shapes' (kernels.py:2160-2178)
+            const float gmu = vjp_contact_mu(c, sa, sb, p.rigid_contact_relaxation, dt, gout);
+            if (gmu != 0.0f) {
+                const int s0 = __float_as_int(r[3].w), s1 = __float_as_int(r[4].w);
+                const int nz = (s0 >= 0) + (s1 >= 0);
+                if (s0 >= 0) atomicAdd(io.grad_shape_mu + s0, (double)gmu / nz);
+                if (s1 >= 0) atomicAdd(io.grad_shape_mu + s1, (double)gmu / nz);
+            }
+        }
         if (dyn_a)
             for (int q = 0; q < 13; ++q)
                 if (ga[q] != 0.0f) atomicAdd(io.grad_acc + 13 * (size_t)(b0 + c.la) + q, (double)ga[q]);
