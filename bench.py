@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned-warm-start arm")
     ap.add_argument("--warm-start-iterations", type=int, default=2)
     ap.add_argument("--no-articulated", action="store_true", help="skip the articulated (C3) batch")
+    ap.add_argument("--warm-start-sweep", default="", metavar="K1,K2,...",
+                    help="also time the plain and the warm-started forms at these iteration counts")
     ap.add_argument("--step-schedule", default=None, metavar="MODE/G",
                     help="fix the step schedule (e.g. groups_compact/32) instead of autotuning it; a run "
                          "under a profiler serialises launches, so its autotuner may pick another schedule")
@@ -435,6 +437,64 @@ def articulated_arm(dev, stream, flush, steps, warmup):
             "scene_build_s": round(build_s, 1)}
 
 
+def plain_arm(model, dt, substeps, sched, stream, flush, steps, warmup, iterations):
+    """The plain form with `iterations` iterations on the same scene and frames (for the warm-start
+    sweep): timed like the main workload, penetration statistics along one pass of the window."""
+    import torch
+
+    from newton_custom_contact_b200 import CollisionPipeline, SolverXPBD
+
+    pipe = CollisionPipeline(model)
+    pipe.set_step_schedule(sched.group_threads, sched.mode)
+    solver = SolverXPBD(model, iterations=iterations)
+    a, b = model.state(), model.state()
+    c = pipe.contacts()
+
+    def frame():
+        x, y = a, b
+        for _ in range(substeps):
+            x.clear_forces()
+            pipe.collide(x, c)
+            solver.step(x, y, None, c, dt)
+            x, y = y, x
+
+    with torch.cuda.stream(stream):
+        for _ in range(WINDOW_START):
+            frame()
+    torch.cuda.synchronize()
+    restore = _state_snapshot([a.body_q, a.body_qd])
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        frame()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        restore()
+    pen = _window_penetration(g, stream, model, c, a, WINDOW_FRAMES)
+    ms = time_windows(g, stream, restore, flush, steps, warmup)
+    del g
+    units = model.world_count * substeps * WINDOW_FRAMES * steps
+    return {"iterations": iterations, "value": units / (ms / 1e3), "ms_per_step": ms / steps,
+            "penetration_mm": _pen_summary(pen)}
+
+
+def warm_start_sweep(model, dt, substeps, sched, stream, flush, steps, warmup, iterations):
+    """Plain and warm-started forms at each of `iterations` on the same frames: throughput and
+    penetration, and for each warm-started form the plain form it matches or beats on the mean of the
+    per-frame largest penetration, with the throughput ratio."""
+    plain = [plain_arm(model, dt, substeps, sched, stream, flush, steps, warmup, k) for k in iterations]
+    warm = [warm_start_arm(model, dt, substeps, sched, stream, flush, steps, warmup, k) for k in iterations]
+    ref8 = next((p for p in plain if p["iterations"] == 8), plain[-1])
+    best = None
+    for w in warm:
+        if w["penetration_mm"]["max"] <= ref8["penetration_mm"]["max"]:
+            r = w["value"] / ref8["value"]
+            if best is None or r > best["throughput_vs_plain"]:
+                best = {"warm_iterations": w["iterations"], "throughput_vs_plain": r,
+                        "plain_iterations": ref8["iterations"]}
+    return {"plain": plain, "warm_start": warm, "best_at_equal_max_penetration": best,
+            "penetration_metric": "mean over frames 6..35 of each frame's largest penetration [mm]"}
+
+
 def run_ours(args, rank, world_size, local_rank):
     import torch
 
@@ -605,6 +665,10 @@ def run_ours(args, rank, world_size, local_rank):
                               args.warm_start_iterations)
         warm["plain_penetration_mm"] = plain_pen
         warm["vs_plain"] = warm["value"] / value
+    sweep = None
+    if args.warm_start_sweep and world_size == 1:
+        its = [int(x) for x in args.warm_start_sweep.split(",")]
+        sweep = warm_start_sweep(model, dt, substeps, sched, stream, flush, args.steps, args.warmup, its)
     arm = None
     if not args.no_articulated and world_size == 1:
         arm = articulated_arm(dev, stream, flush, args.steps, args.warmup)
@@ -668,6 +732,8 @@ def run_ours(args, rank, world_size, local_rank):
         line["warm_start"] = warm
     if arm is not None:
         line["articulated"] = arm
+    if sweep is not None:
+        line["warm_start_sweep"] = sweep
     print(json.dumps(line), flush=True)
 
 

@@ -1,7 +1,8 @@
 // Device-side fp32 vector / quaternion / transform helpers with Warp's builtin
 // semantics (quat = x,y,z,w; transform = p,q; spatial_vector = top,bottom).
 // Every expression keeps the reference call sites' evaluation order; the
-// library is compiled with --fmad=false so no a*b+c is contracted.
+// parity build of the library is compiled with --fmad=false, so no a*b+c is
+// contracted there (the product build lets the compiler contract them).
 #pragma once
 #include <cstdint>
 
@@ -163,20 +164,3 @@ NB_D TF tf_inverse(TF t) {
     return TF{neg(qrot(qi, t.p)), qi};
 }
 
-// ------------------------------------------------------------ fixed point
-// Per-body deltas are summed as int64 in units of 2^-32: exact and therefore
-// independent of the order in which contacts (threads) contribute.
-#define NB_FX_SCALE 4294967296.0f
-#define NB_FX_INV (1.0f / 4294967296.0f)
-#define NB_FX_LIMIT 9.0e18f
-
-NB_D long long fx_quant(float x, unsigned* bad) {
-    float y = x * NB_FX_SCALE;
-    if (!(fabsf(y) < NB_FX_LIMIT)) {
-        *bad |= 1u;
-        if (y != y) y = 0.0f;
-        else y = y > 0.0f ? NB_FX_LIMIT : -NB_FX_LIMIT;
-    }
-    return __float2ll_rn(y);
-}
-NB_D float fx_float(long long v) { return __ll2float_rn(v) * NB_FX_INV; }
