@@ -471,8 +471,11 @@ __device__ __noinline__ bool gjk_pair_separated(const Geom& a, const Geom& b) {
 
 // One thread per MPR/GJK item: provably separated pairs get zero contacts,
 // the rest are compacted (warp-aggregated) into the queue's front, which the
-// analytic kernel has consumed; front and back cannot overlap (the back holds
-// at most pair_count items of 2 * pair_count).
+// analytic kernel has consumed: box-box items from index 0 up, every other
+// pair type from index n1 - 1 down, so the MPR/GJK kernel's warps mostly run
+// one pair type (fewer divergent branches, one code path in the instruction
+// cache).  Front and back cannot overlap (the back holds n1 <= pair_count
+// items of 2 * pair_count).
 __global__ void __launch_bounds__(kNT)
 gjk_prefilter_kernel(NbModelDesc m, NbContactSeg seg) {
     const int n1 = seg.work_counter[3];
@@ -483,7 +486,7 @@ gjk_prefilter_kernel(NbModelDesc m, NbContactSeg seg) {
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n1; base += stride) {
         const int i = base + lane;
-        bool keep = false;
+        bool keep = false, boxes = false;
         int2 e = make_int2(0, 0);
         if (i < n1) {
             e = queue[2 * (size_t)P - 1 - i];
@@ -493,14 +496,21 @@ gjk_prefilter_kernel(NbModelDesc m, NbContactSeg seg) {
             const int nloc = m.world_shape_start[e.y + 1] - s0;
             const int sa = la < nloc ? s0 + la : m.global_shapes[la - nloc];
             const int sb = lb < nloc ? s0 + lb : m.global_shapes[lb - nloc];
-            keep = !gjk_pair_separated(load_geom(geom + 5 * (size_t)sa, sa), load_geom(geom + 5 * (size_t)sb, sb));
+            const Geom ga = load_geom(geom + 5 * (size_t)sa, sa), gb = load_geom(geom + 5 * (size_t)sb, sb);
+            keep = !gjk_pair_separated(ga, gb);
+            boxes = ga.type == NB_GEO_BOX && gb.type == NB_GEO_BOX;
             if (!keep) seg.counts[e.x] = 0;
         }
-        const unsigned bal = __ballot_sync(kFull, keep);
-        int off = 0;
-        if (lane == 0 && bal) off = atomicAdd(&seg.work_counter[5], __popc(bal));
-        off = __shfl_sync(kFull, off, 0);
-        if (keep) queue[off + __popc(bal & ((1u << lane) - 1u))] = e;
+        const unsigned below = (1u << lane) - 1u;
+        const unsigned bal0 = __ballot_sync(kFull, keep && boxes);
+        const unsigned bal1 = __ballot_sync(kFull, keep && !boxes);
+        int off0 = 0, off1 = 0;
+        if (lane == 0 && bal0) off0 = atomicAdd(&seg.work_counter[5], __popc(bal0));
+        if (lane == 0 && bal1) off1 = atomicAdd(&seg.work_counter[6], __popc(bal1));
+        off0 = __shfl_sync(kFull, off0, 0);
+        off1 = __shfl_sync(kFull, off1, 0);
+        if (keep && boxes) queue[off0 + __popc(bal0 & below)] = e;
+        if (keep && !boxes) queue[n1 - 1 - (off1 + __popc(bal1 & below))] = e;
     }
 }
 
@@ -510,11 +520,12 @@ gjk_prefilter_kernel(NbModelDesc m, NbContactSeg seg) {
 // (collide 0.57 vs 0.72 ms per substep on 4096 uneven worlds).
 __global__ void __launch_bounds__(kNT, kGjkMinBlocks)
 narrow_gjk_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
-    const int n = seg.work_counter[5];
+    const int n_box = seg.work_counter[5], n_other = seg.work_counter[6], n1 = seg.work_counter[3];
+    const int n = n_box + n_other;
     const int2* queue = reinterpret_cast<const int2*>(seg.queue);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         NarrowItem it;
-        narrow_setup(m, seg, body_q, queue[i], it);
+        narrow_setup(m, seg, body_q, i < n_box ? queue[i] : queue[n1 - 1 - (i - n_box)], it);
         gjk_pair(it.wr, it.ga, it.gb);
         narrow_finish(seg, it);
     }
@@ -760,7 +771,7 @@ cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const N
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(seg->work_counter, 0, 4 * sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(seg->work_counter + 5, 0, sizeof(int32_t), stream);
+    e = cudaMemsetAsync(seg->work_counter + 5, 0, 2 * sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
     const int sms = sm_count();
     broadphase_kernel<<<sms * 4, kBT, smem, stream>>>(*m, body_q, *seg);

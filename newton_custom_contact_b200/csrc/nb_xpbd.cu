@@ -988,6 +988,58 @@ __device__ __forceinline__ void warm_start(const NbModelDesc& m, const NbStepIO&
     group_sync<G>(g);
 }
 
+// A world's bodies are a contiguous block of every per-body array, so the
+// group stages them with linear loads: element e of a K-float-per-body block
+// (body e / K, component e % K) lands in the structure-of-arrays slab at
+// dst[(e % K) * nb + e / K].  The block is read as float4 from its first
+// 16-byte boundary on (head and tail elements one by one), so consecutive
+// threads read consecutive 16-byte words.
+template <int G, int K>
+__device__ __forceinline__ void stage_block(const float* __restrict__ src, int nb, float* dst, int t) {
+    const int n = K * nb;
+    const int head = min((int)(((16u - ((unsigned)(uintptr_t)src & 15u)) & 15u) >> 2), n);
+    auto put = [&](int e, float v) { dst[(e % K) * nb + e / K] = v; };
+    if (t < head) put(t, __ldg(src + t));
+    const float4* s4 = reinterpret_cast<const float4*>(src + head);
+    const int n4 = (n - head) >> 2;
+    for (int j = t; j < n4; j += G) {
+        const float4 v = __ldg(s4 + j);
+        const int e = head + 4 * j;
+        put(e, v.x);
+        put(e + 1, v.y);
+        put(e + 2, v.z);
+        put(e + 3, v.w);
+    }
+    for (int e = head + 4 * n4 + t; e < n; e += G) put(e, __ldg(src + e));
+}
+
+// The write-back of a K-float-per-body block from the slab (component k of
+// body i at src[k * nb + i]) with float4 stores from the first 16-byte boundary
+// on.  Kinematic bodies keep their input row (keep[e] from `in`); a non-finite
+// value of another body sets *bad.
+template <int G, int K, class SB>
+__device__ __forceinline__ void write_block(const SB& S, const float* src, const float* __restrict__ in, float* dst,
+                                            int t, unsigned* bad) {
+    const int nb = S.nb;
+    const int n = K * nb;
+    const int head = min((int)(((16u - ((unsigned)(uintptr_t)dst & 15u)) & 15u) >> 2), n);
+    auto get = [&](int e) -> float {
+        const int i = e / K;
+        if (S.flags[i] & NB_BODY_KINEMATIC) return in[e];
+        const float x = src[(e % K) * nb + i];
+        if (!isfinite(x)) *bad |= 2u;
+        return x;
+    };
+    if (t < head) dst[t] = get(t);
+    float4* d4 = reinterpret_cast<float4*>(dst + head);
+    const int n4 = (n - head) >> 2;
+    for (int j = t; j < n4; j += G) {
+        const int e = head + 4 * j;
+        d4[j] = make_float4(get(e), get(e + 1), get(e + 2), get(e + 3));
+    }
+    for (int e = head + 4 * n4 + t; e < n; e += G) dst[e] = get(e);
+}
+
 // One world's substep with a group of G threads: stage, joint forces,
 // integrate, `iterations` x (contacts, weighted apply, joints, apply),
 // restitution, write-back.  The caller carved the world's slab into S.
@@ -1008,17 +1060,15 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
     const float4* rec = reinterpret_cast<const float4*>(seg.rec);
     const int b0 = S.b0;
     const int nb = S.nb;
-    // ---- stage bodies (body_f + joint forces go to frc, aliased on acc)
+    // ---- stage bodies (body_f + joint forces go to frc, aliased on acc): the
+    // world's pose, twist and force blocks with linear, coalesced loads
+    stage_block<G, 7>(io.body_q_in + 7 * (size_t)b0, nb, S.f, t);
+    stage_block<G, 6>(io.body_qd_in + 6 * (size_t)b0, nb, S.f + 7 * nb, t);
+    stage_block<G, 6>(io.body_f_in + 6 * (size_t)b0, nb, S.frc, t);
     for (int i = t; i < nb; i += G) {
         const int bi = b0 + i;
         const int fl = m.body_flags[bi];
         S.flags[i] = fl;
-        const float* q = io.body_q_in + 7 * (size_t)bi;
-        const float* qd = io.body_qd_in + 6 * (size_t)bi;
-        for (int k = 0; k < 7; ++k) S.f[k * nb + i] = q[k];
-        for (int k = 0; k < 6; ++k) S.f[(7 + k) * nb + i] = qd[k];
-        const float* fb = io.body_f_in + 6 * (size_t)bi;
-        for (int k = 0; k < 6; ++k) S.frc[k * nb + i] = fb[k];
         if constexpr (!SB::compact) {
             const bool kin = (fl & NB_BODY_KINEMATIC) != 0;
             for (int k = 0; k < 3; ++k) S.c[k * nb + i] = m.body_com[3 * (size_t)bi + k];
@@ -1176,29 +1226,10 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
         }
         group_sync<G>(g);
     }
-    // ---- write back (kinematic bodies pass through unchanged)
-    for (int i = t; i < nb; i += G) {
-        const int bi = b0 + i;
-        float* qo = io.body_q_out + 7 * (size_t)bi;
-        float* qdo = io.body_qd_out + 6 * (size_t)bi;
-        if (S.flags[i] & NB_BODY_KINEMATIC) {
-            for (int k = 0; k < 7; ++k) qo[k] = io.body_q_in[7 * (size_t)bi + k];
-            for (int k = 0; k < 6; ++k) qdo[k] = io.body_qd_in[6 * (size_t)bi + k];
-            continue;
-        }
-        bool finite = true;
-        for (int k = 0; k < 7; ++k) {
-            float x = S.f[k * nb + i];
-            finite = finite && isfinite(x);
-            qo[k] = x;
-        }
-        for (int k = 0; k < 6; ++k) {
-            float x = S.f[(7 + k) * nb + i];
-            finite = finite && isfinite(x);
-            qdo[k] = x;
-        }
-        if (!finite) bad |= 2u;
-    }
+    // ---- write back with linear, coalesced stores (kinematic bodies pass through unchanged)
+    group_sync<G>(g);
+    write_block<G, 7>(S, S.f, io.body_q_in + 7 * (size_t)b0, io.body_q_out + 7 * (size_t)b0, t, &bad);
+    write_block<G, 6>(S, S.f + 7 * nb, io.body_qd_in + 6 * (size_t)b0, io.body_qd_out + 6 * (size_t)b0, t, &bad);
     if (bad) atomicOr(s_bad, bad);
 }
 
