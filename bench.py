@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--step-schedule", default=None, metavar="MODE/G",
                     help="fix the step schedule (e.g. groups_compact/32) instead of autotuning it; a run "
                          "under a profiler serialises launches, so its autotuner may pick another schedule")
+    ap.add_argument("--build", default="product", choices=["product", "exact"],
+                    help="library build: product (FMA contraction in the solver) or exact (the parity build)")
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="weak: every rank simulates its own --worlds scene; strong: the ranks split one scene")
     return ap.parse_args()
@@ -498,8 +500,9 @@ def warm_start_sweep(model, dt, substeps, sched, stream, flush, steps, warmup, i
 def run_ours(args, rank, world_size, local_rank):
     import torch
 
-    from newton_custom_contact_b200 import CollisionPipeline, SolverXPBD, scenes
+    from newton_custom_contact_b200 import CollisionPipeline, SolverXPBD, _lib, scenes
 
+    _lib.use_build(args.build)
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     dist = None
@@ -578,14 +581,16 @@ def run_ours(args, rank, world_size, local_rank):
     n_contacts_acc = torch.zeros((), dtype=torch.float64, device=dev)
     with torch.cuda.stream(stream):
         restore()
-        # keep the host ahead of the device, so no launch gap falls between a pair of events
-        torch.cuda._sleep(50_000_000)
         h = _lib.stream_handle(dev)
         desc = pipe.desc()
         seg = pipe.seg_struct(contacts)
         pub = pipe.public_struct(contacts)
         a, b = s0, s1
         for i in range(n_sub):
+            if i % substeps == 0:
+                # keep the host ahead of the device (a frame's launches take the host a few ms), so no
+                # launch gap falls between a pair of events; short enough for the launch queue
+                torch.cuda._sleep(20_000_000)
             ev = evs[i]
             a.clear_forces()
             ev[0].record(stream)
@@ -705,7 +710,7 @@ def run_ours(args, rank, world_size, local_rank):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": args.scaling,
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
         "config": {"workload": WORKLOAD, "worlds_per_gpu": model.world_count, "bodies_per_gpu": model.body_count,
-                   "substeps": substeps, "iterations": iters, "form": "plain XPBD",
+                   "substeps": substeps, "iterations": iters, "form": "plain XPBD", "build": args.build,
                    "l2": "256 MiB buffer written before every timed step; the frame's working set (pair "
                          "lists, contact slots and records, body state) is larger than L2",
                    "cuda_graph": True,

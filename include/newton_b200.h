@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 14
+#define NB_ABI_VERSION 16
 
 enum {
     NB_OK = 0,
@@ -99,6 +99,12 @@ typedef struct NbModelDesc {
     int32_t max_world_pairs;
     int32_t all_joints_free;      /* 1: every joint is FREE (no joint constraints: the step may use its
                                      lean kernel); 0: unknown or not */
+    int32_t broad_phase;          /* 0: test every pair of the world's pair list; 1: sweep and prune
+                                     (broad_phase_sap.py): sort the world's AABBs along x, sweep, and
+                                     keep the overlaps that are in the pair list -- the same candidate
+                                     set, O(n log n + overlaps) per world of up to 256 shape slots
+                                     (larger worlds test every pair) */
+    int32_t pad_bp;
     int64_t contact_capacity;     /* contact slots = 5 * pair_count */
 
     /* bodies [B] */
@@ -441,6 +447,17 @@ int nb_ws_adam(float* w, const float* grad, float* m1, float* m2, int64_t count,
  * enabled non-free joint is skipped with NB_STATUS_ADJOINT_UNSUPPORTED;
  * restitution returns NB_ERR_UNSUPPORTED.  The forward pass is recomputed
  * inside (optionally written to body_q_out / body_qd_out).
+ *
+ * Branches.  The substep is piecewise smooth: per iteration, which contacts
+ * are active (depth < 0), whether friction, torsional and rolling friction
+ * are clamped to their cones, and whether a body's speeds fall under the
+ * 1e-4 rest threshold.  The cotangents are those of the piece the forward
+ * pass is on.  branch_mode 1 writes the forward pass's branches (one byte per
+ * contact record and iteration, one per body and iteration); branch_mode 2
+ * takes them from those arrays instead of evaluating them, so that a finite
+ * difference around a recorded substep stays on its piece; it requires
+ * forward_only, which runs the forward pass alone (body_q_out / body_qd_out
+ * required; the cotangent pointers and grad_acc may be NULL).
  */
 typedef struct NbAdjointIO {
     const float* body_q_in;      /* [B,7] the step's input state */
@@ -467,6 +484,13 @@ typedef struct NbAdjointIO {
     uint32_t* status;            /* [1] NB_STATUS_* bits (sticky) */
     double* grad_shape_mu;       /* [S] accumulated (+=) cotangent of shape_mu (the friction coefficient a
                                     contact uses is the mean of its shapes'), or NULL */
+    uint8_t* branch_contact;     /* [iterations * model->contact_capacity] branches of each contact record
+                                    (bit 0 active, 1/2 friction error > 0 / clamped, 3/4/5 torsion error != 0
+                                    / clamped low / high, 6/7 rolling error > 0 / clamped), or NULL */
+    uint8_t* branch_body;        /* [iterations * B] rest thresholds of each body update (bits 0/1 linear /
+                                    angular speed zeroed; 2/3 the same in the joint pass's update), or NULL */
+    int32_t branch_mode;         /* 0 evaluate, 1 evaluate and record, 2 replay the recorded branches */
+    int32_t forward_only;        /* nonzero: the forward pass only */
 } NbAdjointIO;
 int nb_xpbd_step_adjoint(const NbModelDesc* model, const NbXpbdParams* params, const NbAdjointIO* io,
                          const NbContactSeg* seg, float dt, void* stream);
@@ -484,8 +508,10 @@ int nb_contact_forces(const float* contact_impulse, const int32_t* count, int32_
  * Move contacts a caller wrote into the dense public arrays (custom contact
  * writers) into solver records, bucketed by world.  Replaces nothing in the
  * reference (its solver reads the dense arrays directly,
- * xpbd/kernels.py:2062-2298); the record order inside a world does not change
- * the solver's result because per-body deltas are summed exactly.
+ * xpbd/kernels.py:2062-2298).  Records keep the public order within each
+ * world, and the solver sums each body's deltas in record order, so a caller
+ * that writes the same contacts in another order changes the bodies' sums by
+ * float rounding only.
  */
 int nb_ingest_contacts(const NbModelDesc* model, const NbContactsPublic* pub,
                        const NbContactSeg* seg, void* stream);

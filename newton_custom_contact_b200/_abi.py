@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 14
+NB_ABI_VERSION = 16
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -91,6 +91,8 @@ class NbModelDesc(C.Structure):
         ("max_world_joints", C.c_int32),
         ("max_world_pairs", C.c_int32),
         ("all_joints_free", C.c_int32),
+        ("broad_phase", C.c_int32),
+        ("pad_bp", C.c_int32),
         ("contact_capacity", C.c_int64),
         ("body_com", _fp),
         ("body_mass", _fp),
@@ -271,6 +273,10 @@ class NbAdjointIO(C.Structure):
         ("pad0", C.c_int32),
         ("status", _fp),
         ("grad_shape_mu", _fp),
+        ("branch_contact", _fp),
+        ("branch_body", _fp),
+        ("branch_mode", C.c_int32),
+        ("forward_only", C.c_int32),
     ]
 
 

@@ -78,30 +78,77 @@ class SubstepAdjoint:
         cotangent of the shapes' friction coefficients is added to it."""
         solver, m = self.solver, self.model
         _lib.require_cuda(m.device)
-        if solver.enable_restitution:
-            raise NotImplementedError("the adjoint does not differentiate restitution")
         B = m.body_count
         for name, t, shape in (("body_q", body_q, (B, 7)), ("body_qd", body_qd, (B, 6)), ("body_f", body_f, (B, 6)),
                                ("grad_q_out", grad_q_out, (B, 7)), ("grad_qd_out", grad_qd_out, (B, 6))):
             solver._check_state(name, t, shape)
-        b = self._alloc(contacts.rigid_contact_max if contacts is not None else 0)
         gq, gqd, gf = torch.empty_like(body_q), torch.empty_like(body_qd), torch.empty_like(body_f)
-        io = NbAdjointIO()
-        io.body_q_in, io.body_qd_in, io.body_f_in = ptr(body_q), ptr(body_qd), ptr(body_f)
+        io = self._io(contacts, body_q, body_qd, body_f)
         io.grad_q_out, io.grad_qd_out = ptr(grad_q_out), ptr(grad_qd_out)
         io.grad_q_in, io.grad_qd_in, io.grad_f_in = ptr(gq), ptr(gqd), ptr(gf)
         if forward_out is not None:
             io.body_q_out, io.body_qd_out = ptr(forward_out[0]), ptr(forward_out[1])
-        for k in ("tape_state", "tape_delta", "tape_weight", "grad_acc", "delta_acc", "count_acc", "active",
-                  "active_count", "status"):
-            setattr(io, k, ptr(b[k]))
-        io.active_capacity = b["active_capacity"]
         if grad_shape_mu is not None:
             if (grad_shape_mu.dtype != torch.float64 or not grad_shape_mu.is_contiguous()
                     or grad_shape_mu.numel() != m.shape_count or grad_shape_mu.device != body_q.device):
                 raise TypeError("grad_shape_mu must be a contiguous float64 tensor of shape_count entries on the "
                                 "model device")
             io.grad_shape_mu = ptr(grad_shape_mu)
+        self._launch(contacts, io, dt)
+        return gq, gqd, gf
+
+    def branch_buffers(self, contacts):
+        """Zeroed (contact, body) branch arrays of one substep for ``forward(..., branches=...)``: one byte
+        per contact record and iteration, one per body and iteration."""
+        m, K = self.model, max(self.solver.iterations, 1)
+        pipe, desc = self.solver._desc_for(contacts)
+        ncap = int(desc.contact_capacity) if contacts is not None else 0
+        dev = m.device
+        return (torch.zeros(K * max(ncap, 1), dtype=torch.uint8, device=dev),
+                torch.zeros(K * max(m.body_count, 1), dtype=torch.uint8, device=dev))
+
+    def forward(self, contacts, body_q, body_qd, body_f, dt: float, q_out, qd_out, branches=None,
+                replay: bool = False) -> None:
+        """The adjoint's forward pass alone: one substep from (body_q, body_qd) into (q_out, qd_out), equal
+        to ``solver.step`` on the same contacts.  With `branches` (from ``branch_buffers``) it records the
+        substep's branch decisions there, or, with `replay`, takes them from there: a finite difference
+        whose two sides replay the nominal substep's branches stays on the piece whose derivative the
+        adjoint computes."""
+        m = self.model
+        _lib.require_cuda(m.device)
+        B = m.body_count
+        for name, t, shape in (("body_q", body_q, (B, 7)), ("body_qd", body_qd, (B, 6)), ("body_f", body_f, (B, 6)),
+                               ("q_out", q_out, (B, 7)), ("qd_out", qd_out, (B, 6))):
+            self.solver._check_state(name, t, shape)
+        if replay and branches is None:
+            raise ValueError("replay needs the recorded branches")
+        io = self._io(contacts, body_q, body_qd, body_f)
+        io.body_q_out, io.body_qd_out = ptr(q_out), ptr(qd_out)
+        io.forward_only = 1
+        if branches is not None:
+            bc, bb = branches
+            want = self.branch_buffers(contacts)
+            for t, w in ((bc, want[0]), (bb, want[1])):
+                if t.dtype != torch.uint8 or not t.is_contiguous() or t.numel() != w.numel() or t.device != w.device:
+                    raise TypeError("branches must be the uint8 arrays branch_buffers() returns")
+            io.branch_contact, io.branch_body = ptr(bc), ptr(bb)
+            io.branch_mode = 2 if replay else 1
+        self._launch(contacts, io, dt)
+
+    def _io(self, contacts, body_q, body_qd, body_f) -> NbAdjointIO:
+        if self.solver.enable_restitution:
+            raise NotImplementedError("the adjoint does not differentiate restitution")
+        b = self._alloc(contacts.rigid_contact_max if contacts is not None else 0)
+        io = NbAdjointIO()
+        io.body_q_in, io.body_qd_in, io.body_f_in = ptr(body_q), ptr(body_qd), ptr(body_f)
+        for k in ("tape_state", "tape_delta", "tape_weight", "grad_acc", "delta_acc", "count_acc", "active",
+                  "active_count", "status"):
+            setattr(io, k, ptr(b[k]))
+        io.active_capacity = b["active_capacity"]
+        return io
+
+    def _launch(self, contacts, io, dt: float) -> None:
+        solver, m = self.solver, self.model
         pipe, desc = solver._desc_for(contacts)
         if contacts is not None:
             if contacts._seg is None or not contacts._seg_valid:
@@ -116,7 +163,6 @@ class SubstepAdjoint:
         _lib.check("nb_xpbd_step_adjoint", lib.nb_xpbd_step_adjoint(
             C.byref(desc), C.byref(params), C.byref(io), C.byref(seg), float(dt),
             C.c_void_p(_lib.stream_handle(m.device))))
-        return gq, gqd, gf
 
     def status(self) -> int:
         return 0 if self._bufs is None else int(self._bufs["status"].item())

@@ -235,7 +235,9 @@ class CollisionPipeline:
             if isinstance(pairs, torch.Tensor):
                 pairs = pairs.detach().cpu().numpy()
         else:
-            # SAP reports the same AABB-overlapping set as NxN; both use the NxN candidate list.
+            # NxN and SAP find the same AABB-overlapping pairs among the pairs the world, group and filter
+            # rules allow (the NxN list): NxN tests every listed pair, SAP sorts the world's boxes along x
+            # and sweeps, keeping the overlaps that are in the list.
             pairs = nxn_pairs(model)
         self.shape_pairs_max = int(np.asarray(pairs).reshape(-1, 2).shape[0])
         self.layout = PairLayout(model, pairs)
@@ -362,6 +364,8 @@ class CollisionPipeline:
             arrays.update(self._layout_dev)
             arrays["schedule"] = self._schedule
             self._desc = self.model.make_desc(arrays, self.layout.info())
+            # broad_phase="sap": sweep and prune per world over the NxN candidate list
+            self._desc.broad_phase = 1 if self.broad_phase_mode == "sap" else 0
         return self._desc
 
     def grid(self) -> int:

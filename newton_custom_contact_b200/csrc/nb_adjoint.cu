@@ -236,6 +236,20 @@ struct BodyT {
 
 // ---------------------------------------------------------------- generic substep pieces
 
+// The branch decisions of one contact or one body update.  Evaluated, each
+// decision that holds sets its bit; replayed, the bits decide instead of the
+// state (the forward pass of a finite difference that must stay on the piece
+// of a recorded substep).
+struct Branches {
+    unsigned bits = 0;
+    bool replay = false;
+    __device__ __forceinline__ bool take(int bit, bool cond) {
+        if (replay) return ((bits >> bit) & 1u) != 0u;
+        if (cond) bits |= 1u << bit;
+        return cond;
+    }
+};
+
 // integrate_bodies (newton/_src/solvers/solver.py:50-94)
 template <class T>
 __device__ __forceinline__ void integrate_g(BodyT<T>& b, const V3T<T>& f0, const V3T<T>& t0, V3 com, const M33& I, float inv_mass,
@@ -263,7 +277,7 @@ __device__ __forceinline__ void integrate_g(BodyT<T>& b, const V3T<T>& f0, const
 // apply_body_deltas (newton/_src/solvers/xpbd/kernels.py:809-878), weight resolved
 template <class T>
 __device__ __forceinline__ void apply_delta_g(BodyT<T>& b, const V3T<T>& dlin, const V3T<T>& dang, float weight, V3 com,
-                              const M33& I, float inv_m, const M33& inv_I, float dt) {
+                              const M33& I, float inv_m, const M33& inv_I, float dt, Branches& br, int bit0) {
     if (inv_m == 0.0f) return;
     const V3T<T> v0 = b.v, w0 = b.w, p0 = b.p;
     const Q4T<T> q0 = b.r;
@@ -281,8 +295,8 @@ __device__ __forceinline__ void apply_delta_g(BodyT<T>& b, const V3T<T>& dlin, c
     p1 = p1 - qrott(q1, vc<T>(com));
     V3T<T> v1 = v0 + dp;
     V3T<T> w1 = w0 + dw1;
-    if (val(vlength(v1)) < 1e-4f) v1 = V3T<T>{T(0.0f), T(0.0f), T(0.0f)};
-    if (val(vlength(w1)) < 1e-4f) w1 = V3T<T>{T(0.0f), T(0.0f), T(0.0f)};
+    if (br.take(bit0, val(vlength(v1)) < 1e-4f)) v1 = V3T<T>{T(0.0f), T(0.0f), T(0.0f)};
+    if (br.take(bit0 + 1, val(vlength(w1)) < 1e-4f)) w1 = V3T<T>{T(0.0f), T(0.0f), T(0.0f)};
     b.p = p1;
     b.r = q1;
     b.v = v1;
@@ -295,11 +309,12 @@ __device__ __forceinline__ void apply_delta_g(BodyT<T>& b, const V3T<T>& dlin, c
 // which only renormalises (solver_xpbd.py:554-630 as the solver kernel runs it)
 template <class T>
 __device__ __forceinline__ void body_update_g(BodyT<T>& b, const V3T<T>& dlin, const V3T<T>& dang, float weight, bool contacts,
-                              bool joints, V3 com, const M33& I, float inv_m, const M33& inv_I, float dt) {
-    if (contacts) apply_delta_g(b, dlin, dang, weight, com, I, inv_m, inv_I, dt);
+                              bool joints, V3 com, const M33& I, float inv_m, const M33& inv_I, float dt,
+                              Branches& br) {
+    if (contacts) apply_delta_g(b, dlin, dang, weight, com, I, inv_m, inv_I, dt, br, 0);
     if (joints) {
         const V3T<T> z{T(0.0f), T(0.0f), T(0.0f)};
-        apply_delta_g(b, z, z, 1.0f, com, I, inv_m, inv_I, dt);
+        apply_delta_g(b, z, z, 1.0f, com, I, inv_m, inv_I, dt, br, 2);
     }
 }
 
@@ -319,14 +334,6 @@ __device__ __forceinline__ T constraint_delta_g(const T& err, const Q4T<T>& qa, 
     return dl * relaxation;
 }
 
-template <class T>
-__device__ __forceinline__ T maxv(const T& a, const T& b) {
-    return val(a) > val(b) ? a : b;
-}
-template <class T>
-__device__ __forceinline__ T minv(const T& a, const T& b) {
-    return val(a) < val(b) ? a : b;
-}
 
 // constants of one contact record
 struct ContactC {
@@ -346,12 +353,13 @@ struct ContactC {
 // (mu: the contact's friction coefficient c.mu, as a T so that its derivative can be carried)
 template <class T>
 __device__ __forceinline__ bool contact_g(const ContactC& c, const BodyT<T>& A, const BodyT<T>& B, float relaxation, float dt,
-                          V3T<T>& lin_da, V3T<T>& ang_da, V3T<T>& lin_db, V3T<T>& ang_db, const T& mu) {
+                          V3T<T>& lin_da, V3T<T>& ang_da, V3T<T>& lin_db, V3T<T>& ang_db, const T& mu,
+                          Branches& br) {
     const V3T<T> bxa0 = qrott(A.r, vc<T>(c.p0)) + A.p;
     const V3T<T> bxb0 = qrott(B.r, vc<T>(c.p1)) + B.p;
     const V3T<T> n = vc<T>(c.n);
     const T d = vdot(n, bxb0 - bxa0) - c.thickness;
-    if (!(val(d) < 0.0f)) return false;  // d >= 0 (NaN counts as active in the solver; not differentiated)
+    if (!br.take(0, val(d) < 0.0f)) return false;  // d >= 0 (NaN counts as active in the solver; not differentiated)
     const V3T<T> r_a0 = bxa0 - (qrott(A.r, vc<T>(c.com_a)) + A.p);
     const V3T<T> r_b0 = bxb0 - (qrott(B.r, vc<T>(c.com_b)) + B.p);
     V3T<T> ang_a = -vcross(r_a0, n);
@@ -385,10 +393,11 @@ __device__ __forceinline__ bool contact_g(const ContactC& c, const BodyT<T>& A, 
         ang_a = -vcross(r_a, perp);
         ang_b = vcross(r_b, perp);
         const T err = vlength(fd);
-        if (val(err) > 0.0f) {
+        if (br.take(1, val(err) > 0.0f)) {
             T lf = constraint_delta_g(err, A.r, B.r, c.m_inv_a, c.m_inv_b, c.Ia, c.Ib, -perp, perp, ang_a, ang_b,
                                       relaxation, dt);
-            lf = maxv(lf, -lambda_n * mu);
+            const T cap = -lambda_n * mu;
+            if (br.take(2, !(val(lf) > val(cap)))) lf = cap;  // lf = max(lf, cap)
             lin_da = lin_da - vmul(perp, lf);
             lin_db = lin_db + vmul(perp, lf);
             ang_da = ang_da + vmul(ang_a, lf);
@@ -399,9 +408,11 @@ __device__ __forceinline__ bool contact_g(const ContactC& c, const BodyT<T>& A, 
     const V3T<T> z{T(0.0f), T(0.0f), T(0.0f)};
     if (c.mut > 0.0f) {
         const T err = vdot(dom, n) * dt;
-        if (fabsf(val(err)) > 0.0f) {
+        if (br.take(3, fabsf(val(err)) > 0.0f)) {
             T lt = constraint_delta_g(err, A.r, B.r, c.m_inv_a, c.m_inv_b, c.Ia, c.Ib, z, z, -n, n, relaxation, dt);
-            lt = minv(maxv(lt, -lambda_n * c.mut), lambda_n * c.mut);
+            const T lo = -lambda_n * c.mut, hi = lambda_n * c.mut;
+            if (br.take(4, !(val(lt) > val(lo)))) lt = lo;  // lt = min(max(lt, lo), hi)
+            if (br.take(5, !(val(lt) < val(hi)))) lt = hi;
             ang_da = ang_da - vmul(n, lt);
             ang_db = ang_db + vmul(n, lt);
         }
@@ -409,10 +420,11 @@ __device__ __forceinline__ bool contact_g(const ContactC& c, const BodyT<T>& A, 
     if (c.mur > 0.0f) {
         dom = dom - vmul(n, vdot(n, dom));
         const T err = vlength(dom) * dt;
-        if (val(err) > 0.0f) {
+        if (br.take(6, val(err) > 0.0f)) {
             const V3T<T> rn = vnormalize(dom);
             T lr = constraint_delta_g(err, A.r, B.r, c.m_inv_a, c.m_inv_b, c.Ia, c.Ib, z, z, -rn, rn, relaxation, dt);
-            lr = maxv(lr, -lambda_n * c.mur);
+            const T cap = -lambda_n * c.mur;
+            if (br.take(7, !(val(lr) > val(cap)))) lr = cap;  // lr = max(lr, cap)
             ang_da = ang_da - vmul(rn, lr);
             ang_db = ang_db + vmul(rn, lr);
         }
@@ -574,8 +586,9 @@ __device__ void vjp_apply(const float* s, const float* dl, float weight, bool co
     for (int k = 0; k < 13; ++k) mid[k] = s[k];
     if (contacts) {
         BodyT<float> b = body_from<float>(s);
+        Branches br;
         apply_delta_g(b, V3T<float>{dl[0], dl[1], dl[2]}, V3T<float>{dl[3], dl[4], dl[5]}, weight, com, I, inv_m,
-                      inv_I, dt);
+                      inv_I, dt, br, 0);
         body_to(b, mid);
     }
     if (joints) {
@@ -660,7 +673,8 @@ __device__ __forceinline__ void vjp_contact(const ContactC& c, const float* sa, 
         B.v = {Dual<kDirs>(sb[7]), Dual<kDirs>(sb[8]), Dual<kDirs>(sb[9])};
         B.w = {seed<kDirs>(sb[10], 17, j0), seed<kDirs>(sb[11], 18, j0), seed<kDirs>(sb[12], 19, j0)};
         V3T<Dual<kDirs>> la, aa, lb, ab;
-        if (!contact_g(c, A, B, relaxation, dt, la, aa, lb, ab, Dual<kDirs>(c.mu))) return;
+        Branches br;
+        if (!contact_g(c, A, B, relaxation, dt, la, aa, lb, ab, Dual<kDirs>(c.mu), br)) return;
         const Dual<kDirs> o[12] = {la.x, la.y, la.z, aa.x, aa.y, aa.z, lb.x, lb.y, lb.z, ab.x, ab.y, ab.z};
 #pragma unroll
         for (int k = 0; k < kDirs && j0 + k < 20; ++k) {
@@ -685,7 +699,8 @@ __device__ __forceinline__ float vjp_contact_mu(const ContactC& c, const float* 
     Dual<1> mu(c.mu);
     mu.d[0] = 1.0f;
     V3T<Dual<1>> la, aa, lb, ab;
-    if (!contact_g(c, A, B, relaxation, dt, la, aa, lb, ab, mu)) return 0.0f;
+    Branches br;
+    if (!contact_g(c, A, B, relaxation, dt, la, aa, lb, ab, mu, br)) return 0.0f;
     const Dual<1> o[12] = {la.x, la.y, la.z, aa.x, aa.y, aa.z, lb.x, lb.y, lb.z, ab.x, ab.y, ab.z};
     float acc = 0.0f;
 #pragma unroll
@@ -831,18 +846,36 @@ __global__ void __launch_bounds__(kThreads) adjoint_forward_kernel(NbModelDesc m
         __syncthreads();
         // the solver's contact pass: each body's delta is the float sum of its active contacts'
         // deltas in record order (nb_ordered.cuh), as in nb_xpbd_step
+        // branch bytes of this iteration's records (record / replay modes)
+        uint8_t* BC = io.branch_mode != 0 && io.branch_contact
+                          ? io.branch_contact + (size_t)it * (size_t)m.contact_capacity + (size_t)seg.world_base[w]
+                          : nullptr;
         auto test = [&](int k, int& ends) -> bool {
             const float4* r = R + (size_t)k * 5;
-            if (__float_as_int(r[3].w) == __float_as_int(r[4].w)) return false;
-            const ContactC c = load_contact(m, r, b0, S_it);
-            if (c.la == c.lb) return false;
-            float sa[13], sb[13];
-            side_state(S_it, b0, c.la, sa);
-            side_state(S_it, b0, c.lb, sb);
-            V3T<float> la, aa, lb, ab;
-            if (!contact_g(c, body_from<float>(sa), body_from<float>(sb), p.rigid_contact_relaxation, dt, la, aa, lb,
-                           ab, c.mu))
+            if (__float_as_int(r[3].w) == __float_as_int(r[4].w)) {
+                if (io.branch_mode == 1 && BC) BC[k] = 0;
                 return false;
+            }
+            const ContactC c = load_contact(m, r, b0, S_it);
+            if (c.la == c.lb) {
+                if (io.branch_mode == 1 && BC) BC[k] = 0;
+                return false;
+            }
+            Branches br;
+            if (io.branch_mode == 2) {
+                br.replay = true;
+                br.bits = BC[k];
+                if (!(br.bits & 1u)) return false;
+            } else {
+                float sa[13], sb[13];
+                side_state(S_it, b0, c.la, sa);
+                side_state(S_it, b0, c.lb, sb);
+                V3T<float> la, aa, lb, ab;
+                const bool on = contact_g(c, body_from<float>(sa), body_from<float>(sb), p.rigid_contact_relaxation,
+                                          dt, la, aa, lb, ab, c.mu, br);
+                if (io.branch_mode == 1 && BC) BC[k] = (uint8_t)br.bits;
+                if (!on) return false;
+            }
             ends = nb::ends_pack(c.la, c.lb);
             return true;
         };
@@ -853,8 +886,13 @@ __global__ void __launch_bounds__(kThreads) adjoint_forward_kernel(NbModelDesc m
             side_state(S_it, b0, c.la, sa);
             side_state(S_it, b0, c.lb, sb);
             V3T<float> la, aa, lb, ab;
+            Branches br;
+            if (io.branch_mode == 2) {
+                br.replay = true;
+                br.bits = BC[k];
+            }
             contact_g(c, body_from<float>(sa), body_from<float>(sb), p.rigid_contact_relaxation, dt, la, aa, lb, ab,
-                      c.mu);
+                      c.mu, br);
             // the reverse pass differentiates this iteration's active contacts only
             const int slot = atomicAdd(io.active_count + it, 1);
             if (slot < io.active_capacity) {
@@ -886,11 +924,18 @@ __global__ void __launch_bounds__(kThreads) adjoint_forward_kernel(NbModelDesc m
             for (int k = 0; k < 6; ++k) D[k] = dl[k];
             io.tape_weight[(size_t)it * B + bi] = weight;
             BodyT<float> b = body_from<float>(S_it + 13 * (size_t)bi);
+            uint8_t* BB = io.branch_mode != 0 && io.branch_body ? io.branch_body + (size_t)it * B + bi : nullptr;
+            Branches br;
+            if (io.branch_mode == 2) {
+                br.replay = true;
+                br.bits = *BB;
+            }
             if (!kinematic(m, bi))
                 body_update_g(b, V3T<float>{dl[0], dl[1], dl[2]}, V3T<float>{dl[3], dl[4], dl[5]}, weight,
                               has_contacts != 0, model_joints, load_v3(m.body_com + 3 * (size_t)bi),
                               load_m33(m.body_inertia + 9 * (size_t)bi), m.body_inv_mass[bi],
-                              load_m33(m.body_inv_inertia + 9 * (size_t)bi), dt);
+                              load_m33(m.body_inv_inertia + 9 * (size_t)bi), dt, br);
+            if (io.branch_mode == 1 && BB) *BB = (uint8_t)br.bits;
             body_to(b, S_next + 13 * (size_t)bi);
         }
         __syncthreads();
@@ -1022,6 +1067,7 @@ cudaError_t nb_launch_xpbd_adjoint(const NbModelDesc* m, const NbXpbdParams* p, 
     cudaError_t e = cudaMemsetAsync(io->active_count, 0, sizeof(int32_t) * (size_t)(K > 0 ? K : 1), s);
     if (e != cudaSuccess) return e;
     adjoint_forward_kernel<<<m->world_count, kThreads, 0, s>>>(*m, *p, *io, *seg, has_contacts, dt);
+    if (io->forward_only) return cudaGetLastError();
     const int gb = nb_contact_grid(m->body_count, kThreads);
     adjoint_seed_kernel<<<gb, kThreads, 0, s>>>(*m, *io);
     const int gc = nb_contact_grid(io->active_capacity > 0 ? io->active_capacity : 1, kThreads);

@@ -91,9 +91,14 @@ cudaError_t nb_raise_dynamic_smem(const void* kernel, size_t bytes) {
         if (e == cudaSuccess) kv.second = bytes;
         return e;
     }
-    if (bytes <= 48 * 1024) {
+    // without the attribute a CTA may use 48 KB of static and dynamic shared memory together
+    cudaFuncAttributes attr;
+    e = cudaFuncGetAttributes(&attr, kernel);
+    if (e != cudaSuccess) return e;
+    const size_t default_limit = attr.sharedSizeBytes < 48 * 1024 ? 48 * 1024 - attr.sharedSizeBytes : 0;
+    if (bytes <= default_limit) {
         // within the default limit: nothing to raise, remember that
-        g_smem_raised[dev].emplace_back(kernel, (size_t)48 * 1024);
+        g_smem_raised[dev].emplace_back(kernel, default_limit);
         return cudaSuccess;
     }
     e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -122,7 +127,7 @@ int nb_collide(const NbModelDesc* model, const float* body_q, const NbContactSeg
     if (!body_q || !model->world_pair_start || !model->pair_shapes || !model->world_shape_start ||
         (model->global_shape_count > 0 && !model->global_shapes))
         return NB_ERR_INVALID;
-    if ((int64_t)(nb_collide_smem_bytes(model) + nb_collide_static_smem_bytes()) > smem_limit())
+    if ((int64_t)(nb_collide_smem_bytes(model) + nb_collide_static_smem_bytes(model)) > smem_limit())
         return NB_ERR_UNSUPPORTED;
     // grid_ctas <= 0: each narrow-phase kernel uses its own default (enough CTAs
     // to reach its register-limited occupancy)
@@ -183,15 +188,21 @@ int nb_xpbd_step_adjoint(const NbModelDesc* model, const NbXpbdParams* params, c
     if (params->iterations < 0 || !(dt > 0.0f)) return NB_ERR_INVALID;
     if (params->enable_restitution) return NB_ERR_UNSUPPORTED;
     if (!model->world_body_start || !model->world_joint_start) return NB_ERR_INVALID;
-    if (model->body_count > 0 &&
-        (!io->body_q_in || !io->body_qd_in || !io->body_f_in || !io->grad_q_out || !io->grad_qd_out ||
-         !io->grad_q_in || !io->grad_qd_in || !io->tape_state || !io->tape_delta || !io->tape_weight ||
-         !io->grad_acc || !io->delta_acc || !io->count_acc))
+    const bool forward_only = io->forward_only != 0;
+    if (model->body_count > 0 && (!io->body_q_in || !io->body_qd_in || !io->body_f_in || !io->tape_state ||
+                                  !io->tape_delta || !io->tape_weight || !io->delta_acc || !io->count_acc))
+        return NB_ERR_INVALID;
+    if (model->body_count > 0 && !forward_only &&
+        (!io->grad_q_out || !io->grad_qd_out || !io->grad_q_in || !io->grad_qd_in || !io->grad_acc))
         return NB_ERR_INVALID;
     if (io->body_q_out && !io->body_qd_out) return NB_ERR_INVALID;
+    if (forward_only && !io->body_q_out) return NB_ERR_INVALID;
     const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
     if (io->active_capacity < 0 || !io->active_count || (has_contacts && io->active_capacity > 0 && !io->active))
         return NB_ERR_INVALID;
+    // replayed branches hold for the forward pass only (the reverse evaluates them at the tape's states)
+    if (io->branch_mode < 0 || io->branch_mode > 2 || (io->branch_mode == 2 && !forward_only)) return NB_ERR_INVALID;
+    if (io->branch_mode != 0 && (!io->branch_body || (has_contacts && !io->branch_contact))) return NB_ERR_INVALID;
     cudaError_t e = nb_launch_xpbd_adjoint(model, params, io, seg, has_contacts, dt, (cudaStream_t)stream);
     return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
 }

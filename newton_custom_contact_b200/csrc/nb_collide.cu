@@ -193,10 +193,17 @@ __device__ __forceinline__ void emit_chunk(const NbContactSeg& seg, int2* queue,
     __syncwarp();
 }
 
+struct SapScratch;
+template <bool kSap>
+__device__ bool world_sap_if(const NbModelDesc& m, const NbContactSeg& seg, int w, const float4* lo, const float4* hi,
+                             QueueStage& st, SapScratch* sc, int lane);
+
 // one world by one warp: shapes, then its pair chunks in order (the next chunk's
-// pairs are loaded while this chunk is tested)
+// pairs are loaded while this chunk is tested); with kSap the sweep and prune
+// path runs first and the pair test only when it cannot take the world
+template <bool kSap = false>
 __device__ void world_by_warp(const NbModelDesc& m, const float* __restrict__ body_q, const NbContactSeg& seg, int k,
-                              float4* lo, float4* hi, QueueStage& st, int lane) {
+                              float4* lo, float4* hi, QueueStage& st, int lane, SapScratch* sc = nullptr) {
     const unsigned* pairs = m.pair_shapes;
     int2* queue = reinterpret_cast<int2*>(seg.queue);
     const long long gjk_back = 2 * (long long)m.pair_count - 1;
@@ -204,6 +211,9 @@ __device__ void world_by_warp(const NbModelDesc& m, const float* __restrict__ bo
     const int ns = m.world_shape_start[w + 1] - m.world_shape_start[w] + m.global_shape_count;
     stage_shapes(m, body_q, w, k, lo, hi, reinterpret_cast<float4*>(seg.geom), lane, 32);
     __syncwarp();
+    if constexpr (kSap) {
+        if (world_sap_if<kSap>(m, seg, w, lo, hi, st, sc, lane)) return;
+    }
     const int p0 = m.world_pair_start[w], p1 = m.world_pair_start[w + 1];
     int ncand = 0;
     unsigned nxt[4];
@@ -289,11 +299,209 @@ __device__ void world_by_cta(const NbModelDesc& m, const float* __restrict__ bod
     __syncthreads();  // shapes and run counts are reused by the next world
 }
 
+// ---- sweep and prune (broad_phase="sap"; broad_phase_sap.py:397-677)
+
+constexpr int kSapShapes = 256;  // shape slots of a world the warp sorts in shared memory
+constexpr int kSapHits = 512;    // overlapping pairs one world may collect before falling back to the pair test
+
+struct SapScratch {
+    float key[kSapShapes];  // lo.x of the sorted slots (+inf padding)
+    int idx[kSapShapes];    // slot at each sorted position
+    int hit[kSapHits];      // pair indices of the overlaps found
+    int nhit;
+};
+
+// global shape index of world slot l
+__device__ __forceinline__ int slot_shape(const NbModelDesc& m, int s0, int nloc, int l) {
+    return l < nloc ? s0 + l : m.global_shapes[l - nloc];
+}
+
+// index of the pair (sa, sb) of global shapes in the world's pair list [p0, p1) (sorted by (sa, sb),
+// the pair list's key order), or -1
+__device__ __forceinline__ int find_pair(const NbModelDesc& m, int p0, int p1, int s0, int nloc, int sa, int sb) {
+    const long long want = ((long long)sa << 32) | (unsigned)sb;
+    int lo = p0, hi = p1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const unsigned pw = m.pair_shapes[mid];
+        const int a = slot_shape(m, s0, nloc, (int)(pw & 0xFFFFu)), b = slot_shape(m, s0, nloc, (int)(pw >> 16));
+        const long long have = ((long long)a << 32) | (unsigned)b;
+        if (have < want) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo < p1) {
+        const unsigned pw = m.pair_shapes[lo];
+        if (slot_shape(m, s0, nloc, (int)(pw & 0xFFFFu)) == sa && slot_shape(m, s0, nloc, (int)(pw >> 16)) == sb)
+            return lo;
+    }
+    return -1;
+}
+
+// warp-wide bitonic sort of n (a power of two) (key, value) pairs, ascending by (key, value)
+__device__ __forceinline__ void warp_bitonic(float* key, int* val, int n, int lane) {
+    for (int size = 2; size <= n; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = lane; t < n / 2; t += 32) {
+                const int i = 2 * t - (t & (stride - 1));
+                const int j = i + stride;
+                const bool up = (i & size) == 0;
+                const float ki = key[i], kj = key[j];
+                const int vi = val[i], vj = val[j];
+                const bool gt = ki > kj || (ki == kj && vi > vj);
+                if (gt == up) {
+                    key[i] = kj;
+                    key[j] = ki;
+                    val[i] = vj;
+                    val[j] = vi;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// emits one candidate per lane (pair index p when `valid`), the warp's candidates in lane order
+__device__ __forceinline__ void emit_hits(const NbContactSeg& seg, int2* queue, long long gjk_back, QueueStage& st,
+                                          int p, bool valid, bool easy, int w, int cand_base, int lane, int& tot) {
+    const unsigned below = (1u << lane) - 1u;
+    const unsigned bh = __ballot_sync(kFull, valid);
+    const unsigned ba = __ballot_sync(kFull, valid && easy);
+    tot = __popc(bh);
+    const int tot_a = __popc(ba), tot_g = tot - tot_a;
+    if (st.nqa + tot_a > kQB) {
+        flush_queue(st.qa, st.nqa, &seg.work_counter[2], queue, 0, lane);
+        st.nqa = 0;
+    }
+    if (st.nqg + tot_g > kQB) {
+        flush_queue(st.qg, st.nqg, &seg.work_counter[3], queue, gjk_back, lane);
+        st.nqg = 0;
+    }
+    if (valid) {
+        const int c = cand_base + __popc(bh & below);
+        seg.cand[c] = p;
+        if (easy) st.qa[st.nqa + __popc(ba & below)] = make_int2(c, w);
+        else st.qg[st.nqg + __popc(bh & ~ba & below)] = make_int2(c, w);
+    }
+    st.nqa += tot_a;
+    st.nqg += tot_g;
+    __syncwarp();
+}
+
+// One world by one warp with sweep and prune: the shape slots sorted by AABB
+// lower x; every slot sweeps the slots after it while their lower x is within
+// its upper x (exactly the pairs that overlap along x) and tests y and z with
+// the pair test's predicate; overlaps whose pair is in the world's pair list
+// (the world, collision-group and filter rules the list encodes) are
+// collected, sorted by pair index and emitted in that order -- the same
+// candidates, in the same order, as testing every pair.  Returns false (and
+// emits nothing) when the world has more slots or overlaps than the shared
+// buffers hold; the caller then tests every pair.
+__device__ bool world_by_warp_sap(const NbModelDesc& m, const NbContactSeg& seg, int w, const float4* lo,
+                                  const float4* hi, QueueStage& st, SapScratch& sc, int lane) {
+    const int s0 = m.world_shape_start[w];
+    const int nloc = m.world_shape_start[w + 1] - s0;
+    const int ns = nloc + m.global_shape_count;
+    if (ns > kSapShapes) return false;
+    int n = 32;
+    while (n < ns) n <<= 1;
+    for (int i = lane; i < n; i += 32) {
+        float k = i < ns ? lo[i].x : INFINITY;
+        if (k != k) k = INFINITY;  // a NaN box overlaps nothing (all its comparisons fail)
+        sc.key[i] = k;
+        sc.idx[i] = i;
+    }
+    if (lane == 0) sc.nhit = 0;
+    __syncwarp();
+    warp_bitonic(sc.key, sc.idx, n, lane);
+    const int p0 = m.world_pair_start[w], p1 = m.world_pair_start[w + 1];
+    for (int i = lane; i < ns; i += 32) {
+        const int a = sc.idx[i];
+        if (a >= ns) continue;
+        const float4 al = lo[a], ah = hi[a];
+        const int ta = __float_as_int(al.w);
+        for (int j = i + 1; j < ns; ++j) {
+            if (!(sc.key[j] <= ah.x)) break;
+            const int b = sc.idx[j];
+            const float4 bl = lo[b], bh = hi[b];
+            if (!(al.x <= bh.x && ah.x >= bl.x && al.y <= bh.y && ah.y >= bl.y && al.z <= bh.z && ah.z >= bl.z))
+                continue;
+            const int tb = __float_as_int(bl.w);
+            const int ga = slot_shape(m, s0, nloc, a), gb = slot_shape(m, s0, nloc, b);
+            // the pair list orders each pair by shape type (narrow_phase.py:207-210); equal types keep the
+            // list's own order, so both orientations are looked up
+            int pidx;
+            if (ta < tb) pidx = find_pair(m, p0, p1, s0, nloc, ga, gb);
+            else if (ta > tb) pidx = find_pair(m, p0, p1, s0, nloc, gb, ga);
+            else {
+                pidx = find_pair(m, p0, p1, s0, nloc, ga, gb);
+                if (pidx < 0) pidx = find_pair(m, p0, p1, s0, nloc, gb, ga);
+            }
+            if (pidx < 0) continue;
+            const int h = atomicAdd(&sc.nhit, 1);
+            if (h < kSapHits) sc.hit[h] = pidx;
+        }
+    }
+    __syncwarp();
+    const int nh = sc.nhit;
+    if (nh > kSapHits) return false;
+    // sort the overlaps by pair index (padded with INT_MAX to a power of two <= kSapHits)
+    int n2 = 32;
+    while (n2 < nh) n2 <<= 1;
+    for (int i = nh + lane; i < n2; i += 32) sc.hit[i] = 0x7fffffff;
+    __syncwarp();
+    for (int size = 2; size <= n2; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = lane; t < n2 / 2; t += 32) {
+                const int i = 2 * t - (t & (stride - 1));
+                const int j = i + stride;
+                const bool up = (i & size) == 0;
+                const int vi = sc.hit[i], vj = sc.hit[j];
+                if ((vi > vj) == up) {
+                    sc.hit[i] = vj;
+                    sc.hit[j] = vi;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    int2* queue = reinterpret_cast<int2*>(seg.queue);
+    const long long gjk_back = 2 * (long long)m.pair_count - 1;
+    int ncand = 0;
+    for (int base = 0; base < nh; base += 32) {
+        const int h = base + lane;
+        const bool valid = h < nh;
+        int p = 0;
+        bool easy = false;
+        if (valid) {
+            p = sc.hit[h];
+            const unsigned pw = m.pair_shapes[p];
+            easy = analytic_pair(__float_as_int(lo[pw & 0xFFFFu].w), __float_as_int(lo[pw >> 16].w));
+        }
+        int tot;
+        emit_hits(seg, queue, gjk_back, st, p, valid, easy, w, p0 + ncand, lane, tot);
+        ncand += tot;
+    }
+    if (lane == 0) {
+        seg.cand_count[w] = ncand;
+        seg.world_count[w] = 0;
+    }
+    __syncwarp();
+    return true;
+}
+
+template <bool kSap>
+__device__ bool world_sap_if(const NbModelDesc& m, const NbContactSeg& seg, int w, const float4* lo, const float4* hi,
+                             QueueStage& st, SapScratch* sc, int lane) {
+    return world_by_warp_sap(m, seg, w, lo, hi, st, *sc, lane);
+}
+
 constexpr int kCtaWorldPairs = 2048;  // worlds with at least this many pairs are shared by a whole CTA
 
 // Worlds are taken in decreasing cost.  While the next world is large, the CTA
 // takes it together (world_by_cta); from the first small world on, every warp
 // takes worlds on its own (world_by_warp).
+// kSap (broad_phase="sap"): every world by one warp, sweep and prune first.
+template <bool kSap>
 __global__ void __launch_bounds__(kBT)
 broadphase_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
     extern __shared__ __align__(16) float4 sbox[];
@@ -304,6 +512,21 @@ broadphase_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg 
     __shared__ int2 s_qa[kBT / 32][kQB], s_qg[kBT / 32][kQB];
     __shared__ int s_k, s_run[kBT / 32];
     QueueStage st{s_qa[warp], s_qg[warp], 0, 0};
+    if constexpr (kSap) {
+        // sweep-and-prune scratch of every warp after the warps' box arrays (dynamic shared memory)
+        SapScratch* s_sap = reinterpret_cast<SapScratch*>(sbox + (size_t)(kBT / 32) * 2 * nsh);
+        for (;;) {
+            int k = 0;
+            if (lane == 0) k = atomicAdd(&seg.work_counter[0], 1);
+            k = __shfl_sync(kFull, k, 0);
+            if (k >= m.world_count) break;
+            world_by_warp<true>(m, body_q, seg, k, lo, hi, st, lane, &s_sap[warp]);
+        }
+        int2* queue = reinterpret_cast<int2*>(seg.queue);
+        flush_queue(st.qa, st.nqa, &seg.work_counter[2], queue, 0, lane);
+        flush_queue(st.qg, st.nqg, &seg.work_counter[3], queue, 2 * (long long)m.pair_count - 1, lane);
+        return;
+    }
     int small_k = -1;  // the first small world this CTA took: warp 0 does it
     for (;;) {
         if (threadIdx.x == 0) s_k = atomicAdd(&seg.work_counter[0], 1);
@@ -722,10 +945,11 @@ int sm_count() {
 }  // namespace
 
 size_t nb_collide_smem_bytes(const NbModelDesc* m) {
-    return (size_t)(kBT / 32) * 2 * (size_t)m->max_world_shapes * sizeof(float4);
+    return (size_t)(kBT / 32) * 2 * (size_t)m->max_world_shapes * sizeof(float4) +
+           (m->broad_phase == 1 ? (kBT / 32) * sizeof(SapScratch) : 0);
 }
 
-size_t nb_collide_static_smem_bytes() { return (size_t)2 * (kBT / 32) * kQB * sizeof(int2); }
+size_t nb_collide_static_smem_bytes(const NbModelDesc*) { return (size_t)2 * (kBT / 32) * kQB * sizeof(int2); }
 
 namespace {
 
@@ -764,7 +988,9 @@ cudaError_t narrow_occupancy(NarrowOccupancy* out) {
 cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const NbContactSeg* seg, int grid,
                               cudaStream_t stream) {
     const size_t smem = nb_collide_smem_bytes(m);
-    cudaError_t e = nb_raise_dynamic_smem((const void*)broadphase_kernel, smem);
+    const bool sap = m->broad_phase == 1;
+    cudaError_t e = nb_raise_dynamic_smem(sap ? (const void*)broadphase_kernel<true> : (const void*)broadphase_kernel<false>,
+                                          smem);
     if (e != cudaSuccess) return e;
     NarrowOccupancy occ;
     e = narrow_occupancy(&occ);
@@ -774,7 +1000,8 @@ cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const N
     e = cudaMemsetAsync(seg->work_counter + 5, 0, 2 * sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
     const int sms = sm_count();
-    broadphase_kernel<<<sms * 4, kBT, smem, stream>>>(*m, body_q, *seg);
+    if (sap) broadphase_kernel<true><<<sms * 4, kBT, smem, stream>>>(*m, body_q, *seg);
+    else broadphase_kernel<false><<<sms * 4, kBT, smem, stream>>>(*m, body_q, *seg);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     narrow_analytic_kernel<<<grid > 0 ? grid : sms * occ.analytic, kNT, 0, stream>>>(*m, body_q, *seg);

@@ -8,7 +8,7 @@
 #define NB_STEP_THREADS 256
 
 size_t nb_collide_smem_bytes(const NbModelDesc* m);
-size_t nb_collide_static_smem_bytes();
+size_t nb_collide_static_smem_bytes(const NbModelDesc* m);
 size_t nb_step_smem_bytes(const NbModelDesc* m);
 
 cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const NbContactSeg* seg, int grid,
@@ -36,7 +36,8 @@ cudaError_t nb_launch_ws_adam(float* w, const float* g, float* m1, float* m2, lo
 
 // Raises `kernel`'s dynamic shared-memory limit on the current device to at
 // least `bytes` (cudaFuncSetAttribute) unless an earlier call on this device
-// already did.  Attributes belong to a device, so the record is kept per
+// already did, or the kernel's static shared memory plus `bytes` fits the
+// 48 KB a CTA may use without the attribute.  Attributes belong to a device, so the record is kept per
 // (kernel, device ordinal); a mutex orders first calls from several host
 // threads.  Calls that need no raise touch no attribute, which keeps them
 // legal inside CUDA-graph capture.

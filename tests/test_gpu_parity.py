@@ -257,3 +257,32 @@ def test_clear_forces_zeroes_body_f(cuda):
     s.clear_forces()
     torch.cuda.synchronize()
     assert bool((s.body_f == 0).all().item())
+
+
+@pytest.mark.parametrize("scene", ["c2", "c1", "c3"])
+def test_sap_broad_phase_same_contacts(cuda, scene):
+    """broad_phase="sap" (per-world sort along x and sweep) finds the same candidates as testing every
+    listed pair, so the published contacts are identical bit for bit, over a few substeps of motion."""
+    if scene == "c2":
+        model, info = _small_c2()
+    elif scene == "c1":
+        model, info = scenes.scene_c1(device="cuda")
+    else:
+        model, info = scenes.scene_c3(worlds=4, device="cuda")
+    dt = info["dt"] / info["substeps"]
+    solver = SolverXPBD(model, iterations=info["iterations"])
+    pipes = {mode: CollisionPipeline(model, broad_phase=mode) for mode in ("nxn", "sap")}
+    cs = {mode: p.contacts() for mode, p in pipes.items()}
+    s0, s1 = model.state(), model.state()
+    for k in range(12):
+        pubs = {}
+        for mode, p in pipes.items():
+            p.collide(s0, cs[mode])
+            pubs[mode] = _published(cs[mode])
+        assert pubs["nxn"][0] == pubs["sap"][0] > 0
+        for f, v in pubs["nxn"][1].items():
+            assert np.array_equal(np.asarray(v).view(np.uint32) if v.dtype == np.float32 else v,
+                                  np.asarray(pubs["sap"][1][f]).view(np.uint32) if v.dtype == np.float32
+                                  else pubs["sap"][1][f]), f"{f} at substep {k}"
+        solver.step(s0, s1, None, cs["nxn"], dt)
+        s0, s1 = s1, s0

@@ -100,7 +100,9 @@ def test_contact_force_parity_c2_with_restitution(cuda, orc):
 
 
 def test_forces_of_ingested_contacts(cuda, orc):
-    """Custom contacts in reversed order: each contact's force lands on its own public row."""
+    """Custom contacts in reversed order: each contact's force lands on its own public row.  Each
+    body sums its contacts' deltas in contact order, so the reversed order moves the bodies and the
+    forces by rounding only."""
     model, info = scenes.scene_c5(worlds=8, device="cuda")
     model.request_contact_attributes("force")
     pipe = CollisionPipeline(model)
@@ -123,9 +125,10 @@ def test_forces_of_ingested_contacts(cuda, orc):
     solver.step(s0, out_b, None, c2, 1.0 / 600.0)
     solver.update_contacts(c2)
     torch.cuda.synchronize()
-    assert torch.equal(out_a.body_q, out_b.body_q)
-    assert torch.equal(c2.force[:n], fa[:n][idx])
-    assert fa[:n].abs().sum() > 0
+    torch.testing.assert_close(out_b.body_q, out_a.body_q, rtol=1e-5, atol=1e-6)
+    scale = float(fa[:n].abs().max())
+    assert scale > 0
+    torch.testing.assert_close(c2.force[:n], fa[:n][idx], rtol=1e-4, atol=1e-4 * scale)
 
 
 def test_update_contacts_errors(cuda):
