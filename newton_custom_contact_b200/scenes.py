@@ -322,10 +322,31 @@ def scene_c3(seed: int = 3, worlds: int = 4096, device=None):
                                  target_kd=20.0, limit_lower=-2.5, limit_upper=2.5)
             parent = body
         nbox = int(rng.integers(8, 49))
+        placed = []  # (centre, bounding radius) of the world's boxes
         for _ in range(nbox):
             he = rng.uniform(0.03, 0.08, size=3)
-            p = np.array([rng.uniform(0.2, 2.0), rng.uniform(-0.6, 0.6), he.max() + rng.uniform(0.0, 0.3)])
-            body = b.add_body(xform=np.concatenate([p, random_quats(rng, 1)[0]]))
+            quat = random_quats(rng, 1)[0]
+            qx_, qy_, qz_, qw_ = quat
+            # the rotated box's half extent along z: its lowest corner clears the table
+            row_z = np.array([2.0 * (qx_ * qz_ - qw_ * qy_), 2.0 * (qy_ * qz_ + qw_ * qx_),
+                              1.0 - 2.0 * (qx_ * qx_ + qy_ * qy_)])
+            ext_z = float(np.abs(row_z) @ he)
+            rb = float(np.linalg.norm(he))
+            p = None
+            for _try in range(64):
+                c = np.array([rng.uniform(0.2, 2.0), rng.uniform(-0.6, 0.6), ext_z + rng.uniform(0.0, 0.3)])
+                # bounding spheres clear of the other boxes and of the arm's capsules (straight at rest)
+                t = np.clip((c[0] - base[0]) / (7 * L), 0.0, 1.0)
+                arm_d = np.linalg.norm(c - (base + np.array([7 * L * t, 0.0, 0.0])))
+                if arm_d >= rb + r and all(np.linalg.norm(c - pc) >= rb + rc for pc, rc in placed):
+                    p = c
+                    break
+            if p is None:
+                # no room: raised above the arm and the world's boxes
+                top = max([base[2] + r] + [pc[2] + rc for pc, rc in placed])
+                p = np.array([rng.uniform(0.2, 2.0), rng.uniform(-0.6, 0.6), top + rb + 0.01])
+            placed.append((p, rb))
+            body = b.add_body(xform=np.concatenate([p, quat]))
             b.add_shape_box(body, hx=he[0], hy=he[1], hz=he[2], cfg=box_cfg)
         b.end_world()
         phases.append(rng.uniform(0.0, 2.0 * math.pi, size=7))

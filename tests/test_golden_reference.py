@@ -169,10 +169,11 @@ def test_fixed_point_sums_leave_the_reference(orc, layouts):
     assert worst > 0.0
 
 
-def test_platform_asin_differs_from_library_asin_by_ulps():
+def test_platform_asin_and_library_asin_rollouts_agree():
     """On the joint scene the only source of difference between the two reference rollouts is the
-    asin / acos implementation: after one substep they agree to a few fp32 ulps of the state."""
+    asin / acos implementation (the platform's or the library's fp32 functions): over all 16 substeps
+    they agree to a few fp32 ulps of the state."""
     fx = _load("c3_arm")
-    q, ql = fx["body_q_all"][1], fx["body_q_all_library_asin"][1]
-    assert np.allclose(q, ql, rtol=1e-6, atol=1e-6)
-    assert not np.array_equal(fx["body_qd_all"][1], fx["body_qd_all_library_asin"][1])
+    for k in range(fx["body_q_all"].shape[0]):
+        assert np.allclose(fx["body_q_all"][k], fx["body_q_all_library_asin"][k], rtol=1e-6, atol=1e-6)
+        assert np.allclose(fx["body_qd_all"][k], fx["body_qd_all_library_asin"][k], rtol=1e-5, atol=1e-5)
