@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--step-schedule", default=None, metavar="MODE/G",
                     help="fix the step schedule (e.g. groups_compact/32) instead of autotuning it; a run "
                          "under a profiler serialises launches, so its autotuner may pick another schedule")
+    ap.add_argument("--broad-phase", default="explicit", choices=["explicit", "nxn", "sap"],
+                    help="CollisionPipeline broad phase of the main workload (the reference's default: explicit)")
     ap.add_argument("--build", default="product", choices=["product", "exact"],
                     help="library build: product (FMA contraction in the solver) or exact (the parity build)")
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
@@ -521,7 +523,7 @@ def run_ours(args, rank, world_size, local_rank):
         model, info = scenes.scene_c2(seed=args.seed + 1000 * rank, worlds=args.worlds, device=dev)
     substeps, iters = info["substeps"], info["iterations"]
     dt = info["dt"] / substeps
-    pipe = CollisionPipeline(model)
+    pipe = CollisionPipeline(model, broad_phase=args.broad_phase)
     solver = SolverXPBD(model, iterations=iters)
     s0, s1 = model.state(), model.state()
     contacts = pipe.contacts()
@@ -711,6 +713,7 @@ def run_ours(args, rank, world_size, local_rank):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
         "config": {"workload": WORKLOAD, "worlds_per_gpu": model.world_count, "bodies_per_gpu": model.body_count,
                    "substeps": substeps, "iterations": iters, "form": "plain XPBD", "build": args.build,
+                   "broad_phase": args.broad_phase,
                    "l2": "256 MiB buffer written before every timed step; the frame's working set (pair "
                          "lists, contact slots and records, body state) is larger than L2",
                    "cuda_graph": True,

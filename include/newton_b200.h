@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 16
+#define NB_ABI_VERSION 17
 
 enum {
     NB_OK = 0,
@@ -167,11 +167,17 @@ typedef struct NbModelDesc {
                                           1: independent groups of group_threads (32/64/128), full
                                              body slab (43 words/body);
                                           2: as 1 with a compact slab (21 words/body, mass
-                                             properties read from the model); modes 1-2 pull worlds
+                                             properties read from body_pack); modes 1-2 pull worlds
                                              in world_order, each group owning
                                              arena * group_threads / cta_threads words */
     const int32_t* batch_world;        /* [batch_count, cta_threads/group_threads] world ids, -1 = none */
     const int32_t* batch_slab;         /* [batch_count, cta_threads/group_threads] arena offsets (words) */
+    const float* body_pack;            /* [B,24], 16-byte aligned: per body com (3), effective inverse mass,
+                                          inertia (9, row-major), effective inverse inertia (9), 2 zeros;
+                                          "effective": zero for kinematic bodies (the solver's
+                                          _update_effective_inv_mass_inertia, solver.py:160-174); the
+                                          caller refreshes it when the model's mass properties or flags
+                                          change.  Required by step_mode 2. */
 } NbModelDesc;
 
 /* Contact slots and the per-substep collision work buffers (written by

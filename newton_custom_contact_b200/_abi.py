@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 16
+NB_ABI_VERSION = 17
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -141,6 +141,7 @@ class NbModelDesc(C.Structure):
         ("step_mode", C.c_int32),
         ("batch_world", _fp),
         ("batch_slab", _fp),
+        ("body_pack", _fp),
     ]
 
 

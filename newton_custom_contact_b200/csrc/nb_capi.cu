@@ -60,6 +60,8 @@ int check_schedule(const NbModelDesc* m) {
         if (g != 32 && g != 64 && g != 128) return NB_ERR_INVALID;
         const int share = (m->smem_floats_per_batch / (NB_STEP_THREADS / g)) & ~1;
         if ((int64_t)m->max_world_bodies * nb_step_slab_words(m->step_mode == 2) > share) return NB_ERR_INVALID;
+        if (m->step_mode == 2 && m->body_count > 0 && (!m->body_pack || !aligned16(m->body_pack)))
+            return NB_ERR_INVALID;
         return NB_OK;
     }
     if (m->step_mode != 0) return NB_ERR_INVALID;

@@ -54,10 +54,7 @@ struct SBodiesT {
     float* c;                  // [4][nb]  com (3), effective inv mass          (full layout)
     float* I;                  // [9][nb]                                         (full layout)
     float* iI;                 // [9][nb]  effective inverse inertia              (full layout)
-    const float* g_com;        // model arrays                                    (compact layout)
-    const float* g_inv_m;
-    const float* g_I;
-    const float* g_iI;
+    const float4* g_pack;      // NbModelDesc.body_pack, 6 float4 per body        (compact layout)
     float* frc;                // [6][nb]  body_f + joint forces (aliases acc before integration)
     int* flags;                // [nb]
     float* acc;                // [6][nb]  delta accumulators (linear 3, angular 3)
@@ -76,24 +73,28 @@ struct SBodiesT {
         f[10 * nb + i] = aw.x; f[11 * nb + i] = aw.y; f[12 * nb + i] = aw.z;
     }
     __device__ bool kinematic(int i) const { return (flags[i] & NB_BODY_KINEMATIC) != 0; }
+    // compact layout: body i's packed mass properties, floats 0..23 in 6 float4 (read-only path)
+    __device__ const float4* pack(int i) const { return g_pack + 6 * (size_t)(b0 + i); }
     __device__ V3 com(int i) const {
         if constexpr (kCompact) {
-            const float* r = g_com + 3 * (size_t)(b0 + i);
-            return V3{__ldg(r), __ldg(r + 1), __ldg(r + 2)};
+            const float4 a = __ldg(pack(i));
+            return V3{a.x, a.y, a.z};
         } else {
             return V3{c[i], c[nb + i], c[2 * nb + i]};
         }
     }
     __device__ float inv_m(int i) const {
-        if constexpr (kCompact) return kinematic(i) ? 0.0f : __ldg(g_inv_m + b0 + i);
+        if constexpr (kCompact) return __ldg(pack(i)).w;
         else return c[3 * nb + i];
     }
     __device__ M33 inertia(int i) const {
         M33 r;
         if constexpr (kCompact) {
-            const float* a = g_I + 9 * (size_t)(b0 + i);
-#pragma unroll
-            for (int k = 0; k < 9; ++k) r.m[k / 3][k % 3] = __ldg(a + k);
+            // floats 4..12
+            const float4 a = __ldg(pack(i) + 1), b = __ldg(pack(i) + 2), c3 = __ldg(pack(i) + 3);
+            r.m[0][0] = a.x; r.m[0][1] = a.y; r.m[0][2] = a.z;
+            r.m[1][0] = a.w; r.m[1][1] = b.x; r.m[1][2] = b.y;
+            r.m[2][0] = b.z; r.m[2][1] = b.w; r.m[2][2] = c3.x;
         } else {
 #pragma unroll
             for (int k = 0; k < 9; ++k) r.m[k / 3][k % 3] = I[k * nb + i];
@@ -103,10 +104,11 @@ struct SBodiesT {
     __device__ M33 inv_inertia(int i) const {
         M33 r;
         if constexpr (kCompact) {
-            const float* a = g_iI + 9 * (size_t)(b0 + i);
-            const bool kin = kinematic(i);
-#pragma unroll
-            for (int k = 0; k < 9; ++k) r.m[k / 3][k % 3] = kin ? 0.0f : __ldg(a + k);
+            // floats 13..21
+            const float4 a = __ldg(pack(i) + 3), b = __ldg(pack(i) + 4), c5 = __ldg(pack(i) + 5);
+            r.m[0][0] = a.y; r.m[0][1] = a.z; r.m[0][2] = a.w;
+            r.m[1][0] = b.x; r.m[1][1] = b.y; r.m[1][2] = b.z;
+            r.m[2][0] = b.w; r.m[2][1] = c5.x; r.m[2][2] = c5.y;
         } else {
 #pragma unroll
             for (int k = 0; k < 9; ++k) r.m[k / 3][k % 3] = iI[k * nb + i];
@@ -149,10 +151,7 @@ __device__ SBodiesT<kCompact> sbodies_carve(unsigned char* slab, const NbModelDe
     s.frc = a;  // used only before integration
     float* fl = a + 6 * (size_t)nb;
     s.f = fl;
-    s.g_com = m.body_com;
-    s.g_inv_m = m.body_inv_mass;
-    s.g_I = m.body_inertia;
-    s.g_iI = m.body_inv_inertia;
+    s.g_pack = reinterpret_cast<const float4*>(m.body_pack);
     float* after;
     if constexpr (kCompact) {
         s.c = s.I = s.iI = nullptr;

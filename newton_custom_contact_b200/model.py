@@ -12,7 +12,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from ._abi import JointType, NbModelDesc, ptr
+from ._abi import BodyFlags, JointType, NbModelDesc, ptr
 
 
 def _dev(device) -> torch.device:
@@ -183,6 +183,25 @@ class Model:
             setattr(self, k, torch.from_numpy(np.ascontiguousarray(v)).to(dev))
         self.shape_contact_pairs = torch.from_numpy(np.ascontiguousarray(h["shape_contact_pairs"]))
         self._part_dev = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in self._part.items()}
+        self._part_dev["body_pack"] = torch.zeros((max(self.body_count, 1), 24), dtype=torch.float32, device=dev)
+        self.update_body_pack()
+
+    def update_body_pack(self) -> None:
+        """Refresh the packed per-body mass properties the step reads (``NbModelDesc.body_pack``): com,
+        effective inverse mass, inertia, effective inverse inertia -- zero inverse mass and inertia for
+        kinematic bodies, as the solver's ``_update_effective_inv_mass_inertia``
+        (newton/_src/solvers/solver.py:160-174), which the reference runs at solver construction and
+        in ``notify_model_changed``.  Updated in place, so descriptors keep their pointer."""
+        B = self.body_count
+        if B == 0:
+            return
+        kin = (self.body_flags.to(torch.int32) & int(BodyFlags.KINEMATIC)) != 0
+        zero = torch.zeros((), dtype=torch.float32, device=self.device)
+        inv_m = torch.where(kin, zero, self.body_inv_mass.reshape(B))
+        inv_I = torch.where(kin[:, None], zero, self.body_inv_inertia.reshape(B, 9))
+        pack = torch.cat([self.body_com.reshape(B, 3), inv_m[:, None], self.body_inertia.reshape(B, 9), inv_I,
+                          torch.zeros((B, 2), dtype=torch.float32, device=self.device)], dim=1)
+        self._part_dev["body_pack"].copy_(pack)
 
     def _build_partition(self) -> None:
         """World ranges + per-world candidate pair layout for the per-world kernels."""
@@ -354,6 +373,8 @@ class Model:
             d.step_mode = int(sched.step_mode)
             d.batch_world = ptr(arrays["batch_world"])
             d.batch_slab = ptr(arrays["batch_slab"])
+        if "body_pack" in arrays:
+            d.body_pack = ptr(arrays["body_pack"])
         return d
 
     def host_arrays(self) -> dict:

@@ -49,6 +49,8 @@ class SolverXPBD:
         if iterations < 0:
             raise ValueError("iterations must be non-negative")
         self.model = model
+        # the effective mass properties, as SolverBase._init_kinematic_state (solver.py:196-215)
+        model.update_body_pack()
         self.iterations = int(iterations)
         self.soft_body_relaxation = soft_body_relaxation
         self.soft_contact_relaxation = soft_contact_relaxation
@@ -75,7 +77,10 @@ class SolverXPBD:
         return self.model.device
 
     def notify_model_changed(self, flags: int) -> None:
-        """Model arrays are read at every step; only cached descriptors are dropped."""
+        """Model arrays are read at every step, except the effective (kinematic-aware) mass properties,
+        which are refreshed here as in the reference (solver.py:160-174); cached descriptors are
+        dropped."""
+        self.model.update_body_pack()
         self._desc_cache.clear()
 
     def params(self) -> NbXpbdParams:
