@@ -206,6 +206,38 @@ def test_collide_bit_exact_in_piled_state(cuda, orc):
     assert table.shape[0] > 5000
 
 
+def test_bench_scene_bit_exact(cuda, orc):
+    """The benchmark scene itself (4096 uneven worlds, seed 1, 8 substeps x 8 iterations): six frames of
+    collide + step free-running on the CUDA path and in the oracle end in bit-identical states, and the
+    contacts of frame 6's first substep are bit-identical too."""
+    model, info = scenes.scene_c2(seed=1, worlds=4096, device="cuda")
+    pipe = CollisionPipeline(model)
+    solver = SolverXPBD(model, iterations=info["iterations"])
+    params = solver.params()
+    s0, s1 = model.state(), model.state()
+    contacts = pipe.contacts()
+    dt = info["dt"] / info["substeps"]
+    q, qd = model.host("body_q"), model.host("body_qd")
+    f = np.zeros((model.body_count, 6), np.float32)
+    for k in range(6 * info["substeps"]):
+        s0.clear_forces()
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, dt)
+        s0, s1 = s1, s0
+        segs = orc.collide(model, pipe.layout, q)
+        q, qd, st = orc.step(model, pipe.layout, params, q, qd, f, segs, dt)
+        assert st == 0
+    torch.cuda.synchronize()
+    assert _bits_equal(s0.body_q.cpu().numpy(), q), "body_q after 6 frames"
+    assert _bits_equal(s0.body_qd.cpu().numpy(), qd), "body_qd after 6 frames"
+    pipe.collide(s0, contacts)
+    torch.cuda.synchronize()
+    assert pipe.status(contacts) == 0
+    segs = orc.collide(model, pipe.layout, q)
+    table = _assert_contacts_equal(model, pipe, contacts, segs, orc)
+    assert table.shape[0] > 100000
+
+
 @pytest.mark.parametrize("n", [1, 4, 5])
 def test_substeps_entry_matches_host_loop(cuda, n):
     """nb_xpbd_substeps (SolverXPBD.step_substeps) against the host loop of collide + step, bit for bit,

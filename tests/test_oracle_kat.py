@@ -38,8 +38,9 @@ def test_plane_box(orc, z, n, dist):
     rows = run(orc, P, [0, 0, 0], [0, 0, 0], B, [0, 0, z], [1, 1, 1])
     assert rows.shape[0] == n
     for r in rows:
-        assert r[11] == pytest.approx(dist, abs=0.01)
-        assert np.dot(r[6:9], [0, 0, 1]) > 0.99
+        # analytic: the box's bottom corners sit at depth z - 1 along the plane normal
+        assert r[11] == pytest.approx(dist, abs=1e-5)
+        assert r[6:9] == pytest.approx([0, 0, 1], abs=1e-6)
 
 
 @pytest.mark.parametrize("z,dist", [(1.0, 0.0), (0.8, -0.2), (0.5, -0.5), (0.2, -0.8)])
@@ -71,7 +72,8 @@ def test_sphere_sphere(orc, x2, r1, dist):
 def test_sphere_box(orc, p, r, dist):
     rows = run(orc, S, p, [r, 0, 0], B, [0, 0, 0], [1, 1, 1])
     assert rows.shape[0] == 1
-    assert rows[0, 11] == pytest.approx(dist, abs=0.01)
+    # analytic: distance from the sphere's centre to the face minus the radius
+    assert rows[0, 11] == pytest.approx(dist, abs=1e-5)
 
 
 def test_box_box_separated_and_overlapping(orc):
