@@ -138,9 +138,14 @@ def test_c5_friction_and_velocity_gradients_1024_worlds(cuda):
         # analytic gradients through the checkpointed rollout (every 16 substeps)
         mu_w = mu_w0.clone().requires_grad_(True)
         qdv = qd0.clone().requires_grad_(True)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record()
         q1, _ = simulate(pipe, solver, q0.clone(), qdv, f, substeps=n, dt=dt, checkpoint_every=16,
                          shape_mu=shape_mu_of(mu_w))
+        ev[1].record()
         world_loss(q1).sum().backward()
+        ev[2].record()
+        torch.cuda.synchronize()
         m.shape_material_mu.copy_(base_mu)
         # the recorded forward equals the solver's rollout bit for bit
         torch.testing.assert_close(rollout(n, mu_w0, qd0, True), q1.detach(), rtol=0, atol=0)
@@ -153,7 +158,8 @@ def test_c5_friction_and_velocity_gradients_1024_worlds(cuda):
         # shows as a smaller difference)
         dmu = g_mu / g_mu.abs().max()
         an_dir = {"friction": float((g_mu * dmu).sum()), "velocity": float(g_v.sum())}
-        st = {"median_abs_grad": {k: float(np.median(np.abs(x))) for k, x in an.items()}, "adjoint_direction": an_dir}
+        st = {"median_abs_grad": {k: float(np.median(np.abs(x))) for k, x in an.items()}, "adjoint_direction": an_dir,
+              "ms": {"forward": ev[0].elapsed_time(ev[1]), "backward": ev[1].elapsed_time(ev[2])}}
         for h in REPLAY_EPS:
             loss = lambda mu, qd: world_loss(rollout(n, mu, qd, True)).cpu().numpy()  # noqa: E731
             fd = {"friction": (loss(mu_w0 + h, qd0) - loss(mu_w0 - h, qd0)) / (2 * h),
