@@ -317,6 +317,8 @@ def warm_start_arm(model, dt, substeps, sched, stream, flush, steps, warmup, ite
             solver.step(x, y, None, c, dt)
             x, y = y, x
 
+    # buffers allocated on the default stream above are used on `stream` below
+    stream.wait_stream(torch.cuda.current_stream(stream.device))
     with torch.cuda.stream(stream):
         for _ in range(WINDOW_START):
             frame()
@@ -387,6 +389,8 @@ def articulated_arm(dev, stream, flush, steps, warmup):
             solver.step(a, b, control, contacts, dt)
             a, b = b, a
 
+    # buffers allocated on the default stream above are used on `stream` below
+    stream.wait_stream(torch.cuda.current_stream(stream.device))
     with torch.cuda.stream(stream):
         for f in range(WINDOW_START):
             control.joint_target_pos.copy_(table_d[f])
@@ -462,6 +466,8 @@ def plain_arm(model, dt, substeps, sched, stream, flush, steps, warmup, iteratio
             solver.step(x, y, None, c, dt)
             x, y = y, x
 
+    # buffers allocated on the default stream above are used on `stream` below
+    stream.wait_stream(torch.cuda.current_stream(stream.device))
     with torch.cuda.stream(stream):
         for _ in range(WINDOW_START):
             frame()
@@ -528,6 +534,8 @@ def run_ours(args, rank, world_size, local_rank):
     s0, s1 = model.state(), model.state()
     contacts = pipe.contacts()
     stream = torch.cuda.Stream(dev)
+    # the scene's and the contacts' buffers were allocated (and zero-filled) on the default stream
+    stream.wait_stream(torch.cuda.current_stream(dev))
 
     def frame():
         a, b = s0, s1

@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 17
+#define NB_ABI_VERSION 18
 
 enum {
     NB_OK = 0,
@@ -178,6 +178,11 @@ typedef struct NbModelDesc {
                                           _update_effective_inv_mass_inertia, solver.py:160-174); the
                                           caller refreshes it when the model's mass properties or flags
                                           change.  Required by step_mode 2. */
+    const int32_t* pair_table;         /* broad_phase 1, optional: per world a dense ns x ns table of
+                                          pair indices (ns = the world's shapes + the global shapes;
+                                          -1 = no listed pair; both orientations), at
+                                          world_table_start[w]; NULL: binary search of the pair list */
+    const int64_t* world_table_start;  /* [W+1] offsets into pair_table */
 } NbModelDesc;
 
 /* Contact slots and the per-substep collision work buffers (written by
@@ -344,6 +349,11 @@ typedef struct NbStepIO {
 
 /* ABI version of the loaded library (NB_ABI_VERSION). */
 int nb_abi_version(void);
+
+/* The cudaError_t behind the last NB_ERR_CUDA an entry point returned on the
+ * calling host thread (0 if none), and CUDA's description of a cudaError_t. */
+int nb_last_cuda_error(void);
+const char* nb_cuda_error_string(int code);
 
 
 /* Number of CTAs the persistent kernels launch on the current device. */

@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 17
+NB_ABI_VERSION = 18
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -142,6 +142,8 @@ class NbModelDesc(C.Structure):
         ("batch_world", _fp),
         ("batch_slab", _fp),
         ("body_pack", _fp),
+        ("pair_table", _fp),
+        ("world_table_start", _fp),
     ]
 
 

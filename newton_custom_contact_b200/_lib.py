@@ -44,6 +44,8 @@ BUILDS = {"product": LIB_PATH, "exact": os.path.join(_HERE, "libnewton_b200_exac
 
 EXPORTS = (
     "nb_abi_version",
+    "nb_last_cuda_error",
+    "nb_cuda_error_string",
     "nb_default_grid",
     "nb_clear_forces",
     "nb_collide",
@@ -101,9 +103,13 @@ class NbError(RuntimeError):
         NB_ERR_CAPACITY: "capacity exceeded",
     }
 
-    def __init__(self, fn: str, code: int):
-        super().__init__(f"{fn} failed: {self._names.get(code, 'error')} (code {code})")
+    def __init__(self, fn: str, code: int, cuda_error: int = 0, cuda_message: str = ""):
+        msg = f"{fn} failed: {self._names.get(code, 'error')} (code {code})"
+        if cuda_error:
+            msg += f": cudaError {cuda_error} ({cuda_message})"
+        super().__init__(msg)
         self.code = code
+        self.cuda_error = cuda_error
 
 
 def load(path: str | None = None) -> C.CDLL:
@@ -118,6 +124,9 @@ def load(path: str | None = None) -> C.CDLL:
         )
     lib = C.CDLL(p)
     lib.nb_abi_version.restype = C.c_int
+    lib.nb_last_cuda_error.restype = C.c_int
+    lib.nb_cuda_error_string.restype = C.c_char_p
+    lib.nb_cuda_error_string.argtypes = [C.c_int]
     lib.nb_default_grid.restype = C.c_int32
     lib.nb_clear_forces.restype = C.c_int
     lib.nb_clear_forces.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
@@ -170,7 +179,12 @@ def load(path: str | None = None) -> C.CDLL:
 
 def check(fn: str, rc: int) -> None:
     if rc != 0:
-        raise NbError(fn, rc)
+        cuda_error, message = 0, ""
+        if rc == NB_ERR_CUDA and _active in _libs:
+            lib = _libs[_active]
+            cuda_error = int(lib.nb_last_cuda_error())
+            message = (lib.nb_cuda_error_string(cuda_error) or b"").decode(errors="replace")
+        raise NbError(fn, rc, cuda_error, message)
 
 
 def require_cuda(device) -> None:

@@ -171,6 +171,26 @@ class PairLayout:
             "world_order": self.world_order,
         }
 
+    def pair_table(self, model) -> tuple:
+        """Per world a dense ns x ns table (ns = the world's shape slots: its own shapes, then the global
+        ones) of pair indices, -1 where the slots form no listed pair, both orientations filled; and the
+        tables' int64 start offsets [W + 1].  The sweep and prune broad phase looks its overlaps up here."""
+        W = self.world_count
+        nloc = np.diff(model._part["world_shape_start"].astype(np.int64))
+        ns = nloc + model._part["global_shapes"].size
+        start = np.zeros(W + 1, np.int64)
+        start[1:] = np.cumsum(ns * ns)
+        table = np.full(int(start[-1]), -1, np.int32)
+        P = self.pair_count
+        if P:
+            w = np.repeat(np.arange(W), np.diff(self.world_pair_start.astype(np.int64)))
+            la = self.pair_slots[:, 0].astype(np.int64)
+            lb = self.pair_slots[:, 1].astype(np.int64)
+            idx = np.arange(P, dtype=np.int32)
+            table[start[w] + la * ns[w] + lb] = idx
+            table[start[w] + lb * ns[w] + la] = idx
+        return table, start
+
     def info(self) -> dict:
         return {"pair_count": self.pair_count, "max_world_pairs": self.max_world_pairs,
                 "contact_capacity": self.contact_capacity}
@@ -244,6 +264,10 @@ class CollisionPipeline:
         hd = self.layout.host_dict()
         self._layout_host = hd
         self._layout_dev = {k: torch.from_numpy(np.ascontiguousarray(v)).to(self.device) for k, v in hd.items()}
+        if mode == "sap":
+            table, start = self.layout.pair_table(model)
+            self._layout_dev["pair_table"] = torch.from_numpy(table).to(self.device)
+            self._layout_dev["world_table_start"] = torch.from_numpy(start).to(self.device)
         self._desc = None
         self._grid = None
         self._schedule = None
@@ -366,6 +390,9 @@ class CollisionPipeline:
             self._desc = self.model.make_desc(arrays, self.layout.info())
             # broad_phase="sap": sweep and prune per world over the NxN candidate list
             self._desc.broad_phase = 1 if self.broad_phase_mode == "sap" else 0
+            if "pair_table" in self._layout_dev:
+                self._desc.pair_table = ptr(self._layout_dev["pair_table"])
+                self._desc.world_table_start = ptr(self._layout_dev["world_table_start"])
         return self._desc
 
     def grid(self) -> int:

@@ -108,9 +108,24 @@ cudaError_t nb_raise_dynamic_smem(const void* kernel, size_t bytes) {
     return e;
 }
 
+namespace {
+// the CUDA error behind the last NB_ERR_CUDA this host thread received
+thread_local int g_last_cuda_error = 0;
+}  // namespace
+
+int nb_cuda_rc(cudaError_t e) {
+    if (e == cudaSuccess) return NB_OK;
+    g_last_cuda_error = (int)e;
+    return NB_ERR_CUDA;
+}
+
 extern "C" {
 
 int nb_abi_version(void) { return NB_ABI_VERSION; }
+
+int nb_last_cuda_error(void) { return g_last_cuda_error; }
+
+const char* nb_cuda_error_string(int code) { return cudaGetErrorString((cudaError_t)code); }
 
 int32_t nb_default_grid(void) { return grid_for(0); }
 
@@ -118,7 +133,7 @@ int nb_clear_forces(float* body_f, int32_t n_bodies, void* stream) {
     if (n_bodies < 0 || (n_bodies > 0 && !body_f)) return NB_ERR_INVALID;
     if (n_bodies == 0) return NB_OK;
     const cudaError_t e = cudaMemsetAsync(body_f, 0, sizeof(float) * 6 * (size_t)n_bodies, (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 int nb_collide(const NbModelDesc* model, const float* body_q, const NbContactSeg* seg, int32_t grid_ctas,
@@ -134,7 +149,7 @@ int nb_collide(const NbModelDesc* model, const float* body_q, const NbContactSeg
     // grid_ctas <= 0: each narrow-phase kernel uses its own default (enough CTAs
     // to reach its register-limited occupancy)
     cudaError_t e = nb_launch_collide(model, body_q, seg, grid_ctas > 0 ? grid_ctas : 0, (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 int nb_publish_contacts(const NbModelDesc* model, const NbContactSeg* seg, const NbContactsPublic* pub,
@@ -147,7 +162,7 @@ int nb_publish_contacts(const NbModelDesc* model, const NbContactSeg* seg, const
                               !pub->offset1 || !pub->normal || !pub->margin0 || !pub->margin1))
         return NB_ERR_INVALID;
     cudaError_t e = nb_launch_publish(model, seg, pub, (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 int nb_ingest_contacts(const NbModelDesc* model, const NbContactsPublic* pub, const NbContactSeg* seg,
@@ -158,7 +173,7 @@ int nb_ingest_contacts(const NbModelDesc* model, const NbContactsPublic* pub, co
     if (!pub || !pub->count || pub->capacity < 0) return NB_ERR_INVALID;
     if (!model->world_pair_start || !model->shape_body) return NB_ERR_INVALID;
     cudaError_t e = nb_launch_ingest(model, pub, seg, (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbStepIO* io, const NbContactSeg* seg,
@@ -179,7 +194,7 @@ int nb_xpbd_step(const NbModelDesc* model, const NbXpbdParams* params, const NbS
     if (seg->rec && (rc = check_step_seg(seg))) return rc;
     if ((int64_t)nb_step_smem_bytes(model) > smem_limit()) return NB_ERR_UNSUPPORTED;
     cudaError_t e = nb_launch_step(model, params, io, seg, dt, grid_for(grid_ctas), (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 int nb_xpbd_step_adjoint(const NbModelDesc* model, const NbXpbdParams* params, const NbAdjointIO* io,
@@ -206,7 +221,7 @@ int nb_xpbd_step_adjoint(const NbModelDesc* model, const NbXpbdParams* params, c
     if (io->branch_mode < 0 || io->branch_mode > 2 || (io->branch_mode == 2 && !forward_only)) return NB_ERR_INVALID;
     if (io->branch_mode != 0 && (!io->branch_body || (has_contacts && !io->branch_contact))) return NB_ERR_INVALID;
     cudaError_t e = nb_launch_xpbd_adjoint(model, params, io, seg, has_contacts, dt, (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 int nb_xpbd_substeps(const NbModelDesc* model, const NbXpbdParams* params, const NbStepIO* io,
@@ -237,7 +252,7 @@ int nb_xpbd_substeps(const NbModelDesc* model, const NbXpbdParams* params, const
                             cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
             cudaMemcpyAsync(io->body_qd_out, io->body_qd_in, sizeof(float) * 6 * (size_t)model->body_count,
                             cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-            return NB_ERR_CUDA;
+            return nb_cuda_rc(cudaGetLastError());
     }
     return NB_OK;
 }
@@ -258,7 +273,7 @@ int nb_match_contacts(const NbModelDesc* model, const float* body_q, const NbCon
         return NB_ERR_INVALID;
     if (st->capacity == 0) return NB_OK;
     cudaError_t e = nb_launch_match(model, body_q, pub, seg, st, (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 int nb_ws_features(const NbModelDesc* model, const float* body_q, const float* body_qd, const NbContactsPublic* pub,
@@ -274,13 +289,13 @@ int nb_ws_features(const NbModelDesc* model, const float* body_q, const float* b
         return NB_ERR_INVALID;
     cudaError_t e = nb_launch_ws_features(model, body_q, body_qd, pub, prev_lambda, match_index, body_count, dt,
                                           features, (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 int nb_ws_targets(const NbContactsPublic* pub, float* impulse, float* lambda, int32_t clear_impulse, void* stream) {
     if (!pub || !pub->count || !pub->normal || !impulse || !lambda || pub->capacity < 0) return NB_ERR_INVALID;
     cudaError_t e = nb_launch_ws_targets(pub, impulse, lambda, clear_impulse != 0, (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 int nb_ws_infer(const NbWsNet* net, const float* features, const int32_t* count, int32_t capacity, float* lambda,
@@ -293,7 +308,7 @@ int nb_ws_infer(const NbWsNet* net, const float* features, const int32_t* count,
          reinterpret_cast<uintptr_t>(net->w3)) & 15u)
         return NB_ERR_INVALID;
     cudaError_t e = nb_launch_ws_infer(net, features, count, capacity, lambda, status, (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 int nb_ws_grads(const NbWsTrain* a, void* stream) {
@@ -303,7 +318,7 @@ int nb_ws_grads(const NbWsTrain* a, void* stream) {
         !a->dh2 || !a->scratch_wq || !a->loss || !a->status)
         return NB_ERR_INVALID;
     cudaError_t e = nb_launch_ws_grads(a, (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 int nb_ws_adam(float* w, const float* grad, float* m1, float* m2, int64_t count, float lr, float beta1, float beta2,
@@ -311,7 +326,7 @@ int nb_ws_adam(float* w, const float* grad, float* m1, float* m2, int64_t count,
     if (!w || !grad || !m1 || !m2 || count < 0 || step < 1) return NB_ERR_INVALID;
     cudaError_t e = nb_launch_ws_adam(w, grad, m1, m2, (long)count, lr, beta1, beta2, eps, weight_decay, step,
                                       (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 int nb_contact_forces(const float* contact_impulse, const int32_t* count, int32_t capacity, float dt, float* force,
@@ -319,7 +334,7 @@ int nb_contact_forces(const float* contact_impulse, const int32_t* count, int32_
     if (capacity < 0 || (capacity > 0 && (!contact_impulse || !count || !force))) return NB_ERR_INVALID;
     if (!(dt > 0.0f)) return NB_ERR_INVALID;
     cudaError_t e = nb_launch_contact_forces(contact_impulse, count, capacity, dt, force, (cudaStream_t)stream);
-    return e == cudaSuccess ? NB_OK : NB_ERR_CUDA;
+    return nb_cuda_rc(e);
 }
 
 }  // extern "C"

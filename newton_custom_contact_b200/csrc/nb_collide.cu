@@ -414,6 +414,7 @@ __device__ bool world_by_warp_sap(const NbModelDesc& m, const NbContactSeg& seg,
     __syncwarp();
     warp_bitonic(sc.key, sc.idx, n, lane);
     const int p0 = m.world_pair_start[w], p1 = m.world_pair_start[w + 1];
+    const int32_t* tbl = m.pair_table ? m.pair_table + m.world_table_start[w] : nullptr;
     for (int i = lane; i < ns; i += 32) {
         const int a = sc.idx[i];
         if (a >= ns) continue;
@@ -425,18 +426,23 @@ __device__ bool world_by_warp_sap(const NbModelDesc& m, const NbContactSeg& seg,
             const float4 bl = lo[b], bh = hi[b];
             if (!(al.x <= bh.x && ah.x >= bl.x && al.y <= bh.y && ah.y >= bl.y && al.z <= bh.z && ah.z >= bl.z))
                 continue;
-            const int tb = __float_as_int(bl.w);
-            const int ga = slot_shape(m, s0, nloc, a), gb = slot_shape(m, s0, nloc, b);
-            // the pair list orders each pair by shape type (narrow_phase.py:207-210); equal types keep the
-            // list's own order, so both orientations are looked up
             int pidx;
-            if (ta < tb) pidx = find_pair(m, p0, p1, s0, nloc, ga, gb);
-            else if (ta > tb) pidx = find_pair(m, p0, p1, s0, nloc, gb, ga);
-            else {
-                pidx = find_pair(m, p0, p1, s0, nloc, ga, gb);
-                if (pidx < 0) pidx = find_pair(m, p0, p1, s0, nloc, gb, ga);
+            if (tbl) {
+                // the world's dense slot-pair table: one load
+                pidx = __ldg(tbl + (size_t)a * ns + b);
+            } else {
+                const int tb = __float_as_int(bl.w);
+                const int ga = slot_shape(m, s0, nloc, a), gb = slot_shape(m, s0, nloc, b);
+                // the pair list orders each pair by shape type (narrow_phase.py:207-210); equal types keep
+                // the list's own order, so both orientations are looked up
+                if (ta < tb) pidx = find_pair(m, p0, p1, s0, nloc, ga, gb);
+                else if (ta > tb) pidx = find_pair(m, p0, p1, s0, nloc, gb, ga);
+                else {
+                    pidx = find_pair(m, p0, p1, s0, nloc, ga, gb);
+                    if (pidx < 0) pidx = find_pair(m, p0, p1, s0, nloc, gb, ga);
+                }
             }
-            if (pidx < 0) continue;
+            if (pidx < p0 || pidx >= p1) continue;  // -1: not a listed pair
             const int h = atomicAdd(&sc.nhit, 1);
             if (h < kSapHits) sc.hit[h] = pidx;
         }
@@ -563,11 +569,18 @@ struct NarrowItem {
     Writer wr;
 };
 
-__device__ __forceinline__ void narrow_setup(const NbModelDesc& m, const NbContactSeg& seg, const float* body_q,
+// false (and NB_STATUS_CONTACT_OVERFLOW) for a queue entry whose candidate or world is out of range --
+// never produced by the broad phase; the check keeps a corrupted queue from indexing past the arrays
+__device__ __forceinline__ bool narrow_setup(const NbModelDesc& m, const NbContactSeg& seg, const float* body_q,
                                              int2 e, NarrowItem& it) {
     const float4* geom = reinterpret_cast<const float4*>(seg.geom);
     it.c = e.x;
     it.w = e.y;
+    if ((unsigned)it.c >= (unsigned)m.pair_count || (unsigned)it.w >= (unsigned)m.world_count ||
+        (unsigned)seg.cand[it.c] >= (unsigned)m.pair_count) {
+        atomicOr(seg.status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
+        return false;
+    }
     const unsigned pw = reinterpret_cast<const unsigned*>(m.pair_shapes)[seg.cand[it.c]];
     const int la = (int)(pw & 0xFFFFu), lb = (int)(pw >> 16);
     const int s0 = m.world_shape_start[it.w];
@@ -587,6 +600,7 @@ __device__ __forceinline__ void narrow_setup(const NbModelDesc& m, const NbConta
     const int lba = it.ga.body < 0 ? -1 : it.ga.body - b0;
     const int lbb = it.gb.body < 0 ? -1 : it.gb.body - b0;
     it.wr.tag = ((lba + 1) & 0xFFF) | (((lbb + 1) & 0xFFF) << 12);
+    return true;
 }
 
 __device__ __forceinline__ void narrow_finish(const NbContactSeg& seg, const NarrowItem& it) {
@@ -604,7 +618,7 @@ narrow_analytic_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContac
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n0; i += gridDim.x * blockDim.x) {
         const int2 e = queue[i];
         NarrowItem it;
-        narrow_setup(m, seg, body_q, e, it);
+        if (!narrow_setup(m, seg, body_q, e, it)) continue;
         if (narrow_analytic(it.wr, it.ga, it.gb)) {
             narrow_finish(seg, it);
         } else {
@@ -748,7 +762,7 @@ narrow_gjk_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg 
     const int2* queue = reinterpret_cast<const int2*>(seg.queue);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         NarrowItem it;
-        narrow_setup(m, seg, body_q, i < n_box ? queue[i] : queue[n1 - 1 - (i - n_box)], it);
+        if (!narrow_setup(m, seg, body_q, i < n_box ? queue[i] : queue[n1 - 1 - (i - n_box)], it)) continue;
         gjk_pair(it.wr, it.ga, it.gb);
         narrow_finish(seg, it);
     }
@@ -820,14 +834,20 @@ __global__ void __launch_bounds__(256) publish_kernel(NbModelDesc m, NbContactSe
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const float4* slots = reinterpret_cast<const float4*>(seg.slots);
     float4* rec = reinterpret_cast<float4*>(seg.rec);
+    const int64_t rec_cap = 5 * (int64_t)m.pair_count;
     for (int w = gw; w < m.world_count; w += nw) {
-        const int nc = seg.cand_count[w];
         const int c0 = m.world_pair_start[w];
+        // a world's candidates never exceed its pairs, a candidate's contacts never exceed 5; the
+        // clamps keep corrupted counts from indexing past the slots
+        const int npair = m.world_pair_start[w + 1] - c0;
+        int nc = seg.cand_count[w];
+        nc = nc < 0 ? 0 : (nc > npair ? npair : nc);
         const int64_t dst0 = pub.world_offset[w];
         int64_t running = 0;
         for (int base = 0; base < nc; base += 32) {
             const int i = base + lane;
-            const int n = i < nc ? (int)seg.counts[c0 + i] : 0;
+            int n = i < nc ? (int)seg.counts[c0 + i] : 0;
+            n = n > 5 ? 5 : n;
             int x = n;  // inclusive scan of the chunk's counts
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -851,7 +871,11 @@ __global__ void __launch_bounds__(256) publish_kernel(NbModelDesc m, NbContactSe
                 const float4 a = sl[0], b = sl[1], c = sl[2], e = sl[3], f = sl[4];
                 // solver record: the tag moves next to the normal so the
                 // penetration test reads the first 48 bytes only
-                float4* r = rec + (size_t)d * 5;  // rec holds 5 * pair_count records: never overflows
+                if (d < 0 || d >= rec_cap) {  // rec holds 5 * pair_count records: only corrupted offsets get here
+                    atomicOr(seg.status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
+                    continue;
+                }
+                float4* r = rec + (size_t)d * 5;
                 r[0] = a;
                 r[1] = b;
                 r[2] = make_float4(c.x, c.y, c.z, f.w);

@@ -43,6 +43,9 @@ cudaError_t nb_launch_ws_adam(float* w, const float* g, float* m1, float* m2, lo
 // legal inside CUDA-graph capture.
 cudaError_t nb_raise_dynamic_smem(const void* kernel, size_t bytes);
 
+// NB_OK for cudaSuccess; otherwise records e for nb_last_cuda_error() and returns NB_ERR_CUDA
+int nb_cuda_rc(cudaError_t e);
+
 cudaError_t nb_launch_xpbd_adjoint(const NbModelDesc* m, const NbXpbdParams* p, const NbAdjointIO* io,
                                    const NbContactSeg* seg, int has_contacts, float dt, cudaStream_t s);
 

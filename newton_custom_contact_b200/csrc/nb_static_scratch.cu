@@ -67,7 +67,8 @@ extern "C" int nb_publish_contacts_static(const NbModelDesc* model, const NbCont
     if (model->world_count <= 0) return NB_ERR_INVALID;
     if (model->world_count > NB_PUBLISH_STATIC_MAX_WORLDS) return NB_ERR_CAPACITY;
     int64_t* scratch = nullptr;
-    if (scratch_address(&scratch) != cudaSuccess) return NB_ERR_CUDA;
+    const cudaError_t e = scratch_address(&scratch);
+    if (e != cudaSuccess) return nb_cuda_rc(e);
     NbContactsPublic p = *pub;
     p.world_offset = scratch;
     return nb_publish_contacts(model, seg, &p, stream);

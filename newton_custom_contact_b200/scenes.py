@@ -177,6 +177,31 @@ def scene_c1(seed: int = 0, device=None):
     return model, dict(dt=1.0 / 60.0, substeps=10, iterations=4, name="C1: 64 boxes, 1 world")
 
 
+def scene_c1_batch(seed: int = 100, worlds: int = 1024, device=None):
+    """C1 scenes side by side: world w is scene_c1(seed + w) (64 boxes, its own random half-extents,
+    jittered grid and orientations), all on one global ground plane (mu 0.5).  The learned warm start's
+    C1 training and evaluation sets.  Returns (model, info) with C1's dt / substeps / iterations."""
+    n = 64
+    half, poses = [], []
+    gx = np.linspace(-0.5, 0.5, 4)
+    gz = np.linspace(0.2, 2.0, 4)
+    cx, cy, cz = np.meshgrid(gx, gx, gz, indexing="ij")
+    grid = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], axis=1)
+    for w in range(worlds):
+        # the same draws, in the same order, as scene_c1(seed + w)
+        rng = np.random.default_rng(seed + w)
+        h = rng.uniform(0.05, 0.15, size=(n, 3))
+        centers = grid + rng.uniform(-0.02, 0.02, size=grid.shape)
+        quats = random_quats(rng, n)
+        half.append(h)
+        poses.append(np.concatenate([centers, quats], axis=1))
+    body_world = np.repeat(np.arange(worlds), n)
+    types = np.full(worlds * n, int(GeoType.BOX))
+    model = assemble_free_bodies(body_world, types, np.concatenate(half), np.concatenate(poses),
+                                 np.full(worlds * n, 0.5), worlds, plane_mu=0.5, device=device)
+    return model, dict(dt=1.0 / 60.0, substeps=10, iterations=4, name=f"C1 x {worlds} (seeds {seed}..)")
+
+
 def _bounding_radius(t, s):
     if t == int(GeoType.BOX):
         return float(np.linalg.norm(s))

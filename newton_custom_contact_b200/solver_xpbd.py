@@ -112,8 +112,11 @@ class SolverXPBD:
         _lib.require_cuda(model.device)
         if model.body_count == 0:
             return
+        # control=None: the model's default targets and no joint forces (the reference builds
+        # model.control(), whose joint_f is zero; a null joint_f skips the same work without a fill)
+        joint_f = None if control is None else control.joint_f
         if control is None:
-            control = model.control(clone_variables=False)
+            control = model
         B = model.body_count
         self._check_state("state_in.body_q", state_in.body_q, (B, 7))
         self._check_state("state_in.body_qd", state_in.body_qd, (B, 6))
@@ -149,7 +152,7 @@ class SolverXPBD:
         io.body_qd_out = ptr(state_out.body_qd)
         io.joint_target_pos = ptr(control.joint_target_pos)
         io.joint_target_vel = ptr(control.joint_target_vel)
-        io.joint_f = ptr(control.joint_f)
+        io.joint_f = ptr(joint_f)
         if state_out.body_parent_f is not None:
             # incoming joint wrench per body (solver_xpbd.py:294-297, 636-655)
             self._check_state("state_out.body_parent_f", state_out.body_parent_f, (B, 6))
@@ -217,13 +220,12 @@ class SolverXPBD:
             contacts._world_offset = torch.zeros(model.world_count + 1, dtype=torch.int64, device=model.device)
         lib = _lib.load()
         desc = pipe.desc()
-        control = model.control(clone_variables=False)
         io = NbStepIO()
         io.body_q_in, io.body_qd_in, io.body_f_in = ptr(state_in.body_q), ptr(state_in.body_qd), ptr(state_in.body_f)
         io.body_q_out, io.body_qd_out = ptr(state_out.body_q), ptr(state_out.body_qd)
-        io.joint_target_pos = ptr(control.joint_target_pos)
-        io.joint_target_vel = ptr(control.joint_target_vel)
-        io.joint_f = ptr(control.joint_f)
+        # the model's default targets, no joint forces (a default Control's joint_f is zero)
+        io.joint_target_pos = ptr(model.joint_target_pos)
+        io.joint_target_vel = ptr(model.joint_target_vel)
         params = self.params()
         _lib.check("nb_xpbd_substeps", lib.nb_xpbd_substeps(
             C.byref(desc), C.byref(params), C.byref(io), C.byref(pipe.seg_struct(contacts)),

@@ -28,14 +28,15 @@ from .metrics import penetration_stats
 from .warmstart import WarmStart, WarmStartNet, corrections
 
 DT = 1.0 / 480.0
-SCENE = "c2"  # "c2": uneven worlds of boxes / spheres / capsules; "c5": 16-box stacks (dt 1/600)
+SCENE = "c2"  # "c2": uneven worlds of boxes / spheres / capsules; "c5": 16-box stacks (dt 1/600);
+              # "c1": C1's 64-box worlds, one seed per world (dt 1/600)
 
 
 def set_scene(kind: str) -> None:
     """Scene family the training / evaluation helpers build (and its substep)."""
     global SCENE, DT
-    if kind not in ("c2", "c5"):
-        raise ValueError("scene must be 'c2' or 'c5'")
+    if kind not in ("c1", "c2", "c5"):
+        raise ValueError("scene must be 'c1', 'c2' or 'c5'")
     SCENE = kind
     DT = 1.0 / 480.0 if kind == "c2" else 1.0 / 600.0
 
@@ -43,6 +44,9 @@ def set_scene(kind: str) -> None:
 def make_scene(seed: int, worlds: int, device):
     if SCENE == "c5":
         m, _ = scenes.scene_c5(seed=seed, worlds=worlds, device=device)
+    elif SCENE == "c1":
+        # C1 seeds: training from 100 on, evaluation from 100000 on (unseen)
+        m, _ = scenes.scene_c1_batch(seed=seed, worlds=worlds, device=device)
     else:
         m, _ = scenes.scene_c2(seed=seed, worlds=worlds, device=device)
     pipe = CollisionPipeline(m, contact_matching="latest")
@@ -142,6 +146,8 @@ def timed_frames(m, pipe, iterations: int, policy: WarmStart | None, warmup: int
     c = pipe.contacts()
     pipe.reset_contact_matching()
     stream = torch.cuda.Stream()
+    # the contacts' buffers were allocated (and zero-filled) on the default stream
+    stream.wait_stream(torch.cuda.current_stream())
 
     def frame():
         a, b = s0, s1
@@ -200,7 +206,7 @@ def evaluate(net: WarmStartNet, device="cuda", worlds: int = 1024, seed: int = 1
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--scene", default="c2", choices=["c2", "c5"])
+    ap.add_argument("--scene", default="c2", choices=["c1", "c2", "c5"])
     ap.add_argument("--out", default=None, help="network file (default: data/warmstart_<scene>.npz)")
     ap.add_argument("--train-seed", type=int, default=None)
     ap.add_argument("--eval-seed", type=int, default=None)
@@ -217,8 +223,8 @@ def main():
     if a.out is None:
         a.out = os.path.join(os.path.dirname(__file__), "data", f"warmstart_{a.scene}.npz")
     # training and evaluation scenes differ (unseen seed at evaluation)
-    train_seed = a.train_seed if a.train_seed is not None else (2 if a.scene == "c2" else 6)
-    eval_seed = a.eval_seed if a.eval_seed is not None else (1 if a.scene == "c2" else 5)
+    train_seed = a.train_seed if a.train_seed is not None else {"c1": 100, "c2": 2, "c5": 6}[a.scene]
+    eval_seed = a.eval_seed if a.eval_seed is not None else {"c1": 100000, "c2": 1, "c5": 5}[a.scene]
     t0 = time.time()
     if a.eval_only:
         net = WarmStartNet.load(a.out)

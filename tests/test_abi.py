@@ -23,7 +23,7 @@ def lib(request):
 
 def declared_functions():
     src = open(os.path.join(ROOT, "include", "newton_b200.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:int|int32_t|int64_t)\s+(nb_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int32_t|int64_t|const char\*)\s+(nb_\w+)\s*\(", src, re.M)))
 
 
 def test_header_declares_entry_points():

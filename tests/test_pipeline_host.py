@@ -221,3 +221,26 @@ def test_per_shape_gap_through_the_pipeline(orc):
     centre = np.array([10.0, 0.0, 0.24])
     sep = abs(float(np.dot(n, (p1 + centre if int(row[2]) == c else p1) - (p0 + centre if int(row[1]) == c else p0))))
     assert sep - (row[19] + row[20]) == pytest.approx(0.04, abs=1e-5)
+
+
+def test_sap_pair_table_indexes_the_pair_list():
+    """The sweep-and-prune pair table: for every listed pair both orientations of its slots give its
+    index in the pair list, and every other slot pair gives -1."""
+    from newton_custom_contact_b200 import scenes
+
+    model, _ = scenes.scene_c2(seed=5, worlds=6, nmin=8, nmax=20, device="cpu")
+    pipe = CollisionPipeline(model, broad_phase="sap")
+    lay = pipe.layout
+    table, start = lay.pair_table(model)
+    nloc = np.diff(model._part["world_shape_start"].astype(np.int64))
+    ns = nloc + model._part["global_shapes"].size
+    assert start[-1] == int(np.sum(ns * ns))
+    wps = lay.world_pair_start.astype(np.int64)
+    for w in range(model.world_count):
+        t = table[start[w]:start[w + 1]].reshape(ns[w], ns[w])
+        expect = np.full((ns[w], ns[w]), -1, np.int32)
+        for p in range(wps[w], wps[w + 1]):
+            a, b = lay.pair_slots[p]
+            expect[a, b] = expect[b, a] = p
+        assert np.array_equal(t, expect)
+    assert "pair_table" in pipe._layout_dev

@@ -97,3 +97,18 @@ def test_desc_all_joints_free():
     b.add_joint_fixed(-1, body)
     fixed = b.finalize(device="cpu")
     assert fixed.make_desc(fixed.host_arrays()).all_joints_free == 0
+
+
+def test_c1_batch_worlds_are_c1_scenes():
+    """scene_c1_batch(seed, W): world w holds exactly scene_c1(seed + w)'s boxes and poses."""
+    batch, info = scenes.scene_c1_batch(seed=100, worlds=5, device="cpu")
+    assert batch.world_count == 5 and batch.body_count == 5 * 64
+    hb = batch.host_arrays()
+    for w in (0, 3):
+        one, _ = scenes.scene_c1(seed=100 + w, device="cpu")
+        h1 = one.host_arrays()
+        sl = slice(64 * w, 64 * (w + 1))
+        assert np.array_equal(hb["body_q"][sl], h1["body_q"])
+        assert np.array_equal(hb["body_inv_mass"][sl], h1["body_inv_mass"])
+        assert np.array_equal(hb["shape_scale"][1 + 64 * w:1 + 64 * (w + 1)], h1["shape_scale"][1:])
+    assert info["substeps"] == 10 and info["iterations"] == 4
