@@ -227,6 +227,45 @@ __device__ void apply_body_delta(TF& q, V3& v, V3& w, V3 dlin, V3 dang, float we
     w = w1;
 }
 
+// apply_body_delta with a zero delta and weight 1 (the apply the joint pass runs after a world whose
+// joints are all free), bit for bit.  With a zero delta and finite inertia the angular terms are signed
+// zeros, and adding a signed zero changes no nonzero value: when every quaternion component is nonzero
+// and finite, no angular velocity component is -0 (the only value a signed zero can flip) or
+// non-finite, and the inertia and inverse inertia are finite, the result is the renormalised
+// quaternion, the position re-expressed about the com, the velocities with +0 added and the rest
+// thresholds -- the inertia terms are skipped.  Otherwise the general form runs.
+__device__ void apply_zero_delta(TF& q, V3& v, V3& w, V3 com, const M33& I, float inv_m, const M33& inv_I,
+                                 float dt) {
+    if (inv_m == 0.0f) return;
+    const Q4 q0 = q.q;
+    const bool q_ok = q0.x != 0.0f && q0.y != 0.0f && q0.z != 0.0f && q0.w != 0.0f && isfinite(q0.x) &&
+                      isfinite(q0.y) && isfinite(q0.z) && isfinite(q0.w);
+    const bool w_ok = isfinite(w.x) && isfinite(w.y) && isfinite(w.z) && !(w.x == 0.0f && signbit(w.x)) &&
+                      !(w.y == 0.0f && signbit(w.y)) && !(w.z == 0.0f && signbit(w.z));
+    // x * 0 is 0 for every finite x and NaN otherwise
+    float inert = 0.0f;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) inert += I.m[r][c] * 0.0f + inv_I.m[r][c] * 0.0f;
+    const V3 zero{0.0f, 0.0f, 0.0f};
+    if (!(q_ok && w_ok && inert == 0.0f)) {
+        apply_body_delta(q, v, w, zero, zero, 1.0f, com, I, inv_m, inv_I, dt);
+        return;
+    }
+    const V3 dp = mul(zero, inv_m * 1.0f);  // +0: the general form's dp
+    const Q4 q1 = qnormalize(q0);
+    V3 p1 = add(add(q.p, qrot(q0, com)), mul(dp, dt));
+    p1 = sub(p1, qrot(q1, com));
+    q = TF{p1, q1};
+    V3 v1 = add(v, dp);
+    V3 w1 = w;
+    if (length(v1) < 1e-4f) v1 = zero;
+    if (length(w1) < 1e-4f) w1 = zero;
+    v = v1;
+    w = w1;
+}
+
 // kernels.py:1945-1979
 __device__ float contact_constraint_delta(float err, Q4 qa, Q4 qb, float m_inv_a, float m_inv_b, const M33& Ia,
                                           const M33& Ib, V3 la, V3 lb, V3 aa, V3 ab, float relaxation, float dt) {
@@ -1156,7 +1195,7 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
                 const float im = S.inv_m(i);
                 const M33 I = S.inertia(i), iI = S.inv_inertia(i);
                 apply_body_delta(q, v, wv, dl, da, weight, com, I, im, iI, dt);
-                if (model_joints && !world_joints) apply_body_delta(q, v, wv, zero3, zero3, 1.0f, com, I, im, iI, dt);
+                if (model_joints && !world_joints) apply_zero_delta(q, v, wv, com, I, im, iI, dt);
                 S.set(i, q, v, wv);
             }
             group_sync<G>(g);
