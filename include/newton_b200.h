@@ -343,9 +343,10 @@ typedef struct NbStepIO {
     const float* ws_lambda;      /* [ws_capacity,3] learned warm start: predicted impulse of each public
                                     contact in its contact frame (n, t1, t2), or NULL (plain solve) */
     int32_t ws_capacity;         /* rows of ws_lambda */
-    int32_t pad1;
+    int32_t ws_flags;            /* NB_WS_KEEP_ALL: keep every world's prediction (no fallback) */
     int32_t* ws_fallback;        /* [1] worlds whose warm start was rejected (counter) or NULL */
 } NbStepIO;
+#define NB_WS_KEEP_ALL 1
 
 /* ABI version of the loaded library (NB_ABI_VERSION). */
 int nb_abi_version(void);

@@ -23,6 +23,8 @@ NB_STATUS_FIXED_OVERFLOW = 1 << 2
 NB_STATUS_QUEUE_TIMEOUT = 1 << 3
 NB_STATUS_WORLD_TOO_LARGE = 1 << 4
 
+NB_WS_KEEP_ALL = 1
+
 
 class GeoType(enum.IntEnum):
     """Shape types (newton/_src/geometry/types.py:46-77)."""
@@ -243,7 +245,7 @@ class NbStepIO(C.Structure):
         ("joint_impulse", _fp),
         ("ws_lambda", _fp),
         ("ws_capacity", C.c_int32),
-        ("pad1", C.c_int32),
+        ("ws_flags", C.c_int32),
         ("ws_fallback", _fp),
     ]
 

@@ -987,7 +987,7 @@ __device__ __forceinline__ void warm_start(const NbModelDesc& m, const NbStepIO&
     }
     group_sync<G>(g);
     const float pen1 = world_penetration<G>(S, R, nc, g, t, scratch);
-    if (!(pen1 <= pen0)) {
+    if (!(io.ws_flags & NB_WS_KEEP_ALL) && !(pen1 <= pen0)) {
         for (int i = t; i < nb; i += G) {
             const float* qo = io.body_q_out + 7 * (size_t)(b0 + i);
             const float* qdo = io.body_qd_out + 6 * (size_t)(b0 + i);

@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import CollisionPipeline, SolverXPBD, scenes
-from .metrics import penetration_stats
+from .metrics import contact_penetrations, penetration_stats
 from .warmstart import WarmStart, WarmStartNet, corrections
 
 DT = 1.0 / 480.0
@@ -204,6 +204,85 @@ def evaluate(net: WarmStartNet, device="cuda", worlds: int = 1024, seed: int = 1
     return out
 
 
+def _world_residuals(m, c, body_q, world_of_contact):
+    """Largest penetration [m] of each world's contacts at poses `body_q` (0 for a world without any)."""
+    pen = contact_penetrations(m, c, body_q)
+    out = torch.zeros(m.world_count, dtype=torch.float64, device=body_q.device)
+    if pen.numel():
+        out.scatter_reduce_(0, world_of_contact[:pen.numel()], pen, reduce="amax")
+    return out
+
+
+def judge_check(net: WarmStartNet, device="cuda", worlds: int = 1024, seed: int = 1, iterations: int = 2,
+                substeps: int = 120, warmup: int = 48) -> dict:
+    """How often the warm start's fallback proxy (a world falls back when the prediction raises its largest
+    penetration before the iterations) disagrees with the north-star rule (a world falls back when its
+    residual after the iterations -- here its largest penetration at the end of the substep -- is worse
+    than the plain solver's).  Every measured substep runs, from the same state and contacts, the plain
+    solver (A), the warm start keeping every prediction (B) and the warm start with the proxy (C), and
+    follows C.  A world falls back under the proxy when C equals A bit for bit (a rejected prediction
+    reproduces the plain step exactly) and under the rule when B's residual exceeds A's; worlds whose
+    prediction changes nothing (B equals A) are not counted."""
+    dev = torch.device(device)
+    m, pipe = make_scene(seed, worlds, dev)
+    plain = SolverXPBD(m, iterations=iterations)
+    solver = SolverXPBD(m, iterations=iterations)
+    ws = WarmStart(net, iterations=iterations)
+    a, A, B, Cs = m.state(), m.state(), m.state(), m.state()
+    c = pipe.contacts()
+    pipe.reset_contact_matching()
+    bw = m.body_world.to(dev).long()
+    stats = {"worlds_judged": 0, "agree": 0, "proxy_keeps_rule_rejects": 0, "proxy_rejects_rule_keeps": 0,
+             "residual_mm": {"plain": 0.0, "proxy": 0.0, "rule": 0.0}}
+    n_meas = 0
+    for i in range(warmup + substeps):
+        a.clear_forces()
+        pipe.collide(a, c)
+        live = i >= warmup
+        if live:
+            plain.step(a, A, None, c, DT)
+            prev = ws._bufs["prev"].clone() if ws._bufs is not None else None
+            ws.judge = "none"
+            solver.warm_start = ws
+            solver.step(a, B, None, c, DT)
+            if prev is not None:
+                ws._bufs["prev"].copy_(prev)
+            ws.judge = "proxy"
+        solver.warm_start = ws
+        solver.step(a, Cs, None, c, DT)
+        if live:
+            wo = c._world_offset
+            woc = torch.repeat_interleave(torch.arange(m.world_count, device=dev), (wo[1:] - wo[:-1]).clamp(min=0))
+            r_a = _world_residuals(m, c, A.body_q, woc)
+            r_b = _world_residuals(m, c, B.body_q, woc)
+            r_c = _world_residuals(m, c, Cs.body_q, woc)
+
+            def world_all(eq):
+                out = torch.ones(m.world_count, dtype=torch.int32, device=dev)
+                return out.scatter_reduce(0, bw, eq.to(torch.int32), reduce="amin") == 1
+
+            same_ab = world_all((A.body_q == B.body_q).all(1) & (A.body_qd == B.body_qd).all(1))
+            same_ac = world_all((A.body_q == Cs.body_q).all(1) & (A.body_qd == Cs.body_qd).all(1))
+            judged = ~same_ab
+            proxy_fb = same_ac & judged
+            rule_fb = (r_b > r_a) & judged
+            stats["worlds_judged"] += int(judged.sum())
+            stats["agree"] += int((judged & (proxy_fb == rule_fb)).sum())
+            stats["proxy_keeps_rule_rejects"] += int((judged & ~proxy_fb & rule_fb).sum())
+            stats["proxy_rejects_rule_keeps"] += int((judged & proxy_fb & ~rule_fb).sum())
+            r_rule = torch.where(rule_fb, r_a, r_b)
+            for k, r in (("plain", r_a), ("proxy", r_c), ("rule", r_rule)):
+                stats["residual_mm"][k] += float(r.max()) * 1e3
+            n_meas += 1
+        a, Cs = Cs, a
+    for k in stats["residual_mm"]:
+        stats["residual_mm"][k] /= max(n_meas, 1)
+    stats["agree_fraction"] = stats["agree"] / max(stats["worlds_judged"], 1)
+    stats["iterations"] = iterations
+    stats["substeps"] = substeps
+    return stats
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--scene", default="c2", choices=["c1", "c2", "c5"])
@@ -218,8 +297,22 @@ def main():
     ap.add_argument("--student-iterations", type=int, default=2)
     ap.add_argument("--report", default=None)
     ap.add_argument("--eval-only", action="store_true", help="evaluate the network saved at --out")
+    ap.add_argument("--judge-check", action="store_true",
+                    help="also measure how often the fallback proxy disagrees with the residual rule")
+    ap.add_argument("--profile-arm", default=None, metavar="plain|warm",
+                    help="only run one arm (--student-iterations iterations, warm: the network at --out) for "
+                         "--profile-substeps substeps after 64 warm-up substeps, for a profiler's launch list")
+    ap.add_argument("--profile-substeps", type=int, default=16)
     a = ap.parse_args()
     set_scene(a.scene)
+    if a.profile_arm is not None:
+        if a.out is None:
+            a.out = os.path.join(os.path.dirname(__file__), "data", f"warmstart_{a.scene}.npz")
+        m, pipe = make_scene(a.eval_seed if a.eval_seed is not None else 1, a.worlds, torch.device("cuda"))
+        pol = WarmStart(WarmStartNet.load(a.out), iterations=a.student_iterations) if a.profile_arm == "warm" else None
+        rollout(m, pipe, a.student_iterations, a.profile_substeps, policy=pol, warmup=64, measure=False)
+        torch.cuda.synchronize()
+        return
     if a.out is None:
         a.out = os.path.join(os.path.dirname(__file__), "data", f"warmstart_{a.scene}.npz")
     # training and evaluation scenes differ (unseen seed at evaluation)
@@ -237,6 +330,8 @@ def main():
         res = {"train": info, "train_s": time.time() - t0}
     res["scene"] = a.scene
     res["eval"] = evaluate(net, worlds=a.worlds, seed=eval_seed, student_iterations=(a.student_iterations, 4))
+    if a.judge_check:
+        res["judge"] = judge_check(net, worlds=a.worlds, seed=eval_seed, iterations=a.student_iterations)
     print(json.dumps(res, indent=1))
     if a.report:
         with open(a.report, "w") as f:

@@ -33,7 +33,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._abi import NbWsNet, NbWsTrain, ptr
+from ._abi import NB_WS_KEEP_ALL, NbWsNet, NbWsTrain, ptr
 
 N_IN, N_HID, N_OUT = 24, 128, 3
 N_FEAT = 27  # network inputs + generalised inverse masses (normal, tangents) + prior
@@ -276,9 +276,14 @@ class WarmStart:
     """
 
     def __init__(self, net: WarmStartNet | None, iterations: int | None = 2, record: bool = False,
-                 record_fraction: float = 1.0, seed: int = 0, gain=(1.0, 0.0)):
+                 record_fraction: float = 1.0, seed: int = 0, gain=(1.0, 0.0), judge: str = "proxy"):
         self.net = net
         self.iterations = iterations
+        # "proxy": a world falls back to no warm start when the prediction raises its largest penetration;
+        # "none": every prediction is kept (the judge measurement of train_warmstart.judge_check)
+        if judge not in ("proxy", "none"):
+            raise ValueError("judge must be 'proxy' or 'none'")
+        self.judge = judge
         # (normal, tangent) factors on the predictions; the tangential (friction) fit is poor
         # (R^2 ~0.4 against ~0.95 for the normal), and applying it raises penetration, so it is off
         self.gain = gain
@@ -331,6 +336,7 @@ class WarmStart:
             io.ws_lambda = ptr(b["lam"])
             io.ws_capacity = contacts.rigid_contact_max
             io.ws_fallback = ptr(b["fallback"])
+            io.ws_flags = NB_WS_KEEP_ALL if self.judge == "none" else 0
         # own impulse buffer (contacts without a force array): zero at allocation and kept zero by
         # nb_ws_targets, which clears the rows it reads; a solver-owned one is zeroed by the solver
         self._clear = not io.contact_impulse
@@ -370,3 +376,59 @@ class WarmStart:
     @property
     def fallback_count(self) -> int:
         return 0 if self._bufs is None else int(self._bufs["fallback"].item())
+
+
+def kernel_timing(kind: str = "infer", rows: int = 111000, warmup: int = 3, reps: int = 20, seed: int = 0,
+                  path: str | None = None) -> dict:
+    """Mean CUDA-event time of the network's tensor-core kernels on random inputs: ``"infer"`` =
+    nb_ws_infer on `rows` feature rows, ``"grads"`` = one nb_ws_grads call on `rows` samples.  The
+    network is the committed C2 one unless `path` is given."""
+    import os
+
+    path = path or os.path.join(os.path.dirname(__file__), "data", "warmstart_c2.npz")
+    net = WarmStartNet.load(path)
+    dev = net.device
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    if kind == "infer":
+        feat = torch.randn(rows, N_FEAT, generator=g).to(dev)
+        count = torch.tensor([rows], dtype=torch.int32, device=dev)
+        out = torch.empty(rows, N_OUT, dtype=torch.float32, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        for _ in range(warmup):
+            net.infer(feat, count, out, status)
+        torch.cuda.synchronize()
+        ev[0].record()
+        for _ in range(reps):
+            net.infer(feat, count, out, status)
+        ev[1].record()
+        flops = 2.0 * (N_IN * N_HID + N_HID * N_HID + N_HID * N_OUT) * rows
+    elif kind == "grads":
+        x = torch.randn(rows, N_IN, generator=g).to(dev)
+        t = torch.randn(rows, N_OUT, generator=g).to(dev)
+        for _ in range(warmup):
+            net.grads(x, t)
+        torch.cuda.synchronize()
+        ev[0].record()
+        for _ in range(reps):
+            net.grads(x, t)
+        ev[1].record()
+        flops = 3.0 * 2.0 * (N_IN * N_HID + N_HID * N_HID + N_HID * N_OUT) * rows
+    else:
+        raise ValueError("kind must be 'infer' or 'grads'")
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / reps
+    return {"kind": kind, "rows": rows, "ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="time the warm-start tensor-core kernels on random inputs")
+    ap.add_argument("--kernel", default="infer", choices=["infer", "grads"])
+    ap.add_argument("--rows", type=int, default=111000)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--reps", type=int, default=20)
+    a = ap.parse_args()
+    print(json.dumps(kernel_timing(a.kernel, a.rows, a.warmup, a.reps)))
