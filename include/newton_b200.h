@@ -526,9 +526,12 @@ int nb_contact_forces(const float* contact_impulse, const int32_t* count, int32_
  * writers) into solver records, bucketed by world.  Replaces nothing in the
  * reference (its solver reads the dense arrays directly,
  * xpbd/kernels.py:2062-2298).  Records keep the public order within each
- * world, and the solver sums each body's deltas in record order, so a caller
- * that writes the same contacts in another order changes the bodies' sums by
- * float rounding only.
+ * world (public indices are bucketed by world, then ranked; the buckets use
+ * seg->slots as scratch, which nb_collide rewrites anyway), and the solver
+ * sums each body's deltas in record order: the pipeline's own contacts
+ * ingested in their published order give the collide path's step bit for
+ * bit, and a caller that writes the same contacts in another order changes
+ * the bodies' sums by float rounding only, the same on every call.
  */
 int nb_ingest_contacts(const NbModelDesc* model, const NbContactsPublic* pub,
                        const NbContactSeg* seg, void* stream);

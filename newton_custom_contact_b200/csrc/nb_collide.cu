@@ -903,11 +903,16 @@ __global__ void __launch_bounds__(256) publish_kernel(NbModelDesc m, NbContactSe
     }
 }
 
-// Custom contacts in the public arrays -> solver records.  World w's k-th
-// contact goes to record world_pair_start[w]*5 + k (every world owns room for
-// 5 contacts per candidate pair); ingest_finalize_kernel clamps the counts and
-// sets world_base.
-__global__ void ingest_kernel(NbModelDesc m, NbContactsPublic pub, NbContactSeg seg) {
+// Custom contacts in the public arrays -> solver records, in two kernels.
+// ingest_bucket_kernel finds each public contact's world and appends its
+// public index to the world's bucket (world_pair_start[w]*5 + k: every world
+// owns room for 5 contacts per candidate pair; the buckets live in the slots
+// buffer, which collide rewrites anyway); the append order is that of the
+// atomics.  ingest_place_kernel (one CTA per world) ranks every bucket entry
+// by its public index and writes the record at the world's base + rank, so
+// the records of a world follow the public order whatever the atomics did
+// -- the order the solver sums each body's deltas in.
+__global__ void ingest_bucket_kernel(NbModelDesc m, NbContactsPublic pub, NbContactSeg seg) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     int n = pub.count[0] < pub.capacity ? pub.count[0] : pub.capacity;
     if (c >= n) return;
@@ -939,25 +944,54 @@ __global__ void ingest_kernel(NbModelDesc m, NbContactsPublic pub, NbContactSeg 
         atomicOr(seg.status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
         return;
     }
-    int la = b0 < 0 ? -1 : b0 - wb, lb = b1 < 0 ? -1 : b1 - wb;
-    int tag = ((la + 1) & 0xFFF) | (((lb + 1) & 0xFFF) << 12);
-    const size_t ri = (size_t)m.world_pair_start[w] * 5 + k;
-    if (seg.rec_index) seg.rec_index[ri] = c;
-    float4* sl = reinterpret_cast<float4*>(seg.rec) + ri * 5;
-    sl[0] = make_float4(pub.point0[3 * c], pub.point0[3 * c + 1], pub.point0[3 * c + 2], pub.margin0[c]);
-    sl[1] = make_float4(pub.point1[3 * c], pub.point1[3 * c + 1], pub.point1[3 * c + 2], pub.margin1[c]);
-    sl[2] = make_float4(pub.normal[3 * c], pub.normal[3 * c + 1], pub.normal[3 * c + 2], __int_as_float(tag));
-    sl[3] = make_float4(pub.offset0[3 * c], pub.offset0[3 * c + 1], pub.offset0[3 * c + 2], __int_as_float(s0));
-    sl[4] = make_float4(pub.offset1[3 * c], pub.offset1[3 * c + 1], pub.offset1[3 * c + 2], __int_as_float(s1));
+    reinterpret_cast<int32_t*>(seg.slots)[(size_t)m.world_pair_start[w] * 5 + k] = c;
 }
 
-__global__ void ingest_finalize_kernel(NbModelDesc m, NbContactSeg seg) {
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= m.world_count) return;
+constexpr int kIngestTile = 2048;  // bucket entries one CTA compares against at a time (shared memory)
+
+__global__ void __launch_bounds__(256) ingest_place_kernel(NbModelDesc m, NbContactsPublic pub, NbContactSeg seg) {
+    __shared__ int32_t s_tile[kIngestTile];
+    const int w = blockIdx.x;
     const int c0 = m.world_pair_start[w];
-    const int cap = 5 * (m.world_pair_start[w + 1] - c0);
-    seg.world_count[w] = seg.world_count[w] < cap ? seg.world_count[w] : cap;
-    seg.world_base[w] = 5 * (int64_t)c0;
+    const int room = 5 * (m.world_pair_start[w + 1] - c0);
+    int nw = seg.world_count[w];
+    nw = nw < room ? nw : room;
+    const int64_t base = 5 * (int64_t)c0;
+    const int32_t* bucket = reinterpret_cast<const int32_t*>(seg.slots) + base;
+    // rank of entry i = the number of the bucket's public indices below its own (indices are distinct)
+    for (int i0 = 0; i0 < nw; i0 += blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        const int32_t x = i < nw ? bucket[i] : 0;
+        int rank = 0;
+        for (int t0 = 0; t0 < nw; t0 += kIngestTile) {
+            const int len = nw - t0 < kIngestTile ? nw - t0 : kIngestTile;
+            __syncthreads();
+            for (int j = threadIdx.x; j < len; j += blockDim.x) s_tile[j] = bucket[t0 + j];
+            __syncthreads();
+            if (i < nw)
+                for (int j = 0; j < len; ++j) rank += s_tile[j] < x ? 1 : 0;
+        }
+        if (i >= nw) continue;
+        const int c = x;
+        const int s0 = pub.shape0[c], s1 = pub.shape1[c];
+        const int b0 = s0 >= 0 ? m.shape_body[s0] : -1;
+        const int b1 = s1 >= 0 ? m.shape_body[s1] : -1;
+        const int wb = m.world_body_start[w];
+        const int la = b0 < 0 ? -1 : b0 - wb, lb = b1 < 0 ? -1 : b1 - wb;
+        const int tag = ((la + 1) & 0xFFF) | (((lb + 1) & 0xFFF) << 12);
+        const int64_t ri = base + rank;
+        if (seg.rec_index) seg.rec_index[ri] = c;
+        float4* sl = reinterpret_cast<float4*>(seg.rec) + ri * 5;
+        sl[0] = make_float4(pub.point0[3 * c], pub.point0[3 * c + 1], pub.point0[3 * c + 2], pub.margin0[c]);
+        sl[1] = make_float4(pub.point1[3 * c], pub.point1[3 * c + 1], pub.point1[3 * c + 2], pub.margin1[c]);
+        sl[2] = make_float4(pub.normal[3 * c], pub.normal[3 * c + 1], pub.normal[3 * c + 2], __int_as_float(tag));
+        sl[3] = make_float4(pub.offset0[3 * c], pub.offset0[3 * c + 1], pub.offset0[3 * c + 2], __int_as_float(s0));
+        sl[4] = make_float4(pub.offset1[3 * c], pub.offset1[3 * c + 1], pub.offset1[3 * c + 2], __int_as_float(s1));
+    }
+    if (threadIdx.x == 0) {
+        seg.world_count[w] = nw;
+        seg.world_base[w] = base;
+    }
 }
 
 int sm_count() {
@@ -1054,10 +1088,10 @@ cudaError_t nb_launch_ingest(const NbModelDesc* m, const NbContactsPublic* pub, 
     cudaError_t e = cudaMemsetAsync(seg->world_count, 0, sizeof(int32_t) * (size_t)m->world_count, stream);
     if (e != cudaSuccess) return e;
     if (pub->capacity > 0) {
-        ingest_kernel<<<(pub->capacity + 255) / 256, 256, 0, stream>>>(*m, *pub, *seg);
+        ingest_bucket_kernel<<<(pub->capacity + 255) / 256, 256, 0, stream>>>(*m, *pub, *seg);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    ingest_finalize_kernel<<<(m->world_count + 255) / 256, 256, 0, stream>>>(*m, *seg);
+    ingest_place_kernel<<<m->world_count, 256, 0, stream>>>(*m, *pub, *seg);
     return cudaGetLastError();
 }

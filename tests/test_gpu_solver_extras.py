@@ -101,7 +101,7 @@ def test_contact_force_parity_c2_with_restitution(cuda, orc):
 
 def test_forces_of_ingested_contacts(cuda, orc):
     """Custom contacts in reversed order: each contact's force lands on its own public row.  Each
-    body sums its contacts' deltas in contact order, so the reversed order moves the bodies and the
+    body sums its contacts' deltas in public order, so the reversed order moves the bodies and the
     forces by rounding only."""
     model, info = scenes.scene_c5(worlds=8, device="cuda")
     model.request_contact_attributes("force")
