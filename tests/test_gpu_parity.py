@@ -301,7 +301,7 @@ def test_clear_forces_zeroes_body_f(cuda):
     assert bool((s.body_f == 0).all().item())
 
 
-@pytest.mark.parametrize("scene", ["c2", "c1", "c3"])
+@pytest.mark.parametrize("scene", ["c2", "c1", "c3", "large"])
 def test_sap_broad_phase_same_contacts(cuda, scene):
     """broad_phase="sap" (per-world sort along x and sweep) finds the same candidates as testing every
     listed pair, so the published contacts are identical bit for bit, over a few substeps of motion."""
@@ -309,8 +309,12 @@ def test_sap_broad_phase_same_contacts(cuda, scene):
         model, info = _small_c2()
     elif scene == "c1":
         model, info = scenes.scene_c1(device="cuda")
-    else:
+    elif scene == "c3":
         model, info = scenes.scene_c3(worlds=4, device="cuda")
+    else:
+        # worlds of 200..300 bodies in the same 1 x 1 x 2 m column: those over the sweep's 256 shape
+        # slots, and those under it with more than its 512 overlap slots, fall back to the pair test
+        model, info = scenes.scene_c2(seed=9, worlds=4, nmin=200, nmax=300, device="cuda")
     dt = info["dt"] / info["substeps"]
     solver = SolverXPBD(model, iterations=info["iterations"])
     pipes = {mode: CollisionPipeline(model, broad_phase=mode) for mode in ("nxn", "sap")}
