@@ -1082,13 +1082,14 @@ __device__ __forceinline__ void write_block(const SB& S, const float* src, const
 // integrate, `iterations` x (contacts, weighted apply, joints, apply),
 // restitution, write-back.  The caller carved the world's slab into S.
 // kLean: the variant for models whose joints are all FREE, called without
-// restitution or per-contact impulses.  It drops those passes and the joint
-// solve at compile time (each of them would be a no-op for such a call),
-// which keeps the world's shared-memory view in registers instead of on the
-// stack; the arithmetic of what remains is the same code.  kWarm: the
-// warm-start pass (inlined) is compiled in; the lean variant is built with
-// and without it, so that plain calls do not carry its code.
-template <int G, bool kLean, bool kWarm, class SB>
+// restitution.  It drops that pass and the joint solve at compile time (each
+// of them would be a no-op for such a call), which keeps the world's
+// shared-memory view in registers instead of on the stack; the arithmetic of
+// what remains is the same code.  kWarm: the warm-start pass (inlined) is
+// compiled in; kImp: the per-contact impulse accumulation (contact forces,
+// the warm start's targets) is compiled in.  The lean variant is built with
+// and without each, so that plain calls carry neither.
+template <int G, bool kLean, bool kWarm, bool kImp, class SB>
 __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdParams& p, const NbStepIO& io,
                                            const NbContactSeg& seg, bool has_contacts, float dt, int w, SB& S,
                                            int g, int t, int* flag, int* pen_slot, Batch<G>& B,
@@ -1160,7 +1161,7 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
     const int nc = has_contacts ? seg.world_count[w] : 0;
     const int64_t rec_base = has_contacts ? seg.world_base[w] : 0;
     const float4* R = rec + (size_t)rec_base * 5;
-    const bool want_imp = !kLean && has_contacts && io.contact_impulse != nullptr;
+    const bool want_imp = (!kLean || kImp) && has_contacts && io.contact_impulse != nullptr;
     unsigned bad = 0u;
     if constexpr (kWarm) {
         if (has_contacts && io.ws_lambda) warm_start<G>(m, io, seg, S, R, nc, rec_base, b0, g, t, pen_slot, B, dt);
@@ -1170,7 +1171,7 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
         if (has_contacts) {
             contact_pass<G>(m, S, R, nc, B, g, t, p.rigid_contact_relaxation, dt, weighting,
                             want_imp ? io.impulse_scratch + (size_t)rec_base * 6 : nullptr);
-            if constexpr (!kLean) {
+            if constexpr (!kLean || kImp) {
                 if (want_imp) {
                     accumulate_impulses<G>(S, R, nc, rec_base, seg.rec_index, io.impulse_scratch,
                                            io.contact_impulse, io.contact_impulse_capacity, weighting, t);
@@ -1274,7 +1275,7 @@ __device__ __forceinline__ void step_world(const NbModelDesc& m, const NbXpbdPar
 // Batch mode: a CTA takes a batch of worlds (host-packed into one arena, one
 // world per group of G threads) from a device counter; the CTA waits for all
 // of a batch's worlds before the next batch reuses the arena.
-template <int G, bool kLean, bool kWarm>
+template <int G, bool kLean, bool kWarm, bool kImp>
 __global__ void __launch_bounds__(kST, 2)
 xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, int has_contacts, float dt) {
     extern __shared__ __align__(16) unsigned char arena[];
@@ -1297,7 +1298,7 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
             const int b0 = m.world_body_start[w];
             const int nb = m.world_body_start[w + 1] - b0;
             SBodiesT<false> S = sbodies_carve<false>(arena + 4 * (size_t)m.batch_slab[b * kGroups + g], m, b0, nb);
-            step_world<G, kLean, kWarm>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], &s_pen[g],
+            step_world<G, kLean, kWarm, kImp>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], &s_pen[g],
                                         s_ob[g], &s_bad);
         }
         __syncthreads();  // every group is done with the arena before the next batch
@@ -1311,7 +1312,7 @@ xpbd_step_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, i
 // never waits for another group's world.  The host picks G and the slab
 // layout so that the largest world fits one share (kCompact stages only the
 // mutable body state).
-template <int G, bool kCompact, bool kLean, bool kWarm>
+template <int G, bool kCompact, bool kLean, bool kWarm, bool kImp>
 __global__ void __launch_bounds__(kST, 2)
 xpbd_step_group_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg seg, int has_contacts, float dt) {
     extern __shared__ __align__(16) unsigned char arena[];
@@ -1348,7 +1349,7 @@ xpbd_step_group_kernel(NbModelDesc m, NbXpbdParams p, NbStepIO io, NbContactSeg 
             continue;
         }
         SBodiesT<kCompact> S = sbodies_carve<kCompact>(region, m, b0, nb);
-        step_world<G, kLean, kWarm>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], &s_pen[g],
+        step_world<G, kLean, kWarm, kImp>(m, p, io, seg, has_contacts != 0, dt, w, S, g, t, &s_flag[g], &s_pen[g],
                                     s_ob[g], &s_bad);
         group_sync<G>(g);
     }
@@ -1387,39 +1388,42 @@ cudaError_t nb_launch_contact_forces(const float* imp, const int32_t* count, int
 }
 
 namespace {
-// the lean step kernel applies: every joint is FREE and the call asks for
-// neither restitution nor per-contact impulses
-bool step_is_lean(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io) {
-    return m->all_joints_free == 1 && p->enable_restitution == 0 && io->contact_impulse == nullptr;
+// the lean step kernel applies: every joint is FREE and the call asks for no
+// restitution (per-contact impulses select its kImp variant)
+bool step_is_lean(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO*) {
+    return m->all_joints_free == 1 && p->enable_restitution == 0;
 }
 
-template <int G, bool kLean, bool kWarm>
+template <int G, bool kLean, bool kWarm, bool kImp>
 cudaError_t launch_step_variant(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
                                 const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
     const size_t smem = nb_step_smem_bytes(m);
-    cudaError_t e = nb_raise_dynamic_smem((const void*)xpbd_step_kernel<G, kLean, kWarm>, smem);
+    cudaError_t e = nb_raise_dynamic_smem((const void*)xpbd_step_kernel<G, kLean, kWarm, kImp>, smem);
     if (e != cudaSuccess) return e;
     const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
-    xpbd_step_kernel<G, kLean, kWarm><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
+    xpbd_step_kernel<G, kLean, kWarm, kImp><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts, dt);
     return cudaGetLastError();
 }
 
 template <int G>
 cudaError_t launch_step(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io, const NbContactSeg* seg,
                         float dt, int grid, cudaStream_t stream) {
-    if (!step_is_lean(m, p, io)) return launch_step_variant<G, false, true>(m, p, io, seg, dt, grid, stream);
-    return io->ws_lambda ? launch_step_variant<G, true, true>(m, p, io, seg, dt, grid, stream)
-                         : launch_step_variant<G, true, false>(m, p, io, seg, dt, grid, stream);
+    if (!step_is_lean(m, p, io)) return launch_step_variant<G, false, true, true>(m, p, io, seg, dt, grid, stream);
+    if (io->contact_impulse)
+        return io->ws_lambda ? launch_step_variant<G, true, true, true>(m, p, io, seg, dt, grid, stream)
+                             : launch_step_variant<G, true, false, true>(m, p, io, seg, dt, grid, stream);
+    return io->ws_lambda ? launch_step_variant<G, true, true, false>(m, p, io, seg, dt, grid, stream)
+                         : launch_step_variant<G, true, false, false>(m, p, io, seg, dt, grid, stream);
 }
 
-template <int G, bool kCompact, bool kLean, bool kWarm>
+template <int G, bool kCompact, bool kLean, bool kWarm, bool kImp>
 cudaError_t launch_step_group_variant(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
                                       const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
     const size_t smem = nb_step_smem_bytes(m);
-    cudaError_t e = nb_raise_dynamic_smem((const void*)xpbd_step_group_kernel<G, kCompact, kLean, kWarm>, smem);
+    cudaError_t e = nb_raise_dynamic_smem((const void*)xpbd_step_group_kernel<G, kCompact, kLean, kWarm, kImp>, smem);
     if (e != cudaSuccess) return e;
     const int has_contacts = seg->rec != nullptr && seg->world_count != nullptr && seg->world_base != nullptr;
-    xpbd_step_group_kernel<G, kCompact, kLean, kWarm><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts,
+    xpbd_step_group_kernel<G, kCompact, kLean, kWarm, kImp><<<grid, kST, smem, stream>>>(*m, *p, *io, *seg, has_contacts,
                                                                                  dt);
     return cudaGetLastError();
 }
@@ -1428,9 +1432,13 @@ template <int G, bool kCompact>
 cudaError_t launch_step_group(const NbModelDesc* m, const NbXpbdParams* p, const NbStepIO* io,
                               const NbContactSeg* seg, float dt, int grid, cudaStream_t stream) {
     if (!step_is_lean(m, p, io))
-        return launch_step_group_variant<G, kCompact, false, true>(m, p, io, seg, dt, grid, stream);
-    return io->ws_lambda ? launch_step_group_variant<G, kCompact, true, true>(m, p, io, seg, dt, grid, stream)
-                         : launch_step_group_variant<G, kCompact, true, false>(m, p, io, seg, dt, grid, stream);
+        return launch_step_group_variant<G, kCompact, false, true, true>(m, p, io, seg, dt, grid, stream);
+    if (io->contact_impulse)
+        return io->ws_lambda
+                   ? launch_step_group_variant<G, kCompact, true, true, true>(m, p, io, seg, dt, grid, stream)
+                   : launch_step_group_variant<G, kCompact, true, false, true>(m, p, io, seg, dt, grid, stream);
+    return io->ws_lambda ? launch_step_group_variant<G, kCompact, true, true, false>(m, p, io, seg, dt, grid, stream)
+                         : launch_step_group_variant<G, kCompact, true, false, false>(m, p, io, seg, dt, grid, stream);
 }
 
 template <bool kCompact>
