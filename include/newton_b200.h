@@ -190,10 +190,14 @@ typedef struct NbModelDesc {
  * records (written by nb_publish_contacts or nb_ingest_contacts, read by
  * nb_xpbd_step): world w's contacts are rec[world_base[w] + k],
  * k < world_count[w], in the solver record layout.  pair_count is
- * NbModelDesc.pair_count. */
+ * NbModelDesc.pair_count; rec_rows = min(pair_count*5, the public capacity
+ * rigid_contact_max): the records hold the contacts the public arrays hold
+ * (publish keeps the first `capacity` in public order and clamps the worlds'
+ * counts past it; ingest takes at most the public count), and never more
+ * than 5 per candidate pair. */
 typedef struct NbContactSeg {
     float* slots;                /* [pair_count*5, 20] contact slots (5 float4 each), 16-byte aligned */
-    float* rec;                  /* [pair_count*5, 20] dense solver contact records, 16-byte aligned */
+    float* rec;                  /* [rec_rows, 20] dense solver contact records, 16-byte aligned */
     int64_t* world_base;         /* [W] first rec index of each world */
     int32_t* cand;               /* [pair_count] pair index of each candidate (world-major, key order) */
     int32_t* cand_count;         /* [W] candidates per world */
@@ -204,7 +208,7 @@ typedef struct NbContactSeg {
     float* geom;                 /* [shape_count, 20] world-space shape geometry staged per substep */
     int32_t* work_counter;       /* [8] device counters, zeroed by the entry points */
     uint32_t* status;            /* [1] NB_STATUS_* bits (sticky, cleared by the caller) */
-    int32_t* rec_index;          /* [pair_count*5] public contact index of each record, or NULL;
+    int32_t* rec_index;          /* [rec_rows] public contact index of each record, or NULL;
                                     needed only for per-contact impulses (written by publish / ingest) */
 } NbContactSeg;
 
@@ -333,7 +337,8 @@ typedef struct NbStepIO {
     const float* joint_f;          /* [D] */
     float* contact_impulse;      /* [cap,6] accumulated weighted A-side impulse per public contact, or
                                     NULL; the caller zeroes it before the step (solver_xpbd.py:286-291) */
-    float* impulse_scratch;      /* [pair_count*5, 6] zero-filled scratch, required with contact_impulse;
+    float* impulse_scratch;      /* [rec_rows, 6] zero-filled scratch (one row per solver record of
+                                    NbContactSeg), required with contact_impulse;
                                     left zero-filled on return */
     int32_t contact_impulse_capacity; /* rows of contact_impulse (rigid_contact_max) */
     int32_t pad0;

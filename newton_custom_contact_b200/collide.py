@@ -347,9 +347,11 @@ class CollisionPipeline:
         W = self.model.world_count
         dev = self.device
         i32 = dict(dtype=torch.int32, device=dev)
+        # solver records: the contacts the public arrays hold, at most 5 per candidate pair
+        R = max(1, min(P * 5, int(c.rigid_contact_max)))
         seg = {
             "slots": torch.zeros((P * 5, 20), dtype=torch.float32, device=dev),
-            "rec": torch.zeros((P * 5, 20), dtype=torch.float32, device=dev),
+            "rec": torch.zeros((R, 20), dtype=torch.float32, device=dev),
             "world_base": torch.zeros(W, dtype=torch.int64, device=dev),
             "cand": torch.zeros(P, **i32),
             "cand_count": torch.zeros(W, **i32),
@@ -362,8 +364,8 @@ class CollisionPipeline:
         }
         if c.force is not None:
             # per-contact impulses: public index of every solver record + the step's scratch
-            seg["rec_index"] = torch.full((P * 5,), -1, **i32)
-            seg["impulse_scratch"] = torch.zeros((P * 5, 6), dtype=torch.float32, device=dev)
+            seg["rec_index"] = torch.full((R,), -1, **i32)
+            seg["impulse_scratch"] = torch.zeros((R, 6), dtype=torch.float32, device=dev)
         c._seg = seg
         c._layout = self
         c._seg_valid = False

@@ -771,7 +771,7 @@ narrow_gjk_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg 
 // Exclusive scan of world contact counts (single CTA) -> world_offset[W+1]
 // (public arrays) and world_base[W] (solver records; same offsets), count[0]
 // = total (may exceed the public capacity, as in the reference).
-__global__ void __launch_bounds__(1024) world_scan_kernel(int W, const int32_t* __restrict__ world_count,
+__global__ void __launch_bounds__(1024) world_scan_kernel(int W, int32_t* __restrict__ world_count,
                                                           int64_t* world_offset, int64_t* world_base,
                                                           int32_t* count_out, int cap, uint32_t* status,
                                                           int32_t* generation) {
@@ -804,6 +804,10 @@ __global__ void __launch_bounds__(1024) world_scan_kernel(int W, const int32_t* 
         if (i < W) {
             world_offset[i] = excl;
             world_base[i] = excl;
+            // the solver records hold the first `cap` contacts (those the public arrays hold): a world
+            // past the capacity keeps only its records below it
+            const int64_t room = (int64_t)cap - excl;
+            if (v > room) world_count[i] = (int32_t)(room > 0 ? room : 0);
         }
         __syncthreads();
         if (threadIdx.x == 1023) carry = excl + v;
@@ -834,7 +838,6 @@ __global__ void __launch_bounds__(256) publish_kernel(NbModelDesc m, NbContactSe
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const float4* slots = reinterpret_cast<const float4*>(seg.slots);
     float4* rec = reinterpret_cast<float4*>(seg.rec);
-    const int64_t rec_cap = 5 * (int64_t)m.pair_count;
     for (int w = gw; w < m.world_count; w += nw) {
         const int c0 = m.world_pair_start[w];
         // a world's candidates never exceed its pairs, a candidate's contacts never exceed 5; the
@@ -871,18 +874,16 @@ __global__ void __launch_bounds__(256) publish_kernel(NbModelDesc m, NbContactSe
                 const float4 a = sl[0], b = sl[1], c = sl[2], e = sl[3], f = sl[4];
                 // solver record: the tag moves next to the normal so the
                 // penetration test reads the first 48 bytes only
-                if (d < 0 || d >= rec_cap) {  // rec holds 5 * pair_count records: only corrupted offsets get here
-                    atomicOr(seg.status, (unsigned)NB_STATUS_CONTACT_OVERFLOW);
-                    continue;
-                }
+                // rec and the public rows hold the first `capacity` contacts (world_scan_kernel flagged
+                // an overflow and clamped the worlds' solver counts; a negative offset is corrupt)
+                if (d < 0 || d >= pub.capacity) continue;
                 float4* r = rec + (size_t)d * 5;
                 r[0] = a;
                 r[1] = b;
                 r[2] = make_float4(c.x, c.y, c.z, f.w);
                 r[3] = make_float4(e.x, e.y, e.z, c.w);
                 r[4] = make_float4(f.x, f.y, f.z, e.w);
-                if (seg.rec_index) seg.rec_index[d] = d < pub.capacity ? (int32_t)d : -1;
-                if (d >= pub.capacity) continue;
+                if (seg.rec_index) seg.rec_index[d] = (int32_t)d;
                 const int s0 = __float_as_int(c.w), s1 = __float_as_int(e.w);
                 pub.shape0[d] = s0;
                 pub.shape1[d] = s1;
@@ -903,15 +904,17 @@ __global__ void __launch_bounds__(256) publish_kernel(NbModelDesc m, NbContactSe
     }
 }
 
-// Custom contacts in the public arrays -> solver records, in two kernels.
+// Custom contacts in the public arrays -> solver records, in three kernels.
 // ingest_bucket_kernel finds each public contact's world and appends its
 // public index to the world's bucket (world_pair_start[w]*5 + k: every world
 // owns room for 5 contacts per candidate pair; the buckets live in the slots
 // buffer, which collide rewrites anyway); the append order is that of the
-// atomics.  ingest_place_kernel (one CTA per world) ranks every bucket entry
-// by its public index and writes the record at the world's base + rank, so
-// the records of a world follow the public order whatever the atomics did
-// -- the order the solver sums each body's deltas in.
+// atomics.  ingest_scan_kernel makes the worlds' record bases (an exclusive
+// scan of the bucket sizes: the records are dense, at most the public
+// capacity).  ingest_place_kernel (one CTA per world) ranks every bucket
+// entry by its public index and writes the record at the world's base +
+// rank, so the records of a world follow the public order whatever the
+// atomics did -- the order the solver sums each body's deltas in.
 __global__ void ingest_bucket_kernel(NbModelDesc m, NbContactsPublic pub, NbContactSeg seg) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     int n = pub.count[0] < pub.capacity ? pub.count[0] : pub.capacity;
@@ -947,17 +950,56 @@ __global__ void ingest_bucket_kernel(NbModelDesc m, NbContactsPublic pub, NbCont
     reinterpret_cast<int32_t*>(seg.slots)[(size_t)m.world_pair_start[w] * 5 + k] = c;
 }
 
+__global__ void __launch_bounds__(1024) ingest_scan_kernel(NbModelDesc m, NbContactSeg seg) {
+    __shared__ int64_t warp_sums[32];
+    __shared__ int64_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int W = m.world_count;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < W; base += 1024) {
+        const int i = base + threadIdx.x;
+        int64_t v = 0;
+        if (i < W) {
+            const int room = 5 * (m.world_pair_start[i + 1] - m.world_pair_start[i]);
+            const int nw = seg.world_count[i];
+            v = nw < room ? nw : room;
+            seg.world_count[i] = (int32_t)v;
+        }
+        int64_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sums[warp] = x;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int64_t run = 0;
+            for (int k = 0; k < 32; ++k) {
+                const int64_t t = warp_sums[k];
+                warp_sums[k] = run;
+                run += t;
+            }
+        }
+        __syncthreads();
+        const int64_t excl = carry + warp_sums[warp] + x - v;
+        if (i < W) seg.world_base[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = excl + v;
+        __syncthreads();
+    }
+}
+
 constexpr int kIngestTile = 2048;  // bucket entries one CTA compares against at a time (shared memory)
 
 __global__ void __launch_bounds__(256) ingest_place_kernel(NbModelDesc m, NbContactsPublic pub, NbContactSeg seg) {
     __shared__ int32_t s_tile[kIngestTile];
     const int w = blockIdx.x;
     const int c0 = m.world_pair_start[w];
-    const int room = 5 * (m.world_pair_start[w + 1] - c0);
-    int nw = seg.world_count[w];
-    nw = nw < room ? nw : room;
-    const int64_t base = 5 * (int64_t)c0;
-    const int32_t* bucket = reinterpret_cast<const int32_t*>(seg.slots) + base;
+    const int nw = seg.world_count[w];  // clamped to the world's room by ingest_scan_kernel
+    const int64_t base = seg.world_base[w];
+    const int32_t* bucket = reinterpret_cast<const int32_t*>(seg.slots) + 5 * (int64_t)c0;
     // rank of entry i = the number of the bucket's public indices below its own (indices are distinct)
     for (int i0 = 0; i0 < nw; i0 += blockDim.x) {
         const int i = i0 + threadIdx.x;
@@ -987,10 +1029,6 @@ __global__ void __launch_bounds__(256) ingest_place_kernel(NbModelDesc m, NbCont
         sl[2] = make_float4(pub.normal[3 * c], pub.normal[3 * c + 1], pub.normal[3 * c + 2], __int_as_float(tag));
         sl[3] = make_float4(pub.offset0[3 * c], pub.offset0[3 * c + 1], pub.offset0[3 * c + 2], __int_as_float(s0));
         sl[4] = make_float4(pub.offset1[3 * c], pub.offset1[3 * c + 1], pub.offset1[3 * c + 2], __int_as_float(s1));
-    }
-    if (threadIdx.x == 0) {
-        seg.world_count[w] = nw;
-        seg.world_base[w] = base;
     }
 }
 
@@ -1092,6 +1130,9 @@ cudaError_t nb_launch_ingest(const NbModelDesc* m, const NbContactsPublic* pub, 
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
+    ingest_scan_kernel<<<1, 1024, 0, stream>>>(*m, *seg);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     ingest_place_kernel<<<m->world_count, 256, 0, stream>>>(*m, *pub, *seg);
     return cudaGetLastError();
 }

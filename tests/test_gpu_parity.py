@@ -19,6 +19,26 @@ def _small_c2(worlds=48, seed=7):
     return scenes.scene_c2(seed=seed, worlds=worlds, nmin=8, nmax=40, device="cuda")
 
 
+def _landed_c2(worlds, seed=11, frames=25, force=False):
+    """A small C2 drop advanced `frames` frames through the pipeline (bodies landed: penetrating
+    contacts; the first poses hold contacts inside the gap only)."""
+    model, info = scenes.scene_c2(seed=seed, worlds=worlds, device="cuda")
+    if force:
+        model.request_contact_attributes("force")
+    pipe = CollisionPipeline(model)
+    solver = SolverXPBD(model, iterations=4)
+    contacts = pipe.contacts()
+    s0, s1 = model.state(), model.state()
+    dt = info["dt"] / info["substeps"]
+    for _ in range(frames * info["substeps"]):
+        s0.clear_forces()
+        pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, dt)
+        s0, s1 = s1, s0
+    pipe.collide(s0, contacts)
+    return model, pipe, solver, contacts, s0
+
+
 def _published(contacts):
     n = int(contacts.rigid_contact_count.item())
     out = {k: getattr(contacts, f"rigid_contact_{k}")[:n].cpu().numpy()
@@ -162,12 +182,7 @@ def test_custom_contacts_ingested(cuda, orc):
     """Contacts written into the dense arrays (custom writer): in the pipeline's own order they give the
     pipeline's step bit for bit (records follow the public order within each world); in reversed order
     the same step up to the rounding of the per-body sums, and the same bits on every call."""
-    model, info = _small_c2(worlds=8)
-    pipe = CollisionPipeline(model)
-    solver = SolverXPBD(model, iterations=4)
-    s0 = model.state()
-    c1 = pipe.contacts()
-    pipe.collide(s0, c1)
+    model, pipe, solver, c1, s0 = _landed_c2(worlds=8)
     out_a = model.state()
     solver.step(s0, out_a, None, c1, 1.0 / 480.0)
     n = int(c1.rigid_contact_count.item())
@@ -191,6 +206,57 @@ def test_custom_contacts_ingested(cuda, orc):
     torch.testing.assert_close(out_b.body_q, out_a.body_q, rtol=1e-5, atol=1e-6)
     torch.testing.assert_close(out_b.body_qd, out_a.body_qd, rtol=1e-5, atol=1e-6 * 480.0)
     assert torch.equal(out_b.body_q, out_c.body_q) and torch.equal(out_b.body_qd, out_c.body_qd)
+
+
+def test_capacity_overflow_solves_the_held_contacts(cuda, orc):
+    """rigid_contact_max below the contact count: collide keeps the first `capacity` contacts in
+    public order and flags the overflow; the solver records hold exactly those (min(5 x pairs,
+    capacity) rows), so the step equals a step over those contacts written by hand (the reference's
+    solver reads rigid_contact_count clamped to rigid_contact_max), per-contact forces included, and
+    ingesting a count past the capacity takes the same contacts."""
+    from newton_custom_contact_b200._abi import NB_STATUS_CONTACT_OVERFLOW
+
+    model, full_pipe, solver, full, s0 = _landed_c2(worlds=8, force=True)
+    n = int(full.rigid_contact_count.item())
+    cap = n // 2 + 3
+    assert 0 < cap < n
+    pipe = CollisionPipeline(model, rigid_contact_max=cap)
+    small = pipe.contacts()
+    assert small._seg["rec"].shape[0] == cap and small._seg["impulse_scratch"].shape[0] == cap
+    pipe.collide(s0, small)
+    assert int(small.rigid_contact_count.item()) == n
+    assert pipe.status(small) & NB_STATUS_CONTACT_OVERFLOW
+    names = ("shape0", "shape1", "point0", "point1", "offset0", "offset1", "normal", "margin0", "margin1")
+    for name in names:
+        assert torch.equal(getattr(small, f"rigid_contact_{name}"), getattr(full, f"rigid_contact_{name}")[:cap])
+    out_a = model.state()
+    solver.step(s0, out_a, None, small, 1.0 / 480.0)
+    solver.update_contacts(small)
+    force_a = small.force.clone()
+
+    def ingested(count):
+        c = pipe.contacts()
+        for name in names:
+            getattr(c, f"rigid_contact_{name}").copy_(getattr(full, f"rigid_contact_{name}")[:cap])
+        c.rigid_contact_count.fill_(count)
+        c.mark_dense_modified()
+        out = model.state()
+        solver.step(s0, out, None, c, 1.0 / 480.0)
+        solver.update_contacts(c)
+        torch.cuda.synchronize()
+        return out, c.force.clone()
+
+    for count in (cap, n):
+        out_b, force_b = ingested(count)
+        assert torch.equal(out_a.body_q, out_b.body_q) and torch.equal(out_a.body_qd, out_b.body_qd), count
+        assert torch.equal(force_a, force_b), count
+    # the step did use the held contacts: some are penetrating and carry a force, and without
+    # contacts the bodies move differently
+    assert float(force_a.abs().max()) > 0
+    out_free = model.state()
+    solver.step(s0, out_free, None, None, 1.0 / 480.0)
+    torch.cuda.synchronize()
+    assert not torch.equal(out_free.body_qd, out_a.body_qd)
 
 
 def test_collide_bit_exact_in_piled_state(cuda, orc):
