@@ -18,7 +18,8 @@
 //      <= 5 contacts written into the candidate's own slots:
 //      narrow_analytic_kernel (primitive pairs), gjk_prefilter_kernel (drops
 //      pairs that are provably farther apart than the contact threshold and
-//      compacts the rest), narrow_gjk_kernel (MPR / GJK / manifold).
+//      compacts the rest), narrow_gjk_kernel (MPR / GJK) and
+//      narrow_manifold_kernel (the manifolds of the pairs within the threshold).
 //   3. publish (world_scan_kernel + publish_kernel) -- the reference's dense
 //      Contacts arrays ordered by (world, key): walking a world's candidates
 //      in order and each candidate's slots in sub-key order is exactly the key
@@ -751,19 +752,79 @@ gjk_prefilter_kernel(NbModelDesc m, NbContactSeg seg) {
     }
 }
 
-// MPR / GJK / manifold on the items that survived the prefilter.  Latency
-// and divergence bound: 12 CTAs per SM (48 warps, 40 registers, a few bytes
-// of spills) hide more of it than the unconstrained 122 registers at 4 CTAs
-// (collide 0.57 vs 0.72 ms per substep on 4096 uneven worlds).
+// MPR / GJK on the items that survived the prefilter, then the manifolds in a
+// second kernel.  Almost every item runs MPR (which rarely finds an overlap),
+// then GJK, and about nine in ten then build a manifold (polygon clipping in
+// local arrays): split in two kernels, each warp runs one of the two code
+// paths at a time and each kernel's code is half the size in the instruction
+// cache.  An item that needs a manifold leaves its witness points and normal
+// (relative frame) in its own last contact slot -- unused until the manifold
+// writes its contacts, read before that -- and its queue entry in the
+// queue's back half, which the prefilter has consumed: box-box items from
+// the top down, the others from the bottom of that region up (the items
+// never exceed the n1 <= pair_count entries the region held).
+// Latency and divergence bound: 12 CTAs per SM (48 warps, 40 registers, a
+// few bytes of spills) hide more of it than 6, 8, 10 or 16 (measured) or the
+// unconstrained 122 registers at 4 CTAs.
 __global__ void __launch_bounds__(kNT, kGjkMinBlocks)
 narrow_gjk_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
     const int n_box = seg.work_counter[5], n_other = seg.work_counter[6], n1 = seg.work_counter[3];
     const int n = n_box + n_other;
+    int2* queue = reinterpret_cast<int2*>(seg.queue);
+    const long long top = 2 * (long long)m.pair_count - 1;
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const int i = base + lane;
+        const bool box = i < n_box;
+        bool manifold = false;
+        int2 e = make_int2(0, 0);
+        if (i < n) {
+            e = box ? queue[i] : queue[n1 - 1 - (i - n_box)];
+            NarrowItem it;
+            if (narrow_setup(m, seg, body_q, e, it)) {
+                V3 pa, pb, nrm;
+                manifold = gjk_stage(it.wr, it.ga, it.gb, pa, pb, nrm);
+                if (manifold) {
+                    float4* h = it.wr.slots + kSlotF4 - 3;
+                    h[0] = make_float4(pa.x, pa.y, pa.z, 0.0f);
+                    h[1] = make_float4(pb.x, pb.y, pb.z, 0.0f);
+                    h[2] = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
+                } else {
+                    narrow_finish(seg, it);
+                }
+            }
+        }
+        const unsigned below = (1u << lane) - 1u;
+        const unsigned bb = __ballot_sync(kFull, manifold && box);
+        const unsigned bo = __ballot_sync(kFull, manifold && !box);
+        int ob = 0, oo = 0;
+        if (lane == 0 && bb) ob = atomicAdd(&seg.work_counter[1], __popc(bb));
+        if (lane == 0 && bo) oo = atomicAdd(&seg.work_counter[7], __popc(bo));
+        ob = __shfl_sync(kFull, ob, 0);
+        oo = __shfl_sync(kFull, oo, 0);
+        if (manifold && box) queue[top - (ob + __popc(bb & below))] = e;
+        if (manifold && !box) queue[top - n1 + 1 + (oo + __popc(bo & below))] = e;
+    }
+}
+
+__global__ void __launch_bounds__(kNT, kGjkMinBlocks)
+narrow_manifold_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
+    const int n1 = seg.work_counter[3];
+    int nb = seg.work_counter[1], no = seg.work_counter[7];
+    // never more than the items the MPR/GJK kernel read; the clamps keep corrupted
+    // counters inside the queue's back region
+    nb = nb < 0 ? 0 : (nb > n1 ? n1 : nb);
+    no = no < 0 ? 0 : (no > n1 - nb ? n1 - nb : no);
     const int2* queue = reinterpret_cast<const int2*>(seg.queue);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const long long top = 2 * (long long)m.pair_count - 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb + no; i += gridDim.x * blockDim.x) {
+        const int2 e = i < nb ? queue[top - i] : queue[top - n1 + 1 + (i - nb)];
         NarrowItem it;
-        if (!narrow_setup(m, seg, body_q, i < n_box ? queue[i] : queue[n1 - 1 - (i - n_box)], it)) continue;
-        gjk_pair(it.wr, it.ga, it.gb);
+        if (!narrow_setup(m, seg, body_q, e, it)) continue;
+        const float4* h = it.wr.slots + kSlotF4 - 3;
+        const float4 h0 = h[0], h1 = h[1], h2 = h[2];
+        gjk_manifold(it.wr, it.ga, it.gb, V3{h0.x, h0.y, h0.z}, V3{h1.x, h1.y, h1.z}, V3{h2.x, h2.y, h2.z});
         narrow_finish(seg, it);
     }
 }
@@ -1053,7 +1114,7 @@ namespace {
 // drive several GPUs; the mutex orders first calls from several host threads).
 constexpr int kMaxCollideDevices = 64;
 struct NarrowOccupancy {
-    int analytic = 0, prefilter = 0, gjk = 0;
+    int analytic = 0, prefilter = 0, gjk = 0, manifold = 0;
 };
 std::mutex g_occ_mutex;
 NarrowOccupancy g_occ[kMaxCollideDevices];
@@ -1067,13 +1128,15 @@ cudaError_t narrow_occupancy(NarrowOccupancy* out) {
     NarrowOccupancy& c = g_occ[dev];
     if (!c.gjk) {
         // default grids: one wave at each kernel's occupancy (grid-stride loops)
-        int a = 0, p = 0, g = 0;
+        int a = 0, p = 0, g = 0, f = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, narrow_analytic_kernel, kNT, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, gjk_prefilter_kernel, kNT, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g, narrow_gjk_kernel, kNT, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f, narrow_manifold_kernel, kNT, 0);
         c.analytic = a > 0 ? a : 4;
         c.prefilter = p > 0 ? p : 4;
         c.gjk = g > 0 ? g : 4;
+        c.manifold = f > 0 ? f : 4;
     }
     *out = c;
     return cudaSuccess;
@@ -1093,7 +1156,7 @@ cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const N
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(seg->work_counter, 0, 4 * sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(seg->work_counter + 5, 0, 2 * sizeof(int32_t), stream);
+    e = cudaMemsetAsync(seg->work_counter + 5, 0, 3 * sizeof(int32_t), stream);
     if (e != cudaSuccess) return e;
     const int sms = sm_count();
     if (sap) broadphase_kernel<true><<<sms * 4, kBT, smem, stream>>>(*m, body_q, *seg);
@@ -1107,6 +1170,9 @@ cudaError_t nb_launch_collide(const NbModelDesc* m, const float* body_q, const N
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     narrow_gjk_kernel<<<grid > 0 ? grid : sms * occ.gjk, kNT, 0, stream>>>(*m, body_q, *seg);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    narrow_manifold_kernel<<<grid > 0 ? grid : sms * occ.manifold, kNT, 0, stream>>>(*m, body_q, *seg);
     return cudaGetLastError();
 }
 

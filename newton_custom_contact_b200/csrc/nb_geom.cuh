@@ -1045,10 +1045,28 @@ NB_D void plane_to_cube(Q4 pq, V3 ppos, V3 other, float other_radius, Shape& out
     adj = sub(surf, mul(n, depth));
 }
 
-__device__ __noinline__ void gjk_pair(Writer& w, const Geom& ga, const Geom& gb) {
+// Everything of the reference's MPR/GJK pair routine (narrow_phase.py:598-720
+// with multicontact.py) that precedes MPR: the infinite-plane rejection and
+// plane-as-cube substitution, the small-radius stand-ins for spheres and
+// capsules, the contact template, the relative frame and MPR's enlargement.
+// A pure function of the two geometries, so the manifold stage recomputes it
+// instead of storing it.
+struct GjkSetup {
+    Pair p;
+    Q4 qa;
+    V3 pa;
+    ContactData tmpl;
+    float threshold;
+    float enlarge;
+    bool skip_multi;
+};
+
+// false: the pair produces nothing (two infinite planes, or an infinite plane
+// beyond the other shape's bounding sphere)
+NB_D bool gjk_prepare(const Geom& ga, const Geom& gb, GjkSetup& s) {
     bool inf_a = ga.type == NB_GEO_PLANE && ga.scale.x == 0.0f && ga.scale.y == 0.0f;
     bool inf_b = gb.type == NB_GEO_PLANE && gb.scale.x == 0.0f && gb.scale.y == 0.0f;
-    if (inf_a && inf_b) return;
+    if (inf_a && inf_b) return false;
     float bra = 0.0f, brb = 0.0f;
     if (inf_a || inf_b) {
         V3 ca = smul(0.5f, add(ga.lo, ga.hi));
@@ -1062,7 +1080,7 @@ __device__ __noinline__ void gjk_pair(Writer& w, const Geom& ga, const Geom& gb)
         else { ppos = gb.xf.p; pq = gb.xf.q; oc = ca; orad = bra; }
         V3 pn = qrot(pq, V3{0.0f, 0.0f, 1.0f});
         float cdist = dot(sub(oc, ppos), pn);
-        if (!(cdist <= orad)) return;
+        if (!(cdist <= orad)) return false;
     }
     float gap_sum = ga.gap + gb.gap;
     Shape A{ga.type, ga.scale}, B{gb.type, gb.scale};
@@ -1074,7 +1092,7 @@ __device__ __noinline__ void gjk_pair(Writer& w, const Geom& ga, const Geom& gb)
     const float small_radius = 0.0001f;
     if (A.type == NB_GEO_SPHERE || A.type == NB_GEO_CAPSULE) { reff_a = A.scale.x; A.scale.x = small_radius; }
     if (B.type == NB_GEO_SPHERE || B.type == NB_GEO_CAPSULE) { reff_b = B.scale.x; B.scale.x = small_radius; }
-    ContactData tmpl;
+    ContactData& tmpl = s.tmpl;
     tmpl.reff_a = reff_a;
     tmpl.reff_b = reff_b;
     tmpl.margin_a = ga.margin;
@@ -1084,44 +1102,63 @@ __device__ __noinline__ void gjk_pair(Writer& w, const Geom& ga, const Geom& gb)
     tmpl.center = V3{0, 0, 0};
     tmpl.normal = V3{0, 0, 0};
     tmpl.dist = 0.0f;
-    float threshold = gap_sum + reff_a + reff_b + ga.margin + gb.margin;
-    bool skip_multi = A.type == NB_GEO_SPHERE || B.type == NB_GEO_SPHERE;
-    Pair p;
-    p.a = A;
-    p.b = B;
-    p.ob = qmul(qinv(qa), qb);
-    p.pb = qrot_inv(qa, sub(pb, pa));
+    s.threshold = gap_sum + reff_a + reff_b + ga.margin + gb.margin;
+    s.skip_multi = A.type == NB_GEO_SPHERE || B.type == NB_GEO_SPHERE;
+    s.p.a = A;
+    s.p.b = B;
+    s.p.ob = qmul(qinv(qa), qb);
+    s.p.pb = qrot_inv(qa, sub(pb, pa));
+    s.qa = qa;
+    s.pa = pa;
     float margin_sum = tmpl.margin_a + tmpl.margin_b;
     const float eps = 1.0e-4f;
-    float enlarge;
-    if (margin_sum <= 0.0f) enlarge = eps;
-    else if (margin_sum < eps) enlarge = 2.0f * eps;
-    else enlarge = 0.0f;
-    V3 point_a, point_b, normal;
+    if (margin_sum <= 0.0f) s.enlarge = eps;
+    else if (margin_sum < eps) s.enlarge = 2.0f * eps;
+    else s.enlarge = 0.0f;
+    return true;
+}
+
+// MPR, then GJK when MPR finds no overlap.  Returns true when the pair still
+// needs its manifold (build_manifold from the returned witness points and
+// normal, in the pair's relative frame); false when it is finished -- rejected
+// early, or its single contact (spheres, or a distance beyond the threshold)
+// already written.
+__device__ __noinline__ bool gjk_stage(Writer& w, const Geom& ga, const Geom& gb, V3& point_a, V3& point_b,
+                                       V3& normal) {
+    GjkSetup s;
+    if (!gjk_prepare(ga, gb, s)) return false;
     float pen, sd;
-    bool collision = mpr_core(p, enlarge, point_a, point_b, normal, pen);
+    bool collision = mpr_core(s.p, s.enlarge, point_a, point_b, normal, pen);
     if (collision) {
-        sd = -pen + enlarge;
-        float he = enlarge * 0.5f;
+        sd = -pen + s.enlarge;
+        float he = s.enlarge * 0.5f;
         point_a = sub(point_a, mul(normal, he));
         point_b = add(point_b, mul(normal, he));
     } else {
-        gjk_core(p, 0.0f, point_a, point_b, normal, sd);
+        gjk_core(s.p, 0.0f, point_a, point_b, normal, sd);
     }
-    if (skip_multi || sd > threshold) {
+    if (s.skip_multi || sd > s.threshold) {
         V3 pt = smul(0.5f, add(point_a, point_b));
-        pt = add(qrot(qa, pt), pa);
-        V3 nws = qrot(qa, normal);
-        ContactData cd = tmpl;
+        pt = add(qrot(s.qa, pt), s.pa);
+        V3 nws = qrot(s.qa, normal);
+        ContactData cd = s.tmpl;
         cd.center = pt;
         cd.normal = nws;
         cd.dist = sd;
-        cd.sub_key = tmpl.sub_key << 3;
-        post_process(cd, A.type, B.type);
+        cd.sub_key = s.tmpl.sub_key << 3;
+        post_process(cd, s.p.a.type, s.p.b.type);
         write_contact(w, cd, true);
-        return;
+        return false;
     }
-    build_manifold(w, p, qa, pa, point_a, point_b, normal, tmpl);
+    return true;
+}
+
+// the manifold of a pair gjk_stage left unfinished, from its witness points and normal
+__device__ __noinline__ void gjk_manifold(Writer& w, const Geom& ga, const Geom& gb, V3 point_a, V3 point_b,
+                                          V3 normal) {
+    GjkSetup s;
+    if (!gjk_prepare(ga, gb, s)) return;  // never: the stage passed the same test
+    build_manifold(w, s.p, s.qa, s.pa, point_a, point_b, normal, s.tmpl);
 }
 
 // narrow_phase_primitive_kernel body for one pair (type_a <= type_b).
@@ -1206,11 +1243,6 @@ __device__ __forceinline__ bool narrow_analytic(Writer& w, const Geom& ga, const
         return true;
     }
     return false;
-}
-
-// full narrow phase of one pair: analytic primitives, else MPR/GJK + manifold
-__device__ __noinline__ void narrow_pair(Writer& w, const Geom& ga, const Geom& gb) {
-    if (!narrow_analytic(w, ga, gb)) gjk_pair(w, ga, gb);
 }
 
 }  // namespace nbg
