@@ -724,8 +724,8 @@ def run_ours(args, rank, world_size, local_rank):
     if not args.no_cpu_baseline and world_size == 1:
         cpu = cpu_baseline(args.seed, args.cpu_sample_seconds, args.worlds)
     # own kernels per substep: broad phase, analytic narrow phase, MPR/GJK
-    # prefilter, MPR/GJK narrow phase, world scan, publish, and the XPBD step
-    launches_per_frame = substeps * 7
+    # prefilter, MPR/GJK, manifolds, world scan, publish, and the XPBD step
+    launches_per_frame = substeps * 8
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": args.scaling,

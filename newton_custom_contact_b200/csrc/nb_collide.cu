@@ -40,6 +40,7 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kBT = 256;             // broad phase: threads per CTA (8 worlds in flight)
 constexpr int kNT = 128;             // narrow phase: threads per CTA
 constexpr int kGjkMinBlocks = 12;     // MPR/GJK kernel: resident CTAs per SM the registers are fitted to
+constexpr int kManifoldMinBlocks = 5;   // manifold kernel (96 registers: fewer, heavier threads measure faster)
 constexpr int kSlotF4 = 25;          // 5 contacts x 5 float4 per candidate
 
 __device__ __forceinline__ void store_geom(float4* g, const Geom& x) {
@@ -808,7 +809,7 @@ narrow_gjk_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg 
     }
 }
 
-__global__ void __launch_bounds__(kNT, kGjkMinBlocks)
+__global__ void __launch_bounds__(kNT, kManifoldMinBlocks)
 narrow_manifold_kernel(NbModelDesc m, const float* __restrict__ body_q, NbContactSeg seg) {
     const int n1 = seg.work_counter[3];
     int nb = seg.work_counter[1], no = seg.work_counter[7];
