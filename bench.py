@@ -701,7 +701,7 @@ def run_ours(args, rank, world_size, local_rank):
     if rank != 0:
         return
     # roofline of the dominant kernel: the XPBD step (the largest single kernel of the launch list; the
-    # collide stage is four kernels), with the stages' figures beside it
+    # collide stage is five kernels), with the stages' figures beside it
     algo = algorithmic_bytes(model, pipe.layout, n_contacts)
     per = {"collide": t_col / n_sub, "publish": t_pub / n_sub, "step": t_step / n_sub}
     dom = "step"
