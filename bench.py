@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned-warm-start arm")
     ap.add_argument("--warm-start-iterations", type=int, default=2)
     ap.add_argument("--no-articulated", action="store_true", help="skip the articulated (C3) batch")
+    ap.add_argument("--no-particles", action="store_true", help="skip the particle drop")
+    ap.add_argument("--particles-only", action="store_true",
+                    help="run only the particle drop and print its line (a diagnostic run, not the benchmark line)")
     ap.add_argument("--warm-start-sweep", default="", metavar="K1,K2,...",
                     help="also time the plain and the warm-started forms at these iteration counts")
     ap.add_argument("--step-schedule", default=None, metavar="MODE/G",
@@ -445,6 +448,75 @@ def articulated_arm(dev, stream, flush, steps, warmup):
             "scene_build_s": round(build_s, 1)}
 
 
+def particles_arm(dev, stream, flush, steps, warmup):
+    """The particle path: a 100 x 100 spring cloth (10,000 particles, 39,402 springs) and 100,000 loose
+    particles dropped onto a ground plane, a box, a sphere and a capsule; dt 1/240 s, 8 iterations.  One
+    step is 60 substeps (collide + solver step each, CUDA-graph captured) from the same start state,
+    taken after 40 untimed substeps, when the cloth and the loose particles are landing."""
+    import torch
+
+    from newton_custom_contact_b200 import CollisionPipeline, SolverXPBD, scenes
+
+    n_sub, pre = 60, 40
+    t0 = time.perf_counter()
+    model, info = scenes.scene_particles(seed=2, cloth=100, loose=100_000, radius=0.01, device=dev,
+                                         loose_extent=1.0, loose_height=(0.33, 1.2))
+    build_s = time.perf_counter() - t0
+    dt = 1.0 / 240.0
+    pipe = CollisionPipeline(model)
+    solver = SolverXPBD(model, iterations=8)
+    s0, s1 = model.state(), model.state()
+    contacts = pipe.contacts()
+
+    def substeps(n):
+        a, b = s0, s1
+        for _ in range(n // 2 * 2):
+            pipe.collide(a, contacts)
+            solver.step(a, b, None, contacts, dt)
+            a, b = b, a
+
+    stream.wait_stream(torch.cuda.current_stream(stream.device))
+    with torch.cuda.stream(stream):
+        substeps(pre)
+    torch.cuda.synchronize()
+    snap = (s0.particle_q.clone(), s0.particle_qd.clone())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        substeps(n_sub)
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    contacts_seen = []
+    with torch.cuda.stream(stream):
+        for k in range(warmup + steps):
+            s0.particle_q.copy_(snap[0])
+            s0.particle_qd.copy_(snap[1])
+            flush.fill_(float(k))
+            if k >= warmup:
+                starts[k - warmup].record(stream)
+            g.replay()
+            if k >= warmup:
+                ends[k - warmup].record(stream)
+                contacts_seen.append(contacts.soft_contact_count.clone())
+    torch.cuda.synchronize()
+    ms = sum(starts[k].elapsed_time(ends[k]) for k in range(steps))
+    q = s0.particle_q
+    r = model.particle_radius
+    act = (model.particle_flags & 1) != 0
+    del g
+    P = model.particle_count
+    return {"workload": "particles: 100x100 spring cloth + 100,000 loose particles (r 5..10 mm) dropped on a "
+                        "plane, box, sphere and capsule; dt 1/240, 8 iterations, substeps 41..100 of the drop",
+            "value": P * n_sub * steps / (ms / 1e3), "unit": "particle-substeps/s",
+            "ms_per_substep": ms / steps / n_sub, "particles": P, "springs": model.spring_count,
+            "soft_contacts_at_step_end": int(torch.stack(contacts_seen).float().mean().item()),
+            "min_height_above_radius_m": float((q[act, 2] - r[act]).min().item()),
+            "final_state_finite": bool(torch.isfinite(q).all().item()),
+            # soft contacts 3 kernels, integrate 1, then constraints + apply per iteration
+            "status": solver._particles.status(), "gpu_launches_per_substep": 3 + 1 + 2 * 8,
+            "scene_build_s": round(build_s, 1)}
+
+
 def plain_arm(model, dt, substeps, sched, stream, flush, steps, warmup, iterations):
     """The plain form with `iterations` iterations on the same scene and frames (for the warm-start
     sweep): timed like the main workload, penetration statistics along one pass of the window."""
@@ -513,6 +585,12 @@ def run_ours(args, rank, world_size, local_rank):
     _lib.use_build(args.build)
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
+    if args.particles_only:
+        stream = torch.cuda.Stream(dev)
+        flush = torch.empty(int(256 * 2**20) // 4, dtype=torch.float32, device=dev)
+        if rank == 0:
+            print(json.dumps({"particles": particles_arm(dev, stream, flush, args.steps, args.warmup)}), flush=True)
+        return
     dist = None
     if world_size > 1:
         import datetime
@@ -694,6 +772,9 @@ def run_ours(args, rank, world_size, local_rank):
     arm = None
     if not args.no_articulated and world_size == 1:
         arm = articulated_arm(dev, stream, flush, args.steps, args.warmup)
+    parts = None
+    if not args.no_particles and world_size == 1:
+        parts = particles_arm(dev, stream, flush, args.steps, args.warmup)
     del g
     if dist:
         dist.barrier()
@@ -760,6 +841,8 @@ def run_ours(args, rank, world_size, local_rank):
         line["warm_start"] = warm
     if arm is not None:
         line["articulated"] = arm
+    if parts is not None:
+        line["particles"] = parts
     if sweep is not None:
         line["warm_start_sweep"] = sweep
     print(json.dumps(line), flush=True)

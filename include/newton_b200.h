@@ -52,7 +52,7 @@
 extern "C" {
 #endif
 
-#define NB_ABI_VERSION 18
+#define NB_ABI_VERSION 19
 
 enum {
     NB_OK = 0,
@@ -562,6 +562,118 @@ int nb_ingest_contacts(const NbModelDesc* model, const NbContactsPublic* pub,
 #define NB_PUBLISH_STATIC_MAX_WORLDS 65536
 int nb_publish_contacts_static(const NbModelDesc* model, const NbContactSeg* seg,
                                const NbContactsPublic* pub, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Particles: the XPBD particle path (newton/_src/solvers/xpbd/kernels.py:
+ * 114-357, 776-807; newton/_src/solvers/solver.py:11-47) and the soft
+ * contacts between particles and shapes (newton/_src/geometry/kernels.py:
+ * 1000-1140).  Particles are independent of the rigid-body step: they
+ * collide with each other and with shapes, and the solver accepts particle
+ * contacts with static shapes only (shape_body == -1).
+ * ------------------------------------------------------------------------ */
+
+/* Particle flag bit (newton/_src/sim/enums.py ParticleFlags.ACTIVE). */
+#define NB_PARTICLE_ACTIVE 1
+/* Status bits of the particle step (sticky, in NbParticleIO.status). */
+#define NB_STATUS_PARTICLE_BODY_CONTACT (1u << 7)  /* a soft contact with a body-attached shape was skipped */
+#define NB_STATUS_NEIGHBOR_OVERFLOW (1u << 8)      /* a particle touched more than NB_PARTICLE_MAX_NEIGHBORS others */
+/* Particle-particle contacts summed per particle and iteration; more are dropped with
+ * NB_STATUS_NEIGHBOR_OVERFLOW (twelve equal spheres can touch one). */
+#define NB_PARTICLE_MAX_NEIGHBORS 32
+
+/* Particles, springs and the shapes particles collide with: the Model arrays of
+ * the same names (newton/_src/sim/model.py particle_*, spring_*, shape_*). */
+typedef struct NbParticleDesc {
+    int32_t particle_count;
+    int32_t spring_count;
+    int32_t shape_count;
+    int32_t world_count;              /* rows of gravity */
+    float particle_max_velocity;      /* Model.particle_max_velocity */
+    float particle_max_radius;        /* Model.particle_max_radius */
+    float particle_mu;                /* Model.particle_mu: particle-particle friction */
+    float particle_cohesion;          /* Model.particle_cohesion */
+    float particle_adhesion;          /* Model.particle_adhesion: particle-shape contact distance */
+    float soft_contact_mu;            /* Model.soft_contact_mu */
+    const float* particle_inv_mass;   /* [P]   */
+    const float* particle_radius;     /* [P]   */
+    const int32_t* particle_flags;    /* [P]   NB_PARTICLE_ACTIVE */
+    const int32_t* particle_world;    /* [P]   (-1 = global) */
+    const float* gravity;             /* [W,3] */
+    const int32_t* spring_indices;    /* [S,2] */
+    const float* spring_rest_length;  /* [S]   */
+    const float* spring_stiffness;    /* [S]   */
+    const float* spring_damping;      /* [S]   */
+    const int32_t* particle_spring_start; /* [P+1] springs of particle p: particle_spring_list[start[p]..start[p+1]) */
+    const int32_t* particle_spring_list;  /* [2S]  spring indices, ascending per particle */
+    const int32_t* shape_body;        /* [Sh]  (-1 = static) */
+    const int32_t* shape_type;        /* [Sh]  NB_GEO_* */
+    const float* shape_transform;     /* [Sh,7] shape in body frame */
+    const float* shape_scale;         /* [Sh,3] */
+    const int32_t* shape_world;       /* [Sh]  */
+    const int32_t* shape_flags;       /* [Sh]  bit 2 = COLLIDE_PARTICLES */
+    const float* shape_mu;            /* [Sh]  */
+} NbParticleDesc;
+
+/* Soft contacts (newton/_src/sim/contacts.py soft_contact_* arrays), in
+ * (particle, shape) order. */
+typedef struct NbSoftContacts {
+    int32_t* count;           /* [1] contacts found; may exceed max, the first max are stored */
+    int32_t* particle;        /* [max] */
+    int32_t* shape;           /* [max] */
+    float* body_pos;          /* [max,3] contact point in the shape's body frame */
+    float* body_vel;          /* [max,3] */
+    float* normal;            /* [max,3] world frame */
+    int32_t max;
+    float margin;             /* contact when the shape's signed distance < margin + radius */
+    int32_t* particle_start;  /* [P + 2 + ceil(P/1024)] scratch written by nb_soft_collide: the first
+                                 contact of every particle ([0, P]), then per-block counts; read
+                                 back by nb_particle_step */
+} NbSoftContacts;
+
+/* Work buffers of one particle substep. */
+typedef struct NbParticleIO {
+    const float* particle_q;   /* [P,3] state_in positions (read only) */
+    const float* particle_qd;  /* [P,3] state_in velocities (read only) */
+    const float* particle_f;   /* [P,3] state_in forces, or NULL for none */
+    float* particle_q_out;     /* [P,3] state_out positions */
+    float* particle_qd_out;    /* [P,3] state_out velocities */
+    float* delta;              /* [P,3] scratch: the iteration's position corrections */
+    int32_t* grid_head;        /* [2*grid_size] scratch: two hashed cell tables (first particle, -1 empty) */
+    int32_t* grid_next;        /* [P] scratch: next particle of the same cell */
+    int32_t grid_size;         /* cells per table, a power of two */
+    int32_t pad;
+    uint32_t* status;          /* [1] NB_STATUS_* bits (sticky, cleared by the caller) */
+} NbParticleIO;
+
+/*
+ * Soft contacts of every active particle with every particle-colliding shape
+ * of its world (create_soft_contacts, newton/_src/geometry/kernels.py:1000-
+ * 1140; launched from newton/_src/sim/collide.py:1194-1230) for plane,
+ * sphere, capsule and box shapes.  The reference appends contacts with an
+ * atomic counter; here every particle's contacts follow one exclusive scan,
+ * so the list is in (particle, shape) order, the order of the reference's
+ * thread ids, on every run.  body_q may be NULL when no shape is attached to
+ * a body.
+ */
+int nb_soft_collide(const NbParticleDesc* pd, const float* particle_q, const float* body_q,
+                    const NbSoftContacts* sc, void* stream);
+
+/*
+ * One XPBD substep of the particles (SolverXPBD.step's particle branch,
+ * newton/_src/solvers/xpbd/solver_xpbd.py:303-320, 377-505, 657-660):
+ * integrate_particles (solver.py:11-47), then `iterations` times the
+ * particle-shape contacts (kernels.py:114-222), particle-particle contacts
+ * (kernels.py:225-289), springs (kernels.py:292-356) and
+ * apply_particle_deltas (kernels.py:776-807).  Each particle gathers its
+ * corrections in a fixed order (its soft contacts, then its particle
+ * neighbours in ascending index, then its springs in ascending index)
+ * instead of the reference's atomic adds, so results do not change from run
+ * to run.  sc may be NULL (no soft contacts); sc->particle_start must come
+ * from nb_soft_collide on the same contacts.  Soft contacts with a
+ * body-attached shape are skipped (NB_STATUS_PARTICLE_BODY_CONTACT).
+ */
+int nb_particle_step(const NbParticleDesc* pd, const NbParticleIO* io, const NbSoftContacts* sc, float dt,
+                     int32_t iterations, float relaxation, void* stream);
 
 #ifdef __cplusplus
 }

@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 
-NB_ABI_VERSION = 18
+NB_ABI_VERSION = 19
 
 NB_OK = 0
 NB_ERR_INVALID = 1
@@ -248,6 +248,47 @@ class NbStepIO(C.Structure):
         ("ws_flags", C.c_int32),
         ("ws_fallback", _fp),
     ]
+
+
+class NbParticleDesc(C.Structure):
+    _fields_ = [
+        ("particle_count", C.c_int32),
+        ("spring_count", C.c_int32),
+        ("shape_count", C.c_int32),
+        ("world_count", C.c_int32),
+        ("particle_max_velocity", C.c_float),
+        ("particle_max_radius", C.c_float),
+        ("particle_mu", C.c_float),
+        ("particle_cohesion", C.c_float),
+        ("particle_adhesion", C.c_float),
+        ("soft_contact_mu", C.c_float),
+    ] + [(k, _fp) for k in ("particle_inv_mass", "particle_radius", "particle_flags", "particle_world", "gravity",
+                            "spring_indices", "spring_rest_length", "spring_stiffness", "spring_damping",
+                            "particle_spring_start", "particle_spring_list", "shape_body", "shape_type",
+                            "shape_transform", "shape_scale", "shape_world", "shape_flags", "shape_mu")]
+
+
+class NbSoftContacts(C.Structure):
+    _fields_ = [(k, _fp) for k in ("count", "particle", "shape", "body_pos", "body_vel", "normal")] + [
+        ("max", C.c_int32),
+        ("margin", C.c_float),
+        ("particle_start", _fp),
+    ]
+
+
+class NbParticleIO(C.Structure):
+    _fields_ = [(k, _fp) for k in ("particle_q", "particle_qd", "particle_f", "particle_q_out", "particle_qd_out",
+                                   "delta", "grid_head", "grid_next")] + [
+        ("grid_size", C.c_int32),
+        ("pad", C.c_int32),
+        ("status", _fp),
+    ]
+
+
+NB_PARTICLE_ACTIVE = 1
+NB_STATUS_PARTICLE_BODY_CONTACT = 1 << 7
+NB_STATUS_NEIGHBOR_OVERFLOW = 1 << 8
+NB_PARTICLE_MAX_NEIGHBORS = 32
 
 
 class NbWsNet(C.Structure):

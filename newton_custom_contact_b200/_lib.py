@@ -27,6 +27,9 @@ from ._abi import (
     NB_ERR_INVALID,
     NB_ERR_UNSUPPORTED,
     NbAdjointIO,
+    NbParticleDesc,
+    NbParticleIO,
+    NbSoftContacts,
     NbContactSeg,
     NbContactsPublic,
     NbMatchState,
@@ -62,6 +65,8 @@ EXPORTS = (
     "nb_ws_adam",
     "nb_xpbd_step_adjoint",
     "nb_xpbd_substeps",
+    "nb_soft_collide",
+    "nb_particle_step",
 )
 
 _libs: dict = {}
@@ -169,6 +174,12 @@ def load(path: str | None = None) -> C.CDLL:
     lib.nb_xpbd_step_adjoint.restype = C.c_int
     lib.nb_xpbd_step_adjoint.argtypes = [C.POINTER(NbModelDesc), C.POINTER(NbXpbdParams), C.POINTER(NbAdjointIO),
                                          C.POINTER(NbContactSeg), C.c_float, C.c_void_p]
+    lib.nb_soft_collide.restype = C.c_int
+    lib.nb_soft_collide.argtypes = [C.POINTER(NbParticleDesc), C.c_void_p, C.c_void_p, C.POINTER(NbSoftContacts),
+                                    C.c_void_p]
+    lib.nb_particle_step.restype = C.c_int
+    lib.nb_particle_step.argtypes = [C.POINTER(NbParticleDesc), C.POINTER(NbParticleIO), C.POINTER(NbSoftContacts),
+                                     C.c_float, C.c_int32, C.c_float, C.c_void_p]
     v = lib.nb_abi_version()
     if v != NB_ABI_VERSION:
         raise RuntimeError(f"{LIB_NAME} ABI version {v} != {NB_ABI_VERSION}; rebuild the library")

@@ -261,6 +261,20 @@ class ModelBuilder:
         self.joint_q: list[float] = []
         self.articulation_start: list[int] = []
         self.num_rigid_contacts_per_world: int | None = None
+        # particles and springs (builder.py:816, 899; add_particle / add_spring at 7186-7320)
+        self.default_particle_radius = 0.1
+        self.particle_max_velocity: float = 1e5
+        self.particle_q: list[tuple] = []
+        self.particle_qd: list[tuple] = []
+        self.particle_mass: list[float] = []
+        self.particle_radius: list[float] = []
+        self.particle_flags: list[int] = []
+        self.particle_world: list[int] = []
+        self.spring_indices: list[int] = []
+        self.spring_rest_length: list[float] = []
+        self.spring_stiffness: list[float] = []
+        self.spring_damping: list[float] = []
+        self.spring_control: list[float] = []
         self._requested_contact_attributes: set[str] = set()
         self._requested_state_attributes: set[str] = set()
 
@@ -280,6 +294,14 @@ class ModelBuilder:
     @property
     def joint_dof_count(self) -> int:
         return len(self.joint_axis)
+
+    @property
+    def particle_count(self) -> int:
+        return len(self.particle_q)
+
+    @property
+    def spring_count(self) -> int:
+        return len(self.spring_rest_length)
 
     @property
     def current_world(self) -> int:
@@ -318,6 +340,20 @@ class ModelBuilder:
 
     def add_builder(self, builder: "ModelBuilder", xform=None):
         xf = _as_xform(xform)
+        p_off = self.particle_count
+        for i in range(builder.particle_count):
+            self.particle_q.append(tuple(_transform_point(xf, np.asarray(builder.particle_q[i], dtype=np.float64))))
+            v = _quat_rotate(xf[3:], np.asarray(builder.particle_qd[i], dtype=np.float64))
+            self.particle_qd.append(tuple(v))
+            self.particle_mass.append(builder.particle_mass[i])
+            self.particle_radius.append(builder.particle_radius[i])
+            self.particle_flags.append(builder.particle_flags[i])
+            self.particle_world.append(self._current_world)
+        self.spring_indices.extend(int(i) + p_off for i in builder.spring_indices)
+        self.spring_rest_length.extend(builder.spring_rest_length)
+        self.spring_stiffness.extend(builder.spring_stiffness)
+        self.spring_damping.extend(builder.spring_damping)
+        self.spring_control.extend(builder.spring_control)
         b_off = self.body_count
         s_off = self.shape_count
         j_off = self.joint_count
@@ -607,6 +643,41 @@ class ModelBuilder:
     def add_ground_plane(self, height: float = 0.0, cfg=None, label=None) -> int:
         return self.add_shape_plane(plane=(*self.up_vector, -height), width=0.0, length=0.0, cfg=cfg,
                                     label=label or "ground_plane")
+
+    # ------------------------------------------------------------------ particles
+    def add_particle(self, pos, vel, mass: float, radius: float | None = None, flags: int = 1,
+                     custom_attributes=None) -> int:
+        """Add one particle (builder.py:7186-7230); mass 0 makes it kinematic."""
+        if custom_attributes:
+            raise NotImplementedError("custom attributes are not supported")
+        self.particle_q.append(tuple(float(x) for x in pos))
+        self.particle_qd.append(tuple(float(x) for x in vel))
+        self.particle_mass.append(float(mass))
+        self.particle_radius.append(float(self.default_particle_radius if radius is None else radius))
+        self.particle_flags.append(int(flags))
+        self.particle_world.append(self._current_world)
+        return self.particle_count - 1
+
+    def add_particles(self, pos, vel, mass, radius=None, flags=None, custom_attributes=None) -> None:
+        """Add a group of particles (builder.py:7232-7276)."""
+        n = len(pos)
+        radius = [self.default_particle_radius] * n if radius is None else radius
+        flags = [1] * n if flags is None else flags
+        for i in range(n):
+            self.add_particle(pos[i], vel[i], mass[i], radius[i], flags[i], custom_attributes)
+
+    def add_spring(self, i: int, j: int, ke: float, kd: float, control: float, custom_attributes=None) -> None:
+        """Spring between particles i and j; its rest length is their current distance (builder.py:7278-7320)."""
+        if custom_attributes:
+            raise NotImplementedError("custom attributes are not supported")
+        self.spring_indices.extend((int(i), int(j)))
+        self.spring_stiffness.append(float(ke))
+        self.spring_damping.append(float(kd))
+        self.spring_control.append(float(control))
+        p = np.asarray(self.particle_q[i], dtype=np.float32)
+        q = np.asarray(self.particle_q[j], dtype=np.float32)
+        delta = np.subtract(p, q)
+        self.spring_rest_length.append(float(np.sqrt(np.dot(delta, delta))))
 
     def request_state_attributes(self, *attributes: str) -> None:
         bad = sorted(set(attributes) - {"body_parent_f"})

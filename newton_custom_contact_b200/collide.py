@@ -244,7 +244,9 @@ class CollisionPipeline:
             rigid_contact_max = mrc if mrc > 0 else _estimate_rigid_contact_max(model)
         self._rigid_contact_max = int(rigid_contact_max)
         model.rigid_contact_max = self._rigid_contact_max
-        self._soft_contact_max = int(soft_contact_max) if soft_contact_max is not None else 0
+        # the reference's default capacity: every (particle, shape) pair (collide.py:814-815)
+        self._soft_contact_max = (int(soft_contact_max) if soft_contact_max is not None
+                                  else model.shape_count * getattr(model, "particle_count", 0))
         if mode == "explicit":
             if shape_pairs_filtered is None:
                 shape_pairs_filtered = model.host("shape_contact_pairs")
@@ -434,6 +436,19 @@ class CollisionPipeline:
     # ------------------------------------------------------------ collide
     def collide(self, state, contacts: Contacts, *, soft_contact_margin: float | None = None) -> None:
         _lib.require_cuda(self.device)
+        if self.model.body_count == 0:
+            # no rigid contacts without bodies
+            contacts.rigid_contact_count.zero_()
+            contacts._seg_valid = False
+        else:
+            self._collide_rigid(state, contacts)
+        if getattr(self.model, "particle_count", 0) and self.model.shape_count and contacts.soft_contact_max > 0:
+            from . import particles
+
+            margin = self.soft_contact_margin if soft_contact_margin is None else soft_contact_margin
+            particles.soft_collide(self.model, state, contacts, margin)
+
+    def _collide_rigid(self, state, contacts: Contacts) -> None:
         if contacts._seg is None or contacts._layout is not self:
             self.attach_segments(contacts)
         if contacts._world_offset.numel() != self.model.world_count + 1:

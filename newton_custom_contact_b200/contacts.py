@@ -79,6 +79,16 @@ class Contacts:
         self.force = torch.zeros((n, 6), **f32) if requested_attributes and "force" in requested_attributes else None
         self.soft_contact_max = int(soft_contact_max)
         self.soft_contact_count = self.contact_counters[1:2]
+        ns = self.soft_contact_max
+        self.soft_contact_particle = torch.zeros(ns, **i32)
+        self.soft_contact_shape = torch.zeros(ns, **i32)
+        self.soft_contact_body_pos = torch.zeros((ns, 3), **f32)
+        self.soft_contact_body_vel = torch.zeros((ns, 3), **f32)
+        self.soft_contact_normal = torch.zeros((ns, 3), **f32)
+        # per-particle first contact, written with the soft contacts (allocated by the first collide)
+        self._soft_particle_start: torch.Tensor | None = None
+        self._soft_margin = 0.0
+        self._soft_valid = False
         self.rigid_contact_max = n
         # solver-format segments; attached by CollisionPipeline.contacts()
         self._seg: dict[str, torch.Tensor] | None = None
@@ -88,6 +98,7 @@ class Contacts:
 
     def clear(self, bump_generation: bool = True) -> None:
         self.contact_counters.zero_()
+        self._soft_valid = False
         if bump_generation:
             self.contact_generation.add_(1)
         if self.clear_buffers:

@@ -31,12 +31,17 @@ class State:
         self.body_q: torch.Tensor | None = None
         self.body_qd: torch.Tensor | None = None
         self.body_f: torch.Tensor | None = None
+        self.particle_q: torch.Tensor | None = None
+        self.particle_qd: torch.Tensor | None = None
+        self.particle_f: torch.Tensor | None = None
         self.body_parent_f: torch.Tensor | None = None
         self.requires_grad = False
 
     def clear_forces(self) -> None:
-        """Zero body_f (state.py:156): a memset on the current stream through the library when body_f is a
-        CUDA tensor."""
+        """Zero body_f and particle_f (state.py:156): body_f by a memset on the current stream through the
+        library when it is a CUDA tensor."""
+        if self.particle_f is not None:
+            self.particle_f.zero_()
         if self.body_f is None:
             return
         if self.body_f.is_cuda and self.body_f.is_contiguous() and self.body_f.dtype == torch.float32:
@@ -50,7 +55,7 @@ class State:
 
     def assign(self, other: "State") -> None:
         """Copy the arrays of ``other`` into this state (state.py:169)."""
-        for name in ("body_q", "body_qd", "body_f"):
+        for name in ("body_q", "body_qd", "body_f", "particle_q", "particle_qd", "particle_f"):
             a, b = getattr(self, name), getattr(other, name)
             if a is not None and b is not None:
                 a.copy_(b)
@@ -86,6 +91,8 @@ class Model:
         self.world_count = 1
         self.rigid_contact_max = 0
         self.particle_count = 0
+        self.spring_count = 0
+        self.particle_max_radius = 0.0
         self._collision_pipeline = None
         self._requested_contact_attributes: set[str] = set()
         self._requested_state_attributes: set[str] = set()
@@ -151,6 +158,10 @@ class Model:
                           filter_pairs={(min(x, y), max(x, y)) for x, y in b.shape_collision_filter_pairs},
                           requested=set(b._requested_contact_attributes))
         m._requested_state_attributes = set(b._requested_state_attributes)
+        if b.particle_count:
+            from . import particles
+
+            particles.attach(m, b)
         return m
 
     @classmethod
@@ -275,6 +286,10 @@ class Model:
         s.body_q = self.body_q.clone()
         s.body_qd = self.body_qd.clone()
         s.body_f = torch.zeros((self.body_count, 6), dtype=torch.float32, device=self.device)
+        if self.particle_count:
+            s.particle_q = self.particle_q.clone()
+            s.particle_qd = self.particle_qd.clone()
+            s.particle_f = torch.zeros((self.particle_count, 3), dtype=torch.float32, device=self.device)
         if "body_parent_f" in self._requested_state_attributes:
             s.body_parent_f = torch.zeros((self.body_count, 6), dtype=torch.float32, device=self.device)
         s.requires_grad = bool(requires_grad) if requires_grad is not None else self.requires_grad

@@ -412,3 +412,53 @@ def scene_falling_shapes(worlds: int = 1, device=None):
                         b.add_shape_capsule(body, radius=0.2, half_height=0.4)
         b.end_world()
     return b.finalize(device=device), np.asarray(z0, np.float32)
+
+
+def scene_particles(seed: int = 7, cloth: int = 12, loose: int = 200, radius: float = 0.02, device=None,
+                    body_shapes: bool = False, loose_extent: float = 0.3, loose_height=(0.33, 0.7)):
+    """Particles dropped onto static shapes: a square cloth of ``cloth`` x ``cloth`` particles joined by
+    structural and shear springs, and ``loose`` free particles of radius U[0.5, 1] x ``radius`` above it.
+
+    Static colliders: the ground plane, a box, a sphere and a capsule under the drop (world -1).  With
+    ``body_shapes`` a free box body is added whose shape does not collide with particles.  The scene
+    exercises every particle kernel: soft contacts with all four shape types, particle-particle contacts
+    (cloth layers and loose particles pile), springs, and one inactive and one kinematic (mass 0) particle.
+    Returns (model, info) with dt 1/60 split into 4 substeps and 8 iterations.
+    """
+    rng = np.random.default_rng(seed)
+    b = ModelBuilder()
+    b.add_ground_plane()
+    b.add_shape_box(-1, xform=(0.15, 0.0, 0.1, 0.0, 0.0, 0.0, 1.0), hx=0.12, hy=0.2, hz=0.1)
+    b.add_shape_sphere(-1, xform=(-0.2, 0.1, 0.12, 0.0, 0.0, 0.0, 1.0), radius=0.12)
+    q = quat_from_axis_angle((1.0, 0.0, 0.0), math.pi / 2)
+    b.add_shape_capsule(-1, xform=(0.0, -0.25, 0.06, *q), radius=0.06, half_height=0.2)
+    if body_shapes:
+        cfg = ModelBuilder.ShapeConfig(has_particle_collision=False)
+        body = b.add_body(xform=(0.6, 0.6, 0.3, 0.0, 0.0, 0.0, 1.0))
+        b.add_joint_free(body)
+        b.add_shape_box(body, hx=0.05, hy=0.05, hz=0.05, cfg=cfg)
+    spacing = 2.2 * radius
+    origin = np.array([-0.5 * (cloth - 1) * spacing, -0.5 * (cloth - 1) * spacing, 0.28])
+    idx = {}
+    for i in range(cloth):
+        for j in range(cloth):
+            p = origin + np.array([i * spacing, j * spacing, 0.0]) + rng.uniform(-1e-3, 1e-3, 3)
+            idx[i, j] = b.add_particle(tuple(p), (0.0, 0.0, 0.0), 0.1, radius=radius)
+    for i in range(cloth):
+        for j in range(cloth):
+            for di, dj in ((1, 0), (0, 1), (1, 1), (1, -1)):
+                if (i + di, j + dj) in idx:
+                    b.add_spring(idx[i, j], idx[i + di, j + dj], 1.0e3 if di * dj == 0 else 2.5e2, 0.5, 0.0)
+    for _ in range(loose):
+        p = (rng.uniform(-loose_extent, loose_extent), rng.uniform(-loose_extent, loose_extent),
+             rng.uniform(*loose_height))
+        v = tuple(rng.normal(0.0, 0.3, 3) + np.array([0.0, 0.0, -1.5]))
+        b.add_particle(p, v, float(rng.uniform(0.005, 0.02)), radius=float(radius * rng.uniform(0.5, 1.0)))
+    # an inactive particle and a kinematic one (mass 0: no gravity, no corrections)
+    b.add_particle((0.4, 0.4, 0.5), (0.0, 0.0, -1.0), 0.01, radius=radius, flags=0)
+    b.add_particle((-0.4, 0.4, 0.02), (0.1, 0.0, 0.0), 0.0, radius=radius)
+    model = b.finalize(device=device)
+    model.particle_mu = 0.4
+    model.particle_cohesion = 0.002
+    model.soft_contact_mu = 0.6
+    return model, {"dt": 1.0 / 60.0, "substeps": 4, "iterations": 8}

@@ -9,8 +9,10 @@ reference that a caller can observe:
   * per-body constraint deltas are summed in float in contact (joint) order --
     the reference's sums run sequentially -- so results are bit-reproducible
     where the reference's atomic order is unspecified;
-  * particles and springs are not part of this build and raise
-    ``NotImplementedError``;
+  * particles (particles.py: integration, springs, particle-particle and
+    particle-static-shape contacts) run before the bodies in every substep;
+    particle contacts with body-attached shapes, particle restitution,
+    triangles, bending edges and tetrahedra raise ``NotImplementedError``;
   * an optional learned warm start (``solver.warm_start``, warmstart.py) has
     no counterpart in the reference; it is off by default.
 """
@@ -44,8 +46,6 @@ class SolverXPBD:
                  joint_angular_compliance: float = 0.0, rigid_contact_relaxation: float = 0.8,
                  rigid_contact_con_weighting: bool = True, angular_damping: float = 0.0,
                  enable_restitution: bool = False):
-        if getattr(model, "particle_count", 0):
-            raise NotImplementedError("particles are not supported by this build")
         if iterations < 0:
             raise ValueError("iterations must be non-negative")
         self.model = model
@@ -71,6 +71,11 @@ class SolverXPBD:
         self._joint_impulse = None
         # optional learned warm start (warmstart.WarmStart); None = the plain solver
         self.warm_start = None
+        self._particles = None
+        if getattr(model, "particle_count", 0):
+            from .particles import ParticleSolver
+
+            self._particles = ParticleSolver(model, self)
 
     @property
     def device(self):
@@ -110,6 +115,9 @@ class SolverXPBD:
     def step(self, state_in, state_out, control, contacts: Contacts | None, dt: float) -> None:
         model = self.model
         _lib.require_cuda(model.device)
+        if self._particles is not None:
+            # particles touch static shapes only, so their substep is independent of the bodies'
+            self._particles.step(state_in, state_out, contacts, dt)
         if model.body_count == 0:
             return
         # control=None: the model's default targets and no joint forces (the reference builds

@@ -1,0 +1,305 @@
+"""TEST INFRASTRUCTURE ONLY -- CPU oracle of the XPBD particle path.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use it.
+
+A numpy float32 restatement of the reference's particle kernels, vectorised
+over particles, contacts and springs (a different structure from the CUDA
+kernels, which run one thread per particle):
+
+  create_soft_contacts       newton/_src/geometry/kernels.py:1000-1140
+  sdf_* and their gradients  newton/_src/geometry/kernels.py:165-330, 568-590
+  integrate_particles        newton/_src/solvers/solver.py:11-47
+  solve_particle_shape_contacts   newton/_src/solvers/xpbd/kernels.py:114-222
+  solve_particle_particle_contacts newton/_src/solvers/xpbd/kernels.py:225-289
+  solve_springs              newton/_src/solvers/xpbd/kernels.py:292-356
+  apply_particle_deltas      newton/_src/solvers/xpbd/kernels.py:776-807
+  iteration order            newton/_src/solvers/xpbd/solver_xpbd.py:303-320, 377-505
+
+Every float operation is a float32 numpy operation in the order the
+reference writes it (numpy never fuses a*b+c, sqrt and division are
+correctly rounded).  Where the reference scatters with atomic adds, whose
+order varies from run to run, the oracle fixes one order per particle: its
+soft contacts in list order, then its particle neighbours in ascending index
+(all j within the contact distance, found by brute force), then its springs in
+ascending index.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+F = np.float32
+ACTIVE = 1
+COLLIDE_PARTICLES = 1 << 2
+GEO_PLANE, GEO_SPHERE, GEO_CAPSULE, GEO_BOX = 1, 3, 4, 7
+
+
+def _dot(a, b):
+    return a[..., 0] * b[..., 0] + a[..., 1] * b[..., 1] + a[..., 2] * b[..., 2]
+
+
+def _length(a):
+    return np.sqrt(_dot(a, a))
+
+
+def _normalize(a):
+    n = _length(a)
+    safe = np.where(n > 0, n, F(1))
+    return np.where((n > 0)[..., None], a / safe[..., None], F(0))
+
+
+def _cross(a, b):
+    return np.stack([a[..., 1] * b[..., 2] - a[..., 2] * b[..., 1], a[..., 2] * b[..., 0] - a[..., 0] * b[..., 2],
+                     a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0]], axis=-1)
+
+
+def _max(a, b):  # wp.max: a > b ? a : b
+    return np.where(a > b, a, b)
+
+
+def _min(a, b):
+    return np.where(a < b, a, b)
+
+
+def _qrot(q, v, sign=1):
+    """wp.quat_rotate (sign=1) / quat_rotate_inv (sign=-1) for quaternions (x, y, z, w)."""
+    qx, qy, qz, qw = q[..., 0], q[..., 1], q[..., 2], q[..., 3]
+    vx, vy, vz = v[..., 0], v[..., 1], v[..., 2]
+    c = F(2) * qw * qw - F(1)
+    d = F(2) * (qx * vx + qy * vy + qz * vz)
+    tx = (qy * vz - qz * vy) * qw * F(2)
+    ty = (qz * vx - qx * vz) * qw * F(2)
+    tz = (qx * vy - qy * vx) * qw * F(2)
+    if sign > 0:
+        return np.stack([vx * c + qx * d + tx, vy * c + qy * d + ty, vz * c + qz * d + tz], axis=-1)
+    return np.stack([vx * c + qx * d - tx, vy * c + qy * d - ty, vz * c + qz * d - tz], axis=-1)
+
+
+def _qmul(a, b):
+    ax, ay, az, aw = a[..., 0], a[..., 1], a[..., 2], a[..., 3]
+    bx, by, bz, bw = b[..., 0], b[..., 1], b[..., 2], b[..., 3]
+    return np.stack([aw * bx + bw * ax + ay * bz - by * az, aw * by + bw * ay + az * bx - bz * ax,
+                     aw * bz + bw * az + ax * by - bx * ay, aw * bw - ax * bx - ay * by - az * bz], axis=-1)
+
+
+def _tf_point(p, q, v):
+    return _qrot(q, v) + p
+
+
+def _sdf(geo, x, scale):
+    """Signed distance and gradient of one shape type for an array of local points."""
+    P = x.shape[0]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        if geo == GEO_SPHERE:
+            l = _length(x)
+            d = l - scale[0]
+            n = np.where((l > F(1e-8))[:, None], x / np.where(l > 0, l, F(1))[:, None], np.array([0, 0, 1], F))
+            return d, n
+        if geo == GEO_BOX:
+            hx, hy, hz = scale
+            qx, qy, qz = np.abs(x[:, 0]) - hx, np.abs(x[:, 1]) - hy, np.abs(x[:, 2]) - hz
+            e = np.stack([_max(qx, F(0)), _max(qy, F(0)), _max(qz, F(0))], axis=-1)
+            d = _length(e) + _min(_max(qx, _max(qy, qz)), F(0))
+            cl = np.stack([_min(_max(x[:, 0], -hx), hx), _min(_max(x[:, 1], -hy), hy),
+                           _min(_max(x[:, 2], -hz), hz)], axis=-1)
+            ext = _normalize(x - cl)
+            sgn = np.where(x < 0, F(-1), F(1))
+            z = np.zeros(P, F)
+            nx = np.stack([sgn[:, 0], z, z], -1)
+            ny = np.stack([z, sgn[:, 1], z], -1)
+            nz = np.stack([z, z, sgn[:, 2]], -1)
+            outside = (qx > 0) | (qy > 0) | (qz > 0)
+            use_x = ((qx > qy) & (qx > qz)) | ((qy == 0) & (qz == 0))
+            use_y = ((qy > qx) & (qy > qz)) | ((qx == 0) & (qz == 0))
+            inner = np.where(use_x[:, None], nx, np.where(use_y[:, None], ny, nz))
+            return d, np.where(outside[:, None], ext, inner)
+        if geo == GEO_CAPSULE:
+            r, hh = scale[0], scale[1]
+            top, bot = x[:, 2] > hh, x[:, 2] < -hh
+            vz = np.where(top, x[:, 2] - hh, np.where(bot, x[:, 2] + hh, F(0)))
+            v = np.stack([x[:, 0], x[:, 1], vz], -1)
+            l = _length(v)
+            d = l - r
+            fb = np.where(bot[:, None], np.array([0, 0, -1], F), np.array([0, 0, 1], F))
+            n = np.where((l > F(1e-8))[:, None], v / np.where(l > 0, l, F(1))[:, None], fb)
+            return d, n
+        if geo == GEO_PLANE:
+            w, ln = scale[0] * F(0.5), scale[1] * F(0.5)
+            if w > 0 and ln > 0:
+                d = _max(_max(np.abs(x[:, 0]) - w, np.abs(x[:, 1]) - ln), np.abs(x[:, 2]))
+            else:
+                d = x[:, 2].copy()
+            return d, np.tile(np.array([0, 0, 1], F), (P, 1))
+    return np.full(P, F(1e6)), np.zeros((P, 3), F)
+
+
+def soft_collide(h: dict, particle_q, body_q, margin: float, soft_contact_max: int):
+    """Soft contacts in (particle, shape) order.  ``h`` holds the model's host arrays (particle_*, shape_*).
+
+    Returns (count, particle, shape, body_pos, body_vel, normal) with the first soft_contact_max stored.
+    """
+    x = np.asarray(particle_q, F).reshape(-1, 3)
+    P, S = x.shape[0], h["shape_type"].shape[0]
+    radius = h["particle_radius"].astype(F)
+    act = (h["particle_flags"] & ACTIVE) != 0
+    pw = h["particle_world"]
+    margin = F(margin)
+    hit = np.zeros((P, S), bool)
+    out = {k: np.zeros((P, S, 3), F) for k in ("body_pos", "body_vel", "normal")}
+    ident = np.array([0, 0, 0, 0, 0, 0, 1], F)
+    for s in range(S):
+        if not (h["shape_flags"][s] & COLLIDE_PARTICLES):
+            continue
+        sw = h["shape_world"][s]
+        ok = act & ~((pw != -1) & (sw != -1) & (pw != sw))
+        b = h["shape_body"][s]
+        X_wb = np.asarray(body_q, F).reshape(-1, 7)[b] if b >= 0 else ident
+        X_bs = h["shape_transform"][s].astype(F)
+        ws_p = _tf_point(X_wb[:3], X_wb[3:], X_bs[:3])
+        ws_q = _qmul(X_wb[3:], X_bs[3:])
+        qi = ws_q * np.array([-1, -1, -1, 1], F)
+        sw_p = -_qrot(qi, ws_p)
+        xl = _tf_point(sw_p, qi, x)
+        d, n = _sdf(int(h["shape_type"][s]), xl, h["shape_scale"][s].astype(F))
+        hit[:, s] = ok & (d < margin + radius)
+        out["body_pos"][:, s] = _tf_point(X_bs[:3], X_bs[3:], xl - n * d[:, None])
+        out["body_vel"][:, s] = _qrot(X_bs[3:], np.zeros((P, 3), F))
+        out["normal"][:, s] = _qrot(ws_q, n)
+    pi, si = np.nonzero(hit)
+    count = int(pi.shape[0])
+    keep = min(count, int(soft_contact_max))
+    return (count, pi[:keep].astype(np.int32), si[:keep].astype(np.int32),
+            out["body_pos"][pi, si][:keep], out["body_vel"][pi, si][:keep], out["normal"][pi, si][:keep])
+
+
+def _spring_csr(h):
+    P = h["particle_radius"].shape[0]
+    idx = h["spring_indices"].reshape(-1, 2)
+    lists = [[] for _ in range(P)]
+    for s, (a, b) in enumerate(idx):
+        lists[a].append(s)
+        lists[b].append(s)
+    return [sorted(x) for x in lists]
+
+
+def _accumulate(delta, owner, contrib):
+    """delta[owner[k]] += contrib[k] for k in list order, sequentially per owner."""
+    if owner.size == 0:
+        return
+    order = np.argsort(owner, kind="stable")
+    owner, contrib = owner[order], contrib[order]
+    first = np.r_[0, np.nonzero(np.diff(owner))[0] + 1]
+    rank = np.arange(owner.size) - np.repeat(first, np.diff(np.r_[first, owner.size]))
+    for lvl in range(int(rank.max()) + 1):
+        m = rank == lvl
+        delta[owner[m]] = delta[owner[m]] + contrib[m]
+
+
+def step(h: dict, params: dict, q, qd, f, soft, dt: float, iterations: int, relaxation: float):
+    """One particle substep; returns (q_out, qd_out).  ``soft`` is soft_collide's tuple or None."""
+    dt, relax = F(dt), F(relaxation)
+    x0 = np.asarray(q, F).reshape(-1, 3)
+    v0 = np.asarray(qd, F).reshape(-1, 3)
+    P = x0.shape[0]
+    f0 = np.zeros_like(x0) if f is None else np.asarray(f, F).reshape(-1, 3)
+    w = h["particle_inv_mass"].astype(F)
+    radius = h["particle_radius"].astype(F)
+    act = (h["particle_flags"] & ACTIVE) != 0
+    vmax = F(params["particle_max_velocity"])
+    grav = h["gravity"].astype(F).reshape(-1, 3)[np.maximum(h["particle_world"], 0)]
+    gate = np.where(-w < 0, F(1), F(0))
+    v1 = v0 + (f0 * w[:, None] + grav * gate[:, None]) * dt
+    mag = _length(v1)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        v1 = np.where((mag > vmax)[:, None], v1 * (vmax / mag)[:, None], v1)
+    x1 = x0 + v1 * dt
+    x = np.where(act[:, None], x1, x0)
+    v = np.where(act[:, None], v1, v0)
+
+    max_r = F(params["particle_max_radius"])
+    coh = F(params["particle_cohesion"])
+    pp_on = max_r > 0 and P > 1
+    springs = h["spring_indices"].reshape(-1, 2)
+    csr = _spring_csr(h) if springs.shape[0] else None
+    shape_mu = h["shape_material_mu"].astype(F)
+    for _ in range(iterations):
+        delta = np.zeros((P, 3), F)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            # particle-shape contacts (static shapes)
+            if soft is not None and soft[0] > 0:
+                cnt, cp, cs, bpos, bvel, cn = soft
+                ok = act[cp] & (h["shape_body"][cs] < 0)
+                bx = bpos + np.zeros(3, F)  # identity body transform
+                r = bx - np.zeros(3, F)
+                c = _dot(cn, x[cp] - bx) - radius[cp]
+                ok &= ~(c > F(params["particle_adhesion"]))
+                mu = F(0.5) * (F(params["soft_contact_mu"]) + shape_mu[cs])
+                bv = (np.zeros(3, F) + _cross(np.zeros_like(r), r)) + bvel
+                vr = v[cp] - bv
+                dn = cn * c[:, None]
+                vt = vr - cn * _dot(cn, vr)[:, None]
+                denom = w[cp] + F(0)
+                ok &= denom != 0
+                lf = _max(mu * c, -_length(vt) * dt)
+                df = _normalize(vt) * lf[:, None]
+                dtot = (df - dn) / denom[:, None] * relax
+                _accumulate(delta, cp[ok], w[cp][ok][:, None] * dtot[ok])
+            # particle-particle contacts, neighbours in ascending index
+            if pp_on:
+                nvec = x[:, None, :] - x[None, :, :]
+                d = _length(nvec)
+                err = d - radius[:, None] - radius[None, :]
+                denom = w[:, None] + w[None, :]
+                acc = (act[:, None] & act[None, :] & ~np.eye(P, dtype=bool) & (err <= coh) & (denom > 0))
+                n = nvec / d[..., None]
+                vrel = v[:, None, :] - v[None, :, :]
+                dn = n * err[..., None]
+                vt = vrel - n * _dot(n, vrel)[..., None]
+                lf = _max(F(params["particle_mu"]) * err, -_length(vt) * dt)
+                df = _normalize(vt) * lf[..., None]
+                contrib = np.where(acc[..., None], (df - dn) / denom[..., None], F(0))
+                dpp = np.zeros((P, 3), F)
+                for j in range(P):  # sequential over j: dpp += contribution of j where accepted
+                    m = acc[:, j]
+                    dpp[m] = dpp[m] + contrib[m, j]
+                delta = np.where(act[:, None], delta + dpp * w[:, None] * relax, delta)
+            # springs, ascending spring index per particle
+            if csr is not None:
+                a, b = springs[:, 0], springs[:, 1]
+                xij = x[a] - x[b]
+                vij = v[a] - v[b]
+                l = _length(xij)
+                n = xij / l[:, None]
+                c = l - h["spring_rest_length"].astype(F)
+                wi, wj = w[a], w[b]
+                den = wi + wj
+                ke, kd = h["spring_stiffness"].astype(F), h["spring_damping"].astype(F)
+                ok = (l != 0) & ~((den <= 0) | (ke <= 0) | (kd < 0))
+                alpha = F(1) / (ke * dt * dt)
+                gamma = kd / (ke * dt)
+                gcv = dt * _dot(n, vij)
+                dl = F(-1) * (c + alpha * F(0) + gamma * gcv) / ((F(1) + gamma) * den + alpha)
+                dxi = n * (wi * dl)[:, None]
+                dxj = (F(-1) * n) * (wj * dl)[:, None]
+                owners, contribs = [], []
+                for p in range(P):
+                    for s in csr[p]:
+                        if not ok[s]:
+                            continue
+                        if a[s] == p:
+                            owners.append(p)
+                            contribs.append(dxi[s])
+                        if b[s] == p:
+                            owners.append(p)
+                            contribs.append(dxj[s])
+                if owners:
+                    _accumulate(delta, np.asarray(owners), np.asarray(contribs, F))
+        # apply_particle_deltas
+        xn = x + delta
+        vn = (xn - x0) / dt
+        mag = _length(vn)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            vn = np.where((mag > vmax)[:, None], vn * (vmax / mag)[:, None], vn)
+        x = np.where(act[:, None], xn, x)
+        v = np.where(act[:, None], vn, v)
+    return x, v

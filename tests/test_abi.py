@@ -41,7 +41,8 @@ def test_struct_layouts_match_header(tmp_path):
     """sizeof / offsetof of every struct, compiled from the header, equal the ctypes mirrors."""
     structs = {"NbModelDesc": _abi.NbModelDesc, "NbContactSeg": _abi.NbContactSeg,
                "NbContactsPublic": _abi.NbContactsPublic, "NbXpbdParams": _abi.NbXpbdParams,
-               "NbStepIO": _abi.NbStepIO}
+               "NbStepIO": _abi.NbStepIO, "NbParticleDesc": _abi.NbParticleDesc,
+               "NbSoftContacts": _abi.NbSoftContacts, "NbParticleIO": _abi.NbParticleIO}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "newton_b200.h"', "int main(void) {"]
     for name, cls in structs.items():
         lines.append(f'printf("{name} %zu\\n", sizeof({name}));')
