@@ -449,7 +449,7 @@ def articulated_arm(dev, stream, flush, steps, warmup):
 
 
 def particles_arm(dev, stream, flush, steps, warmup):
-    """The particle path: a 100 x 100 spring cloth (10,000 particles, 39,402 springs) and 100,000 loose
+    """The particle path: a 100 x 100 spring cloth (10,000 particles, 39,402 springs, 9,801 bending edges) and 100,000 loose
     particles dropped onto a ground plane, a box, a sphere and a capsule; dt 1/240 s, 8 iterations.  One
     step is 60 substeps (collide + solver step each, CUDA-graph captured) from the same start state,
     taken after 40 untimed substeps, when the cloth and the loose particles are landing."""
@@ -505,15 +505,16 @@ def particles_arm(dev, stream, flush, steps, warmup):
     act = (model.particle_flags & 1) != 0
     del g
     P = model.particle_count
-    return {"workload": "particles: 100x100 spring cloth + 100,000 loose particles (r 5..10 mm) dropped on a "
+    return {"workload": "particles: 100x100 spring + bending cloth + 100,000 loose particles (r 5..10 mm) dropped on a "
                         "plane, box, sphere and capsule; dt 1/240, 8 iterations, substeps 41..100 of the drop",
             "value": P * n_sub * steps / (ms / 1e3), "unit": "particle-substeps/s",
             "ms_per_substep": ms / steps / n_sub, "particles": P, "springs": model.spring_count,
             "soft_contacts_at_step_end": int(torch.stack(contacts_seen).float().mean().item()),
             "min_height_above_radius_m": float((q[act, 2] - r[act]).min().item()),
             "final_state_finite": bool(torch.isfinite(q).all().item()),
-            # soft contacts 3 kernels, integrate 1, then constraints + apply per iteration
-            "status": solver._particles.status(), "gpu_launches_per_substep": 3 + 1 + 2 * 8,
+            # soft contacts 3 kernels, integrate 1, then constraints (+ bending) + apply per iteration
+            "status": solver._particles.status(),
+            "gpu_launches_per_substep": 3 + 1 + (3 if model.edge_count else 2) * 8, "bending_edges": model.edge_count,
             "scene_build_s": round(build_s, 1)}
 
 

@@ -612,6 +612,13 @@ typedef struct NbParticleDesc {
     const int32_t* shape_world;       /* [Sh]  */
     const int32_t* shape_flags;       /* [Sh]  bit 2 = COLLIDE_PARTICLES */
     const float* shape_mu;            /* [Sh]  */
+    int32_t edge_count;               /* bending edges */
+    int32_t pad_e;
+    const int32_t* edge_indices;      /* [E,4] (i, j, k, l): opposite vertices i, j of the hinge edge k-l */
+    const float* edge_rest_angle;     /* [E]   */
+    const float* edge_bending_properties; /* [E,2] (ke, kd) */
+    const int32_t* particle_edge_start;   /* [P+1] edges of particle p: particle_edge_list[start[p]..start[p+1]) */
+    const int32_t* particle_edge_list;    /* edge indices, ascending per particle */
 } NbParticleDesc;
 
 /* Soft contacts (newton/_src/sim/contacts.py soft_contact_* arrays), in
@@ -663,10 +670,13 @@ int nb_soft_collide(const NbParticleDesc* pd, const float* particle_q, const flo
  * newton/_src/solvers/xpbd/solver_xpbd.py:303-320, 377-505, 657-660):
  * integrate_particles (solver.py:11-47), then `iterations` times the
  * particle-shape contacts (kernels.py:114-222), particle-particle contacts
- * (kernels.py:225-289), springs (kernels.py:292-356) and
- * apply_particle_deltas (kernels.py:776-807).  Each particle gathers its
+ * (kernels.py:225-289), springs (kernels.py:292-356), bending edges
+ * (bending_constraint, kernels.py:358-457; the dihedral angle through an
+ * atan2 built on the library's own asin, so that the oracle can match it bit
+ * for bit) and apply_particle_deltas (kernels.py:776-807).  Each particle gathers its
  * corrections in a fixed order (its soft contacts, then its particle
- * neighbours in ascending index, then its springs in ascending index)
+ * neighbours in ascending index, then its springs, then its bending edges,
+ * each in ascending index)
  * instead of the reference's atomic adds, so results do not change from run
  * to run.  sc may be NULL (no soft contacts); sc->particle_start must come
  * from nb_soft_collide on the same contacts.  Soft contacts with a

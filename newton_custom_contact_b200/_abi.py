@@ -265,7 +265,11 @@ class NbParticleDesc(C.Structure):
     ] + [(k, _fp) for k in ("particle_inv_mass", "particle_radius", "particle_flags", "particle_world", "gravity",
                             "spring_indices", "spring_rest_length", "spring_stiffness", "spring_damping",
                             "particle_spring_start", "particle_spring_list", "shape_body", "shape_type",
-                            "shape_transform", "shape_scale", "shape_world", "shape_flags", "shape_mu")]
+                            "shape_transform", "shape_scale", "shape_world", "shape_flags", "shape_mu")] + [
+        ("edge_count", C.c_int32),
+        ("pad_e", C.c_int32),
+    ] + [(k, _fp) for k in ("edge_indices", "edge_rest_angle", "edge_bending_properties", "particle_edge_start",
+                            "particle_edge_list")]
 
 
 class NbSoftContacts(C.Structure):

@@ -275,6 +275,13 @@ class ModelBuilder:
         self.spring_stiffness: list[float] = []
         self.spring_damping: list[float] = []
         self.spring_control: list[float] = []
+        # bending edges (builder.py:840-843, 999-1006; add_edge at 7589-7650)
+        self.default_edge_ke = 100.0
+        self.default_edge_kd = 0.0
+        self.edge_indices: list[tuple[int, int, int, int]] = []
+        self.edge_rest_angle: list[float] = []
+        self.edge_rest_length: list[float] = []
+        self.edge_bending_properties: list[tuple[float, float]] = []
         self._requested_contact_attributes: set[str] = set()
         self._requested_state_attributes: set[str] = set()
 
@@ -302,6 +309,10 @@ class ModelBuilder:
     @property
     def spring_count(self) -> int:
         return len(self.spring_rest_length)
+
+    @property
+    def edge_count(self) -> int:
+        return len(self.edge_rest_angle)
 
     @property
     def current_world(self) -> int:
@@ -354,6 +365,11 @@ class ModelBuilder:
         self.spring_stiffness.extend(builder.spring_stiffness)
         self.spring_damping.extend(builder.spring_damping)
         self.spring_control.extend(builder.spring_control)
+        for e in builder.edge_indices:
+            self.edge_indices.append(tuple(int(v) + p_off if v != -1 else -1 for v in e))
+        self.edge_rest_angle.extend(builder.edge_rest_angle)
+        self.edge_rest_length.extend(builder.edge_rest_length)
+        self.edge_bending_properties.extend(builder.edge_bending_properties)
         b_off = self.body_count
         s_off = self.shape_count
         j_off = self.joint_count
@@ -678,6 +694,34 @@ class ModelBuilder:
         q = np.asarray(self.particle_q[j], dtype=np.float32)
         delta = np.subtract(p, q)
         self.spring_rest_length.append(float(np.sqrt(np.dot(delta, delta))))
+
+    def add_edge(self, i: int, j: int, k: int, l: int, rest: float | None = None, edge_ke: float | None = None,
+                 edge_kd: float | None = None, custom_attributes=None) -> int:
+        """Bending edge k-l between the triangles (i, k, l) and (j, l, k) (builder.py:7589-7650); the rest
+        angle defaults to the current dihedral angle."""
+        if custom_attributes:
+            raise NotImplementedError("custom attributes are not supported")
+        edge_ke = self.default_edge_ke if edge_ke is None else edge_ke
+        edge_kd = self.default_edge_kd if edge_kd is None else edge_kd
+        x3 = np.asarray(self.particle_q[k], dtype=np.float32)
+        x4 = np.asarray(self.particle_q[l], dtype=np.float32)
+        if rest is None:
+            rest = 0.0
+            if i != -1 and j != -1:
+                x1 = np.asarray(self.particle_q[i], dtype=np.float32)
+                x2 = np.asarray(self.particle_q[j], dtype=np.float32)
+                unit = lambda a: a / np.linalg.norm(a)  # noqa: E731
+                n1 = unit(np.cross(x3 - x1, x4 - x1))
+                n2 = unit(np.cross(x4 - x2, x3 - x2))
+                e = unit(x4 - x3)
+                cos_theta = np.clip(np.dot(n1, n2), -1.0, 1.0)
+                sin_theta = np.dot(np.cross(n1, n2), e)
+                rest = math.atan2(sin_theta, cos_theta)
+        self.edge_indices.append((int(i), int(j), int(k), int(l)))
+        self.edge_rest_angle.append(float(rest))
+        self.edge_rest_length.append(float(np.linalg.norm(x4 - x3)))
+        self.edge_bending_properties.append((float(edge_ke), float(edge_kd)))
+        return len(self.edge_indices) - 1
 
     def request_state_attributes(self, *attributes: str) -> None:
         bad = sorted(set(attributes) - {"body_parent_f"})

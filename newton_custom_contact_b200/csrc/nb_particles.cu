@@ -35,6 +35,21 @@ NB_D void st3(float* a, int i, V3 v) {
 // wp.sign: -1 for negative arguments, +1 otherwise
 NB_D float warp_sign(float x) { return x < 0.0f ? -1.0f : 1.0f; }
 
+// atan2 from the library's asin (nb_math.cuh), so the CPU oracle reproduces it bit for bit: the angle
+// is asin of the smaller of |x|, |y| over the radius (argument at most 1/sqrt 2, where asin is well
+// conditioned), shifted into its quadrant.  atan2(0, 0) = 0.
+NB_D float nb_atan2(float y, float x) {
+    const float r = sqrtf(x * x + y * y);
+    if (r == 0.0f) return 0.0f;
+    if (fabsf(y) <= fabsf(x)) {
+        const float a = nb_asin(y / r);
+        if (x > 0.0f) return a;
+        return y < 0.0f ? -3.1415927410125732f - a : 3.1415927410125732f - a;
+    }
+    const float a = 1.5707963705062866f - nb_asin(x / r);
+    return y < 0.0f ? -a : a;
+}
+
 // Signed distance and outward gradient in the shape frame (newton/_src/geometry/
 // kernels.py:165-330 sdf_sphere/_grad, sdf_box/_grad, sdf_capsule/_grad with the
 // Z up axis, 568-590 sdf_plane).
@@ -432,6 +447,56 @@ __global__ void __launch_bounds__(kThreads) particle_constraints_kernel(NbPartic
     st3(io.delta, i, delta);
 }
 
+// Bending edges (bending_constraint, kernels.py:358-457) of one particle, added to its delta after the
+// constraint kernel's terms (the same order as one sequential sum); a kernel of its own so that the
+// constraint kernel keeps its register budget.  The solver zeroes the multipliers every iteration.
+__global__ void __launch_bounds__(kThreads) particle_bending_kernel(NbParticleDesc pd, NbParticleIO io, float dt) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= pd.particle_count) return;
+    const int e_lo = pd.particle_edge_start[i], e_hi = pd.particle_edge_start[i + 1];
+    if (e_lo == e_hi) return;
+    const float* xq = io.particle_q_out;
+    const float* vq = io.particle_qd_out;
+    V3 delta = ld3(io.delta, i);
+    {
+        for (int k = e_lo; k < e_hi; ++k) {
+            const int e = pd.particle_edge_list[k];
+            const int* ix = pd.edge_indices + 4 * e;
+            const float ke = pd.edge_bending_properties[2 * e], kd = pd.edge_bending_properties[2 * e + 1];
+            const V3 x1 = ld3(xq, ix[0]), x2 = ld3(xq, ix[1]), x3 = ld3(xq, ix[2]), x4 = ld3(xq, ix[3]);
+            const float w[4] = {pd.particle_inv_mass[ix[0]], pd.particle_inv_mass[ix[1]],
+                                pd.particle_inv_mass[ix[2]], pd.particle_inv_mass[ix[3]]};
+            const V3 n1 = cross(sub(x3, x1), sub(x4, x1));
+            const V3 n2 = cross(sub(x4, x2), sub(x3, x2));
+            const V3 ev = sub(x4, x3);
+            const float n1_length = length(n1), n2_length = length(n2), e_length = length(ev);
+            if (n1_length < 1.0e-6f || n2_length < 1.0e-6f || e_length < 1.0e-6f) continue;
+            const V3 n1_hat = divs(n1, n1_length), n2_hat = divs(n2, n2_length), e_hat = divs(ev, e_length);
+            const float cos_theta = dot(n1_hat, n2_hat);
+            const float sin_theta = dot(cross(n1_hat, n2_hat), e_hat);
+            const float c = nb_atan2(sin_theta, cos_theta) - pd.edge_rest_angle[e];
+            V3 grad[4];
+            grad[0] = mul(neg(n1_hat), e_length);
+            grad[1] = mul(neg(n2_hat), e_length);
+            grad[2] = sub(mul(neg(n1_hat), dot(sub(x1, x4), e_hat)), mul(n2_hat, dot(sub(x2, x4), e_hat)));
+            grad[3] = sub(mul(neg(n1_hat), dot(sub(x3, x1), e_hat)), mul(n2_hat, dot(sub(x3, x2), e_hat)));
+            const float denominator = w[0] * length_sq(grad[0]) + w[1] * length_sq(grad[1]) +
+                                      w[2] * length_sq(grad[2]) + w[3] * length_sq(grad[3]);
+            if (denominator <= 0.0f || ke <= 0.0f || kd < 0.0f) continue;
+            const float alpha = 1.0f / (ke * dt * dt);
+            const float gamma = kd / (ke * dt);
+            const float grad_dot_v = dt * (dot(grad[0], ld3(vq, ix[0])) + dot(grad[1], ld3(vq, ix[1])) +
+                                           dot(grad[2], ld3(vq, ix[2])) + dot(grad[3], ld3(vq, ix[3])));
+            const float lambda_prev = 0.0f;
+            const float dlambda =
+                -1.0f * (c + alpha * lambda_prev + gamma * grad_dot_v) / ((1.0f + gamma) * denominator + alpha);
+            for (int r = 0; r < 4; ++r)
+                if (ix[r] == i) delta = add(delta, mul(grad[r], w[r] * dlambda));
+        }
+    }
+    st3(io.delta, i, delta);
+}
+
 // apply_particle_deltas (kernels.py:776-807), in place; then the particle enters the next cell table.
 __global__ void __launch_bounds__(kThreads) particle_apply_kernel(NbParticleDesc pd, NbParticleIO io, float dt,
                                                                   Grid g, int next_table, int insert) {
@@ -457,6 +522,10 @@ bool check_pd(const NbParticleDesc* pd) {
         return false;
     if (pd->spring_count > 0 && (!pd->spring_indices || !pd->spring_rest_length || !pd->spring_stiffness ||
                                  !pd->spring_damping || !pd->particle_spring_start || !pd->particle_spring_list))
+        return false;
+    if (pd->edge_count < 0 || (pd->edge_count > 0 && (!pd->edge_indices || !pd->edge_rest_angle ||
+                                                       !pd->edge_bending_properties || !pd->particle_edge_start ||
+                                                       !pd->particle_edge_list)))
         return false;
     if (pd->shape_count > 0 && (!pd->shape_body || !pd->shape_type || !pd->shape_transform || !pd->shape_scale ||
                                 !pd->shape_world || !pd->shape_flags || !pd->shape_mu))
@@ -520,6 +589,7 @@ int nb_particle_step(const NbParticleDesc* pd, const NbParticleIO* io, const NbS
         const int table = it & 1;
         particle_constraints_kernel<<<con_blocks, kThreads, 0, st>>>(*pd, *io, scv, has_sc, dt, relaxation, g,
                                                                      table);
+        if (pd->edge_count > 0) particle_bending_kernel<<<blocks, kThreads, 0, st>>>(*pd, *io, dt);
         particle_apply_kernel<<<blocks, kThreads, 0, st>>>(*pd, *io, dt, g, table ^ 1,
                                                            g.on && it + 1 < iterations ? 1 : 0);
     }

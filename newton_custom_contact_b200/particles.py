@@ -13,8 +13,8 @@ The particle branch of the reference's pipeline, on the library's kernels
 
 Particles collide with each other and with STATIC shapes: the solver raises
 for a model where a particle-colliding shape is attached to a body (the
-two-way particle-body coupling is not built).  Triangles, bending edges,
-tetrahedra and particle restitution are not built either.
+two-way particle-body coupling is not built).  Bending edges are built;
+triangles, tetrahedra and particle restitution are not.
 """
 
 from __future__ import annotations
@@ -62,6 +62,22 @@ def attach(model, b) -> None:
     start = np.zeros(P + 1, dtype=np.int32)
     np.cumsum(np.bincount(owner, minlength=P), out=start[1:])
     h["particle_spring_start"] = start
+    E = b.edge_count
+    model.edge_count = E
+    h["edge_indices"] = np.asarray(b.edge_indices, dtype=np.int32).reshape(E, 4)
+    h["edge_rest_angle"] = np.asarray(b.edge_rest_angle, dtype=f32).reshape(E)
+    h["edge_rest_length"] = np.asarray(b.edge_rest_length, dtype=f32).reshape(E)
+    h["edge_bending_properties"] = np.asarray(b.edge_bending_properties, dtype=f32).reshape(E, 2)
+    # bending edges of each particle, ascending edge index (an edge with a -1 vertex does nothing)
+    ev = h["edge_indices"]
+    live = np.nonzero((ev >= 0).all(axis=1))[0]
+    owner = ev[live].reshape(-1).astype(np.int64)
+    edge = np.repeat(live, 4).astype(np.int64)
+    pairs = np.unique(np.stack([owner, edge], axis=1), axis=0) if owner.size else np.zeros((0, 2), np.int64)
+    h["particle_edge_list"] = pairs[:, 1].astype(np.int32)
+    estart = np.zeros(P + 1, dtype=np.int32)
+    np.cumsum(np.bincount(pairs[:, 0], minlength=P), out=estart[1:])
+    h["particle_edge_start"] = estart
     model.particle_max_radius = float(h["particle_radius"].max()) if P else 0.0
     model._host.update(h)
     dev = model.device
@@ -89,6 +105,10 @@ def desc(model) -> NbParticleDesc:
               "shape_flags"):
         setattr(d, k, ptr(getattr(model, k)))
     d.shape_mu = ptr(model.shape_material_mu)
+    d.edge_count = model.edge_count
+    for k in ("edge_indices", "edge_rest_angle", "edge_bending_properties", "particle_edge_start",
+              "particle_edge_list"):
+        setattr(d, k, ptr(getattr(model, k)))
     return d
 
 

@@ -417,7 +417,7 @@ def scene_falling_shapes(worlds: int = 1, device=None):
 def scene_particles(seed: int = 7, cloth: int = 12, loose: int = 200, radius: float = 0.02, device=None,
                     body_shapes: bool = False, loose_extent: float = 0.3, loose_height=(0.33, 0.7)):
     """Particles dropped onto static shapes: a square cloth of ``cloth`` x ``cloth`` particles joined by
-    structural and shear springs, and ``loose`` free particles of radius U[0.5, 1] x ``radius`` above it.
+    structural and shear springs and bent across each quad's diagonal (bending edges), and ``loose`` free particles of radius U[0.5, 1] x ``radius`` above it.
 
     Static colliders: the ground plane, a box, a sphere and a capsule under the drop (world -1).  With
     ``body_shapes`` a free box body is added whose shape does not collide with particles.  The scene
@@ -449,6 +449,10 @@ def scene_particles(seed: int = 7, cloth: int = 12, loose: int = 200, radius: fl
             for di, dj in ((1, 0), (0, 1), (1, 1), (1, -1)):
                 if (i + di, j + dj) in idx:
                     b.add_spring(idx[i, j], idx[i + di, j + dj], 1.0e3 if di * dj == 0 else 2.5e2, 0.5, 0.0)
+    # bending hinges across every quad's diagonal, flat at rest (add_edge: triangles (i, k, l), (j, l, k))
+    for i in range(cloth - 1):
+        for j in range(cloth - 1):
+            b.add_edge(idx[i + 1, j], idx[i, j + 1], idx[i, j], idx[i + 1, j + 1], edge_ke=20.0, edge_kd=0.0)
     for _ in range(loose):
         p = (rng.uniform(-loose_extent, loose_extent), rng.uniform(-loose_extent, loose_extent),
              rng.uniform(*loose_height))

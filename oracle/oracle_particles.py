@@ -12,6 +12,7 @@ kernels, which run one thread per particle):
   solve_particle_shape_contacts   newton/_src/solvers/xpbd/kernels.py:114-222
   solve_particle_particle_contacts newton/_src/solvers/xpbd/kernels.py:225-289
   solve_springs              newton/_src/solvers/xpbd/kernels.py:292-356
+  bending_constraint         newton/_src/solvers/xpbd/kernels.py:358-457
   apply_particle_deltas      newton/_src/solvers/xpbd/kernels.py:776-807
   iteration order            newton/_src/solvers/xpbd/solver_xpbd.py:303-320, 377-505
 
@@ -21,7 +22,9 @@ correctly rounded).  Where the reference scatters with atomic adds, whose
 order varies from run to run, the oracle fixes one order per particle: its
 soft contacts in list order, then its particle neighbours in ascending index
 (all j within the contact distance, found by brute force), then its springs in
-ascending index.
+ascending index, then its bending edges in ascending index.  The dihedral
+angle's atan2 is the library's: asin (the C oracle's ``orc_asin``) of the
+smaller coordinate over the radius, shifted into its quadrant.
 """
 
 from __future__ import annotations
@@ -172,6 +175,65 @@ def soft_collide(h: dict, particle_q, body_q, margin: float, soft_contact_max: i
             out["body_pos"][pi, si][:keep], out["body_vel"][pi, si][:keep], out["normal"][pi, si][:keep])
 
 
+def _asin(u):
+    import oracle
+
+    f = oracle.load().orc_asin
+    return np.asarray([f(float(x)) for x in np.asarray(u, F).reshape(-1)], F).reshape(np.shape(u))
+
+
+def atan2(y, x):
+    """Elementwise float32 atan2 as the particle kernels compute it (see the module docstring)."""
+    y, x = np.asarray(y, F), np.asarray(x, F)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.sqrt(x * x + y * y)
+        safe = np.where(r == 0, F(1), r)
+        lo = np.abs(y) <= np.abs(x)
+        a_lo = _asin(np.where(lo, y / safe, F(0)))
+        a_lo = np.where(x > 0, a_lo, np.where(y < 0, F(-3.1415927410125732) - a_lo, F(3.1415927410125732) - a_lo))
+        a_hi = F(1.5707963705062866) - _asin(np.where(lo, F(0), x / safe))
+        a_hi = np.where(y < 0, -a_hi, a_hi)
+    return np.where(r == 0, F(0), np.where(lo, a_lo, a_hi)).astype(F)
+
+
+def _bending(h, x, v, w, dt):
+    """Per-edge corrections of bending_constraint: (owner particle, correction) in edge order, roles i, j, k, l."""
+    ev = h["edge_indices"].reshape(-1, 4)
+    if ev.shape[0] == 0:
+        return [], []
+    live = (ev >= 0).all(axis=1)
+    idx = np.where(ev >= 0, ev, 0)
+    x1, x2, x3, x4 = (x[idx[:, r]] for r in range(4))
+    n1 = _cross(x3 - x1, x4 - x1)
+    n2 = _cross(x4 - x2, x3 - x2)
+    e = x4 - x3
+    n1l, n2l, el = _length(n1), _length(n2), _length(e)
+    ok = live & ~((n1l < F(1e-6)) | (n2l < F(1e-6)) | (el < F(1e-6)))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        n1h, n2h, eh = n1 / n1l[:, None], n2 / n2l[:, None], e / el[:, None]
+        theta = atan2(_dot(_cross(n1h, n2h), eh), _dot(n1h, n2h))
+        c = theta - h["edge_rest_angle"].astype(F)
+        g = [-n1h * el[:, None], -n2h * el[:, None],
+             -n1h * _dot(x1 - x4, eh)[:, None] - n2h * _dot(x2 - x4, eh)[:, None],
+             -n1h * _dot(x3 - x1, eh)[:, None] - n2h * _dot(x3 - x2, eh)[:, None]]
+        ws = [w[idx[:, r]] for r in range(4)]
+        den = ws[0] * _dot(g[0], g[0]) + ws[1] * _dot(g[1], g[1]) + ws[2] * _dot(g[2], g[2]) + ws[3] * _dot(g[3], g[3])
+        bp = h["edge_bending_properties"].reshape(-1, 2).astype(F)
+        ke, kd = bp[:, 0], bp[:, 1]
+        ok &= ~((den <= 0) | (ke <= 0) | (kd < 0))
+        alpha = F(1) / (ke * dt * dt)
+        gamma = kd / (ke * dt)
+        gdv = dt * (_dot(g[0], v[idx[:, 0]]) + _dot(g[1], v[idx[:, 1]]) + _dot(g[2], v[idx[:, 2]]) +
+                    _dot(g[3], v[idx[:, 3]]))
+        dl = F(-1) * (c + alpha * F(0) + gamma * gdv) / ((F(1) + gamma) * den + alpha)
+    owners, contribs = [], []
+    for e_i in np.nonzero(ok)[0]:
+        for r in range(4):
+            owners.append(int(idx[e_i, r]))
+            contribs.append(g[r][e_i] * (ws[r][e_i] * dl[e_i]))
+    return owners, contribs
+
+
 def _spring_csr(h):
     P = h["particle_radius"].shape[0]
     idx = h["spring_indices"].reshape(-1, 2)
@@ -294,6 +356,10 @@ def step(h: dict, params: dict, q, qd, f, soft, dt: float, iterations: int, rela
                             contribs.append(dxj[s])
                 if owners:
                     _accumulate(delta, np.asarray(owners), np.asarray(contribs, F))
+            # bending edges, ascending edge index per particle
+            owners, contribs = _bending(h, x, v, w, dt)
+            if owners:
+                _accumulate(delta, np.asarray(owners), np.asarray(contribs, F))
         # apply_particle_deltas
         xn = x + delta
         vn = (xn - x0) / dt

@@ -169,3 +169,50 @@ def test_solver_rejects_particle_contacts_with_bodies():
         SolverXPBD(_model(build))
     m, _ = scenes.scene_particles(device="cpu", cloth=3, loose=4, body_shapes=True)
     SolverXPBD(m)  # a body shape built with has_particle_collision=False is fine
+
+
+def test_atan2_matches_float64_in_every_quadrant():
+    rng = np.random.default_rng(0)
+    y = rng.normal(size=20000).astype(F)
+    x = rng.normal(size=20000).astype(F)
+    y[:8] = [0, 1, -1, 0, 1, -1, 1e-30, -1e-30]
+    x[:8] = [1, 0, 0, -1, -1, 1, -1, -1]
+    got = op.atan2(y, x).astype(np.float64)
+    ref = np.arctan2(y.astype(np.float64), x.astype(np.float64))
+    # a few float32 ulps of the angle (|angle| <= pi)
+    assert np.abs(got - ref).max() < 1e-6
+    assert op.atan2(np.float32(0), np.float32(0)) == 0
+
+
+def test_bending_hinge_rest_angle_and_relaxation():
+    """Two triangles folded 90 degrees about the x axis: the builder's rest angle of the flat hinge is 0;
+    the bending constraint (kernels.py:358-457) unfolds the hinge toward it."""
+
+    def build(b):
+        b.add_particle((0.0, 0.0, 0.0), (0, 0, 0), 1.0, radius=0.01)   # k
+        b.add_particle((1.0, 0.0, 0.0), (0, 0, 0), 1.0, radius=0.01)   # l
+        b.add_particle((0.5, -0.5, 0.0), (0, 0, 0), 1.0, radius=0.01)  # i
+        b.add_particle((0.5, 0.5, 0.0), (0, 0, 0), 1.0, radius=0.01)   # j
+        b.add_edge(2, 3, 0, 1, edge_ke=50.0, edge_kd=0.0)
+
+    m = _model(build)
+    assert m.host("edge_rest_angle")[0] == pytest.approx(0.0, abs=1e-7)
+    np.testing.assert_array_equal(m.host("particle_edge_start"), [0, 1, 2, 3, 4])
+    m._host["gravity"] = np.zeros((1, 3), F)
+    q = m.host("particle_q").copy()
+    q[3] = (0.5, 0.0, 0.5)  # fold j up by 90 degrees
+    qd = m.host("particle_qd")
+
+    def angle(q):
+        n1 = np.cross(q[0] - q[2], q[1] - q[2])
+        n2 = np.cross(q[1] - q[3], q[0] - q[3])
+        e = (q[1] - q[0]) / np.linalg.norm(q[1] - q[0])
+        n1, n2 = n1 / np.linalg.norm(n1), n2 / np.linalg.norm(n2)
+        return float(np.arctan2(np.dot(np.cross(n1, n2), e), np.dot(n1, n2)))
+
+    a0 = angle(q)
+    assert abs(abs(a0) - np.pi / 2) < 1e-5
+    for _ in range(40):
+        q, qd = _step(m, q, qd, dt=1.0 / 240.0, iterations=8)
+    assert abs(angle(q)) < 0.5 * abs(a0)
+    assert abs(float(qd.sum(axis=0)[2])) < 1e-3  # internal constraint: no net momentum
