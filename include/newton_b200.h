@@ -613,7 +613,7 @@ typedef struct NbParticleDesc {
     const int32_t* shape_flags;       /* [Sh]  bit 2 = COLLIDE_PARTICLES */
     const float* shape_mu;            /* [Sh]  */
     int32_t edge_count;               /* bending edges */
-    int32_t pad_e;
+    float soft_contact_restitution;   /* Model.soft_contact_restitution */
     const int32_t* edge_indices;      /* [E,4] (i, j, k, l): opposite vertices i, j of the hinge edge k-l */
     const float* edge_rest_angle;     /* [E]   */
     const float* edge_bending_properties; /* [E,2] (ke, kd) */
@@ -648,7 +648,7 @@ typedef struct NbParticleIO {
     int32_t* grid_head;        /* [2*grid_size] scratch: two hashed cell tables (first particle, -1 empty) */
     int32_t* grid_next;        /* [P] scratch: next particle of the same cell */
     int32_t grid_size;         /* cells per table, a power of two */
-    int32_t pad;
+    int32_t enable_restitution; /* 1: apply_particle_shape_restitution (kernels.py:34-112) after the iterations */
     uint32_t* status;          /* [1] NB_STATUS_* bits (sticky, cleared by the caller) */
 } NbParticleIO;
 
@@ -680,7 +680,10 @@ int nb_soft_collide(const NbParticleDesc* pd, const float* particle_q, const flo
  * instead of the reference's atomic adds, so results do not change from run
  * to run.  sc may be NULL (no soft contacts); sc->particle_start must come
  * from nb_soft_collide on the same contacts.  Soft contacts with a
- * body-attached shape are skipped (NB_STATUS_PARTICLE_BODY_CONTACT).
+ * body-attached shape are skipped (NB_STATUS_PARTICLE_BODY_CONTACT).  With
+ * io->enable_restitution, every particle then adds the restitution velocity
+ * change of each of its soft contacts, in list order, all computed from its
+ * velocity after the iterations.
  */
 int nb_particle_step(const NbParticleDesc* pd, const NbParticleIO* io, const NbSoftContacts* sc, float dt,
                      int32_t iterations, float relaxation, void* stream);

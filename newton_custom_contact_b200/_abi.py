@@ -267,7 +267,7 @@ class NbParticleDesc(C.Structure):
                             "particle_spring_start", "particle_spring_list", "shape_body", "shape_type",
                             "shape_transform", "shape_scale", "shape_world", "shape_flags", "shape_mu")] + [
         ("edge_count", C.c_int32),
-        ("pad_e", C.c_int32),
+        ("soft_contact_restitution", C.c_float),
     ] + [(k, _fp) for k in ("edge_indices", "edge_rest_angle", "edge_bending_properties", "particle_edge_start",
                             "particle_edge_list")]
 
@@ -284,7 +284,7 @@ class NbParticleIO(C.Structure):
     _fields_ = [(k, _fp) for k in ("particle_q", "particle_qd", "particle_f", "particle_q_out", "particle_qd_out",
                                    "delta", "grid_head", "grid_next")] + [
         ("grid_size", C.c_int32),
-        ("pad", C.c_int32),
+        ("enable_restitution", C.c_int32),
         ("status", _fp),
     ]
 

@@ -513,6 +513,38 @@ __global__ void __launch_bounds__(kThreads) particle_apply_kernel(NbParticleDesc
     if (insert) grid_insert(g, next_table, p, x_new);
 }
 
+// apply_particle_shape_restitution (kernels.py:34-112) for static shapes: contacts tested at the
+// substep's start position; each particle adds the velocity change of its contacts, in list order, to
+// its velocity after the iterations (every change computed from that velocity).
+__global__ void __launch_bounds__(kThreads) particle_restitution_kernel(NbParticleDesc pd, NbParticleIO io,
+                                                                        NbSoftContacts sc) {
+    const int p = blockIdx.x * kThreads + threadIdx.x;
+    if (p >= pd.particle_count || !active(pd, p)) return;
+    const int lim = min(sc.max, sc.count[0]);
+    const int lo = sc.particle_start[p], hi = min(sc.particle_start[p + 1], lim);
+    if (lo >= hi) return;
+    const V3 v_new = ld3(io.particle_qd_out, p);
+    const V3 px = ld3(io.particle_q, p);
+    const V3 v_old = ld3(io.particle_qd, p);
+    V3 v_out = v_new;
+    for (int k = lo; k < hi; ++k) {
+        if (pd.shape_body[sc.shape[k]] >= 0) continue;  // body-attached shapes: not coupled
+        const TF X_wb = tf_identity(), X_wb_prev = tf_identity();
+        const V3 bx = tf_point(X_wb, ld3(sc.body_pos, k));
+        const V3 n = ld3(sc.normal, k);
+        const float c = dot(n, sub(px, bx)) - pd.particle_radius[p];
+        if (c > pd.particle_adhesion) continue;
+        const V3 bv_contact = tf_vector(X_wb_prev, ld3(sc.body_vel, k));
+        const float rel_vel_old = dot(n, sub(v_old, bv_contact));
+        const float rel_vel_new = dot(n, sub(v_new, bv_contact));
+        if (rel_vel_old < 0.0f) {
+            const V3 dv = mul(n, -rel_vel_new + fmaxw(-pd.soft_contact_restitution * rel_vel_old, 0.0f));
+            v_out = add(v_out, dv);
+        }
+    }
+    st3(io.particle_qd_out, p, v_out);
+}
+
 bool check_pd(const NbParticleDesc* pd) {
     if (!pd || pd->particle_count < 0 || pd->spring_count < 0 || pd->shape_count < 0 || pd->world_count < 1)
         return false;
@@ -593,6 +625,8 @@ int nb_particle_step(const NbParticleDesc* pd, const NbParticleIO* io, const NbS
         particle_apply_kernel<<<blocks, kThreads, 0, st>>>(*pd, *io, dt, g, table ^ 1,
                                                            g.on && it + 1 < iterations ? 1 : 0);
     }
+    if (io->enable_restitution && has_sc)
+        particle_restitution_kernel<<<blocks, kThreads, 0, st>>>(*pd, *io, scv);
     return nb_cuda_rc(cudaGetLastError());
 }
 

@@ -13,8 +13,8 @@ The particle branch of the reference's pipeline, on the library's kernels
 
 Particles collide with each other and with STATIC shapes: the solver raises
 for a model where a particle-colliding shape is attached to a body (the
-two-way particle-body coupling is not built).  Bending edges are built;
-triangles, tetrahedra and particle restitution are not.
+two-way particle-body coupling is not built).  Bending edges and particle
+restitution are built; triangles and tetrahedra are not.
 """
 
 from __future__ import annotations
@@ -38,6 +38,7 @@ def attach(model, b) -> None:
     model.particle_cohesion = 0.0
     model.particle_adhesion = 0.0
     model.soft_contact_mu = 0.5
+    model.soft_contact_restitution = 0.0
     f32 = np.float32
     h = {}
     h["particle_q"] = np.asarray(b.particle_q, dtype=f32).reshape(P, 3)
@@ -88,7 +89,8 @@ def attach(model, b) -> None:
 def params(model) -> dict:
     """The model's particle scalars (the oracle reads the same dict)."""
     return {k: float(getattr(model, k)) for k in ("particle_max_velocity", "particle_max_radius", "particle_mu",
-                                                  "particle_cohesion", "particle_adhesion", "soft_contact_mu")}
+                                                  "particle_cohesion", "particle_adhesion", "soft_contact_mu",
+                                                  "soft_contact_restitution")}
 
 
 def desc(model) -> NbParticleDesc:
@@ -160,8 +162,6 @@ class ParticleSolver:
                 f"particle contacts with body-attached shapes (e.g. shape {int(coupled[0])}) are not supported: "
                 "this build couples particles to static shapes only; build those shapes with "
                 "has_particle_collision=False")
-        if solver.enable_restitution:
-            raise NotImplementedError("particle restitution is not supported")
         self.model = model
         self.solver = solver
         P = model.particle_count
@@ -190,6 +190,7 @@ class ParticleSolver:
         io.grid_head = ptr(self.grid_head)
         io.grid_next = ptr(self.grid_next)
         io.grid_size = self.grid_size
+        io.enable_restitution = int(bool(self.solver.enable_restitution))
         io.status = ptr(self.status_word)
         sc = None
         if contacts is not None and contacts.soft_contact_max > 0 and getattr(contacts, "_soft_valid", False):

@@ -14,6 +14,7 @@ kernels, which run one thread per particle):
   solve_springs              newton/_src/solvers/xpbd/kernels.py:292-356
   bending_constraint         newton/_src/solvers/xpbd/kernels.py:358-457
   apply_particle_deltas      newton/_src/solvers/xpbd/kernels.py:776-807
+  apply_particle_shape_restitution newton/_src/solvers/xpbd/kernels.py:34-112 (static shapes)
   iteration order            newton/_src/solvers/xpbd/solver_xpbd.py:303-320, 377-505
 
 Every float operation is a float32 numpy operation in the order the
@@ -257,7 +258,8 @@ def _accumulate(delta, owner, contrib):
         delta[owner[m]] = delta[owner[m]] + contrib[m]
 
 
-def step(h: dict, params: dict, q, qd, f, soft, dt: float, iterations: int, relaxation: float):
+def step(h: dict, params: dict, q, qd, f, soft, dt: float, iterations: int, relaxation: float,
+         restitution: bool = False):
     """One particle substep; returns (q_out, qd_out).  ``soft`` is soft_collide's tuple or None."""
     dt, relax = F(dt), F(relaxation)
     x0 = np.asarray(q, F).reshape(-1, 3)
@@ -368,4 +370,16 @@ def step(h: dict, params: dict, q, qd, f, soft, dt: float, iterations: int, rela
             vn = np.where((mag > vmax)[:, None], vn * (vmax / mag)[:, None], vn)
         x = np.where(act[:, None], xn, x)
         v = np.where(act[:, None], vn, v)
+    if restitution and soft is not None and soft[0] > 0:
+        # velocity change of every soft contact, tested at the substep's start position and computed from
+        # the velocity after the iterations, added per particle in list order
+        cnt, cp, cs, bpos, bvel, cn = soft
+        ok = act[cp] & (h["shape_body"][cs] < 0)
+        c = _dot(cn, x0[cp] - (bpos + np.zeros(3, F))) - radius[cp]
+        ok &= ~(c > F(params["particle_adhesion"]))
+        rvo = _dot(cn, v0[cp] - bvel)
+        rvn = _dot(cn, v[cp] - bvel)
+        ok &= rvo < 0
+        dv = cn * (-rvn + _max(-F(params["soft_contact_restitution"]) * rvo, F(0)))[:, None]
+        _accumulate(v, cp[ok], dv[ok])
     return x, v

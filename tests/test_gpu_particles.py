@@ -24,9 +24,9 @@ def _bits(a):
     return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
 
 
-def _gpu_run(model, substeps, q0=None, qd0=None, record=None):
+def _gpu_run(model, substeps, q0=None, qd0=None, record=None, restitution=False):
     pipe = CollisionPipeline(model)
-    solver = SolverXPBD(model, iterations=ITERS, soft_contact_relaxation=0.9)
+    solver = SolverXPBD(model, iterations=ITERS, soft_contact_relaxation=0.9, enable_restitution=restitution)
     s0, s1 = model.state(), model.state()
     if q0 is not None:
         s0.particle_q.copy_(torch.from_numpy(q0))
@@ -49,9 +49,9 @@ def _gpu_run(model, substeps, q0=None, qd0=None, record=None):
     return s0, solver, pipe
 
 
-def _oracle_substep(model, q, qd, margin, smax):
+def _oracle_substep(model, q, qd, margin, smax, restitution=False):
     soft = op.soft_collide(model._host, q, None, margin, smax)
-    q, qd = op.step(model._host, particles.params(model), q, qd, None, soft, DT, ITERS, 0.9)
+    q, qd = op.step(model._host, particles.params(model), q, qd, None, soft, DT, ITERS, 0.9, restitution)
     return soft, q, qd
 
 
@@ -141,3 +141,19 @@ def test_large_particle_drop_stays_above_the_ground(cuda):
     active = (model.host("particle_flags") & 1) != 0
     assert float((q[active, 2] - r[active]).min()) > -1e-2
     assert solver._particles.status() == 0
+
+
+def test_particle_restitution_bit_exact(cuda):
+    """enable_restitution with soft_contact_restitution 0.6: apply_particle_shape_restitution after the
+    iterations, bit for bit over 24 substeps from a landing state."""
+    model, q0, qd0 = _prerolled(cuda, steps=30)
+    model.soft_contact_restitution = 0.6
+    s, solver, pipe = _gpu_run(model, 24, q0, qd0, restitution=True)
+    q, qd = q0.copy(), qd0.copy()
+    for _ in range(24):
+        _, q, qd = _oracle_substep(model, q, qd, pipe.soft_contact_margin, pipe.soft_contact_max, True)
+    assert np.array_equal(_bits(s.particle_q.cpu().numpy()), _bits(q))
+    assert np.array_equal(_bits(s.particle_qd.cpu().numpy()), _bits(qd))
+    # restitution changed the trajectory
+    s2, _, _ = _gpu_run(model, 24, q0, qd0, restitution=False)
+    assert not torch.equal(s.particle_qd, s2.particle_qd)

@@ -216,3 +216,24 @@ def test_bending_hinge_rest_angle_and_relaxation():
         q, qd = _step(m, q, qd, dt=1.0 / 240.0, iterations=8)
     assert abs(angle(q)) < 0.5 * abs(a0)
     assert abs(float(qd.sum(axis=0)[2])) < 1e-3  # internal constraint: no net momentum
+
+
+def test_restitution_bounce_off_the_ground():
+    """apply_particle_shape_restitution (kernels.py:34-112): a particle hitting the plane leaves it with
+    the restitution coefficient times its approach speed."""
+    r = 0.02
+
+    def build(b):
+        b.add_ground_plane()
+        b.add_particle((0.0, 0.0, r - 0.0005), (0.0, 0.0, -2.0), 0.05, radius=r)  # touching at the start
+
+    m = _model(build)
+    m.soft_contact_restitution = 0.5
+    m._host["gravity"] = np.zeros((1, 3), F)
+    q, qd = m.host("particle_q"), m.host("particle_qd")
+    dt = 1.0 / 240.0
+    soft = op.soft_collide(m._host, q, None, 0.01, 8)
+    q1, qd1 = op.step(m._host, particles.params(m), q, qd, None, soft, dt, 4, 0.9, restitution=True)
+    assert qd1[0, 2] == pytest.approx(1.0, rel=1e-5)  # 0.5 x 2 m/s, upwards
+    _, qd0 = op.step(m._host, particles.params(m), q, qd, None, soft, dt, 4, 0.9, restitution=False)
+    assert qd0[0, 2] < 0.5  # without restitution it leaves at the projection speed only
