@@ -619,6 +619,12 @@ typedef struct NbParticleDesc {
     const float* edge_bending_properties; /* [E,2] (ke, kd) */
     const int32_t* particle_edge_start;   /* [P+1] edges of particle p: particle_edge_list[start[p]..start[p+1]) */
     const int32_t* particle_edge_list;    /* edge indices, ascending per particle */
+    int32_t tet_count;                /* tetrahedra */
+    float soft_body_relaxation;       /* SolverXPBD.soft_body_relaxation: the tetrahedra's compliance */
+    const int32_t* tet_indices;       /* [T,4] */
+    const float* tet_poses;           /* [T,9] inverse rest matrices (row-major mat33) */
+    const int32_t* particle_tet_start;    /* [P+1] tetrahedra of particle p: particle_tet_list[start[p]..start[p+1]) */
+    const int32_t* particle_tet_list;     /* tetrahedron indices, ascending per particle */
 } NbParticleDesc;
 
 /* Soft contacts (newton/_src/sim/contacts.py soft_contact_* arrays), in
@@ -673,7 +679,8 @@ int nb_soft_collide(const NbParticleDesc* pd, const float* particle_q, const flo
  * (kernels.py:225-289), springs (kernels.py:292-356), bending edges
  * (bending_constraint, kernels.py:358-457; the dihedral angle through an
  * atan2 built on the library's own asin, so that the oracle can match it bit
- * for bit) and apply_particle_deltas (kernels.py:776-807).  Each particle gathers its
+ * for bit), tetrahedra (solve_tetrahedra, kernels.py:459-628) and
+ * apply_particle_deltas (kernels.py:776-807).  Each particle gathers its
  * corrections in a fixed order (its soft contacts, then its particle
  * neighbours in ascending index, then its springs, then its bending edges,
  * each in ascending index)

@@ -269,7 +269,10 @@ class NbParticleDesc(C.Structure):
         ("edge_count", C.c_int32),
         ("soft_contact_restitution", C.c_float),
     ] + [(k, _fp) for k in ("edge_indices", "edge_rest_angle", "edge_bending_properties", "particle_edge_start",
-                            "particle_edge_list")]
+                            "particle_edge_list")] + [
+        ("tet_count", C.c_int32),
+        ("soft_body_relaxation", C.c_float),
+    ] + [(k, _fp) for k in ("tet_indices", "tet_poses", "particle_tet_start", "particle_tet_list")]
 
 
 class NbSoftContacts(C.Structure):

@@ -282,6 +282,11 @@ class ModelBuilder:
         self.edge_rest_angle: list[float] = []
         self.edge_rest_length: list[float] = []
         self.edge_bending_properties: list[tuple[float, float]] = []
+        # tetrahedra (builder.py:7522-7587)
+        self.tet_indices: list[tuple[int, int, int, int]] = []
+        self.tet_poses: list[list] = []
+        self.tet_activations: list[float] = []
+        self.tet_materials: list[tuple[float, float, float]] = []
         self._requested_contact_attributes: set[str] = set()
         self._requested_state_attributes: set[str] = set()
 
@@ -309,6 +314,10 @@ class ModelBuilder:
     @property
     def spring_count(self) -> int:
         return len(self.spring_rest_length)
+
+    @property
+    def tet_count(self) -> int:
+        return len(self.tet_indices)
 
     @property
     def edge_count(self) -> int:
@@ -370,6 +379,10 @@ class ModelBuilder:
         self.edge_rest_angle.extend(builder.edge_rest_angle)
         self.edge_rest_length.extend(builder.edge_rest_length)
         self.edge_bending_properties.extend(builder.edge_bending_properties)
+        self.tet_indices.extend(tuple(int(v) + p_off for v in t) for t in builder.tet_indices)
+        self.tet_poses.extend(builder.tet_poses)
+        self.tet_activations.extend(builder.tet_activations)
+        self.tet_materials.extend(builder.tet_materials)
         b_off = self.body_count
         s_off = self.shape_count
         j_off = self.joint_count
@@ -722,6 +735,24 @@ class ModelBuilder:
         self.edge_rest_length.append(float(np.linalg.norm(x4 - x3)))
         self.edge_bending_properties.append((float(edge_ke), float(edge_kd)))
         return len(self.edge_indices) - 1
+
+    def add_tetrahedron(self, i: int, j: int, k: int, l: int, k_mu: float = 1.0e3, k_lambda: float = 1.0e3,
+                        k_damp: float = 0.0, custom_attributes=None) -> float:
+        """Tetrahedral element (builder.py:7522-7587): its inverse rest matrix from the particles' current
+        positions; returns the rest volume (an inverted element is reported and not added)."""
+        if custom_attributes:
+            raise NotImplementedError("custom attributes are not supported")
+        p, q, r, s = (np.array(self.particle_q[x]) for x in (i, j, k, l))
+        Dm = np.array((q - p, r - p, s - p)).T
+        volume = np.linalg.det(Dm) / 6.0
+        if volume <= 0.0:
+            print("inverted tetrahedral element")
+        else:
+            self.tet_indices.append((int(i), int(j), int(k), int(l)))
+            self.tet_poses.append(np.linalg.inv(Dm).tolist())
+            self.tet_activations.append(0.0)
+            self.tet_materials.append((float(k_mu), float(k_lambda), float(k_damp)))
+        return volume
 
     def request_state_attributes(self, *attributes: str) -> None:
         bad = sorted(set(attributes) - {"body_parent_f"})

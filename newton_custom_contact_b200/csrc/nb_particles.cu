@@ -447,14 +447,85 @@ __global__ void __launch_bounds__(kThreads) particle_constraints_kernel(NbPartic
     st3(io.delta, i, delta);
 }
 
-// Bending edges (bending_constraint, kernels.py:358-457) of one particle, added to its delta after the
-// constraint kernel's terms (the same order as one sequential sum); a kernel of its own so that the
-// constraint kernel keeps its register budget.  The solver zeroes the multipliers every iteration.
+NB_D float det3(const M33& m) {
+    return m.m[0][0] * (m.m[1][1] * m.m[2][2] - m.m[1][2] * m.m[2][1]) -
+           m.m[0][1] * (m.m[1][0] * m.m[2][2] - m.m[1][2] * m.m[2][0]) +
+           m.m[0][2] * (m.m[1][0] * m.m[2][1] - m.m[1][1] * m.m[2][0]);
+}
+NB_D M33 matmul3(const M33& a, const M33& b) {
+    M33 r;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) r.m[i][j] = a.m[i][0] * b.m[0][j] + a.m[i][1] * b.m[1][j] + a.m[i][2] * b.m[2][j];
+    return r;
+}
+NB_D M33 from_cols(V3 a, V3 b, V3 c) {
+    M33 r;
+    r.m[0][0] = a.x; r.m[1][0] = a.y; r.m[2][0] = a.z;
+    r.m[0][1] = b.x; r.m[1][1] = b.y; r.m[2][1] = b.z;
+    r.m[0][2] = c.x; r.m[1][2] = c.y; r.m[2][2] = c.z;
+    return r;
+}
+NB_D V3 col(const M33& m, int c) { return V3{m.m[0][c], m.m[1][c], m.m[2][c]}; }
+
+// Tetrahedra of one particle (solve_tetrahedra, kernels.py:459-628): per element a stretch term
+// (trace(F^T F) - 3) and a volume term (det F - 1), each a compliant constraint with compliance
+// `relaxation` (the solver's soft_body_relaxation) scaled by the inverse rest volume.
+NB_D V3 tet_terms(const NbParticleDesc& pd, const float* xq, int i, int t, float dt, V3 delta) {
+    const int* ix = pd.tet_indices + 4 * t;
+    const V3 x0 = ld3(xq, ix[0]), x1 = ld3(xq, ix[1]), x2 = ld3(xq, ix[2]), x3 = ld3(xq, ix[3]);
+    const float w[4] = {pd.particle_inv_mass[ix[0]], pd.particle_inv_mass[ix[1]], pd.particle_inv_mass[ix[2]],
+                        pd.particle_inv_mass[ix[3]]};
+    const M33 Ds = from_cols(sub(x1, x0), sub(x2, x0), sub(x3, x0));
+    M33 Dm, inv_QT;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) Dm.m[r][c] = pd.tet_poses[9 * t + 3 * r + c];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) inv_QT.m[r][c] = Dm.m[c][r];
+    const float inv_rest_volume = det3(Dm) * 6.0f;
+    const M33 Fm = matmul3(Ds, Dm);
+    const V3 f1 = col(Fm, 0), f2 = col(Fm, 1), f3 = col(Fm, 2);
+    const float tr = dot(f1, f1) + dot(f2, f2) + dot(f3, f3);
+    for (int term = 0; term < 2; ++term) {
+        float C;
+        M33 dC;
+        if (term == 0) {
+            C = tr - 3.0f;
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) dC.m[r][c] = Fm.m[r][c] * 2.0f;
+        } else {
+            C = det3(Fm) - 1.0f;
+            dC = from_cols(cross(f2, f3), cross(f3, f1), cross(f1, f2));
+        }
+        if (C == 0.0f) continue;
+        const M33 dP = matmul3(dC, inv_QT);
+        V3 grad[4];
+        grad[1] = col(dP, 0);
+        grad[2] = col(dP, 1);
+        grad[3] = col(dP, 2);
+        grad[0] = sub(sub(neg(grad[1]), grad[2]), grad[3]);
+        const float wsum = dot(grad[0], grad[0]) * w[0] + dot(grad[1], grad[1]) * w[1] +
+                           dot(grad[2], grad[2]) * w[2] + dot(grad[3], grad[3]) * w[3];
+        if (!(wsum > 0.0f)) continue;
+        float alpha = pd.soft_body_relaxation / dt / dt;
+        if (inv_rest_volume > 0.0f) alpha *= inv_rest_volume;
+        const float dlambda = -C / (wsum + alpha);
+        for (int r = 0; r < 4; ++r)
+            if (ix[r] == i) delta = add(delta, mul(grad[r], w[r] * dlambda));
+    }
+    return delta;
+}
+
+// Bending edges (bending_constraint, kernels.py:358-457), then tetrahedra, of one particle, added to its
+// delta after the constraint kernel's terms (the same order as one sequential sum); a kernel of its own
+// so that the constraint kernel keeps its register budget.  The solver zeroes the multipliers every iteration.
 __global__ void __launch_bounds__(kThreads) particle_bending_kernel(NbParticleDesc pd, NbParticleIO io, float dt) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     if (i >= pd.particle_count) return;
-    const int e_lo = pd.particle_edge_start[i], e_hi = pd.particle_edge_start[i + 1];
-    if (e_lo == e_hi) return;
+    const int e_lo = pd.edge_count > 0 ? pd.particle_edge_start[i] : 0;
+    const int e_hi = pd.edge_count > 0 ? pd.particle_edge_start[i + 1] : 0;
+    const int t_lo = pd.tet_count > 0 ? pd.particle_tet_start[i] : 0;
+    const int t_hi = pd.tet_count > 0 ? pd.particle_tet_start[i + 1] : 0;
+    if (e_lo == e_hi && t_lo == t_hi) return;
     const float* xq = io.particle_q_out;
     const float* vq = io.particle_qd_out;
     V3 delta = ld3(io.delta, i);
@@ -494,6 +565,7 @@ __global__ void __launch_bounds__(kThreads) particle_bending_kernel(NbParticleDe
                 if (ix[r] == i) delta = add(delta, mul(grad[r], w[r] * dlambda));
         }
     }
+    for (int k = t_lo; k < t_hi; ++k) delta = tet_terms(pd, xq, i, pd.particle_tet_list[k], dt, delta);
     st3(io.delta, i, delta);
 }
 
@@ -554,6 +626,9 @@ bool check_pd(const NbParticleDesc* pd) {
         return false;
     if (pd->spring_count > 0 && (!pd->spring_indices || !pd->spring_rest_length || !pd->spring_stiffness ||
                                  !pd->spring_damping || !pd->particle_spring_start || !pd->particle_spring_list))
+        return false;
+    if (pd->tet_count < 0 || (pd->tet_count > 0 && (!pd->tet_indices || !pd->tet_poses || !pd->particle_tet_start ||
+                                                     !pd->particle_tet_list)))
         return false;
     if (pd->edge_count < 0 || (pd->edge_count > 0 && (!pd->edge_indices || !pd->edge_rest_angle ||
                                                        !pd->edge_bending_properties || !pd->particle_edge_start ||
@@ -621,7 +696,8 @@ int nb_particle_step(const NbParticleDesc* pd, const NbParticleIO* io, const NbS
         const int table = it & 1;
         particle_constraints_kernel<<<con_blocks, kThreads, 0, st>>>(*pd, *io, scv, has_sc, dt, relaxation, g,
                                                                      table);
-        if (pd->edge_count > 0) particle_bending_kernel<<<blocks, kThreads, 0, st>>>(*pd, *io, dt);
+        if (pd->edge_count > 0 || pd->tet_count > 0)
+            particle_bending_kernel<<<blocks, kThreads, 0, st>>>(*pd, *io, dt);
         particle_apply_kernel<<<blocks, kThreads, 0, st>>>(*pd, *io, dt, g, table ^ 1,
                                                            g.on && it + 1 < iterations ? 1 : 0);
     }

@@ -93,6 +93,7 @@ class Model:
         self.particle_count = 0
         self.spring_count = 0
         self.edge_count = 0
+        self.tet_count = 0
         self.particle_max_radius = 0.0
         self._collision_pipeline = None
         self._requested_contact_attributes: set[str] = set()

@@ -13,8 +13,8 @@ The particle branch of the reference's pipeline, on the library's kernels
 
 Particles collide with each other and with STATIC shapes: the solver raises
 for a model where a particle-colliding shape is attached to a body (the
-two-way particle-body coupling is not built).  Bending edges and particle
-restitution are built; triangles and tetrahedra are not.
+two-way particle-body coupling is not built).  Bending edges, tetrahedra
+and particle restitution are built.
 """
 
 from __future__ import annotations
@@ -79,6 +79,19 @@ def attach(model, b) -> None:
     estart = np.zeros(P + 1, dtype=np.int32)
     np.cumsum(np.bincount(pairs[:, 0], minlength=P), out=estart[1:])
     h["particle_edge_start"] = estart
+    T = b.tet_count
+    model.tet_count = T
+    h["tet_indices"] = np.asarray(b.tet_indices, dtype=np.int32).reshape(T, 4)
+    h["tet_poses"] = np.asarray(b.tet_poses, dtype=f32).reshape(T, 9)
+    h["tet_activations"] = np.asarray(b.tet_activations, dtype=f32).reshape(T)
+    h["tet_materials"] = np.asarray(b.tet_materials, dtype=f32).reshape(T, 3)
+    tv = h["tet_indices"]
+    tpairs = (np.unique(np.stack([tv.reshape(-1).astype(np.int64), np.repeat(np.arange(T), 4)], axis=1), axis=0)
+              if T else np.zeros((0, 2), np.int64))
+    h["particle_tet_list"] = tpairs[:, 1].astype(np.int32)
+    tstart = np.zeros(P + 1, dtype=np.int32)
+    np.cumsum(np.bincount(tpairs[:, 0], minlength=P), out=tstart[1:])
+    h["particle_tet_start"] = tstart
     model.particle_max_radius = float(h["particle_radius"].max()) if P else 0.0
     model._host.update(h)
     dev = model.device
@@ -107,6 +120,9 @@ def desc(model) -> NbParticleDesc:
               "shape_flags"):
         setattr(d, k, ptr(getattr(model, k)))
     d.shape_mu = ptr(model.shape_material_mu)
+    d.tet_count = model.tet_count
+    for k in ("tet_indices", "tet_poses", "particle_tet_start", "particle_tet_list"):
+        setattr(d, k, ptr(getattr(model, k)))
     d.edge_count = model.edge_count
     for k in ("edge_indices", "edge_rest_angle", "edge_bending_properties", "particle_edge_start",
               "particle_edge_list"):
@@ -196,6 +212,7 @@ class ParticleSolver:
         if contacts is not None and contacts.soft_contact_max > 0 and getattr(contacts, "_soft_valid", False):
             sc = soft_struct(contacts, P)
         d = desc(model)
+        d.soft_body_relaxation = float(self.solver.soft_body_relaxation)
         lib = _lib.load()
         _lib.check("nb_particle_step", lib.nb_particle_step(
             C.byref(d), C.byref(io), C.byref(sc) if sc is not None else None, float(dt),

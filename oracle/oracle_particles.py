@@ -13,6 +13,7 @@ kernels, which run one thread per particle):
   solve_particle_particle_contacts newton/_src/solvers/xpbd/kernels.py:225-289
   solve_springs              newton/_src/solvers/xpbd/kernels.py:292-356
   bending_constraint         newton/_src/solvers/xpbd/kernels.py:358-457
+  solve_tetrahedra           newton/_src/solvers/xpbd/kernels.py:459-628
   apply_particle_deltas      newton/_src/solvers/xpbd/kernels.py:776-807
   apply_particle_shape_restitution newton/_src/solvers/xpbd/kernels.py:34-112 (static shapes)
   iteration order            newton/_src/solvers/xpbd/solver_xpbd.py:303-320, 377-505
@@ -235,6 +236,61 @@ def _bending(h, x, v, w, dt):
     return owners, contribs
 
 
+def _det3(m):
+    return (m[..., 0, 0] * (m[..., 1, 1] * m[..., 2, 2] - m[..., 1, 2] * m[..., 2, 1]) -
+            m[..., 0, 1] * (m[..., 1, 0] * m[..., 2, 2] - m[..., 1, 2] * m[..., 2, 0]) +
+            m[..., 0, 2] * (m[..., 1, 0] * m[..., 2, 1] - m[..., 1, 1] * m[..., 2, 0]))
+
+
+def _matmul3(a, b):
+    """Row-by-column products summed k = 0, 1, 2 in order (no BLAS, whose summation order is its own)."""
+    out = np.empty(np.broadcast_shapes(a.shape, b.shape), F)
+    for i in range(3):
+        for j in range(3):
+            out[..., i, j] = a[..., i, 0] * b[..., 0, j] + a[..., i, 1] * b[..., 1, j] + a[..., i, 2] * b[..., 2, j]
+    return out
+
+
+def _tets(h, x, w, dt, relax):
+    """Corrections of solve_tetrahedra: (owner, correction) in tet order, stretch then volume term, roles."""
+    tv = h["tet_indices"].reshape(-1, 4)
+    if tv.shape[0] == 0:
+        return [], []
+    X = [x[tv[:, r]] for r in range(4)]
+    ws = [w[tv[:, r]] for r in range(4)]
+    Ds = np.stack([X[1] - X[0], X[2] - X[0], X[3] - X[0]], axis=-1)  # columns
+    Dm = h["tet_poses"].reshape(-1, 3, 3).astype(F)
+    inv_QT = np.swapaxes(Dm, -1, -2)
+    inv_rest_volume = _det3(Dm) * F(6)
+    Fm = _matmul3(Ds, Dm)
+    f1, f2, f3 = Fm[..., :, 0], Fm[..., :, 1], Fm[..., :, 2]
+    tr = _dot(f1, f1) + _dot(f2, f2) + _dot(f3, f3)
+    terms = [(tr - F(3), Fm * F(2)),
+             (_det3(Fm) - F(1), np.stack([_cross(f2, f3), _cross(f3, f1), _cross(f1, f2)], axis=-1))]
+    alpha = F(relax) / dt / dt
+    alpha = np.where(inv_rest_volume > 0, alpha * inv_rest_volume, alpha)
+    per_term = []
+    for C, dC in terms:
+        dP = _matmul3(dC, inv_QT)
+        g1, g2, g3 = dP[..., :, 0], dP[..., :, 1], dP[..., :, 2]
+        g0 = -g1 - g2 - g3
+        g = [g0, g1, g2, g3]
+        wsum = _dot(g0, g0) * ws[0] + _dot(g1, g1) * ws[1] + _dot(g2, g2) * ws[2] + _dot(g3, g3) * ws[3]
+        ok = (C != 0) & (wsum > 0)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            dl = -C / (wsum + alpha)
+        per_term.append((ok, g, dl))
+    owners, contribs = [], []
+    for t in range(tv.shape[0]):
+        for ok, g, dl in per_term:
+            if not ok[t]:
+                continue
+            for r in range(4):
+                owners.append(int(tv[t, r]))
+                contribs.append(g[r][t] * (ws[r][t] * dl[t]))
+    return owners, contribs
+
+
 def _spring_csr(h):
     P = h["particle_radius"].shape[0]
     idx = h["spring_indices"].reshape(-1, 2)
@@ -259,7 +315,7 @@ def _accumulate(delta, owner, contrib):
 
 
 def step(h: dict, params: dict, q, qd, f, soft, dt: float, iterations: int, relaxation: float,
-         restitution: bool = False):
+         restitution: bool = False, soft_body_relaxation: float = 0.9):
     """One particle substep; returns (q_out, qd_out).  ``soft`` is soft_collide's tuple or None."""
     dt, relax = F(dt), F(relaxation)
     x0 = np.asarray(q, F).reshape(-1, 3)
@@ -362,6 +418,11 @@ def step(h: dict, params: dict, q, qd, f, soft, dt: float, iterations: int, rela
             owners, contribs = _bending(h, x, v, w, dt)
             if owners:
                 _accumulate(delta, np.asarray(owners), np.asarray(contribs, F))
+            # tetrahedra, ascending per particle
+            if "tet_indices" in h:
+                owners, contribs = _tets(h, x, w, dt, soft_body_relaxation)
+                if owners:
+                    _accumulate(delta, np.asarray(owners), np.asarray(contribs, F))
         # apply_particle_deltas
         xn = x + delta
         vn = (xn - x0) / dt

@@ -157,3 +157,41 @@ def test_particle_restitution_bit_exact(cuda):
     # restitution changed the trajectory
     s2, _, _ = _gpu_run(model, 24, q0, qd0, restitution=False)
     assert not torch.equal(s.particle_qd, s2.particle_qd)
+
+
+def _soft_block(cuda):
+    """A 3 x 3 x 3 lattice of particles cut into 5 tetrahedra per cube, dropped tilted onto the ground."""
+    from newton_custom_contact_b200 import ModelBuilder
+
+    b = ModelBuilder()
+    b.add_ground_plane()
+    n, h = 3, 0.05
+    idx = {}
+    for i in range(n):
+        for j in range(n):
+            for k in range(n):
+                p = (i * h + 0.3 * k * h, j * h, 0.08 + k * h + 0.2 * i * h)
+                idx[i, j, k] = b.add_particle(p, (0.0, 0.0, -0.5), 0.02, radius=0.01)
+    for i in range(n - 1):
+        for j in range(n - 1):
+            for k in range(n - 1):
+                c = [idx[i + (v & 1), j + ((v >> 1) & 1), k + ((v >> 2) & 1)] for v in range(8)]
+                for t in ((0, 1, 2, 4), (1, 3, 2, 7), (1, 4, 5, 7), (2, 7, 6, 4), (1, 2, 4, 7)):
+                    a, bb, cc, d = (c[x] for x in t)
+                    if b.add_tetrahedron(a, bb, cc, d, 1e3, 1e3) <= 0:
+                        b.add_tetrahedron(a, cc, bb, d, 1e3, 1e3)
+    return b.finalize(device=cuda)
+
+
+def test_tetrahedral_block_bit_exact(cuda):
+    model = _soft_block(cuda)
+    assert model.tet_count == 40
+    s, solver, pipe = _gpu_run(model, 48)
+    q, qd = model.host("particle_q").copy(), model.host("particle_qd").copy()
+    for _ in range(48):
+        soft = op.soft_collide(model._host, q, None, pipe.soft_contact_margin, pipe.soft_contact_max)
+        q, qd = op.step(model._host, particles.params(model), q, qd, None, soft, DT, ITERS, 0.9,
+                        soft_body_relaxation=solver.soft_body_relaxation)
+    assert np.array_equal(_bits(s.particle_q.cpu().numpy()), _bits(q))
+    assert np.array_equal(_bits(s.particle_qd.cpu().numpy()), _bits(qd))
+    assert float(q[:, 2].min()) < 0.02  # it reached the ground

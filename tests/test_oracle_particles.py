@@ -237,3 +237,29 @@ def test_restitution_bounce_off_the_ground():
     assert qd1[0, 2] == pytest.approx(1.0, rel=1e-5)  # 0.5 x 2 m/s, upwards
     _, qd0 = op.step(m._host, particles.params(m), q, qd, None, soft, dt, 4, 0.9, restitution=False)
     assert qd0[0, 2] < 0.5  # without restitution it leaves at the projection speed only
+
+
+def test_compressed_tetrahedron_recovers_its_volume():
+    """solve_tetrahedra (kernels.py:459-628): a tet squashed to 60 % height regains volume; no net momentum."""
+
+    def build(b):
+        for p in ((0, 0, 0), (0.1, 0, 0), (0, 0.1, 0), (0, 0, 0.1)):
+            b.add_particle(p, (0, 0, 0), 0.01, radius=0.005)
+        assert b.add_tetrahedron(0, 1, 2, 3) == pytest.approx(0.1 ** 3 / 6)
+
+    m = _model(build)
+    assert m.tet_count == 1
+    m._host["gravity"] = np.zeros((1, 3), F)
+    q = m.host("particle_q").copy()
+    q[3, 2] = 0.06
+    qd = m.host("particle_qd")
+
+    def vol(q):
+        return float(np.linalg.det(np.stack([q[1] - q[0], q[2] - q[0], q[3] - q[0]], axis=1)) / 6)
+
+    v0 = vol(q)
+    for _ in range(30):
+        q, qd = op.step(m._host, particles.params(m), q, qd, None, None, 1.0 / 240.0, 8, 0.9,
+                        soft_body_relaxation=1e-6)
+    assert vol(q) > v0 + 0.5 * (0.1 ** 3 / 6 - v0)
+    assert np.abs(qd.sum(axis=0)).max() < 1e-3
