@@ -277,7 +277,11 @@ __global__ void __launch_bounds__(kThreads) particle_integrate_kernel(NbParticle
 // order, then adds the soft contacts and springs.  Which lane computes a contribution does not change
 // its bits, so the result equals a sequential sum in ascending neighbour index.  The kernel also
 // clears the cell table the following apply fills.
-constexpr int kGroup = 8;
+#ifndef NB_PARTICLE_GROUP
+#define NB_PARTICLE_GROUP 8
+#endif
+constexpr int kGroup = NB_PARTICLE_GROUP;  // lanes per particle: 2, 4, 8 or 16
+static_assert(kGroup >= 2 && kGroup <= 16 && (kGroup & (kGroup - 1)) == 0, "lanes per particle");
 constexpr int kSlots = kThreads / kGroup;  // particles per block
 
 __global__ void __launch_bounds__(kThreads) particle_constraints_kernel(NbParticleDesc pd, NbParticleIO io,
@@ -293,7 +297,7 @@ __global__ void __launch_bounds__(kThreads) particle_constraints_kernel(NbPartic
     }
     const int lane = threadIdx.x & (kGroup - 1);
     const int slot = threadIdx.x / kGroup;
-    const unsigned gmask = 0xffu << (threadIdx.x & 31 & ~(kGroup - 1));
+    const unsigned gmask = ((1u << kGroup) - 1u) << (threadIdx.x & 31 & ~(kGroup - 1));
     const int i = blockIdx.x * kSlots + slot;
     const bool valid = i < pd.particle_count;
     const bool act = valid && active(pd, i);
